@@ -1,0 +1,325 @@
+"""MeshBVH: the mesh query object (drop-in for atom3d.core.mesh_bvh.MeshBVH).
+
+Keeps the reference's constructor and query signatures
+(atom3d/core/mesh_bvh.py:59-117, :297-335, :601-757) while every
+computation runs in libatom3d_b200.so on the GPU:
+
+* construction: pseudo-normal precompute (a3d_mesh_normals) and the GPU
+  wide-BVH build (a3d_bvh_build) instead of the reference's host SAH build;
+* ``udf`` / ``sdf``: one fused traversal launch (a3d_udf), sign included;
+* ``udf(return_grad=True)``: a torch.autograd.Function whose backward is the
+  hand-written adjoint kernel (a3d_udf_backward) for points and vertices;
+* ``intersect_aabb(mode=0)``: SAT any-hit over the BVH (a3d_aabb_hit).
+
+There is no CPU path: a CPU device raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Union
+
+import torch
+
+from .. import _lib
+from .data_structures import AABBIntersectResult, ClosestPointResult
+from .device_utils import resolve_device
+
+
+class WideBVH:
+    """Device-resident 4-wide quantised BVH (64-B nodes, 48-B triangle records)."""
+
+    def __init__(self, vertices: torch.Tensor, faces: torch.Tensor):
+        _lib.require_cuda(vertices, "vertices")
+        dev = vertices.device
+        v = vertices.detach().contiguous().float()
+        f = faces.contiguous().int()
+        nf = int(f.shape[0])
+        if nf == 0:
+            raise ValueError("MeshBVH needs at least one face")
+        self.device = dev
+        self.num_tris = nf
+        cap = max(nf, 1)
+        with torch.cuda.device(dev):
+            nodes = torch.empty(cap * 64 + 64, dtype=torch.uint8, device=dev)
+            off = (-nodes.data_ptr()) % 64
+            nodes = nodes[off:off + cap * 64]
+            tris = torch.empty(nf * 48, dtype=torch.uint8, device=dev)
+            ws = _lib.workspace(_lib.lib().a3d_bvh_build_workspace_bytes(nf), dev)
+            nn = ctypes.c_int64(0)
+            bounds = (ctypes.c_float * 6)()
+            _lib.call(
+                "a3d_bvh_build", v.data_ptr(), v.shape[0], f.data_ptr(), nf, nodes.data_ptr(), cap,
+                tris.data_ptr(), ws.data_ptr(), ws.numel(), ctypes.byref(nn), bounds, _lib.stream_ptr(dev),
+            )
+        self.num_nodes = int(nn.value)
+        self.nodes = nodes[: self.num_nodes * 64]
+        self.tris = tris
+        self.lo = [bounds[0], bounds[1], bounds[2]]
+        self.hi = [bounds[3], bounds[4], bounds[5]]
+        self._view = _lib.BvhView(
+            self.nodes.data_ptr(), self.tris.data_ptr(), self.num_nodes, self.num_tris,
+            (ctypes.c_float * 3)(*self.lo), (ctypes.c_float * 3)(*self.hi),
+        )
+
+    @property
+    def view(self) -> _lib.BvhView:
+        return self._view
+
+    def query(self, points: torch.Tensor, sign: Optional[_lib.SignData] = None, bound: Optional[torch.Tensor] = None,
+              want_uvw: bool = True, stats: Optional[torch.Tensor] = None, sort_queries: bool = True):
+        """Raw closest-point query: (distances, face_ids int32, closest [N,3], uvw [N,3] or None)."""
+        _lib.require_cuda(points, "points")
+        p = points.detach().contiguous().float()
+        n = int(p.shape[0])
+        dev = self.device
+        dist = torch.empty(n, dtype=torch.float32, device=dev)
+        fid = torch.empty(n, dtype=torch.int32, device=dev)
+        cp = torch.empty(n, 3, dtype=torch.float32, device=dev)
+        uvw = torch.empty(n, 3, dtype=torch.float32, device=dev) if want_uvw else None
+        if n == 0:
+            return dist, fid, cp, uvw
+        flags = _lib.A3D_UDF_SORT_QUERIES if sort_queries else 0
+        ws = _lib.workspace(_lib.lib().a3d_udf_workspace_bytes(n, flags), dev)
+        b = None
+        if bound is not None:
+            b = bound.detach().contiguous().float()
+            if b.shape[0] != n:
+                raise ValueError("bound must have one entry per query")
+        _lib.call(
+            "a3d_udf", ctypes.byref(self._view), p.data_ptr(), n, dist.data_ptr(), fid.data_ptr(), cp.data_ptr(),
+            _lib.ptr(uvw), ctypes.byref(sign) if sign is not None else None, _lib.ptr(b), _lib.ptr(stats), flags,
+            ws.data_ptr(), ws.numel(), _lib.stream_ptr(dev),
+        )
+        return dist, fid, cp, uvw
+
+
+class _DistanceFn(torch.autograd.Function):
+    """dist(points, vertices) with the hand-written adjoint kernel.
+
+    Forward runs the (optionally signed) closest-point query; backward calls
+    a3d_udf_backward: d|p-c|/dp = (p-c)/|p-c| and, by the envelope theorem,
+    d|p-c|/dv_i = -w_i (p-c)/|p-c| with w the closest point's barycentrics.
+    """
+
+    @staticmethod
+    def forward(ctx, points, vertices, mesh, sign_flag, bound):
+        dist, fid, cp, uvw = mesh._bvh.query(points, sign=mesh._sign_data() if sign_flag else None, bound=bound)
+        ctx.mesh = mesh
+        ctx.save_for_backward(points, cp, fid, uvw, dist)
+        ctx.mark_non_differentiable(fid, cp, uvw)
+        return dist, fid, cp, uvw
+
+    @staticmethod
+    def backward(ctx, g_dist, _g_fid, _g_cp, _g_uvw):
+        points, cp, fid, uvw, dist = ctx.saved_tensors
+        mesh = ctx.mesh
+        need_p, need_v = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        if g_dist is None or not (need_p or need_v):
+            return None, None, None, None, None
+        # signed distance = sign * |p - c|: fold the sign into the incoming grad
+        g = (g_dist * torch.where(dist < 0, -1.0, 1.0)).contiguous().float()
+        n = points.shape[0]
+        gp = torch.empty(n, 3, dtype=torch.float32, device=points.device) if need_p else None
+        gv = torch.zeros_like(mesh.vertices, dtype=torch.float32) if need_v else None
+        _lib.call(
+            "a3d_udf_backward", points.detach().contiguous().float().data_ptr(), n, cp.data_ptr(), fid.data_ptr(),
+            uvw.data_ptr(), g.data_ptr(), mesh.faces.data_ptr(), _lib.ptr(gp), _lib.ptr(gv),
+            _lib.stream_ptr(points.device),
+        )
+        if gp is not None:
+            gp = gp.to(points.dtype)
+        return gp, gv, None, None, None
+
+
+class MeshBVH:
+    """Mesh with a GPU wide BVH; closest-point, signed-distance and box queries.
+
+    Args:
+        vertices: [V, 3] vertex coordinates
+        faces: [F, 3] vertex indices
+        device: compute device (must resolve to CUDA)
+        face_normals: optional [F, 3] normals used by the sign test
+        vertex_normals: optional [V, 3] vertex normals (then the sign uses
+            face normals only, like the reference)
+    """
+
+    def __init__(
+        self,
+        vertices: torch.Tensor,
+        faces: torch.Tensor,
+        device: Optional[Union[str, torch.device]] = None,
+        face_normals: Optional[torch.Tensor] = None,
+        vertex_normals: Optional[torch.Tensor] = None,
+    ):
+        dev = resolve_device(vertices, faces, device=device, default="cuda")
+        if dev.type != "cuda":
+            raise RuntimeError(
+                f"MeshBVH runs on CUDA only (resolved device {dev}); there is no CPU fallback"
+            )
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        self.vertices = vertices.to(dev).float()
+        self.faces = faces.to(dev).int().contiguous()
+        self.num_vertices = int(self.vertices.shape[0])
+        self.num_faces = int(self.faces.shape[0])
+        vd = self.vertices.detach()
+        self._bounds = torch.stack([vd.min(dim=0)[0], vd.max(dim=0)[0]])
+        self._is_cuda = True
+        self._edge_pn = None
+        self._he_edge_idx = None
+        self._face_angles = None
+        self._precompute_normals()
+        if face_normals is not None:
+            self._face_normals = face_normals.to(dev).float().contiguous()
+        if vertex_normals is not None:
+            self._vertex_pn = vertex_normals.to(dev).float().contiguous()
+            self._edge_pn = None
+            self._he_edge_idx = None
+            self._face_angles = None
+        self._vertex_normals = self._vertex_pn
+        self._bvh = WideBVH(vd, self.faces)
+        self._sign_cache = None
+
+    # ------------------------------------------------------------------ setup
+    def _precompute_normals(self) -> None:
+        dev = self.device
+        nv, nf = self.num_vertices, self.num_faces
+        v = self.vertices.detach().contiguous()
+        fn = torch.empty(nf, 3, dtype=torch.float32, device=dev)
+        ang = torch.empty(nf, 3, dtype=torch.float32, device=dev)
+        vpn = torch.empty(nv, 3, dtype=torch.float32, device=dev)
+        epn = torch.empty(3 * nf, 3, dtype=torch.float32, device=dev)
+        he = torch.empty(3 * nf, dtype=torch.int64, device=dev)
+        ne = ctypes.c_int64(0)
+        ws = _lib.workspace(_lib.lib().a3d_mesh_normals_workspace_bytes(nv, nf), dev)
+        _lib.call(
+            "a3d_mesh_normals", v.data_ptr(), nv, self.faces.data_ptr(), nf, fn.data_ptr(), ang.data_ptr(),
+            vpn.data_ptr(), epn.data_ptr(), 3 * nf, he.data_ptr(), ctypes.byref(ne), ws.data_ptr(), ws.numel(),
+            _lib.stream_ptr(dev),
+        )
+        self._face_normals = fn
+        self._face_angles = ang
+        self._vertex_pn = vpn
+        self._edge_pn = epn[: int(ne.value)]
+        self._he_edge_idx = he
+
+    def _sign_data(self) -> _lib.SignData:
+        key = (id(self._face_normals), id(self._vertex_pn), id(self._edge_pn))
+        if self._sign_cache is None or self._sign_cache[0] != key:
+            face_only = self._edge_pn is None or self._he_edge_idx is None
+            sd = _lib.SignData(
+                self._face_normals.data_ptr(),
+                None if face_only else self._vertex_pn.data_ptr(),
+                None if face_only else self._edge_pn.data_ptr(),
+                None if face_only else self._he_edge_idx.data_ptr(),
+                self.faces.data_ptr(),
+            )
+            self._sign_cache = (key, sd)
+        return self._sign_cache[1]
+
+    # ------------------------------------------------------------- properties
+    def get_bounds(self) -> torch.Tensor:
+        return self._bounds
+
+    def get_face_normals(self) -> torch.Tensor:
+        return self._face_normals
+
+    def get_vertex_normals(self) -> Optional[torch.Tensor]:
+        return self._vertex_normals
+
+    def get_face_aabb(self, face_indices: Optional[torch.Tensor] = None):
+        f = self.faces if face_indices is None else self.faces[face_indices]
+        tv = self.vertices.detach()[f.long()]
+        return tv.min(dim=1)[0], tv.max(dim=1)[0]
+
+    # ------------------------------------------------------------ box queries
+    def intersect_aabb(self, aabb_min: torch.Tensor, aabb_max: torch.Tensor, mode: int = 1) -> AABBIntersectResult:
+        """Triangle/box intersection.  mode 0: SAT hit mask (sat_eps 1e-6).
+
+        Pair outputs (modes 1-3, polygon clipping) are not provided by this
+        build and raise NotImplementedError.
+        """
+        if mode != 0:
+            raise NotImplementedError("intersect_aabb: only mode=0 (hit mask) is provided by atom3d_b200")
+        return AABBIntersectResult(hit=self.aabb_hit(aabb_min, aabb_max))
+
+    def aabb_hit(self, aabb_min: torch.Tensor, aabb_max: torch.Tensor) -> torch.Tensor:
+        _lib.require_cuda(aabb_min, "aabb_min")
+        mn = aabb_min.detach().contiguous().float()
+        mx = aabb_max.detach().contiguous().float()
+        n = int(mn.shape[0])
+        hit = torch.zeros(n, dtype=torch.bool, device=self.device)
+        if n == 0:
+            return hit
+        ws = _lib.workspace(_lib.lib().a3d_aabb_hit_workspace_bytes(n), self.device)
+        _lib.call(
+            "a3d_aabb_hit", ctypes.byref(self._bvh.view), mn.data_ptr(), mx.data_ptr(), n, hit.data_ptr(),
+            ws.data_ptr(), ws.numel(), _lib.stream_ptr(self.device),
+        )
+        return hit
+
+    # -------------------------------------------------------- distance queries
+    def udf(
+        self,
+        points: torch.Tensor,
+        return_grad: bool = False,
+        return_closest: bool = False,
+        return_uvw: bool = False,
+        return_face_ids: bool = False,
+        bound: Optional[torch.Tensor] = None,
+    ) -> Union[torch.Tensor, ClosestPointResult]:
+        """Unsigned distance (reference: atom3d/core/mesh_bvh.py:601-648).
+
+        ``bound`` (extension): per-query upper bound on the distance used to
+        seed the pruning radius; results are identical with or without it.
+        """
+        result = self._udf_with_grad(points, bound=bound) if return_grad else self._udf_query(points, bound=bound)
+        return self._filter(result, return_closest, return_uvw, return_face_ids)
+
+    def sdf(
+        self,
+        points: torch.Tensor,
+        mode: str = "pseudo_normal",
+        return_grad: bool = False,
+        return_closest: bool = False,
+        return_uvw: bool = False,
+        return_face_ids: bool = False,
+        bound: Optional[torch.Tensor] = None,
+        **kwargs,
+    ) -> Union[torch.Tensor, ClosestPointResult]:
+        """Signed distance with the Baerentzen-Aanaes pseudo-normal sign
+        (reference: atom3d/core/mesh_bvh.py:702-827), fused into the query."""
+        if mode != "pseudo_normal":
+            raise NotImplementedError(f"sdf mode {mode!r} is not provided by atom3d_b200 (use 'pseudo_normal')")
+        if return_grad:
+            result = self._udf_with_grad(points, sign=True, bound=bound)
+        else:
+            result = self._udf_query(points, sign=True, bound=bound)
+        return self._filter(result, return_closest, return_uvw, return_face_ids)
+
+    @staticmethod
+    def _filter(result: ClosestPointResult, closest: bool, uvw: bool, fids: bool):
+        if not (closest or uvw or fids):
+            return result.distances
+        if not closest:
+            result.closest_points = None
+        if not uvw:
+            result.uvw = None
+        if not fids:
+            result.face_ids = None
+        return result
+
+    def _udf_query(self, points: torch.Tensor, sign: bool = False, bound: Optional[torch.Tensor] = None):
+        dist, fid, cp, uvw = self._bvh.query(points, sign=self._sign_data() if sign else None, bound=bound)
+        return ClosestPointResult(distances=dist, face_ids=fid, closest_points=cp, uvw=uvw)
+
+    def _udf_with_grad(self, points: torch.Tensor, sign: bool = False, bound: Optional[torch.Tensor] = None):
+        dist, fid, cp, uvw = _DistanceFn.apply(points, self.vertices, self, sign, bound)
+        return ClosestPointResult(distances=dist, face_ids=fid, closest_points=cp.detach(), uvw=uvw)
+
+    def _compute_sign(self, points: torch.Tensor, closest_points=None, face_ids=None, uvw=None) -> torch.Tensor:
+        """Sign (+1/-1) of the signed distance at ``points`` (fused kernel)."""
+        d = self._udf_query(points, sign=True).distances
+        return torch.where(d < 0, -1.0, 1.0)

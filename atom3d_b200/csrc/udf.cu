@@ -1,0 +1,499 @@
+// Closest-triangle queries over the wide BVH: UDF, fused pseudo-normal SDF
+// sign, learned-bound seeding, and the distance adjoints.
+//
+// Replaces bvh_udf_kernel (atom3d/kernels/bvh_kernels.cu:363-463) and the
+// PyTorch sign gathers of MeshBVH._compute_sign (atom3d/core/mesh_bvh.py:
+// 759-827).  Design:
+//   * queries are Morton-sorted (30-bit key, in-house radix sort) so a warp
+//     walks neighbouring regions of the tree together;
+//   * one 64-B node = four 16-B loads; the four child boxes are decoded from
+//     8-bit offsets, sorted by distance with a 5-exchange network, the
+//     nearest qualifying child is visited next and the others pushed;
+//   * the traversal stack lives in shared memory ([depth][thread] layout, no
+//     bank conflicts); a query that would overflow it is re-run by a
+//     fallback launch with a deep local-memory stack, never truncated;
+//   * a per-query bound (learned upper bound on the distance) seeds the
+//     pruning radius; a query whose bound proves too small is re-run
+//     without it, so results are identical with and without the bound.
+#include <math.h>
+
+#include "bvh_layout.cuh"
+#include "primitives.cuh"
+#include "tri_math.cuh"
+
+namespace a3d {
+
+namespace {
+
+constexpr int kUdfThreads = 128;
+constexpr int kSharedDepth = 24;
+constexpr int kDeepDepth = 256;
+
+struct SignArgs {
+  const float* face_normals;
+  const float* vertex_pn;
+  const float* edge_pn;
+  const int64_t* he_edge_idx;
+  const int32_t* faces;
+};
+
+struct QueryOut {
+  float* dist;
+  int32_t* fid;
+  float* cp;
+  float* uvw;
+};
+
+struct Counters {
+  unsigned long long nodes;
+  unsigned long long tris;
+};
+
+__device__ __forceinline__ void cswap(float& da, uint32_t& ra, float& db, uint32_t& rb) {
+  if (db < da) {
+    float t = da; da = db; db = t;
+    uint32_t u = ra; ra = rb; rb = u;
+  }
+}
+
+__device__ __forceinline__ float box_dist_sq(float px, float py, float pz, float lx, float ly, float lz, float hx,
+                                             float hy, float hz) {
+  const float dx = fmaxf(fmaxf(lx - px, px - hx), 0.f);
+  const float dy = fmaxf(fmaxf(ly - py, py - hy), 0.f);
+  const float dz = fmaxf(fmaxf(lz - pz, pz - hz), 0.f);
+  return dx * dx + dy * dy + dz * dz;
+}
+
+__device__ __forceinline__ float tri_dist_sq(const TriRec& t, float px, float py, float pz) {
+  if (__float_as_uint(t.b.w) & kTriFlagNearDegenerate) {
+    const V3<double> p = mk<double>(px, py, pz);
+    const double d = TriEval<double>::dist_sq(p, mk<double>(t.a.x, t.a.y, t.a.z), mk<double>(t.b.x, t.b.y, t.b.z),
+                                              mk<double>(t.c.x, t.c.y, t.c.z));
+    return (float)d;
+  }
+  return TriEval<float>::dist_sq(mk(px, py, pz), mk(t.a.x, t.a.y, t.a.z), mk(t.b.x, t.b.y, t.b.z),
+                                 mk(t.c.x, t.c.y, t.c.z));
+}
+
+__device__ __forceinline__ TriRec load_tri(const TriRec* tris, uint32_t i) {
+  const float4* p = reinterpret_cast<const float4*>(tris + i);
+  TriRec r;
+  r.a = __ldg(p);
+  r.b = __ldg(p + 1);
+  r.c = __ldg(p + 2);
+  return r;
+}
+
+// Stack in shared memory, [depth][blockDim] layout.
+struct SharedStack {
+  uint2* base;  // points at s[0][threadIdx.x]
+  int sp;
+  static constexpr int kDepth = kSharedDepth;
+  __device__ __forceinline__ void push(uint32_t ref, float d) {
+    base[sp * kUdfThreads] = make_uint2(ref, __float_as_uint(d));
+    ++sp;
+  }
+  __device__ __forceinline__ uint2 pop() {
+    --sp;
+    return base[sp * kUdfThreads];
+  }
+};
+
+struct LocalStack {
+  uint2 s[kDeepDepth];
+  int sp;
+  static constexpr int kDepth = kDeepDepth;
+  __device__ __forceinline__ void push(uint32_t ref, float d) { s[sp++] = make_uint2(ref, __float_as_uint(d)); }
+  __device__ __forceinline__ uint2 pop() { return s[--sp]; }
+};
+
+// Core traversal.  Returns false when the stack would overflow (result then
+// invalid).  best_sq: in = initial pruning radius^2, out = best distance^2.
+template <typename Stack>
+__device__ __forceinline__ bool traverse(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
+                                         float px, float py, float pz, Stack& st, float& best_sq,
+                                         uint32_t& best_tri, Counters& ctr) {
+  uint32_t ref = 0;  // root is internal node 0 (a single-leaf tree still has a root node)
+  bool have = true;
+  for (;;) {
+    if (have) {
+      if (!ref_is_leaf(ref)) {
+        ++ctr.nodes;
+        const int4* np = reinterpret_cast<const int4*>(nodes + ref);
+        const int4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3);
+        const float ox = __int_as_float(w0.x), oy = __int_as_float(w0.y), oz = __int_as_float(w0.z);
+        const uint32_t meta = (uint32_t)w0.w;
+        const float sx = __uint_as_float((meta & 0xffu) << 23);
+        const float sy = __uint_as_float(((meta >> 8) & 0xffu) << 23);
+        const float sz = __uint_as_float(((meta >> 16) & 0xffu) << 23);
+        const uint32_t qlx = (uint32_t)w1.x, qly = (uint32_t)w1.y, qlz = (uint32_t)w1.z;
+        const uint32_t qhx = (uint32_t)w1.w, qhy = (uint32_t)w2.x, qhz = (uint32_t)w2.y;
+        float d[4];
+        uint32_t r[4] = {(uint32_t)w2.z, (uint32_t)w2.w, (uint32_t)w3.x, (uint32_t)w3.y};
+        const int nch = (int)(meta >> 24);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int sh = 8 * c;
+          const float lx = fmaf((float)((qlx >> sh) & 0xffu), sx, ox);
+          const float ly = fmaf((float)((qly >> sh) & 0xffu), sy, oy);
+          const float lz = fmaf((float)((qlz >> sh) & 0xffu), sz, oz);
+          const float hx = fmaf((float)((qhx >> sh) & 0xffu), sx, ox);
+          const float hy = fmaf((float)((qhy >> sh) & 0xffu), sy, oy);
+          const float hz = fmaf((float)((qhz >> sh) & 0xffu), sz, oz);
+          d[c] = c < nch ? box_dist_sq(px, py, pz, lx, ly, lz, hx, hy, hz) : INFINITY;
+        }
+        cswap(d[0], r[0], d[1], r[1]);
+        cswap(d[2], r[2], d[3], r[3]);
+        cswap(d[0], r[0], d[2], r[2]);
+        cswap(d[1], r[1], d[3], r[3]);
+        cswap(d[1], r[1], d[2], r[2]);
+        int q = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) q += d[c] < best_sq ? 1 : 0;
+        if (q > 0) {
+          if (st.sp + (q - 1) > Stack::kDepth) return false;
+#pragma unroll
+          for (int c = 3; c >= 1; --c)
+            if (c < q) st.push(r[c], d[c]);
+          ref = r[0];
+          continue;
+        }
+      } else {
+        const uint32_t f0 = leaf_first(ref), cnt = leaf_count(ref);
+        for (uint32_t i = 0; i < cnt; ++i) {
+          const TriRec t = load_tri(tris, f0 + i);
+          ++ctr.tris;
+          const float dsq = tri_dist_sq(t, px, py, pz);
+          if (dsq < best_sq) {
+            best_sq = dsq;
+            best_tri = f0 + i;
+          }
+        }
+      }
+    }
+    // pop the next candidate that can still beat best_sq
+    have = false;
+    while (st.sp > 0) {
+      const uint2 e = st.pop();
+      if (__uint_as_float(e.y) < best_sq) {
+        ref = e.x;
+        have = true;
+        break;
+      }
+    }
+    if (!have) return true;
+  }
+}
+
+__device__ __forceinline__ void finish_query(const TriRec* __restrict__ tris, uint32_t best_tri, float best_sq,
+                                             float px, float py, float pz, int64_t qi, const QueryOut& out,
+                                             const SignArgs& sg, bool do_sign) {
+  float cx = px, cy = py, cz = pz;
+  int32_t face = -1;
+  float u = 0.f, v = 0.f, w = 0.f;
+  float dist = sqrtf(best_sq);
+  if (best_tri != 0xffffffffu) {
+    const TriRec t = load_tri(tris, best_tri);
+    face = __float_as_int(t.a.w);
+    const V3<float> a = mk(t.a.x, t.a.y, t.a.z), b = mk(t.b.x, t.b.y, t.b.z), c = mk(t.c.x, t.c.y, t.c.z);
+    const V3<float> p = mk(px, py, pz);
+    V3<float> cp;
+    if (__float_as_uint(t.b.w) & kTriFlagNearDegenerate) {
+      const V3<double> cd = TriEval<double>::closest(mk<double>(px, py, pz), mk<double>(a.x, a.y, a.z),
+                                                     mk<double>(b.x, b.y, b.z), mk<double>(c.x, c.y, c.z));
+      cp = mk((float)cd.x, (float)cd.y, (float)cd.z);
+    } else {
+      cp = TriEval<float>::closest(p, a, b, c);
+    }
+    cx = cp.x; cy = cp.y; cz = cp.z;
+    const V3<float> bc = TriEval<float>::bary(cp, a, b, c);
+    u = bc.x; v = bc.y; w = bc.z;
+    if (do_sign) {
+      // Baerentzen-Aanaes pseudo-normal selected from the barycentrics
+      const float eps = 1e-4f;
+      const bool z0 = u < eps, z1 = v < eps, z2 = w < eps;
+      const int nz = (int)z0 + (int)z1 + (int)z2;
+      const float* nrm = sg.face_normals + 3 * (int64_t)face;
+      if (sg.edge_pn == nullptr) {
+        // face normals only (caller supplied vertex normals)
+      } else if (nz == 2) {
+        const int dom = !z0 ? 0 : (!z1 ? 1 : 2);
+        const int64_t vid = sg.faces[3 * (int64_t)face + dom];
+        nrm = sg.vertex_pn + 3 * vid;
+      } else if (nz == 1) {
+        const int zi = z0 ? 0 : (z1 ? 1 : 2);
+        const int he = zi == 0 ? 1 : (zi == 1 ? 2 : 0);
+        const int64_t eid = sg.he_edge_idx[3 * (int64_t)face + he];
+        nrm = sg.edge_pn + 3 * eid;
+      }
+      const float nx = __ldg(nrm), ny = __ldg(nrm + 1), nzv = __ldg(nrm + 2);
+      float s;
+      if (dist < 1e-3f) {
+        // near the surface the sign is decided in FP64 from an FP64 closest point
+        const V3<double> cd = TriEval<double>::closest(mk<double>(px, py, pz), mk<double>(a.x, a.y, a.z),
+                                                       mk<double>(b.x, b.y, b.z), mk<double>(c.x, c.y, c.z));
+        const double dd = ((double)px - cd.x) * nx + ((double)py - cd.y) * ny + ((double)pz - cd.z) * nzv;
+        s = dd < 0.0 ? -1.f : 1.f;
+      } else {
+        const float dd = (px - cx) * nx + (py - cy) * ny + (pz - cz) * nzv;
+        s = dd < 0.f ? -1.f : 1.f;
+      }
+      dist *= s;
+    }
+  }
+  out.dist[qi] = dist;
+  out.fid[qi] = face;
+  out.cp[3 * qi] = cx;
+  out.cp[3 * qi + 1] = cy;
+  out.cp[3 * qi + 2] = cz;
+  if (out.uvw && best_tri != 0xffffffffu) {
+    out.uvw[3 * qi] = u;
+    out.uvw[3 * qi + 1] = v;
+    out.uvw[3 * qi + 2] = w;
+  }
+}
+
+__device__ __forceinline__ void flush_counters(const Counters& c, unsigned long long* stats) {
+  unsigned long long a = warp_reduce_sum(c.nodes), b = warp_reduce_sum(c.tris);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(stats, a);
+    atomicAdd(stats + 1, b);
+  }
+}
+
+// queries in [0, n): perm maps the launch index to the query index
+template <bool kSign, bool kStats>
+__global__ void __launch_bounds__(kUdfThreads)
+    udf_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris, const float* __restrict__ pts,
+               int64_t n, const uint32_t* __restrict__ perm, const float* __restrict__ bound, QueryOut out,
+               SignArgs sg, unsigned long long* stats, uint32_t* __restrict__ rerun, uint32_t* __restrict__ nrerun) {
+  __shared__ uint2 s_stack[kSharedDepth * kUdfThreads];
+  const int64_t t = (int64_t)blockIdx.x * kUdfThreads + threadIdx.x;
+  Counters ctr{0, 0};
+  if (t < n) {
+    const int64_t qi = perm ? (int64_t)perm[t] : t;
+    const float px = pts[3 * qi], py = pts[3 * qi + 1], pz = pts[3 * qi + 2];
+    float best_sq = INFINITY;
+    if (bound) {
+      const float b = bound[qi];
+      best_sq = b * b;
+      if (!(best_sq >= 0.f)) best_sq = INFINITY;
+    }
+    uint32_t best_tri = 0xffffffffu;
+    SharedStack st{s_stack + threadIdx.x, 0};
+    const bool ok = traverse(nodes, tris, px, py, pz, st, best_sq, best_tri, ctr);
+    if (!ok || best_tri == 0xffffffffu) {
+      // stack overflow, or the bound excluded every triangle: exact re-run
+      const uint32_t slot = atomicAdd(nrerun, 1u);
+      rerun[slot] = (uint32_t)qi;
+    } else {
+      finish_query(tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
+    }
+  }
+  if (kStats) flush_counters(ctr, stats);
+}
+
+template <bool kSign, bool kStats>
+__global__ void __launch_bounds__(64)
+    udf_rerun_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
+                     const float* __restrict__ pts, const uint32_t* __restrict__ rerun,
+                     const uint32_t* __restrict__ nrerun, QueryOut out, SignArgs sg, unsigned long long* stats,
+                     int* __restrict__ overflow) {
+  const uint32_t m = *nrerun;
+  Counters ctr{0, 0};
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t qi = rerun[t];
+    const float px = pts[3 * qi], py = pts[3 * qi + 1], pz = pts[3 * qi + 2];
+    float best_sq = INFINITY;
+    uint32_t best_tri = 0xffffffffu;
+    LocalStack st;
+    st.sp = 0;
+    if (!traverse(nodes, tris, px, py, pz, st, best_sq, best_tri, ctr)) atomicExch(overflow, 1);
+    finish_query(tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
+  }
+  if (kStats) {
+    // counters only for threads of full warps; partial warps add directly
+    atomicAdd(stats, ctr.nodes);
+    atomicAdd(stats + 1, ctr.tris);
+  }
+}
+
+__global__ void query_morton_kernel(const float* __restrict__ pts, int64_t n, float lox, float loy, float loz,
+                                    float ix, float iy, float iz, uint32_t* __restrict__ keys,
+                                    uint32_t* __restrict__ vals) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float q[3] = {(pts[3 * i] - lox) * ix, (pts[3 * i + 1] - loy) * iy, (pts[3 * i + 2] - loz) * iz};
+  uint32_t code = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float t = fminf(fmaxf(q[a], 0.f), 1023.f);
+    if (!(t == t)) t = 0.f;
+    code |= (uint32_t)spread3_21((uint64_t)t) << a;
+  }
+  keys[i] = code;
+  vals[i] = (uint32_t)i;
+}
+
+struct UdfWs {
+  uint32_t* keys;
+  uint32_t* keys_alt;
+  uint32_t* vals;
+  uint32_t* vals_alt;
+  uint32_t* rs_scratch;
+  uint32_t* rerun;
+  uint32_t* nrerun;  // [0] rerun count, [1] overflow flag
+};
+
+size_t carve_udf(UdfWs& w, Workspace& ws, int64_t n, uint32_t flags) {
+  if (flags & A3D_UDF_SORT_QUERIES) {
+    w.keys = ws.take<uint32_t>(n);
+    w.keys_alt = ws.take<uint32_t>(n);
+    w.vals = ws.take<uint32_t>(n);
+    w.vals_alt = ws.take<uint32_t>(n);
+    w.rs_scratch = ws.take<uint32_t>((int64_t)radix_sort_scratch_elems(n));
+  } else {
+    w.keys = w.keys_alt = w.vals = w.vals_alt = w.rs_scratch = nullptr;
+  }
+  w.rerun = ws.take<uint32_t>(n);
+  w.nrerun = ws.take<uint32_t>(4);
+  return ws.used;
+}
+
+template <bool kSign, bool kStats>
+int launch_udf(const a3d_bvh_view* bvh, const float* pts, int64_t n, const uint32_t* perm, const float* bound,
+               const QueryOut& out, const SignArgs& sg, unsigned long long* stats, UdfWs& w, cudaStream_t s) {
+  const WideNode* nodes = (const WideNode*)bvh->nodes;
+  const TriRec* tris = (const TriRec*)bvh->tris;
+  udf_kernel<kSign, kStats><<<(unsigned)ceil_div(n, kUdfThreads), kUdfThreads, 0, s>>>(
+      nodes, tris, pts, n, perm, bound, out, sg, stats, w.rerun, w.nrerun);
+  A3D_LAUNCH_CHECK();
+  udf_rerun_kernel<kSign, kStats><<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, pts, w.rerun, w.nrerun, out, sg, stats,
+                                                            (int*)(w.nrerun + 1));
+  A3D_LAUNCH_CHECK();
+  return A3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// adjoints
+// ---------------------------------------------------------------------------
+__global__ void udf_backward_kernel(const float* __restrict__ pts, int64_t n, const float* __restrict__ cp,
+                                    const int32_t* __restrict__ fid, const float* __restrict__ uvw,
+                                    const float* __restrict__ gd, const int32_t* __restrict__ faces,
+                                    float* __restrict__ gp, float* __restrict__ gv) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float dx = pts[3 * i] - cp[3 * i], dy = pts[3 * i + 1] - cp[3 * i + 1], dz = pts[3 * i + 2] - cp[3 * i + 2];
+  const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+  const float g = gd[i];
+  // d|p-c|/dp = (p-c)/|p-c| (zero at the surface, like norm's subgradient)
+  const float inv = d > 0.f ? g / d : 0.f;
+  const float gx = dx * inv, gy = dy * inv, gz = dz * inv;
+  if (gp) {
+    gp[3 * i] = gx;
+    gp[3 * i + 1] = gy;
+    gp[3 * i + 2] = gz;
+  }
+  const int32_t f = fid[i];
+  if (gv && f >= 0 && uvw) {
+    // closest-point barycentrics clamped to the simplex (they are exact
+    // for the closest point up to rounding)
+    float w0 = fmaxf(uvw[3 * i], 0.f), w1 = fmaxf(uvw[3 * i + 1], 0.f), w2 = fmaxf(uvw[3 * i + 2], 0.f);
+    const float sw = w0 + w1 + w2;
+    if (sw > 0.f) { w0 /= sw; w1 /= sw; w2 /= sw; }
+    const float ws[3] = {w0, w1, w2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int64_t v = faces[3 * (int64_t)f + k];
+      atomicAdd(&gv[3 * v], -ws[k] * gx);
+      atomicAdd(&gv[3 * v + 1], -ws[k] * gy);
+      atomicAdd(&gv[3 * v + 2], -ws[k] * gz);
+    }
+  }
+}
+
+}  // namespace
+
+}  // namespace a3d
+
+using namespace a3d;
+
+extern "C" size_t a3d_udf_workspace_bytes(int64_t num_points, uint32_t flags) {
+  Workspace ws(nullptr, 0);
+  UdfWs w;
+  return carve_udf(w, ws, num_points > 0 ? num_points : 1, flags) + 256;
+}
+
+extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num_points, float* distances,
+                       int32_t* face_ids, float* closest_points, float* uvw, const a3d_sign_data* sign,
+                       const float* bound, unsigned long long* stats, uint32_t flags, void* workspace,
+                       size_t workspace_bytes, a3d_stream_t stream_) {
+  cudaStream_t s = (cudaStream_t)stream_;
+  A3D_REQUIRE(bvh && bvh->nodes && bvh->tris && bvh->num_nodes > 0, A3D_ERR_ARGUMENT, "udf: invalid bvh");
+  A3D_REQUIRE(num_points >= 0 && num_points < (1ll << 32), A3D_ERR_ARGUMENT, "udf: bad number of points");
+  if (num_points == 0) return A3D_OK;
+  A3D_REQUIRE(points && distances && face_ids && closest_points, A3D_ERR_ARGUMENT, "udf: null output");
+  if (sign) {
+    A3D_REQUIRE(sign->face_normals && sign->faces, A3D_ERR_ARGUMENT, "udf: sign data needs face normals and faces");
+    const bool all = sign->vertex_pn && sign->edge_pn && sign->he_edge_idx;
+    const bool none = !sign->vertex_pn && !sign->edge_pn && !sign->he_edge_idx;
+    A3D_REQUIRE(all || none, A3D_ERR_ARGUMENT, "udf: pseudo-normal data must be all present or all absent");
+  }
+  Workspace ws(workspace, workspace_bytes);
+  UdfWs w;
+  carve_udf(w, ws, num_points, flags);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "udf: workspace too small");
+  const int64_t n = num_points;
+  const uint32_t* perm = nullptr;
+  if (flags & A3D_UDF_SORT_QUERIES) {
+    const float ext[3] = {bvh->hi[0] - bvh->lo[0], bvh->hi[1] - bvh->lo[1], bvh->hi[2] - bvh->lo[2]};
+    float emax = fmaxf(ext[0], fmaxf(ext[1], ext[2]));
+    emax = emax > 0.f ? emax : 1.f;
+    // queries may lie outside the mesh box: use a cube of twice its extent
+    const float lo[3] = {0.5f * (bvh->lo[0] + bvh->hi[0]) - emax, 0.5f * (bvh->lo[1] + bvh->hi[1]) - emax,
+                         0.5f * (bvh->lo[2] + bvh->hi[2]) - emax};
+    const float inv = 1023.0f / (2.0f * emax);
+    query_morton_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(points, n, lo[0], lo[1], lo[2], inv, inv, inv,
+                                                                   w.keys, w.vals);
+    A3D_LAUNCH_CHECK();
+    bool alt = false;
+    A3D_TRY(radix_sort_pairs<uint32_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, n, 0, 32, w.rs_scratch, &alt, s));
+    perm = alt ? w.vals_alt : w.vals;
+  }
+  A3D_CUDA_TRY(cudaMemsetAsync(w.nrerun, 0, 4 * sizeof(uint32_t), s));
+  QueryOut out{distances, face_ids, closest_points, uvw};
+  SignArgs sg{nullptr, nullptr, nullptr, nullptr, nullptr};
+  if (sign) {
+    const bool pn = sign->edge_pn != nullptr;
+    sg = SignArgs{sign->face_normals, pn ? sign->vertex_pn : nullptr, pn ? sign->edge_pn : nullptr,
+                  pn ? sign->he_edge_idx : nullptr, sign->faces};
+  }
+  if (sign) {
+    if (stats) A3D_TRY((launch_udf<true, true>(bvh, points, n, perm, bound, out, sg, stats, w, s)));
+    else A3D_TRY((launch_udf<true, false>(bvh, points, n, perm, bound, out, sg, stats, w, s)));
+  } else {
+    if (stats) A3D_TRY((launch_udf<false, true>(bvh, points, n, perm, bound, out, sg, stats, w, s)));
+    else A3D_TRY((launch_udf<false, false>(bvh, points, n, perm, bound, out, sg, stats, w, s)));
+  }
+  if (stats) {
+    // reruns are reported as bound misses / spills (same counter: re-run queries)
+    A3D_CUDA_TRY(cudaMemcpyAsync(stats + 2, w.nrerun, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  }
+  return A3D_OK;
+}
+
+extern "C" int a3d_udf_backward(const float* points, int64_t num_points, const float* closest_points,
+                                const int32_t* face_ids, const float* uvw, const float* grad_dist,
+                                const int32_t* faces, float* grad_points, float* grad_vertices,
+                                a3d_stream_t stream_) {
+  cudaStream_t s = (cudaStream_t)stream_;
+  A3D_REQUIRE(num_points >= 0, A3D_ERR_ARGUMENT, "udf_backward: bad size");
+  if (num_points == 0) return A3D_OK;
+  A3D_REQUIRE(points && closest_points && grad_dist, A3D_ERR_ARGUMENT, "udf_backward: null input");
+  A3D_REQUIRE(!grad_vertices || (face_ids && uvw && faces), A3D_ERR_ARGUMENT,
+              "udf_backward: vertex adjoint needs face ids, uvw and faces");
+  udf_backward_kernel<<<(unsigned)ceil_div(num_points, 256), 256, 0, s>>>(
+      points, num_points, closest_points, face_ids, uvw, grad_dist, faces, grad_points, grad_vertices);
+  A3D_LAUNCH_CHECK();
+  return A3D_OK;
+}

@@ -1,0 +1,160 @@
+/*
+ * atom3d_b200 — C ABI of the B200 geometry hot path.
+ *
+ * Every function takes raw device pointers, element counts and a CUDA
+ * stream, allocates nothing itself (scratch comes from a caller-provided
+ * workspace whose size is queried first), and returns an int status
+ * (A3D_OK == 0).  No C++ exception or torch type crosses this boundary.
+ * The host-side Python package (atom3d_b200) binds these with ctypes and
+ * keeps the reference's Python signatures on top of them.
+ *
+ * Each entry point names the reference interface it replaces (file:line
+ * inside the Luo-Yihao/Atom3d project).
+ */
+#ifndef ATOM3D_B200_H_
+#define ATOM3D_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* a3d_stream_t; /* == cudaStream_t */
+
+/* ---- status codes ------------------------------------------------------ */
+#define A3D_OK 0
+#define A3D_ERR_ARGUMENT 1      /* bad size / null pointer / unsupported option */
+#define A3D_ERR_WORKSPACE 2     /* workspace or output capacity too small       */
+#define A3D_ERR_CUDA 3          /* a CUDA runtime call or launch failed         */
+#define A3D_ERR_OVERFLOW 4      /* a device-side queue or stack overflowed      */
+#define A3D_ERR_TIMEOUT 5       /* a bounded device-side wait gave up           */
+
+/* Last error message of the calling host thread ("" when none). */
+const char* a3d_last_error(void);
+/* Library version string. */
+const char* a3d_version(void);
+
+/* ---- BVH ---------------------------------------------------------------- */
+/* Device-resident wide BVH: 64-byte 4-wide quantised nodes (node 0 = root)
+ * and 48-byte triangle records stored in leaf order.  The memory is owned by
+ * the caller; a3d_bvh_build fills it. */
+typedef struct a3d_bvh_view {
+  const void* nodes;   /* num_nodes x 64 B, 64-B aligned                     */
+  const void* tris;    /* num_tris  x 48 B, 16-B aligned                     */
+  int64_t num_nodes;
+  int64_t num_tris;
+  float lo[3];         /* scene bounds (triangle AABB union)                 */
+  float hi[3];
+} a3d_bvh_view;
+
+#define A3D_BVH_NODE_BYTES 64
+#define A3D_BVH_TRI_BYTES 48
+
+/* Replaces build_bvh_cuda / build_bvh_recursive
+ * (atom3d/kernels/bvh_kernels.cu:860-925, :667-854) behind
+ * BVHAccelerator.__init__ (atom3d/kernels/bvh.py:66-93).
+ * GPU build: Morton codes -> in-house radix sort -> binary radix tree ->
+ * bottom-up refit -> SAH-guided collapse into 4-wide quantised nodes.
+ * node_capacity >= max(num_faces, 1) always suffices. */
+size_t a3d_bvh_build_workspace_bytes(int64_t num_faces);
+int a3d_bvh_build(const float* vertices, int64_t num_vertices,
+                  const int32_t* faces, int64_t num_faces,
+                  void* nodes_out, int64_t node_capacity, void* tris_out,
+                  void* workspace, size_t workspace_bytes,
+                  int64_t* num_nodes_out /* host */,
+                  float* bounds_out /* host, 6 floats: lo xyz, hi xyz */,
+                  a3d_stream_t stream);
+
+/* ---- pseudo-normal precompute for the SDF sign -------------------------- */
+/* Replaces MeshBVH._precompute_face_normals and
+ * MeshBVH._precompute_pseudo_normal_data (atom3d/core/mesh_bvh.py:129-232).
+ * Outputs: face_normals_sign [F,3] (n/(|n|+1e-8), used by the sign test),
+ * face_angles [F,3], vertex_pn [V,3], edge_pn [edge_capacity,3],
+ * he_edge_idx [3F] int64 (half-edge -> edge id, edges numbered in ascending
+ * key lo*V+hi order like torch.unique). *num_edges_out receives E. */
+size_t a3d_mesh_normals_workspace_bytes(int64_t num_vertices, int64_t num_faces);
+int a3d_mesh_normals(const float* vertices, int64_t num_vertices,
+                     const int32_t* faces, int64_t num_faces,
+                     float* face_normals_sign, float* face_angles,
+                     float* vertex_pn, float* edge_pn, int64_t edge_capacity,
+                     int64_t* he_edge_idx, int64_t* num_edges_out /* host */,
+                     void* workspace, size_t workspace_bytes, a3d_stream_t stream);
+
+/* Sign inputs for a3d_udf (all device pointers). */
+typedef struct a3d_sign_data {
+  const float* face_normals;   /* [F,3]  */
+  const float* vertex_pn;      /* [V,3]  */
+  const float* edge_pn;        /* [E,3]  */
+  const int64_t* he_edge_idx;  /* [3F]   */
+  const int32_t* faces;        /* [F,3]  */
+} a3d_sign_data;
+
+/* ---- closest-point queries --------------------------------------------- */
+/* Replaces bvh_udf_cuda + bvh_udf_kernel (atom3d/kernels/bvh_kernels.cu:
+ * 1028-1066, :363-463) and, when sign != NULL, the pseudo-normal sign of
+ * MeshBVH._compute_sign (atom3d/core/mesh_bvh.py:759-827) fused into the
+ * same launch: distances then hold signed distances.
+ * uvw may be NULL.  bound (nullable) is a per-query upper bound on the
+ * unsigned distance that seeds the pruning radius; queries whose bound proves
+ * too small are re-run unbounded, so results never depend on it.
+ * flags: A3D_UDF_SORT_QUERIES (Morton-sort queries for warp coherence).
+ * stats (nullable, device, 4 x uint64): node visits, triangle tests,
+ * bound misses, stack spills.  */
+#define A3D_UDF_SORT_QUERIES 1u
+size_t a3d_udf_workspace_bytes(int64_t num_points, uint32_t flags);
+int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num_points,
+            float* distances, int32_t* face_ids, float* closest_points,
+            float* uvw, const a3d_sign_data* sign, const float* bound,
+            unsigned long long* stats, uint32_t flags,
+            void* workspace, size_t workspace_bytes, a3d_stream_t stream);
+
+/* Adjoint of the unsigned distance with respect to the mesh vertices:
+ * grad_vertices[V,3] += sum_q grad_dist[q] * d dist_q / d vertex.
+ * With closest point c = sum_i w_i v_i (w = clamped barycentrics of the
+ * closest point) the envelope theorem gives d dist / d v_i = -w_i (p-c)/|p-c|.
+ * grad_points[Q,3] (nullable) receives grad_dist * (p-c)/|p-c| like
+ * MeshBVH._udf_with_grad (atom3d/core/mesh_bvh.py:685-700). */
+int a3d_udf_backward(const float* points, int64_t num_points,
+                     const float* closest_points, const int32_t* face_ids,
+                     const float* uvw, const float* grad_dist,
+                     const int32_t* faces, float* grad_points,
+                     float* grad_vertices, a3d_stream_t stream);
+
+/* ---- Morton keys -------------------------------------------------------- */
+/* Replaces OctreeIndexer._ijk_to_morton / _morton_to_ijk
+ * (atom3d/grid/octree_indexer.py:162-185): x -> bit 3i, y -> 3i+1,
+ * z -> 3i+2, 21 bits per axis. decode keeps bits of levels 0..level. */
+int a3d_morton_encode(const int64_t* ijk, int64_t n, int64_t* morton, a3d_stream_t stream);
+int a3d_morton_decode(const int64_t* morton, int64_t n, int level, int64_t* ijk, a3d_stream_t stream);
+
+/* ---- triangle/box SAT --------------------------------------------------- */
+/* Replaces bvh_aabb_intersect_cuda / bvh_aabb_intersect_kernel in hit-mask
+ * mode (atom3d/kernels/bvh_kernels.cu:1192-1242, :555-610; triangle_aabb_sat
+ * :285-353) behind MeshBVH.intersect_aabb(mode=0). hit[n] = 1 when some
+ * triangle passes the SAT test with sat_eps = 1e-6. */
+size_t a3d_aabb_hit_workspace_bytes(int64_t n);
+int a3d_aabb_hit(const a3d_bvh_view* bvh, const float* box_min, const float* box_max,
+                 int64_t n, uint8_t* hit, void* workspace, size_t workspace_bytes,
+                 a3d_stream_t stream);
+
+/* Replaces OctreeIndexer.octree_traverse (atom3d/grid/octree_indexer.py:470-509):
+ * coarse-to-fine candidate voxels at max_level in the reference's order
+ * (meshgrid 'ij' at min_level, then parent-major x 8 CUBE_CORNERS children,
+ * stable compaction).  grid_lo / cell sizes per level come from the caller
+ * (cell_sizes[level] as float32 = (hi-lo)/2^level).  out_ijk [cap,3] int64.
+ * *count_out (host) receives K; A3D_ERR_WORKSPACE when K > cap (count still
+ * reported). */
+size_t a3d_octree_workspace_bytes(int min_level, int max_level, int64_t cap);
+int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo /* host[3] */,
+                        const float* cell_sizes /* host [(max_level+1)*3] */,
+                        int min_level, int max_level,
+                        int64_t* out_ijk, int64_t cap, int64_t* count_out /* host */,
+                        void* workspace, size_t workspace_bytes, a3d_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ATOM3D_B200_H_ */
