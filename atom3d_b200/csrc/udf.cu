@@ -26,7 +26,8 @@ namespace a3d {
 namespace {
 
 constexpr int kUdfThreads = 128;
-constexpr int kSharedDepth = 24;
+constexpr int kSharedDepth = 32;
+constexpr int kQueriesPerThread = 8;
 constexpr int kDeepDepth = 256;
 
 struct SignArgs {
@@ -261,33 +262,104 @@ __device__ __forceinline__ void flush_counters(const Counters& c, unsigned long 
   }
 }
 
-// queries in [0, n): perm maps the launch index to the query index
+// Greedy root-to-leaf probe: follows the nearest child and tests that
+// leaf's triangles.  Gives a real triangle (and its distance) that seeds the
+// pruning radius of the full traversal.
+__device__ __forceinline__ void probe(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris, float px,
+                                     float py, float pz, uint32_t& tri, float& dsq, Counters& ctr) {
+  uint32_t ref = 0;
+  while (!ref_is_leaf(ref)) {
+    ++ctr.nodes;
+    const int4* np = reinterpret_cast<const int4*>(nodes + ref);
+    const int4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3);
+    const float ox = __int_as_float(w0.x), oy = __int_as_float(w0.y), oz = __int_as_float(w0.z);
+    const uint32_t meta = (uint32_t)w0.w;
+    const float sx = __uint_as_float((meta & 0xffu) << 23);
+    const float sy = __uint_as_float(((meta >> 8) & 0xffu) << 23);
+    const float sz = __uint_as_float(((meta >> 16) & 0xffu) << 23);
+    const uint32_t r[4] = {(uint32_t)w2.z, (uint32_t)w2.w, (uint32_t)w3.x, (uint32_t)w3.y};
+    const int nch = (int)(meta >> 24);
+    float bd = INFINITY;
+    uint32_t br = r[0];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int sh = 8 * c;
+      const float lx = fmaf((float)(((uint32_t)w1.x >> sh) & 0xffu), sx, ox);
+      const float ly = fmaf((float)(((uint32_t)w1.y >> sh) & 0xffu), sy, oy);
+      const float lz = fmaf((float)(((uint32_t)w1.z >> sh) & 0xffu), sz, oz);
+      const float hx = fmaf((float)(((uint32_t)w1.w >> sh) & 0xffu), sx, ox);
+      const float hy = fmaf((float)(((uint32_t)w2.x >> sh) & 0xffu), sy, oy);
+      const float hz = fmaf((float)(((uint32_t)w2.y >> sh) & 0xffu), sz, oz);
+      const float d = c < nch ? box_dist_sq(px, py, pz, lx, ly, lz, hx, hy, hz) : INFINITY;
+      if (d < bd) { bd = d; br = r[c]; }
+    }
+    ref = br;
+  }
+  const uint32_t f0 = leaf_first(ref), cnt = leaf_count(ref);
+  dsq = INFINITY;
+  tri = f0;
+  for (uint32_t i = 0; i < cnt; ++i) {
+    ++ctr.tris;
+    const float d = tri_dist_sq(load_tri(tris, f0 + i), px, py, pz);
+    if (d < dsq) { dsq = d; tri = f0 + i; }
+  }
+}
+
+// Each thread walks `chunk` consecutive Morton-sorted queries.  The pruning
+// radius of a query starts just above its distance to the previous query's
+// closest triangle (a greedy probe for the first one), so a valid triangle
+// always lies inside it and the traversal returns exactly what an
+// unbounded traversal returns: the nodes it skips all lie at or beyond a
+// distance some tested triangle already beats or ties earlier in the same
+// nearest-first order.  An external bound, when given, tightens the radius
+// further; if it excludes every triangle the query is re-run unbounded.
 template <bool kSign, bool kStats>
 __global__ void __launch_bounds__(kUdfThreads)
     udf_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris, const float* __restrict__ pts,
-               int64_t n, const uint32_t* __restrict__ perm, const float* __restrict__ bound, QueryOut out,
-               SignArgs sg, unsigned long long* stats, uint32_t* __restrict__ rerun, uint32_t* __restrict__ nrerun) {
+               int64_t n, int chunk, const uint32_t* __restrict__ perm, const float* __restrict__ bound,
+               QueryOut out, SignArgs sg, unsigned long long* stats, uint32_t* __restrict__ rerun,
+               uint32_t* __restrict__ nrerun) {
   __shared__ uint2 s_stack[kSharedDepth * kUdfThreads];
   const int64_t t = (int64_t)blockIdx.x * kUdfThreads + threadIdx.x;
   Counters ctr{0, 0};
-  if (t < n) {
-    const int64_t qi = perm ? (int64_t)perm[t] : t;
+  const int64_t k0 = t * chunk;
+  const int64_t k1 = k0 + chunk < n ? k0 + chunk : n;
+  uint32_t prev = 0xffffffffu;
+  for (int64_t k = k0; k < k1; ++k) {
+    const int64_t qi = perm ? (int64_t)perm[k] : k;
     const float px = pts[3 * qi], py = pts[3 * qi + 1], pz = pts[3 * qi + 2];
-    float best_sq = INFINITY;
+    uint32_t seed_tri;
+    float seed_sq;
+    if (prev != 0xffffffffu) {
+      seed_tri = prev;
+      ++ctr.tris;
+      seed_sq = tri_dist_sq(load_tri(tris, prev), px, py, pz);
+    } else {
+      probe(nodes, tris, px, py, pz, seed_tri, seed_sq, ctr);
+    }
+    // strictly above the seed distance so the seed triangle itself qualifies
+    float best_sq = seed_sq < INFINITY ? nextafterf(seed_sq, INFINITY) : INFINITY;
+    bool bounded = false;
     if (bound) {
       const float b = bound[qi];
-      best_sq = b * b;
-      if (!(best_sq >= 0.f)) best_sq = INFINITY;
+      const float bsq = b * b;
+      if (bsq >= 0.f && bsq < best_sq) {
+        best_sq = bsq;
+        bounded = true;
+      }
     }
     uint32_t best_tri = 0xffffffffu;
     SharedStack st{s_stack + threadIdx.x, 0};
     const bool ok = traverse(nodes, tris, px, py, pz, st, best_sq, best_tri, ctr);
     if (!ok || best_tri == 0xffffffffu) {
-      // stack overflow, or the bound excluded every triangle: exact re-run
+      // stack overflow, or an external bound excluded every triangle
+      (void)bounded;
       const uint32_t slot = atomicAdd(nrerun, 1u);
       rerun[slot] = (uint32_t)qi;
+      prev = 0xffffffffu;
     } else {
       finish_query(tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
+      prev = best_tri;
     }
   }
   if (kStats) flush_counters(ctr, stats);
@@ -365,8 +437,10 @@ int launch_udf(const a3d_bvh_view* bvh, const float* pts, int64_t n, const uint3
                const QueryOut& out, const SignArgs& sg, unsigned long long* stats, UdfWs& w, cudaStream_t s) {
   const WideNode* nodes = (const WideNode*)bvh->nodes;
   const TriRec* tris = (const TriRec*)bvh->tris;
-  udf_kernel<kSign, kStats><<<(unsigned)ceil_div(n, kUdfThreads), kUdfThreads, 0, s>>>(
-      nodes, tris, pts, n, perm, bound, out, sg, stats, w.rerun, w.nrerun);
+  const int chunk = perm ? kQueriesPerThread : 1;
+  const int64_t nthreads = ceil_div(n, chunk);
+  udf_kernel<kSign, kStats><<<(unsigned)ceil_div(nthreads, kUdfThreads), kUdfThreads, 0, s>>>(
+      nodes, tris, pts, n, chunk, perm, bound, out, sg, stats, w.rerun, w.nrerun);
   A3D_LAUNCH_CHECK();
   udf_rerun_kernel<kSign, kStats><<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, pts, w.rerun, w.nrerun, out, sg, stats,
                                                             (int*)(w.nrerun + 1));

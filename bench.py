@@ -1,0 +1,370 @@
+"""Benchmark of the closest-point (UDF) hot path on B200.
+
+Workload: icosphere level 8 (655,362 vertices, 1,310,720 triangles)
+radially displaced by 16 seeded sinusoids (amplitude 0.05 each), 16,777,216
+queries: half area-weighted surface samples + N(0, 0.02), half uniform in
+the mesh box scaled by 1.2.  One step = one closest-point pass over all
+queries (distance, face id, closest point) through the C ABI.
+
+  value  : queries/s with inputs resident in HBM (device-timed, CUDA events)
+  e2e    : queries/s through MeshBVH.udf with pinned host buffers, H2D of
+           the queries and D2H of the results inside the timed region
+  roofline.achieved : algorithmic bytes of the traversal kernel per launch
+           (per-query reference-layout bytes) / its average
+           CUDA-event duration
+  cpu_baseline : the CPU brute-force port of the reference's closest-point
+           maths on a bounded query sample, all host threads
+
+Multi-GPU (torchrun): replicas only (weak scaling); each rank runs the full
+workload on its own GPU, value = total queries / max-over-ranks time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+import torch.distributed as dist
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "UDF Mqueries/s (plain traversal, 1.31M-triangle mesh, 16M queries)"
+UNIT = "Mqueries/s"
+WORKLOAD = "udf_large: icosphere L8 (1,310,720 tris) + 16 sinusoids, 16,777,216 mixed queries"
+
+# Per-query algorithmic traversal counts of the plain method on the
+# reference's binary SAH tree (counted once by the oracle's instrumented
+# restatement of bvh_udf_kernel over the reference build_bvh output for this
+# mesh, on a 16,384-query sample of this distribution; see
+# tests/golden/make_traversal_counts.py).  Bytes per unit: node 24 B,
+# triangle 36 B, compulsory 32 B per query.
+COUNTS_FILE = os.path.join(HERE, "tests", "golden", "udf_large_counts.json")
+
+
+def load_counts():
+    try:
+        with open(COUNTS_FILE) as f:
+            return json.load(f)
+    except OSError:
+        return None
+
+
+def peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except OSError:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def flush_l2(buf):
+    buf.add_(1.0)
+
+
+def setup_dist(gpus):
+    if gpus > 1 or "RANK" in os.environ:
+        dist.init_process_group(backend="nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        rank = dist.get_rank()
+        local = int(os.environ.get("LOCAL_RANK", rank))
+        return rank, dist.get_world_size(), local
+    return 0, 1, 0
+
+
+def barrier(world):
+    if world > 1:
+        dist.barrier()
+
+
+def max_over_ranks(x, world, dev):
+    if world == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(v, f, q, budget_s=15.0):
+    """Brute-force CPU port of the reference's closest-point maths (oracle),
+    on a bounded prefix of the query set, all host threads."""
+    from oracle import orc
+
+    orc.build()
+    n = 64
+    t = 0.0
+    while True:
+        t0 = time.perf_counter()
+        orc.ref_udf_bruteforce(v.numpy(), f.numpy(), q[:n].numpy())
+        t = time.perf_counter() - t0
+        if t > budget_s / 4 or n >= 8192:
+            break
+        n *= 2
+    return {"value": n / t / 1e6, "unit": UNIT, "cores": orc.threads(), "kind": "port",
+            "sample": f"{n} of the 16,777,216 queries (brute force over all 1,310,720 triangles)"}
+
+
+def run_reference(args):
+    rank, world, local = setup_dist(args.gpus)
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    from atom3d_b200 import synthetic
+
+    v, f, q = synthetic.udf_large()
+    base = cpu_baseline(v, f, q, budget_s=20.0)
+    steps = []
+    from oracle import orc
+
+    n = int(base["sample"].split()[0])
+    for _ in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        orc.ref_udf_bruteforce(v.numpy(), f.numpy(), q[:n].numpy())
+        steps.append(time.perf_counter() - t0)
+    t = statistics.mean(steps[args.warmup:])
+    val = n / t / 1e6
+    base["value"] = val
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample_queries": n},
+            "cpu_baseline": base, "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--queries", type=int, default=16 * 1024 * 1024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank, world, local = setup_dist(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from atom3d_b200 import MeshBVH, _lib, synthetic
+
+    v, f, q = synthetic.udf_large(n_queries=args.queries)
+    n = q.shape[0]
+    mesh = MeshBVH(v.to(dev), f.to(dev))
+    qd = q.to(dev)
+    bvh = mesh._bvh
+    flags = _lib.A3D_UDF_SORT_QUERIES
+    dist_o = torch.empty(n, device=dev)
+    fid_o = torch.empty(n, dtype=torch.int32, device=dev)
+    cp_o = torch.empty(n, 3, device=dev)
+    ws = _lib.workspace(_lib.lib().a3d_udf_workspace_bytes(n, flags), dev)
+    import ctypes
+
+    view = bvh.view
+    stream = torch.cuda.current_stream(dev)
+
+    def step(stats=None):
+        _lib.call("a3d_udf", ctypes.byref(view), qd.data_ptr(), n, dist_o.data_ptr(), fid_o.data_ptr(),
+                  cp_o.data_ptr(), None, None, None, _lib.ptr(stats), flags, ws.data_ptr(), ws.numel(),
+                  stream.cuda_stream)
+
+    # traversal statistics of our tree (one untimed pass)
+    st = torch.zeros(4, dtype=torch.int64, device=dev)
+    step(st)
+    torch.cuda.synchronize()
+    our_nodes, our_tris, reruns = (int(x) for x in st[:3].cpu())
+
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ms, world, dev)
+    clocks = clk.summary()
+
+    # dominant kernel duration: time the traversal launch alone (queries
+    # pre-sorted by one untimed call; same stream, CUDA events)
+    kernel_ms = time_traversal_kernel(bvh, qd, dist_o, fid_o, cp_o, ws, flags, stream, args.steps)
+
+    # end to end through the public API, pinned host buffers
+    qh = q.pin_memory()
+    dh = torch.empty(n, pin_memory=True)
+    fh = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    ch = torch.empty(n, 3, pin_memory=True)
+
+    def e2e_step():
+        qq = qh.to(dev, non_blocking=True)
+        r = mesh.udf(qq, return_closest=True, return_face_ids=True)
+        dh.copy_(r.distances, non_blocking=True)
+        fh.copy_(r.face_ids, non_blocking=True)
+        ch.copy_(r.closest_points, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world, dev)
+
+    peak, peak_kind = peaks()
+    counts = load_counts()
+    roof = None
+    if counts is not None:
+        per_q = 32.0 + 24.0 * counts["nodes_per_query"] + 36.0 * counts["tris_per_query"]
+        achieved = per_q * n / (kernel_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "peak_kind": peak_kind, "bytes_per_query": per_q,
+                "kernel": "udf_kernel", "kernel_ms": kernel_ms}
+    total_q = n * world
+    line = {
+        "metric": METRIC, "value": total_q / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "queries_per_gpu": n, "triangles": int(f.shape[0]),
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (192 MB queries, 512 MB outputs)"},
+        "e2e": {"value": total_q / (e2e_ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": n * 12,
+                "d2h_bytes_per_step": n * (4 + 4 + 12)},
+        "roofline": roof,
+        "gpu_launches": args.steps * launches_per_udf(),
+        "clocks": clocks,
+        "traversal": {"nodes_per_query": our_nodes / n, "tris_per_query": our_tris / n, "reruns": reruns},
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(v, f, q)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def launches_per_udf():
+    # query Morton keys (1) + 4 radix passes x (upsweep, 3 scan kernels,
+    # downsweep) + traversal + re-run kernel
+    return 1 + 4 * 5 + 2
+
+
+def time_traversal_kernel(bvh, qd, dist_o, fid_o, cp_o, ws, flags, stream, steps):
+    """Average duration of the traversal launch itself: the same call with
+    pre-sorted queries and sorting disabled, so only the traversal kernel
+    (plus its empty re-run launch) is inside the events."""
+    import ctypes
+
+    from atom3d_b200 import _lib, synthetic  # noqa: F401
+
+    n = qd.shape[0]
+    # Morton order of the queries (same key as the library) via one sorted call
+    lo = torch.tensor(bvh.lo, device=qd.device)
+    hi = torch.tensor(bvh.hi, device=qd.device)
+    emax = float((hi - lo).max())
+    c = (lo + hi) * 0.5 - emax
+    key = ((qd - c) * (1023.0 / (2 * emax))).clamp(0, 1023).to(torch.int64)
+    code = torch.zeros(n, dtype=torch.int64, device=qd.device)
+    for b in range(10):
+        for a in range(3):
+            code |= ((key[:, a] >> b) & 1) << (3 * b + a)
+    order = torch.argsort(code, stable=True)
+    qs = qd[order].contiguous()
+    view = bvh.view
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def call():
+        _lib.call("a3d_udf", ctypes.byref(view), qs.data_ptr(), n, dist_o.data_ptr(), fid_o.data_ptr(),
+                  cp_o.data_ptr(), None, None, None, None, 0, ws.data_ptr(), ws.numel(), stream.cuda_stream)
+
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(steps):
+        call()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / steps
+
+
+if __name__ == "__main__":
+    main()

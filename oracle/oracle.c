@@ -576,3 +576,57 @@ void orc_flood_fill(const uint8_t* occ, int D, int H, int W, int sx, int sy, int
   }
   free(q);
 }
+
+/* bvh_udf_kernel restated with counters: counts[0] += node AABB distance
+ * evaluations (24-B box reads), counts[1] += triangle distance evaluations
+ * (36-B triangle reads), summed over all queries.  Used once to fix the
+ * per-query algorithmic traversal bytes of the plain method. */
+typedef struct { const float* nodes; const float* tris; const float* P; atomic_llong* cnt; } rcnt_ctx;
+static void rcnt_body(int64_t qi, void* c_) {
+  rcnt_ctx* c = (rcnt_ctx*)c_;
+  const float* nodes = c->nodes; const float* tris = c->tris;
+  f3 p = lfv(c->P, qi);
+  float best = 1e30f;
+  long long nn = 0, nt = 0;
+  int stack[128];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp > 0) {
+    int idx = stack[--sp];
+    const float* n = nodes + 9 * (int64_t)idx;
+    ++nn;
+    if (ref_point_aabb(p, n) >= best) continue;
+    int l = fbits(n[6]), r = fbits(n[7]);
+    if (l < 0) {
+      int s = -l - 1, e = -r - 1;
+      for (int i = s; i < e; ++i) {
+        const float* t = tris + 10 * (int64_t)i;
+        f3 a = {t[0], t[1], t[2]}, b = {t[3], t[4], t[5]}, cc = {t[6], t[7], t[8]};
+        float d = ref_dist_sq(p, a, b, cc);
+        ++nt;
+        if (d < best) best = d;
+      }
+    } else {
+      float d1 = ref_point_aabb(p, nodes + 9 * (int64_t)l), d2 = ref_point_aabb(p, nodes + 9 * (int64_t)r);
+      nn += 2;
+      if (d1 < d2) {
+        if (d2 < best && sp < 128) stack[sp++] = r;
+        if (d1 < best && sp < 128) stack[sp++] = l;
+      } else {
+        if (d1 < best && sp < 128) stack[sp++] = l;
+        if (d2 < best && sp < 128) stack[sp++] = r;
+      }
+    }
+  }
+  atomic_fetch_add(&c->cnt[0], nn);
+  atomic_fetch_add(&c->cnt[1], nt);
+}
+void orc_ref_bvh_udf_counts(const float* nodes, const float* tris, const float* P, int64_t np, int64_t* counts) {
+  atomic_llong cnt[2];
+  atomic_init(&cnt[0], 0);
+  atomic_init(&cnt[1], 0);
+  rcnt_ctx c = {nodes, tris, P, cnt};
+  par_for(np, 16, rcnt_body, &c);
+  counts[0] = atomic_load(&cnt[0]);
+  counts[1] = atomic_load(&cnt[1]);
+}

@@ -272,3 +272,12 @@ def sparse_flood_fill_from_dam(dam, resolution, source=(0, 0, 0), connectivity=2
         "extended_tide_ijk": nb[signs == 1],
         "dry_adjacent_ijk": nb[signs == -1],
     }
+
+
+def ref_bvh_udf_counts(nodes, tris, P):
+    """(node box evaluations, triangle evaluations) of bvh_udf_kernel over a
+    reference tree, summed over the queries."""
+    nodes, tris, P = _f32(nodes), _f32(tris), _f32(P)
+    c = np.zeros(2, np.int64)
+    lib().orc_ref_bvh_udf_counts(_p(nodes), _p(tris), _p(P), I64(P.shape[0]), _p(c))
+    return int(c[0]), int(c[1])
