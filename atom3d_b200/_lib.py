@@ -51,7 +51,7 @@ _SIGNATURES: dict[str, tuple] = {
     "a3d_bvh_build_workspace_bytes": (c_size, [c_i64]),
     "a3d_bvh_build": (
         c_int,
-        [c_vp, c_i64, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp, c_size, ctypes.POINTER(c_i64), c_fp, c_vp],
+        [c_vp, c_i64, c_vp, c_i64, c_int, c_vp, c_i64, c_vp, c_vp, c_size, ctypes.POINTER(c_i64), c_fp, c_vp],
     ),
     "a3d_mesh_normals_workspace_bytes": (c_size, [c_i64, c_i64]),
     "a3d_mesh_normals": (
@@ -85,6 +85,7 @@ A3D_ERR_CUDA = 3
 A3D_ERR_OVERFLOW = 4
 A3D_ERR_TIMEOUT = 5
 A3D_UDF_SORT_QUERIES = 1
+A3D_UDF_ASSUME_SORTED = 2
 
 _lib = None
 _lock = threading.Lock()

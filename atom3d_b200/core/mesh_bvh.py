@@ -17,6 +17,7 @@ There is no CPU path: a CPU device raises.
 from __future__ import annotations
 
 import ctypes
+import os
 from typing import Optional, Union
 
 import torch
@@ -27,10 +28,13 @@ from .device_utils import resolve_device
 
 
 class WideBVH:
-    """Device-resident 4-wide quantised BVH (64-B nodes, 48-B triangle records)."""
+    """Device-resident 4-wide quantised BVH (64-B nodes, 64-B triangle records)."""
 
-    def __init__(self, vertices: torch.Tensor, faces: torch.Tensor):
+    DEFAULT_LEAF_MAX = int(os.environ.get("ATOM3D_B200_LEAF_MAX", "4"))
+
+    def __init__(self, vertices: torch.Tensor, faces: torch.Tensor, leaf_max: int | None = None):
         _lib.require_cuda(vertices, "vertices")
+        self.leaf_max = int(leaf_max or self.DEFAULT_LEAF_MAX)
         dev = vertices.device
         v = vertices.detach().contiguous().float()
         f = faces.contiguous().int()
@@ -44,12 +48,12 @@ class WideBVH:
             nodes = torch.empty(cap * 64 + 64, dtype=torch.uint8, device=dev)
             off = (-nodes.data_ptr()) % 64
             nodes = nodes[off:off + cap * 64]
-            tris = torch.empty(nf * 48, dtype=torch.uint8, device=dev)
+            tris = torch.empty(nf * 64, dtype=torch.uint8, device=dev)
             ws = _lib.workspace(_lib.lib().a3d_bvh_build_workspace_bytes(nf), dev)
             nn = ctypes.c_int64(0)
             bounds = (ctypes.c_float * 6)()
             _lib.call(
-                "a3d_bvh_build", v.data_ptr(), v.shape[0], f.data_ptr(), nf, nodes.data_ptr(), cap,
+                "a3d_bvh_build", v.data_ptr(), v.shape[0], f.data_ptr(), nf, self.leaf_max, nodes.data_ptr(), cap,
                 tris.data_ptr(), ws.data_ptr(), ws.numel(), ctypes.byref(nn), bounds, _lib.stream_ptr(dev),
             )
         self.num_nodes = int(nn.value)

@@ -404,10 +404,21 @@ __global__ void write_tris_kernel(const float* __restrict__ V, const int32_t* __
   const double lm = fmax(l0, fmax(l1, l2));
   uint32_t flags = 0;
   if (nsq < 1e-12 || nsq < 1e-6 * lm * lm) flags |= kTriFlagNearDegenerate;
+  // reciprocals of the quantities the FP32 test divides by, evaluated with
+  // the test's own FP32 expressions
+  const float v21x = b.x - a.x, v21y = b.y - a.y, v21z = b.z - a.z;
+  const float v32x = c.x - b.x, v32y = c.y - b.y, v32z = c.z - b.z;
+  const float v13x = a.x - c.x, v13y = a.y - c.y, v13z = a.z - c.z;
+  const float nrx = v21y * v13z - v21z * v13y, nry = v21z * v13x - v21x * v13z, nrz = v21x * v13y - v21y * v13x;
+  const float nsqf = nrx * nrx + nry * nry + nrz * nrz;
+  const float e0 = v21x * v21x + v21y * v21y + v21z * v21z;
+  const float e1 = v32x * v32x + v32y * v32y + v32z * v32z;
+  const float e2 = v13x * v13x + v13y * v13y + v13z * v13z;
   TriRec r;
   r.a = make_float4(a.x, a.y, a.z, __int_as_float((int)f));
   r.b = make_float4(b.x, b.y, b.z, __uint_as_float(flags));
-  r.c = make_float4(c.x, c.y, c.z, 0.f);
+  r.c = make_float4(c.x, c.y, c.z, nsqf > 0.f ? 1.0f / nsqf : 0.f);
+  r.r = make_float4(1.0f / fmaxf(e0, 1e-12f), 1.0f / fmaxf(e1, 1e-12f), 1.0f / fmaxf(e2, 1e-12f), 0.f);
   tris[j] = r;
 }
 
@@ -424,7 +435,7 @@ extern "C" size_t a3d_bvh_build_workspace_bytes(int64_t num_faces) {
 }
 
 extern "C" int a3d_bvh_build(const float* vertices, int64_t num_vertices, const int32_t* faces, int64_t num_faces,
-                             void* nodes_out, int64_t node_capacity, void* tris_out, void* workspace,
+                             int leaf_max, void* nodes_out, int64_t node_capacity, void* tris_out, void* workspace,
                              size_t workspace_bytes, int64_t* num_nodes_out, float* bounds_out,
                              a3d_stream_t stream_) {
   cudaStream_t s = (cudaStream_t)stream_;
@@ -440,7 +451,8 @@ extern "C" int a3d_bvh_build(const float* vertices, int64_t num_vertices, const 
   BuildWs w;
   carve(w, ws, n);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "bvh_build: workspace too small");
-  const int leaf_max = 4;
+  if (leaf_max == 0) leaf_max = 4;
+  A3D_REQUIRE(leaf_max >= 1 && leaf_max <= kMaxLeafTris, A3D_ERR_ARGUMENT, "bvh_build: leaf_max must be in 1..8");
 
   init_bounds_kernel<<<1, 32, 0, s>>>(w.bounds, w.err);
   A3D_LAUNCH_CHECK();

@@ -15,8 +15,12 @@
 // Child c's box is origin + q * scale per axis; quantisation rounds outward,
 // so the decoded box always contains the exact one.
 //
-// TriRec (48 B): float4 a (xyz, w = original face id as int bits),
-//                float4 b (xyz, w = flag bits), float4 c (xyz, w = 0).
+// TriRec (64 B): float4 a (xyz, w = original face id as int bits),
+//                float4 b (xyz, w = flag bits),
+//                float4 c (xyz, w = 1 / |n|^2 with n = (b - a) x (a - c)),
+//                float4 r (1 / max(|b-a|^2, 1e-12), 1 / max(|c-b|^2, 1e-12),
+//                          1 / max(|a-c|^2, 1e-12), 0)
+// The reciprocals let the per-triangle distance test run without a divide.
 #pragma once
 
 #include <stdint.h>
@@ -33,13 +37,24 @@ struct __align__(64) WideNode {
 static_assert(sizeof(WideNode) == 64, "WideNode must be 64 bytes");
 
 struct __align__(16) TriRec {
-  float4 a, b, c;
+  float4 a, b, c, r;
 };
-static_assert(sizeof(TriRec) == 48, "TriRec must be 48 bytes");
+static_assert(sizeof(TriRec) == 64, "TriRec must be 64 bytes");
 
 constexpr uint32_t kLeafBit = 0x80000000u;
 constexpr uint32_t kTriFlagNearDegenerate = 1u;  // evaluate in FP64
 constexpr int kMaxLeafTris = 8;
+
+// Decoded child-box coordinate origin + q * scale for the 8-bit value q held
+// in byte `byte` of `word`.  The byte is turned into a float without the
+// conversion unit: placed in the mantissa of 2^23 (0x4B0000qq) and 2^23
+// subtracted, which is exact for q < 2^23; q * scale is exact (scale is a
+// power of two), so the result equals fmaf((float)q, scale, origin).
+__device__ __forceinline__ float dequant(uint32_t word, int byte, float scale, float origin) {
+  const uint32_t sel = (uint32_t)byte | (4u << 4) | (5u << 8) | (7u << 12);
+  const float q = __uint_as_float(__byte_perm(word, 0x4B000000u, sel)) - 8388608.0f;
+  return fmaf(q, scale, origin);
+}
 
 __host__ __device__ __forceinline__ bool ref_is_leaf(uint32_t r) { return (r & kLeafBit) != 0; }
 __host__ __device__ __forceinline__ uint32_t leaf_first(uint32_t r) { return r & 0x0fffffffu; }

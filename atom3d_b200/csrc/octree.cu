@@ -116,13 +116,12 @@ __device__ int box_any_hit(const WideNode* __restrict__ nodes, const TriRec* __r
       const int nch = (int)(meta >> 24);
       const uint32_t r[4] = {(uint32_t)w2.z, (uint32_t)w2.w, (uint32_t)w3.x, (uint32_t)w3.y};
       for (int c = nch - 1; c >= 0; --c) {
-        const int sh = 8 * c;
-        const float clx = fmaf((float)(((uint32_t)w1.x >> sh) & 0xffu), sx, ox);
-        const float cly = fmaf((float)(((uint32_t)w1.y >> sh) & 0xffu), sy, oy);
-        const float clz = fmaf((float)(((uint32_t)w1.z >> sh) & 0xffu), sz, oz);
-        const float chx = fmaf((float)(((uint32_t)w1.w >> sh) & 0xffu), sx, ox);
-        const float chy = fmaf((float)(((uint32_t)w2.x >> sh) & 0xffu), sy, oy);
-        const float chz = fmaf((float)(((uint32_t)w2.y >> sh) & 0xffu), sz, oz);
+        const float clx = dequant((uint32_t)w1.x, c, sx, ox);
+        const float cly = dequant((uint32_t)w1.y, c, sy, oy);
+        const float clz = dequant((uint32_t)w1.z, c, sz, oz);
+        const float chx = dequant((uint32_t)w1.w, c, sx, ox);
+        const float chy = dequant((uint32_t)w2.x, c, sy, oy);
+        const float chz = dequant((uint32_t)w2.y, c, sz, oz);
         const bool ov = clx <= ux && chx >= lx && cly <= uy && chy >= ly && clz <= uz && chz >= lz;
         if (ov) {
           if (st.sp >= Stack::kDepth) return 2;
@@ -134,7 +133,7 @@ __device__ int box_any_hit(const WideNode* __restrict__ nodes, const TriRec* __r
       for (uint32_t i = 0; i < cnt; ++i) {
         const float4* p = reinterpret_cast<const float4*>(tris + f0 + i);
         TriRec t;
-        t.a = __ldg(p); t.b = __ldg(p + 1); t.c = __ldg(p + 2);
+        t.a = __ldg(p); t.b = __ldg(p + 1); t.c = __ldg(p + 2); t.r = make_float4(0.f, 0.f, 0.f, 0.f);
         if (sat_test(t, mnx, mny, mnz, mxx, mxy, mxz)) return 1;
       }
     }

@@ -33,6 +33,11 @@ __device__ __forceinline__ V3<T> cross(V3<T> a, V3<T> b) {
 template <typename T>
 __device__ __forceinline__ T clamp01(T v) { return v < T(0) ? T(0) : (v > T(1) ? T(1) : v); }
 
+// Division used by the FP32 evaluation: the fast approximate divide (max
+// error 2 ulp); the FP64 evaluation divides exactly.
+__device__ __forceinline__ float tdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double tdiv(double a, double b) { return a / b; }
+
 template <typename T>
 struct TriEval {
   static constexpr T kDegen = T(1e-12);
@@ -46,14 +51,14 @@ struct TriEval {
                         dot(cross(v13, nor), p3) >= T(0);
     if (inside) {
       const T d = dot(nor, p1);
-      return d * d / nsq;
+      return tdiv(d * d, nsq);
     }
     const T e1 = edge_sq(v21, p1), e2 = edge_sq(v32, p2), e3 = edge_sq(v13, p3);
     return e1 < e2 ? (e1 < e3 ? e1 : e3) : (e2 < e3 ? e2 : e3);
   }
   __device__ static __forceinline__ T edge_sq(V3<T> v, V3<T> p) {
     const T vv = dot(v, v);
-    const T t = clamp01(dot(v, p) / (vv > kDegen ? vv : kDegen));
+    const T t = clamp01(tdiv(dot(v, p), vv > kDegen ? vv : kDegen));
     const V3<T> d = sub(scl(v, t), p);
     return dot(d, d);
   }
@@ -65,7 +70,7 @@ struct TriEval {
     const bool inside = nsq >= kDegen && dot(cross(v21, nor), p1) >= T(0) && dot(cross(v32, nor), p2) >= T(0) &&
                         dot(cross(v13, nor), p3) >= T(0);
     if (inside) {
-      const T d = dot(nor, p1) / nsq;
+      const T d = tdiv(dot(nor, p1), nsq);
       return sub(p, scl(nor, d));
     }
     const V3<T> c1 = edge_pt(v21, p1, a), c2 = edge_pt(v32, p2, b), c3 = edge_pt(v13, p3, c);
@@ -77,7 +82,7 @@ struct TriEval {
   }
   __device__ static __forceinline__ V3<T> edge_pt(V3<T> v, V3<T> p, V3<T> o) {
     const T vv = dot(v, v);
-    const T t = clamp01(dot(v, p) / (vv > kDegen ? vv : kDegen));
+    const T t = clamp01(tdiv(dot(v, p), vv > kDegen ? vv : kDegen));
     return add(o, scl(v, t));
   }
   // barycentric coordinates (u, v, w) of q in (a, b, c), denominators clamped
@@ -87,10 +92,33 @@ struct TriEval {
     const T d00 = dot(v0, v0), d01 = dot(v0, v1), d11 = dot(v1, v1), d20 = dot(v2, v0), d21 = dot(v2, v1);
     T den = d00 * d11 - d01 * d01;
     den = den > T(1e-10) ? den : T(1e-10);
-    const T v = (d11 * d20 - d01 * d21) / den;
-    const T w = (d00 * d21 - d01 * d20) / den;
+    const T v = tdiv(d11 * d20 - d01 * d21, den);
+    const T w = tdiv(d00 * d21 - d01 * d20, den);
     return mk(T(1) - v - w, v, w);
   }
 };
+
+// FP32 squared distance with the triangle's precomputed reciprocals (no
+// divide): same branch structure and products as TriEval<float>::dist_sq.
+__device__ __forceinline__ float dist_sq_rcp(V3<float> p, V3<float> a, V3<float> b, V3<float> c, float inv_nsq,
+                                             float inv_e0, float inv_e1, float inv_e2) {
+  const V3<float> v21 = sub(b, a), v32 = sub(c, b), v13 = sub(a, c);
+  const V3<float> p1 = sub(p, a), p2 = sub(p, b), p3 = sub(p, c);
+  const V3<float> nor = cross(v21, v13);
+  const float nsq = dot(nor, nor);
+  const bool inside = nsq >= 1e-12f && dot(cross(v21, nor), p1) >= 0.f && dot(cross(v32, nor), p2) >= 0.f &&
+                      dot(cross(v13, nor), p3) >= 0.f;
+  if (inside) {
+    const float d = dot(nor, p1);
+    return d * d * inv_nsq;
+  }
+  auto edge = [](V3<float> v, V3<float> q, float inv) {
+    const float t = clamp01(dot(v, q) * inv);
+    const V3<float> e = sub(scl(v, t), q);
+    return dot(e, e);
+  };
+  const float e1 = edge(v21, p1, inv_e0), e2 = edge(v32, p2, inv_e1), e3 = edge(v13, p3, inv_e2);
+  return e1 < e2 ? (e1 < e3 ? e1 : e3) : (e2 < e3 ? e2 : e3);
+}
 
 }  // namespace a3d

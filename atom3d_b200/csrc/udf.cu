@@ -27,7 +27,6 @@ namespace {
 
 constexpr int kUdfThreads = 128;
 constexpr int kSharedDepth = 32;
-constexpr int kQueriesPerThread = 8;
 constexpr int kDeepDepth = 256;
 
 struct SignArgs {
@@ -50,8 +49,15 @@ struct Counters {
   unsigned long long tris;
 };
 
+// children are visited in ascending (distance, ref) order: a total order, so
+// every traversal variant (single lane, quad of lanes) walks the same
+// sequence and breaks distance ties identically
+__device__ __forceinline__ bool child_less(float da, uint32_t ra, float db, uint32_t rb) {
+  return da < db || (da == db && ra < rb);
+}
+
 __device__ __forceinline__ void cswap(float& da, uint32_t& ra, float& db, uint32_t& rb) {
-  if (db < da) {
+  if (child_less(db, rb, da, ra)) {
     float t = da; da = db; db = t;
     uint32_t u = ra; ra = rb; rb = u;
   }
@@ -65,15 +71,20 @@ __device__ __forceinline__ float box_dist_sq(float px, float py, float pz, float
   return dx * dx + dy * dy + dz * dz;
 }
 
+// FP64 evaluation for near-degenerate triangles, kept out of line so the
+// hot loop does not carry its registers.
+__device__ __noinline__ float tri_dist_sq_f64(float ax, float ay, float az, float bx, float by, float bz, float cx,
+                                              float cy, float cz, float px, float py, float pz) {
+  const double d = TriEval<double>::dist_sq(mk<double>(px, py, pz), mk<double>(ax, ay, az), mk<double>(bx, by, bz),
+                                            mk<double>(cx, cy, cz));
+  return (float)d;
+}
+
 __device__ __forceinline__ float tri_dist_sq(const TriRec& t, float px, float py, float pz) {
-  if (__float_as_uint(t.b.w) & kTriFlagNearDegenerate) {
-    const V3<double> p = mk<double>(px, py, pz);
-    const double d = TriEval<double>::dist_sq(p, mk<double>(t.a.x, t.a.y, t.a.z), mk<double>(t.b.x, t.b.y, t.b.z),
-                                              mk<double>(t.c.x, t.c.y, t.c.z));
-    return (float)d;
-  }
-  return TriEval<float>::dist_sq(mk(px, py, pz), mk(t.a.x, t.a.y, t.a.z), mk(t.b.x, t.b.y, t.b.z),
-                                 mk(t.c.x, t.c.y, t.c.z));
+  if (__float_as_uint(t.b.w) & kTriFlagNearDegenerate)
+    return tri_dist_sq_f64(t.a.x, t.a.y, t.a.z, t.b.x, t.b.y, t.b.z, t.c.x, t.c.y, t.c.z, px, py, pz);
+  return dist_sq_rcp(mk(px, py, pz), mk(t.a.x, t.a.y, t.a.z), mk(t.b.x, t.b.y, t.b.z), mk(t.c.x, t.c.y, t.c.z),
+                     t.c.w, t.r.x, t.r.y, t.r.z);
 }
 
 __device__ __forceinline__ TriRec load_tri(const TriRec* tris, uint32_t i) {
@@ -82,6 +93,7 @@ __device__ __forceinline__ TriRec load_tri(const TriRec* tris, uint32_t i) {
   r.a = __ldg(p);
   r.b = __ldg(p + 1);
   r.c = __ldg(p + 2);
+  r.r = __ldg(p + 3);
   return r;
 }
 
@@ -134,13 +146,12 @@ __device__ __forceinline__ bool traverse(const WideNode* __restrict__ nodes, con
         const int nch = (int)(meta >> 24);
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          const int sh = 8 * c;
-          const float lx = fmaf((float)((qlx >> sh) & 0xffu), sx, ox);
-          const float ly = fmaf((float)((qly >> sh) & 0xffu), sy, oy);
-          const float lz = fmaf((float)((qlz >> sh) & 0xffu), sz, oz);
-          const float hx = fmaf((float)((qhx >> sh) & 0xffu), sx, ox);
-          const float hy = fmaf((float)((qhy >> sh) & 0xffu), sy, oy);
-          const float hz = fmaf((float)((qhz >> sh) & 0xffu), sz, oz);
+            const float lx = dequant(qlx, c, sx, ox);
+          const float ly = dequant(qly, c, sy, oy);
+          const float lz = dequant(qlz, c, sz, oz);
+          const float hx = dequant(qhx, c, sx, ox);
+          const float hy = dequant(qhy, c, sy, oy);
+          const float hz = dequant(qhz, c, sz, oz);
           d[c] = c < nch ? box_dist_sq(px, py, pz, lx, ly, lz, hx, hy, hz) : INFINITY;
         }
         cswap(d[0], r[0], d[1], r[1]);
@@ -186,7 +197,7 @@ __device__ __forceinline__ bool traverse(const WideNode* __restrict__ nodes, con
   }
 }
 
-__device__ __forceinline__ void finish_query(const TriRec* __restrict__ tris, uint32_t best_tri, float best_sq,
+__device__ __noinline__ void finish_query(const TriRec* __restrict__ tris, uint32_t best_tri, float best_sq,
                                              float px, float py, float pz, int64_t qi, const QueryOut& out,
                                              const SignArgs& sg, bool do_sign) {
   float cx = px, cy = py, cz = pz;
@@ -283,13 +294,12 @@ __device__ __forceinline__ void probe(const WideNode* __restrict__ nodes, const 
     uint32_t br = r[0];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const int sh = 8 * c;
-      const float lx = fmaf((float)(((uint32_t)w1.x >> sh) & 0xffu), sx, ox);
-      const float ly = fmaf((float)(((uint32_t)w1.y >> sh) & 0xffu), sy, oy);
-      const float lz = fmaf((float)(((uint32_t)w1.z >> sh) & 0xffu), sz, oz);
-      const float hx = fmaf((float)(((uint32_t)w1.w >> sh) & 0xffu), sx, ox);
-      const float hy = fmaf((float)(((uint32_t)w2.x >> sh) & 0xffu), sy, oy);
-      const float hz = fmaf((float)(((uint32_t)w2.y >> sh) & 0xffu), sz, oz);
+      const float lx = dequant((uint32_t)w1.x, c, sx, ox);
+      const float ly = dequant((uint32_t)w1.y, c, sy, oy);
+      const float lz = dequant((uint32_t)w1.z, c, sz, oz);
+      const float hx = dequant((uint32_t)w1.w, c, sx, ox);
+      const float hy = dequant((uint32_t)w2.x, c, sy, oy);
+      const float hz = dequant((uint32_t)w2.y, c, sz, oz);
       const float d = c < nch ? box_dist_sq(px, py, pz, lx, ly, lz, hx, hy, hz) : INFINITY;
       if (d < bd) { bd = d; br = r[c]; }
     }
@@ -320,12 +330,18 @@ __global__ void __launch_bounds__(kUdfThreads)
                QueryOut out, SignArgs sg, unsigned long long* stats, uint32_t* __restrict__ rerun,
                uint32_t* __restrict__ nrerun) {
   __shared__ uint2 s_stack[kSharedDepth * kUdfThreads];
-  const int64_t t = (int64_t)blockIdx.x * kUdfThreads + threadIdx.x;
+  __shared__ uint32_t s_next[kUdfThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // each warp owns 32 * chunk consecutive (sorted) queries and hands them out
+  // to its lanes as they finish, so fast lanes do not idle behind slow ones
+  const int64_t w0 = ((int64_t)blockIdx.x * (kUdfThreads / 32) + warp) * 32 * chunk;
+  const int64_t w1 = w0 + 32 * chunk < n ? w0 + 32 * chunk : n;
+  if (lane == 0) s_next[warp] = 32;
+  __syncwarp();
   Counters ctr{0, 0};
-  const int64_t k0 = t * chunk;
-  const int64_t k1 = k0 + chunk < n ? k0 + chunk : n;
   uint32_t prev = 0xffffffffu;
-  for (int64_t k = k0; k < k1; ++k) {
+  int64_t k = w0 + lane;
+  while (k < w1) {
     const int64_t qi = perm ? (int64_t)perm[k] : k;
     const float px = pts[3 * qi], py = pts[3 * qi + 1], pz = pts[3 * qi + 2];
     uint32_t seed_tri;
@@ -339,21 +355,16 @@ __global__ void __launch_bounds__(kUdfThreads)
     }
     // strictly above the seed distance so the seed triangle itself qualifies
     float best_sq = seed_sq < INFINITY ? nextafterf(seed_sq, INFINITY) : INFINITY;
-    bool bounded = false;
     if (bound) {
       const float b = bound[qi];
       const float bsq = b * b;
-      if (bsq >= 0.f && bsq < best_sq) {
-        best_sq = bsq;
-        bounded = true;
-      }
+      if (bsq >= 0.f && bsq < best_sq) best_sq = bsq;
     }
     uint32_t best_tri = 0xffffffffu;
     SharedStack st{s_stack + threadIdx.x, 0};
     const bool ok = traverse(nodes, tris, px, py, pz, st, best_sq, best_tri, ctr);
     if (!ok || best_tri == 0xffffffffu) {
       // stack overflow, or an external bound excluded every triangle
-      (void)bounded;
       const uint32_t slot = atomicAdd(nrerun, 1u);
       rerun[slot] = (uint32_t)qi;
       prev = 0xffffffffu;
@@ -361,6 +372,273 @@ __global__ void __launch_bounds__(kUdfThreads)
       finish_query(tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
       prev = best_tri;
     }
+    k = w0 + (int64_t)atomicAdd(&s_next[warp], 1u);
+  }
+  if (kStats) {
+    __syncwarp();
+    flush_counters(ctr, stats);
+  }
+}
+
+
+
+__device__ __forceinline__ void quad_child_box(const WideNode* __restrict__ nodes, uint32_t ref, int c, float px,
+                                               float py, float pz, float& d, uint32_t& r) {
+  const int4* np = reinterpret_cast<const int4*>(nodes + ref);
+  const int4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3);
+  const uint32_t meta = (uint32_t)w0.w;
+  const int nch = (int)(meta >> 24);
+  const float sx = __uint_as_float((meta & 0xffu) << 23);
+  const float sy = __uint_as_float(((meta >> 8) & 0xffu) << 23);
+  const float sz = __uint_as_float(((meta >> 16) & 0xffu) << 23);
+  const float ox = __int_as_float(w0.x), oy = __int_as_float(w0.y), oz = __int_as_float(w0.z);
+  const float lx = dequant((uint32_t)w1.x, c, sx, ox);
+  const float ly = dequant((uint32_t)w1.y, c, sy, oy);
+  const float lz = dequant((uint32_t)w1.z, c, sz, oz);
+  const float hx = dequant((uint32_t)w1.w, c, sx, ox);
+  const float hy = dequant((uint32_t)w2.x, c, sy, oy);
+  const float hz = dequant((uint32_t)w2.y, c, sz, oz);
+  r = c == 0 ? (uint32_t)w2.z : (c == 1 ? (uint32_t)w2.w : (c == 2 ? (uint32_t)w3.x : (uint32_t)w3.y));
+  d = c < nch ? box_dist_sq(px, py, pz, lx, ly, lz, hx, hy, hz) : INFINITY;
+}
+
+// ---------------------------------------------------------------------------
+// warp task traversal
+// ---------------------------------------------------------------------------
+// Each lane owns one query (its point, best distance and a stack in shared
+// memory).  Every round, each owner contributes the work of its current item:
+// four child-box tests for an internal node, one triangle test per triangle
+// of a leaf (or of the seed triangle).  The tasks of all 32 owners are packed
+// into dense lists and evaluated by all lanes in lockstep, then each owner
+// consumes its results: sorts the four children by (distance, ref) and
+// pushes the qualifying ones, or folds its triangle distances in order with a
+// strict "<".  The per-query visiting order is therefore the one of the
+// single-lane traversal above and results are identical; only the lane that
+// evaluates each test changes.
+constexpr int kTaskWarps = 2;
+constexpr int kTaskDepth = 32;
+constexpr int kTaskTriCap = 32 * kMaxLeafTris;
+constexpr int kTaskPool = 64;  // queries per pool taken from the global counter
+
+struct TaskSmem {
+  uint2 stack[kTaskDepth][32];
+  float px[32], py[32], pz[32];
+  uint32_t nref[32];
+  uint8_t nown[32];
+  float boxd[128];
+  uint32_t boxr[128];
+  uint32_t tidx[kTaskTriCap];
+  float trid[kTaskTriCap];
+  uint8_t town[kTaskTriCap];
+};
+
+enum : int { kIdle = 0, kProbe = 1, kSeed = 2, kTrav = 3, kAbandon = 4 };
+
+template <bool kSign, bool kStats>
+__global__ void __launch_bounds__(kTaskWarps * 32)
+    udf_task_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
+                    const float* __restrict__ pts, int64_t n, const uint32_t* __restrict__ perm,
+                    const float* __restrict__ bound, QueryOut out, SignArgs sg, unsigned long long* stats,
+                    uint32_t* __restrict__ rerun, uint32_t* __restrict__ nrerun, uint32_t* __restrict__ pool_counter) {
+  __shared__ TaskSmem smem[kTaskWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  TaskSmem& S = smem[warp];
+  const unsigned FULL = 0xffffffffu;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  // persistent warps: pools of kTaskPool consecutive (sorted) queries are
+  // taken from a global counter; inside a pool, lanes take queries as they
+  // finish their previous one
+  int64_t pos = 0, end = 0;
+  bool exhausted = false;
+  Counters ctr{0, 0};
+
+  // owner state
+  int64_t qi = -1, kprev = -(1ll << 40);
+  int phase = kIdle;
+  uint32_t ref = 0, prev = 0xffffffffu, best_tri = 0xffffffffu;
+  float best_sq = INFINITY, px = 0.f, py = 0.f, pz = 0.f, bsq = INFINITY;
+  bool have = false;
+  int sp = 0;
+
+  auto start = [&](int64_t k) {
+    qi = perm ? (int64_t)perm[k] : k;
+    px = pts[3 * qi]; py = pts[3 * qi + 1]; pz = pts[3 * qi + 2];
+    S.px[lane] = px; S.py[lane] = py; S.pz[lane] = pz;
+    bsq = INFINITY;
+    if (bound) {
+      const float b = bound[qi];
+      if (b * b >= 0.f) bsq = b * b;
+    }
+    best_sq = INFINITY;
+    best_tri = 0xffffffffu;
+    sp = 0;
+    // the previous result seeds the radius only for a nearby query in the
+    // sorted order; otherwise a greedy probe does
+    if (prev != 0xffffffffu && k - kprev <= 64 && k > kprev) {
+      phase = kSeed;
+    } else {
+      prev = 0xffffffffu;
+      phase = kProbe;
+      ref = 0;
+      have = true;
+    }
+    kprev = k;
+  };
+
+  // hands new queries to the lanes in `want` (warp-uniform bookkeeping)
+  auto distribute = [&](unsigned want) {
+    while (want) {
+      if (pos >= end) {
+        if (exhausted) break;
+        uint32_t p = 0;
+        if (lane == 0) p = atomicAdd(pool_counter, 1u);
+        p = __shfl_sync(FULL, p, 0);
+        pos = (int64_t)p * kTaskPool;
+        end = pos + kTaskPool < n ? pos + kTaskPool : n;
+        if (pos >= n) { exhausted = true; break; }
+      }
+      const int64_t avail = end - pos;
+      const int cnt = __popc(want);
+      const int take = (int)(avail < cnt ? avail : cnt);
+      const int rank = __popc(want & lt_mask);
+      const bool mine = ((want >> lane) & 1u) && rank < take;
+      if (mine) start(pos + rank);
+      pos += take;
+      want &= ~__ballot_sync(FULL, mine);
+    }
+  };
+  distribute(FULL);
+
+  while (__any_sync(FULL, phase != kIdle)) {
+    // (a) traversing owners without an item pop; finished owners emit and refetch
+    bool done = false;
+    if (phase == kTrav && !have) {
+      while (sp > 0) {
+        --sp;
+        const uint2 e = S.stack[sp][lane];
+        if (__uint_as_float(e.y) < best_sq) { ref = e.x; have = true; break; }
+      }
+      done = !have;
+    }
+    if (phase == kAbandon) done = true;
+    if (done) {
+      if (phase == kAbandon || best_tri == 0xffffffffu) {
+        rerun[atomicAdd(nrerun, 1u)] = (uint32_t)qi;
+        prev = 0xffffffffu;
+      } else {
+        finish_query(tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
+        prev = best_tri;
+      }
+      phase = kIdle;
+    }
+    distribute(__ballot_sync(FULL, done));
+    // (b) classify this round's item
+    const bool is_node = (phase == kProbe || phase == kTrav) && have && !ref_is_leaf(ref);
+    const bool is_leaf = (phase == kProbe || phase == kTrav) && have && ref_is_leaf(ref);
+    const bool is_seed = phase == kSeed;
+    const unsigned nmask = __ballot_sync(FULL, is_node);
+    const int nrank = __popc(nmask & lt_mask);
+    const int nnodes = __popc(nmask);
+    if (is_node) {
+      S.nref[nrank] = ref;
+      S.nown[nrank] = (uint8_t)lane;
+      if (kStats) ++ctr.nodes;
+    }
+    const int tcnt = is_leaf ? (int)leaf_count(ref) : (is_seed ? 1 : 0);
+    int toff = tcnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(FULL, toff, o);
+      if (lane >= o) toff += v;
+    }
+    const int ttotal = __shfl_sync(FULL, toff, 31);
+    toff -= tcnt;
+    if (tcnt > 0) {
+      const uint32_t f0 = is_seed ? prev : leaf_first(ref);
+      for (int i = 0; i < tcnt; ++i) {
+        S.tidx[toff + i] = f0 + i;
+        S.town[toff + i] = (uint8_t)lane;
+      }
+      if (kStats) ctr.tris += tcnt;
+    }
+    __syncwarp();
+    // (c) dense evaluation: child boxes, then triangles
+    for (int t = lane; t < 4 * nnodes; t += 32) {
+      const int r = t >> 2, c = t & 3;
+      const int o = S.nown[r];
+      float d;
+      uint32_t cr;
+      quad_child_box(nodes, S.nref[r], c, S.px[o], S.py[o], S.pz[o], d, cr);
+      S.boxd[t] = d;
+      S.boxr[t] = cr;
+    }
+    for (int t = lane; t < ttotal; t += 32) {
+      const int o = S.town[t];
+      S.trid[t] = tri_dist_sq(load_tri(tris, S.tidx[t]), S.px[o], S.py[o], S.pz[o]);
+    }
+    __syncwarp();
+    // (d) owners consume their results
+    if (is_node) {
+      float d[4];
+      uint32_t r[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        d[c] = S.boxd[4 * nrank + c];
+        r[c] = S.boxr[4 * nrank + c];
+      }
+      if (phase == kProbe) {
+        // greedy: the (distance, ref)-smallest child
+        float bd = d[0];
+        uint32_t br = r[0];
+#pragma unroll
+        for (int c = 1; c < 4; ++c)
+          if (child_less(d[c], r[c], bd, br)) { bd = d[c]; br = r[c]; }
+        ref = br;
+      } else {
+        cswap(d[0], r[0], d[1], r[1]);
+        cswap(d[2], r[2], d[3], r[3]);
+        cswap(d[0], r[0], d[2], r[2]);
+        cswap(d[1], r[1], d[3], r[3]);
+        cswap(d[1], r[1], d[2], r[2]);
+        int q = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) q += d[c] < best_sq ? 1 : 0;
+        if (q > 0) {
+          if (sp + (q - 1) > kTaskDepth) {
+            // would overflow: the deep-stack kernel re-runs the query
+            phase = kAbandon;
+            have = false;
+          } else {
+#pragma unroll
+            for (int c = 3; c >= 1; --c)
+              if (c < q) S.stack[sp++][lane] = make_uint2(r[c], __float_as_uint(d[c]));
+            ref = r[0];
+          }
+        } else {
+          have = false;
+        }
+      }
+    } else if (is_leaf || is_seed) {
+      float dmin = INFINITY;
+      uint32_t imin = 0xffffffffu;
+      for (int i = 0; i < tcnt; ++i) {
+        const float dd = S.trid[toff + i];
+        if (dd < dmin) { dmin = dd; imin = S.tidx[toff + i]; }
+      }
+      if (phase == kTrav) {
+        if (dmin < best_sq) { best_sq = dmin; best_tri = imin; }
+        have = false;
+      } else {
+        // probe leaf or seed triangle: radius just above its distance
+        float b = dmin < INFINITY ? nextafterf(dmin, INFINITY) : INFINITY;
+        if (bsq < b) b = bsq;
+        best_sq = b;
+        phase = kTrav;
+        ref = 0;
+        have = true;
+      }
+    }
+    __syncwarp();
   }
   if (kStats) flush_counters(ctr, stats);
 }
@@ -376,7 +654,10 @@ __global__ void __launch_bounds__(64)
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t qi = rerun[t];
     const float px = pts[3 * qi], py = pts[3 * qi + 1], pz = pts[3 * qi + 2];
-    float best_sq = INFINITY;
+    uint32_t seed_tri;
+    float seed_sq;
+    probe(nodes, tris, px, py, pz, seed_tri, seed_sq, ctr);
+    float best_sq = seed_sq < INFINITY ? nextafterf(seed_sq, INFINITY) : INFINITY;
     uint32_t best_tri = 0xffffffffu;
     LocalStack st;
     st.sp = 0;
@@ -433,17 +714,37 @@ size_t carve_udf(UdfWs& w, Workspace& ws, int64_t n, uint32_t flags) {
 }
 
 template <bool kSign, bool kStats>
-int launch_udf(const a3d_bvh_view* bvh, const float* pts, int64_t n, const uint32_t* perm, const float* bound,
-               const QueryOut& out, const SignArgs& sg, unsigned long long* stats, UdfWs& w, cudaStream_t s) {
+int launch_udf(const a3d_bvh_view* bvh, const float* pts, int64_t n, const uint32_t* perm, bool coherent,
+               const float* bound, const QueryOut& out, const SignArgs& sg, unsigned long long* stats, UdfWs& w,
+               cudaStream_t s) {
   const WideNode* nodes = (const WideNode*)bvh->nodes;
   const TriRec* tris = (const TriRec*)bvh->tris;
-  const int chunk = perm ? kQueriesPerThread : 1;
-  const int64_t nthreads = ceil_div(n, chunk);
-  udf_kernel<kSign, kStats><<<(unsigned)ceil_div(nthreads, kUdfThreads), kUdfThreads, 0, s>>>(
-      nodes, tris, pts, n, chunk, perm, bound, out, sg, stats, w.rerun, w.nrerun);
+  if (coherent) {
+    static int blocks_per_sm[2][2] = {{0, 0}, {0, 0}};
+    int& bps = blocks_per_sm[kSign][kStats];
+    if (bps == 0) {
+      A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, udf_task_kernel<kSign, kStats>,
+                                                                 kTaskWarps * 32, 0));
+      if (bps < 1) bps = 1;
+    }
+    int dev = 0, sms = kNumSMs;
+    A3D_CUDA_TRY(cudaGetDevice(&dev));
+    A3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t pools = ceil_div(n, kTaskPool);
+    const int64_t want_blocks = ceil_div(pools, kTaskWarps);
+    const int64_t grid = want_blocks < (int64_t)sms * bps ? want_blocks : (int64_t)sms * bps;
+    udf_task_kernel<kSign, kStats><<<(unsigned)grid, kTaskWarps * 32, 0, s>>>(
+        nodes, tris, pts, n, perm, bound, out, sg, stats, w.rerun, w.nrerun, w.nrerun + 2);
+  } else {
+    udf_kernel<kSign, kStats><<<(unsigned)ceil_div(n, kUdfThreads), kUdfThreads, 0, s>>>(
+        nodes, tris, pts, n, 1, perm, bound, out, sg, stats, w.rerun, w.nrerun);
+  }
   A3D_LAUNCH_CHECK();
-  udf_rerun_kernel<kSign, kStats><<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, pts, w.rerun, w.nrerun, out, sg, stats,
-                                                            (int*)(w.nrerun + 1));
+  // the re-run list length is only known on the device: launch enough
+  // threads for a few percent of the queries, each thread strides
+  const int64_t rr_threads = n / 16 > (int64_t)kNumSMs * 256 ? n / 16 : (int64_t)kNumSMs * 256;
+  udf_rerun_kernel<kSign, kStats><<<(unsigned)ceil_div(rr_threads, 64), 64, 0, s>>>(
+      nodes, tris, pts, w.rerun, w.nrerun, out, sg, stats, (int*)(w.nrerun + 1));
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
@@ -534,6 +835,7 @@ extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num
     A3D_TRY(radix_sort_pairs<uint32_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, n, 0, 32, w.rs_scratch, &alt, s));
     perm = alt ? w.vals_alt : w.vals;
   }
+  const bool coherent = perm != nullptr || (flags & A3D_UDF_ASSUME_SORTED) != 0;
   A3D_CUDA_TRY(cudaMemsetAsync(w.nrerun, 0, 4 * sizeof(uint32_t), s));
   QueryOut out{distances, face_ids, closest_points, uvw};
   SignArgs sg{nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -543,11 +845,11 @@ extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num
                   pn ? sign->he_edge_idx : nullptr, sign->faces};
   }
   if (sign) {
-    if (stats) A3D_TRY((launch_udf<true, true>(bvh, points, n, perm, bound, out, sg, stats, w, s)));
-    else A3D_TRY((launch_udf<true, false>(bvh, points, n, perm, bound, out, sg, stats, w, s)));
+    if (stats) A3D_TRY((launch_udf<true, true>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, s)));
+    else A3D_TRY((launch_udf<true, false>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, s)));
   } else {
-    if (stats) A3D_TRY((launch_udf<false, true>(bvh, points, n, perm, bound, out, sg, stats, w, s)));
-    else A3D_TRY((launch_udf<false, false>(bvh, points, n, perm, bound, out, sg, stats, w, s)));
+    if (stats) A3D_TRY((launch_udf<false, true>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, s)));
+    else A3D_TRY((launch_udf<false, false>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, s)));
   }
   if (stats) {
     // reruns are reported as bound misses / spills (same counter: re-run queries)

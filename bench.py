@@ -328,9 +328,9 @@ def launches_per_udf():
 
 
 def time_traversal_kernel(bvh, qd, dist_o, fid_o, cp_o, ws, flags, stream, steps):
-    """Average duration of the traversal launch itself: the same call with
-    pre-sorted queries and sorting disabled, so only the traversal kernel
-    (plus its empty re-run launch) is inside the events."""
+    """Average duration of the traversal launch itself: the same call on
+    pre-sorted queries with A3D_UDF_ASSUME_SORTED, so only the traversal
+    kernel (plus its empty re-run launch) is inside the events."""
     import ctypes
 
     from atom3d_b200 import _lib, synthetic  # noqa: F401
@@ -353,7 +353,8 @@ def time_traversal_kernel(bvh, qd, dist_o, fid_o, cp_o, ws, flags, stream, steps
 
     def call():
         _lib.call("a3d_udf", ctypes.byref(view), qs.data_ptr(), n, dist_o.data_ptr(), fid_o.data_ptr(),
-                  cp_o.data_ptr(), None, None, None, None, 0, ws.data_ptr(), ws.numel(), stream.cuda_stream)
+                  cp_o.data_ptr(), None, None, None, None, _lib.A3D_UDF_ASSUME_SORTED, ws.data_ptr(), ws.numel(),
+                  stream.cuda_stream)
 
     for _ in range(3):
         call()

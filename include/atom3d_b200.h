@@ -38,11 +38,11 @@ const char* a3d_version(void);
 
 /* ---- BVH ---------------------------------------------------------------- */
 /* Device-resident wide BVH: 64-byte 4-wide quantised nodes (node 0 = root)
- * and 48-byte triangle records stored in leaf order.  The memory is owned by
+ * and 64-byte triangle records stored in leaf order.  The memory is owned by
  * the caller; a3d_bvh_build fills it. */
 typedef struct a3d_bvh_view {
   const void* nodes;   /* num_nodes x 64 B, 64-B aligned                     */
-  const void* tris;    /* num_tris  x 48 B, 16-B aligned                     */
+  const void* tris;    /* num_tris  x 64 B, 16-B aligned                     */
   int64_t num_nodes;
   int64_t num_tris;
   float lo[3];         /* scene bounds (triangle AABB union)                 */
@@ -50,17 +50,18 @@ typedef struct a3d_bvh_view {
 } a3d_bvh_view;
 
 #define A3D_BVH_NODE_BYTES 64
-#define A3D_BVH_TRI_BYTES 48
+#define A3D_BVH_TRI_BYTES 64
 
 /* Replaces build_bvh_cuda / build_bvh_recursive
  * (atom3d/kernels/bvh_kernels.cu:860-925, :667-854) behind
  * BVHAccelerator.__init__ (atom3d/kernels/bvh.py:66-93).
  * GPU build: Morton codes -> in-house radix sort -> binary radix tree ->
  * bottom-up refit -> SAH-guided collapse into 4-wide quantised nodes.
- * node_capacity >= max(num_faces, 1) always suffices. */
+ * node_capacity >= max(num_faces, 1) always suffices.  leaf_max (1..8, 0 =
+ * default 4): subtrees with at most this many triangles become leaves. */
 size_t a3d_bvh_build_workspace_bytes(int64_t num_faces);
 int a3d_bvh_build(const float* vertices, int64_t num_vertices,
-                  const int32_t* faces, int64_t num_faces,
+                  const int32_t* faces, int64_t num_faces, int leaf_max,
                   void* nodes_out, int64_t node_capacity, void* tris_out,
                   void* workspace, size_t workspace_bytes,
                   int64_t* num_nodes_out /* host */,
@@ -99,10 +100,12 @@ typedef struct a3d_sign_data {
  * uvw may be NULL.  bound (nullable) is a per-query upper bound on the
  * unsigned distance that seeds the pruning radius; queries whose bound proves
  * too small are re-run unbounded, so results never depend on it.
- * flags: A3D_UDF_SORT_QUERIES (Morton-sort queries for warp coherence).
+ * flags: A3D_UDF_SORT_QUERIES (Morton-sort queries for warp coherence),
+ * A3D_UDF_ASSUME_SORTED (caller's order is already coherent).
  * stats (nullable, device, 4 x uint64): node visits, triangle tests,
  * bound misses, stack spills.  */
 #define A3D_UDF_SORT_QUERIES 1u
+#define A3D_UDF_ASSUME_SORTED 2u  /* queries already spatially coherent: skip the sort */
 size_t a3d_udf_workspace_bytes(int64_t num_points, uint32_t flags);
 int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num_points,
             float* distances, int32_t* face_ids, float* closest_points,

@@ -35,7 +35,7 @@ def test_version_and_error_string(lib):
 
 def test_argument_errors_are_reported_without_a_gpu(lib):
     # a null mesh is rejected before any CUDA call
-    st = lib.a3d_bvh_build(None, 0, None, 0, None, 0, None, None, 0, None, None, None)
+    st = lib.a3d_bvh_build(None, 0, None, 0, 0, None, 0, None, None, 0, None, None, None)
     assert st == 1  # A3D_ERR_ARGUMENT
     assert b"empty mesh" in lib.a3d_last_error()
 
