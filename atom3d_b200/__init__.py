@@ -12,6 +12,7 @@ from .core.data_structures import AABBIntersectResult, ClosestPointResult
 from .core.mesh_bvh import MeshBVH
 from .grid.cube_grid import CubeGrid
 from .grid.octree_indexer import OctreeIndexer
+from .apps.sparse_flood_fill import flood_fill_3d_sparse, sparse_flood_fill
 
 __all__ = [
     "MeshBVH",
@@ -19,4 +20,6 @@ __all__ = [
     "ClosestPointResult",
     "OctreeIndexer",
     "CubeGrid",
+    "sparse_flood_fill",
+    "flood_fill_3d_sparse",
 ]

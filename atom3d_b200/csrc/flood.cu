@@ -1,0 +1,528 @@
+// Flood fill of the octree's dam voxels on a bit-packed crop, plus the dam
+// neighbourhood classification.
+//
+// Replaces flood_fill_3d_sparse + flood_fill_kernel + the host BFS loop
+// (atom3d/kernels/flood_fill.py:118-258, atom3d/kernels/flood_fill_kernels.cu:
+// 21-175) and get_dam_neighborhood_signs (atom3d/apps/sparse_flood_fill.py:
+// 34-100).  The reference's labels are set properties of the crop:
+//   water W    the connected component (6/18/26-connectivity) of free voxels
+//              containing the seed
+//   collision  W voxels with an occupied neighbour
+//   dam        occupied voxels with a W neighbour, plus (extension) occupied
+//              voxels in the 6-cross (connectivity 6) or 3x3x3 (otherwise)
+//              dilation of W
+//   dry        everything else in the crop
+// so they are computed here with bit operations instead of a BFS:
+//   * volume: one bit per voxel, 32 z-voxels per word, rows (x, y) in raster
+//     order, so extraction in word order is the reference's lexicographic
+//     (x, y, z) nonzero order;
+//   * W grows by monotone relaxation over 32x32-row bricks: a CTA loads its
+//     brick and a one-row halo into shared memory and iterates (dilate in
+//     x/y, flood whole free runs along z with a Kogge-Stone prefix) until
+//     the brick is stable, then marks its neighbours dirty if it changed.
+//     Bits only ever get set, so reading a neighbour's word while it is
+//     being updated is safe; rounds repeat until no brick is dirty;
+//   * labels, k-ring dilation and counts are word-parallel passes; the
+//     coordinates are written after an exclusive scan of per-word counts.
+#include <limits.h>
+
+#include "primitives.cuh"
+
+namespace a3d {
+namespace {
+
+constexpr int kBX = 32, kBY = 32;  // rows per brick (one word of 32 z each)
+
+struct Geom {
+  int nx, ny, nz, nw;      // volume size, words per row
+  int vx, vy, vz;          // volume origin in grid coordinates
+  int cx0, cy0, cz0;       // crop box (flood domain) in volume coordinates
+  int cx1, cy1, cz1;       // inclusive
+  int conn;
+};
+
+__device__ __forceinline__ int64_t widx(const Geom& g, int x, int y, int w) {
+  return ((int64_t)x * g.ny + y) * g.nw + w;
+}
+
+// z bits of word w inside [lo, hi] (inclusive), volume coordinates
+__device__ __forceinline__ uint32_t zmask(int w, int lo, int hi) {
+  const int b0 = w * 32, b1 = b0 + 31;
+  if (hi < b0 || lo > b1) return 0u;
+  const int s = lo > b0 ? lo - b0 : 0;
+  const int e = hi < b1 ? hi - b0 : 31;
+  const uint32_t top = e == 31 ? 0xffffffffu : ((1u << (e + 1)) - 1u);
+  return top & ~((1u << s) - 1u);
+}
+
+__device__ __forceinline__ uint32_t valid_mask(const Geom& g, int w) { return zmask(w, 0, g.nz - 1); }
+
+__device__ __forceinline__ uint32_t crop_mask(const Geom& g, int x, int y, int w) {
+  if (x < g.cx0 || x > g.cx1 || y < g.cy0 || y > g.cy1) return 0u;
+  return zmask(w, g.cz0, g.cz1);
+}
+
+// all free bits connected (along z, inside this word) to a bit of r
+__device__ __forceinline__ uint32_t fill_runs(uint32_t r, uint32_t f) {
+  r &= f;
+  uint32_t m = f;
+  uint32_t u = r;
+  u |= (u << 1) & m; m &= m << 1;
+  u |= (u << 2) & m; m &= m << 2;
+  u |= (u << 4) & m; m &= m << 4;
+  u |= (u << 8) & m; m &= m << 8;
+  u |= (u << 16) & m;
+  m = f;
+  uint32_t d = r;
+  d |= (d >> 1) & m; m &= m >> 1;
+  d |= (d >> 2) & m; m &= m >> 2;
+  d |= (d >> 4) & m; m &= m >> 4;
+  d |= (d >> 8) & m; m &= m >> 8;
+  d |= (d >> 16) & m;
+  return u | d;
+}
+
+// z-dilation of word c with its neighbours a (w-1) and b (w+1)
+__device__ __forceinline__ uint32_t zdil(uint32_t a, uint32_t c, uint32_t b) {
+  return c | (c << 1) | (c >> 1) | (a >> 31) | (b << 31);
+}
+
+__global__ void bbox_kernel(const int64_t* __restrict__ ijk, int64_t n, long long* __restrict__ bb) {
+  long long lo[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, hi[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const long long v = ijk[3 * i + a];
+      lo[a] = v < lo[a] ? v : lo[a];
+      hi[a] = v > hi[a] ? v : hi[a];
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const long long l = __shfl_xor_sync(0xffffffffu, lo[a], o), h = __shfl_xor_sync(0xffffffffu, hi[a], o);
+      lo[a] = l < lo[a] ? l : lo[a];
+      hi[a] = h > hi[a] ? h : hi[a];
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int a = 0; a < 3; ++a) {
+      atomicMin(&bb[a], lo[a]);
+      atomicMax(&bb[3 + a], hi[a]);
+    }
+  }
+}
+
+__global__ void set_bits_kernel(const int64_t* __restrict__ ijk, int64_t n, Geom g, uint32_t* __restrict__ vol) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int x = (int)(ijk[3 * i] - g.vx), y = (int)(ijk[3 * i + 1] - g.vy), z = (int)(ijk[3 * i + 2] - g.vz);
+  if (x < 0 || y < 0 || z < 0 || x >= g.nx || y >= g.ny || z >= g.nz) return;
+  atomicOr(&vol[widx(g, x, y, z >> 5)], 1u << (z & 31));
+}
+
+// one relaxation round over the dirty bricks
+__global__ void __launch_bounds__(kBX * kBY) flood_brick_kernel(Geom g, const uint32_t* __restrict__ occ,
+                                                              uint32_t* water, const uint8_t* __restrict__ dirty,
+                                                              uint8_t* __restrict__ next_dirty, int nbx, int nby,
+                                                              int max_iters, uint32_t* __restrict__ any_dirty) {
+  const int bid = blockIdx.x;
+  if (!dirty[bid]) return;
+  const int bw = bid / (nbx * nby);
+  const int rem = bid % (nbx * nby);
+  const int bxi = rem / nby, byi = rem % nby;
+  const int x0 = bxi * kBX, y0 = byi * kBY;
+  __shared__ uint32_t s_r[3][kBX + 2][kBY + 2];  // words w-1, w, w+1 of the rows with halo
+  const int tx = threadIdx.x / kBY, ty = threadIdx.x % kBY;
+  // load the halo'd water words (monotone: a racing update is harmless)
+  for (int i = threadIdx.x; i < 3 * (kBX + 2) * (kBY + 2); i += blockDim.x) {
+    const int k = i / ((kBX + 2) * (kBY + 2));
+    const int r2 = i % ((kBX + 2) * (kBY + 2));
+    const int hx = r2 / (kBY + 2), hy = r2 % (kBY + 2);
+    const int x = x0 + hx - 1, y = y0 + hy - 1, w = bw + k - 1;
+    uint32_t v = 0;
+    if (x >= 0 && x < g.nx && y >= 0 && y < g.ny && w >= 0 && w < g.nw) v = __ldcg(&water[widx(g, x, y, w)]);
+    s_r[k][hx][hy] = v;
+  }
+  const int x = x0 + tx, y = y0 + ty;
+  const bool inside = x < g.nx && y < g.ny;
+  uint32_t f = 0;
+  if (inside) f = ~occ[widx(g, x, y, bw)] & crop_mask(g, x, y, bw);
+  __syncthreads();
+  const uint32_t orig = s_r[1][tx + 1][ty + 1];
+  bool changed_any = false;
+  for (int it = 0; it < max_iters; ++it) {
+    uint32_t acc = 0;
+    const uint32_t self = s_r[1][tx + 1][ty + 1];
+    // neighbours along z of this row (words of the adjacent bricks)
+    acc |= (s_r[0][tx + 1][ty + 1] >> 31) | (s_r[2][tx + 1][ty + 1] << 31);
+#pragma unroll
+    for (int dx = -1; dx <= 1; ++dx) {
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy) {
+        if (dx == 0 && dy == 0) continue;
+        const int l1 = (dx != 0) + (dy != 0);
+        const uint32_t a = s_r[0][tx + 1 + dx][ty + 1 + dy];
+        const uint32_t c = s_r[1][tx + 1 + dx][ty + 1 + dy];
+        const uint32_t b = s_r[2][tx + 1 + dx][ty + 1 + dy];
+        if (g.conn == 6) {
+          if (l1 == 1) acc |= c;
+        } else if (g.conn == 18) {
+          acc |= (l1 == 1) ? zdil(a, c, b) : c;
+        } else {
+          acc |= zdil(a, c, b);
+        }
+      }
+    }
+    const uint32_t nw = inside ? fill_runs(self | (acc & f), f) | self : self;
+    const bool ch = nw != self;
+    if (ch) s_r[1][tx + 1][ty + 1] = nw;
+    changed_any |= ch;
+    if (!__syncthreads_or(ch)) break;
+  }
+  const uint32_t fin = s_r[1][tx + 1][ty + 1];
+  if (inside && fin != orig) water[widx(g, x, y, bw)] = fin;
+  if (__syncthreads_or(inside && fin != orig)) {
+    if (threadIdx.x < 27) {
+      const int dz = threadIdx.x / 9 - 1, dxx = (threadIdx.x / 3) % 3 - 1, dyy = threadIdx.x % 3 - 1;
+      const int nbw = bw + dz, nbxx = bxi + dxx, nbyy = byi + dyy;
+      const int nbz = (g.nw + 0);
+      if (nbw >= 0 && nbw < nbz && nbxx >= 0 && nbxx < nbx && nbyy >= 0 && nbyy < nby) {
+        next_dirty[(nbw * nbx + nbxx) * nby + nbyy] = 1;
+        *any_dirty = 1u;
+      }
+    }
+  }
+  (void)changed_any;
+}
+
+// label volumes.  slot order: 0 water(pure) 1 dry 2 tide(collision) 3 dam
+// 4 extended dam 5 extended tide 6 dry adjacent 7 ring (scratch)
+enum { kWater = 0, kDry = 1, kTide = 2, kDam = 3, kExt = 4, kExtTide = 5, kDryAdj = 6, kRing = 7, kLabels = 8 };
+
+template <int kConn>
+__device__ __forceinline__ uint32_t dil_conn(const uint32_t* __restrict__ v, const Geom& g, int x, int y, int w) {
+  uint32_t acc = 0;
+  auto word = [&](int xx, int yy, int ww) -> uint32_t {
+    if (xx < 0 || yy < 0 || ww < 0 || xx >= g.nx || yy >= g.ny || ww >= g.nw) return 0u;
+    return v[widx(g, xx, yy, ww)];
+  };
+  const uint32_t c0 = word(x, y, w);
+  acc |= (c0 << 1) | (c0 >> 1) | (word(x, y, w - 1) >> 31) | (word(x, y, w + 1) << 31);
+#pragma unroll
+  for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+      if (dx == 0 && dy == 0) continue;
+      const int l1 = (dx != 0) + (dy != 0);
+      if (kConn == 6 && l1 != 1) continue;
+      const uint32_t c = word(x + dx, y + dy, w);
+      if (kConn == 6 || (kConn == 18 && l1 == 2)) {
+        acc |= c;
+      } else {
+        acc |= zdil(word(x + dx, y + dy, w - 1), c, word(x + dx, y + dy, w + 1));
+      }
+    }
+  return acc;
+}
+
+__global__ void labels_kernel(Geom g, const uint32_t* __restrict__ occ, const uint32_t* __restrict__ water,
+                              uint32_t* __restrict__ lab, int64_t nwords) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nwords) return;
+  const int w = (int)(i % g.nw);
+  const int64_t row = i / g.nw;
+  const int y = (int)(row % g.ny), x = (int)(row / g.ny);
+  const uint32_t crop = crop_mask(g, x, y, w);
+  const uint32_t o = occ[i] & crop, r = water[i] & crop;
+  uint32_t near_occ, near_w;
+  if (g.conn == 6) {
+    near_occ = dil_conn<6>(occ, g, x, y, w);
+    near_w = dil_conn<6>(water, g, x, y, w);
+  } else if (g.conn == 18) {
+    near_occ = dil_conn<18>(occ, g, x, y, w);
+    near_w = dil_conn<18>(water, g, x, y, w);
+  } else {
+    near_occ = dil_conn<26>(occ, g, x, y, w);
+    near_w = dil_conn<26>(water, g, x, y, w);
+  }
+  const uint32_t near_w_ext = g.conn == 6 ? near_w : (g.conn == 18 ? dil_conn<26>(water, g, x, y, w) : near_w);
+  const uint32_t tide = r & near_occ;
+  const uint32_t dam0 = o & near_w;
+  const uint32_t ext = o & ~dam0 & near_w_ext;
+  const uint32_t dam = dam0 | ext;
+  const int64_t nwv = nwords;
+  lab[kWater * nwv + i] = r & ~tide;
+  lab[kTide * nwv + i] = tide;
+  lab[kDam * nwv + i] = dam;
+  lab[kExt * nwv + i] = ext;
+  lab[kDry * nwv + i] = crop & ~r & ~dam;
+}
+
+// 3x3x3 box dilation of src into dst (one ring of get_dam_neighborhood_signs)
+__global__ void box_dilate_kernel(Geom g, const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                                  int64_t nwords) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nwords) return;
+  const int w = (int)(i % g.nw);
+  const int64_t row = i / g.nw;
+  const int y = (int)(row % g.ny), x = (int)(row / g.ny);
+  dst[i] = (src[i] | dil_conn<26>(src, g, x, y, w)) & valid_mask(g, w);
+}
+
+__global__ void ring_classify_kernel(const uint32_t* __restrict__ ring, uint32_t* __restrict__ lab, int64_t nwords) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nwords) return;
+  const uint32_t n = ring[i];
+  const uint32_t dam = lab[kDam * nwords + i], dry = lab[kDry * nwords + i];
+  lab[kExtTide * nwords + i] = n & ~dam & ~dry;
+  lab[kDryAdj * nwords + i] = n & dry & ~dam;
+}
+
+__global__ void popc_kernel(const uint32_t* __restrict__ v, int64_t n, uint32_t* __restrict__ c) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) c[i] = (uint32_t)__popc(v[i]);
+}
+
+__global__ void extract_kernel(Geom g, const uint32_t* __restrict__ v, const int64_t* __restrict__ offs,
+                               int64_t nwords, int32_t* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nwords) return;
+  uint32_t m = v[i];
+  if (!m) return;
+  const int w = (int)(i % g.nw);
+  const int64_t row = i / g.nw;
+  const int y = (int)(row % g.ny), x = (int)(row / g.ny);
+  int64_t o = offs[i];
+  while (m) {
+    const int b = __ffs(m) - 1;
+    m &= m - 1;
+    out[3 * o] = x + g.vx;
+    out[3 * o + 1] = y + g.vy;
+    out[3 * o + 2] = w * 32 + b + g.vz;
+    ++o;
+  }
+}
+
+__global__ void test_bits_kernel(Geom g, const uint32_t* __restrict__ v, const int64_t* __restrict__ ijk, int64_t n,
+                                 uint8_t* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int x = (int)(ijk[3 * i] - g.vx), y = (int)(ijk[3 * i + 1] - g.vy), z = (int)(ijk[3 * i + 2] - g.vz);
+  uint8_t r = 0;
+  if (x >= 0 && y >= 0 && z >= 0 && x < g.nx && y < g.ny && z < g.nz)
+    r = (uint8_t)((v[widx(g, x, y, z >> 5)] >> (z & 31)) & 1u);
+  out[i] = r;
+}
+
+__global__ void seed_kernel(Geom g, const uint32_t* __restrict__ occ, uint32_t* __restrict__ water, int sx, int sy,
+                            int sz, uint32_t* __restrict__ status) {
+  const int64_t i = widx(g, sx, sy, sz >> 5);
+  const uint32_t bit = 1u << (sz & 31);
+  if (occ[i] & bit) {
+    status[0] = 1u;  // seed occupied
+  } else {
+    water[i] |= bit;
+    status[0] = 0u;
+  }
+}
+
+}  // namespace
+}  // namespace a3d
+
+using namespace a3d;
+
+namespace {
+Geom to_geom(const a3d_flood_geom* p) {
+  Geom g;
+  g.nx = p->vol_dims[0]; g.ny = p->vol_dims[1]; g.nz = p->vol_dims[2];
+  g.nw = (g.nz + 31) / 32;
+  g.vx = (int)p->vol_lo[0]; g.vy = (int)p->vol_lo[1]; g.vz = (int)p->vol_lo[2];
+  g.cx0 = (int)(p->crop_lo[0] - p->vol_lo[0]); g.cy0 = (int)(p->crop_lo[1] - p->vol_lo[1]);
+  g.cz0 = (int)(p->crop_lo[2] - p->vol_lo[2]);
+  g.cx1 = (int)(p->crop_hi[0] - p->vol_lo[0]); g.cy1 = (int)(p->crop_hi[1] - p->vol_lo[1]);
+  g.cz1 = (int)(p->crop_hi[2] - p->vol_lo[2]);
+  g.conn = p->connectivity;
+  return g;
+}
+
+struct FloodWs {
+  uint32_t* occ;
+  uint32_t* water;
+  uint32_t* lab;     // kLabels volumes
+  uint32_t* ring2;   // second ring buffer
+  uint8_t* dirty;
+  uint8_t* dirty2;
+  uint32_t* cnt;     // per-word counts
+  int64_t* offs;
+  int64_t* scan_tmp;
+  uint32_t* misc;    // [0] seed status [1] any dirty
+};
+
+size_t carve_flood(FloodWs& w, Workspace& ws, const Geom& g) {
+  const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
+  const int64_t nbricks = (int64_t)ceil_div(g.nx, kBX) * ceil_div(g.ny, kBY) * g.nw;
+  w.occ = ws.take<uint32_t>(nwords);
+  w.water = ws.take<uint32_t>(nwords);
+  w.lab = ws.take<uint32_t>(kLabels * nwords);
+  w.ring2 = ws.take<uint32_t>(nwords);
+  w.dirty = ws.take<uint8_t>(nbricks);
+  w.dirty2 = ws.take<uint8_t>(nbricks);
+  w.cnt = ws.take<uint32_t>(nwords);
+  w.offs = ws.take<int64_t>(nwords + 1);
+  w.scan_tmp = ws.take<int64_t>((int64_t)scan_workspace_elems(nwords));
+  w.misc = ws.take<uint32_t>(8);
+  return ws.used;
+}
+}  // namespace
+
+extern "C" int a3d_flood_bbox(const int64_t* ijk, int64_t n, int64_t* bbox_out, void* workspace,
+                              size_t workspace_bytes, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(n > 0 && ijk && bbox_out, A3D_ERR_ARGUMENT, "flood_bbox: empty input");
+  A3D_REQUIRE(workspace && workspace_bytes >= 6 * sizeof(long long), A3D_ERR_WORKSPACE, "flood_bbox: workspace");
+  long long init[6] = {LLONG_MAX, LLONG_MAX, LLONG_MAX, LLONG_MIN, LLONG_MIN, LLONG_MIN};
+  long long* bb = (long long*)workspace;
+  A3D_CUDA_TRY(cudaMemcpyAsync(bb, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  const int64_t blocks = ceil_div(n, 256) < 4096 ? ceil_div(n, 256) : 4096;
+  bbox_kernel<<<(unsigned)blocks, 256, 0, s>>>(ijk, n, bb);
+  A3D_LAUNCH_CHECK();
+  long long h[6];
+  A3D_CUDA_TRY(cudaMemcpyAsync(h, bb, sizeof(h), cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int a = 0; a < 6; ++a) bbox_out[a] = h[a];
+  return A3D_OK;
+}
+
+extern "C" size_t a3d_flood_workspace_bytes(const a3d_flood_geom* geom) {
+  if (!geom) return 0;
+  Geom g = to_geom(geom);
+  Workspace ws(nullptr, 0);
+  FloodWs w;
+  return carve_flood(w, ws, g) + 256;
+}
+
+extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood_geom* geom, void* workspace,
+                              size_t workspace_bytes, int64_t* counts_out, int* rounds_out, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(geom && counts_out, A3D_ERR_ARGUMENT, "flood_fill: null argument");
+  const int conn = geom->connectivity;
+  A3D_REQUIRE(conn == 6 || conn == 18 || conn == 26, A3D_ERR_ARGUMENT, "flood_fill: connectivity must be 6, 18 or 26");
+  A3D_REQUIRE(geom->k_ring >= 0, A3D_ERR_ARGUMENT, "flood_fill: k_ring must be >= 0");
+  Geom g = to_geom(geom);
+  A3D_REQUIRE(g.nx > 0 && g.ny > 0 && g.nz > 0, A3D_ERR_ARGUMENT, "flood_fill: empty volume");
+  Workspace ws(workspace, workspace_bytes);
+  FloodWs w;
+  carve_flood(w, ws, g);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "flood_fill: workspace too small");
+  const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
+  const int nbx = (int)ceil_div(g.nx, kBX), nby = (int)ceil_div(g.ny, kBY);
+  const int64_t nbricks = (int64_t)nbx * nby * g.nw;
+  for (int k = 0; k < kLabels; ++k) counts_out[k] = 0;
+  A3D_CUDA_TRY(cudaMemsetAsync(w.occ, 0, nwords * 4, s));
+  A3D_CUDA_TRY(cudaMemsetAsync(w.water, 0, nwords * 4, s));
+  A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, 32, s));
+  if (n > 0) {
+    set_bits_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(dam_ijk, n, g, w.occ);
+    A3D_LAUNCH_CHECK();
+  }
+  const int sx = (int)(geom->seed[0] - geom->vol_lo[0]), sy = (int)(geom->seed[1] - geom->vol_lo[1]),
+            sz = (int)(geom->seed[2] - geom->vol_lo[2]);
+  A3D_REQUIRE(sx >= g.cx0 && sx <= g.cx1 && sy >= g.cy0 && sy <= g.cy1 && sz >= g.cz0 && sz <= g.cz1,
+              A3D_ERR_ARGUMENT, "flood_fill: seed outside the crop");
+  seed_kernel<<<1, 1, 0, s>>>(g, w.occ, w.water, sx, sy, sz, w.misc);
+  A3D_LAUNCH_CHECK();
+  uint32_t seed_status = 0;
+  A3D_CUDA_TRY(cudaMemcpyAsync(&seed_status, w.misc, 4, cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  if (seed_status) {
+    counts_out[kLabels] = 1;  // seed occupied: empty result, like the reference
+    return A3D_OK;
+  }
+  counts_out[kLabels] = 0;
+  // relaxation rounds over dirty bricks
+  A3D_CUDA_TRY(cudaMemsetAsync(w.dirty, 0, nbricks, s));
+  const int64_t sb = ((int64_t)(sz >> 5) * nbx + sx / kBX) * nby + sy / kBY;
+  const uint8_t one = 1;
+  A3D_CUDA_TRY(cudaMemcpyAsync(w.dirty + sb, &one, 1, cudaMemcpyHostToDevice, s));
+  uint8_t *cur = w.dirty, *nxt = w.dirty2;
+  int rounds = 0;
+  const int max_rounds = 1 << 20;
+  for (; rounds < max_rounds; ++rounds) {
+    A3D_CUDA_TRY(cudaMemsetAsync(nxt, 0, nbricks, s));
+    A3D_CUDA_TRY(cudaMemsetAsync(w.misc + 1, 0, 4, s));
+    flood_brick_kernel<<<(unsigned)nbricks, kBX * kBY, 0, s>>>(g, w.occ, w.water, cur, nxt, nbx, nby, 4 * (kBX + kBY),
+                                                                w.misc + 1);
+    A3D_LAUNCH_CHECK();
+    uint32_t any = 0;
+    A3D_CUDA_TRY(cudaMemcpyAsync(&any, w.misc + 1, 4, cudaMemcpyDeviceToHost, s));
+    A3D_CUDA_TRY(cudaStreamSynchronize(s));
+    uint8_t* t = cur; cur = nxt; nxt = t;
+    if (!any) break;
+  }
+  if (rounds_out) *rounds_out = rounds + 1;
+  const unsigned gw = (unsigned)ceil_div(nwords, 256);
+  labels_kernel<<<gw, 256, 0, s>>>(g, w.occ, w.water, w.lab, nwords);
+  A3D_LAUNCH_CHECK();
+  // k-ring box dilation of the dam, ping-ponging ring buffers
+  uint32_t* ring_a = w.lab + (int64_t)kRing * nwords;
+  A3D_CUDA_TRY(cudaMemcpyAsync(ring_a, w.lab + (int64_t)kDam * nwords, nwords * 4, cudaMemcpyDeviceToDevice, s));
+  uint32_t* ring_b = w.ring2;
+  for (int k = 0; k < geom->k_ring; ++k) {
+    box_dilate_kernel<<<gw, 256, 0, s>>>(g, ring_a, ring_b, nwords);
+    A3D_LAUNCH_CHECK();
+    uint32_t* t = ring_a; ring_a = ring_b; ring_b = t;
+  }
+  ring_classify_kernel<<<gw, 256, 0, s>>>(ring_a, w.lab, nwords);
+  A3D_LAUNCH_CHECK();
+  // counts per label
+  for (int k = 0; k < kRing; ++k) {
+    popc_kernel<<<gw, 256, 0, s>>>(w.lab + (int64_t)k * nwords, nwords, w.cnt);
+    A3D_LAUNCH_CHECK();
+    A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.cnt, w.offs, nwords, w.scan_tmp, w.offs + nwords, s)));
+    int64_t c = 0;
+    A3D_CUDA_TRY(cudaMemcpyAsync(&c, w.offs + nwords, 8, cudaMemcpyDeviceToHost, s));
+    A3D_CUDA_TRY(cudaStreamSynchronize(s));
+    counts_out[k] = c;
+  }
+  return A3D_OK;
+}
+
+extern "C" int a3d_flood_extract(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes, int label,
+                                 int32_t* out_ijk, int64_t count, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(geom && label >= 0 && label < kRing, A3D_ERR_ARGUMENT, "flood_extract: bad label");
+  Geom g = to_geom(geom);
+  Workspace ws(workspace, workspace_bytes);
+  FloodWs w;
+  carve_flood(w, ws, g);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "flood_extract: workspace too small");
+  if (count == 0) return A3D_OK;
+  A3D_REQUIRE(out_ijk, A3D_ERR_ARGUMENT, "flood_extract: null output");
+  const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
+  const unsigned gw = (unsigned)ceil_div(nwords, 256);
+  const uint32_t* v = w.lab + (int64_t)label * nwords;
+  popc_kernel<<<gw, 256, 0, s>>>(v, nwords, w.cnt);
+  A3D_LAUNCH_CHECK();
+  A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.cnt, w.offs, nwords, w.scan_tmp, w.offs + nwords, s)));
+  extract_kernel<<<gw, 256, 0, s>>>(g, v, w.offs, nwords, out_ijk);
+  A3D_LAUNCH_CHECK();
+  return A3D_OK;
+}
+
+extern "C" int a3d_flood_test(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes, int label,
+                              const int64_t* ijk, int64_t n, uint8_t* out, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(geom && label >= 0 && label < kRing, A3D_ERR_ARGUMENT, "flood_test: bad label");
+  Geom g = to_geom(geom);
+  Workspace ws(workspace, workspace_bytes);
+  FloodWs w;
+  carve_flood(w, ws, g);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "flood_test: workspace too small");
+  if (n == 0) return A3D_OK;
+  const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
+  test_bits_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(g, w.lab + (int64_t)label * nwords, ijk, n, out);
+  A3D_LAUNCH_CHECK();
+  return A3D_OK;
+}

@@ -156,6 +156,51 @@ int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo /* host[3]
                         int64_t* out_ijk, int64_t cap, int64_t* count_out /* host */,
                         void* workspace, size_t workspace_bytes, a3d_stream_t stream);
 
+/* ---- sparse flood fill ------------------------------------------------- */
+/* Replaces flood_fill_3d_sparse / flood_fill_kernel / the host BFS loop
+ * (atom3d/kernels/flood_fill.py:118-258, atom3d/kernels/flood_fill_kernels.cu:
+ * 21-175) and get_dam_neighborhood_signs (atom3d/apps/sparse_flood_fill.py:
+ * 34-100).  Work on a bit-packed volume: vol_lo/vol_dims (grid coordinates)
+ * contains the flood domain crop_lo..crop_hi (inclusive); the k-ring needs
+ * the volume to reach k voxels beyond the dam where the grid allows. */
+typedef struct a3d_flood_geom {
+  int64_t vol_lo[3];
+  int32_t vol_dims[3];
+  int64_t crop_lo[3];
+  int64_t crop_hi[3];
+  int64_t seed[3];        /* grid coordinates, inside the crop */
+  int32_t connectivity;   /* 6, 18 or 26 */
+  int32_t k_ring;         /* >= 0 */
+} a3d_flood_geom;
+
+/* label slots of a3d_flood_fill / _extract / _test */
+#define A3D_FLOOD_WATER 0      /* pure water (reference mask == 2)          */
+#define A3D_FLOOD_DRY 1        /* mask == -2                               */
+#define A3D_FLOOD_TIDE 2       /* collision, mask == 1                     */
+#define A3D_FLOOD_DAM 3        /* mask == -1 (extension included)          */
+#define A3D_FLOOD_EXT_DAM 4    /* the extension alone                      */
+#define A3D_FLOOD_EXT_TIDE 5   /* k-ring neighbours with sign +1           */
+#define A3D_FLOOD_DRY_ADJ 6    /* k-ring neighbours with sign -1           */
+
+/* bbox_out (host, 6): min xyz, max xyz of the n voxels (synchronises). */
+int a3d_flood_bbox(const int64_t* ijk, int64_t n, int64_t* bbox_out,
+                   void* workspace, size_t workspace_bytes, a3d_stream_t stream);
+size_t a3d_flood_workspace_bytes(const a3d_flood_geom* geom);
+/* Floods and labels; counts_out (host, 9): voxel count per label slot 0..7
+ * and [8] = 1 when the seed is occupied (then nothing else is computed,
+ * like the reference's empty result).  The labelled volumes stay in the
+ * workspace for a3d_flood_extract / a3d_flood_test.  rounds_out (nullable):
+ * relaxation rounds used. */
+int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood_geom* geom,
+                   void* workspace, size_t workspace_bytes, int64_t* counts_out,
+                   int* rounds_out, a3d_stream_t stream);
+/* Writes the voxels of one label as int32 [count,3] in lexicographic order. */
+int a3d_flood_extract(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes,
+                      int label, int32_t* out_ijk, int64_t count, a3d_stream_t stream);
+/* out[i] = 1 when voxel ijk[i] carries the label. */
+int a3d_flood_test(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes,
+                   int label, const int64_t* ijk, int64_t n, uint8_t* out, a3d_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
