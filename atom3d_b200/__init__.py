@@ -13,6 +13,7 @@ from .core.mesh_bvh import MeshBVH
 from .grid.cube_grid import CubeGrid
 from .grid.octree_indexer import OctreeIndexer
 from .apps.sparse_flood_fill import flood_fill_3d_sparse, sparse_flood_fill
+from .mesh_extractor.sparse_diffdmc import SparseDiffDMC, SparseDMC
 
 __all__ = [
     "MeshBVH",
@@ -22,4 +23,6 @@ __all__ = [
     "CubeGrid",
     "sparse_flood_fill",
     "flood_fill_3d_sparse",
+    "SparseDiffDMC",
+    "SparseDMC",
 ]

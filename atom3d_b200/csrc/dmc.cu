@@ -1,0 +1,830 @@
+// Sparse differentiable Dual Marching Cubes (training mode: weighted-average
+// dual vertices, 4-triangle quad split) and its adjoint.
+//
+// Replaces the PyTorch pipeline of SparseDiffDMC.forward
+// (atom3d/mesh_extractor/sparse_diffdmc.py:76-232) and the autograd graph
+// behind it.  Steps and the reference functions they restate:
+//   corner positions, world map grid*2/res - 1 (+deform)          :151-168
+//   surface cubes, 8-bit case ids                                   :516-521
+//   C16/C19 fix through a hash of the problematic cubes            :524-579
+//   surface edges: crossing (cube, edge) entries sorted by the
+//     endpoint pair (i0, i1) with the in-house radix sort; runs give
+//     the unique edges in torch.unique(dim=0) order                 :582-599
+//   zero crossings and edge normals                                 :263-287, :859-871
+//   dual vertices: numbered by ascending vertex count per cube,
+//     then cube order, then slot (the reference's grouping loop);
+//     one thread per dual vertex folds its edges in order, so the
+//     sums are the reference's index_add_ order                    :601-780
+//   L_dev (mean absolute deviation of crossing distances)           :255-261
+//   quads from edges shared by four surface cubes, winding by the
+//     sign at the edge's first endpoint, centre + 4 triangles       :782-826
+// The adjoint recomputes every per-edge quantity from sdf/positions/
+// weights instead of storing them.  The float operations follow the
+// reference's order with explicit round-to-nearest intrinsics where the
+// reference is single-rounded per operation (no FMA contraction).
+#include <math.h>
+
+#include "primitives.cuh"
+#include "dmc_tables.inc"
+
+namespace a3d {
+namespace {
+
+__constant__ unsigned char kCE[24] = {0, 1, 1, 5, 4, 5, 0, 4, 2, 3, 3, 7, 6, 7, 2, 6, 2, 0, 3, 1, 7, 5, 6, 4};
+
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsb(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+
+struct DmcIn {
+  const int64_t* vox;     // [N,3]
+  const float* sdf;       // [M]
+  const int64_t* cidx;    // [N,8]
+  const float* deform;    // [M,3] or null
+  const float* alpha;     // [N,8] raw or null
+  const float* beta;      // [N,12] raw or null
+  int64_t n, m;
+  int res;
+  float iso;
+  float wscale;           // weight_scale
+};
+
+// interpolation of one edge: (x0*w0 + x1*w1) / (w0 + w1), w0 = s1, w1 = -s0
+__device__ __forceinline__ float interp1(float x0, float x1, float w0, float w1, float den) {
+  return fd(fa(fm(x0, w0), fm(x1, w1)), den);
+}
+
+__device__ __forceinline__ float norm_w(float v, float ws, bool given) {
+  return given ? fa(fm(tanhf(v), ws), 1.0f) : 1.0f;
+}
+
+// ---- stage A ---------------------------------------------------------------
+__global__ void init_pos_kernel(int64_t m, const float* __restrict__ deform, float* __restrict__ x) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float v = -1.0f;  // grid position 0 mapped to world
+    if (deform) v = fa(v, deform[3 * i + a]);
+    x[3 * i + a] = v;
+  }
+}
+
+__global__ void corner_pos_kernel(DmcIn in, float ws, float* __restrict__ x) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= in.n * 8) return;
+  const int64_t i = t >> 3;
+  const int c = (int)(t & 7);
+  const int64_t mi = in.cidx[t];
+  const int off[3] = {c & 1, (c >> 1) & 1, (c >> 2) & 1};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float g = fa((float)in.vox[3 * i + a], (float)off[a]);
+    float v = fsb(fm(g, ws), 1.0f);
+    if (in.deform) v = fa(v, in.deform[3 * mi + a]);
+    x[3 * mi + a] = v;
+  }
+}
+
+__global__ void case_kernel(DmcIn in, uint8_t* __restrict__ cases, uint32_t* __restrict__ flag) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= in.n) return;
+  uint32_t c = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) c |= (fsb(in.sdf[in.cidx[8 * i + k]], in.iso) < 0.f ? 1u : 0u) << k;
+  cases[i] = (uint8_t)c;
+  flag[i] = (c != 0u && c != 255u) ? 1u : 0u;
+}
+
+__global__ void compact_kernel(int64_t n, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off,
+                               uint32_t* __restrict__ list) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && flag[i]) list[off[i]] = (uint32_t)i;
+}
+
+__device__ __forceinline__ uint64_t hash64(uint64_t k) {
+  k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
+  return k;
+}
+
+__global__ void prob_insert_kernel(DmcIn in, int64_t ns, const uint32_t* __restrict__ list,
+                                   const uint8_t* __restrict__ cases, unsigned long long* __restrict__ table,
+                                   uint64_t mask) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns) return;
+  const uint32_t i = list[t];
+  const int c = cases[i];
+  if (kCheck[c][0] != 1) return;
+  const uint64_t r = (uint64_t)in.res;
+  const uint64_t key = ((uint64_t)in.vox[3 * i] * r + (uint64_t)in.vox[3 * i + 1]) * r + (uint64_t)in.vox[3 * i + 2];
+  uint64_t h = hash64(key) & mask;
+  for (uint64_t probe = 0; probe <= mask; ++probe) {
+    const unsigned long long prev = atomicCAS(&table[h], ~0ull, (unsigned long long)key);
+    if (prev == ~0ull || prev == key) return;
+    h = (h + 1) & mask;
+  }
+}
+
+__global__ void case_fix_kernel(DmcIn in, int64_t ns, const uint32_t* __restrict__ list,
+                                const uint8_t* __restrict__ cases, const unsigned long long* __restrict__ table,
+                                uint64_t mask, uint8_t* __restrict__ case_s) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns) return;
+  const uint32_t i = list[t];
+  const int c = cases[i];
+  int out = c;
+  if (kCheck[c][0] == 1) {
+    const int64_t ax = in.vox[3 * i] + kCheck[c][1], ay = in.vox[3 * i + 1] + kCheck[c][2],
+                  az = in.vox[3 * i + 2] + kCheck[c][3];
+    if (ax >= 0 && ay >= 0 && az >= 0 && ax < in.res && ay < in.res && az < in.res) {
+      const uint64_t r = (uint64_t)in.res;
+      const uint64_t key = ((uint64_t)ax * r + (uint64_t)ay) * r + (uint64_t)az;
+      uint64_t h = hash64(key) & mask;
+      for (uint64_t probe = 0; probe <= mask; ++probe) {
+        const unsigned long long v = table[h];
+        if (v == key) { out = kCheck[c][4]; break; }
+        if (v == ~0ull) break;
+        h = (h + 1) & mask;
+      }
+    }
+  }
+  case_s[t] = (uint8_t)out;
+}
+
+__device__ __forceinline__ void edge_ends(const DmcIn& in, uint32_t cube, int e, int64_t& i0, int64_t& i1) {
+  i0 = in.cidx[8 * (int64_t)cube + kCE[2 * e]];
+  i1 = in.cidx[8 * (int64_t)cube + kCE[2 * e + 1]];
+}
+
+__global__ void cross_count_kernel(DmcIn in, int64_t ns, const uint32_t* __restrict__ list,
+                                   uint16_t* __restrict__ mask12, uint32_t* __restrict__ cnt) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns) return;
+  const uint32_t i = list[t];
+  uint32_t m = 0;
+#pragma unroll
+  for (int e = 0; e < 12; ++e) {
+    int64_t i0, i1;
+    edge_ends(in, i, e, i0, i1);
+    const bool n0 = fsb(in.sdf[i0], in.iso) < 0.f, n1 = fsb(in.sdf[i1], in.iso) < 0.f;
+    if (n0 != n1) m |= 1u << e;
+  }
+  mask12[t] = (uint16_t)m;
+  cnt[t] = (uint32_t)__popc(m);
+}
+
+__global__ void cross_write_kernel(DmcIn in, int64_t ns, const uint32_t* __restrict__ list,
+                                   const uint16_t* __restrict__ mask12, const uint32_t* __restrict__ off,
+                                   uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns) return;
+  const uint32_t i = list[t];
+  uint32_t m = mask12[t];
+  uint32_t o = off[t];
+  while (m) {
+    const int e = __ffs(m) - 1;
+    m &= m - 1;
+    int64_t i0, i1;
+    edge_ends(in, i, e, i0, i1);
+    keys[o] = (uint64_t)i0 * (uint64_t)in.m + (uint64_t)i1;
+    vals[o] = (uint32_t)(t * 12 + e);
+    ++o;
+  }
+}
+
+__global__ void run_flag_kernel(const uint64_t* __restrict__ k, int64_t n, uint32_t* __restrict__ flag) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) flag[j] = (j == 0 || k[j] != k[j - 1]) ? 1u : 0u;
+}
+
+__global__ void run_info_kernel(const uint64_t* __restrict__ k, const uint32_t* __restrict__ v, int64_t n,
+                                const uint32_t* __restrict__ flag, const uint32_t* __restrict__ rid, int64_t m,
+                                int32_t* __restrict__ idx_map, int64_t* __restrict__ e0, int64_t* __restrict__ e1,
+                                uint32_t* __restrict__ rfirst) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  // rid holds the exclusive scan of the run-start flags: the run of entry j
+  // is the number of starts up to and including j, minus one
+  const uint32_t r = rid[j] + flag[j] - 1u;
+  idx_map[v[j]] = (int32_t)r;
+  if (flag[j]) {
+    e0[r] = (int64_t)(k[j] / (uint64_t)m);
+    e1[r] = (int64_t)(k[j] % (uint64_t)m);
+    rfirst[r] = (uint32_t)j;
+  }
+}
+
+__global__ void quad_flag_kernel(int64_t ne, int64_t nc, const uint32_t* __restrict__ rfirst,
+                                 uint32_t* __restrict__ qflag) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= ne) return;
+  const int64_t end = r + 1 < ne ? rfirst[r + 1] : nc;
+  qflag[r] = (end - rfirst[r]) == 4 ? 1u : 0u;
+}
+
+// per-surface-cube dual-vertex bookkeeping (vertex count class 1..4)
+__global__ void vd_class_kernel(int64_t ns, const uint8_t* __restrict__ case_s, int cls, uint32_t* __restrict__ f) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < ns) f[t] = kNumVd[case_s[t]] == cls ? 1u : 0u;
+}
+
+__global__ void vd_assign_kernel(int64_t ns, const uint8_t* __restrict__ case_s, int cls,
+                                 const uint32_t* __restrict__ f, const uint32_t* __restrict__ rank, uint32_t base,
+                                 uint32_t* __restrict__ vd_cube, uint8_t* __restrict__ vd_slot,
+                                 uint32_t* __restrict__ vd_ne) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns || !f[t]) return;
+  const int c = case_s[t];
+  const uint32_t v0 = base + rank[t] * (uint32_t)cls;
+  for (int j = 0; j < cls; ++j) {
+    uint32_t ne = 0;
+    for (int k = 0; k < 7; ++k) ne += kDmcTable[c][j][k] != -1 ? 1u : 0u;
+    vd_cube[v0 + j] = (uint32_t)t;
+    vd_slot[v0 + j] = (uint8_t)j;
+    vd_ne[v0 + j] = ne;
+  }
+}
+
+struct EdgeData {
+  const int64_t* e0;
+  const int64_t* e1;
+  const int32_t* idx_map;
+};
+
+struct VdOut {
+  float* verts;      // [V+Q,3]
+  float* ldev;       // [G]
+  float* palpha;     // [G,3]
+  float* nalpha;     // [G,3]
+  int32_t* vd_map;   // [12*Ns]
+};
+
+// edge normal of the training mode: normalize(edge_dir * sign(s1 - s0))
+__device__ __forceinline__ void edge_normal(const float* x0, const float* x1, float s0, float s1, float* n) {
+  float ev[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) ev[a] = fsb(x1[a], x0[a]);
+  const float len = fa(sqrtf(fa(fa(fm(ev[0], ev[0]), fm(ev[1], ev[1])), fm(ev[2], ev[2]))), 1e-8f);
+  const float gm = fd(fsb(s1, s0), len);
+  const float sg = gm > 0.f ? 1.f : (gm < 0.f ? -1.f : 0.f);
+  float u[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) u[a] = fm(fd(ev[a], len), sg);
+  const float ul = sqrtf(fa(fa(fm(u[0], u[0]), fm(u[1], u[1])), fm(u[2], u[2])));
+  const float den = fmaxf(ul, 1e-12f);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) n[a] = fd(u[a], den);
+}
+
+__device__ __forceinline__ float ldf(const float* p, int64_t i) { return __ldg(p + i); }
+
+// one thread per dual vertex: crossings, weighted average, L_dev
+__global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, const uint32_t* __restrict__ list,
+                          const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
+                          const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
+                          VdOut out) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const uint32_t t = vd_cube[v];
+  const int j = vd_slot[v];
+  const int c = case_s[t];
+  const uint32_t cube = list[t];
+  const int64_t g0 = goff[v];
+  float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
+  int64_t g = g0;
+  for (int k = 0; k < 7; ++k) {
+    const int e = kDmcTable[c][j][k];
+    if (e < 0) continue;
+    const int64_t flat = (int64_t)t * 12 + e;
+    const int32_t r = ed.idx_map[flat];
+    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
+    const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
+    const float a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
+    const float a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
+    const float b = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
+    const float w0 = fm(s1, a1), w1 = -fm(s0, a0);
+    const float den = fa(w0, w1);
+    float xa[3], xb[3], n[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { xa[a] = ldf(x, 3 * i0 + a); xb[a] = ldf(x, 3 * i1 + a); }
+    edge_normal(xa, xb, s0, s1, n);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float ue = interp1(xa[a], xb[a], w0, w1, den);
+      out.palpha[3 * g + a] = ue;
+      out.nalpha[3 * g + a] = n[a];
+      acc[a] = fa(acc[a], fm(ue, b));
+    }
+    bsum = fa(bsum, b);
+    out.vd_map[flat] = (int32_t)v;
+    ++g;
+  }
+  const int64_t ne = g - g0;
+  float vd[3];
+  const float den = fa(bsum, 1e-8f);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    vd[a] = fd(acc[a], den);
+    out.verts[3 * v + a] = vd[a];
+  }
+  // L_dev: distances of the plain zero crossings to the dual vertex
+  float msum = 0.f;
+  float dist[7];
+  g = g0;
+  for (int k = 0; k < 7; ++k) {
+    const int e = kDmcTable[c][j][k];
+    if (e < 0) continue;
+    const int32_t r = ed.idx_map[(int64_t)t * 12 + e];
+    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
+    const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
+    const float w0 = s1, w1 = -s0, dn = fa(w0, w1);
+    float d2 = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float z = interp1(ldf(x, 3 * i0 + a), ldf(x, 3 * i1 + a), w0, w1, dn);
+      const float dd = fsb(z, vd[a]);
+      d2 = fa(d2, fm(dd, dd));
+    }
+    dist[g - g0] = sqrtf(d2);
+    msum = fa(msum, dist[g - g0]);
+    ++g;
+  }
+  const float mean = fd(msum, (float)ne);
+  for (int64_t q = 0; q < ne; ++q) out.ldev[g0 + q] = fabsf(fsb(dist[q], mean));
+}
+
+__global__ void quad_kernel(int64_t ne, int64_t nc, const uint32_t* __restrict__ qflag, const uint32_t* __restrict__ qoff,
+                            const uint32_t* __restrict__ rfirst, const uint32_t* __restrict__ vals,
+                            const int32_t* __restrict__ vd_map, const int64_t* __restrict__ e0,
+                            const float* __restrict__ sdf, float iso, int64_t nvd, float* __restrict__ verts,
+                            int64_t* __restrict__ faces, int32_t* __restrict__ quads) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= ne || !qflag[r]) return;
+  const int64_t q = qoff[r];
+  int32_t v[4];
+  for (int k = 0; k < 4; ++k) v[k] = vd_map[vals[rfirst[r] + k]];
+  const bool flip = fsb(sdf[e0[r]], iso) > 0.f;
+  int32_t o[4];
+  if (flip) { o[0] = v[0]; o[1] = v[1]; o[2] = v[3]; o[3] = v[2]; }
+  else { o[0] = v[2]; o[1] = v[3]; o[2] = v[1]; o[3] = v[0]; }
+  const int64_t cidx = nvd + q;
+  float s[3] = {0.f, 0.f, 0.f};
+  for (int k = 0; k < 4; ++k) {
+    quads[4 * q + k] = o[k];
+    for (int a = 0; a < 3; ++a) s[a] = fa(s[a], verts[3 * (int64_t)o[k] + a]);
+    faces[3 * (4 * q + k)] = o[k];
+    faces[3 * (4 * q + k) + 1] = o[(k + 1) & 3];
+    faces[3 * (4 * q + k) + 2] = cidx;
+  }
+  for (int a = 0; a < 3; ++a) verts[3 * cidx + a] = fm(s[a], 0.25f);
+}
+
+// ---- adjoint ------------------------------------------------------------------
+struct DmcGrad {
+  const float* g_verts;   // [V+Q,3] or null
+  const float* g_ldev;    // [G] or null
+  const float* g_palpha;  // [G,3] or null
+  const float* g_nalpha;  // [G,3] or null
+  float* g_sdf;           // [M] or null
+  float* g_deform;        // [M,3] or null
+  float* g_alpha;         // [N,8] raw or null
+  float* g_beta;          // [N,12] raw or null
+  float* g_vd;            // [V,3] scratch (quad centre contributions)
+};
+
+__global__ void quad_bwd_kernel(int64_t nq, int64_t nvd, const int32_t* __restrict__ quads, DmcGrad gr) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq || !gr.g_verts) return;
+  const float* gc = gr.g_verts + 3 * (nvd + q);
+  for (int k = 0; k < 4; ++k) {
+    const int64_t v = quads[4 * q + k];
+    for (int a = 0; a < 3; ++a) atomicAdd(&gr.g_vd[3 * v + a], gc[a] * 0.25f);
+  }
+}
+
+__device__ __forceinline__ void scatter_interp_grad(const DmcIn& in, const float* gue, const float* xa, const float* xb,
+                                                    float ue[3], float w0, float w1, float den, int64_t i0, int64_t i1,
+                                                    float& gw0, float& gw1, DmcGrad& gr) {
+  // ue = (xa w0 + xb w1) / den: d/dxa = w0/den, d/dxb = w1/den,
+  // d/dw0 = (xa - ue)/den, d/dw1 = (xb - ue)/den
+  gw0 = 0.f;
+  gw1 = 0.f;
+  for (int a = 0; a < 3; ++a) {
+    gw0 += gue[a] * (xa[a] - ue[a]) / den;
+    gw1 += gue[a] * (xb[a] - ue[a]) / den;
+    if (gr.g_deform) {
+      atomicAdd(&gr.g_deform[3 * i0 + a], gue[a] * w0 / den);
+      atomicAdd(&gr.g_deform[3 * i1 + a], gue[a] * w1 / den);
+    }
+  }
+}
+
+__global__ void vd_bwd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, const uint32_t* __restrict__ list,
+                              const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
+                              const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
+                              DmcGrad gr) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const uint32_t t = vd_cube[v];
+  const int j = vd_slot[v];
+  const int c = case_s[t];
+  const uint32_t cube = list[t];
+  const int64_t g0 = goff[v];
+  // recompute the forward quantities of this dual vertex
+  int64_t I0[7], I1[7];
+  int E[7];
+  float A[7][2], S[7][2], B[7], UE[7][3];
+  int ne = 0;
+  float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
+  for (int k = 0; k < 7; ++k) {
+    const int e = kDmcTable[c][j][k];
+    if (e < 0) continue;
+    const int32_t r = ed.idx_map[(int64_t)t * 12 + e];
+    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
+    I0[ne] = i0; I1[ne] = i1; E[ne] = e;
+    S[ne][0] = fsb(in.sdf[i0], in.iso); S[ne][1] = fsb(in.sdf[i1], in.iso);
+    A[ne][0] = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
+    A[ne][1] = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
+    B[ne] = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
+    const float w0 = fm(S[ne][1], A[ne][1]), w1 = -fm(S[ne][0], A[ne][0]), den = fa(w0, w1);
+    for (int a = 0; a < 3; ++a) {
+      UE[ne][a] = interp1(x[3 * i0 + a], x[3 * i1 + a], w0, w1, den);
+      acc[a] = fa(acc[a], fm(UE[ne][a], B[ne]));
+    }
+    bsum = fa(bsum, B[ne]);
+    ++ne;
+  }
+  const float bden = fa(bsum, 1e-8f);
+  float vd[3];
+  for (int a = 0; a < 3; ++a) vd[a] = fd(acc[a], bden);
+  // incoming gradient of the dual vertex
+  float gvd[3] = {0.f, 0.f, 0.f};
+  if (gr.g_verts)
+    for (int a = 0; a < 3; ++a) gvd[a] = gr.g_verts[3 * v + a] + gr.g_vd[3 * v + a];
+  // L_dev backward (mad = |dist - mean|, mean = sum(dist)/ne)
+  float Z[7][3], D[7], gD[7];
+  float msum = 0.f;
+  for (int q = 0; q < ne; ++q) {
+    const float w0 = S[q][1], w1 = -S[q][0], dn = fa(w0, w1);
+    float d2 = 0.f;
+    for (int a = 0; a < 3; ++a) {
+      Z[q][a] = interp1(x[3 * I0[q] + a], x[3 * I1[q] + a], w0, w1, dn);
+      const float dd = fsb(Z[q][a], vd[a]);
+      d2 = fa(d2, fm(dd, dd));
+    }
+    D[q] = sqrtf(d2);
+    msum = fa(msum, D[q]);
+    gD[q] = 0.f;
+  }
+  const float mean = fd(msum, (float)ne);
+  if (gr.g_ldev) {
+    float gmean = 0.f;
+    for (int q = 0; q < ne; ++q) {
+      const float gl = gr.g_ldev[g0 + q];
+      const float df = D[q] - mean;
+      const float sg = df > 0.f ? 1.f : (df < 0.f ? -1.f : 0.f);
+      gD[q] += gl * sg;
+      gmean -= gl * sg;
+    }
+    for (int q = 0; q < ne; ++q) gD[q] += gmean / (float)ne;
+  }
+  // dist -> crossing z and dual vertex
+  float gZ[7][3];
+  for (int q = 0; q < ne; ++q) {
+    for (int a = 0; a < 3; ++a) {
+      const float u = D[q] > 0.f ? (Z[q][a] - vd[a]) / D[q] : 0.f;
+      gZ[q][a] = gD[q] * u;
+      gvd[a] -= gD[q] * u;
+    }
+  }
+  // vd = sum(b ue) / (sum b + 1e-8)
+  float gB = 0.f;
+  for (int a = 0; a < 3; ++a) gB -= gvd[a] * vd[a] / bden;
+  for (int q = 0; q < ne; ++q) {
+    const int e = E[q];
+    const int64_t i0 = I0[q], i1 = I1[q];
+    float gue[3];
+    float gb = gB;
+    for (int a = 0; a < 3; ++a) {
+      gue[a] = gvd[a] * B[q] / bden;
+      if (gr.g_palpha) gue[a] += gr.g_palpha[3 * (g0 + q) + a];
+      gb += gvd[a] * UE[q][a] / bden;
+    }
+    float xa[3], xb[3];
+    for (int a = 0; a < 3; ++a) { xa[a] = x[3 * i0 + a]; xb[a] = x[3 * i1 + a]; }
+    // ue through w0 = s1 a1, w1 = -s0 a0
+    {
+      const float w0 = S[q][1] * A[q][1], w1 = -(S[q][0] * A[q][0]), den = w0 + w1;
+      float gw0, gw1;
+      scatter_interp_grad(in, gue, xa, xb, UE[q], w0, w1, den, i0, i1, gw0, gw1, gr);
+      if (gr.g_sdf) {
+        atomicAdd(&gr.g_sdf[i1], gw0 * A[q][1]);
+        atomicAdd(&gr.g_sdf[i0], -gw1 * A[q][0]);
+      }
+      if (gr.g_alpha && in.alpha) {
+        const int c0 = kCE[2 * e], c1 = kCE[2 * e + 1];
+        const float t0 = tanhf(in.alpha[8 * (int64_t)cube + c0]), t1 = tanhf(in.alpha[8 * (int64_t)cube + c1]);
+        atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c1], gw0 * S[q][1] * in.wscale * (1.f - t1 * t1));
+        atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c0], -gw1 * S[q][0] * in.wscale * (1.f - t0 * t0));
+      }
+    }
+    // plain crossing z through w0 = s1, w1 = -s0
+    {
+      const float w0 = S[q][1], w1 = -S[q][0], den = w0 + w1;
+      float gw0, gw1;
+      scatter_interp_grad(in, gZ[q], xa, xb, Z[q], w0, w1, den, i0, i1, gw0, gw1, gr);
+      if (gr.g_sdf) {
+        atomicAdd(&gr.g_sdf[i1], gw0);
+        atomicAdd(&gr.g_sdf[i0], -gw1);
+      }
+    }
+    // edge normal (n_alpha) through the edge vector
+    if (gr.g_nalpha && gr.g_deform) {
+      float ev[3];
+      for (int a = 0; a < 3; ++a) ev[a] = xb[a] - xa[a];
+      const float el = sqrtf(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+      const float L = el + 1e-8f;
+      const float ds = S[q][1] - S[q][0];
+      const float sg = ds > 0.f ? 1.f : (ds < 0.f ? -1.f : 0.f);
+      float u[3], n[3];
+      for (int a = 0; a < 3; ++a) u[a] = ev[a] / L * sg;
+      const float ul = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+      const float* gn = gr.g_nalpha + 3 * (g0 + q);
+      if (ul > 1e-12f && el > 0.f) {
+        for (int a = 0; a < 3; ++a) n[a] = u[a] / ul;
+        const float ndg = n[0] * gn[0] + n[1] * gn[1] + n[2] * gn[2];
+        float ged[3];
+        for (int a = 0; a < 3; ++a) ged[a] = sg * (gn[a] - n[a] * ndg) / ul;
+        const float gdot = ged[0] * ev[0] + ged[1] * ev[1] + ged[2] * ev[2];
+        for (int a = 0; a < 3; ++a) {
+          const float gev = ged[a] / L - ev[a] * gdot / (L * L * el);
+          atomicAdd(&gr.g_deform[3 * i1 + a], gev);
+          atomicAdd(&gr.g_deform[3 * i0 + a], -gev);
+        }
+      }
+    }
+    if (gr.g_beta && in.beta) {
+      const float tb = tanhf(in.beta[12 * (int64_t)cube + e]);
+      gr.g_beta[12 * (int64_t)cube + e] += gb * in.wscale * (1.f - tb * tb);
+    }
+  }
+}
+
+// ---- workspace ------------------------------------------------------------------
+struct DmcWs {
+  float* x;            // [M,3]
+  uint8_t* cases;      // [N]
+  uint32_t* flag;      // [N]
+  uint32_t* off;       // [N]
+  uint32_t* list;      // [N]
+  unsigned long long* table;  // hash
+  uint8_t* case_s;     // [N]
+  uint16_t* mask12;    // [N]
+  uint32_t* ccnt;      // [N]
+  uint32_t* coff;      // [N]
+  uint64_t* keys;      // [12N]
+  uint64_t* keys2;
+  uint32_t* vals;
+  uint32_t* vals2;
+  uint32_t* rs;
+  uint32_t* rflag;     // [12N]
+  uint32_t* rid;       // [12N]
+  int32_t* idx_map;    // [12N]
+  int32_t* vd_map;     // [12N]
+  int64_t* e0;         // [12N]
+  int64_t* e1;
+  uint32_t* rfirst;    // [12N]
+  uint32_t* qflag;     // [12N]
+  uint32_t* qoff;      // [12N]
+  uint32_t* vd_cube;   // [4N]
+  uint8_t* vd_slot;    // [4N]
+  uint32_t* vd_ne;     // [4N]
+  uint32_t* goff;      // [4N]
+  uint32_t* cls_f;     // [N]
+  uint32_t* cls_r;     // [N]
+  int32_t* quads;      // [12N/4*4]
+  float* g_vd;         // [4N,3]
+  uint32_t* scan_tmp;
+  uint32_t* misc;      // counters
+  uint64_t table_mask;
+};
+
+uint64_t pow2_at_least(uint64_t v) {
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+size_t carve_dmc(DmcWs& w, Workspace& ws, int64_t n, int64_t m) {
+  const int64_t n12 = 12 * n + 1;
+  const uint64_t tsize = pow2_at_least((uint64_t)(2 * n + 2));
+  w.table_mask = tsize - 1;
+  w.x = ws.take<float>(3 * m);
+  w.cases = ws.take<uint8_t>(n);
+  w.flag = ws.take<uint32_t>(n);
+  w.off = ws.take<uint32_t>(n + 1);
+  w.list = ws.take<uint32_t>(n);
+  w.table = ws.take<unsigned long long>((int64_t)tsize);
+  w.case_s = ws.take<uint8_t>(n);
+  w.mask12 = ws.take<uint16_t>(n);
+  w.ccnt = ws.take<uint32_t>(n);
+  w.coff = ws.take<uint32_t>(n + 1);
+  w.keys = ws.take<uint64_t>(n12);
+  w.keys2 = ws.take<uint64_t>(n12);
+  w.vals = ws.take<uint32_t>(n12);
+  w.vals2 = ws.take<uint32_t>(n12);
+  w.rs = ws.take<uint32_t>((int64_t)radix_sort_scratch_elems(n12));
+  w.rflag = ws.take<uint32_t>(n12);
+  w.rid = ws.take<uint32_t>(n12);
+  w.idx_map = ws.take<int32_t>(n12);
+  w.vd_map = ws.take<int32_t>(n12);
+  w.e0 = ws.take<int64_t>(n12);
+  w.e1 = ws.take<int64_t>(n12);
+  w.rfirst = ws.take<uint32_t>(n12);
+  w.qflag = ws.take<uint32_t>(n12);
+  w.qoff = ws.take<uint32_t>(n12 + 1);
+  w.vd_cube = ws.take<uint32_t>(4 * n + 1);
+  w.vd_slot = ws.take<uint8_t>(4 * n + 1);
+  w.vd_ne = ws.take<uint32_t>(4 * n + 1);
+  w.goff = ws.take<uint32_t>(4 * n + 2);
+  w.cls_f = ws.take<uint32_t>(n);
+  w.cls_r = ws.take<uint32_t>(n + 1);
+  w.quads = ws.take<int32_t>(n12);
+  w.g_vd = ws.take<float>(12 * n + 3);
+  w.scan_tmp = ws.take<uint32_t>((int64_t)scan_workspace_elems(n12 > 4 * n ? n12 : 4 * n));
+  w.misc = ws.take<uint32_t>(16);
+  return ws.used;
+}
+
+unsigned gsz(int64_t n, int b = 256) { return (unsigned)ceil_div(n > 0 ? n : 1, b); }
+
+int read_u32(const uint32_t* d, uint32_t* h, cudaStream_t s) {
+  A3D_CUDA_TRY(cudaMemcpyAsync(h, d, 4, cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  return A3D_OK;
+}
+
+DmcIn make_in(const a3d_dmc_inputs* p) {
+  DmcIn in;
+  in.vox = p->voxel_coords; in.sdf = p->sdf; in.cidx = p->cube_idx; in.deform = p->deform;
+  in.alpha = p->alpha; in.beta = p->beta; in.n = p->num_cubes; in.m = p->num_corners; in.res = p->resolution;
+  in.iso = p->isovalue; in.wscale = p->weight_scale;
+  return in;
+}
+
+}  // namespace
+}  // namespace a3d
+
+using namespace a3d;
+
+extern "C" size_t a3d_dmc_workspace_bytes(int64_t num_cubes, int64_t num_corners) {
+  Workspace ws(nullptr, 0);
+  DmcWs w;
+  return carve_dmc(w, ws, num_cubes > 0 ? num_cubes : 1, num_corners > 0 ? num_corners : 1) + 256;
+}
+
+extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t workspace_bytes, int64_t* counts,
+                               a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(p && counts, A3D_ERR_ARGUMENT, "dmc_prepare: null argument");
+  A3D_REQUIRE(p->num_cubes >= 0 && p->num_corners >= 0 && p->resolution > 0, A3D_ERR_ARGUMENT, "dmc_prepare: sizes");
+  A3D_REQUIRE(p->num_cubes < (1ll << 28) && p->num_corners < (1ll << 31), A3D_ERR_ARGUMENT, "dmc_prepare: too large");
+  const int64_t n = p->num_cubes, m = p->num_corners;
+  Workspace ws(workspace, workspace_bytes);
+  DmcWs w;
+  carve_dmc(w, ws, n > 0 ? n : 1, m > 0 ? m : 1);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "dmc_prepare: workspace too small");
+  for (int k = 0; k < 6; ++k) counts[k] = 0;
+  if (n == 0 || m == 0) return A3D_OK;
+  DmcIn in = make_in(p);
+  const float wsc = (float)(2.0 / (double)p->resolution);
+  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x);
+  A3D_LAUNCH_CHECK();
+  corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, wsc, w.x);
+  A3D_LAUNCH_CHECK();
+  case_kernel<<<gsz(n), 256, 0, s>>>(in, w.cases, w.flag);
+  A3D_LAUNCH_CHECK();
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flag, w.off, n, w.scan_tmp, w.off + n, s)));
+  uint32_t ns32 = 0;
+  A3D_TRY(read_u32(w.off + n, &ns32, s));
+  const int64_t ns = ns32;
+  counts[0] = ns;
+  if (ns == 0) return A3D_OK;
+  compact_kernel<<<gsz(n), 256, 0, s>>>(n, w.flag, w.off, w.list);
+  A3D_LAUNCH_CHECK();
+  A3D_CUDA_TRY(cudaMemsetAsync(w.table, 0xff, (w.table_mask + 1) * sizeof(unsigned long long), s));
+  prob_insert_kernel<<<gsz(ns), 256, 0, s>>>(in, ns, w.list, w.cases, w.table, w.table_mask);
+  A3D_LAUNCH_CHECK();
+  case_fix_kernel<<<gsz(ns), 256, 0, s>>>(in, ns, w.list, w.cases, w.table, w.table_mask, w.case_s);
+  A3D_LAUNCH_CHECK();
+  cross_count_kernel<<<gsz(ns), 256, 0, s>>>(in, ns, w.list, w.mask12, w.ccnt);
+  A3D_LAUNCH_CHECK();
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ccnt, w.coff, ns, w.scan_tmp, w.coff + ns, s)));
+  uint32_t nc32 = 0;
+  A3D_TRY(read_u32(w.coff + ns, &nc32, s));
+  const int64_t nc = nc32;
+  counts[1] = nc;  // crossing (cube, edge) entries == groups
+  cross_write_kernel<<<gsz(ns), 256, 0, s>>>(in, ns, w.list, w.mask12, w.coff, w.keys, w.vals);
+  A3D_LAUNCH_CHECK();
+  int bits = 1;
+  while (bits < 64 && ((unsigned __int128)1 << bits) < (unsigned __int128)m * (unsigned __int128)m) ++bits;
+  bool alt = false;
+  A3D_TRY(radix_sort_pairs<uint64_t>(w.keys, w.vals, w.keys2, w.vals2, nc, 0, ((bits + 7) / 8) * 8, w.rs, &alt, s));
+  const uint64_t* sk = alt ? w.keys2 : w.keys;
+  const uint32_t* sv = alt ? w.vals2 : w.vals;
+  if (alt) {
+    A3D_CUDA_TRY(cudaMemcpyAsync(w.keys, sk, nc * 8, cudaMemcpyDeviceToDevice, s));
+    A3D_CUDA_TRY(cudaMemcpyAsync(w.vals, sv, nc * 4, cudaMemcpyDeviceToDevice, s));
+  }
+  run_flag_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, nc, w.rflag);
+  A3D_LAUNCH_CHECK();
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.rflag, w.rid, nc, w.scan_tmp, w.misc, s)));
+  uint32_t ne32 = 0;
+  A3D_TRY(read_u32(w.misc, &ne32, s));
+  const int64_t ne = ne32;
+  counts[2] = ne;
+  A3D_CUDA_TRY(cudaMemsetAsync(w.idx_map, 0xff, 12 * ns * sizeof(int32_t), s));
+  A3D_CUDA_TRY(cudaMemsetAsync(w.vd_map, 0, 12 * ns * sizeof(int32_t), s));
+  run_info_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, w.vals, nc, w.rflag, w.rid, m, w.idx_map, w.e0, w.e1, w.rfirst);
+  A3D_LAUNCH_CHECK();
+  quad_flag_kernel<<<gsz(ne), 256, 0, s>>>(ne, nc, w.rfirst, w.qflag);
+  A3D_LAUNCH_CHECK();
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.qflag, w.qoff, ne, w.scan_tmp, w.qoff + ne, s)));
+  uint32_t nq32 = 0;
+  A3D_TRY(read_u32(w.qoff + ne, &nq32, s));
+  counts[3] = nq32;
+  // dual vertices per vertex-count class 1..4
+  uint32_t base = 0;
+  for (int cls = 1; cls <= 4; ++cls) {
+    vd_class_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, cls, w.cls_f);
+    A3D_LAUNCH_CHECK();
+    A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.cls_f, w.cls_r, ns, w.scan_tmp, w.cls_r + ns, s)));
+    vd_assign_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, cls, w.cls_f, w.cls_r, base, w.vd_cube, w.vd_slot,
+                                             w.vd_ne);
+    A3D_LAUNCH_CHECK();
+    uint32_t cnt = 0;
+    A3D_TRY(read_u32(w.cls_r + ns, &cnt, s));
+    base += cnt * (uint32_t)cls;
+  }
+  const int64_t nv = base;
+  counts[4] = nv;
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.vd_ne, w.goff, nv, w.scan_tmp, w.goff + nv, s)));
+  uint32_t ng = 0;
+  A3D_TRY(read_u32(w.goff + nv, &ng, s));
+  counts[5] = ng;
+  A3D_REQUIRE((int64_t)ng == nc, A3D_ERR_ARGUMENT, "dmc_prepare: crossing edges without a dual vertex (bad tables?)");
+  return A3D_OK;
+}
+
+extern "C" int a3d_dmc_emit(const a3d_dmc_inputs* p, void* workspace, size_t workspace_bytes, const int64_t* counts,
+                            float* vertices, int64_t* faces, float* l_dev, float* p_alpha, float* n_alpha,
+                            a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(p && counts, A3D_ERR_ARGUMENT, "dmc_emit: null argument");
+  const int64_t n = p->num_cubes, m = p->num_corners;
+  Workspace ws(workspace, workspace_bytes);
+  DmcWs w;
+  carve_dmc(w, ws, n > 0 ? n : 1, m > 0 ? m : 1);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "dmc_emit: workspace too small");
+  const int64_t ns = counts[0], nc = counts[1], ne = counts[2], nq = counts[3], nv = counts[4];
+  if (ns == 0 || nv == 0) return A3D_OK;
+  DmcIn in = make_in(p);
+  EdgeData ed{w.e0, w.e1, w.idx_map};
+  VdOut out{vertices, l_dev, p_alpha, n_alpha, w.vd_map};
+  vd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, w.x, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, out);
+  A3D_LAUNCH_CHECK();
+  (void)nc;
+  if (nq > 0) {
+    quad_kernel<<<gsz(ne), 256, 0, s>>>(ne, nc, w.qflag, w.qoff, w.rfirst, w.vals, w.vd_map, w.e0, p->sdf, p->isovalue,
+                                        nv, vertices, faces, w.quads);
+    A3D_LAUNCH_CHECK();
+  }
+  return A3D_OK;
+}
+
+extern "C" int a3d_dmc_backward(const a3d_dmc_inputs* p, void* workspace, size_t workspace_bytes,
+                                const int64_t* counts, const float* g_vertices, const float* g_l_dev,
+                                const float* g_p_alpha, const float* g_n_alpha, float* g_sdf, float* g_deform,
+                                float* g_alpha, float* g_beta, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(p && counts, A3D_ERR_ARGUMENT, "dmc_backward: null argument");
+  const int64_t n = p->num_cubes, m = p->num_corners;
+  Workspace ws(workspace, workspace_bytes);
+  DmcWs w;
+  carve_dmc(w, ws, n > 0 ? n : 1, m > 0 ? m : 1);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "dmc_backward: workspace too small");
+  const int64_t ns = counts[0], nq = counts[3], nv = counts[4];
+  if (ns == 0 || nv == 0) return A3D_OK;
+  DmcIn in = make_in(p);
+  DmcGrad gr{g_vertices, g_l_dev, g_p_alpha, g_n_alpha, g_sdf, g_deform, g_alpha, g_beta, w.g_vd};
+  A3D_CUDA_TRY(cudaMemsetAsync(w.g_vd, 0, 3 * nv * sizeof(float), s));
+  if (nq > 0 && g_vertices) {
+    quad_bwd_kernel<<<gsz(nq), 256, 0, s>>>(nq, nv, w.quads, gr);
+    A3D_LAUNCH_CHECK();
+  }
+  EdgeData ed{w.e0, w.e1, w.idx_map};
+  vd_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, w.x, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, gr);
+  A3D_LAUNCH_CHECK();
+  return A3D_OK;
+}

@@ -201,6 +201,46 @@ int a3d_flood_extract(const a3d_flood_geom* geom, void* workspace, size_t worksp
 int a3d_flood_test(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes,
                    int label, const int64_t* ijk, int64_t n, uint8_t* out, a3d_stream_t stream);
 
+/* ---- sparse differentiable dual marching cubes ------------------------ */
+/* Replaces SparseDiffDMC.forward in training mode (weighted-average dual
+ * vertices, 4-triangle quad split) and its autograd backward
+ * (atom3d/mesh_extractor/sparse_diffdmc.py:76-232, :234-287, :516-871).
+ * All pointers are device memory; deform/alpha/beta may be NULL (then the
+ * reference's defaults: no deformation, unit weights). */
+typedef struct a3d_dmc_inputs {
+  const int64_t* voxel_coords;  /* [N,3]  */
+  const float* sdf;             /* [M]    */
+  const int64_t* cube_idx;      /* [N,8]  */
+  const float* deform;          /* [M,3]  */
+  const float* alpha;           /* [N,8]  raw (tanh-normalised inside) */
+  const float* beta;            /* [N,12] raw */
+  int64_t num_cubes;            /* N */
+  int64_t num_corners;          /* M */
+  int32_t resolution;
+  float isovalue;
+  float weight_scale;
+} a3d_dmc_inputs;
+
+size_t a3d_dmc_workspace_bytes(int64_t num_cubes, int64_t num_corners);
+/* Topology pass.  counts (host, 6): surface cubes, groups G (crossing
+ * cube-edges == L_dev/p_alpha/n_alpha rows), surface edges, quads Q, dual
+ * vertices V; the workspace keeps the topology for _emit and _backward. */
+int a3d_dmc_prepare(const a3d_dmc_inputs* in, void* workspace, size_t workspace_bytes,
+                    int64_t* counts, a3d_stream_t stream);
+/* Geometry pass: vertices [V+Q,3], faces [4Q,3] int64, L_dev [G],
+ * p_alpha [G,3], n_alpha [G,3]. */
+int a3d_dmc_emit(const a3d_dmc_inputs* in, void* workspace, size_t workspace_bytes,
+                 const int64_t* counts, float* vertices, int64_t* faces, float* l_dev,
+                 float* p_alpha, float* n_alpha, a3d_stream_t stream);
+/* Adjoint: accumulates into g_sdf [M], g_deform [M,3], g_alpha [N,8],
+ * g_beta [N,12] (each nullable, zero-initialised by the caller) from the
+ * incoming gradients of the five outputs (each nullable).  Per-edge
+ * quantities are recomputed, not stored. */
+int a3d_dmc_backward(const a3d_dmc_inputs* in, void* workspace, size_t workspace_bytes,
+                     const int64_t* counts, const float* g_vertices, const float* g_l_dev,
+                     const float* g_p_alpha, const float* g_n_alpha, float* g_sdf,
+                     float* g_deform, float* g_alpha, float* g_beta, a3d_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

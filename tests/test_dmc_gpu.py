@@ -1,0 +1,106 @@
+"""Parity of the native SparseDiffDMC (training mode) with the reference's
+golden outputs/gradients and the numpy oracle; adjoint vs FP64 central
+differences.  Topology (faces) bit-exact; vertices, L_dev, p_alpha, n_alpha
+within 1e-6 of the bounding-box diagonal of the grid ([-1, 1]^3: 2*sqrt(3))."""
+
+import numpy as np
+import pytest
+import torch
+
+from atom3d_b200 import SparseDiffDMC, synthetic
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-6 * 2 * np.sqrt(3)
+
+
+def run(g, **kw):
+    dmc = SparseDiffDMC(device="cuda")
+    s = torch.from_numpy(g["sdf"]).cuda().requires_grad_(True)
+    args = {k: torch.from_numpy(v).cuda().requires_grad_(True) for k, v in kw.items()}
+    o = dmc(torch.from_numpy(g["vox"]).cuda(), s, torch.from_numpy(g["cidx"]).cuda(), int(g["res"]), **args)
+    (o.vertices ** 2).sum().backward()
+    return o, s.grad, {k: v.grad for k, v in args.items()}
+
+
+def test_dmc_forward_matches_reference_golden(golden):
+    g = golden("dmc_small.npz")
+    o, gs, ga = run(g, deform=g["deform"])
+    assert np.array_equal(o.faces.cpu().numpy(), g["train_faces"])
+    for k in ("vertices", "L_dev", "p_alpha", "n_alpha"):
+        a, b = getattr(o, k).detach().cpu().numpy(), g["train_" + k]
+        assert a.shape == b.shape, k
+        assert np.abs(a - b).max() <= TOL, (k, np.abs(a - b).max())
+    # reference autograd gradients (loss = sum |v|^2)
+    assert np.abs(gs.cpu().numpy() - g["train_grad_sdf"]).max() <= 1e-4 * max(1.0, np.abs(g["train_grad_sdf"]).max())
+    gd = ga["deform"].cpu().numpy()
+    assert np.abs(gd - g["train_grad_deform"]).max() <= 1e-4 * max(1.0, np.abs(g["train_grad_deform"]).max())
+
+
+def test_dmc_alpha_beta_matches_reference_golden(golden):
+    g = golden("dmc_small.npz")
+    o, gs, _ = run(g, alpha=g["alpha"], beta=g["beta"])
+    assert np.array_equal(o.faces.cpu().numpy(), g["ab_faces"])
+    assert np.abs(o.vertices.detach().cpu().numpy() - g["ab_vertices"]).max() <= TOL
+    assert np.abs(o.L_dev.detach().cpu().numpy() - g["ab_L_dev"]).max() <= TOL
+    assert np.abs(gs.cpu().numpy() - g["ab_grad_sdf"]).max() <= 1e-4 * max(1.0, np.abs(g["ab_grad_sdf"]).max())
+
+
+def test_dmc_matches_numpy_oracle_medium():
+    from oracle import dmc_oracle as D
+
+    vox, sdf, cidx, _ = synthetic.dmc_spheres(res=96, seed=7, n_spheres=10)
+    o = SparseDiffDMC(device="cuda")(vox.cuda(), sdf.cuda(), cidx.cuda(), 96)
+    r = D.forward(vox.numpy(), sdf.numpy(), cidx.numpy(), 96)
+    assert np.array_equal(o.faces.cpu().numpy(), r["faces"])
+    for k in ("vertices", "L_dev", "p_alpha", "n_alpha"):
+        assert np.abs(getattr(o, k).cpu().numpy() - r[k]).max() <= TOL, k
+
+
+def test_dmc_grad_vs_fp64_central_differences():
+    from oracle import dmc_oracle as D
+
+    vox, sdf, cidx, _ = synthetic.dmc_spheres(res=24, seed=3, n_spheres=3, noise=0.0)
+    s = sdf.double().numpy()
+    rng = np.random.default_rng(0)
+    deform = rng.normal(0, 1e-3, (s.shape[0], 3))
+    o = SparseDiffDMC(device="cuda")
+    st = torch.from_numpy(s).float().cuda().requires_grad_(True)
+    dt = torch.from_numpy(deform).float().cuda().requires_grad_(True)
+    out = o(vox.cuda(), st, cidx.cuda(), 24, deform=dt)
+    (out.vertices ** 2).sum().backward()
+    gs, gd = st.grad.cpu().double().numpy(), dt.grad.cpu().double().numpy()
+    active = np.nonzero(np.abs(gs) > 1e-6)[0]
+    pick = rng.choice(active, size=min(40, active.shape[0]), replace=False)
+    h = 1e-6
+    for i in pick:
+        sp, sm = s.copy(), s.copy()
+        sp[i] += h
+        sm[i] -= h
+        fp = D.loss_vertices_sq(vox.numpy(), sp, cidx.numpy(), 24, deform=deform, dtype=np.float64)
+        fm = D.loss_vertices_sq(vox.numpy(), sm, cidx.numpy(), 24, deform=deform, dtype=np.float64)
+        fdv = (fp - fm) / (2 * h)
+        assert abs(fdv - gs[i]) <= 2e-3 * max(1.0, abs(fdv)), (i, fdv, gs[i])
+    for i in pick[:15]:
+        for a in range(3):
+            dp, dm = deform.copy(), deform.copy()
+            dp[i, a] += h
+            dm[i, a] -= h
+            fp = D.loss_vertices_sq(vox.numpy(), s, cidx.numpy(), 24, deform=dp, dtype=np.float64)
+            fm = D.loss_vertices_sq(vox.numpy(), s, cidx.numpy(), 24, deform=dm, dtype=np.float64)
+            fdv = (fp - fm) / (2 * h)
+            assert abs(fdv - gd[i, a]) <= 2e-3 * max(1.0, abs(fdv)), (i, a, fdv, gd[i, a])
+
+
+def test_dmc_empty_surface():
+    vox = torch.tensor([[0, 0, 0]], device="cuda")
+    cidx = torch.arange(8, device="cuda").view(1, 8)
+    out = SparseDiffDMC(device="cuda")(vox, torch.ones(8, device="cuda"), cidx, 4)
+    assert out.vertices.shape == (0, 3) and out.faces.shape == (0, 3)
+
+
+def test_dmc_eval_mode_not_provided():
+    dmc = SparseDiffDMC(device="cuda").eval()
+    with pytest.raises(NotImplementedError):
+        dmc(torch.zeros(1, 3, dtype=torch.long, device="cuda"), torch.ones(8, device="cuda"),
+            torch.arange(8, device="cuda").view(1, 8), 4)
