@@ -113,6 +113,19 @@ int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num_points,
             unsigned long long* stats, uint32_t flags,
             void* workspace, size_t workspace_bytes, a3d_stream_t stream);
 
+/* Allocation-free variant of a3d_udf (no counterpart in the reference).
+ * For callers that may not call cudaMalloc (a host application owning all
+ * device memory, or a latency-critical loop where an allocation would
+ * synchronise the device): scratch lives in a 24 MiB file-scope device
+ * array held by every GPU that loads the library.  At most 1,048,576
+ * queries per call (larger: A3D_ERR_ARGUMENT).  The first call on a device
+ * looks up the array's address; make it before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race.  Queries are
+ * Morton-sorted; results equal a3d_udf's. */
+int a3d_udf_noalloc(const a3d_bvh_view* bvh, const float* points, int64_t num_points,
+                    float* distances, int32_t* face_ids, float* closest_points,
+                    float* uvw, a3d_stream_t stream);
+
 /* Adjoint of the unsigned distance with respect to the mesh vertices:
  * grad_vertices[V,3] += sum_q grad_dist[q] * d dist_q / d vertex.
  * With closest point c = sum_i w_i v_i (w = clamped barycentrics of the
