@@ -417,6 +417,8 @@ __device__ __forceinline__ void quad_child_box(const WideNode* __restrict__ node
 // evaluates each test changes.
 constexpr int kTaskWarps = 2;
 constexpr int kTaskDepth = 32;
+constexpr int kSpillCap = 96;    // per-owner global overflow stack (entries)
+constexpr int kSpillChunk = 16;  // entries moved per spill / refill
 constexpr int kTaskTriCap = 32 * kMaxLeafTris;
 constexpr int kTaskPool = 64;  // queries per pool taken from the global counter
 
@@ -439,7 +441,8 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
     udf_task_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
                     const float* __restrict__ pts, int64_t n, const uint32_t* __restrict__ perm,
                     const float* __restrict__ bound, QueryOut out, SignArgs sg, unsigned long long* stats,
-                    uint32_t* __restrict__ rerun, uint32_t* __restrict__ nrerun, uint32_t* __restrict__ pool_counter) {
+                    uint32_t* __restrict__ rerun, uint32_t* __restrict__ nrerun, uint32_t* __restrict__ pool_counter,
+                    uint2* __restrict__ spill, int64_t spill_owners) {
   __shared__ TaskSmem smem[kTaskWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   TaskSmem& S = smem[warp];
@@ -459,6 +462,12 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
   float best_sq = INFINITY, px = 0.f, py = 0.f, pz = 0.f, bsq = INFINITY;
   bool have = false;
   int sp = 0;
+  // overflow stack in global memory (the workspace's spill region), used
+  // when the shared stack is full; owners beyond the region have none
+  const int64_t owner = ((int64_t)blockIdx.x * kTaskWarps + warp) * 32 + lane;
+  uint2* my_spill = (spill != nullptr && owner < spill_owners) ? spill + owner * kSpillCap : nullptr;
+  int gsp = 0;
+  unsigned long long rounds = 0;
 
   auto start = [&](int64_t k) {
     qi = perm ? (int64_t)perm[k] : k;
@@ -472,6 +481,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
     best_sq = INFINITY;
     best_tri = 0xffffffffu;
     sp = 0;
+    gsp = 0;
     // the previous result seeds the radius only for a nearby query in the
     // sorted order; otherwise a greedy probe does
     if (prev != 0xffffffffu && k - kprev <= 64 && k > kprev) {
@@ -510,13 +520,22 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
   distribute(FULL);
 
   while (__any_sync(FULL, phase != kIdle)) {
+    ++rounds;
     // (a) traversing owners without an item pop; finished owners emit and refetch
     bool done = false;
     if (phase == kTrav && !have) {
-      while (sp > 0) {
-        --sp;
-        const uint2 e = S.stack[sp][lane];
-        if (__uint_as_float(e.y) < best_sq) { ref = e.x; have = true; break; }
+      for (;;) {
+        while (sp > 0) {
+          --sp;
+          const uint2 e = S.stack[sp][lane];
+          if (__uint_as_float(e.y) < best_sq) { ref = e.x; have = true; break; }
+        }
+        if (have || gsp == 0) break;
+        // shared stack empty: bring back the most recently spilled chunk
+        const int k = gsp < kSpillChunk ? gsp : kSpillChunk;
+        gsp -= k;
+        for (int i = 0; i < k; ++i) S.stack[i][lane] = my_spill[gsp + i];
+        sp = k;
       }
       done = !have;
     }
@@ -604,8 +623,15 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
 #pragma unroll
         for (int c = 0; c < 4; ++c) q += d[c] < best_sq ? 1 : 0;
         if (q > 0) {
+          if (sp + (q - 1) > kTaskDepth && my_spill != nullptr && gsp + kSpillChunk <= kSpillCap) {
+            // move the oldest entries (visited last) to the global overflow stack
+            for (int i = 0; i < kSpillChunk; ++i) my_spill[gsp + i] = S.stack[i][lane];
+            for (int i = kSpillChunk; i < sp; ++i) S.stack[i - kSpillChunk][lane] = S.stack[i][lane];
+            gsp += kSpillChunk;
+            sp -= kSpillChunk;
+          }
           if (sp + (q - 1) > kTaskDepth) {
-            // would overflow: the deep-stack kernel re-runs the query
+            // still no room: the deep-stack kernel re-runs the query
             phase = kAbandon;
             have = false;
           } else {
@@ -640,7 +666,10 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
     }
     __syncwarp();
   }
-  if (kStats) flush_counters(ctr, stats);
+  if (kStats) {
+    flush_counters(ctr, stats);
+    if (lane == 0) atomicAdd(stats + 3, rounds);
+  }
 }
 
 template <bool kSign, bool kStats>
@@ -695,7 +724,9 @@ struct UdfWs {
   uint32_t* vals_alt;
   uint32_t* rs_scratch;
   uint32_t* rerun;
-  uint32_t* nrerun;  // [0] rerun count, [1] overflow flag
+  uint32_t* nrerun;  // [0] rerun count, [1] overflow flag, [2] pool counter
+  uint2* spill;      // optional overflow stacks (trailing workspace)
+  int64_t spill_owners;
 };
 
 size_t carve_udf(UdfWs& w, Workspace& ws, int64_t n, uint32_t flags) {
@@ -711,6 +742,13 @@ size_t carve_udf(UdfWs& w, Workspace& ws, int64_t n, uint32_t flags) {
   w.rerun = ws.take<uint32_t>(n);
   w.nrerun = ws.take<uint32_t>(4);
   return ws.used;
+}
+
+// owners of the persistent traversal that get an overflow stack when the
+// workspace has room for it (bounded: 148 SMs x 10 blocks x 64 lanes)
+int64_t spill_owner_bound(int64_t n) {
+  const int64_t cap = (int64_t)kNumSMs * 10 * 64;
+  return n + 128 < cap ? n + 128 : cap;
 }
 
 template <bool kSign, bool kStats>
@@ -734,7 +772,7 @@ int launch_udf(const a3d_bvh_view* bvh, const float* pts, int64_t n, const uint3
     const int64_t want_blocks = ceil_div(pools, kTaskWarps);
     const int64_t grid = want_blocks < (int64_t)sms * bps ? want_blocks : (int64_t)sms * bps;
     udf_task_kernel<kSign, kStats><<<(unsigned)grid, kTaskWarps * 32, 0, s>>>(
-        nodes, tris, pts, n, perm, bound, out, sg, stats, w.rerun, w.nrerun, w.nrerun + 2);
+        nodes, tris, pts, n, perm, bound, out, sg, stats, w.rerun, w.nrerun, w.nrerun + 2, w.spill, w.spill_owners);
   } else {
     udf_kernel<kSign, kStats><<<(unsigned)ceil_div(n, kUdfThreads), kUdfThreads, 0, s>>>(
         nodes, tris, pts, n, 1, perm, bound, out, sg, stats, w.rerun, w.nrerun);
@@ -793,10 +831,21 @@ __global__ void udf_backward_kernel(const float* __restrict__ pts, int64_t n, co
 
 using namespace a3d;
 
-extern "C" size_t a3d_udf_workspace_bytes(int64_t num_points, uint32_t flags) {
+namespace a3d {
+// Workspace a3d_udf needs at least (without the optional overflow stacks).
+size_t udf_required_workspace_bytes(int64_t num_points, uint32_t flags) {
   Workspace ws(nullptr, 0);
   UdfWs w;
   return carve_udf(w, ws, num_points > 0 ? num_points : 1, flags) + 256;
+}
+}  // namespace a3d
+
+extern "C" size_t a3d_udf_workspace_bytes(int64_t num_points, uint32_t flags) {
+  Workspace ws(nullptr, 0);
+  UdfWs w;
+  const int64_t n = num_points > 0 ? num_points : 1;
+  const size_t base = carve_udf(w, ws, n, flags);
+  return base + (size_t)spill_owner_bound(n) * kSpillCap * sizeof(uint2) + 512;
 }
 
 extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num_points, float* distances,
@@ -818,6 +867,14 @@ extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num
   UdfWs w;
   carve_udf(w, ws, num_points, flags);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "udf: workspace too small");
+  // whatever trails the required part holds per-owner overflow stacks
+  {
+    const uintptr_t base = ((uintptr_t)workspace + ws.used + 255) & ~(uintptr_t)255;
+    const uintptr_t endp = (uintptr_t)workspace + workspace_bytes;
+    const int64_t owners = base < endp ? (int64_t)((endp - base) / (kSpillCap * sizeof(uint2))) : 0;
+    w.spill = owners > 0 ? (uint2*)base : nullptr;
+    w.spill_owners = owners;
+  }
   const int64_t n = num_points;
   const uint32_t* perm = nullptr;
   if (flags & A3D_UDF_SORT_QUERIES) {

@@ -20,6 +20,10 @@
 
 #include "a3d_common.cuh"
 
+namespace a3d {
+size_t udf_required_workspace_bytes(int64_t num_points, uint32_t flags);
+}
+
 namespace {
 
 constexpr int64_t kNoAllocMaxQueries = 1ll << 20;    // 1,048,576 queries per call
@@ -60,7 +64,9 @@ extern "C" int a3d_udf_noalloc(const a3d_bvh_view* bvh, const float* points, int
   A3D_REQUIRE(num_points <= kNoAllocMaxQueries, A3D_ERR_ARGUMENT,
               "udf_noalloc: at most 1048576 queries per call; split larger batches");
   if (num_points == 0) return A3D_OK;
-  const size_t need = a3d_udf_workspace_bytes(num_points, A3D_UDF_SORT_QUERIES);
+  // the query's required scratch; any remainder of the array serves as
+  // optional overflow stacks
+  const size_t need = a3d::udf_required_workspace_bytes(num_points, A3D_UDF_SORT_QUERIES);
   A3D_REQUIRE(need <= kNoAllocScratchBytes, A3D_ERR_WORKSPACE, "udf_noalloc: static scratch smaller than required");
   void* scratch = nullptr;
   A3D_TRY(scratch_address(&scratch));

@@ -210,6 +210,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--queries", type=int, default=16 * 1024 * 1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the DMC and octree/flood measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -244,7 +245,7 @@ def main():
     st = torch.zeros(4, dtype=torch.int64, device=dev)
     step(st)
     torch.cuda.synchronize()
-    our_nodes, our_tris, reruns = (int(x) for x in st[:3].cpu())
+    our_nodes, our_tris, reruns, rounds = (int(x) for x in st[:4].cpu())
 
     for _ in range(args.warmup):
         step()
@@ -311,14 +312,111 @@ def main():
         "roofline": roof,
         "gpu_launches": args.steps * launches_per_udf(),
         "clocks": clocks,
-        "traversal": {"nodes_per_query": our_nodes / n, "tris_per_query": our_tris / n, "reruns": reruns},
+        "traversal": {"nodes_per_query": our_nodes / n, "tris_per_query": our_tris / n, "reruns": reruns,
+                      "warp_rounds_per_query": rounds / n},
     }
+    if not args.no_extra:
+        line["dmc"] = bench_dmc(dev, max(2, args.steps // 2), 2, cpu=(rank == 0 and not args.no_cpu_baseline))
+        line["octree_flood"] = bench_octree_flood(dev, max(2, args.steps // 2), 3)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(v, f, q)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def bench_dmc(dev, steps, warmup, cpu=True):
+    """SparseDiffDMC forward + backward (loss = sum |v|^2, grad w.r.t. sdf) on
+    the 32-sphere union sampled at 512^3 (2.2M active cubes)."""
+    from atom3d_b200 import SparseDiffDMC, synthetic
+
+    vox, sdf, cidx, _ = synthetic.dmc_spheres(res=512)
+    vd, sd, cd = vox.to(dev), sdf.to(dev), cidx.to(dev)
+    dmc = SparseDiffDMC(device=str(dev))
+    stream = torch.cuda.current_stream(dev)
+
+    def fwd_bwd():
+        s_ = sd.detach().requires_grad_(True)
+        o = dmc(vd, s_, cd, 512)
+        (o.vertices ** 2).sum().backward()
+        return o
+
+    for _ in range(warmup):
+        o = fwd_bwd()
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    fwd_ms = bwd_ms = 0.0
+    tot = 0.0
+    for _ in range(steps):
+        s_ = sd.detach().requires_grad_(True)
+        e0.record(stream)
+        o = dmc(vd, s_, cd, 512)
+        e1.record(stream)
+        (o.vertices ** 2).sum().backward()
+        e2.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms += e0.elapsed_time(e1)
+        bwd_ms += e1.elapsed_time(e2)
+        tot += e0.elapsed_time(e2)
+    n_cubes, n_v, n_f = vox.shape[0], o.vertices.shape[0], o.faces.shape[0]
+    peak, kind = peaks()
+    fwd = fwd_ms / steps
+    alg = 108.0 * n_cubes + 12.0 * n_v + 24.0 * n_f
+    out = {"metric": "DMC fwd+bwd ms (32-sphere SDF, 512^3, 2.2M active cubes)", "value": tot / steps, "unit": "ms",
+           "higher_is_better": False, "fwd_ms": fwd, "bwd_ms": bwd_ms / steps, "active_cubes": int(n_cubes),
+           "vertices": int(n_v), "faces": int(n_f),
+           "roofline_fwd": {"bound": "hbm", "achieved": alg / (fwd * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                            "frac": alg / (fwd * 1e-3) / 1e9 / peak, "peak_kind": kind,
+                            "bytes": "108 B/active cube + 12 B/vertex + 24 B/face"}}
+    if cpu:
+        from oracle import dmc_oracle, orc
+
+        t0 = time.perf_counter()
+        dmc_oracle.forward(vox.numpy(), sdf.numpy(), cidx.numpy(), 512)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": t * 1e3, "unit": "ms", "cores": orc.threads(), "kind": "port",
+                               "sample": "full forward only (numpy restatement of the reference's train mode)"}
+    return out
+
+
+def bench_octree_flood(dev, steps, warmup):
+    """octree_traverse (levels 4..10, 1024^3) and sparse_flood_fill on the
+    327,680-triangle displaced sphere, bounds [-1.5, 1.5]^3."""
+    from atom3d_b200 import MeshBVH, OctreeIndexer, sparse_flood_fill, synthetic
+
+    v, f = synthetic.octree_mesh()
+    bounds = torch.tensor([[-1.5] * 3, [1.5] * 3], device=dev)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mesh = MeshBVH(v.to(dev), f.to(dev))
+    torch.cuda.synchronize()
+    build_ms = (time.perf_counter() - t0) * 1e3
+    oc = OctreeIndexer(max_level=10, bounds=bounds, device=dev)
+    for _ in range(warmup):
+        cand = oc.octree_traverse(mesh, min_level=4)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        cand = oc.octree_traverse(mesh, min_level=4)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    oct_ms = e0.elapsed_time(e1) / steps
+    for _ in range(max(1, warmup - 2)):
+        out = sparse_flood_fill(mesh, 1024, min_level=4, bounds=bounds, verbose=False)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        out = sparse_flood_fill(mesh, 1024, min_level=4, bounds=bounds, verbose=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ff_ms = e0.elapsed_time(e1) / steps
+    return {"metric": "octree SAT 4->10 + sparse flood fill at 1024^3 (327,680 tris)", "unit": "ms",
+            "bvh_build_ms": build_ms, "octree_ms": oct_ms, "sparse_flood_fill_ms": ff_ms,
+            "candidate_voxels": int(cand.shape[0]),
+            "labels": {k: int(t.shape[0]) for k, t in out.items()}}
 
 
 def launches_per_udf():
