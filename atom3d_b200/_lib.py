@@ -86,6 +86,8 @@ A3D_ERR_OVERFLOW = 4
 A3D_ERR_TIMEOUT = 5
 A3D_UDF_SORT_QUERIES = 1
 A3D_UDF_ASSUME_SORTED = 2
+A3D_UDF_NO_REUSE = 4
+A3D_UDF_BOUND_SEEDS = 8
 
 _lib = None
 _lock = threading.Lock()

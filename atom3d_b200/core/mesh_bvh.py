@@ -71,7 +71,8 @@ class WideBVH:
         return self._view
 
     def query(self, points: torch.Tensor, sign: Optional[_lib.SignData] = None, bound: Optional[torch.Tensor] = None,
-              want_uvw: bool = True, stats: Optional[torch.Tensor] = None, sort_queries: bool = True):
+              want_uvw: bool = True, stats: Optional[torch.Tensor] = None, sort_queries: bool = True,
+              seeding: int = 0):
         """Raw closest-point query: (distances, face_ids int32, closest [N,3], uvw [N,3] or None)."""
         _lib.require_cuda(points, "points")
         p = points.detach().contiguous().float()
@@ -83,7 +84,7 @@ class WideBVH:
         uvw = torch.empty(n, 3, dtype=torch.float32, device=dev) if want_uvw else None
         if n == 0:
             return dist, fid, cp, uvw
-        flags = _lib.A3D_UDF_SORT_QUERIES if sort_queries else 0
+        flags = (_lib.A3D_UDF_SORT_QUERIES if sort_queries else 0) | seeding
         ws = _lib.workspace(_lib.lib().a3d_udf_workspace_bytes(n, flags), dev)
         b = None
         if bound is not None:

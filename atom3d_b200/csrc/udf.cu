@@ -435,6 +435,8 @@ struct TaskSmem {
 };
 
 enum : int { kIdle = 0, kProbe = 1, kSeed = 2, kTrav = 3, kAbandon = 4 };
+// radius seeding of the task kernel
+enum : uint32_t { kSeedReuse = 1u, kSeedBoundOnly = 2u };
 
 template <bool kSign, bool kStats>
 __global__ void __launch_bounds__(kTaskWarps * 32)
@@ -442,7 +444,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
                     const float* __restrict__ pts, int64_t n, const uint32_t* __restrict__ perm,
                     const float* __restrict__ bound, QueryOut out, SignArgs sg, unsigned long long* stats,
                     uint32_t* __restrict__ rerun, uint32_t* __restrict__ nrerun, uint32_t* __restrict__ pool_counter,
-                    uint2* __restrict__ spill, int64_t spill_owners) {
+                    uint2* __restrict__ spill, int64_t spill_owners, uint32_t seeding) {
   __shared__ TaskSmem smem[kTaskWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   TaskSmem& S = smem[warp];
@@ -482,9 +484,15 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
     best_tri = 0xffffffffu;
     sp = 0;
     gsp = 0;
-    // the previous result seeds the radius only for a nearby query in the
+    // a finite caller bound alone seeds the radius when asked to (no probe
+    // descent); else the previous result seeds it for a nearby query in the
     // sorted order; otherwise a greedy probe does
-    if (prev != 0xffffffffu && k - kprev <= 64 && k > kprev) {
+    if ((seeding & kSeedBoundOnly) && bsq < INFINITY) {
+      best_sq = bsq;
+      phase = kTrav;
+      ref = 0;
+      have = true;
+    } else if ((seeding & kSeedReuse) && prev != 0xffffffffu && k - kprev <= 64 && k > kprev) {
       phase = kSeed;
     } else {
       prev = 0xffffffffu;
@@ -672,6 +680,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
   }
 }
 
+
 template <bool kSign, bool kStats>
 __global__ void __launch_bounds__(64)
     udf_rerun_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
@@ -754,7 +763,7 @@ int64_t spill_owner_bound(int64_t n) {
 template <bool kSign, bool kStats>
 int launch_udf(const a3d_bvh_view* bvh, const float* pts, int64_t n, const uint32_t* perm, bool coherent,
                const float* bound, const QueryOut& out, const SignArgs& sg, unsigned long long* stats, UdfWs& w,
-               cudaStream_t s) {
+               uint32_t seeding, cudaStream_t s) {
   const WideNode* nodes = (const WideNode*)bvh->nodes;
   const TriRec* tris = (const TriRec*)bvh->tris;
   if (coherent) {
@@ -772,7 +781,8 @@ int launch_udf(const a3d_bvh_view* bvh, const float* pts, int64_t n, const uint3
     const int64_t want_blocks = ceil_div(pools, kTaskWarps);
     const int64_t grid = want_blocks < (int64_t)sms * bps ? want_blocks : (int64_t)sms * bps;
     udf_task_kernel<kSign, kStats><<<(unsigned)grid, kTaskWarps * 32, 0, s>>>(
-        nodes, tris, pts, n, perm, bound, out, sg, stats, w.rerun, w.nrerun, w.nrerun + 2, w.spill, w.spill_owners);
+        nodes, tris, pts, n, perm, bound, out, sg, stats, w.rerun, w.nrerun, w.nrerun + 2, w.spill, w.spill_owners,
+        seeding);
   } else {
     udf_kernel<kSign, kStats><<<(unsigned)ceil_div(n, kUdfThreads), kUdfThreads, 0, s>>>(
         nodes, tris, pts, n, 1, perm, bound, out, sg, stats, w.rerun, w.nrerun);
@@ -893,6 +903,8 @@ extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num
     perm = alt ? w.vals_alt : w.vals;
   }
   const bool coherent = perm != nullptr || (flags & A3D_UDF_ASSUME_SORTED) != 0;
+  const uint32_t seeding = ((flags & A3D_UDF_NO_REUSE) ? 0u : kSeedReuse) |
+                           ((flags & A3D_UDF_BOUND_SEEDS) && bound ? kSeedBoundOnly : 0u);
   A3D_CUDA_TRY(cudaMemsetAsync(w.nrerun, 0, 4 * sizeof(uint32_t), s));
   QueryOut out{distances, face_ids, closest_points, uvw};
   SignArgs sg{nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -902,11 +914,11 @@ extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num
                   pn ? sign->he_edge_idx : nullptr, sign->faces};
   }
   if (sign) {
-    if (stats) A3D_TRY((launch_udf<true, true>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, s)));
-    else A3D_TRY((launch_udf<true, false>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, s)));
+    if (stats) A3D_TRY((launch_udf<true, true>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, seeding, s)));
+    else A3D_TRY((launch_udf<true, false>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, seeding, s)));
   } else {
-    if (stats) A3D_TRY((launch_udf<false, true>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, s)));
-    else A3D_TRY((launch_udf<false, false>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, s)));
+    if (stats) A3D_TRY((launch_udf<false, true>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, seeding, s)));
+    else A3D_TRY((launch_udf<false, false>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, seeding, s)));
   }
   if (stats) {
     // reruns are reported as bound misses / spills (same counter: re-run queries)

@@ -226,7 +226,7 @@ def main():
     mesh = MeshBVH(v.to(dev), f.to(dev))
     qd = q.to(dev)
     bvh = mesh._bvh
-    flags = _lib.A3D_UDF_SORT_QUERIES
+    flags = _lib.A3D_UDF_SORT_QUERIES | int(os.environ.get("ATOM3D_B200_UDF_FLAGS", "0"))
     dist_o = torch.empty(n, device=dev)
     fid_o = torch.empty(n, dtype=torch.int32, device=dev)
     cp_o = torch.empty(n, 3, device=dev)
@@ -451,7 +451,8 @@ def time_traversal_kernel(bvh, qd, dist_o, fid_o, cp_o, ws, flags, stream, steps
 
     def call():
         _lib.call("a3d_udf", ctypes.byref(view), qs.data_ptr(), n, dist_o.data_ptr(), fid_o.data_ptr(),
-                  cp_o.data_ptr(), None, None, None, None, _lib.A3D_UDF_ASSUME_SORTED, ws.data_ptr(), ws.numel(),
+                  cp_o.data_ptr(), None, None, None, None, _lib.A3D_UDF_ASSUME_SORTED | (flags & ~_lib.A3D_UDF_SORT_QUERIES),
+                  ws.data_ptr(), ws.numel(),
                   stream.cuda_stream)
 
     for _ in range(3):

@@ -106,6 +106,14 @@ typedef struct a3d_sign_data {
  * bound misses, stack spills.  */
 #define A3D_UDF_SORT_QUERIES 1u
 #define A3D_UDF_ASSUME_SORTED 2u  /* queries already spatially coherent: skip the sort */
+/* radius seeding (results never depend on it): by default a query's pruning
+ * radius starts just above the distance to the closest triangle of the
+ * previous query in the sorted order, or of a greedy descent, capped by
+ * `bound`.  NO_REUSE drops the previous-query seed; BOUND_SEEDS lets a
+ * finite `bound` alone seed the radius (no greedy descent).  A query with
+ * no triangle inside a too-small bound is re-run without it. */
+#define A3D_UDF_NO_REUSE 4u
+#define A3D_UDF_BOUND_SEEDS 8u
 size_t a3d_udf_workspace_bytes(int64_t num_points, uint32_t flags);
 int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num_points,
             float* distances, int32_t* face_ids, float* closest_points,
@@ -253,6 +261,53 @@ int a3d_dmc_backward(const a3d_dmc_inputs* in, void* workspace, size_t workspace
                      const int64_t* counts, const float* g_vertices, const float* g_l_dev,
                      const float* g_p_alpha, const float* g_n_alpha, float* g_sdf,
                      float* g_deform, float* g_alpha, float* g_beta, a3d_stream_t stream);
+
+/* ---- learned distance bound (no counterpart in the reference) ----------- */
+/* A Fourier-feature MLP (3 -> 64 -> 128 -> 128 -> 128 -> 1, ReLU) predicts
+ * a query's unsigned distance; bound = max(y, 0) * scale + margin seeds
+ * a3d_udf's pruning radius (results never depend on it).  Inference is one
+ * fused BF16 tensor-core kernel; training uses the kernels below. */
+typedef struct a3d_mlp_weights {
+  const void* w1t;   /* bf16 [128][64]  (W1 transposed, out-major) */
+  const void* w2t;   /* bf16 [128][128] */
+  const void* w3t;   /* bf16 [128][128] */
+  const float* b1;   /* [128] */
+  const float* b2;
+  const float* b3;
+  const float* w4;   /* [128] head weights */
+  float b4;
+  const float* freq; /* [32][3] Fourier frequencies */
+  float norm[4];     /* x_hat = (x - norm[0..2]) * norm[3] */
+  float scale;
+  float margin;
+} a3d_mlp_weights;
+
+int a3d_mlp_bound(const a3d_mlp_weights* w, const float* x, int64_t n, float* bound,
+                  a3d_stream_t stream);
+
+/* training building blocks (BF16 operands, FP32 accumulation) */
+typedef struct a3d_gemm_args {
+  const void* A;           /* bf16, element (m,k) at A[m*sam + k*sak] */
+  const void* B;           /* bf16, element (k,n) at B[k*sbk + n*sbn] */
+  int64_t sam, sak, sbk, sbn;
+  int32_t m, n, k;
+  const float* bias;       /* [n] or NULL */
+  const void* mask;        /* bf16 [m,n]: result zeroed where mask <= 0, or NULL */
+  int32_t relu;
+  float* Cf;               /* fp32 [m,n] or NULL */
+  int32_t accumulate;      /* Cf += result */
+  void* Cb;                /* bf16 [m,n] or NULL */
+} a3d_gemm_args;
+int a3d_gemm_bf16(const a3d_gemm_args* args, a3d_stream_t stream);
+int a3d_mlp_fourier(const float* x, int64_t n, const float* norm4, const float* freq,
+                    void* feat_bf16, a3d_stream_t stream);
+int a3d_mlp_head(const void* h_bf16, int64_t n, const float* w4, const float* b4,
+                 const float* target, float under_weight, float* y, void* dh_bf16,
+                 float* dw4, float* db4, float* loss, a3d_stream_t stream);
+int a3d_mlp_colsum(const void* g_bf16, int64_t n, int cols, float* out, a3d_stream_t stream);
+int a3d_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float beta1,
+             float beta2, float eps, int step, a3d_stream_t stream);
+int a3d_to_bf16(const float* in, int64_t n, void* out, a3d_stream_t stream);
 
 #ifdef __cplusplus
 }
