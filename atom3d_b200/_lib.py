@@ -48,6 +48,7 @@ class SignData(ctypes.Structure):
 _SIGNATURES: dict[str, tuple] = {
     "a3d_last_error": (ctypes.c_char_p, []),
     "a3d_version": (ctypes.c_char_p, []),
+    "a3d_udf_status": (c_int, [c_vp, ctypes.POINTER(c_u32), c_vp]),
     "a3d_bvh_build_workspace_bytes": (c_size, [c_i64]),
     "a3d_bvh_build": (
         c_int,

@@ -86,6 +86,7 @@ class WideBVH:
             return dist, fid, cp, uvw
         flags = (_lib.A3D_UDF_SORT_QUERIES if sort_queries else 0) | seeding
         ws = _lib.workspace(_lib.lib().a3d_udf_workspace_bytes(n, flags), dev)
+        self._last_ws = ws
         b = None
         if bound is not None:
             b = bound.detach().contiguous().float()
@@ -97,6 +98,19 @@ class WideBVH:
             ws.data_ptr(), ws.numel(), _lib.stream_ptr(dev),
         )
         return dist, fid, cp, uvw
+
+
+    def status(self) -> dict:
+        """Status words of the last query (synchronises): queries re-run,
+        deep-stack overflow, guard faults."""
+        return udf_status(self._last_ws, self.device)
+
+
+def udf_status(ws: torch.Tensor, device) -> dict:
+    """Read the status words a query left at the start of its workspace."""
+    st = (ctypes.c_uint32 * 4)()
+    _lib.call("a3d_udf_status", ws.data_ptr(), st, _lib.stream_ptr(device))
+    return {"reruns": int(st[0]), "overflow": int(st[1]), "faults": int(st[3])}
 
 
 class _DistanceFn(torch.autograd.Function):

@@ -1,20 +1,32 @@
-// GPU construction of the wide BVH.
+// GPU construction of the wide BVH, for one mesh or a batch of meshes.
 //
 // Replaces the reference's single-threaded host SAH builder
-// (atom3d/kernels/bvh_kernels.cu:616-925).  Pipeline, all on the stream:
-//   1. per-triangle AABB/centroid + scene and centroid bounds (block reduce,
-//      one atomic per block)
-//   2. 63-bit Morton code of each centroid
-//   3. stable radix sort of (code, face id) with the in-house sort
-//   4. binary radix tree over the sorted codes (one thread per internal node,
-//      duplicate codes disambiguated by index)
+// (atom3d/kernels/bvh_kernels.cu:616-925).  Pipeline, all on the stream and
+// without a host synchronisation, so a whole (batched) build can be captured
+// in a CUDA graph:
+//   1. per-triangle AABB/centroid; per-mesh scene and centroid bounds
+//      (block reduce, one atomic per block and mesh)
+//   2. sort key = mesh id in the high bits | Morton code of the centroid in
+//      its mesh's centroid box (21 bits per axis for one mesh; fewer when
+//      the mesh id needs bits)
+//   3. stable radix sort of (key, face) with the in-house sort; mesh m's
+//      faces then occupy sorted positions [face_off[m], face_off[m+1])
+//   4. one binary radix tree per mesh over its sorted range [s, e): internal
+//      nodes s..e-2 with root s, leaf j at N + j (duplicate codes
+//      disambiguated by index)
 //   5. bottom-up refit (second arriving child computes the union box)
 //   6. surface-area-guided collapse into 4-wide quantised nodes: starting
 //      from a binary node, the child with the largest surface area is opened
 //      until four slots are used; subtrees of <= leaf_max triangles become
-//      leaves.  Level-synchronous, node indices assigned by prefix sum so the
-//      layout is deterministic.
+//      leaves.  Level-synchronous over device-side worklists; a wide node is
+//      written at the slot of its binary node, so the order in which a
+//      level's work is done does not matter
+//   7. layout: wide nodes stably sorted by level -- breadth first, each
+//      node's children contiguous, mesh roots at 0..M-1 -- and child
+//      references renumbered
+//   8. triangle records in sorted order (64 B, with reciprocals)
 #include <math.h>
+#include <string.h>
 
 #include "bvh_layout.cuh"
 #include "primitives.cuh"
@@ -24,13 +36,19 @@ namespace a3d {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kMaxLevels = 64;  // wide levels; deeper trees report A3D_ERR_OVERFLOW
+constexpr int kLevelBlocks = kNumSMs * 8;
+constexpr uint32_t kNoLevel = 255u;
 
 struct BuildWs {
+  int64_t* face_off;    // single-mesh builds: offsets written on the device
+  int64_t* vert_off;
   float4* tri_lo;
   float4* tri_hi;
   float4* centroid;
-  uint32_t* bounds;  // 12 flipped floats: scene lo, scene hi, cent lo, cent hi
-  int32_t* err;
+  uint32_t* mesh_of;    // mesh id per (original) face
+  uint32_t* bounds;     // [M][12] flipped floats: scene lo, scene hi, cent lo, cent hi
+  int32_t* err;         // [0] face index out of range / empty mesh, [1] depth overflow
   uint64_t* keys;
   uint64_t* keys_alt;
   uint32_t* vals;
@@ -38,31 +56,32 @@ struct BuildWs {
   uint32_t* rs_scratch;
   int32_t* left;
   int32_t* right;
-  int32_t* parent;
+  int32_t* parent;      // [2N]
   int32_t* first;
   int32_t* last;
-  float4* box_lo;  // [2n-1]: internal 0..n-2, leaf j at n-1+j
+  float4* box_lo;       // [2N]: internal 0..N-1 (per-mesh ranges), leaf j at N+j
   float4* box_hi;
   uint32_t* visit;
-  int32_t* work_a_bin;
-  int32_t* work_a_node;
-  int32_t* work_b_bin;
-  int32_t* work_b_node;
-  int32_t* child_bin;  // [n*4]
-  uint8_t* child_leaf; // [n*4]
-  int32_t* nchild;
-  uint32_t* nwide;
-  uint32_t* nwide_off;
-  uint32_t* scan_tmp;
-  uint32_t* total;
+  int32_t* work_a;
+  int32_t* work_b;
+  uint32_t* counters;   // [kMaxLevels + 1] worklist sizes per level
+  WideNode* tmp_nodes;  // [N] wide node at the slot of its binary node
+  uint32_t* lvl;        // [N] level of the wide node at a slot, kNoLevel if none
+  uint32_t* lvl_alt;
+  uint32_t* slot;
+  uint32_t* slot_alt;
+  uint32_t* newidx;     // [N] slot -> final node index
+  int64_t* count;       // single-mesh builds: node count
 };
 
-size_t carve(BuildWs& w, Workspace& ws, int64_t n) {
-  const int64_t nn = n > 1 ? 2 * n - 1 : 1;
+size_t carve(BuildWs& w, Workspace& ws, int64_t n, int64_t m) {
+  w.face_off = ws.take<int64_t>(2);
+  w.vert_off = ws.take<int64_t>(2);
   w.tri_lo = ws.take<float4>(n);
   w.tri_hi = ws.take<float4>(n);
   w.centroid = ws.take<float4>(n);
-  w.bounds = ws.take<uint32_t>(12);
+  w.mesh_of = ws.take<uint32_t>(n);
+  w.bounds = ws.take<uint32_t>(12 * m);
   w.err = ws.take<int32_t>(4);
   w.keys = ws.take<uint64_t>(n);
   w.keys_alt = ws.take<uint64_t>(n);
@@ -71,23 +90,22 @@ size_t carve(BuildWs& w, Workspace& ws, int64_t n) {
   w.rs_scratch = ws.take<uint32_t>((int64_t)radix_sort_scratch_elems(n));
   w.left = ws.take<int32_t>(n);
   w.right = ws.take<int32_t>(n);
-  w.parent = ws.take<int32_t>(nn);
+  w.parent = ws.take<int32_t>(2 * n);
   w.first = ws.take<int32_t>(n);
   w.last = ws.take<int32_t>(n);
-  w.box_lo = ws.take<float4>(nn);
-  w.box_hi = ws.take<float4>(nn);
+  w.box_lo = ws.take<float4>(2 * n);
+  w.box_hi = ws.take<float4>(2 * n);
   w.visit = ws.take<uint32_t>(n);
-  w.work_a_bin = ws.take<int32_t>(n);
-  w.work_a_node = ws.take<int32_t>(n);
-  w.work_b_bin = ws.take<int32_t>(n);
-  w.work_b_node = ws.take<int32_t>(n);
-  w.child_bin = ws.take<int32_t>(4 * n);
-  w.child_leaf = ws.take<uint8_t>(4 * n);
-  w.nchild = ws.take<int32_t>(n);
-  w.nwide = ws.take<uint32_t>(n);
-  w.nwide_off = ws.take<uint32_t>(n);
-  w.scan_tmp = ws.take<uint32_t>((int64_t)scan_workspace_elems(n));
-  w.total = ws.take<uint32_t>(2);
+  w.work_a = ws.take<int32_t>(n);
+  w.work_b = ws.take<int32_t>(n);
+  w.counters = ws.take<uint32_t>(kMaxLevels + 1);
+  w.tmp_nodes = ws.take<WideNode>(n);
+  w.lvl = ws.take<uint32_t>(n);
+  w.lvl_alt = ws.take<uint32_t>(n);
+  w.slot = ws.take<uint32_t>(n);
+  w.slot_alt = ws.take<uint32_t>(n);
+  w.newidx = ws.take<uint32_t>(n);
+  w.count = ws.take<int64_t>(1);
   return ws.used;
 }
 
@@ -95,32 +113,82 @@ __device__ __forceinline__ float3 ld3(const float* p, int64_t i) {
   return make_float3(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
 }
 
-__global__ void init_bounds_kernel(uint32_t* bounds, int32_t* err) {
-  int t = threadIdx.x;
-  if (t < 12) bounds[t] = ((t / 3) % 2 == 0) ? 0xffffffffu : 0u;  // lo slots: min, hi slots: max
-  if (t < 4) err[t] = 0;
+// index m with off[m] <= i < off[m+1] (off ascending, off[0] = 0)
+__device__ __forceinline__ int segment_of(const int64_t* __restrict__ off, int nseg, int64_t i) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 
-// 1. triangle boxes, centroids, bounds, triangle records (original order)
+__global__ void single_offsets_kernel(int64_t* face_off, int64_t* vert_off, int64_t nf, int64_t nv) {
+  if (threadIdx.x == 0) {
+    face_off[0] = 0;
+    face_off[1] = nf;
+    vert_off[0] = 0;
+    vert_off[1] = nv;
+  }
+}
+
+// per-mesh bounds, error words, level counters and the level-0 worklist
+// (the mesh roots: internal node s, or the lone leaf N + s)
+__global__ void init_kernel(const int64_t* __restrict__ face_off, int nmesh, int64_t n, uint32_t* bounds,
+                            int32_t* err, uint32_t* counters, int32_t* work0) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < 12 * (int64_t)nmesh) bounds[t] = (((t % 12) / 3) % 2 == 0) ? 0xffffffffu : 0u;
+  if (t < 4) err[t] = 0;
+  if (t <= kMaxLevels) counters[t] = t == 0 ? (uint32_t)nmesh : 0u;
+  if (t < nmesh) {
+    const int64_t s = face_off[t], e = face_off[t + 1];
+    if (e <= s) atomicExch(err, 1);
+    work0[t] = (int32_t)(e - s > 1 ? s : n + s);
+  }
+}
+
+// v[0..5]: minima (scene lo, centroid lo), v[6..11]: maxima (scene hi, centroid hi)
+__device__ __forceinline__ void bounds_atomic(uint32_t* b, const float* v) {
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    const int slot = k < 3 ? k : (k < 6 ? 6 + (k - 3) : (k < 9 ? 3 + (k - 6) : 9 + (k - 9)));
+    if (isfinite(v[k])) {
+      if (k < 6) atomicMin(&b[slot], float_flip(v[k]));
+      else atomicMax(&b[slot], float_flip(v[k]));
+    }
+  }
+}
+
+// 1. triangle boxes, centroids, mesh ids, per-mesh bounds
 __global__ void __launch_bounds__(kThreads)
-    tri_prep_kernel(const float* __restrict__ V, int64_t nv, const int32_t* __restrict__ F, int64_t nf,
-                    float4* __restrict__ tri_lo, float4* __restrict__ tri_hi, float4* __restrict__ cen,
+    tri_prep_kernel(const float* __restrict__ V, const int64_t* __restrict__ vert_off, const int32_t* __restrict__ F,
+                    const int64_t* __restrict__ face_off, int nmesh, int64_t nf, float4* __restrict__ tri_lo,
+                    float4* __restrict__ tri_hi, float4* __restrict__ cen, uint32_t* __restrict__ mesh_of,
                     uint32_t* __restrict__ bounds, int32_t* __restrict__ err) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i0b = (int64_t)blockIdx.x * blockDim.x;
+  __shared__ int s_m0;
+  if (threadIdx.x == 0) s_m0 = segment_of(face_off, nmesh, i0b);
+  __syncthreads();
+  const int m0 = s_m0;
   float v[12];
 #pragma unroll
   for (int k = 0; k < 6; ++k) { v[k] = INFINITY; v[k + 6] = -INFINITY; }
   if (i < nf) {
+    const int m = segment_of(face_off, nmesh, i);
+    mesh_of[i] = (uint32_t)m;
+    const int64_t vb = vert_off[m], nv = vert_off[m + 1] - vb;
     int32_t i0 = F[3 * i], i1 = F[3 * i + 1], i2 = F[3 * i + 2];
     if (i0 < 0 || i1 < 0 || i2 < 0 || i0 >= nv || i1 >= nv || i2 >= nv) {
       atomicExch(err, 1);
       i0 = i1 = i2 = 0;
     }
-    float3 a = ld3(V, i0), b = ld3(V, i1), c = ld3(V, i2);
-    float3 lo = make_float3(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z));
-    float3 hi = make_float3(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z));
-    float3 ce = make_float3((a.x + b.x + c.x) * (1.0f / 3.0f), (a.y + b.y + c.y) * (1.0f / 3.0f),
-                            (a.z + b.z + c.z) * (1.0f / 3.0f));
+    const float3 a = ld3(V, vb + i0), b = ld3(V, vb + i1), c = ld3(V, vb + i2);
+    const float3 lo = make_float3(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z));
+    const float3 hi = make_float3(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z));
+    const float3 ce = make_float3((a.x + b.x + c.x) * (1.0f / 3.0f), (a.y + b.y + c.y) * (1.0f / 3.0f),
+                                  (a.z + b.z + c.z) * (1.0f / 3.0f));
     tri_lo[i] = make_float4(lo.x, lo.y, lo.z, 0.f);
     tri_hi[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
     cen[i] = make_float4(ce.x, ce.y, ce.z, 0.f);
@@ -128,8 +196,15 @@ __global__ void __launch_bounds__(kThreads)
     v[3] = ce.x; v[4] = ce.y; v[5] = ce.z;
     v[6] = hi.x; v[7] = hi.y; v[8] = hi.z;
     v[9] = ce.x; v[10] = ce.y; v[11] = ce.z;
+    if (m != m0) {
+      // a block straddling meshes: faces not of the block's first mesh
+      // contribute directly
+      bounds_atomic(bounds + 12 * (int64_t)m, v);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) { v[k] = INFINITY; v[k + 6] = -INFINITY; }
+    }
   }
-  // block reduce: min of v[0..5], max of v[6..11]
+  // block reduce for the block's first mesh
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -143,81 +218,91 @@ __global__ void __launch_bounds__(kThreads)
   if (lane == 0)
     for (int k = 0; k < 12; ++k) s[warp][k] = v[k];
   __syncthreads();
-  if (threadIdx.x < 12) {
-    const int k = threadIdx.x;
-    float r = s[0][k];
-    for (int w = 1; w < kThreads / 32; ++w) r = k < 6 ? fminf(r, s[w][k]) : fmaxf(r, s[w][k]);
-    // bounds layout: [0..2] scene lo, [3..5] scene hi, [6..8] cent lo, [9..11] cent hi
-    const int slot = k < 3 ? k : (k < 6 ? 6 + (k - 3) : (k < 9 ? 3 + (k - 6) : 9 + (k - 9)));
-    if (isfinite(r)) {
-      if (k < 6) atomicMin(&bounds[slot], float_flip(r));
-      else atomicMax(&bounds[slot], float_flip(r));
+  if (threadIdx.x == 0 && i0b < nf) {
+    float r[12];
+    for (int k = 0; k < 12; ++k) {
+      r[k] = s[0][k];
+      for (int w = 1; w < kThreads / 32; ++w) r[k] = k < 6 ? fminf(r[k], s[w][k]) : fmaxf(r[k], s[w][k]);
     }
+    bounds_atomic(bounds + 12 * (int64_t)m0, r);
   }
 }
 
-// 2. Morton codes of centroids
-__global__ void morton_kernel(const float4* __restrict__ cen, int64_t n, const uint32_t* __restrict__ bounds,
-                              uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+// 2. sort keys: mesh id above the Morton code of the centroid
+__global__ void morton_kernel(const float4* __restrict__ cen, const uint32_t* __restrict__ mesh_of, int64_t n,
+                              const uint32_t* __restrict__ bounds, int bits, uint64_t* __restrict__ keys,
+                              uint32_t* __restrict__ vals) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float lo[3] = {float_unflip(bounds[6]), float_unflip(bounds[7]), float_unflip(bounds[8])};
-  const float hi[3] = {float_unflip(bounds[9]), float_unflip(bounds[10]), float_unflip(bounds[11])};
+  const uint32_t m = mesh_of[i];
+  const uint32_t* b = bounds + 12 * (int64_t)m;
+  const float lo[3] = {float_unflip(b[6]), float_unflip(b[7]), float_unflip(b[8])};
+  const float hi[3] = {float_unflip(b[9]), float_unflip(b[10]), float_unflip(b[11])};
   const float4 c = cen[i];
   const float cc[3] = {c.x, c.y, c.z};
+  const float qmax = (float)((1u << bits) - 1u);
   uint64_t code = 0;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const float ext = hi[a] - lo[a];
     float t = ext > 0.f ? (cc[a] - lo[a]) / ext : 0.f;
     t = fminf(fmaxf(t, 0.f), 1.f);
-    const uint64_t q = (uint64_t)(t * 2097151.0f);
+    const uint64_t q = (uint64_t)(t * qmax);
     code |= spread3_21(q) << a;
   }
-  keys[i] = code;
+  keys[i] = ((uint64_t)m << (3 * bits)) | code;
   vals[i] = (uint32_t)i;
 }
 
-// 4. binary radix tree
-__device__ __forceinline__ int delta(const uint64_t* keys, int64_t n, int i, int j) {
-  if (j < 0 || j >= n) return -1;
+// 4. binary radix tree of each mesh's sorted range
+__device__ __forceinline__ int delta(const uint64_t* keys, int64_t s, int64_t e, int i, int j) {
+  if (j < s || j >= e) return -1;
   const uint64_t a = keys[i], b = keys[j];
   if (a != b) return __clzll((long long)(a ^ b));
   return 64 + __clz(i ^ j);
 }
 
-__global__ void radix_tree_kernel(const uint64_t* __restrict__ keys, int64_t n, int32_t* __restrict__ left,
-                                  int32_t* __restrict__ right, int32_t* __restrict__ parent,
-                                  int32_t* __restrict__ first, int32_t* __restrict__ last) {
-  const int i = (int)((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
-  if (i >= n - 1) return;
-  const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
-  const int dmin = delta(keys, n, i, i - d);
+__global__ void radix_tree_kernel(const uint64_t* __restrict__ keys, const int64_t* __restrict__ face_off, int nmesh,
+                                  int64_t n, int32_t* __restrict__ left, int32_t* __restrict__ right,
+                                  int32_t* __restrict__ parent, int32_t* __restrict__ first,
+                                  int32_t* __restrict__ last) {
+  const int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ii >= n) return;
+  const int i = (int)ii;
+  const int m = segment_of(face_off, nmesh, ii);
+  const int64_t s = face_off[m], e = face_off[m + 1];
+  if (ii == e - 1) {
+    // the last position of a range carries no internal node; a lone leaf
+    // is its mesh's root
+    if (e - s == 1) parent[n + s] = -1;
+    return;
+  }
+  const int d = (delta(keys, s, e, i, i + 1) - delta(keys, s, e, i, i - 1)) >= 0 ? 1 : -1;
+  const int dmin = delta(keys, s, e, i, i - d);
   int lmax = 2;
-  while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  while (delta(keys, s, e, i, i + lmax * d) > dmin) lmax <<= 1;
   int l = 0;
   for (int t = lmax >> 1; t > 0; t >>= 1)
-    if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    if (delta(keys, s, e, i, i + (l + t) * d) > dmin) l += t;
   const int j = i + l * d;
-  const int dnode = delta(keys, n, i, j);
-  int s = 0;
+  const int dnode = delta(keys, s, e, i, j);
+  int sp = 0;
   int t = l;
   do {
     t = (t + 1) >> 1;
-    if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    if (delta(keys, s, e, i, i + (sp + t) * d) > dnode) sp += t;
   } while (t > 1);
-  const int gamma = i + s * d + (d < 0 ? -1 : 0);
+  const int gamma = i + sp * d + (d < 0 ? -1 : 0);
   const int lo = min(i, j), hi = max(i, j);
-  const int nm1 = (int)(n - 1);
-  const int lc = (lo == gamma) ? nm1 + gamma : gamma;
-  const int rc = (hi == gamma + 1) ? nm1 + gamma + 1 : gamma + 1;
+  const int lc = (lo == gamma) ? (int)n + gamma : gamma;
+  const int rc = (hi == gamma + 1) ? (int)n + gamma + 1 : gamma + 1;
   left[i] = lc;
   right[i] = rc;
   parent[lc] = i;
   parent[rc] = i;
   first[i] = lo;
   last[i] = hi;
-  if (i == 0) parent[0] = -1;
+  if (ii == s) parent[i] = -1;
 }
 
 // 5. refit: leaf boxes from sorted triangles, unions bottom-up
@@ -227,11 +312,10 @@ __global__ void refit_kernel(const uint32_t* __restrict__ order, const float4* _
                              float4* box_lo, float4* box_hi, uint32_t* visit) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
-  const int64_t leaf = (n - 1) + j;
+  const int64_t leaf = n + j;
   const uint32_t f = order[j];
   box_lo[leaf] = tri_lo[f];
   box_hi[leaf] = tri_hi[f];
-  if (n == 1) return;
   __threadfence();
   int p = parent[leaf];
   while (p >= 0) {
@@ -250,62 +334,6 @@ __global__ void refit_kernel(const uint32_t* __restrict__ order, const float4* _
 __device__ __forceinline__ float half_area(float4 lo, float4 hi) {
   const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
   return dx * dy + dy * dz + dz * dx;
-}
-
-// 6a. choose the (up to 4) children of each wide node of this level
-__global__ void collapse_select_kernel(const int32_t* __restrict__ work_bin, int64_t nwork, int64_t n,
-                                       int leaf_max, const int32_t* __restrict__ left,
-                                       const int32_t* __restrict__ right, const int32_t* __restrict__ first,
-                                       const int32_t* __restrict__ last, const float4* __restrict__ box_lo,
-                                       const float4* __restrict__ box_hi, int32_t* __restrict__ child_bin,
-                                       uint8_t* __restrict__ child_leaf, int32_t* __restrict__ nchild,
-                                       uint32_t* __restrict__ nwide) {
-  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nwork) return;
-  const int nm1 = (int)(n - 1);
-  const int b = work_bin[k];
-  int c[4];
-  int cnt;
-  if (b >= nm1) {  // a lone leaf as root (single-triangle mesh)
-    c[0] = b;
-    cnt = 1;
-  } else {
-    c[0] = left[b];
-    c[1] = right[b];
-    cnt = 2;
-    while (cnt < 4) {
-      int best = -1;
-      float best_a = -1.f;
-      for (int j = 0; j < cnt; ++j) {
-        if (c[j] < nm1) {
-          const float a = half_area(box_lo[c[j]], box_hi[c[j]]);
-          if (a > best_a) { best_a = a; best = j; }
-        }
-      }
-      if (best < 0) break;
-      const int x = c[best];
-      for (int j = cnt; j > best + 1; --j) c[j] = c[j - 1];
-      c[best] = left[x];
-      c[best + 1] = right[x];
-      ++cnt;
-    }
-  }
-  uint32_t w = 0;
-  for (int j = 0; j < 4; ++j) {
-    if (j < cnt) {
-      const int cj = c[j];
-      const int count = cj >= nm1 ? 1 : last[cj] - first[cj] + 1;
-      const bool leaf = count <= leaf_max;
-      child_bin[4 * k + j] = cj;
-      child_leaf[4 * k + j] = leaf ? 1 : 0;
-      if (!leaf) ++w;
-    } else {
-      child_bin[4 * k + j] = -1;
-      child_leaf[4 * k + j] = 0;
-    }
-  }
-  nchild[k] = cnt;
-  nwide[k] = w;
 }
 
 __device__ __forceinline__ uint32_t scale_exponent(float ext) {
@@ -330,68 +358,145 @@ __device__ __forceinline__ void quantize_axis(float o, float s, float lo, float 
   qhi = (uint32_t)qh;
 }
 
-// 6b. write the wide nodes of this level and the next worklist
-__global__ void collapse_emit_kernel(const int32_t* __restrict__ work_bin, const int32_t* __restrict__ work_node,
-                                     int64_t nwork, int64_t n, const int32_t* __restrict__ first,
-                                     const int32_t* __restrict__ last, const float4* __restrict__ box_lo,
-                                     const float4* __restrict__ box_hi, const int32_t* __restrict__ child_bin,
-                                     const uint8_t* __restrict__ child_leaf, const int32_t* __restrict__ nchild,
-                                     const uint32_t* __restrict__ nwide_off, int64_t level_base,
-                                     WideNode* __restrict__ nodes, int32_t* __restrict__ next_bin,
-                                     int32_t* __restrict__ next_node) {
-  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nwork) return;
-  const int nm1 = (int)(n - 1);
-  const int b = work_bin[k];
-  const float4 plo = box_lo[b], phi = box_hi[b];
-  WideNode nd;
-  nd.ox = plo.x; nd.oy = plo.y; nd.oz = plo.z;
-  const uint32_t ex = scale_exponent(phi.x - plo.x);
-  const uint32_t ey = scale_exponent(phi.y - plo.y);
-  const uint32_t ez = scale_exponent(phi.z - plo.z);
-  const float sx = __uint_as_float(ex << 23), sy = __uint_as_float(ey << 23), sz = __uint_as_float(ez << 23);
-  const int cnt = nchild[k];
-  nd.meta = ex | (ey << 8) | (ez << 16) | ((uint32_t)cnt << 24);
-  for (int a = 0; a < 6; ++a) nd.q[a] = 0;
-  nd.pad[0] = (uint32_t)b;
-  nd.pad[1] = 0;
-  uint32_t m = nwide_off[k];
-  for (int j = 0; j < 4; ++j) {
-    if (j >= cnt) {
-      // empty slot: inverted box (lo = 255, hi = 0) never passes a test
-      nd.q[0] |= 255u << (8 * j); nd.q[1] |= 255u << (8 * j); nd.q[2] |= 255u << (8 * j);
-      nd.ref[j] = 0xffffffffu;
-      continue;
-    }
-    const int cj = child_bin[4 * k + j];
-    const float4 lo = box_lo[cj], hi = box_hi[cj];
-    uint32_t a0, a1;
-    quantize_axis(nd.ox, sx, lo.x, hi.x, a0, a1); nd.q[0] |= a0 << (8 * j); nd.q[3] |= a1 << (8 * j);
-    quantize_axis(nd.oy, sy, lo.y, hi.y, a0, a1); nd.q[1] |= a0 << (8 * j); nd.q[4] |= a1 << (8 * j);
-    quantize_axis(nd.oz, sz, lo.z, hi.z, a0, a1); nd.q[2] |= a0 << (8 * j); nd.q[5] |= a1 << (8 * j);
-    if (child_leaf[4 * k + j]) {
-      const uint32_t f0 = cj >= nm1 ? (uint32_t)(cj - nm1) : (uint32_t)first[cj];
-      const uint32_t c0 = cj >= nm1 ? 1u : (uint32_t)(last[cj] - first[cj] + 1);
-      nd.ref[j] = make_leaf_ref(f0, c0);
+// 6. one collapse level: each worklist entry becomes a wide node at the slot
+// of its binary node; its internal children (binary node indices, which are
+// also their slots) form the next level's worklist
+__global__ void __launch_bounds__(kThreads)
+    collapse_level_kernel(int level, uint32_t* __restrict__ counters, const int32_t* __restrict__ cur,
+                          int32_t* __restrict__ nxt, int64_t n, int leaf_max, const int32_t* __restrict__ left,
+                          const int32_t* __restrict__ right, const int32_t* __restrict__ first,
+                          const int32_t* __restrict__ last, const float4* __restrict__ box_lo,
+                          const float4* __restrict__ box_hi, WideNode* __restrict__ tmp, uint32_t* __restrict__ lvl) {
+  const uint32_t cnt = counters[level];
+  const int nn = (int)n;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += (int64_t)gridDim.x * blockDim.x) {
+    const int b = cur[k];
+    int c[4];
+    int nc;
+    if (b >= nn) {  // a lone leaf as root (single-triangle mesh)
+      c[0] = b;
+      nc = 1;
     } else {
-      const int64_t idx = level_base + m;
-      nd.ref[j] = (uint32_t)idx;
-      next_bin[m] = cj;
-      next_node[m] = (int32_t)idx;
-      ++m;
+      c[0] = left[b];
+      c[1] = right[b];
+      nc = 2;
+      while (nc < 4) {
+        int best = -1;
+        float best_a = -1.f;
+        for (int j = 0; j < nc; ++j) {
+          if (c[j] < nn) {
+            const float a = half_area(box_lo[c[j]], box_hi[c[j]]);
+            if (a > best_a) { best_a = a; best = j; }
+          }
+        }
+        if (best < 0) break;
+        const int x = c[best];
+        for (int j = nc; j > best + 1; --j) c[j] = c[j - 1];
+        c[best] = left[x];
+        c[best + 1] = right[x];
+        ++nc;
+      }
     }
+    const float4 plo = box_lo[b], phi = box_hi[b];
+    WideNode nd;
+    nd.ox = plo.x; nd.oy = plo.y; nd.oz = plo.z;
+    const uint32_t ex = scale_exponent(phi.x - plo.x);
+    const uint32_t ey = scale_exponent(phi.y - plo.y);
+    const uint32_t ez = scale_exponent(phi.z - plo.z);
+    const float sx = __uint_as_float(ex << 23), sy = __uint_as_float(ey << 23), sz = __uint_as_float(ez << 23);
+    nd.meta = ex | (ey << 8) | (ez << 16) | ((uint32_t)nc << 24);
+    for (int a = 0; a < 6; ++a) nd.q[a] = 0;
+    const int slot = b < nn ? b : b - nn;
+    nd.pad[0] = (uint32_t)slot;
+    nd.pad[1] = 0;
+    for (int j = 0; j < 4; ++j) {
+      if (j >= nc) {
+        // empty slot: inverted box (lo = 255, hi = 0) never passes a test
+        nd.q[0] |= 255u << (8 * j); nd.q[1] |= 255u << (8 * j); nd.q[2] |= 255u << (8 * j);
+        nd.ref[j] = 0xffffffffu;
+        continue;
+      }
+      const int cj = c[j];
+      const float4 lo = box_lo[cj], hi = box_hi[cj];
+      uint32_t a0, a1;
+      quantize_axis(nd.ox, sx, lo.x, hi.x, a0, a1); nd.q[0] |= a0 << (8 * j); nd.q[3] |= a1 << (8 * j);
+      quantize_axis(nd.oy, sy, lo.y, hi.y, a0, a1); nd.q[1] |= a0 << (8 * j); nd.q[4] |= a1 << (8 * j);
+      quantize_axis(nd.oz, sz, lo.z, hi.z, a0, a1); nd.q[2] |= a0 << (8 * j); nd.q[5] |= a1 << (8 * j);
+      const int count = cj >= nn ? 1 : last[cj] - first[cj] + 1;
+      if (count <= leaf_max) {
+        const uint32_t f0 = cj >= nn ? (uint32_t)(cj - nn) : (uint32_t)first[cj];
+        nd.ref[j] = make_leaf_ref(f0, (uint32_t)count);
+      } else {
+        nd.ref[j] = (uint32_t)cj;  // slot; renumbered by the layout pass
+        const uint32_t at = atomicAdd(&counters[level + 1], 1u);
+        if (level + 1 < kMaxLevels) nxt[at] = cj;
+      }
+    }
+    tmp[slot] = nd;
+    lvl[slot] = (uint32_t)level;
   }
-  nodes[work_node[k]] = nd;
 }
 
-// 7. triangle records in leaf (sorted) order
-__global__ void write_tris_kernel(const float* __restrict__ V, const int32_t* __restrict__ F,
-                                  const uint32_t* __restrict__ order, int64_t n, TriRec* __restrict__ tris) {
+__global__ void depth_check_kernel(const uint32_t* counters, int32_t* err) {
+  if (threadIdx.x == 0 && counters[kMaxLevels] != 0u) err[1] = 1;
+}
+
+// 7a. final index of each wide node
+__global__ void layout_index_kernel(const uint32_t* __restrict__ sorted_lvl, const uint32_t* __restrict__ sorted_slot,
+                                    int64_t n, uint32_t* __restrict__ newidx) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  if ((sorted_lvl[r] & 0xffu) != kNoLevel) newidx[sorted_slot[r]] = (uint32_t)r;
+}
+
+// 7b. copy in the final order with child references renumbered
+__global__ void layout_copy_kernel(const uint32_t* __restrict__ sorted_lvl, const uint32_t* __restrict__ sorted_slot,
+                                   int64_t n, const uint32_t* __restrict__ newidx, const WideNode* __restrict__ tmp,
+                                   WideNode* __restrict__ out) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  if ((sorted_lvl[r] & 0xffu) == kNoLevel) return;
+  WideNode nd = tmp[sorted_slot[r]];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const uint32_t ref = nd.ref[j];
+    if (ref != 0xffffffffu && !ref_is_leaf(ref)) nd.ref[j] = newidx[ref];
+  }
+  out[r] = nd;
+}
+
+// 7c. mesh roots, mesh bounds, node count
+__global__ void finish_kernel(const int64_t* __restrict__ face_off, int nmesh, const uint32_t* __restrict__ counters,
+                              const uint32_t* __restrict__ newidx, const uint32_t* __restrict__ bounds,
+                              uint32_t* __restrict__ roots, float* __restrict__ bounds_out,
+                              int64_t* __restrict__ num_nodes) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0 && num_nodes) {
+    int64_t total = 0;
+    for (int l = 0; l < kMaxLevels; ++l) total += counters[l];
+    *num_nodes = total;
+  }
+  if (t >= nmesh) return;
+  if (roots) roots[t] = newidx[face_off[t]];
+  if (bounds_out) {
+    for (int k = 0; k < 6; ++k) bounds_out[6 * t + k] = float_unflip(bounds[12 * t + k]);
+  }
+}
+
+// 8. triangle records in leaf (sorted) order; the face id stored is the
+// mesh-local one
+__global__ void write_tris_kernel(const float* __restrict__ V, const int64_t* __restrict__ vert_off,
+                                  const int32_t* __restrict__ F, const int64_t* __restrict__ face_off,
+                                  const uint32_t* __restrict__ mesh_of, const uint32_t* __restrict__ order, int64_t n,
+                                  TriRec* __restrict__ tris) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const uint32_t f = order[j];
-  const int32_t i0 = F[3 * f], i1 = F[3 * f + 1], i2 = F[3 * f + 2];
-  const float3 a = ld3(V, i0), b = ld3(V, i1), c = ld3(V, i2);
+  const uint32_t m = mesh_of[f];
+  const int64_t vb = vert_off[m], nv = vert_off[m + 1] - vb;
+  int32_t i0 = F[3 * (int64_t)f], i1 = F[3 * (int64_t)f + 1], i2 = F[3 * (int64_t)f + 2];
+  if (i0 < 0 || i1 < 0 || i2 < 0 || i0 >= nv || i1 >= nv || i2 >= nv) i0 = i1 = i2 = 0;  // reported by tri_prep
+  const float3 a = ld3(V, vb + i0), b = ld3(V, vb + i1), c = ld3(V, vb + i2);
   // near-degenerate test in FP64: |n|^2 tiny in absolute terms (the
   // reference's 1e-12 cut) or relative to the longest edge (slivers)
   const double e0x = (double)b.x - a.x, e0y = (double)b.y - a.y, e0z = (double)b.z - a.z;
@@ -414,12 +519,84 @@ __global__ void write_tris_kernel(const float* __restrict__ V, const int32_t* __
   const float e0 = v21x * v21x + v21y * v21y + v21z * v21z;
   const float e1 = v32x * v32x + v32y * v32y + v32z * v32z;
   const float e2 = v13x * v13x + v13y * v13y + v13z * v13z;
+  const int local = (int)((int64_t)f - face_off[m]);
   TriRec r;
-  r.a = make_float4(a.x, a.y, a.z, __int_as_float((int)f));
+  r.a = make_float4(a.x, a.y, a.z, __int_as_float(local));
   r.b = make_float4(b.x, b.y, b.z, __uint_as_float(flags));
   r.c = make_float4(c.x, c.y, c.z, nsqf > 0.f ? 1.0f / nsqf : 0.f);
   r.r = make_float4(1.0f / fmaxf(e0, 1e-12f), 1.0f / fmaxf(e1, 1e-12f), 1.0f / fmaxf(e2, 1e-12f), 0.f);
   tris[j] = r;
+}
+
+int mesh_bits_of(int nmesh) {
+  int mbits = 0;
+  while ((1ll << mbits) < nmesh) ++mbits;
+  return mbits;
+}
+
+// The whole build, launches only.  Offsets are device arrays [nmesh + 1].
+int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, const int64_t* face_off, int nmesh,
+                   int64_t n, int leaf_max, WideNode* nodes_out, TriRec* tris_out, uint32_t* roots_out,
+                   float* bounds_out, int64_t* num_nodes_out, int32_t* status_out, BuildWs& w, cudaStream_t s) {
+  const int mbits = mesh_bits_of(nmesh);
+  const int bits = (64 - mbits) / 3 < 21 ? (64 - mbits) / 3 : 21;
+  const int64_t init_threads = 12ll * nmesh > kMaxLevels + 1 ? 12ll * nmesh : kMaxLevels + 1;
+  init_kernel<<<(unsigned)ceil_div(init_threads, kThreads), kThreads, 0, s>>>(face_off, nmesh, n, w.bounds, w.err,
+                                                                              w.counters, w.work_a);
+  A3D_LAUNCH_CHECK();
+  const unsigned g = (unsigned)ceil_div(n, kThreads);
+  tri_prep_kernel<<<g, kThreads, 0, s>>>(V, vert_off, F, face_off, nmesh, n, w.tri_lo, w.tri_hi, w.centroid,
+                                         w.mesh_of, w.bounds, w.err);
+  A3D_LAUNCH_CHECK();
+  morton_kernel<<<g, kThreads, 0, s>>>(w.centroid, w.mesh_of, n, w.bounds, bits, w.keys, w.vals);
+  A3D_LAUNCH_CHECK();
+  bool alt = false;
+  A3D_TRY(radix_sort_pairs<uint64_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, n, 0, 3 * bits + mbits, w.rs_scratch,
+                                     &alt, s));
+  const uint64_t* keys = alt ? w.keys_alt : w.keys;
+  const uint32_t* order = alt ? w.vals_alt : w.vals;
+
+  radix_tree_kernel<<<g, kThreads, 0, s>>>(keys, face_off, nmesh, n, w.left, w.right, w.parent, w.first, w.last);
+  A3D_LAUNCH_CHECK();
+  A3D_CUDA_TRY(cudaMemsetAsync(w.visit, 0, sizeof(uint32_t) * n, s));
+  refit_kernel<<<g, kThreads, 0, s>>>(order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.box_lo, w.box_hi,
+                                      w.visit);
+  A3D_LAUNCH_CHECK();
+  write_tris_kernel<<<g, kThreads, 0, s>>>(V, vert_off, F, face_off, w.mesh_of, order, n, tris_out);
+  A3D_LAUNCH_CHECK();
+
+  // collapse: a fixed number of level launches (empty levels return at once)
+  A3D_CUDA_TRY(cudaMemsetAsync(w.lvl, 0xff, sizeof(uint32_t) * n, s));
+  const int64_t lb = ceil_div(n, kThreads) < kLevelBlocks ? ceil_div(n, kThreads) : kLevelBlocks;
+  int32_t *cur = w.work_a, *nxt = w.work_b;
+  for (int level = 0; level < kMaxLevels; ++level) {
+    collapse_level_kernel<<<(unsigned)lb, kThreads, 0, s>>>(level, w.counters, cur, nxt, n, leaf_max, w.left,
+                                                            w.right, w.first, w.last, w.box_lo, w.box_hi,
+                                                            w.tmp_nodes, w.lvl);
+    A3D_LAUNCH_CHECK();
+    int32_t* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  depth_check_kernel<<<1, 32, 0, s>>>(w.counters, w.err);
+  A3D_LAUNCH_CHECK();
+  // breadth-first layout: stable sort of the slots by level
+  iota_u32_kernel<<<g, kThreads, 0, s>>>(w.slot, n);
+  A3D_LAUNCH_CHECK();
+  bool lalt = false;
+  A3D_TRY(radix_sort_pairs<uint32_t>(w.lvl, w.slot, w.lvl_alt, w.slot_alt, n, 0, 8, w.rs_scratch, &lalt, s));
+  const uint32_t* slvl = lalt ? w.lvl_alt : w.lvl;
+  const uint32_t* sslot = lalt ? w.slot_alt : w.slot;
+  layout_index_kernel<<<g, kThreads, 0, s>>>(slvl, sslot, n, w.newidx);
+  A3D_LAUNCH_CHECK();
+  layout_copy_kernel<<<g, kThreads, 0, s>>>(slvl, sslot, n, w.newidx, w.tmp_nodes, nodes_out);
+  A3D_LAUNCH_CHECK();
+  finish_kernel<<<(unsigned)ceil_div(nmesh, kThreads), kThreads, 0, s>>>(face_off, nmesh, w.counters, w.newidx,
+                                                                         w.bounds, roots_out, bounds_out,
+                                                                         num_nodes_out);
+  A3D_LAUNCH_CHECK();
+  if (status_out) A3D_CUDA_TRY(cudaMemcpyAsync(status_out, w.err, 2 * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+  return A3D_OK;
 }
 
 }  // namespace
@@ -431,7 +608,7 @@ using namespace a3d;
 extern "C" size_t a3d_bvh_build_workspace_bytes(int64_t num_faces) {
   Workspace ws(nullptr, 0);
   BuildWs w;
-  return carve(w, ws, num_faces > 0 ? num_faces : 1) + 256;
+  return carve(w, ws, num_faces > 0 ? num_faces : 1, 1) + 256;
 }
 
 extern "C" int a3d_bvh_build(const float* vertices, int64_t num_vertices, const int32_t* faces, int64_t num_faces,
@@ -445,78 +622,64 @@ extern "C" int a3d_bvh_build(const float* vertices, int64_t num_vertices, const 
               "bvh_build: null pointer");
   A3D_REQUIRE(((uintptr_t)nodes_out & 63) == 0 && ((uintptr_t)tris_out & 15) == 0, A3D_ERR_ARGUMENT,
               "bvh_build: nodes must be 64-B and triangles 16-B aligned");
-  A3D_REQUIRE(node_capacity >= 1, A3D_ERR_WORKSPACE, "bvh_build: node capacity");
   const int64_t n = num_faces;
+  A3D_REQUIRE(node_capacity >= n, A3D_ERR_WORKSPACE, "bvh_build: node capacity must be at least num_faces");
   Workspace ws(workspace, workspace_bytes);
   BuildWs w;
-  carve(w, ws, n);
+  carve(w, ws, n, 1);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "bvh_build: workspace too small");
   if (leaf_max == 0) leaf_max = 4;
   A3D_REQUIRE(leaf_max >= 1 && leaf_max <= kMaxLeafTris, A3D_ERR_ARGUMENT, "bvh_build: leaf_max must be in 1..8");
-
-  init_bounds_kernel<<<1, 32, 0, s>>>(w.bounds, w.err);
+  single_offsets_kernel<<<1, 32, 0, s>>>(w.face_off, w.vert_off, n, num_vertices);
   A3D_LAUNCH_CHECK();
-  const unsigned g = (unsigned)ceil_div(n, kThreads);
-  tri_prep_kernel<<<g, kThreads, 0, s>>>(vertices, num_vertices, faces, n, w.tri_lo, w.tri_hi, w.centroid, w.bounds,
-                                         w.err);
-  A3D_LAUNCH_CHECK();
-  morton_kernel<<<g, kThreads, 0, s>>>(w.centroid, n, w.bounds, w.keys, w.vals);
-  A3D_LAUNCH_CHECK();
-  bool alt = false;
-  A3D_TRY(radix_sort_pairs<uint64_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, n, 0, 64, w.rs_scratch, &alt, s));
-  const uint64_t* keys = alt ? w.keys_alt : w.keys;
-  const uint32_t* order = alt ? w.vals_alt : w.vals;
-
-  if (n > 1) {
-    radix_tree_kernel<<<(unsigned)ceil_div(n - 1, kThreads), kThreads, 0, s>>>(keys, n, w.left, w.right, w.parent,
-                                                                              w.first, w.last);
-    A3D_LAUNCH_CHECK();
-    A3D_CUDA_TRY(cudaMemsetAsync(w.visit, 0, sizeof(uint32_t) * (n - 1), s));
-  }
-  refit_kernel<<<g, kThreads, 0, s>>>(order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.box_lo, w.box_hi,
-                                      w.visit);
-  A3D_LAUNCH_CHECK();
-  write_tris_kernel<<<g, kThreads, 0, s>>>(vertices, faces, order, n, (TriRec*)tris_out);
-  A3D_LAUNCH_CHECK();
-
-  // level-synchronous collapse
-  int32_t root_bin = 0;  // internal root, or the single leaf when n == 1 (index n-1 == 0)
-  A3D_CUDA_TRY(cudaMemcpyAsync(w.work_a_bin, &root_bin, sizeof(int32_t), cudaMemcpyHostToDevice, s));
-  A3D_CUDA_TRY(cudaMemsetAsync(w.work_a_node, 0, sizeof(int32_t), s));
-  int64_t nwork = 1, level_base = 1;
-  int32_t *cur_bin = w.work_a_bin, *cur_node = w.work_a_node, *nxt_bin = w.work_b_bin, *nxt_node = w.work_b_node;
-  while (nwork > 0) {
-    const unsigned gw = (unsigned)ceil_div(nwork, kThreads);
-    collapse_select_kernel<<<gw, kThreads, 0, s>>>(cur_bin, nwork, n, leaf_max, w.left, w.right, w.first, w.last,
-                                                   w.box_lo, w.box_hi, w.child_bin, w.child_leaf, w.nchild, w.nwide);
-    A3D_LAUNCH_CHECK();
-    A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.nwide, w.nwide_off, nwork, w.scan_tmp, w.total, s)));
-    uint32_t total = 0;
-    A3D_CUDA_TRY(cudaMemcpyAsync(&total, w.total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    A3D_CUDA_TRY(cudaStreamSynchronize(s));
-    A3D_REQUIRE(level_base + (int64_t)total <= node_capacity, A3D_ERR_WORKSPACE, "bvh_build: node capacity exceeded");
-    collapse_emit_kernel<<<gw, kThreads, 0, s>>>(cur_bin, cur_node, nwork, n, w.first, w.last, w.box_lo, w.box_hi,
-                                                 w.child_bin, w.child_leaf, w.nchild, w.nwide_off, level_base,
-                                                 (WideNode*)nodes_out, nxt_bin, nxt_node);
-    A3D_LAUNCH_CHECK();
-    level_base += total;
-    nwork = total;
-    int32_t* t0 = cur_bin; cur_bin = nxt_bin; nxt_bin = t0;
-    int32_t* t1 = cur_node; cur_node = nxt_node; nxt_node = t1;
-  }
+  A3D_TRY(build_wide_bvh(vertices, w.vert_off, faces, w.face_off, 1, n, leaf_max, (WideNode*)nodes_out,
+                         (TriRec*)tris_out, nullptr, nullptr, w.count, nullptr, w, s));
   uint32_t hb[12];
   int32_t herr[4];
+  int64_t count = 0;
   A3D_CUDA_TRY(cudaMemcpyAsync(hb, w.bounds, sizeof(hb), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaMemcpyAsync(herr, w.err, sizeof(herr), cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaMemcpyAsync(&count, w.count, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
   A3D_REQUIRE(herr[0] == 0, A3D_ERR_ARGUMENT, "bvh_build: face index out of range");
+  A3D_REQUIRE(herr[1] == 0, A3D_ERR_OVERFLOW, "bvh_build: tree deeper than the collapse's level limit");
   if (bounds_out) {
     for (int k = 0; k < 6; ++k) {
-      uint32_t u = hb[k];
-      uint32_t f = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+      const uint32_t u = hb[k];
+      const uint32_t f = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
       memcpy(&bounds_out[k], &f, 4);
     }
   }
-  *num_nodes_out = level_base;
+  *num_nodes_out = count;
   return A3D_OK;
+}
+
+extern "C" size_t a3d_batch_build_workspace_bytes(int64_t num_faces, int32_t num_meshes) {
+  Workspace ws(nullptr, 0);
+  BuildWs w;
+  return carve(w, ws, num_faces > 0 ? num_faces : 1, num_meshes > 0 ? num_meshes : 1) + 256;
+}
+
+extern "C" int a3d_batch_build(const float* vertices, const int64_t* vertex_offsets, const int32_t* faces,
+                               const int64_t* face_offsets, int32_t num_meshes, int64_t num_faces, int leaf_max,
+                               void* nodes_out, void* tris_out, uint32_t* roots_out, float* bounds_out,
+                               int64_t* num_nodes_out, int32_t* status_out, void* workspace, size_t workspace_bytes,
+                               a3d_stream_t stream_) {
+  cudaStream_t s = (cudaStream_t)stream_;
+  A3D_REQUIRE(num_meshes > 0 && num_faces >= num_meshes, A3D_ERR_ARGUMENT,
+              "batch_build: needs at least one face per mesh");
+  A3D_REQUIRE(num_faces < (1ll << 28), A3D_ERR_ARGUMENT, "batch_build: more than 2^28 faces in the batch");
+  A3D_REQUIRE(vertices && vertex_offsets && faces && face_offsets && nodes_out && tris_out && roots_out,
+              A3D_ERR_ARGUMENT, "batch_build: null pointer");
+  A3D_REQUIRE(((uintptr_t)nodes_out & 63) == 0 && ((uintptr_t)tris_out & 15) == 0, A3D_ERR_ARGUMENT,
+              "batch_build: nodes must be 64-B and triangles 16-B aligned");
+  if (leaf_max == 0) leaf_max = 4;
+  A3D_REQUIRE(leaf_max >= 1 && leaf_max <= kMaxLeafTris, A3D_ERR_ARGUMENT, "batch_build: leaf_max must be in 1..8");
+  Workspace ws(workspace, workspace_bytes);
+  BuildWs w;
+  carve(w, ws, num_faces, num_meshes);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "batch_build: workspace too small");
+  return build_wide_bvh(vertices, vertex_offsets, faces, face_offsets, num_meshes, num_faces, leaf_max,
+                        (WideNode*)nodes_out, (TriRec*)tris_out, roots_out, bounds_out, num_nodes_out, status_out, w,
+                        s);
 }

@@ -49,6 +49,27 @@ struct Counters {
   unsigned long long tris;
 };
 
+// Which tree a query walks.  One mesh: the root is node 0.  A batch: query
+// qi (index qbase + qi in the caller's array) belongs to mesh m with
+// qoff[m] <= qbase + qi < qoff[m+1], whose root is roots[m].
+struct MeshSel {
+  const int64_t* qoff;
+  const uint32_t* roots;
+  int nmesh;
+  int64_t qbase;
+  __device__ __forceinline__ uint32_t root_of(int64_t qi) const {
+    if (qoff == nullptr) return 0u;
+    const int64_t g = qbase + qi;
+    int lo = 0, hi = nmesh - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(qoff + mid) <= g) lo = mid;
+      else hi = mid - 1;
+    }
+    return __ldg(roots + lo);
+  }
+};
+
 // children are visited in ascending (distance, ref) order: a total order, so
 // every traversal variant (single lane, quad of lanes) walks the same
 // sequence and breaks distance ties identically
@@ -97,6 +118,35 @@ __device__ __forceinline__ TriRec load_tri(const TriRec* tris, uint32_t i) {
   return r;
 }
 
+// The arrays a traversal reads.  With kGuard (batches, whose node count is
+// only known on the device) a node or triangle index outside the arrays is
+// recorded in *fault (kFaultNode / kFaultTri) and replaced by 0, so no
+// access leaves them whatever the tree holds.
+constexpr uint32_t kFaultNode = 1u, kFaultTri = 2u;
+
+template <bool kGuard>
+struct TreeT {
+  const WideNode* __restrict__ nodes;
+  const TriRec* __restrict__ tris;
+  uint32_t num_nodes;
+  uint32_t num_tris;
+  uint32_t* fault;
+  __device__ __forceinline__ const int4* node(uint32_t ref) const {
+    if (kGuard && ref >= num_nodes) {
+      atomicOr(fault, kFaultNode);
+      ref = 0;
+    }
+    return reinterpret_cast<const int4*>(nodes + ref);
+  }
+  __device__ __forceinline__ TriRec tri(uint32_t i) const {
+    if (kGuard && i >= num_tris) {
+      atomicOr(fault, kFaultTri);
+      i = 0;
+    }
+    return load_tri(tris, i);
+  }
+};
+
 // Stack in shared memory, [depth][blockDim] layout.
 struct SharedStack {
   uint2* base;  // points at s[0][threadIdx.x]
@@ -122,17 +172,16 @@ struct LocalStack {
 
 // Core traversal.  Returns false when the stack would overflow (result then
 // invalid).  best_sq: in = initial pruning radius^2, out = best distance^2.
-template <typename Stack>
-__device__ __forceinline__ bool traverse(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
-                                         float px, float py, float pz, Stack& st, float& best_sq,
-                                         uint32_t& best_tri, Counters& ctr) {
-  uint32_t ref = 0;  // root is internal node 0 (a single-leaf tree still has a root node)
+template <typename Stack, typename Tree>
+__device__ __forceinline__ bool traverse(const Tree& T, float px, float py, float pz, Stack& st, float& best_sq,
+                                         uint32_t& best_tri, Counters& ctr, uint32_t root = 0u) {
+  uint32_t ref = root;  // a root is always an internal node (a single-leaf tree still has one)
   bool have = true;
   for (;;) {
     if (have) {
       if (!ref_is_leaf(ref)) {
         ++ctr.nodes;
-        const int4* np = reinterpret_cast<const int4*>(nodes + ref);
+        const int4* np = T.node(ref);
         const int4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3);
         const float ox = __int_as_float(w0.x), oy = __int_as_float(w0.y), oz = __int_as_float(w0.z);
         const uint32_t meta = (uint32_t)w0.w;
@@ -173,7 +222,7 @@ __device__ __forceinline__ bool traverse(const WideNode* __restrict__ nodes, con
       } else {
         const uint32_t f0 = leaf_first(ref), cnt = leaf_count(ref);
         for (uint32_t i = 0; i < cnt; ++i) {
-          const TriRec t = load_tri(tris, f0 + i);
+          const TriRec t = T.tri(f0 + i);
           ++ctr.tris;
           const float dsq = tri_dist_sq(t, px, py, pz);
           if (dsq < best_sq) {
@@ -197,7 +246,8 @@ __device__ __forceinline__ bool traverse(const WideNode* __restrict__ nodes, con
   }
 }
 
-__device__ __noinline__ void finish_query(const TriRec* __restrict__ tris, uint32_t best_tri, float best_sq,
+__device__ __noinline__ void finish_query(const TriRec* __restrict__ tris, uint32_t num_tris, uint32_t best_tri,
+                                          float best_sq,
                                              float px, float py, float pz, int64_t qi, const QueryOut& out,
                                              const SignArgs& sg, bool do_sign) {
   float cx = px, cy = py, cz = pz;
@@ -205,7 +255,7 @@ __device__ __noinline__ void finish_query(const TriRec* __restrict__ tris, uint3
   float u = 0.f, v = 0.f, w = 0.f;
   float dist = sqrtf(best_sq);
   if (best_tri != 0xffffffffu) {
-    const TriRec t = load_tri(tris, best_tri);
+    const TriRec t = load_tri(tris, best_tri < num_tris ? best_tri : 0u);
     face = __float_as_int(t.a.w);
     const V3<float> a = mk(t.a.x, t.a.y, t.a.z), b = mk(t.b.x, t.b.y, t.b.z), c = mk(t.c.x, t.c.y, t.c.z);
     const V3<float> p = mk(px, py, pz);
@@ -276,12 +326,13 @@ __device__ __forceinline__ void flush_counters(const Counters& c, unsigned long 
 // Greedy root-to-leaf probe: follows the nearest child and tests that
 // leaf's triangles.  Gives a real triangle (and its distance) that seeds the
 // pruning radius of the full traversal.
-__device__ __forceinline__ void probe(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris, float px,
-                                     float py, float pz, uint32_t& tri, float& dsq, Counters& ctr) {
-  uint32_t ref = 0;
+template <typename Tree>
+__device__ __forceinline__ void probe(const Tree& T, float px, float py, float pz, uint32_t& tri, float& dsq,
+                                     Counters& ctr, uint32_t root = 0u) {
+  uint32_t ref = root;
   while (!ref_is_leaf(ref)) {
     ++ctr.nodes;
-    const int4* np = reinterpret_cast<const int4*>(nodes + ref);
+    const int4* np = T.node(ref);
     const int4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3);
     const float ox = __int_as_float(w0.x), oy = __int_as_float(w0.y), oz = __int_as_float(w0.z);
     const uint32_t meta = (uint32_t)w0.w;
@@ -310,7 +361,7 @@ __device__ __forceinline__ void probe(const WideNode* __restrict__ nodes, const 
   tri = f0;
   for (uint32_t i = 0; i < cnt; ++i) {
     ++ctr.tris;
-    const float d = tri_dist_sq(load_tri(tris, f0 + i), px, py, pz);
+    const float d = tri_dist_sq(T.tri(f0 + i), px, py, pz);
     if (d < dsq) { dsq = d; tri = f0 + i; }
   }
 }
@@ -325,7 +376,7 @@ __device__ __forceinline__ void probe(const WideNode* __restrict__ nodes, const 
 // further; if it excludes every triangle the query is re-run unbounded.
 template <bool kSign, bool kStats>
 __global__ void __launch_bounds__(kUdfThreads)
-    udf_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris, const float* __restrict__ pts,
+    udf_kernel(TreeT<false> T, const float* __restrict__ pts,
                int64_t n, int chunk, const uint32_t* __restrict__ perm, const float* __restrict__ bound,
                QueryOut out, SignArgs sg, unsigned long long* stats, uint32_t* __restrict__ rerun,
                uint32_t* __restrict__ nrerun) {
@@ -349,9 +400,9 @@ __global__ void __launch_bounds__(kUdfThreads)
     if (prev != 0xffffffffu) {
       seed_tri = prev;
       ++ctr.tris;
-      seed_sq = tri_dist_sq(load_tri(tris, prev), px, py, pz);
+      seed_sq = tri_dist_sq(T.tri(prev), px, py, pz);
     } else {
-      probe(nodes, tris, px, py, pz, seed_tri, seed_sq, ctr);
+      probe(T, px, py, pz, seed_tri, seed_sq, ctr);
     }
     // strictly above the seed distance so the seed triangle itself qualifies
     float best_sq = seed_sq < INFINITY ? nextafterf(seed_sq, INFINITY) : INFINITY;
@@ -362,14 +413,14 @@ __global__ void __launch_bounds__(kUdfThreads)
     }
     uint32_t best_tri = 0xffffffffu;
     SharedStack st{s_stack + threadIdx.x, 0};
-    const bool ok = traverse(nodes, tris, px, py, pz, st, best_sq, best_tri, ctr);
+    const bool ok = traverse(T, px, py, pz, st, best_sq, best_tri, ctr);
     if (!ok || best_tri == 0xffffffffu) {
       // stack overflow, or an external bound excluded every triangle
       const uint32_t slot = atomicAdd(nrerun, 1u);
       rerun[slot] = (uint32_t)qi;
       prev = 0xffffffffu;
     } else {
-      finish_query(tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
+      finish_query(T.tris, T.num_tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
       prev = best_tri;
     }
     k = w0 + (int64_t)atomicAdd(&s_next[warp], 1u);
@@ -382,9 +433,10 @@ __global__ void __launch_bounds__(kUdfThreads)
 
 
 
-__device__ __forceinline__ void quad_child_box(const WideNode* __restrict__ nodes, uint32_t ref, int c, float px,
+template <typename Tree>
+__device__ __forceinline__ void quad_child_box(const Tree& T, uint32_t ref, int c, float px,
                                                float py, float pz, float& d, uint32_t& r) {
-  const int4* np = reinterpret_cast<const int4*>(nodes + ref);
+  const int4* np = T.node(ref);
   const int4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3);
   const uint32_t meta = (uint32_t)w0.w;
   const int nch = (int)(meta >> 24);
@@ -421,6 +473,9 @@ constexpr int kSpillCap = 96;    // per-owner global overflow stack (entries)
 constexpr int kSpillChunk = 16;  // entries moved per spill / refill
 constexpr int kTaskTriCap = 32 * kMaxLeafTris;
 constexpr int kTaskPool = 64;  // queries per pool taken from the global counter
+// 64-thread blocks with 24 KB of shared memory: at <= 112 registers a thread,
+// 9 blocks (18 warps) stay resident per SM
+constexpr int kTaskMaxRegs = 112;
 
 struct TaskSmem {
   uint2 stack[kTaskDepth][32];
@@ -438,13 +493,12 @@ enum : int { kIdle = 0, kProbe = 1, kSeed = 2, kTrav = 3, kAbandon = 4 };
 // radius seeding of the task kernel
 enum : uint32_t { kSeedReuse = 1u, kSeedBoundOnly = 2u };
 
-template <bool kSign, bool kStats>
-__global__ void __launch_bounds__(kTaskWarps * 32)
-    udf_task_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
-                    const float* __restrict__ pts, int64_t n, const uint32_t* __restrict__ perm,
+template <bool kSign, bool kStats, bool kBatch>
+__global__ void __maxnreg__(kTaskMaxRegs)
+    udf_task_kernel(TreeT<kBatch> T, const float* __restrict__ pts, int64_t n, const uint32_t* __restrict__ perm,
                     const float* __restrict__ bound, QueryOut out, SignArgs sg, unsigned long long* stats,
                     uint32_t* __restrict__ rerun, uint32_t* __restrict__ nrerun, uint32_t* __restrict__ pool_counter,
-                    uint2* __restrict__ spill, int64_t spill_owners, uint32_t seeding) {
+                    uint2* __restrict__ spill, int64_t spill_owners, uint32_t seeding, MeshSel sel, int pool) {
   __shared__ TaskSmem smem[kTaskWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   TaskSmem& S = smem[warp];
@@ -460,7 +514,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
   // owner state
   int64_t qi = -1, kprev = -(1ll << 40);
   int phase = kIdle;
-  uint32_t ref = 0, prev = 0xffffffffu, best_tri = 0xffffffffu;
+  uint32_t ref = 0, prev = 0xffffffffu, best_tri = 0xffffffffu, root = 0u, prev_root = 0u;
   float best_sq = INFINITY, px = 0.f, py = 0.f, pz = 0.f, bsq = INFINITY;
   bool have = false;
   int sp = 0;
@@ -473,6 +527,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
 
   auto start = [&](int64_t k) {
     qi = perm ? (int64_t)perm[k] : k;
+    root = kBatch ? sel.root_of(qi) : 0u;
     px = pts[3 * qi]; py = pts[3 * qi + 1]; pz = pts[3 * qi + 2];
     S.px[lane] = px; S.py[lane] = py; S.pz[lane] = pz;
     bsq = INFINITY;
@@ -490,17 +545,19 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
     if ((seeding & kSeedBoundOnly) && bsq < INFINITY) {
       best_sq = bsq;
       phase = kTrav;
-      ref = 0;
+      ref = root;
       have = true;
-    } else if ((seeding & kSeedReuse) && prev != 0xffffffffu && k - kprev <= 64 && k > kprev) {
+    } else if ((seeding & kSeedReuse) && prev != 0xffffffffu && (!kBatch || root == prev_root) &&
+               k - kprev <= 64 && k > kprev) {
       phase = kSeed;
     } else {
       prev = 0xffffffffu;
       phase = kProbe;
-      ref = 0;
+      ref = root;
       have = true;
     }
     kprev = k;
+    if (kBatch) prev_root = root;
   };
 
   // hands new queries to the lanes in `want` (warp-uniform bookkeeping)
@@ -511,8 +568,9 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
         uint32_t p = 0;
         if (lane == 0) p = atomicAdd(pool_counter, 1u);
         p = __shfl_sync(FULL, p, 0);
-        pos = (int64_t)p * kTaskPool;
-        end = pos + kTaskPool < n ? pos + kTaskPool : n;
+        const int psize = kBatch ? pool : kTaskPool;
+        pos = (int64_t)p * psize;
+        end = pos + psize < n ? pos + psize : n;
         if (pos >= n) { exhausted = true; break; }
       }
       const int64_t avail = end - pos;
@@ -553,7 +611,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
         rerun[atomicAdd(nrerun, 1u)] = (uint32_t)qi;
         prev = 0xffffffffu;
       } else {
-        finish_query(tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
+        finish_query(T.tris, T.num_tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
         prev = best_tri;
       }
       phase = kIdle;
@@ -595,13 +653,13 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
       const int o = S.nown[r];
       float d;
       uint32_t cr;
-      quad_child_box(nodes, S.nref[r], c, S.px[o], S.py[o], S.pz[o], d, cr);
+      quad_child_box(T, S.nref[r], c, S.px[o], S.py[o], S.pz[o], d, cr);
       S.boxd[t] = d;
       S.boxr[t] = cr;
     }
     for (int t = lane; t < ttotal; t += 32) {
       const int o = S.town[t];
-      S.trid[t] = tri_dist_sq(load_tri(tris, S.tidx[t]), S.px[o], S.py[o], S.pz[o]);
+      S.trid[t] = tri_dist_sq(T.tri(S.tidx[t]), S.px[o], S.py[o], S.pz[o]);
     }
     __syncwarp();
     // (d) owners consume their results
@@ -668,7 +726,7 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
         if (bsq < b) b = bsq;
         best_sq = b;
         phase = kTrav;
-        ref = 0;
+        ref = root;
         have = true;
       }
     }
@@ -681,29 +739,29 @@ __global__ void __launch_bounds__(kTaskWarps * 32)
 }
 
 
-template <bool kSign, bool kStats>
+template <bool kSign, bool kStats, bool kBatch>
 __global__ void __launch_bounds__(64)
-    udf_rerun_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
-                     const float* __restrict__ pts, const uint32_t* __restrict__ rerun,
+    udf_rerun_kernel(TreeT<kBatch> T, const float* __restrict__ pts, const uint32_t* __restrict__ rerun,
                      const uint32_t* __restrict__ nrerun, QueryOut out, SignArgs sg, unsigned long long* stats,
-                     int* __restrict__ overflow) {
+                     uint32_t* __restrict__ overflow, uint32_t* __restrict__ total_reruns, MeshSel sel) {
   const uint32_t m = *nrerun;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && m > 0) atomicAdd(total_reruns, m);
   Counters ctr{0, 0};
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t qi = rerun[t];
     const float px = pts[3 * qi], py = pts[3 * qi + 1], pz = pts[3 * qi + 2];
     uint32_t seed_tri;
     float seed_sq;
-    probe(nodes, tris, px, py, pz, seed_tri, seed_sq, ctr);
+    const uint32_t root = kBatch ? sel.root_of(qi) : 0u;
+    probe(T, px, py, pz, seed_tri, seed_sq, ctr, root);
     float best_sq = seed_sq < INFINITY ? nextafterf(seed_sq, INFINITY) : INFINITY;
     uint32_t best_tri = 0xffffffffu;
     LocalStack st;
     st.sp = 0;
-    if (!traverse(nodes, tris, px, py, pz, st, best_sq, best_tri, ctr)) atomicExch(overflow, 1);
-    finish_query(tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
+    if (!traverse(T, px, py, pz, st, best_sq, best_tri, ctr, root)) atomicExch(overflow, 1u);
+    finish_query(T.tris, T.num_tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
   }
-  if (kStats) {
-    // counters only for threads of full warps; partial warps add directly
+  if (kStats && (ctr.nodes | ctr.tris)) {
     atomicAdd(stats, ctr.nodes);
     atomicAdd(stats + 1, ctr.tris);
   }
@@ -726,6 +784,8 @@ __global__ void query_morton_kernel(const float* __restrict__ pts, int64_t n, fl
   vals[i] = (uint32_t)i;
 }
 
+constexpr int kStatusWords = 8;
+
 struct UdfWs {
   uint32_t* keys;
   uint32_t* keys_alt;
@@ -733,12 +793,15 @@ struct UdfWs {
   uint32_t* vals_alt;
   uint32_t* rs_scratch;
   uint32_t* rerun;
-  uint32_t* nrerun;  // [0] rerun count, [1] overflow flag, [2] pool counter
+  uint32_t* nrerun;  // status words: [0] re-run list length, [1] deep-stack overflow, [2] pool counter,
+                     // [3] guard faults, [4] queries re-run in total
   uint2* spill;      // optional overflow stacks (trailing workspace)
   int64_t spill_owners;
 };
 
 size_t carve_udf(UdfWs& w, Workspace& ws, int64_t n, uint32_t flags) {
+  // status words at the start of the workspace (read by a3d_udf_status)
+  w.nrerun = ws.take<uint32_t>(kStatusWords);
   if (flags & A3D_UDF_SORT_QUERIES) {
     w.keys = ws.take<uint32_t>(n);
     w.keys_alt = ws.take<uint32_t>(n);
@@ -749,7 +812,6 @@ size_t carve_udf(UdfWs& w, Workspace& ws, int64_t n, uint32_t flags) {
     w.keys = w.keys_alt = w.vals = w.vals_alt = w.rs_scratch = nullptr;
   }
   w.rerun = ws.take<uint32_t>(n);
-  w.nrerun = ws.take<uint32_t>(4);
   return ws.used;
 }
 
@@ -760,39 +822,58 @@ int64_t spill_owner_bound(int64_t n) {
   return n + 128 < cap ? n + 128 : cap;
 }
 
-template <bool kSign, bool kStats>
-int launch_udf(const a3d_bvh_view* bvh, const float* pts, int64_t n, const uint32_t* perm, bool coherent,
+// launch shape of the persistent traversal: queries per pool, resident
+// blocks per SM (0 = as many as fit)
+struct TaskShape {
+  int pool;
+  int blocks_per_sm;
+};
+
+template <bool kSign, bool kStats, bool kBatch>
+int task_blocks_per_sm(int* out) {
+  static int cached = 0;
+  if (cached == 0) {
+    int b = 0;
+    A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, udf_task_kernel<kSign, kStats, kBatch>,
+                                                               kTaskWarps * 32, 0));
+    cached = b < 1 ? 1 : b;
+  }
+  *out = cached;
+  return A3D_OK;
+}
+
+template <bool kSign, bool kStats, bool kBatch>
+int launch_udf(const TreeT<kBatch>& T, const float* pts, int64_t n, const uint32_t* perm, bool coherent,
                const float* bound, const QueryOut& out, const SignArgs& sg, unsigned long long* stats, UdfWs& w,
-               uint32_t seeding, cudaStream_t s) {
-  const WideNode* nodes = (const WideNode*)bvh->nodes;
-  const TriRec* tris = (const TriRec*)bvh->tris;
+               uint32_t seeding, const MeshSel& sel, TaskShape shape, cudaStream_t s) {
   if (coherent) {
-    static int blocks_per_sm[2][2] = {{0, 0}, {0, 0}};
-    int& bps = blocks_per_sm[kSign][kStats];
-    if (bps == 0) {
-      A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, udf_task_kernel<kSign, kStats>,
-                                                                 kTaskWarps * 32, 0));
-      if (bps < 1) bps = 1;
-    }
+    int bps = 0;
+    A3D_TRY((task_blocks_per_sm<kSign, kStats, kBatch>(&bps)));
+    if (shape.blocks_per_sm > 0 && shape.blocks_per_sm < bps) bps = shape.blocks_per_sm;
+    const int pool = shape.pool > 0 ? shape.pool : kTaskPool;
     int dev = 0, sms = kNumSMs;
     A3D_CUDA_TRY(cudaGetDevice(&dev));
     A3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int64_t pools = ceil_div(n, kTaskPool);
+    const int64_t pools = ceil_div(n, pool);
     const int64_t want_blocks = ceil_div(pools, kTaskWarps);
     const int64_t grid = want_blocks < (int64_t)sms * bps ? want_blocks : (int64_t)sms * bps;
-    udf_task_kernel<kSign, kStats><<<(unsigned)grid, kTaskWarps * 32, 0, s>>>(
-        nodes, tris, pts, n, perm, bound, out, sg, stats, w.rerun, w.nrerun, w.nrerun + 2, w.spill, w.spill_owners,
-        seeding);
+    udf_task_kernel<kSign, kStats, kBatch><<<(unsigned)grid, kTaskWarps * 32, 0, s>>>(
+        T, pts, n, perm, bound, out, sg, stats, w.rerun, w.nrerun, w.nrerun + 2, w.spill, w.spill_owners, seeding,
+        sel, pool);
   } else {
-    udf_kernel<kSign, kStats><<<(unsigned)ceil_div(n, kUdfThreads), kUdfThreads, 0, s>>>(
-        nodes, tris, pts, n, 1, perm, bound, out, sg, stats, w.rerun, w.nrerun);
+    if constexpr (!kBatch) {
+      udf_kernel<kSign, kStats><<<(unsigned)ceil_div(n, kUdfThreads), kUdfThreads, 0, s>>>(
+          T, pts, n, 1, perm, bound, out, sg, stats, w.rerun, w.nrerun);
+    } else {
+      A3D_REQUIRE(false, A3D_ERR_ARGUMENT, "udf: batches are always sorted");
+    }
   }
   A3D_LAUNCH_CHECK();
   // the re-run list length is only known on the device: launch enough
   // threads for a few percent of the queries, each thread strides
   const int64_t rr_threads = n / 16 > (int64_t)kNumSMs * 256 ? n / 16 : (int64_t)kNumSMs * 256;
-  udf_rerun_kernel<kSign, kStats><<<(unsigned)ceil_div(rr_threads, 64), 64, 0, s>>>(
-      nodes, tris, pts, w.rerun, w.nrerun, out, sg, stats, (int*)(w.nrerun + 1));
+  udf_rerun_kernel<kSign, kStats, kBatch><<<(unsigned)ceil_div(rr_threads, 64), 64, 0, s>>>(
+      T, pts, w.rerun, w.nrerun, out, sg, stats, w.nrerun + 1, w.nrerun + 4, sel);
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
@@ -905,7 +986,11 @@ extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num
   const bool coherent = perm != nullptr || (flags & A3D_UDF_ASSUME_SORTED) != 0;
   const uint32_t seeding = ((flags & A3D_UDF_NO_REUSE) ? 0u : kSeedReuse) |
                            ((flags & A3D_UDF_BOUND_SEEDS) && bound ? kSeedBoundOnly : 0u);
-  A3D_CUDA_TRY(cudaMemsetAsync(w.nrerun, 0, 4 * sizeof(uint32_t), s));
+  A3D_CUDA_TRY(cudaMemsetAsync(w.nrerun, 0, kStatusWords * sizeof(uint32_t), s));
+  const TreeT<false> T{(const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, (uint32_t)bvh->num_nodes,
+                       (uint32_t)bvh->num_tris, w.nrerun + 3};
+  const MeshSel sel{nullptr, nullptr, 1, 0};
+  const TaskShape shape{kTaskPool, 0};
   QueryOut out{distances, face_ids, closest_points, uvw};
   SignArgs sg{nullptr, nullptr, nullptr, nullptr, nullptr};
   if (sign) {
@@ -914,15 +999,15 @@ extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num
                   pn ? sign->he_edge_idx : nullptr, sign->faces};
   }
   if (sign) {
-    if (stats) A3D_TRY((launch_udf<true, true>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, seeding, s)));
-    else A3D_TRY((launch_udf<true, false>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, seeding, s)));
+    if (stats) A3D_TRY((launch_udf<true, true, false>(T, points, n, perm, coherent, bound, out, sg, stats, w, seeding, sel, shape, s)));
+    else A3D_TRY((launch_udf<true, false, false>(T, points, n, perm, coherent, bound, out, sg, stats, w, seeding, sel, shape, s)));
   } else {
-    if (stats) A3D_TRY((launch_udf<false, true>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, seeding, s)));
-    else A3D_TRY((launch_udf<false, false>(bvh, points, n, perm, coherent, bound, out, sg, stats, w, seeding, s)));
+    if (stats) A3D_TRY((launch_udf<false, true, false>(T, points, n, perm, coherent, bound, out, sg, stats, w, seeding, sel, shape, s)));
+    else A3D_TRY((launch_udf<false, false, false>(T, points, n, perm, coherent, bound, out, sg, stats, w, seeding, sel, shape, s)));
   }
   if (stats) {
     // reruns are reported as bound misses / spills (same counter: re-run queries)
-    A3D_CUDA_TRY(cudaMemcpyAsync(stats + 2, w.nrerun, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    A3D_CUDA_TRY(cudaMemcpyAsync(stats + 2, w.nrerun + 4, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
   }
   return A3D_OK;
 }
@@ -940,5 +1025,264 @@ extern "C" int a3d_udf_backward(const float* points, int64_t num_points, const f
   udf_backward_kernel<<<(unsigned)ceil_div(num_points, 256), 256, 0, s>>>(
       points, num_points, closest_points, face_ids, uvw, grad_dist, faces, grad_points, grad_vertices);
   A3D_LAUNCH_CHECK();
+  return A3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batches of meshes: one sort and one persistent traversal per chunk of
+// queries, all meshes together
+// ---------------------------------------------------------------------------
+namespace a3d {
+namespace {
+
+// queries per traversal launch of a batch (bounds the scratch: ~380 MB)
+constexpr int64_t kBatchChunk = 1ll << 24;
+
+__device__ __forceinline__ int segment_of64(const int64_t* __restrict__ off, int nseg, int64_t i) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// key = mesh id above the Morton code of the query in a cube of twice its
+// mesh's extent about the mesh centre; i is local to the chunk at qbase
+__global__ void batch_query_morton_kernel(const float* __restrict__ pts, int64_t n, int64_t qbase,
+                                          const int64_t* __restrict__ qoff, int nmesh,
+                                          const float* __restrict__ bounds, int bits, uint32_t* __restrict__ keys,
+                                          uint32_t* __restrict__ vals) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int m = segment_of64(qoff, nmesh, qbase + i);
+  const float* b = bounds + 6 * (int64_t)m;
+  float emax = fmaxf(b[3] - b[0], fmaxf(b[4] - b[1], b[5] - b[2]));
+  emax = emax > 0.f ? emax : 1.f;
+  const float qmax = (float)((1u << bits) - 1u);
+  const float inv = qmax / (2.0f * emax);
+  const float q[3] = {(pts[3 * i] - (0.5f * (b[0] + b[3]) - emax)) * inv,
+                      (pts[3 * i + 1] - (0.5f * (b[1] + b[4]) - emax)) * inv,
+                      (pts[3 * i + 2] - (0.5f * (b[2] + b[5]) - emax)) * inv};
+  uint32_t code = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float t = fminf(fmaxf(q[a], 0.f), qmax);
+    if (!(t == t)) t = 0.f;
+    code |= (uint32_t)spread3_21((uint64_t)t) << a;
+  }
+  keys[i] = ((uint32_t)m << (3 * bits)) | code;
+  vals[i] = (uint32_t)i;
+}
+
+int mesh_bits(int nmesh) {
+  int mbits = 0;
+  while ((1ll << mbits) < nmesh) ++mbits;
+  return mbits;
+}
+
+size_t batch_udf_bytes(int64_t n) {
+  const int64_t c = n < kBatchChunk ? (n > 0 ? n : 1) : kBatchChunk;
+  Workspace ws(nullptr, 0);
+  UdfWs w;
+  const size_t base = carve_udf(w, ws, c, A3D_UDF_SORT_QUERIES);
+  return base + (size_t)spill_owner_bound(c) * kSpillCap * sizeof(uint2) + 512;
+}
+
+int batch_udf(const a3d_bvh_batch* bvh, const float* points, const int64_t* qoff, int64_t n, float* distances,
+              int32_t* face_ids, float* closest_points, float* uvw, TaskShape shape, unsigned long long* stats,
+              void* workspace, size_t workspace_bytes, cudaStream_t s) {
+  A3D_REQUIRE(bvh && bvh->nodes && bvh->tris && bvh->roots && bvh->bounds && bvh->num_meshes > 0 &&
+                  bvh->num_faces > 0 && bvh->num_faces < (1ll << 28),
+              A3D_ERR_ARGUMENT, "batch_udf: invalid batch");
+  A3D_REQUIRE(n >= 0 && n < (1ll << 40), A3D_ERR_ARGUMENT, "batch_udf: bad number of queries");
+  A3D_REQUIRE(workspace, A3D_ERR_WORKSPACE, "batch_udf: no workspace");
+  const int mbits = mesh_bits(bvh->num_meshes);
+  A3D_REQUIRE(mbits <= 26, A3D_ERR_ARGUMENT, "batch_udf: too many meshes");
+  int bits = (32 - mbits) / 3;
+  bits = bits < 10 ? bits : 10;
+  const int64_t c = n < kBatchChunk ? (n > 0 ? n : 1) : kBatchChunk;
+  Workspace ws(workspace, workspace_bytes);
+  UdfWs w;
+  carve_udf(w, ws, c, A3D_UDF_SORT_QUERIES);
+  A3D_REQUIRE(ws.ok(), A3D_ERR_WORKSPACE, "batch_udf: workspace too small");
+  {
+    const uintptr_t base = ((uintptr_t)workspace + ws.used + 255) & ~(uintptr_t)255;
+    const uintptr_t endp = (uintptr_t)workspace + workspace_bytes;
+    const int64_t owners = base < endp ? (int64_t)((endp - base) / (kSpillCap * sizeof(uint2))) : 0;
+    w.spill = owners > 0 ? (uint2*)base : nullptr;
+    w.spill_owners = owners;
+  }
+  A3D_CUDA_TRY(cudaMemsetAsync(w.nrerun, 0, kStatusWords * sizeof(uint32_t), s));
+  if (n == 0) return A3D_OK;
+  A3D_REQUIRE(points && qoff && distances && face_ids && closest_points, A3D_ERR_ARGUMENT, "batch_udf: null pointer");
+  // the node count is only known on the device: guard with the capacity
+  const TreeT<true> T{(const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, (uint32_t)bvh->num_faces,
+                      (uint32_t)bvh->num_faces, w.nrerun + 3};
+  const SignArgs sg{nullptr, nullptr, nullptr, nullptr, nullptr};
+  for (int64_t base = 0; base < n; base += kBatchChunk) {
+    const int64_t cn = n - base < kBatchChunk ? n - base : kBatchChunk;
+    const float* pts = points + 3 * base;
+    batch_query_morton_kernel<<<(unsigned)ceil_div(cn, 256), 256, 0, s>>>(pts, cn, base, qoff, bvh->num_meshes,
+                                                                          bvh->bounds, bits, w.keys, w.vals);
+    A3D_LAUNCH_CHECK();
+    bool alt = false;
+    A3D_TRY(radix_sort_pairs<uint32_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, cn, 0, 3 * bits + mbits,
+                                       w.rs_scratch, &alt, s));
+    const uint32_t* perm = alt ? w.vals_alt : w.vals;
+    // per chunk: the re-run list and the pool counter start at zero
+    A3D_CUDA_TRY(cudaMemsetAsync(w.nrerun, 0, sizeof(uint32_t), s));
+    A3D_CUDA_TRY(cudaMemsetAsync(w.nrerun + 2, 0, sizeof(uint32_t), s));
+    const QueryOut out{distances + base, face_ids + base, closest_points + 3 * base, uvw ? uvw + 3 * base : nullptr};
+    const MeshSel sel{qoff, bvh->roots, bvh->num_meshes, base};
+    if (stats)
+      A3D_TRY((launch_udf<false, true, true>(T, pts, cn, perm, true, nullptr, out, sg, stats, w, kSeedReuse, sel,
+                                             shape, s)));
+    else
+      A3D_TRY((launch_udf<false, false, true>(T, pts, cn, perm, true, nullptr, out, sg, stats, w, kSeedReuse, sel,
+                                              shape, s)));
+  }
+  if (stats) A3D_CUDA_TRY(cudaMemcpyAsync(stats + 2, w.nrerun + 4, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  return A3D_OK;
+}
+
+// every stride-th query, with the offsets of the sample per mesh
+__global__ void sample_queries_kernel(const float* __restrict__ pts, int64_t stride, const int64_t* __restrict__ qoff,
+                                      int nmesh, float* __restrict__ spts, int64_t ns, int64_t* __restrict__ sqoff) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ns) {
+    const int64_t j = i * stride;
+    spts[3 * i] = pts[3 * j];
+    spts[3 * i + 1] = pts[3 * j + 1];
+    spts[3 * i + 2] = pts[3 * j + 2];
+  }
+  if (i <= nmesh) sqoff[i] = (qoff[i] + stride - 1) / stride;  // first sample at or after qoff[i]
+}
+
+struct TuneWs {
+  float* pts;
+  int64_t* qoff;
+  float* dist;
+  int32_t* fid;
+  float* cp;
+  void* udf_ws;
+  size_t udf_bytes;
+};
+
+size_t carve_tune(TuneWs& t, Workspace& ws, int64_t ns, int nmesh) {
+  t.pts = ws.take<float>(3 * ns);
+  t.qoff = ws.take<int64_t>(nmesh + 1);
+  t.dist = ws.take<float>(ns);
+  t.fid = ws.take<int32_t>(ns);
+  t.cp = ws.take<float>(3 * ns);
+  t.udf_bytes = batch_udf_bytes(ns);
+  t.udf_ws = ws.take<unsigned char>((int64_t)t.udf_bytes);
+  return ws.used;
+}
+
+}  // namespace
+}  // namespace a3d
+
+extern "C" int a3d_udf_status(const void* workspace, uint32_t* status_out, a3d_stream_t stream) {
+  A3D_REQUIRE(workspace && status_out, A3D_ERR_ARGUMENT, "udf_status: null pointer");
+  uint32_t w[a3d::kStatusWords];
+  A3D_CUDA_TRY(cudaMemcpyAsync(w, workspace, sizeof(w), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  A3D_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  status_out[0] = w[4];  // queries re-run by the deep-stack kernel
+  status_out[1] = w[1];  // deep-stack overflow
+  status_out[2] = 0u;
+  status_out[3] = w[3];  // guard faults
+  return A3D_OK;
+}
+
+extern "C" size_t a3d_batch_udf_workspace_bytes(int64_t num_queries, int32_t num_meshes) {
+  (void)num_meshes;
+  return a3d::batch_udf_bytes(num_queries);
+}
+
+extern "C" int a3d_batch_udf(const a3d_bvh_batch* bvh, const float* points, const int64_t* query_offsets,
+                             int64_t num_queries, float* distances, int32_t* face_ids, float* closest_points,
+                             float* uvw, const a3d_udf_tuning* tuning, unsigned long long* stats, void* workspace,
+                             size_t workspace_bytes, a3d_stream_t stream) {
+  a3d::TaskShape shape{a3d::kTaskPool, 0};
+  if (tuning) {
+    A3D_REQUIRE(tuning->pool >= 0 && tuning->pool <= 4096 && tuning->blocks_per_sm >= 0, A3D_ERR_ARGUMENT,
+                "batch_udf: bad tuning");
+    if (tuning->pool > 0) shape.pool = tuning->pool;
+    shape.blocks_per_sm = tuning->blocks_per_sm;
+  }
+  return a3d::batch_udf(bvh, points, query_offsets, num_queries, distances, face_ids, closest_points, uvw, shape,
+                        stats, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+extern "C" size_t a3d_batch_autotune_workspace_bytes(int64_t sample_queries, int32_t num_meshes) {
+  a3d::Workspace ws(nullptr, 0);
+  a3d::TuneWs t;
+  return a3d::carve_tune(t, ws, sample_queries > 0 ? sample_queries : 1, num_meshes > 0 ? num_meshes : 1) + 256;
+}
+
+extern "C" int a3d_batch_autotune(const a3d_bvh_batch* bvh, const float* points, const int64_t* query_offsets,
+                                  int64_t num_queries, int64_t sample_queries, void* workspace,
+                                  size_t workspace_bytes, a3d_udf_tuning* best, float* best_ms,
+                                  a3d_stream_t stream_) {
+  using namespace a3d;
+  cudaStream_t s = (cudaStream_t)stream_;
+  A3D_REQUIRE(bvh && points && query_offsets && best && num_queries > 0 && sample_queries > 0, A3D_ERR_ARGUMENT,
+              "batch_autotune: bad argument");
+  A3D_REQUIRE(sample_queries <= kBatchChunk, A3D_ERR_ARGUMENT, "batch_autotune: sample larger than one launch");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  A3D_CUDA_TRY(cudaStreamIsCapturing(s, &cap));
+  A3D_REQUIRE(cap == cudaStreamCaptureStatusNone, A3D_ERR_ARGUMENT,
+              "batch_autotune: times launches on the host; call it outside stream capture");
+  const int64_t stride = (num_queries + sample_queries - 1) / sample_queries;
+  const int64_t ns = (num_queries + stride - 1) / stride;
+  Workspace ws(workspace, workspace_bytes);
+  TuneWs t;
+  carve_tune(t, ws, ns, bvh->num_meshes);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "batch_autotune: workspace too small");
+  const int64_t th = ns > (int64_t)bvh->num_meshes + 1 ? ns : (int64_t)bvh->num_meshes + 1;
+  sample_queries_kernel<<<(unsigned)ceil_div(th, 256), 256, 0, s>>>(points, stride, query_offsets, bvh->num_meshes,
+                                                                    t.pts, ns, t.qoff);
+  A3D_LAUNCH_CHECK();
+  int occ = 0;
+  A3D_TRY((task_blocks_per_sm<false, false, true>(&occ)));
+  const int pools[4] = {32, 64, 128, 256};
+  const int bpss[3] = {occ, occ * 3 / 4, occ / 2};
+  cudaEvent_t e0, e1;
+  A3D_CUDA_TRY(cudaEventCreate(&e0));
+  A3D_CUDA_TRY(cudaEventCreate(&e1));
+  float best_t = INFINITY;
+  a3d_udf_tuning bt{kTaskPool, occ, 0, 0};
+  int rc = A3D_OK;
+  for (int pi = 0; pi < 4 && rc == A3D_OK; ++pi) {
+    for (int bi = 0; bi < 3 && rc == A3D_OK; ++bi) {
+      const int bps = bpss[bi];
+      if (bps < 1 || (bi > 0 && bps == bpss[bi - 1])) continue;
+      const TaskShape shape{pools[pi], bps};
+      // one warm-up run, then two timed
+      for (int rep = 0; rep < 3 && rc == A3D_OK; ++rep) {
+        if (rep == 1 && cudaEventRecord(e0, s) != cudaSuccess) rc = A3D_ERR_CUDA;
+        if (rc == A3D_OK)
+          rc = batch_udf(bvh, t.pts, t.qoff, ns, t.dist, t.fid, t.cp, nullptr, shape, nullptr, t.udf_ws, t.udf_bytes,
+                         s);
+      }
+      float ms = 0.f;
+      if (rc == A3D_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                           cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        rc = A3D_ERR_CUDA;
+      if (rc != A3D_OK) break;
+      ms *= 0.5f;
+      if (ms < best_t) {
+        best_t = ms;
+        bt = a3d_udf_tuning{pools[pi], bps, 0, 0};
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != A3D_OK) return rc;
+  *best = bt;
+  if (best_ms) *best_ms = best_t;
   return A3D_OK;
 }

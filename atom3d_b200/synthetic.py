@@ -120,8 +120,8 @@ def surface_samples(v: torch.Tensor, f: torch.Tensor, n: int, g: torch.Generator
     a, b, c = vd[f[:, 0].long()], vd[f[:, 1].long()], vd[f[:, 2].long()]
     area = torch.linalg.cross(b - a, c - a).norm(dim=1)
     idx = torch.multinomial(area, n, replacement=True, generator=g)
-    r1 = torch.rand(n, generator=g, dtype=torch.float64)
-    r2 = torch.rand(n, generator=g, dtype=torch.float64)
+    r1 = torch.rand(n, generator=g, dtype=torch.float64, device=vd.device)
+    r2 = torch.rand(n, generator=g, dtype=torch.float64, device=vd.device)
     s = r1.sqrt()
     w0, w1, w2 = 1 - s, s * (1 - r2), s * r2
     return w0[:, None] * a[idx] + w1[:, None] * b[idx] + w2[:, None] * c[idx]
@@ -133,10 +133,11 @@ def mixed_queries(v: torch.Tensor, f: torch.Tensor, n: int, g: torch.Generator, 
     box scaled by ``box_scale`` about its centre."""
     n_s = n // 2
     n_u = n - n_s
-    near = surface_samples(v, f, n_s, g) + sigma * torch.randn(n_s, 3, generator=g, dtype=torch.float64)
+    dev = v.device
+    near = surface_samples(v, f, n_s, g) + sigma * torch.randn(n_s, 3, generator=g, dtype=torch.float64, device=dev)
     lo, hi = v.double().min(0).values, v.double().max(0).values
     c, h = (lo + hi) * 0.5, (hi - lo) * 0.5 * box_scale
-    uni = c + (torch.rand(n_u, 3, generator=g, dtype=torch.float64) * 2.0 - 1.0) * h
+    uni = c + (torch.rand(n_u, 3, generator=g, dtype=torch.float64, device=dev) * 2.0 - 1.0) * h
     return torch.cat([near, uni], 0).float()
 
 
@@ -161,20 +162,56 @@ def _random_rotation(g: torch.Generator) -> torch.Tensor:
     )
 
 
-def batch_meshes(n_meshes: int = 256, seed: int = 4, min_level: int = 3, max_level: int = 8,
-                 queries_per_tri: int = 8):
-    """List of (vertices, faces, queries) under seeded affine maps."""
+def batch_specs(n_meshes: int = 256, seed: int = 4, min_level: int = 3, max_level: int = 8):
+    """Per-mesh parameters of the batched workload: subdivision level drawn
+    uniformly from [min_level, max_level] (log-uniform triangle counts),
+    displacement seed, scale U[0.5, 2], rotation from a normalised
+    quaternion, translation U[-1, 1]^3, query seed."""
     g = torch.Generator().manual_seed(seed)
-    out = []
+    specs = []
     for i in range(n_meshes):
         level = int(torch.randint(min_level, max_level + 1, (1,), generator=g))
-        v, f = displaced_sphere(level, 8, 0.05, seed * 1000 + i)
         scale = float(torch.rand(1, generator=g, dtype=torch.float64)) * 1.5 + 0.5
         rot = _random_rotation(g)
         trans = torch.rand(3, generator=g, dtype=torch.float64) * 2.0 - 1.0
-        vw = (v.double() @ rot.T) * scale + trans
-        q = mixed_queries(vw.float(), f, queries_per_tri * f.shape[0], g)
-        out.append((vw.float(), f, q))
+        specs.append({"level": level, "disp_seed": seed * 1000 + i, "scale": scale, "rot": rot, "trans": trans,
+                      "query_seed": seed * 100000 + i})
+    return specs
+
+
+_ICO_CACHE: dict = {}
+
+
+def _icosphere_cached(level: int):
+    if level not in _ICO_CACHE:
+        _ICO_CACHE[level] = icosphere(level)
+    return _ICO_CACHE[level]
+
+
+def batch_meshes(n_meshes: int = 256, seed: int = 4, min_level: int = 3, max_level: int = 8,
+                 queries_per_tri: int = 8, device="cpu"):
+    """List of (vertices, faces, queries) generated on ``device``: each mesh
+    is a level-L icosphere radially displaced by 8 seeded sinusoids of
+    amplitude 0.05, then scaled, rotated and translated; its queries
+    (queries_per_tri per triangle) follow ``mixed_queries``."""
+    out = []
+    dev = torch.device(device)
+    for sp in batch_specs(n_meshes, seed, min_level, max_level):
+        v0, f = _icosphere_cached(sp["level"])
+        g = torch.Generator().manual_seed(sp["disp_seed"])
+        freq = torch.rand(8, generator=g, dtype=torch.float64) * 6.0 + 2.0
+        d = torch.randn(8, 3, generator=g, dtype=torch.float64)
+        d = d / d.norm(dim=1, keepdim=True)
+        phase = torch.rand(8, generator=g, dtype=torch.float64) * (2 * math.pi)
+        vd = v0.to(dev).double()
+        x = vd / vd.norm(dim=1, keepdim=True)
+        r = 1.0 + 0.05 * torch.sin(freq.to(dev)[None, :] * (x @ d.to(dev).T) + phase.to(dev)[None, :]).sum(dim=1)
+        v = (vd * r[:, None]).float().double()
+        vw = (v @ sp["rot"].to(dev).T) * sp["scale"] + sp["trans"].to(dev)
+        fd = f.to(dev)
+        gq = torch.Generator(device=dev).manual_seed(sp["query_seed"])
+        q = mixed_queries(vw.float(), fd, queries_per_tri * f.shape[0], gq)
+        out.append((vw.float(), fd, q))
     return out
 
 

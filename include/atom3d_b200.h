@@ -262,6 +262,64 @@ int a3d_dmc_backward(const a3d_dmc_inputs* in, void* workspace, size_t workspace
                      const float* g_p_alpha, const float* g_n_alpha, float* g_sdf,
                      float* g_deform, float* g_alpha, float* g_beta, a3d_stream_t stream);
 
+/* Status words of the last a3d_udf / a3d_batch_udf / a3d_udf_noalloc call
+ * that used `workspace`, copied to the host after the stream drains:
+ * [0] queries re-run by the deep-stack kernel, [1] deep-stack overflow (a
+ * re-run query's result may be inexact), [2] 0, [3] guard faults of batch
+ * queries (bit 0: a node index outside the node array, bit 1: a triangle
+ * index outside the triangle array; the access was skipped).  No
+ * counterpart in the reference. */
+int a3d_udf_status(const void* workspace, uint32_t* status_out, a3d_stream_t stream);
+
+/* ---- batches of meshes (no counterpart in the reference) ---------------- */
+/* Many meshes of uneven size built into one wide-BVH array and queried by
+ * persistent traversal launches shared by all meshes, with no host
+ * synchronisation (build + query can be captured in a CUDA graph).  Mesh m
+ * owns vertices [vertex_offsets[m], vertex_offsets[m+1]), faces
+ * [face_offsets[m], face_offsets[m+1]) (vertex indices local to the mesh)
+ * and queries [query_offsets[m], query_offsets[m+1]); the offset arrays live
+ * on the device.  Face ids returned are local to the query's mesh.  Queries
+ * are processed in launches of at most 16,777,216. */
+typedef struct a3d_bvh_batch {
+  const void* nodes;           /* num_faces x 64 B (capacity; the build writes the count) */
+  const void* tris;            /* num_faces x 64 B */
+  int64_t num_faces;
+  int32_t num_meshes;
+  const uint32_t* roots;       /* device [M]: root node of each mesh */
+  const float* bounds;         /* device [M][6]: lo xyz, hi xyz */
+} a3d_bvh_batch;
+
+size_t a3d_batch_build_workspace_bytes(int64_t num_faces, int32_t num_meshes);
+/* status_out (device int32[2], nullable): [0] bad face index or empty mesh,
+ * [1] tree deeper than the collapse's level limit; read after the stream. */
+int a3d_batch_build(const float* vertices, const int64_t* vertex_offsets, const int32_t* faces,
+                    const int64_t* face_offsets, int32_t num_meshes, int64_t num_faces, int leaf_max,
+                    void* nodes_out, void* tris_out, uint32_t* roots_out, float* bounds_out,
+                    int64_t* num_nodes_out, int32_t* status_out, void* workspace,
+                    size_t workspace_bytes, a3d_stream_t stream);
+
+/* launch shape of the persistent traversal (0 = default) */
+typedef struct a3d_udf_tuning {
+  int32_t pool;           /* queries taken per work request */
+  int32_t blocks_per_sm;  /* resident blocks per SM */
+  int32_t leaf_max;       /* informational: the build's leaf size */
+  int32_t reserved;
+} a3d_udf_tuning;
+
+size_t a3d_batch_udf_workspace_bytes(int64_t num_queries, int32_t num_meshes);
+int a3d_batch_udf(const a3d_bvh_batch* bvh, const float* points, const int64_t* query_offsets,
+                  int64_t num_queries, float* distances, int32_t* face_ids, float* closest_points,
+                  float* uvw, const a3d_udf_tuning* tuning, unsigned long long* stats,
+                  void* workspace, size_t workspace_bytes, a3d_stream_t stream);
+/* Times the traversal's launch shapes on every ceil(Q/sample)-th query
+ * (sample <= 16,777,216) and returns the fastest (host-synchronous; not
+ * inside stream capture). */
+size_t a3d_batch_autotune_workspace_bytes(int64_t sample_queries, int32_t num_meshes);
+int a3d_batch_autotune(const a3d_bvh_batch* bvh, const float* points, const int64_t* query_offsets,
+                       int64_t num_queries, int64_t sample_queries, void* workspace,
+                       size_t workspace_bytes, a3d_udf_tuning* best, float* best_ms,
+                       a3d_stream_t stream);
+
 /* ---- learned distance bound (no counterpart in the reference) ----------- */
 /* A Fourier-feature MLP (3 -> 64 -> 128 -> 128 -> 128 -> 1, ReLU) predicts
  * a query's unsigned distance; bound = max(y, 0) * scale + margin seeds
