@@ -316,14 +316,169 @@ def main():
                       "warp_rounds_per_query": rounds / n},
     }
     if not args.no_extra:
+        line["learned"] = bench_learned(dev, v, f, mesh, qd, max(3, args.steps // 2))
         line["dmc"] = bench_dmc(dev, max(2, args.steps // 2), 2, cpu=(rank == 0 and not args.no_cpu_baseline))
         line["octree_flood"] = bench_octree_flood(dev, max(2, args.steps // 2), 3)
+        line["batch"] = bench_batch(dev, 2, 1, cpu=(rank == 0 and not args.no_cpu_baseline))
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(v, f, q)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def _time_ms(fn, steps, warmup=2):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def bench_learned(dev, v, f, mesh, qd, steps):
+    """Learned-bound UDF vs plain on the 16M-query workload: the bound MLP is
+    trained on 4,194,304 plain-method samples of the same distribution
+    (other seed) with the hand-written BF16 kernels; every variant returns
+    identical distances and face ids (checked here)."""
+    from atom3d_b200 import _lib, synthetic
+    from atom3d_b200.learned import train_for_mesh
+
+    n = qd.shape[0]
+    g = torch.Generator().manual_seed(77)
+    train = synthetic.mixed_queries(v, f, 1 << 22, g)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lb = train_for_mesh(mesh, train, epochs=8, coverage=0.99)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    bvh = mesh._bvh
+    ref = bvh.query(qd)
+    bound = lb(qd)
+    exact = torch.nextafter(ref[0], torch.full_like(ref[0], float("inf"))) * (1 + 1e-6)
+    infer_ms = _time_ms(lambda: lb(qd, out=bound), steps)
+    NR, BS = _lib.A3D_UDF_NO_REUSE, _lib.A3D_UDF_BOUND_SEEDS
+    variants = {
+        "plain": (None, 0),
+        "plain_no_neighbour_seed": (None, NR),
+        "learned_cap": (bound, 0),
+        "learned_seeds": (bound, NR | BS),
+        "exact_bound_cap": (exact, 0),
+        "exact_bound_seeds": (exact, NR | BS),
+    }
+    out = {"metric": "UDF Mqueries/s, learned bound vs plain (same 16M queries)", "unit": UNIT,
+           "train_s": train_s, "train_samples": 1 << 22, "margin": lb.margin, "infer_ms": infer_ms,
+           "bound_covers": float((ref[0] <= bound).float().mean())}
+    for name, (b, flags) in variants.items():
+        r = bvh.query(qd, bound=b, seeding=flags)
+        same = bool(torch.equal(r[0], ref[0]) and torch.equal(r[1], ref[1]))
+        ms = _time_ms(lambda: bvh.query(qd, bound=b, seeding=flags), steps)
+        if name.startswith("learned"):
+            ms += infer_ms  # the bound's inference is part of the learned path
+        out[name] = {"ms": ms, "mqs": n / ms / 1e3, "identical": same}
+    out["speedup_learned_vs_plain"] = out["plain"]["ms"] / min(out["learned_cap"]["ms"], out["learned_seeds"]["ms"])
+    out["speedup_exact_bound_vs_plain"] = out["plain"]["ms"] / min(out["exact_bound_cap"]["ms"],
+                                                                     out["exact_bound_seeds"]["ms"])
+    return out
+
+
+def launches_per_batch(num_queries, num_meshes):
+    """Kernels of one batched build + query (the graph's kernel nodes)."""
+    mbits = max(0, int(np.ceil(np.log2(max(num_meshes, 1)))))
+    bits = min(21, (64 - mbits) // 3)
+    sort_passes = -(-(3 * bits + mbits) // 8)
+    build = 3 + 5 * sort_passes + 3 + 64 + 2 + 5 + 3
+    chunks = -(-num_queries // (1 << 24))
+    qbits = min(10, (32 - mbits) // 3)
+    per_chunk = 1 + 5 * (-(-(3 * qbits + mbits) // 8)) + 2
+    return build + chunks * per_chunk
+
+
+def bench_batch(dev, steps, warmup, cpu=True):
+    """256 displaced icospheres (levels 3-8, 74.6M triangles) under seeded
+    affine maps, 8 queries per triangle (597M); one step = the batched
+    build + UDF of all meshes replayed from a captured CUDA graph."""
+    from atom3d_b200 import synthetic
+    from atom3d_b200.batch import BatchedMeshBVH, offsets
+
+    t0 = time.perf_counter()
+    meshes = synthetic.batch_meshes(256, seed=4, device=dev)
+    vc = [int(m[0].shape[0]) for m in meshes]
+    fc = [int(m[1].shape[0]) for m in meshes]
+    qc = [int(m[2].shape[0]) for m in meshes]
+    V = torch.cat([m[0] for m in meshes]).contiguous()
+    F = torch.cat([m[1] for m in meshes]).int().contiguous()
+    Q = torch.cat([m[2] for m in meshes]).contiguous()
+    sample_meshes = [(m[0].cpu(), m[1].cpu(), m[2][:: max(1, m[2].shape[0] // 8)][:8].cpu()) for m in meshes]
+    del meshes
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    nq, nf = int(Q.shape[0]), int(F.shape[0])
+    bb = BatchedMeshBVH(vertices=V, faces=F, vertex_counts=vc, face_counts=fc)
+    qoff = offsets(qc, dev)
+    tune = bb.autotune(Q, qoff, sample=1 << 21)
+    dist_o = torch.empty(nq, device=dev)
+    fid_o = torch.empty(nq, dtype=torch.int32, device=dev)
+    cp_o = torch.empty(nq, 3, device=dev)
+    st = torch.zeros(4, dtype=torch.int64, device=dev)
+    bb.udf_into(Q, qoff, dist_o, fid_o, cp_o, stats=st)
+    torch.cuda.synchronize()
+    stats = [int(x) for x in st.cpu()]
+    build_ms = _time_ms(bb.build, 3, 1)
+    query_ms = _time_ms(lambda: bb.udf_into(Q, qoff, dist_o, fid_o, cp_o), 1, 0)
+    g = bb.capture(Q, qoff, dist_o, fid_o, cp_o)
+    with ClockSampler(dev.index or 0) as clk:
+        ms = _time_ms(g.replay, steps, warmup)
+    status = bb.query_status()
+    bb.check()
+    out = {"metric": "batched build + UDF, Mqueries/s (256 meshes, 74.6M tris, 597M queries, CUDA graph)",
+           "value": nq / ms / 1e3, "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": warmup,
+           "meshes": len(fc), "triangles": nf, "queries": nq, "build_ms": build_ms, "query_ms": query_ms,
+           "generate_s": gen_s, "autotune": tune, "status": status, "clocks": clk.summary(),
+           "gpu_launches": steps * launches_per_batch(nq, len(fc)),
+           "traversal": {"nodes_per_query": stats[0] / nq, "tris_per_query": stats[1] / nq, "reruns": stats[2]}}
+    # end to end: pinned host mesh + queries in, distances + face ids +
+    # closest points out, around the same graph
+    try:
+        hV, hF, hQ = V.cpu().pin_memory(), F.cpu().pin_memory(), Q.cpu().pin_memory()
+        hd = torch.empty(nq, pin_memory=True)
+        hf = torch.empty(nq, dtype=torch.int32, pin_memory=True)
+        hc = torch.empty(nq, 3, pin_memory=True)
+
+        def e2e():
+            bb.vertices.copy_(hV, non_blocking=True)
+            bb.faces.copy_(hF, non_blocking=True)
+            Q.copy_(hQ, non_blocking=True)
+            g.replay()
+            hd.copy_(dist_o, non_blocking=True)
+            hf.copy_(fid_o, non_blocking=True)
+            hc.copy_(cp_o, non_blocking=True)
+
+        e_ms = _time_ms(e2e, 1, 1)
+        out["e2e"] = {"value": nq / e_ms / 1e3, "unit": UNIT, "h2d_bytes_per_step": hV.numel() * 4 + hF.numel() * 4
+                      + hQ.numel() * 4, "d2h_bytes_per_step": nq * 20}
+        del hV, hF, hQ, hd, hf, hc
+    except RuntimeError as e:  # pinned host memory is limited on some hosts
+        out["e2e"] = {"value": None, "unavailable": str(e)[:200]}
+    if cpu:
+        from oracle import orc
+
+        orc.build()
+        t0 = time.perf_counter()
+        done = 0
+        for v_, f_, q_ in sample_meshes:
+            orc.ref_udf_bruteforce(v_.numpy(), f_.numpy(), q_.numpy())
+            done += q_.shape[0]
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": done / t / 1e6, "unit": UNIT, "cores": orc.threads(), "kind": "port",
+                               "sample": f"{done} queries, 8 per mesh, brute force over each mesh's triangles"}
+    del g
+    return out
 
 
 def bench_dmc(dev, steps, warmup, cpu=True):
