@@ -88,7 +88,7 @@ class BatchedMeshBVH:
 
     def __init__(self, meshes=None, *, vertices: Optional[torch.Tensor] = None, faces: Optional[torch.Tensor] = None,
                  vertex_counts: Optional[Sequence[int]] = None, face_counts: Optional[Sequence[int]] = None,
-                 leaf_max: int = 4, device=None, build: bool = True):
+                 leaf_max: int = 8, device=None, build: bool = True):
         if meshes is not None:
             vertex_counts = [int(v.shape[0]) for v, _ in meshes]
             face_counts = [int(f.shape[0]) for _, f in meshes]

@@ -30,7 +30,7 @@ from .device_utils import resolve_device
 class WideBVH:
     """Device-resident 4-wide quantised BVH (64-B nodes, 64-B triangle records)."""
 
-    DEFAULT_LEAF_MAX = int(os.environ.get("ATOM3D_B200_LEAF_MAX", "4"))
+    DEFAULT_LEAF_MAX = int(os.environ.get("ATOM3D_B200_LEAF_MAX", "8"))
 
     def __init__(self, vertices: torch.Tensor, faces: torch.Tensor, leaf_max: int | None = None):
         _lib.require_cuda(vertices, "vertices")

@@ -39,6 +39,10 @@ constexpr int kThreads = 256;
 constexpr int kMaxLevels = 64;  // wide levels; deeper trees report A3D_ERR_OVERFLOW
 constexpr int kLevelBlocks = kNumSMs * 8;
 constexpr uint32_t kNoLevel = 255u;
+// leaves of up to 8 triangles: fewer, larger leaves trade node tests for
+// cheaper triangle tests (16M-query closest-point workload on a 1.31M-
+// triangle mesh: 201 ms at 8 vs 226 ms at 4)
+constexpr int kDefaultLeafMax = 8;
 
 struct BuildWs {
   int64_t* face_off;    // single-mesh builds: offsets written on the device
@@ -628,7 +632,7 @@ extern "C" int a3d_bvh_build(const float* vertices, int64_t num_vertices, const 
   BuildWs w;
   carve(w, ws, n, 1);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "bvh_build: workspace too small");
-  if (leaf_max == 0) leaf_max = 4;
+  if (leaf_max == 0) leaf_max = kDefaultLeafMax;
   A3D_REQUIRE(leaf_max >= 1 && leaf_max <= kMaxLeafTris, A3D_ERR_ARGUMENT, "bvh_build: leaf_max must be in 1..8");
   single_offsets_kernel<<<1, 32, 0, s>>>(w.face_off, w.vert_off, n, num_vertices);
   A3D_LAUNCH_CHECK();
@@ -673,7 +677,7 @@ extern "C" int a3d_batch_build(const float* vertices, const int64_t* vertex_offs
               A3D_ERR_ARGUMENT, "batch_build: null pointer");
   A3D_REQUIRE(((uintptr_t)nodes_out & 63) == 0 && ((uintptr_t)tris_out & 15) == 0, A3D_ERR_ARGUMENT,
               "batch_build: nodes must be 64-B and triangles 16-B aligned");
-  if (leaf_max == 0) leaf_max = 4;
+  if (leaf_max == 0) leaf_max = kDefaultLeafMax;
   A3D_REQUIRE(leaf_max >= 1 && leaf_max <= kMaxLeafTris, A3D_ERR_ARGUMENT, "batch_build: leaf_max must be in 1..8");
   Workspace ws(workspace, workspace_bytes);
   BuildWs w;

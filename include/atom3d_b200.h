@@ -58,7 +58,7 @@ typedef struct a3d_bvh_view {
  * GPU build: Morton codes -> in-house radix sort -> binary radix tree ->
  * bottom-up refit -> SAH-guided collapse into 4-wide quantised nodes.
  * node_capacity >= max(num_faces, 1) always suffices.  leaf_max (1..8, 0 =
- * default 4): subtrees with at most this many triangles become leaves. */
+ * default 8): subtrees with at most this many triangles become leaves. */
 size_t a3d_bvh_build_workspace_bytes(int64_t num_faces);
 int a3d_bvh_build(const float* vertices, int64_t num_vertices,
                   const int32_t* faces, int64_t num_faces, int leaf_max,
