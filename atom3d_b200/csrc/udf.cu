@@ -473,20 +473,37 @@ constexpr int kSpillCap = 96;    // per-owner global overflow stack (entries)
 constexpr int kSpillChunk = 16;  // entries moved per spill / refill
 constexpr int kTaskTriCap = 32 * kMaxLeafTris;
 constexpr int kTaskPool = 64;  // queries per pool taken from the global counter
-// 64-thread blocks with 24 KB of shared memory: at <= 112 registers a thread,
-// 9 blocks (18 warps) stay resident per SM
-constexpr int kTaskMaxRegs = 112;
+// register cap of the task kernel: each of the SM's four sub-partitions
+// holds 16K registers, so 64-thread blocks reach 8 resident blocks (16
+// warps) at <= 128 registers a thread and 9 (18 warps, also the 24 KB
+// shared-memory limit) at <= 96
+#ifndef A3D_TASK_MAX_REGS
+#define A3D_TASK_MAX_REGS 128
+#endif
+constexpr int kTaskMaxRegs = A3D_TASK_MAX_REGS;
+
+// Per-warp shared state.  Child-box results sit at node rank * 5 + child and
+// triangle results at position-in-leaf * 33 + owner, so that the owners'
+// reads in the consume step fall in distinct banks.  Finished queries wait
+// in fin_* and are written out 32 at a time by the whole warp.
+constexpr int kBoxStride = 5;
+constexpr int kTriRow = 33;
+constexpr int kFinCap = 64;
 
 struct TaskSmem {
   uint2 stack[kTaskDepth][32];
   float px[32], py[32], pz[32];
   uint32_t nref[32];
   uint8_t nown[32];
-  float boxd[128];
-  uint32_t boxr[128];
+  float boxd[32 * kBoxStride];
+  uint32_t boxr[32 * kBoxStride];
   uint32_t tidx[kTaskTriCap];
-  float trid[kTaskTriCap];
   uint8_t town[kTaskTriCap];
+  uint8_t tpos[kTaskTriCap];
+  float trid[kMaxLeafTris * kTriRow];
+  uint32_t fin_q[kFinCap];
+  uint32_t fin_tri[kFinCap];
+  float fin_sq[kFinCap];
 };
 
 enum : int { kIdle = 0, kProbe = 1, kSeed = 2, kTrav = 3, kAbandon = 4 };
@@ -523,7 +540,15 @@ __global__ void __maxnreg__(kTaskMaxRegs)
   const int64_t owner = ((int64_t)blockIdx.x * kTaskWarps + warp) * 32 + lane;
   uint2* my_spill = (spill != nullptr && owner < spill_owners) ? spill + owner * kSpillCap : nullptr;
   int gsp = 0;
+  int nfin = 0;  // finished queries waiting in S.fin_* (warp-uniform)
   unsigned long long rounds = 0;
+
+  // writes out finished query e of S.fin_*
+  auto finish_entry = [&](int e) {
+    const int64_t q = (int64_t)S.fin_q[e];
+    finish_query(T.tris, T.num_tris, S.fin_tri[e], S.fin_sq[e], pts[3 * q], pts[3 * q + 1], pts[3 * q + 2], q, out,
+                 sg, kSign);
+  };
 
   auto start = [&](int64_t k) {
     qi = perm ? (int64_t)perm[k] : k;
@@ -606,16 +631,30 @@ __global__ void __maxnreg__(kTaskMaxRegs)
       done = !have;
     }
     if (phase == kAbandon) done = true;
-    if (done) {
-      if (phase == kAbandon || best_tri == 0xffffffffu) {
-        rerun[atomicAdd(nrerun, 1u)] = (uint32_t)qi;
-        prev = 0xffffffffu;
-      } else {
-        finish_query(T.tris, T.num_tris, best_tri, best_sq, px, py, pz, qi, out, sg, kSign);
+    const bool found = done && phase != kAbandon && best_tri != 0xffffffffu;
+    if (done && !found) {
+      rerun[atomicAdd(nrerun, 1u)] = (uint32_t)qi;
+      prev = 0xffffffffu;
+    }
+    {
+      // queue the finished queries; once 32 wait, every lane writes one out
+      const unsigned fmask = __ballot_sync(FULL, found);
+      if (found) {
+        const int at = nfin + __popc(fmask & lt_mask);
+        S.fin_q[at] = (uint32_t)qi;
+        S.fin_tri[at] = best_tri;
+        S.fin_sq[at] = best_sq;
         prev = best_tri;
       }
-      phase = kIdle;
+      nfin += __popc(fmask);
+      if (nfin >= 32) {
+        __syncwarp();
+        finish_entry(nfin - 32 + lane);
+        nfin -= 32;
+        __syncwarp();
+      }
     }
+    if (done) phase = kIdle;
     distribute(__ballot_sync(FULL, done));
     // (b) classify this round's item
     const bool is_node = (phase == kProbe || phase == kTrav) && have && !ref_is_leaf(ref);
@@ -638,11 +677,12 @@ __global__ void __maxnreg__(kTaskMaxRegs)
     }
     const int ttotal = __shfl_sync(FULL, toff, 31);
     toff -= tcnt;
+    const uint32_t f0 = is_seed ? prev : leaf_first(ref);
     if (tcnt > 0) {
-      const uint32_t f0 = is_seed ? prev : leaf_first(ref);
       for (int i = 0; i < tcnt; ++i) {
         S.tidx[toff + i] = f0 + i;
         S.town[toff + i] = (uint8_t)lane;
+        S.tpos[toff + i] = (uint8_t)i;
       }
       if (kStats) ctr.tris += tcnt;
     }
@@ -654,12 +694,12 @@ __global__ void __maxnreg__(kTaskMaxRegs)
       float d;
       uint32_t cr;
       quad_child_box(T, S.nref[r], c, S.px[o], S.py[o], S.pz[o], d, cr);
-      S.boxd[t] = d;
-      S.boxr[t] = cr;
+      S.boxd[r * kBoxStride + c] = d;
+      S.boxr[r * kBoxStride + c] = cr;
     }
     for (int t = lane; t < ttotal; t += 32) {
       const int o = S.town[t];
-      S.trid[t] = tri_dist_sq(T.tri(S.tidx[t]), S.px[o], S.py[o], S.pz[o]);
+      S.trid[S.tpos[t] * kTriRow + o] = tri_dist_sq(T.tri(S.tidx[t]), S.px[o], S.py[o], S.pz[o]);
     }
     __syncwarp();
     // (d) owners consume their results
@@ -668,8 +708,8 @@ __global__ void __maxnreg__(kTaskMaxRegs)
       uint32_t r[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        d[c] = S.boxd[4 * nrank + c];
-        r[c] = S.boxr[4 * nrank + c];
+        d[c] = S.boxd[kBoxStride * nrank + c];
+        r[c] = S.boxr[kBoxStride * nrank + c];
       }
       if (phase == kProbe) {
         // greedy: the (distance, ref)-smallest child
@@ -714,8 +754,8 @@ __global__ void __maxnreg__(kTaskMaxRegs)
       float dmin = INFINITY;
       uint32_t imin = 0xffffffffu;
       for (int i = 0; i < tcnt; ++i) {
-        const float dd = S.trid[toff + i];
-        if (dd < dmin) { dmin = dd; imin = S.tidx[toff + i]; }
+        const float dd = S.trid[i * kTriRow + lane];
+        if (dd < dmin) { dmin = dd; imin = f0 + (uint32_t)i; }
       }
       if (phase == kTrav) {
         if (dmin < best_sq) { best_sq = dmin; best_tri = imin; }
@@ -732,6 +772,9 @@ __global__ void __maxnreg__(kTaskMaxRegs)
     }
     __syncwarp();
   }
+  // queries still waiting to be written out
+  __syncwarp();
+  if (lane < nfin) finish_entry(lane);
   if (kStats) {
     flush_counters(ctr, stats);
     if (lane == 0) atomicAdd(stats + 3, rounds);
