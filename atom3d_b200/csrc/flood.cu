@@ -285,23 +285,33 @@ __global__ void popc_kernel(const uint32_t* __restrict__ v, int64_t n, uint32_t*
   if (i < n) c[i] = (uint32_t)__popc(v[i]);
 }
 
+// One warp per 32 consecutive words; for each word the 32 lanes take its 32
+// bits, so the set voxels' coordinates are written as one contiguous run
+// (coalesced) in the word's bit order -- lexicographic (x, y, z) overall.
 __global__ void extract_kernel(Geom g, const uint32_t* __restrict__ v, const int64_t* __restrict__ offs,
                                int64_t nwords, int32_t* __restrict__ out) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nwords) return;
-  uint32_t m = v[i];
-  if (!m) return;
-  const int w = (int)(i % g.nw);
-  const int64_t row = i / g.nw;
-  const int y = (int)(row % g.ny), x = (int)(row / g.ny);
-  int64_t o = offs[i];
-  while (m) {
-    const int b = __ffs(m) - 1;
-    m &= m - 1;
-    out[3 * o] = x + g.vx;
-    out[3 * o + 1] = y + g.vy;
-    out[3 * o + 2] = w * 32 + b + g.vz;
-    ++o;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+  if (w0 >= nwords) return;
+  const int nw = nwords - w0 < 32 ? (int)(nwords - w0) : 32;
+  const uint32_t mine = lane < nw ? v[w0 + lane] : 0u;
+  const int64_t my_off = lane < nw ? offs[w0 + lane] : 0;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int j = 0; j < nw; ++j) {
+    const uint32_t m = __shfl_sync(FULL, mine, j);
+    if (m == 0u) continue;
+    const int64_t o = __shfl_sync(FULL, my_off, j);
+    const int64_t i = w0 + j;
+    const int w = (int)(i % g.nw);
+    const int64_t row = i / g.nw;
+    const int y = (int)(row % g.ny), x = (int)(row / g.ny);
+    if ((m >> lane) & 1u) {
+      int32_t* p = out + 3 * (o + __popc(m & lt));
+      p[0] = x + g.vx;
+      p[1] = y + g.vy;
+      p[2] = w * 32 + lane + g.vz;
+    }
   }
 }
 
