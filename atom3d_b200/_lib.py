@@ -49,6 +49,15 @@ _SIGNATURES: dict[str, tuple] = {
     "a3d_last_error": (ctypes.c_char_p, []),
     "a3d_version": (ctypes.c_char_p, []),
     "a3d_udf_status": (c_int, [c_vp, ctypes.POINTER(c_u32), c_vp]),
+    "a3d_ray_workspace_bytes": (c_size, [c_i64]),
+    "a3d_ray_nearest": (c_int, [c_vp, c_vp, c_vp, c_i64, ctypes.c_float, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                c_vp, c_size, c_vp]),
+    "a3d_ray_all_count": (c_int, [c_vp, c_vp, c_vp, c_i64, ctypes.c_float, c_vp, c_vp, c_size, c_vp]),
+    "a3d_ray_all_collect": (c_int, [c_vp, c_vp, c_vp, c_i64, ctypes.c_float, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                    c_vp, c_vp]),
+    "a3d_ray_parity_votes": (c_int, [c_vp, c_vp, c_i64, c_vp, ctypes.c_int32, ctypes.c_float, ctypes.c_float, c_vp,
+                                     c_vp, c_size, c_vp]),
+    "a3d_ray_status": (c_int, [c_vp, ctypes.POINTER(c_u32), c_vp]),
     "a3d_bvh_build_workspace_bytes": (c_size, [c_i64]),
     "a3d_bvh_build": (
         c_int,

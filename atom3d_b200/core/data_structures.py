@@ -38,9 +38,27 @@ class ClosestPointResult:
 
 @dataclass
 class RayIntersectResult:
+    """Nearest hit per ray: hit [N] bool, t [N] (max_t on a miss), face ids [N]
+    int32 (-1 on a miss), hit points [N,3], face normals [N,3], optional
+    barycentrics [N,3]."""
+
     hit: torch.Tensor
     t: torch.Tensor
     face_ids: torch.Tensor
     hit_points: torch.Tensor
     normals: torch.Tensor
     bary_coords: Optional[torch.Tensor] = None
+
+
+@dataclass
+class RayAllHitResult:
+    """Every hit of every ray, grouped by ray: ray index [H] int32, t [H],
+    face ids [H] int32, sign(normal . direction) [H] int32, points [H,3],
+    barycentrics [H,3]."""
+
+    ray_idx: torch.Tensor
+    t: torch.Tensor
+    face_ids: torch.Tensor
+    sign: torch.Tensor
+    hit_points: torch.Tensor
+    bary_coords: torch.Tensor

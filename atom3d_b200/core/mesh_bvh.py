@@ -23,7 +23,7 @@ from typing import Optional, Union
 import torch
 
 from .. import _lib
-from .data_structures import AABBIntersectResult, ClosestPointResult
+from .data_structures import AABBIntersectResult, ClosestPointResult, RayAllHitResult, RayIntersectResult
 from .device_utils import resolve_device
 
 
@@ -310,13 +310,108 @@ class MeshBVH:
     ) -> Union[torch.Tensor, ClosestPointResult]:
         """Signed distance with the Baerentzen-Aanaes pseudo-normal sign
         (reference: atom3d/core/mesh_bvh.py:702-827), fused into the query."""
+        if mode == "parity":
+            return self._sdf_parity(points, **kwargs)
         if mode != "pseudo_normal":
-            raise NotImplementedError(f"sdf mode {mode!r} is not provided by atom3d_b200 (use 'pseudo_normal')")
+            raise ValueError(f"sdf mode {mode!r}: use 'pseudo_normal' or 'parity'")
         if return_grad:
             result = self._udf_with_grad(points, sign=True, bound=bound)
         else:
             result = self._udf_query(points, sign=True, bound=bound)
         return self._filter(result, return_closest, return_uvw, return_face_ids)
+
+    # ---------------------------------------------------------------- rays
+    def intersect_ray(self, rays_o: torch.Tensor, rays_d: torch.Tensor, max_t: float = 1e10,
+                      return_uvw: bool = False, mode: str = "nearest"):
+        """Ray-mesh intersection (reference: atom3d/core/mesh_bvh.py:1076-1160).
+
+        mode "nearest": closest hit per ray (RayIntersectResult); "all": every
+        non-grazing hit, grouped by ray (RayAllHitResult).
+        """
+        if mode == "all":
+            return self._intersect_ray_all(rays_o, rays_d, max_t)
+        if mode != "nearest":
+            raise ValueError(f"intersect_ray mode {mode!r}: use 'nearest' or 'all'")
+        o, d = self._rays(rays_o, rays_d)
+        n = o.shape[0]
+        dev = self.device
+        hit = torch.empty(n, dtype=torch.bool, device=dev)
+        t = torch.empty(n, dtype=torch.float32, device=dev)
+        fid = torch.empty(n, dtype=torch.int32, device=dev)
+        hp = torch.empty(n, 3, dtype=torch.float32, device=dev)
+        nrm = torch.empty(n, 3, dtype=torch.float32, device=dev)
+        uvw = torch.empty(n, 3, dtype=torch.float32, device=dev) if return_uvw else None
+        ws = _lib.workspace(_lib.lib().a3d_ray_workspace_bytes(n), dev)
+        self._last_ray_ws = ws
+        _lib.call("a3d_ray_nearest", ctypes.byref(self._bvh.view), o.data_ptr(), d.data_ptr(), n, float(max_t),
+                  self._face_normals.data_ptr(), hit.data_ptr(), t.data_ptr(), fid.data_ptr(), hp.data_ptr(),
+                  nrm.data_ptr(), _lib.ptr(uvw), ws.data_ptr(), ws.numel(), _lib.stream_ptr(dev))
+        return RayIntersectResult(hit=hit, t=t, face_ids=fid, hit_points=hp, normals=nrm, bary_coords=uvw)
+
+    def _rays(self, rays_o: torch.Tensor, rays_d: torch.Tensor):
+        _lib.require_cuda(rays_o, "rays_o")
+        _lib.require_cuda(rays_d, "rays_d")
+        o = rays_o.detach().to(self.device).float().contiguous()
+        d = rays_d.detach().to(self.device).float().contiguous()
+        if o.shape != d.shape or o.dim() != 2 or o.shape[1] != 3:
+            raise ValueError("rays_o and rays_d must both be [N, 3]")
+        return o, d
+
+    def _intersect_ray_all(self, rays_o: torch.Tensor, rays_d: torch.Tensor, max_t: float = 1e10) -> RayAllHitResult:
+        o, d = self._rays(rays_o, rays_d)
+        n = o.shape[0]
+        dev = self.device
+        lib = _lib.lib()
+        ws = _lib.workspace(lib.a3d_ray_workspace_bytes(n), dev)
+        self._last_ray_ws = ws
+        offs = torch.empty(n + 1, dtype=torch.int64, device=dev)
+        st = _lib.stream_ptr(dev)
+        _lib.call("a3d_ray_all_count", ctypes.byref(self._bvh.view), o.data_ptr(), d.data_ptr(), n, float(max_t),
+                  offs.data_ptr(), ws.data_ptr(), ws.numel(), st)
+        total = int(offs[n].item()) if n else 0
+        ray_idx = torch.empty(total, dtype=torch.int32, device=dev)
+        t = torch.empty(total, dtype=torch.float32, device=dev)
+        fid = torch.empty(total, dtype=torch.int32, device=dev)
+        sign = torch.empty(total, dtype=torch.int32, device=dev)
+        hp = torch.empty(total, 3, dtype=torch.float32, device=dev)
+        uvw = torch.empty(total, 3, dtype=torch.float32, device=dev)
+        if total:
+            _lib.call("a3d_ray_all_collect", ctypes.byref(self._bvh.view), o.data_ptr(), d.data_ptr(), n,
+                      float(max_t), offs.data_ptr(), ray_idx.data_ptr(), t.data_ptr(), fid.data_ptr(),
+                      sign.data_ptr(), hp.data_ptr(), uvw.data_ptr(), st)
+        return RayAllHitResult(ray_idx=ray_idx, t=t, face_ids=fid, sign=sign, hit_points=hp, bary_coords=uvw)
+
+    def ray_status(self) -> dict:
+        """Status of the last ray call (synchronises): rays re-run with the
+        deep stack, and whether a stack or hit buffer overflowed."""
+        st = (ctypes.c_uint32 * 2)()
+        _lib.call("a3d_ray_status", self._last_ray_ws.data_ptr(), st, _lib.stream_ptr(self.device))
+        return {"reruns": int(st[0]), "overflow": int(st[1])}
+
+    def _sdf_parity(self, points: torch.Tensor, n_dirs: int = 8, max_t: float = 1e6, coalesce_t: float = 1e-4,
+                    seed: int = 42, **_unused) -> torch.Tensor:
+        """Signed distance with the ray-parity sign (reference:
+        atom3d/core/mesh_bvh.py:850-948): for n_dirs seeded random
+        directions, hits within coalesce_t along a ray are merged and the
+        signed crossing count taken; a point is inside when more than half of
+        the directions give an odd count.  All directions are traced by one
+        fused kernel (traverse, sort by t, merge, vote)."""
+        _lib.require_cuda(points, "points")
+        p = points.detach().to(self.device).float().contiguous()
+        n = p.shape[0]
+        udf = self.udf(p)
+        gen = torch.Generator(device=self.device)
+        gen.manual_seed(seed)
+        dirs = torch.randn(n_dirs, 3, device=self.device, generator=gen)
+        dirs = (dirs / dirs.norm(dim=1, keepdim=True)).contiguous()
+        votes = torch.empty(n, dtype=torch.int32, device=self.device)
+        ws = _lib.workspace(_lib.lib().a3d_ray_workspace_bytes(0), self.device)
+        self._last_ray_ws = ws
+        _lib.call("a3d_ray_parity_votes", ctypes.byref(self._bvh.view), p.data_ptr(), n, dirs.data_ptr(), int(n_dirs),
+                  float(max_t), float(coalesce_t), votes.data_ptr(), ws.data_ptr(), ws.numel(),
+                  _lib.stream_ptr(self.device))
+        inside = votes > (n_dirs // 2)
+        return torch.where(inside, -udf, udf)
 
     @staticmethod
     def _filter(result: ClosestPointResult, closest: bool, uvw: bool, fids: bool):

@@ -271,6 +271,41 @@ int a3d_dmc_backward(const a3d_dmc_inputs* in, void* workspace, size_t workspace
  * counterpart in the reference. */
 int a3d_udf_status(const void* workspace, uint32_t* status_out, a3d_stream_t stream);
 
+/* ---- ray queries ---------------------------------------------------------
+ * Replace bvh_ray_intersect_kernel / bvh_ray_all_hit_kernel
+ * (atom3d/kernels/bvh_kernels.cu:469-553, :935-1022) behind
+ * MeshBVH.intersect_ray (atom3d/core/mesh_bvh.py:1076-1160) and the
+ * crossing-count loop of MeshBVH._sdf_parity (:850-948).  Triangle test:
+ * Moller-Trumbore with the reference's thresholds (|det| >= 1e-8, FP64
+ * u, v with FLT_EPSILON slack, t > 1e-8). */
+size_t a3d_ray_workspace_bytes(int64_t num_rays);
+/* Nearest hit per ray: hit flag, t (max_t on a miss), face id (-1 on a
+ * miss), hit point (0 on a miss; nullable), normal = face_normals[face]
+ * (nullable; needs face_normals), barycentrics as MeshBVH._bary_from_hit
+ * (nullable). */
+int a3d_ray_nearest(const a3d_bvh_view* bvh, const float* rays_o, const float* rays_d, int64_t num_rays,
+                    float max_t, const float* face_normals, uint8_t* hit, float* t, int32_t* face_ids,
+                    float* hit_points, float* normals, float* uvw, void* workspace,
+                    size_t workspace_bytes, a3d_stream_t stream);
+/* All non-grazing hits (|n.d| >= 1e-4) with 0 < t < max_t: the count pass
+ * writes exclusive offsets [num_rays + 1] (device; total at the end), the
+ * collect pass fills ray index, t, face id, sign(n.d), point and
+ * barycentrics (Triangle::barycentric; both nullable), grouped by ray. */
+int a3d_ray_all_count(const a3d_bvh_view* bvh, const float* rays_o, const float* rays_d, int64_t num_rays,
+                      float max_t, int64_t* offsets_out, void* workspace, size_t workspace_bytes,
+                      a3d_stream_t stream);
+int a3d_ray_all_collect(const a3d_bvh_view* bvh, const float* rays_o, const float* rays_d, int64_t num_rays,
+                        float max_t, const int64_t* offsets, int32_t* ray_idx, float* t, int32_t* face_ids,
+                        int32_t* sign, float* hit_points, float* uvw, a3d_stream_t stream);
+/* Per point, the number of directions whose signed crossing count, after
+ * merging hits closer than coalesce_t along the ray, is odd. */
+int a3d_ray_parity_votes(const a3d_bvh_view* bvh, const float* points, int64_t num_points, const float* dirs,
+                         int32_t num_dirs, float max_t, float coalesce_t, int32_t* votes, void* workspace,
+                         size_t workspace_bytes, a3d_stream_t stream);
+/* [0] rays re-run with the deep stack, [1] stack or hit-buffer overflow
+ * (results of some ray may be incomplete) of the last ray call on workspace. */
+int a3d_ray_status(const void* workspace, uint32_t* status_out, a3d_stream_t stream);
+
 /* ---- batches of meshes (no counterpart in the reference) ---------------- */
 /* Many meshes of uneven size built into one wide-BVH array and queried by
  * persistent traversal launches shared by all meshes, with no host

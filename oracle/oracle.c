@@ -630,3 +630,164 @@ void orc_ref_bvh_udf_counts(const float* nodes, const float* tris, const float* 
   counts[0] = atomic_load(&cnt[0]);
   counts[1] = atomic_load(&cnt[1]);
 }
+
+/* ------------------------------------------------------------------------
+ * Rays, brute force over all faces in face order:
+ *   Triangle::ray_intersect  (atom3d/kernels/bvh_kernels.cu:185-202)
+ *   Triangle::normal         (:89-99), Triangle::barycentric (:205-221)
+ *   bvh_ray_intersect_kernel (:469-553): nearest hit, strict "<" (first wins)
+ *   bvh_ray_all_hit_kernel   (:935-1022): every hit 0 < t < max_t that is
+ *       not grazing (|n.d| >= 1e-4), sign = sign(n.d)
+ *   MeshBVH._bary_from_hit   (atom3d/core/mesh_bvh.py:1218-1244)
+ *   MeshBVH._sdf_parity / _signed_crossing_count (:850-948), hits of a ray
+ *       ordered by t (the reference's float32 sort key keeps that order
+ *       only for ray indices below ~8; the intent is t order)
+ * ------------------------------------------------------------------------ */
+static inline f3 fsub3(f3 a, f3 b) { f3 r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+static inline f3 fcross3(f3 a, f3 b) {
+  f3 r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+  return r;
+}
+static inline float fdot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline f3 ldf(const float* V, int64_t i) { f3 r = {V[3 * i], V[3 * i + 1], V[3 * i + 2]}; return r; }
+
+static float ray_tri_f32(f3 a, f3 b, f3 c, f3 ro, f3 rd) {
+  const float eps = 1e-8f;
+  const double eps_edge = 1.19209290e-7;
+  f3 e1 = fsub3(b, a), e2 = fsub3(c, a);
+  f3 h = fcross3(rd, e2);
+  float det = fdot3(e1, h);
+  if (fabsf(det) < eps) return 1e10f;
+  float f = 1.0f / det;
+  f3 s = fsub3(ro, a);
+  double u = (double)f * (double)fdot3(s, h);
+  if (u < -eps_edge || u > 1.0 + eps_edge) return 1e10f;
+  f3 q = fcross3(s, e1);
+  double v = (double)f * (double)fdot3(rd, q);
+  if (v < -eps_edge || u + v > 1.0 + eps_edge) return 1e10f;
+  float t = f * fdot3(e2, q);
+  return (t > eps) ? t : 1e10f;
+}
+
+static f3 tri_normal_f32(f3 a, f3 b, f3 c) {
+  f3 n = fcross3(fsub3(b, a), fsub3(c, a));
+  float len = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
+  if (len > 1e-10f) {
+    float inv = 1.0f / len;
+    f3 r = {n.x * inv, n.y * inv, n.z * inv};
+    return r;
+  }
+  f3 z = {0.f, 0.f, 1.f};
+  return z;
+}
+
+typedef struct {
+  const float* V; const int32_t* F; int64_t nf; const float* O; const float* D; float max_t;
+  uint8_t* hit; float* t; int32_t* fid; float* hp; float* uvw;
+} ray_near_ctx;
+
+static void ray_near_body(int64_t i, void* vc) {
+  ray_near_ctx* c = (ray_near_ctx*)vc;
+  f3 ro = ldf(c->O, i), rd = ldf(c->D, i);
+  float mint = c->max_t;
+  int32_t best = -1;
+  for (int64_t f = 0; f < c->nf; ++f) {
+    f3 a = ldf(c->V, c->F[3 * f]), b = ldf(c->V, c->F[3 * f + 1]), cc = ldf(c->V, c->F[3 * f + 2]);
+    float t = ray_tri_f32(a, b, cc, ro, rd);
+    if (t < mint) { mint = t; best = (int32_t)f; }
+  }
+  c->hit[i] = best >= 0;
+  c->t[i] = mint;
+  c->fid[i] = best;
+  if (best >= 0) {
+    f3 hp = {ro.x + rd.x * mint, ro.y + rd.y * mint, ro.z + rd.z * mint};
+    c->hp[3 * i] = hp.x; c->hp[3 * i + 1] = hp.y; c->hp[3 * i + 2] = hp.z;
+    f3 a = ldf(c->V, c->F[3 * best]), b = ldf(c->V, c->F[3 * best + 1]), cc = ldf(c->V, c->F[3 * best + 2]);
+    f3 e0 = fsub3(b, a), e1 = fsub3(cc, a), vp = fsub3(hp, a);
+    float d00 = fdot3(e0, e0), d01 = fdot3(e0, e1), d11 = fdot3(e1, e1), d20 = fdot3(vp, e0), d21 = fdot3(vp, e1);
+    float denom = d00 * d11 - d01 * d01 + 1e-12f;
+    float bv = (d11 * d20 - d01 * d21) / denom, bw = (d00 * d21 - d01 * d20) / denom;
+    c->uvw[3 * i] = 1.0f - bv - bw; c->uvw[3 * i + 1] = bv; c->uvw[3 * i + 2] = bw;
+  } else {
+    c->hp[3 * i] = c->hp[3 * i + 1] = c->hp[3 * i + 2] = 0.f;
+    c->uvw[3 * i] = c->uvw[3 * i + 1] = c->uvw[3 * i + 2] = 0.f;
+  }
+}
+
+void orc_ray_nearest(const float* V, const int32_t* F, int64_t nf, const float* O, const float* D, int64_t n,
+                     float max_t, uint8_t* hit, float* t, int32_t* fid, float* hp, float* uvw) {
+  ray_near_ctx c = {V, F, nf, O, D, max_t, hit, t, fid, hp, uvw};
+  par_for(n, 16, ray_near_body, &c);
+}
+
+/* every non-grazing hit of ray i, in face order; returns the count, writes
+ * at most cap entries */
+static int64_t ray_all_one(const float* V, const int32_t* F, int64_t nf, f3 ro, f3 rd, float max_t, int64_t cap,
+                           float* ts, int32_t* fids, int32_t* signs) {
+  int64_t k = 0;
+  for (int64_t f = 0; f < nf; ++f) {
+    f3 a = ldf(V, F[3 * f]), b = ldf(V, F[3 * f + 1]), cc = ldf(V, F[3 * f + 2]);
+    float t = ray_tri_f32(a, b, cc, ro, rd);
+    if (t > 0.0f && t < max_t) {
+      f3 nn = tri_normal_f32(a, b, cc);
+      float ndotd = fdot3(nn, rd);
+      if (ndotd > -1e-4f && ndotd < 1e-4f) continue;
+      if (k < cap) { ts[k] = t; fids[k] = (int32_t)f; signs[k] = ndotd > 0.0f ? 1 : -1; }
+      ++k;
+    }
+  }
+  return k;
+}
+
+void orc_ray_all(const float* V, const int32_t* F, int64_t nf, const float* O, const float* D, int64_t n, float max_t,
+                 int64_t cap_per_ray, int32_t* counts, float* t, int32_t* fid, int32_t* sign) {
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t k = ray_all_one(V, F, nf, ldf(O, i), ldf(D, i), max_t, cap_per_ray, t + i * cap_per_ray,
+                            fid + i * cap_per_ray, sign + i * cap_per_ray);
+    counts[i] = (int32_t)k;
+  }
+}
+
+typedef struct {
+  const float* V; const int32_t* F; int64_t nf; const float* P; const float* dirs; int ndir; float max_t;
+  float coalesce; int32_t* votes;
+} parity_ctx;
+
+static void parity_body(int64_t i, void* vc) {
+  parity_ctx* c = (parity_ctx*)vc;
+  enum { CAP = 4096 };
+  float ts[CAP];
+  int32_t fids[CAP], sg[CAP];
+  int32_t votes = 0;
+  for (int d = 0; d < c->ndir; ++d) {
+    f3 ro = ldf(c->P, i), rd = ldf(c->dirs, d);
+    int64_t k = ray_all_one(c->V, c->F, c->nf, ro, rd, c->max_t, CAP, ts, fids, sg);
+    if (k > CAP) k = CAP;
+    /* stable insertion sort by t */
+    for (int64_t a = 1; a < k; ++a) {
+      float tv = ts[a]; int32_t sv = sg[a]; int64_t b = a - 1;
+      while (b >= 0 && ts[b] > tv) { ts[b + 1] = ts[b]; sg[b + 1] = sg[b]; --b; }
+      ts[b + 1] = tv; sg[b + 1] = sv;
+    }
+    int32_t sc = 0;
+    int64_t a = 0;
+    while (a < k) {
+      int64_t b = a + 1;
+      int32_t cnt = 1, sum = sg[a];
+      while (b < k && fabsf(ts[b] - ts[b - 1]) < c->coalesce) { ++cnt; sum += sg[b]; ++b; }
+      int32_t sgn = sum > 0 ? 1 : (sum < 0 ? -1 : 0);
+      int32_t asum = sum < 0 ? -sum : sum;
+      sc += (asum == cnt) ? sgn : (asum % 2) * sgn;
+      a = b;
+    }
+    int32_t asc = sc < 0 ? -sc : sc;
+    votes += (asc % 2) == 1;
+  }
+  c->votes[i] = votes;
+}
+
+void orc_parity_votes(const float* V, const int32_t* F, int64_t nf, const float* P, int64_t n, const float* dirs,
+                      int ndir, float max_t, float coalesce, int32_t* votes) {
+  parity_ctx c = {V, F, nf, P, dirs, ndir, max_t, coalesce, votes};
+  par_for(n, 4, parity_body, &c);
+}

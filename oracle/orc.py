@@ -281,3 +281,44 @@ def ref_bvh_udf_counts(nodes, tris, P):
     c = np.zeros(2, np.int64)
     lib().orc_ref_bvh_udf_counts(_p(nodes), _p(tris), _p(P), I64(P.shape[0]), _p(c))
     return int(c[0]), int(c[1])
+
+
+# --------------------------------------------------------------------- rays
+def ray_nearest(V, F, O, D, max_t=1e10):
+    """Brute-force nearest hit (reference ray maths): hit, t, face, point, uvw."""
+    V, F, O, D = _f32(V), _i32(F), _f32(O), _f32(D)
+    n = O.shape[0]
+    hit = np.empty(n, np.uint8)
+    t = np.empty(n, np.float32)
+    fid = np.empty(n, np.int32)
+    hp = np.empty((n, 3), np.float32)
+    uvw = np.empty((n, 3), np.float32)
+    lib().orc_ray_nearest(_p(V), _p(F), I64(F.shape[0]), _p(O), _p(D), I64(n), ctypes.c_float(max_t), _p(hit),
+                          _p(t), _p(fid), _p(hp), _p(uvw))
+    return hit.astype(bool), t, fid, hp, uvw
+
+
+def ray_all(V, F, O, D, max_t=1e10, cap=256):
+    """Every non-grazing hit per ray (face order): list of (t, face, sign) arrays."""
+    V, F, O, D = _f32(V), _i32(F), _f32(O), _f32(D)
+    n = O.shape[0]
+    counts = np.empty(n, np.int32)
+    t = np.empty((n, cap), np.float32)
+    fid = np.empty((n, cap), np.int32)
+    sign = np.empty((n, cap), np.int32)
+    lib().orc_ray_all(_p(V), _p(F), I64(F.shape[0]), _p(O), _p(D), I64(n), ctypes.c_float(max_t), I64(cap),
+                      _p(counts), _p(t), _p(fid), _p(sign))
+    out = []
+    for i in range(n):
+        k = min(int(counts[i]), cap)
+        out.append((t[i, :k].copy(), fid[i, :k].copy(), sign[i, :k].copy()))
+    return counts, out
+
+
+def parity_votes(V, F, P, dirs, max_t=1e6, coalesce=1e-4):
+    """Per point, number of directions whose coalesced signed crossing count is odd."""
+    V, F, P, dirs = _f32(V), _i32(F), _f32(P), _f32(dirs)
+    votes = np.empty(P.shape[0], np.int32)
+    lib().orc_parity_votes(_p(V), _p(F), I64(F.shape[0]), _p(P), I64(P.shape[0]), _p(dirs), ctypes.c_int(dirs.shape[0]),
+                           ctypes.c_float(max_t), ctypes.c_float(coalesce), _p(votes))
+    return votes

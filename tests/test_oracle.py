@@ -152,3 +152,19 @@ def test_dam_neighbourhood_signs_oracle(orc):
     r_out = np.linalg.norm(d["extended_tide_ijk"] - c, axis=1)
     assert r_in.max() < r_out.max()
     assert len(set(map(tuple, nb.tolist())) & set(map(tuple, d["dam_ijk"].tolist()))) == 0
+
+
+def test_ray_oracle_matches_reference_cpu_path(golden, orc):
+    """The oracle's restatement of the reference's ray maths against the
+    reference's own CPU nearest-hit results (it rejects t <= 1e-6 where the
+    GPU kernel rejects t <= 1e-8, and rounds u, v in FP32 first)."""
+    g = golden("ray_small.npz")
+    hit, t, fid, hp, _ = orc.ray_nearest(g["v"], g["f"], g["o"], g["d"])
+    ok = (g["t"] > 1e-5) | ~g["hit"]
+    assert ((hit == g["hit"]) | ~ok).mean() > 0.999
+    both = hit & g["hit"]
+    # same formula; torch's reductions order the dot products differently and
+    # the determinant's cancellation amplifies that: up to ~5e-6 relative
+    assert np.allclose(t[both], g["t"][both], rtol=1e-5, atol=0)
+    assert (fid[both] == g["face_ids"][both]).mean() > 0.99
+    assert np.allclose(hp[both], g["hit_points"][both], atol=1e-5)
