@@ -210,7 +210,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--queries", type=int, default=16 * 1024 * 1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extra", action="store_true", help="skip the DMC and octree/flood measurements")
+    ap.add_argument("--no-extra", action="store_true", help="skip every measurement besides the main UDF line")
+    ap.add_argument("--skip", default="", help="comma-separated extra sections to skip: learned,dmc,octree,rays,batch")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -315,11 +316,19 @@ def main():
         "traversal": {"nodes_per_query": our_nodes / n, "tris_per_query": our_tris / n, "reruns": reruns,
                       "warp_rounds_per_query": rounds / n},
     }
+    skip = set(x for x in args.skip.split(",") if x)
     if not args.no_extra:
-        line["learned"] = bench_learned(dev, v, f, mesh, qd, max(3, args.steps // 2))
-        line["dmc"] = bench_dmc(dev, max(2, args.steps // 2), 2, cpu=(rank == 0 and not args.no_cpu_baseline))
-        line["octree_flood"] = bench_octree_flood(dev, max(2, args.steps // 2), 3)
-        line["batch"] = bench_batch(dev, 2, 1, cpu=(rank == 0 and not args.no_cpu_baseline))
+        cpu = rank == 0 and not args.no_cpu_baseline
+        if "learned" not in skip:
+            line["learned"] = bench_learned(dev, v, f, mesh, qd, max(3, args.steps // 2))
+        if "dmc" not in skip:
+            line["dmc"] = bench_dmc(dev, max(2, args.steps // 2), 2, cpu=cpu)
+        if "octree" not in skip:
+            line["octree_flood"] = bench_octree_flood(dev, max(2, args.steps // 2), 3)
+        if "rays" not in skip:
+            line["rays"] = bench_rays(dev, mesh, v, max(3, args.steps // 2))
+        if "batch" not in skip:
+            line["batch"] = bench_batch(dev, 2, 1, cpu=cpu)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(v, f, q)
     if rank == 0:
@@ -385,6 +394,32 @@ def bench_learned(dev, v, f, mesh, qd, steps):
     out["speedup_exact_bound_vs_plain"] = out["plain"]["ms"] / min(out["exact_bound_cap"]["ms"],
                                                                      out["exact_bound_seeds"]["ms"])
     return out
+
+
+def bench_rays(dev, mesh, v, steps):
+    """Ray queries on the 1.31M-triangle mesh: nearest hit for 16,777,216 rays
+    (origins uniform in the 1.2x box, uniform directions), all hits for
+    1,048,576 of them, and the ray-parity SDF (8 directions) for 1,048,576
+    points."""
+    g = torch.Generator().manual_seed(31)
+    n = 1 << 24
+    lo, hi = v.min(0).values, v.max(0).values
+    c, h = (lo + hi) * 0.5, (hi - lo) * 0.6
+    o = (c + (torch.rand(n, 3, generator=g) * 2 - 1) * h).float().to(dev)
+    d = torch.randn(n, 3, generator=g)
+    d = (d / d.norm(dim=1, keepdim=True)).float().to(dev)
+    near_ms = _time_ms(lambda: mesh.intersect_ray(o, d), steps)
+    r = mesh.intersect_ray(o, d)
+    m = 1 << 20
+    all_ms = _time_ms(lambda: mesh.intersect_ray(o[:m], d[:m], mode="all"), steps)
+    ra = mesh.intersect_ray(o[:m], d[:m], mode="all")
+    par_ms = _time_ms(lambda: mesh.sdf(o[:m], mode="parity"), steps)
+    return {"metric": "ray queries on the 1.31M-triangle mesh", "unit": "Mrays/s",
+            "nearest": {"rays": n, "ms": near_ms, "mrays_s": n / near_ms / 1e3,
+                        "hit_fraction": float(r.hit.float().mean())},
+            "all_hits": {"rays": m, "ms": all_ms, "mrays_s": m / all_ms / 1e3, "hits": int(ra.t.numel())},
+            "parity_sdf": {"points": m, "directions": 8, "ms": par_ms, "mpoints_s": m / par_ms / 1e3},
+            "status": mesh.ray_status()}
 
 
 def launches_per_batch(num_queries, num_meshes):
