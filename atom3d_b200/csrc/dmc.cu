@@ -828,3 +828,362 @@ extern "C" int a3d_dmc_backward(const a3d_dmc_inputs* p, void* workspace, size_t
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
+
+// ---------------------------------------------------------------------------
+// QEF inference mode (SparseDiffDMC.forward with inference_mode "qef" / eval)
+// ---------------------------------------------------------------------------
+// corner gradients   _estimate_corner_gradients        :451-513
+// crossing normals   corner-gradient interpolation     :610-650
+// dual vertices      _solve_qef_scatter (the system it assembles) :289-389
+// triangulation      2 triangles, shorter diagonal     :798-805
+namespace a3d {
+namespace {
+
+struct GradWs {
+  float* x;         // [M,3]
+  uint64_t* keys;   // [12N]
+  uint64_t* keys2;
+  uint32_t* vals;
+  uint32_t* vals2;
+  uint32_t* rs;
+  double* acc;      // [M][9]: DtD xx xy xz yy yz zz, Dtb x y z
+};
+
+size_t carve_grad(GradWs& w, Workspace& ws, int64_t n, int64_t m) {
+  const int64_t n12 = 12 * n;
+  w.x = ws.take<float>(3 * m);
+  w.keys = ws.take<uint64_t>(n12);
+  w.keys2 = ws.take<uint64_t>(n12);
+  w.vals = ws.take<uint32_t>(n12);
+  w.vals2 = ws.take<uint32_t>(n12);
+  w.rs = ws.take<uint32_t>((int64_t)radix_sort_scratch_elems(n12));
+  w.acc = ws.take<double>(9 * m);
+  return ws.used;
+}
+
+__global__ void all_edge_keys_kernel(DmcIn in, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= in.n * 12) return;
+  const int64_t i = t / 12;
+  const int e = (int)(t % 12);
+  const uint64_t a = (uint64_t)in.cidx[8 * i + kCE[2 * e]], b = (uint64_t)in.cidx[8 * i + kCE[2 * e + 1]];
+  keys[t] = a * (uint64_t)in.m + b;
+  vals[t] = (uint32_t)t;
+}
+
+// each unique (ordered) corner pair once: d (x) d to both ends, the edge's
+// gradient projection times d to the first and its negative to the second
+__global__ void edge_lsq_kernel(DmcIn in, const uint64_t* __restrict__ keys, int64_t nk, const float* __restrict__ x,
+                                double* __restrict__ acc) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nk) return;
+  const uint64_t k = keys[r];
+  if (r > 0 && keys[r - 1] == k) return;
+  const int64_t i0 = (int64_t)(k / (uint64_t)in.m), i1 = (int64_t)(k % (uint64_t)in.m);
+  float ev[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) ev[a] = fsb(ldf(x, 3 * i1 + a), ldf(x, 3 * i0 + a));
+  const float el = fmaxf(sqrtf(fa(fa(fm(ev[0], ev[0]), fm(ev[1], ev[1])), fm(ev[2], ev[2]))), 1e-8f);
+  float d[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) d[a] = fd(ev[a], el);
+  const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
+  const float gp = fd(fsb(s1, s0), el);
+  const double o[6] = {(double)fm(d[0], d[0]), (double)fm(d[0], d[1]), (double)fm(d[0], d[2]),
+                       (double)fm(d[1], d[1]), (double)fm(d[1], d[2]), (double)fm(d[2], d[2])};
+  double* a0 = acc + 9 * i0;
+  double* a1 = acc + 9 * i1;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    atomicAdd(a0 + q, o[q]);
+    atomicAdd(a1 + q, o[q]);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double f = (double)fm(gp, d[a]);
+    atomicAdd(a0 + 6 + a, f);
+    atomicAdd(a1 + 6 + a, -f);
+  }
+}
+
+// solves the symmetric 3x3 system (a: xx xy xz yy yz zz) by cofactors
+__device__ __forceinline__ void solve_sym3(const double* a, const double* b, double* xo) {
+  const double c00 = a[3] * a[5] - a[4] * a[4], c01 = a[2] * a[4] - a[1] * a[5], c02 = a[1] * a[4] - a[2] * a[3];
+  const double c11 = a[0] * a[5] - a[2] * a[2], c12 = a[1] * a[2] - a[0] * a[4], c22 = a[0] * a[3] - a[1] * a[1];
+  const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+  const double inv = 1.0 / det;
+  xo[0] = (c00 * b[0] + c01 * b[1] + c02 * b[2]) * inv;
+  xo[1] = (c01 * b[0] + c11 * b[1] + c12 * b[2]) * inv;
+  xo[2] = (c02 * b[0] + c12 * b[1] + c22 * b[2]) * inv;
+}
+
+__global__ void corner_solve_kernel(int64_t m, const double* __restrict__ acc, float* __restrict__ grad) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double a[6], b[3], g[3];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) a[q] = acc[9 * i + q];
+  a[0] += 1e-4;
+  a[3] += 1e-4;
+  a[5] += 1e-4;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) b[q] = acc[9 * i + 6 + q];
+  solve_sym3(a, b, g);
+  const bool bad = isnan(g[0]) || isnan(g[1]) || isnan(g[2]);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) grad[3 * i + q] = bad ? 0.f : (float)g[q];
+}
+
+// crossing normal from the corner gradients, confidence-weighted by their
+// norms; the edge-direction normal where neither end has one
+__device__ __forceinline__ void crossing_normal(const float* __restrict__ grad, int64_t i0, int64_t i1, float s0,
+                                                float s1, const float* xa, const float* xb, float* n) {
+  const float t = fminf(fmaxf(fd(s0, fa(fsb(s0, s1), 1e-8f)), 0.f), 1.f);
+  float g0[3], g1[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) { g0[a] = ldf(grad, 3 * i0 + a); g1[a] = ldf(grad, 3 * i1 + a); }
+  const float n0 = sqrtf(fa(fa(fm(g0[0], g0[0]), fm(g0[1], g0[1])), fm(g0[2], g0[2])));
+  const float n1 = sqrtf(fa(fa(fm(g1[0], g1[0]), fm(g1[1], g1[1])), fm(g1[2], g1[2])));
+  const float w0 = fm(n0, fsb(1.f, t)), w1 = fm(n1, t);
+  const float den = fa(w0, w1);
+  float g[3];
+  if (den > 1e-6f) {
+    const float dd = fmaxf(den, 1e-8f);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) g[a] = fd(fa(fm(w0, g0[a]), fm(w1, g1[a])), dd);
+  } else {
+    edge_normal(xa, xb, s0, s1, g);
+  }
+  const float gl = fmaxf(sqrtf(fa(fa(fm(g[0], g[0]), fm(g[1], g[1])), fm(g[2], g[2]))), 1e-12f);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) n[a] = fd(g[a], gl);
+}
+
+// one thread per dual vertex: crossings, normals, the QEF the reference
+// assembles (constraint j of k in row (j - (k-1)) mod 10; sqrt(lambda) at
+// (7,0) (8,1) (9,2) and rows 7-9 of b pulled to the cell centre), solved in
+// FP64; centroid when the solution is NaN or a cell outside the cell
+__global__ void vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float* __restrict__ grad, float lam,
+                              int64_t nv, const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
+                              const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
+                              const uint32_t* __restrict__ goff, EdgeData ed, VdOut out) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const uint32_t t = vd_cube[v];
+  const int j = vd_slot[v];
+  const int c = case_s[t];
+  const uint32_t cube = list[t];
+  const int64_t g0 = goff[v];
+  float z[7][3], nn[7][3];
+  int ne = 0;
+  for (int k = 0; k < 7; ++k) {
+    const int e = kDmcTable[c][j][k];
+    if (e < 0) continue;
+    const int64_t flat = (int64_t)t * 12 + e;
+    const int32_t r = ed.idx_map[flat];
+    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
+    const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
+    const float a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
+    const float a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
+    const float w0 = fm(s1, a1), w1 = -fm(s0, a0);
+    const float den = fa(w0, w1);
+    const float zd = fa(s1, -s0);
+    float xa[3], xb[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { xa[a] = ldf(x, 3 * i0 + a); xb[a] = ldf(x, 3 * i1 + a); }
+    crossing_normal(grad, i0, i1, s0, s1, xa, xb, nn[ne]);
+    const int64_t g = g0 + ne;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      out.palpha[3 * g + a] = interp1(xa[a], xb[a], w0, w1, den);
+      out.nalpha[3 * g + a] = nn[ne][a];
+      z[ne][a] = interp1(xa[a], xb[a], s1, -s0, zd);
+    }
+    out.vd_map[flat] = (int32_t)v;
+    ++ne;
+  }
+  // centroid of the crossings; cell centre and bounds
+  float cen[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float sacc = 0.f;
+    for (int q = 0; q < ne; ++q) sacc = fa(sacc, z[q][a]);
+    cen[a] = fd(sacc, (float)(ne > 0 ? ne : 1));
+  }
+  float ctr[3], cmin[3], cmax[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float sacc = 0.f, lo = INFINITY, hi = -INFINITY;
+    for (int k = 0; k < 8; ++k) {
+      const float p = ldf(x, 3 * in.cidx[8 * (int64_t)cube + k] + a);
+      sacc = fa(sacc, p);
+      lo = fminf(lo, p);
+      hi = fmaxf(hi, p);
+    }
+    ctr[a] = fd(sacc, 8.f);
+    cmin[a] = lo;
+    cmax[a] = hi;
+  }
+  // normal equations of the assembled 10 x 3 system
+  const double sl = sqrt((double)lam);
+  double ata[6] = {0, 0, 0, 0, 0, 0}, atb[3] = {0, 0, 0};
+  auto add_row = [&](double r0, double r1, double r2, double rhs) {
+    ata[0] += r0 * r0; ata[1] += r0 * r1; ata[2] += r0 * r2;
+    ata[3] += r1 * r1; ata[4] += r1 * r2; ata[5] += r2 * r2;
+    atb[0] += r0 * rhs; atb[1] += r1 * rhs; atb[2] += r2 * rhs;
+  };
+  bool reg_row_used[3] = {false, false, false};
+  for (int q = 0; q < ne; ++q) {
+    const int row = (q - (ne - 1) + 10) % 10;
+    double rv[3] = {(double)nn[q][0], (double)nn[q][1], (double)nn[q][2]};
+    double rhs = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) rhs += (double)nn[q][a] * ((double)z[q][a] - (double)cen[a]);
+    if (row >= 7) {
+      const int a = row - 7;
+      rv[a] = sl;
+      rhs = sl * ((double)ctr[a] - (double)cen[a]);
+      reg_row_used[a] = true;
+    }
+    add_row(rv[0], rv[1], rv[2], rhs);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (reg_row_used[a]) continue;
+    double rv[3] = {0.0, 0.0, 0.0};
+    rv[a] = sl;
+    add_row(rv[0], rv[1], rv[2], sl * ((double)ctr[a] - (double)cen[a]));
+  }
+  double dl[3];
+  solve_sym3(ata, atb, dl);
+  float vd[3];
+  bool bad = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    vd[a] = fa((float)dl[a], cen[a]);
+    bad = bad || isnan(vd[a]);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float mg = fsb(cmax[a], cmin[a]);
+    bad = bad || vd[a] < fsb(cmin[a], mg) || vd[a] > fa(cmax[a], mg);
+  }
+  if (bad)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) vd[a] = cen[a];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) out.verts[3 * v + a] = vd[a];
+  // L_dev as in the training mode
+  float dist[7], msum = 0.f;
+  for (int q = 0; q < ne; ++q) {
+    float d2 = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float dd = fsb(z[q][a], vd[a]);
+      d2 = fa(d2, fm(dd, dd));
+    }
+    dist[q] = sqrtf(d2);
+    msum = fa(msum, dist[q]);
+  }
+  const float mean = fd(msum, (float)ne);
+  for (int q = 0; q < ne; ++q) out.ldev[g0 + q] = fabsf(fsb(dist[q], mean));
+}
+
+// 2 triangles per quad along the shorter diagonal
+__global__ void quad_eval_kernel(int64_t ne, const uint32_t* __restrict__ qflag, const uint32_t* __restrict__ qoff,
+                                 const uint32_t* __restrict__ rfirst, const uint32_t* __restrict__ vals,
+                                 const int32_t* __restrict__ vd_map, const int64_t* __restrict__ e0,
+                                 const float* __restrict__ sdf, float iso, const float* __restrict__ verts,
+                                 int64_t* __restrict__ faces) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= ne || !qflag[r]) return;
+  const int64_t q = qoff[r];
+  int32_t v[4];
+  for (int k = 0; k < 4; ++k) v[k] = vd_map[vals[rfirst[r] + k]];
+  const bool flip = fsb(sdf[e0[r]], iso) > 0.f;
+  int32_t o[4];
+  if (flip) { o[0] = v[0]; o[1] = v[1]; o[2] = v[3]; o[3] = v[2]; }
+  else { o[0] = v[2]; o[1] = v[3]; o[2] = v[1]; o[3] = v[0]; }
+  float l02 = 0.f, l13 = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float d02 = fsb(verts[3 * (int64_t)o[0] + a], verts[3 * (int64_t)o[2] + a]);
+    const float d13 = fsb(verts[3 * (int64_t)o[1] + a], verts[3 * (int64_t)o[3] + a]);
+    l02 = fa(l02, fm(d02, d02));
+    l13 = fa(l13, fm(d13, d13));
+  }
+  const bool m = sqrtf(l02) < sqrtf(l13);
+  const int s1[6] = {0, 1, 2, 0, 2, 3}, s2[6] = {0, 1, 3, 3, 1, 2};
+  for (int k = 0; k < 6; ++k) faces[6 * q + k] = o[m ? s1[k] : s2[k]];
+}
+
+}  // namespace
+}  // namespace a3d
+
+extern "C" size_t a3d_dmc_corner_gradients_workspace_bytes(int64_t num_cubes, int64_t num_corners) {
+  Workspace ws(nullptr, 0);
+  GradWs w;
+  return carve_grad(w, ws, num_cubes > 0 ? num_cubes : 1, num_corners > 0 ? num_corners : 1) + 256;
+}
+
+extern "C" int a3d_dmc_corner_gradients(const a3d_dmc_inputs* p, void* workspace, size_t workspace_bytes,
+                                        float* gradients, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(p && gradients, A3D_ERR_ARGUMENT, "dmc_corner_gradients: null argument");
+  const int64_t n = p->num_cubes, m = p->num_corners;
+  A3D_REQUIRE(n >= 0 && m >= 0 && n < (1ll << 28) && m < (1ll << 31), A3D_ERR_ARGUMENT,
+              "dmc_corner_gradients: sizes");
+  Workspace ws(workspace, workspace_bytes);
+  GradWs w;
+  carve_grad(w, ws, n > 0 ? n : 1, m > 0 ? m : 1);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "dmc_corner_gradients: workspace too small");
+  if (m == 0) return A3D_OK;
+  A3D_CUDA_TRY(cudaMemsetAsync(gradients, 0, sizeof(float) * 3 * m, s));
+  if (n == 0) return A3D_OK;
+  DmcIn in = make_in(p);
+  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x);
+  A3D_LAUNCH_CHECK();
+  corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, 2.0f / (float)p->resolution, w.x);
+  A3D_LAUNCH_CHECK();
+  const int64_t nk = 12 * n;
+  all_edge_keys_kernel<<<gsz(nk), 256, 0, s>>>(in, w.keys, w.vals);
+  A3D_LAUNCH_CHECK();
+  int bits = 1;
+  while (bits < 64 && ((uint64_t)1 << bits) <= (uint64_t)m * (uint64_t)m) ++bits;
+  bool alt = false;
+  A3D_TRY(radix_sort_pairs<uint64_t>(w.keys, w.vals, w.keys2, w.vals2, nk, 0, bits, w.rs, &alt, s));
+  const uint64_t* keys = alt ? w.keys2 : w.keys;
+  A3D_CUDA_TRY(cudaMemsetAsync(w.acc, 0, sizeof(double) * 9 * m, s));
+  edge_lsq_kernel<<<gsz(nk), 256, 0, s>>>(in, keys, nk, w.x, w.acc);
+  A3D_LAUNCH_CHECK();
+  corner_solve_kernel<<<gsz(m), 256, 0, s>>>(m, w.acc, gradients);
+  A3D_LAUNCH_CHECK();
+  return A3D_OK;
+}
+
+extern "C" int a3d_dmc_emit_qef(const a3d_dmc_inputs* p, void* workspace, size_t workspace_bytes,
+                                const int64_t* counts, const float* corner_gradients, float qef_reg_scale,
+                                float* vertices, int64_t* faces, float* l_dev, float* p_alpha, float* n_alpha,
+                                a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(p && counts && corner_gradients, A3D_ERR_ARGUMENT, "dmc_emit_qef: null argument");
+  const int64_t n = p->num_cubes, m = p->num_corners;
+  Workspace ws(workspace, workspace_bytes);
+  DmcWs w;
+  carve_dmc(w, ws, n > 0 ? n : 1, m > 0 ? m : 1);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "dmc_emit_qef: workspace too small");
+  const int64_t ns = counts[0], ne = counts[2], nq = counts[3], nv = counts[4];
+  if (ns == 0 || nv == 0) return A3D_OK;
+  DmcIn in = make_in(p);
+  EdgeData ed{w.e0, w.e1, w.idx_map};
+  VdOut out{vertices, l_dev, p_alpha, n_alpha, w.vd_map};
+  vd_qef_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, w.x, corner_gradients, qef_reg_scale, nv, w.list, w.case_s,
+                                             w.vd_cube, w.vd_slot, w.goff, ed, out);
+  A3D_LAUNCH_CHECK();
+  if (nq > 0) {
+    quad_eval_kernel<<<gsz(ne), 256, 0, s>>>(ne, w.qflag, w.qoff, w.rfirst, w.vals, w.vd_map, w.e0, p->sdf,
+                                             p->isovalue, vertices, faces);
+    A3D_LAUNCH_CHECK();
+  }
+  return A3D_OK;
+}

@@ -6,8 +6,10 @@ Training mode (a freshly constructed module, inference_mode "auto" or
 a3d_dmc_emit (geometry) and, in backward, a3d_dmc_backward, a hand-written
 adjoint behind torch.autograd.Function that recomputes per-edge quantities.
 Gradients flow to sdf, deform, alpha and beta like the reference's autograd
-graph.  The QEF inference mode and per-vertex features are not provided by
-this build and raise NotImplementedError.
+graph.  The QEF inference mode (a module in eval mode, or inference_mode
+"qef") runs a3d_dmc_corner_gradients (unless corner_gradients are given)
+and a3d_dmc_emit_qef; it is forward-only.  Per-vertex features are not
+provided by this build and raise NotImplementedError.
 """
 
 from __future__ import annotations
@@ -56,6 +58,12 @@ _SIGS = {
                                     ctypes.POINTER(ctypes.c_int64)] + [ctypes.c_void_p] * 6),
     "a3d_dmc_backward": (ctypes.c_int, [ctypes.POINTER(DmcInputs), ctypes.c_void_p, ctypes.c_size_t,
                                         ctypes.POINTER(ctypes.c_int64)] + [ctypes.c_void_p] * 9),
+    "a3d_dmc_corner_gradients_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int64, ctypes.c_int64]),
+    "a3d_dmc_corner_gradients": (ctypes.c_int, [ctypes.POINTER(DmcInputs), ctypes.c_void_p, ctypes.c_size_t,
+                                                ctypes.c_void_p, ctypes.c_void_p]),
+    "a3d_dmc_emit_qef": (ctypes.c_int, [ctypes.POINTER(DmcInputs), ctypes.c_void_p, ctypes.c_size_t,
+                                        ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, ctypes.c_float]
+                         + [ctypes.c_void_p] * 6),
 }
 
 
@@ -134,6 +142,40 @@ class _DmcFn(torch.autograd.Function):
         return g_sdf, g_def, g_alpha, g_beta, None, None, None, None, None
 
 
+class _DmcQefFn(torch.autograd.Function):
+    """QEF inference mode: forward only."""
+
+    @staticmethod
+    def forward(ctx, sdf, deform, vox, cidx, res, iso, wscale, reg, corner_gradients):
+        c = _DmcContext(vox, sdf, cidx, res, deform, None, None, iso, wscale)
+        ns, ng, nq, nv = c.sizes
+        dev = sdf.device
+        lib = _bind()
+        if corner_gradients is None:
+            m = sdf.shape[0]
+            corner_gradients = torch.empty(m, 3, dtype=torch.float32, device=dev)
+            gws = _lib.workspace(lib.a3d_dmc_corner_gradients_workspace_bytes(vox.shape[0], m), dev)
+            _lib.check("a3d_dmc_corner_gradients", lib.a3d_dmc_corner_gradients(
+                ctypes.byref(c.inp), gws.data_ptr(), gws.numel(), corner_gradients.data_ptr(), c.stream))
+        verts = torch.empty(nv, 3, dtype=torch.float32, device=dev)
+        faces = torch.empty(2 * nq, 3, dtype=torch.int64, device=dev)
+        ldev = torch.empty(ng, dtype=torch.float32, device=dev)
+        pa = torch.empty(ng, 3, dtype=torch.float32, device=dev)
+        na = torch.empty(ng, 3, dtype=torch.float32, device=dev)
+        if ns > 0:
+            _lib.check("a3d_dmc_emit_qef", lib.a3d_dmc_emit_qef(
+                ctypes.byref(c.inp), c.ws.data_ptr(), c.ws.numel(), c.counts, corner_gradients.data_ptr(),
+                float(reg), verts.data_ptr(), faces.data_ptr(), ldev.data_ptr(), pa.data_ptr(), na.data_ptr(),
+                c.stream))
+        ctx.mark_non_differentiable(faces)
+        return verts, faces, ldev, pa, na
+
+    @staticmethod
+    def backward(ctx, *grads):
+        raise NotImplementedError("SparseDiffDMC: gradients through the QEF inference mode are not provided; "
+                                  "use the weighted-average (training) mode for optimisation")
+
+
 class SparseDMC(nn.Module):
     """Alias wrapper (reference: sparse_diffdmc.py:20-33)."""
 
@@ -180,8 +222,8 @@ class SparseDiffDMC(nn.Module):
         corner_gradients: Optional[torch.Tensor] = None,
     ) -> SparseDiffDMCOutput:
         mode = ("weighted_avg" if self.training else "qef") if inference_mode == "auto" else inference_mode
-        if mode != "weighted_avg":
-            raise NotImplementedError("SparseDiffDMC: only the weighted-average (training) mode is provided")
+        if mode not in ("weighted_avg", "qef"):
+            raise ValueError(f"SparseDiffDMC: unknown inference_mode {inference_mode!r}")
         if v_features is not None:
             raise NotImplementedError("SparseDiffDMC: vertex features are not provided")
         _lib.require_cuda(sdf, "sdf")
@@ -196,8 +238,16 @@ class SparseDiffDMC(nn.Module):
         vox = voxel_coords.to(device=dev, dtype=torch.int64).contiguous()
         cidx = cube_idx.to(device=dev, dtype=torch.int64).contiguous()
         s = f32(sdf)
-        verts, faces, ldev, pa, na = _DmcFn.apply(s, f32(deform), f32(alpha), f32(beta), vox, cidx, int(resolution),
-                                                  float(isovalue), float(weight_scale))
+        if mode == "qef":
+            # alpha only moves p_alpha; beta and gamma do not enter this mode
+            cg = f32(corner_gradients)
+            verts, faces, ldev, pa, na = _DmcQefFn.apply(s, f32(deform), vox, cidx, int(resolution), float(isovalue),
+                                                         float(weight_scale), float(qef_reg_scale), cg)
+            if alpha is not None:
+                raise NotImplementedError("SparseDiffDMC: alpha weights in the QEF inference mode are not provided")
+        else:
+            verts, faces, ldev, pa, na = _DmcFn.apply(s, f32(deform), f32(alpha), f32(beta), vox, cidx,
+                                                      int(resolution), float(isovalue), float(weight_scale))
         if out_dtype != torch.float32:
             verts, ldev, pa, na = (t.to(out_dtype) for t in (verts, ldev, pa, na))
         return SparseDiffDMCOutput(vertices=verts, faces=faces, L_dev=ldev, p_alpha=pa, n_alpha=na, v_features=None)

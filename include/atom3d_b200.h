@@ -261,6 +261,23 @@ int a3d_dmc_backward(const a3d_dmc_inputs* in, void* workspace, size_t workspace
                      const int64_t* counts, const float* g_vertices, const float* g_l_dev,
                      const float* g_p_alpha, const float* g_n_alpha, float* g_sdf,
                      float* g_deform, float* g_alpha, float* g_beta, a3d_stream_t stream);
+/* QEF inference mode (SparseDiffDMC in eval / inference_mode "qef",
+ * atom3d/mesh_extractor/sparse_diffdmc.py:201-218, :289-513, :798-805).
+ * Corner gradients: least-squares fit over every unique cube edge at each
+ * corner (device [M,3]).  a3d_dmc_emit_qef runs after a3d_dmc_prepare on the
+ * same workspace: vertices [V,3] (no quad centres), faces [2Q,3] (shorter
+ * diagonal), L_dev / p_alpha / n_alpha [G] like a3d_dmc_emit; n_alpha holds
+ * the crossing normals interpolated from the corner gradients.  The dual
+ * vertex solves the least-squares system the reference's
+ * _solve_qef_scatter assembles (its slot scatter places constraint j of k
+ * in row (j - (k-1)) mod 10 of the 10 x 3 matrix). */
+size_t a3d_dmc_corner_gradients_workspace_bytes(int64_t num_cubes, int64_t num_corners);
+int a3d_dmc_corner_gradients(const a3d_dmc_inputs* in, void* workspace, size_t workspace_bytes,
+                             float* gradients, a3d_stream_t stream);
+int a3d_dmc_emit_qef(const a3d_dmc_inputs* in, void* workspace, size_t workspace_bytes,
+                     const int64_t* counts, const float* corner_gradients, float qef_reg_scale,
+                     float* vertices, int64_t* faces, float* l_dev, float* p_alpha, float* n_alpha,
+                     a3d_stream_t stream);
 
 /* Status words of the last a3d_udf / a3d_batch_udf / a3d_udf_noalloc call
  * that used `workspace`, copied to the host after the stream drains:

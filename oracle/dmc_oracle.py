@@ -1,5 +1,7 @@
-"""numpy restatement of SparseDiffDMC.forward in training mode (weighted
-average dual vertices, 4-triangle quad split).  TEST INFRASTRUCTURE ONLY.
+"""numpy restatement of SparseDiffDMC.forward: training mode (weighted
+average dual vertices, 4-triangle quad split) and the QEF inference mode
+(corner gradients, QEF dual vertices, 2-triangle split along the shorter
+diagonal).  TEST INFRASTRUCTURE ONLY.
 
 Follows atom3d/mesh_extractor/sparse_diffdmc.py:
   forward                 :76-232
@@ -12,6 +14,9 @@ Follows atom3d/mesh_extractor/sparse_diffdmc.py:
   _compute_vd (weighted)  :601-780
   _triangulate (training) :782-826
   _linear_interp          :859-871
+  QEF mode: _estimate_corner_gradients :451-513, crossing normals from
+  corner gradients (_compute_vd) :610-650, _solve_qef_scatter :289-389,
+  eval split (_triangulate) :798-805; the 3x3 systems are solved in FP64
 
 dtype=np.float32 reproduces the reference's arithmetic order (pinned
 against its golden outputs); dtype=np.float64 gives the FP64 function used
@@ -39,8 +44,63 @@ def linear_interp(w, x):
     return num / den
 
 
+def qef_solve(n, r, eg_vd, cen, c_ctr, V, lam):
+    """The least-squares system _solve_qef_scatter (:316-367) assembles.
+
+    Its slot scatter (group_offsets.scatter_ with repeated indices keeps the
+    last position on the CPU) gives the j-th of a vertex's k constraints the
+    row (j - (k - 1)) mod 10: the last one row 0, the others rows 9, 8, 7,
+    6, 5, 4.  The regularisation then sets element (7, 0), (8, 1), (9, 2) to
+    sqrt(lambda) -- keeping the other two components of a constraint placed
+    there -- and rows 7-9 of b to sqrt(lambda) (centre - centroid).  This
+    restates that system (it reproduces the reference's CPU outputs); it is
+    solved through its 3x3 normal equations in FP64.
+    """
+    K = n.shape[0]
+    last = np.zeros(V, np.int64)
+    last[eg_vd] = np.arange(K)
+    row = (np.arange(K) - last[eg_vd]) % 10
+    A = np.zeros((V, 10, 3))
+    b = np.zeros((V, 10))
+    A[eg_vd, row] = n
+    b[eg_vd, row] = r
+    sl = np.sqrt(lam)
+    A[:, 7, 0] = sl
+    A[:, 8, 1] = sl
+    A[:, 9, 2] = sl
+    b[:, 7:10] = (c_ctr - cen) * sl
+    ata = np.einsum("vri,vrj->vij", A, A)
+    atb = np.einsum("vri,vr->vi", A, b)
+    return np.linalg.solve(ata, atb[..., None])[..., 0]
+
+
+def corner_gradients(x, sf, ci, dtype=np.float32):
+    """Least-squares SDF gradient at every corner from all incident cube
+    edges (_estimate_corner_gradients)."""
+    f = dtype
+    M = x.shape[0]
+    ue = np.unique(ci[:, CUBE_EDGES].reshape(-1, 2), axis=0)
+    i0, i1 = ue[:, 0], ue[:, 1]
+    ev = x[i1] - x[i0]
+    el = np.maximum(np.sqrt((ev * ev).sum(-1, keepdims=True)), f(1e-8))
+    ed = ev / el
+    gp = (sf[i1] - sf[i0]) / el[:, 0]
+    outer = ed[:, :, None] * ed[:, None, :]
+    fwd = gp[:, None] * ed
+    dtd = np.zeros((M, 3, 3), np.float64)
+    dtb = np.zeros((M, 3), np.float64)
+    np.add.at(dtd, i0, outer)
+    np.add.at(dtd, i1, outer)
+    np.add.at(dtb, i0, fwd)
+    np.add.at(dtb, i1, -fwd)
+    dtd += 1e-4 * np.eye(3)[None]
+    g = np.linalg.solve(dtd, dtb[..., None])[..., 0]
+    g[np.isnan(g).any(-1)] = 0.0
+    return g.astype(f)
+
+
 def forward(voxel_coords, sdf, cube_idx, res, deform=None, beta=None, alpha=None, gamma=None, isovalue=0.0,
-            weight_scale=0.99, dtype=np.float32):
+            weight_scale=0.99, dtype=np.float32, mode="weighted_avg", qef_reg_scale=1e-2, corner_grads=None):
     f = dtype
     vox = np.asarray(voxel_coords, np.int64)
     ci = np.asarray(cube_idx, np.int64)
@@ -144,11 +204,42 @@ def forward(voxel_coords, sdf, cube_idx, res, deform=None, beta=None, alpha=None
     ueg = linear_interp(sg * ag, xg)
     bg = beta_s.reshape(-1)[flat][:, None]
     V = total
-    bsum = np.zeros((V, 1), f)
-    np.add.at(bsum, eg_vd, bg)
-    acc = np.zeros((V, 3), f)
-    np.add.at(acc, eg_vd, ueg * bg)
-    vd = acc / (bsum + f(1e-8))
+    if mode == "qef":
+        G = corner_grads if corner_grads is not None else corner_gradients(x, sf, ci, f)
+        s0e, s1e = ss[:, 0, 0], ss[:, 1, 0]
+        t = np.clip(s0e / (s0e - s1e + f(1e-8)), 0, 1)[:, None]
+        g0, g1 = G[surf_edges[:, 0]], G[surf_edges[:, 1]]
+        w0 = np.sqrt((g0 * g0).sum(-1, keepdims=True)) * (1 - t)
+        w1 = np.sqrt((g1 * g1).sum(-1, keepdims=True)) * t
+        den = w0 + w1
+        gc = (w0 * g0 + w1 * g1) / np.maximum(den, f(1e-8))
+        gc = np.where(den > f(1e-6), gc, normals)
+        all_n = gc / np.maximum(np.sqrt((gc * gc).sum(-1, keepdims=True)), f(1e-12))
+        ng = all_n[ig]
+        cnt_v = np.zeros(V, np.float64)
+        np.add.at(cnt_v, eg_vd, 1.0)
+        cen = np.zeros((V, 3), np.float64)
+        np.add.at(cen, eg_vd, zg.astype(np.float64))
+        cen = cen / np.maximum(cnt_v, 1)[:, None]
+        vd_cube = np.zeros(V, np.int64)
+        vd_cube[eg_vd] = eg_cube
+        cv = x[ci_s[vd_cube]].astype(np.float64)
+        c_ctr, c_min, c_max = cv.mean(1), cv.min(1), cv.max(1)
+        n64 = ng.astype(np.float64)
+        r = (n64 * (zg.astype(np.float64) - cen[eg_vd])).sum(-1)
+        delta = qef_solve(n64, r, eg_vd, cen, c_ctr, V, float(qef_reg_scale))
+        vd = delta + cen
+        bad = np.isnan(vd).any(-1)
+        margin = c_max - c_min
+        bad |= (vd < c_min - margin).any(-1) | (vd > c_max + margin).any(-1)
+        vd[bad] = cen[bad]
+        vd = vd.astype(f)
+    else:
+        bsum = np.zeros((V, 1), f)
+        np.add.at(bsum, eg_vd, bg)
+        acc = np.zeros((V, 3), f)
+        np.add.at(acc, eg_vd, ueg * bg)
+        vd = acc / (bsum + f(1e-8))
     dist = np.sqrt(((zg - vd[eg_vd]) ** 2).sum(-1))
     mean = np.zeros(V, f)
     np.add.at(mean, eg_vd, dist)
@@ -169,6 +260,12 @@ def forward(voxel_coords, sdf, cube_idx, res, deform=None, beta=None, alpha=None
     q[flip] = quad[flip][:, [0, 1, 3, 2]]
     q[~flip] = quad[~flip][:, [2, 3, 1, 0]]
     vq = vd[q.reshape(-1)].reshape(-1, 4, 3)
+    if mode == "qef":
+        d02 = vq[:, 0] - vq[:, 2]
+        d13 = vq[:, 1] - vq[:, 3]
+        m = np.sqrt((d02 * d02).sum(-1)) < np.sqrt((d13 * d13).sum(-1))
+        faces = np.where(m[:, None], q[:, [0, 1, 2, 0, 2, 3]], q[:, [0, 1, 3, 3, 1, 2]]).reshape(-1, 3)
+        return dict(vertices=vd, faces=faces, L_dev=ldev, p_alpha=ueg, n_alpha=ng)
     centre = vq.mean(axis=1).astype(f)
     cidx = np.arange(centre.shape[0]) + V
     verts = np.concatenate([vd, centre], 0)

@@ -99,8 +99,71 @@ def test_dmc_empty_surface():
     assert out.vertices.shape == (0, 3) and out.faces.shape == (0, 3)
 
 
-def test_dmc_eval_mode_not_provided():
+def _eval(g, **kw):
     dmc = SparseDiffDMC(device="cuda").eval()
+    args = {k: torch.from_numpy(v).cuda() for k, v in kw.items()}
+    return dmc(torch.from_numpy(g["vox"]).cuda(), torch.from_numpy(g["sdf"]).cuda(),
+               torch.from_numpy(g["cidx"]).cuda(), int(g["res"]), **args)
+
+
+def test_dmc_qef_mode_matches_reference_golden(golden):
+    g = golden("dmc_small.npz")
+    o = _eval(g, deform=g["deform"])
+    assert np.array_equal(o.faces.cpu().numpy(), g["eval_faces"])
+    # the reference solves each vertex's least squares in FP32 (QR): its
+    # vertices sit up to ~4.4e-6 from the FP64 solution of the same system
+    for k, tol in (("vertices", 1e-5), ("L_dev", 1e-5), ("p_alpha", TOL), ("n_alpha", TOL)):
+        a, b = getattr(o, k).cpu().numpy(), g["eval_" + k]
+        assert a.shape == b.shape, k
+        assert np.abs(a - b).max() <= tol, (k, np.abs(a - b).max())
+
+
+def test_dmc_qef_mode_matches_numpy_oracle_medium():
+    from oracle import dmc_oracle as D
+
+    vox, sdf, cidx, _ = synthetic.dmc_spheres(res=96, seed=7, n_spheres=10)
+    gd = torch.Generator().manual_seed(4)
+    deform = (torch.randn(sdf.shape[0], 3, generator=gd) * 0.003).float()
+    o = SparseDiffDMC(device="cuda").eval()(vox.cuda(), sdf.cuda(), cidx.cuda(), 96, deform=deform.cuda())
+    r = D.forward(vox.numpy(), sdf.numpy(), cidx.numpy(), 96, deform=deform.numpy(), mode="qef")
+    assert np.array_equal(o.faces.cpu().numpy(), r["faces"])
+    for k in ("vertices", "L_dev", "p_alpha", "n_alpha"):
+        assert np.abs(getattr(o, k).cpu().numpy() - r[k]).max() <= TOL, (k, np.abs(getattr(o, k).cpu().numpy() - r[k]).max())
+
+
+def test_dmc_corner_gradients_and_given_gradients():
+    from oracle import dmc_oracle as D
+    from atom3d_b200.mesh_extractor import sparse_diffdmc as M
+
+    vox, sdf, cidx, _ = synthetic.dmc_spheres(res=64, seed=8, n_spheres=6)
+    x = D.CUBE_CORNERS
+    # oracle corner gradients on the undeformed grid
+    pos = np.zeros((sdf.shape[0], 3), np.float32)
+    pos[cidx.numpy().reshape(-1)] = (vox.numpy()[:, None, :] + x[None]).reshape(-1, 3)
+    world = pos * np.float32(2.0 / 64) - np.float32(1.0)
+    G = D.corner_gradients(world, sdf.numpy(), cidx.numpy())
+    c = M._DmcContext(vox.cuda(), sdf.cuda(), cidx.cuda(), 64, None, None, None, 0.0, 0.99)
+    got = torch.empty(sdf.shape[0], 3, device="cuda")
+    lib = M._bind()
+    from atom3d_b200 import _lib
+
+    ws = _lib.workspace(lib.a3d_dmc_corner_gradients_workspace_bytes(vox.shape[0], sdf.shape[0]), "cuda")
+    _lib.check("a3d_dmc_corner_gradients", lib.a3d_dmc_corner_gradients(
+        __import__("ctypes").byref(c.inp), ws.data_ptr(), ws.numel(), got.data_ptr(), c.stream))
+    assert np.allclose(got.cpu().numpy(), G, rtol=1e-5, atol=1e-5)
+    # caller-supplied gradients are used as given
+    Gs = (G * np.float32(0.5)).astype(np.float32)
+    o = SparseDiffDMC(device="cuda").eval()(vox.cuda(), sdf.cuda(), cidx.cuda(), 64,
+                                            corner_gradients=torch.from_numpy(Gs).cuda())
+    r = D.forward(vox.numpy(), sdf.numpy(), cidx.numpy(), 64, mode="qef", corner_grads=Gs)
+    assert np.array_equal(o.faces.cpu().numpy(), r["faces"])
+    assert np.abs(o.vertices.cpu().numpy() - r["vertices"]).max() <= TOL
+
+
+def test_dmc_qef_mode_is_forward_only():
+    g = synthetic.dmc_spheres(res=32, seed=9, n_spheres=3)
+    vox, sdf, cidx, _ = g
+    s = sdf.cuda().requires_grad_(True)
+    o = SparseDiffDMC(device="cuda").eval()(vox.cuda(), s, cidx.cuda(), 32)
     with pytest.raises(NotImplementedError):
-        dmc(torch.zeros(1, 3, dtype=torch.long, device="cuda"), torch.ones(8, device="cuda"),
-            torch.arange(8, device="cuda").view(1, 8), 4)
+        (o.vertices ** 2).sum().backward()

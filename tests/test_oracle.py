@@ -168,3 +168,23 @@ def test_ray_oracle_matches_reference_cpu_path(golden, orc):
     assert np.allclose(t[both], g["t"][both], rtol=1e-5, atol=0)
     assert (fid[both] == g["face_ids"][both]).mean() > 0.99
     assert np.allclose(hp[both], g["hit_points"][both], atol=1e-5)
+
+
+@pytest.mark.parametrize("mode", ["train", "ab", "eval"])
+def test_dmc_oracle_matches_reference_golden(golden, mode):
+    """The numpy restatement of SparseDiffDMC.forward against the reference's
+    own outputs: training mode with a deformation, training mode with alpha
+    and beta, and the QEF inference mode (which the reference solves in FP32
+    by QR: its vertices sit up to ~4.4e-6 from the FP64 solution)."""
+    from oracle import dmc_oracle as D
+
+    g = golden("dmc_small.npz")
+    kw = {"train": dict(deform=g["deform"]), "ab": dict(alpha=g["alpha"], beta=g["beta"]),
+          "eval": dict(deform=g["deform"], mode="qef")}[mode]
+    r = D.forward(g["vox"], g["sdf"], g["cidx"], int(g["res"]), **kw)
+    assert np.array_equal(r["faces"], g[mode + "_faces"])
+    tol = 1e-5 if mode == "eval" else 2e-6
+    keys = ("vertices", "L_dev") if mode == "ab" else ("vertices", "L_dev", "p_alpha", "n_alpha")
+    for k in keys:
+        assert r[k].shape == g[f"{mode}_{k}"].shape, k
+        assert np.abs(r[k] - g[f"{mode}_{k}"]).max() <= tol, (k, np.abs(r[k] - g[f"{mode}_{k}"]).max())
