@@ -1,3 +1,2 @@
-from .sparse_flood_fill import flood_fill_3d_sparse, sparse_flood_fill
-
-__all__ = ["sparse_flood_fill", "flood_fill_3d_sparse"]
+from .sparse_flood_fill import (construct_surface_dual_graph, flood_fill_3d_sparse, get_dam_wet_corners,
+                                get_dam_wet_edges, get_dam_wet_faces, sparse_flood_fill)

@@ -1,10 +1,15 @@
-"""Sparse flood fill (drop-in for atom3d/apps/sparse_flood_fill.py:34-166 and
-atom3d/kernels/flood_fill.py:118-258).
+"""Sparse flood fill and the surface dual graph (drop-in for
+atom3d/apps/sparse_flood_fill.py:34-291 and atom3d/kernels/flood_fill.py:
+118-258).
 
 sparse_flood_fill: octree SAT descent for the dam voxels, then the native
 bit-volume flood fill and k-ring classification (a3d_flood_*).  Output
 dictionary, dtypes (int32 [K,3]) and ordering (lexicographic (x, y, z), like
 torch.nonzero / torch.unique(dim=0)) are the reference's.
+
+construct_surface_dual_graph and get_dam_wet_faces / _edges / _corners run
+on bit volumes over the cells' bounding box (a3d_dual_graph_*, a3d_dam_wet):
+no sort, no dense resolution^3 mask.
 """
 
 from __future__ import annotations
@@ -37,6 +42,10 @@ class FloodGeom(ctypes.Structure):
     ]
 
 
+class DualGeom(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_int64 * 3), ("hi", ctypes.c_int64 * 3), ("resolution", ctypes.c_int64)]
+
+
 _SIGS = {
     "a3d_flood_bbox": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p,
                                       ctypes.c_size_t, ctypes.c_void_p]),
@@ -48,6 +57,21 @@ _SIGS = {
                                          ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     "a3d_flood_test": (ctypes.c_int, [ctypes.POINTER(FloodGeom), ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
                                       ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
+    "a3d_cells_bbox": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64), ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, ctypes.c_size_t,
+                                      ctypes.c_void_p]),
+    "a3d_dual_workspace_bytes": (ctypes.c_size_t, [ctypes.POINTER(DualGeom)]),
+    "a3d_dual_graph_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64),
+                                            ctypes.c_int, ctypes.POINTER(DualGeom), ctypes.c_void_p,
+                                            ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]),
+    "a3d_dual_graph_emit": (ctypes.c_int, [ctypes.POINTER(DualGeom), ctypes.c_void_p, ctypes.c_size_t,
+                                           ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(ctypes.c_float),
+                                           ctypes.POINTER(ctypes.c_float), ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "a3d_dam_wet_workspace_bytes": (ctypes.c_size_t, [ctypes.POINTER(ctypes.c_int64)]),
+    "a3d_dam_wet": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                   ctypes.POINTER(ctypes.c_int64), ctypes.c_int64, ctypes.c_void_p, ctypes.c_size_t,
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 
@@ -195,4 +219,134 @@ def sparse_flood_fill(
     return out
 
 
-__all__ = ["sparse_flood_fill", "flood_fill_3d_sparse", "SIGN_WATER", "SIGN_DRY"]
+# ---------------------------------------------------------------------------
+# surface dual graph and dam wet masks
+# ---------------------------------------------------------------------------
+def _cells32(t: torch.Tensor, what: str) -> torch.Tensor:
+    _lib.require_cuda(t, what)
+    if t.dim() != 2 or t.shape[1] != 3:
+        raise ValueError(f"{what} must be [K,3], got {tuple(t.shape)}")
+    return t.to(torch.int32).contiguous()
+
+
+def _bbox(lib, cells, dev):
+    """(lo, hi) over the lists, None when all are empty (synchronises)."""
+    ptrs = (ctypes.c_void_p * len(cells))(*[c.data_ptr() for c in cells])
+    cnts = (ctypes.c_int64 * len(cells))(*[c.shape[0] for c in cells])
+    bb = (ctypes.c_int64 * 6)()
+    ws = _lib.workspace(64, dev)
+    _lib.check("a3d_cells_bbox", lib.a3d_cells_bbox(ptrs, cnts, len(cells), bb, ws.data_ptr(), ws.numel(),
+                                                    _lib.stream_ptr(dev)))
+    if bb[0] > bb[3]:
+        return None
+    return list(bb[:3]), list(bb[3:])
+
+
+def _check_range(box, resolution, what):
+    lo, hi = box
+    if min(lo) < 0 or max(hi) >= resolution:
+        raise ValueError(f"{what}: coordinates must lie in [0, {resolution}), got range {lo}..{hi}")
+
+
+def _dam_wet(dam_ijk, collision_ijk, resolution, which):
+    dev = dam_ijk.device
+    width = {"faces": 6, "edges": 12, "corners": 8}[which]
+    if len(dam_ijk) == 0:
+        return torch.zeros((0, width), dtype=torch.bool, device=dev)
+    lib = _bind()
+    dam = _cells32(dam_ijk, "dam_ijk")
+    out = torch.empty((dam.shape[0], width), dtype=torch.bool, device=dev)
+    coll = _cells32(collision_ijk, "collision_ijk") if len(collision_ijk) else torch.empty(0, 3, dtype=torch.int32,
+                                                                                           device=dev)
+    box = _bbox(lib, [coll], dev) if coll.shape[0] else None
+    bb = (ctypes.c_int64 * 6)()
+    if box is not None:
+        _check_range(box, resolution, "collision_ijk")
+        for a in range(3):
+            bb[a], bb[3 + a] = box[0][a], box[1][a]
+    ws = _lib.workspace(lib.a3d_dam_wet_workspace_bytes(bb) if box is not None else 256, dev)
+    ptr = {k: (out.data_ptr() if k == which else None) for k in ("faces", "edges", "corners")}
+    _lib.check("a3d_dam_wet", lib.a3d_dam_wet(dam.data_ptr(), dam.shape[0], coll.data_ptr(), coll.shape[0], bb,
+                                              int(resolution), ws.data_ptr(), ws.numel(), ptr["faces"],
+                                              ptr["edges"], ptr["corners"], _lib.stream_ptr(dev)))
+    return out
+
+
+def get_dam_wet_faces(dam_ijk: torch.Tensor, collision_ijk: torch.Tensor, resolution: int) -> torch.Tensor:
+    """bool [N,6]: the face neighbour (+x,-x,+y,-y,+z,-z) of each dam cell is a
+    collision cell (atom3d/apps/sparse_flood_fill.py:169-185)."""
+    return _dam_wet(dam_ijk, collision_ijk, resolution, "faces")
+
+
+def get_dam_wet_edges(dam_ijk: torch.Tensor, collision_ijk: torch.Tensor, resolution: int) -> torch.Tensor:
+    """bool [N,12]: one of the 3 cells sharing each edge is a collision cell
+    (atom3d/apps/sparse_flood_fill.py:188-204; EDGE_NEIGHBOR_OFFSETS)."""
+    return _dam_wet(dam_ijk, collision_ijk, resolution, "edges")
+
+
+def get_dam_wet_corners(dam_ijk: torch.Tensor, collision_ijk: torch.Tensor, resolution: int) -> torch.Tensor:
+    """bool [N,8]: one of the 7 cells sharing each corner is a collision cell
+    (atom3d/apps/sparse_flood_fill.py:207-223; CORNER_NEIGHBOR_OFFSETS)."""
+    return _dam_wet(dam_ijk, collision_ijk, resolution, "corners")
+
+
+def construct_surface_dual_graph(
+    dam_ijk: torch.Tensor,
+    collision_ijk: torch.Tensor,
+    dry_adjacent_ijk: Optional[torch.Tensor],
+    octree: OctreeIndexer,
+) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor]:
+    """Topology of the active cells (dam, collision and dry-adjacent union).
+
+    Returns, like atom3d/apps/sparse_flood_fill.py:226-291:
+      voxelgrid_vertices float32 [V,3]  octree.bounds[0] + vertices_ijk * cell
+      vertices_ijk       int64 [V,3]    unique cube corners, lexicographic
+      cube_idx           int64 [N,8]    corners of each cell (CUBE_CORNERS order)
+      adj_idx            int64 [N,6]    face neighbours (+x,-x,+y,-y,+z,-z) or -1
+      active_cells_ijk   [N,3]          unique cells, lexicographic; the
+                                        promoted dtype of the inputs
+    Cells must lie in [0, 2^max_level).
+    """
+    lists = [c for c in (dam_ijk, collision_ijk, dry_adjacent_ijk) if c is not None and len(c) > 0]
+    if not lists:
+        raise RuntimeError("construct_surface_dual_graph: no active cells (all inputs are empty)")
+    dev = lists[0].device
+    out_dtype = lists[0].dtype
+    for c in lists[1:]:
+        out_dtype = torch.promote_types(out_dtype, c.dtype)
+    lib = _bind()
+    cells = [_cells32(c, "cell list") for c in lists]
+    R = 2 ** int(octree.max_level)
+    box = _bbox(lib, cells, dev)
+    _check_range(box, R, "construct_surface_dual_graph")
+    g = DualGeom()
+    for a in range(3):
+        g.lo[a], g.hi[a] = box[0][a], box[1][a]
+    g.resolution = R
+    ws = _lib.workspace(lib.a3d_dual_workspace_bytes(ctypes.byref(g)), dev)
+    stream = _lib.stream_ptr(dev)
+    ptrs = (ctypes.c_void_p * len(cells))(*[c.data_ptr() for c in cells])
+    cnts = (ctypes.c_int64 * len(cells))(*[c.shape[0] for c in cells])
+    nv = (ctypes.c_int64 * 2)()
+    _lib.check("a3d_dual_graph_count", lib.a3d_dual_graph_count(ptrs, cnts, len(cells), ctypes.byref(g),
+                                                                ws.data_ptr(), ws.numel(), nv, stream))
+    n, v = int(nv[0]), int(nv[1])
+    # the reference's float32 (hi - lo) / R and lo, as host floats
+    b = octree.bounds.to(torch.float32)
+    cmin = b[0].tolist()
+    cell = ((b[1] - b[0]) / float(R)).tolist()
+    cells_ijk = torch.empty((n, 3), dtype=torch.int32, device=dev)
+    vijk = torch.empty((v, 3), dtype=torch.int64, device=dev)
+    world = torch.empty((v, 3), dtype=torch.float32, device=dev)
+    cube_idx = torch.empty((n, 8), dtype=torch.int64, device=dev)
+    adj_idx = torch.empty((n, 6), dtype=torch.int64, device=dev)
+    _lib.check("a3d_dual_graph_emit", lib.a3d_dual_graph_emit(
+        ctypes.byref(g), ws.data_ptr(), ws.numel(), n, v, (ctypes.c_float * 3)(*cmin), (ctypes.c_float * 3)(*cell),
+        cells_ijk.data_ptr(), vijk.data_ptr(), world.data_ptr(), cube_idx.data_ptr(), adj_idx.data_ptr(), stream))
+    if out_dtype != torch.int32:
+        cells_ijk = cells_ijk.to(out_dtype)
+    return world, vijk, cube_idx, adj_idx, cells_ijk
+
+
+__all__ = ["sparse_flood_fill", "flood_fill_3d_sparse", "get_dam_wet_faces", "get_dam_wet_edges",
+           "get_dam_wet_corners", "construct_surface_dual_graph", "SIGN_WATER", "SIGN_DRY"]

@@ -40,3 +40,29 @@ NEIGHBOR_OFFSETS_26 = torch.tensor(
 SIGN_WATER = 1
 SIGN_DRY = -1
 SIGN_DAM_DEFAULT = -1
+
+# Neighbours sharing edge e of a cell (4 edges per axis, x-, y-, then
+# z-aligned).  The two axes p < q perpendicular to the edge get a + or -
+# offset by bit 0 and bit 1 of e % 4; the neighbours are p, q and p+q.
+def _edge_neighbours():
+    rows = []
+    for e in range(12):
+        axis, k = divmod(e, 4)
+        p, q = [a for a in range(3) if a != axis]
+        op, oq = [0, 0, 0], [0, 0, 0]
+        op[p] = -1 if k & 1 else 1
+        oq[q] = -1 if k & 2 else 1
+        rows.append([op, oq, [op[a] + oq[a] for a in range(3)]])
+    return rows
+
+
+EDGE_NEIGHBOR_OFFSETS = torch.tensor(_edge_neighbours(), dtype=torch.int32)
+
+# Neighbours sharing corner c: with s = CUBE_CORNER_SIGNS[c], the faces
+# (sx,0,0), (0,sy,0), (0,0,sz), the edges (sx,sy,0), (sx,0,sz), (0,sy,sz) and
+# the corner (sx,sy,sz).
+CORNER_NEIGHBOR_OFFSETS = torch.tensor(
+    [[[sx, 0, 0], [0, sy, 0], [0, 0, sz], [sx, sy, 0], [sx, 0, sz], [0, sy, sz], [sx, sy, sz]]
+     for sx, sy, sz in CUBE_CORNER_SIGNS.int().tolist()],
+    dtype=torch.int32,
+)

@@ -20,6 +20,11 @@ generated here from a fixed seed:
   (c ~ U[-0.7, 0.7]^3, r ~ U[0.05, 0.2]) + N(0, 1e-3), sampled at the
   unique corners of the cubes of a [-1, 1]^3 grid whose centre satisfies
   |sdf| <= 2h + sqrt(3)/2 h (h = 2 / res).
+* ``shell_cells`` — flood-fill-like cell sets of a sphere of radius
+  0.3 res about a jittered centre: dam = cells whose centre lies within 0.9
+  of the sphere, collision = the next shell outside (0.9..1.9), dry
+  adjacent = the next shell inside; plus cells on the grid's faces and
+  duplicates across the lists.
 """
 
 from __future__ import annotations
@@ -268,3 +273,30 @@ def dmc_spheres(res: int = 512, seed: int = 5, n_spheres: int = 32, noise: float
         sdf[s:s + step] = spheres_sdf(vx[s:s + step], centres, radii)
     sdf = sdf + noise * torch.randn(sdf.shape[0], generator=g, dtype=torch.float64)
     return (vox.to(device), sdf.float().to(device), inv.view(-1, 8).to(device), vijk.to(device))
+
+
+def shell_cells(res: int = 32, seed: int = 6, face_cells: int = 24):
+    """(dam, collision, dry_adjacent) int32 [K,3] cell lists in [0, res)^3.
+
+    Besides the three shells, collision also holds ``face_cells`` random
+    cells on the six faces of the grid (where the reference's linear-key
+    neighbour lookup wraps) and a few dam cells again (duplicates across
+    lists); dry_adjacent repeats some of its own rows.
+    """
+    g = torch.Generator().manual_seed(seed)
+    c = res / 2 + (torch.rand(3, generator=g, dtype=torch.float64) - 0.5) * 0.1 * res
+    r = 0.3 * res
+    ijk = torch.stack(torch.meshgrid(*[torch.arange(res)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    d = ((ijk.double() + 0.5) - c).norm(dim=1) - r
+    dam = ijk[d.abs() < 0.9]
+    coll = ijk[(d >= 0.9) & (d < 1.9)]
+    dry = ijk[(d <= -0.9) & (d > -1.9)]
+    fc = torch.randint(0, res, (face_cells, 3), generator=g)
+    axis = torch.randint(0, 3, (face_cells,), generator=g)
+    side = torch.randint(0, 2, (face_cells,), generator=g) * (res - 1)
+    fc[torch.arange(face_cells), axis] = side
+    pick = torch.randperm(dam.shape[0], generator=g)[: max(1, dam.shape[0] // 20)]
+    coll = torch.cat([coll, fc, dam[pick]])
+    coll = coll[torch.randperm(coll.shape[0], generator=g)]
+    dry = torch.cat([dry, dry[: dry.shape[0] // 10]])
+    return dam.int().contiguous(), coll.int().contiguous(), dry.int().contiguous()

@@ -222,6 +222,55 @@ int a3d_flood_extract(const a3d_flood_geom* geom, void* workspace, size_t worksp
 int a3d_flood_test(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes,
                    int label, const int64_t* ijk, int64_t n, uint8_t* out, a3d_stream_t stream);
 
+/* ---- surface dual graph and dam wet masks -------------------------------- */
+/* Replace construct_surface_dual_graph and get_dam_wet_faces / _edges /
+ * _corners (atom3d/apps/sparse_flood_fill.py:169-291).  Cells are int32
+ * [n,3] grid coordinates in [0, resolution). */
+
+/* bbox_out (host, 6): min xyz, max xyz over up to 8 cell lists (host arrays
+ * of device pointers and counts); synchronises.  An all-empty union gives
+ * min > max.  workspace >= 64 bytes. */
+int a3d_cells_bbox(const int32_t* const* lists, const int64_t* counts, int num_lists,
+                   int64_t* bbox_out, void* workspace, size_t workspace_bytes,
+                   a3d_stream_t stream);
+
+typedef struct a3d_dual_geom {
+  int64_t lo[3];       /* bounding box of the active cells, inclusive */
+  int64_t hi[3];
+  int64_t resolution;  /* R = 2^max_level of the octree */
+} a3d_dual_geom;
+
+size_t a3d_dual_workspace_bytes(const a3d_dual_geom* geom);
+/* Marks the union of the lists (the active cells) and their cube corners;
+ * counts_out (host, 2): unique cells N, unique vertices V.  Synchronises.
+ * The marked sets stay in the workspace for a3d_dual_graph_emit. */
+int a3d_dual_graph_count(const int32_t* const* lists, const int64_t* counts, int num_lists,
+                         const a3d_dual_geom* geom, void* workspace, size_t workspace_bytes,
+                         int64_t* counts_out, a3d_stream_t stream);
+/* Writes, in the reference's orders:
+ *   cells_ijk      int32 [N,3]  active cells, lexicographic (x, y, z)
+ *   vertices_ijk   int64 [V,3]  cube corners, lexicographic
+ *   vertices_world f32   [V,3]  origin + ijk * cell (product, then sum)
+ *   cube_idx       int64 [N,8]  corner c = (c&1, (c>>1)&1, (c>>2)&1)
+ *   adj_idx        int64 [N,6]  +x,-x,+y,-y,+z,-z neighbour or -1, found by
+ *                               the reference's linear key (x*R + y)*R + z
+ * origin and cell are host float[3]; cube_idx and adj_idx 16-byte aligned. */
+int a3d_dual_graph_emit(const a3d_dual_geom* geom, void* workspace, size_t workspace_bytes,
+                        int64_t num_cells, int64_t num_vertices, const float* origin,
+                        const float* cell, int32_t* cells_ijk, int64_t* vertices_ijk,
+                        float* vertices_world, int64_t* cube_idx, int64_t* adj_idx,
+                        a3d_stream_t stream);
+
+/* collision_bbox: a3d_cells_bbox of the collision cells. */
+size_t a3d_dam_wet_workspace_bytes(const int64_t* collision_bbox);
+/* Per dam cell, whether a neighbour sharing each face [n,6] (+x,-x,+y,-y,
+ * +z,-z), edge [n,12] or corner [n,8] is a collision cell (uint8 0/1; each
+ * output nullable).  Neighbours outside [0, resolution) are never wet. */
+int a3d_dam_wet(const int32_t* dam_ijk, int64_t n, const int32_t* collision_ijk, int64_t m,
+                const int64_t* collision_bbox, int64_t resolution, void* workspace,
+                size_t workspace_bytes, uint8_t* wet_faces, uint8_t* wet_edges,
+                uint8_t* wet_corners, a3d_stream_t stream);
+
 /* ---- sparse differentiable dual marching cubes ------------------------ */
 /* Replaces SparseDiffDMC.forward in training mode (weighted-average dual
  * vertices, 4-triangle quad split) and its autograd backward

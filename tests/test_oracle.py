@@ -188,3 +188,21 @@ def test_dmc_oracle_matches_reference_golden(golden, mode):
     for k in keys:
         assert r[k].shape == g[f"{mode}_{k}"].shape, k
         assert np.abs(r[k] - g[f"{mode}_{k}"]).max() <= tol, (k, np.abs(r[k] - g[f"{mode}_{k}"]).max())
+
+
+@pytest.mark.parametrize("case", ["shell", "dense", "nodry"])
+def test_dual_oracle_matches_reference_golden(golden, case):
+    """The numpy restatement of construct_surface_dual_graph and the dam wet
+    masks against the reference's own outputs (three cell sets, including
+    neighbours whose linear key wraps at the grid's faces)."""
+    from oracle import dual_oracle as D
+
+    g = golden("dual_small.npz")
+    lv = int(g[f"{case}_level"])
+    dry = g[f"{case}_dry"] if f"{case}_dry" in g else None
+    w, v, ci, adj, cells = D.dual_graph(g[f"{case}_dam"], g[f"{case}_coll"], dry, lv, g["bounds"])
+    for k, a in (("world", w), ("vijk", v), ("cube_idx", ci), ("adj_idx", adj), ("cells", cells)):
+        assert np.array_equal(a, g[f"{case}_{k}"]), k
+    R = 2 ** lv
+    for fn, k in ((D.dam_wet_faces, "faces"), (D.dam_wet_edges, "edges"), (D.dam_wet_corners, "corners")):
+        assert np.array_equal(fn(g[f"{case}_dam"], g[f"{case}_coll"], R), g[f"{case}_wet_{k}"]), k
