@@ -9,7 +9,8 @@ computation runs in libatom3d_b200.so on the GPU:
 * ``udf`` / ``sdf``: one fused traversal launch (a3d_udf), sign included;
 * ``udf(return_grad=True)``: a torch.autograd.Function whose backward is the
   hand-written adjoint kernel (a3d_udf_backward) for points and vertices;
-* ``intersect_aabb(mode=0)``: SAT any-hit over the BVH (a3d_aabb_hit).
+* ``intersect_aabb``: SAT any-hit over the BVH (mode 0, a3d_aabb_hit) and
+  the (box, face) pairs, clipped for modes 2-3 (a3d_aabb_pairs_*).
 
 There is no CPU path: a CPU device raises.
 """
@@ -255,14 +256,58 @@ class MeshBVH:
 
     # ------------------------------------------------------------ box queries
     def intersect_aabb(self, aabb_min: torch.Tensor, aabb_max: torch.Tensor, mode: int = 1) -> AABBIntersectResult:
-        """Triangle/box intersection.  mode 0: SAT hit mask (sat_eps 1e-6).
+        """Triangle/box intersection (atom3d/core/mesh_bvh.py:297-479).
 
-        Pair outputs (modes 1-3, polygon clipping) are not provided by this
-        build and raise NotImplementedError.
+        mode 0: hit mask (some face passes SAT, sat_eps 1e-6)
+        mode 1: hit mask + (aabb_ids, face_ids) int32 pairs passing SAT
+        mode 2: pairs whose Sutherland-Hodgman clip against the box is
+                non-empty (int64 ids), with centroids [P,3] (polygon mean
+                clamped to the box, projected onto the triangle), areas [P]
+                and poly_counts [P] int32; hit = box has such a pair
+        mode 3: mode 2 plus poly_verts [P,8,3] (zero padded)
+        Pairs come grouped by box in ascending order (tree order within a
+        box); the reference returns them in atomic-counter order.
         """
-        if mode != 0:
-            raise NotImplementedError("intersect_aabb: only mode=0 (hit mask) is provided by atom3d_b200")
-        return AABBIntersectResult(hit=self.aabb_hit(aabb_min, aabb_max))
+        if mode == 0:
+            return AABBIntersectResult(hit=self.aabb_hit(aabb_min, aabb_max))
+        if mode not in (1, 2, 3):
+            raise ValueError(f"intersect_aabb: mode must be 0, 1, 2 or 3, got {mode}")
+        _lib.require_cuda(aabb_min, "aabb_min")
+        mn = aabb_min.detach().contiguous().float()
+        mx = aabb_max.detach().contiguous().float()
+        n = int(mn.shape[0])
+        dev = self.device
+        hit = torch.zeros(n, dtype=torch.bool, device=dev)
+        idt = torch.int32 if mode == 1 else torch.int64
+        if n == 0:
+            e = torch.empty(0, dtype=idt, device=dev)
+            return AABBIntersectResult(hit=hit, aabb_ids=e, face_ids=e.clone()) if mode == 1 else \
+                AABBIntersectResult(hit=hit)
+        lib = _lib.lib()
+        ws = _lib.workspace(lib.a3d_aabb_pairs_workspace_bytes(n), dev)
+        stream = _lib.stream_ptr(dev)
+        totals = (ctypes.c_int64 * 2)()
+        _lib.call("a3d_aabb_pairs_count", ctypes.byref(self._bvh.view), mn.data_ptr(), mx.data_ptr(), n, mode,
+                  hit.data_ptr(), ws.data_ptr(), ws.numel(), totals, stream)
+        P, n_sat = int(totals[0]), int(totals[1])
+        if mode >= 2 and n_sat == 0:
+            return AABBIntersectResult(hit=hit)  # no SAT candidate at all: the reference returns the mask alone
+        a_ids = torch.empty(P, dtype=idt, device=dev)
+        f_ids = torch.empty(P, dtype=idt, device=dev)
+        pc = cen = ar = pv = None
+        if mode >= 2:
+            pc = torch.empty(P, dtype=torch.int32, device=dev)
+            cen = torch.empty(P, 3, dtype=torch.float32, device=dev)
+            ar = torch.empty(P, dtype=torch.float32, device=dev)
+        if mode == 3:
+            pv = torch.empty(P, 8, 3, dtype=torch.float32, device=dev)
+        if P:
+            ptr = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
+            _lib.call("a3d_aabb_pairs_write", ctypes.byref(self._bvh.view), mn.data_ptr(), mx.data_ptr(), n, mode,
+                      ws.data_ptr(), ws.numel(), a_ids.data_ptr(), f_ids.data_ptr(), ptr(pc), ptr(cen), ptr(ar),
+                      ptr(pv), stream)
+        return AABBIntersectResult(hit=hit, aabb_ids=a_ids, face_ids=f_ids, centroids=cen, areas=ar, poly_verts=pv,
+                                   poly_counts=pc)
 
     def aabb_hit(self, aabb_min: torch.Tensor, aabb_max: torch.Tensor) -> torch.Tensor:
         _lib.require_cuda(aabb_min, "aabb_min")

@@ -163,6 +163,28 @@ int a3d_aabb_hit(const a3d_bvh_view* bvh, const float* box_min, const float* box
                  int64_t n, uint8_t* hit, void* workspace, size_t workspace_bytes,
                  a3d_stream_t stream);
 
+/* Replaces the pair outputs of MeshBVH.intersect_aabb modes 1-3
+ * (atom3d/core/mesh_bvh.py:297-479): bvh_aabb_intersect_kernel's
+ * (box, face) pairs (atom3d/kernels/bvh_kernels.cu:555-610) and
+ * sat_clip_polygon_kernel (atom3d/kernels/cumtv_kernels.cu:209-460).
+ *   mode 1: faces passing SAT;  modes 2, 3: faces passing SAT whose clip
+ *   against the box (eps 1e-8) is non-empty.
+ * Count pass: hit[n] (uint8) = box has a pair; totals_out (host, 2): [0]
+ * pairs, [1] faces passing SAT over all boxes.  Synchronises.  The counts
+ * stay in the workspace for the write pass, which writes the pairs grouped
+ * by box (ascending), in tree order within a box:
+ *   aabb_ids, face_ids  int32 [P] (mode 1) or int64 [P] (modes 2, 3)
+ *   poly_counts int32 [P], centroids f32 [P,3], areas f32 [P]  (modes 2, 3)
+ *   poly_verts f32 [P,8,3], 16-byte aligned, zero padded      (mode 3) */
+size_t a3d_aabb_pairs_workspace_bytes(int64_t n);
+int a3d_aabb_pairs_count(const a3d_bvh_view* bvh, const float* box_min, const float* box_max,
+                         int64_t n, int mode, uint8_t* hit, void* workspace,
+                         size_t workspace_bytes, int64_t* totals_out, a3d_stream_t stream);
+int a3d_aabb_pairs_write(const a3d_bvh_view* bvh, const float* box_min, const float* box_max,
+                         int64_t n, int mode, void* workspace, size_t workspace_bytes,
+                         void* aabb_ids, void* face_ids, int32_t* poly_counts, float* centroids,
+                         float* areas, float* poly_verts, a3d_stream_t stream);
+
 /* Replaces OctreeIndexer.octree_traverse (atom3d/grid/octree_indexer.py:470-509):
  * coarse-to-fine candidate voxels at max_level in the reference's order
  * (meshgrid 'ij' at min_level, then parent-major x 8 CUBE_CORNERS children,

@@ -29,6 +29,16 @@
  *   orc_flood_fill         flood_fill_kernel + host BFS loop
  *                          (atom3d/kernels/flood_fill_kernels.cu:21-175),
  *                          sequential BFS with the same label rules.
+ *   orc_clip_pair          sat_clip_polygon_kernel + clip_with_plane
+ *                          (atom3d/kernels/cumtv_kernels.cu:209-265,
+ *                          :277-460): Sutherland-Hodgman clip of a triangle
+ *                          against the box's 6 planes, centroid projected
+ *                          onto the triangle, fan area.
+ *   orc_aabb_pair_counts / orc_aabb_pairs_fill
+ *                          MeshBVH.intersect_aabb modes 1-3
+ *                          (atom3d/core/mesh_bvh.py:297-479) by brute force:
+ *                          per box, faces in order, SAT then (modes 2-3)
+ *                          the clip.
  */
 #include <math.h>
 #include <stdint.h>
@@ -790,4 +800,172 @@ void orc_parity_votes(const float* V, const int32_t* F, int64_t nf, const float*
                       int ndir, float max_t, float coalesce, int32_t* votes) {
   parity_ctx c = {V, F, nf, P, dirs, ndir, max_t, coalesce, votes};
   par_for(n, 4, parity_body, &c);
+}
+
+
+/* ---------------- triangle/box clipping (intersect_aabb modes 2-3) ------ */
+#define CLIP_MAXV 8
+
+/* One Sutherland-Hodgman step against the half space n.p - d <= eps.  An
+ * emitted vertex past the 8-vertex buffer is dropped (the reference's
+ * buffer would overflow there); the count saturates at 8. */
+static int clip_plane(float in[CLIP_MAXV][3], int n_in, const float nrm[3], float d, float out[CLIP_MAXV][3],
+                      float eps) {
+  if (n_in <= 0) return 0;
+  float dist[CLIP_MAXV];
+  int ins[CLIP_MAXV];
+  for (int i = 0; i < n_in; ++i) {
+    dist[i] = in[i][0] * nrm[0] + in[i][1] * nrm[1] + in[i][2] * nrm[2] - d;
+    ins[i] = dist[i] <= eps;
+  }
+  int m = 0;
+  for (int i = 0; i < n_in; ++i) {
+    const int j = (i + 1 == n_in) ? 0 : i + 1;
+    const float* P = in[i];
+    const float* Q = in[j];
+    const float dP = dist[i], dQ = dist[j];
+    if (ins[i] && ins[j]) {
+      if (m < CLIP_MAXV) { out[m][0] = Q[0]; out[m][1] = Q[1]; out[m][2] = Q[2]; }
+      ++m;
+    } else if (ins[i] != ins[j]) {
+      const float den = dP - dQ;
+      if (fabsf(den) > eps) {
+        const float t = dP / den;
+        if (m < CLIP_MAXV)
+          for (int a = 0; a < 3; ++a) out[m][a] = P[a] + t * (Q[a] - P[a]);
+        ++m;
+      }
+      if (ins[j]) {
+        if (m < CLIP_MAXV) { out[m][0] = Q[0]; out[m][1] = Q[1]; out[m][2] = Q[2]; }
+        ++m;
+      }
+    }
+    if (m >= CLIP_MAXV) return CLIP_MAXV;
+  }
+  return m;
+}
+
+/* Returns 1 when the clipped polygon is non-empty.  verts (24 floats, zero
+ * padded), count, centroid and area follow the reference kernel; area stays
+ * 0 for a degenerate triangle (its centroid is then vertex a). */
+int orc_clip_pair(const float* mn, const float* mx, const float* t, float eps, float* verts, int* count,
+                  float* centroid, float* area) {
+  float A[CLIP_MAXV][3], B[CLIP_MAXV][3];
+  for (int i = 0; i < 3; ++i)
+    for (int a = 0; a < 3; ++a) A[i][a] = t[3 * i + a];
+  static const float nrm[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  const float dd[6] = {mx[0], -mn[0], mx[1], -mn[1], mx[2], -mn[2]};
+  int n = 3;
+  for (int k = 0; k < 6; ++k) {
+    n = (k & 1) ? clip_plane(B, n, nrm[k], dd[k], A, eps) : clip_plane(A, n, nrm[k], dd[k], B, eps);
+    if (!n) {
+      *count = 0;
+      *area = 0.0f;
+      return 0;
+    }
+  }
+  const int cnt = n > CLIP_MAXV ? CLIP_MAXV : n;
+  *count = cnt;
+  for (int i = 0; i < CLIP_MAXV; ++i)
+    for (int a = 0; a < 3; ++a) verts[3 * i + a] = i < cnt ? A[i][a] : 0.0f;
+  *area = 0.0f;
+  float c[3] = {0.0f, 0.0f, 0.0f};
+  for (int i = 0; i < cnt; ++i)
+    for (int a = 0; a < 3; ++a) c[a] += A[i][a];
+  for (int a = 0; a < 3; ++a) {
+    c[a] /= (float)cnt;
+    c[a] = fminf(fmaxf(c[a], mn[a]), mx[a]);
+  }
+  const float ax = t[0], ay = t[1], az = t[2], bx = t[3], by = t[4], bz = t[5], qx = t[6], qy = t[7], qz = t[8];
+  const float e1x = bx - ax, e1y = by - ay, e1z = bz - az;
+  const float e2x = qx - ax, e2y = qy - ay, e2z = qz - az;
+  const float vx = c[0] - ax, vy = c[1] - ay, vz = c[2] - az;
+  const float d00 = e1x * e1x + e1y * e1y + e1z * e1z;
+  const float d01 = e1x * e2x + e1y * e2y + e1z * e2z;
+  const float d11 = e2x * e2x + e2y * e2y + e2z * e2z;
+  const float d20 = vx * e1x + vy * e1y + vz * e1z;
+  const float d21 = vx * e2x + vy * e2y + vz * e2z;
+  const float den = d00 * d11 - d01 * d01;
+  if (fabsf(den) < eps * eps) {
+    centroid[0] = ax; centroid[1] = ay; centroid[2] = az;
+    return 1;
+  }
+  float v = (d11 * d20 - d01 * d21) / den;
+  float w = (d00 * d21 - d01 * d20) / den;
+  float u = 1.0f - v - w;
+  if (u < 0) u = 0;
+  if (v < 0) v = 0;
+  if (w < 0) w = 0;
+  float nn = u + v + w;
+  if (nn <= eps) { u = 1; v = 0; w = 0; nn = 1; }
+  u /= nn; v /= nn; w /= nn;
+  centroid[0] = u * ax + v * bx + w * qx;
+  centroid[1] = u * ay + v * by + w * qy;
+  centroid[2] = u * az + v * bz + w * qz;
+  float ar = 0.0f;
+  for (int i = 0; i < cnt; ++i) {
+    const int j = (i + 1) % cnt;
+    const float p0 = A[i][0] - c[0], p1 = A[i][1] - c[1], p2 = A[i][2] - c[2];
+    const float q0 = A[j][0] - c[0], q1 = A[j][1] - c[1], q2 = A[j][2] - c[2];
+    const float cx = p1 * q2 - p2 * q1, cy = p2 * q0 - p0 * q2, cz = p0 * q1 - p1 * q0;
+    ar += 0.5f * sqrtf(cx * cx + cy * cy + cz * cz);
+  }
+  *area = ar < eps ? 0.0f : ar;
+  return 1;
+}
+
+typedef struct {
+  const float* V; const int32_t* F; int64_t nf; const float* tb; const float* bmin; const float* bmax;
+  int clip; float eps; int64_t* counts; const int64_t* offs;
+  int64_t* box_ids; int64_t* face_ids; int32_t* poly_counts; float* centroids; float* areas; float* poly_verts;
+} pairs_ctx;
+
+static void pairs_body(int64_t i, void* c_) {
+  pairs_ctx* c = (pairs_ctx*)c_;
+  const float* mn = c->bmin + 3 * i;
+  const float* mx = c->bmax + 3 * i;
+  int64_t k = c->offs ? c->offs[i] : 0, cnt = 0;
+  for (int64_t f = 0; f < c->nf; ++f) {
+    const float* b = c->tb + 6 * f;
+    if (b[0] > mx[0] || b[3] < mn[0] || b[1] > mx[1] || b[4] < mn[1] || b[2] > mx[2] || b[5] < mn[2]) continue;
+    float t[9];
+    gather_tri(c->V, c->F, f, t);
+    if (!orc_sat(t, mn, mx)) continue;
+    float verts[24], cen[3] = {0, 0, 0}, ar = 0;
+    int pc = 0;
+    if (c->clip && !orc_clip_pair(mn, mx, t, c->eps, verts, &pc, cen, &ar)) continue;
+    ++cnt;
+    if (!c->offs) continue;
+    c->box_ids[k] = i;
+    c->face_ids[k] = f;
+    if (c->clip) {
+      c->poly_counts[k] = pc;
+      for (int a = 0; a < 3; ++a) c->centroids[3 * k + a] = cen[a];
+      c->areas[k] = ar;
+      if (c->poly_verts) memcpy(c->poly_verts + 24 * k, verts, sizeof(verts));
+    }
+    ++k;
+  }
+  if (c->counts) c->counts[i] = cnt;
+}
+
+/* per box: number of faces passing SAT (clip = 0) or SAT and the clip */
+void orc_aabb_pair_counts(const float* V, const int32_t* F, int64_t nf, const float* bmin, const float* bmax, int64_t n,
+                          int clip, float eps, int64_t* counts) {
+  float* tb = tri_boxes(V, F, nf);
+  pairs_ctx c = {V, F, nf, tb, bmin, bmax, clip, eps, counts, NULL, NULL, NULL, NULL, NULL, NULL, NULL};
+  par_for(n, 16, pairs_body, &c);
+  free(tb);
+}
+
+/* the pairs, box i's at offs[i] in face order; clip outputs when clip != 0
+ * (poly_verts [.,8,3] nullable) */
+void orc_aabb_pairs_fill(const float* V, const int32_t* F, int64_t nf, const float* bmin, const float* bmax, int64_t n,
+                         int clip, float eps, const int64_t* offs, int64_t* box_ids, int64_t* face_ids,
+                         int32_t* poly_counts, float* centroids, float* areas, float* poly_verts) {
+  float* tb = tri_boxes(V, F, nf);
+  pairs_ctx c = {V, F, nf, tb, bmin, bmax, clip, eps, NULL, offs, box_ids, face_ids, poly_counts, centroids, areas,
+                 poly_verts};
+  par_for(n, 16, pairs_body, &c);
+  free(tb);
 }

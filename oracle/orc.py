@@ -322,3 +322,44 @@ def parity_votes(V, F, P, dirs, max_t=1e6, coalesce=1e-4):
     lib().orc_parity_votes(_p(V), _p(F), I64(F.shape[0]), _p(P), I64(P.shape[0]), _p(dirs), ctypes.c_int(dirs.shape[0]),
                            ctypes.c_float(max_t), ctypes.c_float(coalesce), _p(votes))
     return votes
+
+
+# ------------------------------------------------------------ box/mesh pairs
+def clip_pair(bmin, bmax, tri9, eps=1e-8):
+    """One triangle clipped against one box: (hit, count, verts [8,3], centroid, area)."""
+    mn, mx, t = _f32(bmin).reshape(3), _f32(bmax).reshape(3), _f32(tri9).reshape(9)
+    verts = np.zeros(24, np.float32)
+    cen = np.zeros(3, np.float32)
+    cnt = ctypes.c_int(0)
+    area = ctypes.c_float(0)
+    hit = lib().orc_clip_pair(_p(mn), _p(mx), _p(t), ctypes.c_float(eps), _p(verts), ctypes.byref(cnt), _p(cen),
+                              ctypes.byref(area))
+    return bool(hit), cnt.value, verts.reshape(8, 3), cen, np.float32(area.value)
+
+
+def aabb_pairs(V, F, bmin, bmax, mode=1, eps=1e-8):
+    """MeshBVH.intersect_aabb by brute force: dict with hit [N] and, per
+    (box, face) pair in box then face order, aabb_ids / face_ids (int64) and
+    for modes 2-3 poly_counts, centroids, areas (+ poly_verts for mode 3)."""
+    V, F, bmin, bmax = _f32(V), _i32(F), _f32(bmin), _f32(bmax)
+    n, nf = bmin.shape[0], F.shape[0]
+    clip = 1 if mode >= 2 else 0
+    counts = np.zeros(n, np.int64)
+    lib().orc_aabb_pair_counts(_p(V), _p(F), I64(nf), _p(bmin), _p(bmax), I64(n), ctypes.c_int(clip),
+                               ctypes.c_float(eps), _p(counts))
+    offs = np.zeros(n + 1, np.int64)
+    np.cumsum(counts, out=offs[1:])
+    P = int(offs[-1])
+    out = dict(hit=counts > 0, aabb_ids=np.zeros(P, np.int64), face_ids=np.zeros(P, np.int64))
+    pc = np.zeros(P, np.int32)
+    cen = np.zeros((P, 3), np.float32)
+    ar = np.zeros(P, np.float32)
+    pv = np.zeros((P, 8, 3), np.float32) if mode == 3 else None
+    lib().orc_aabb_pairs_fill(_p(V), _p(F), I64(nf), _p(bmin), _p(bmax), I64(n), ctypes.c_int(clip),
+                              ctypes.c_float(eps), _p(offs), _p(out["aabb_ids"]), _p(out["face_ids"]), _p(pc), _p(cen),
+                              _p(ar), _p(pv) if pv is not None else None)
+    if mode >= 2:
+        out.update(poly_counts=pc, centroids=cen, areas=ar)
+    if mode == 3:
+        out["poly_verts"] = pv
+    return out
