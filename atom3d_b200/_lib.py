@@ -82,10 +82,17 @@ _SIGNATURES: dict[str, tuple] = {
     "a3d_aabb_hit_workspace_bytes": (c_size, [c_i64]),
     "a3d_aabb_hit": (c_int, [ctypes.POINTER(BvhView), c_vp, c_vp, c_i64, c_vp, c_vp, c_size, c_vp]),
     "a3d_aabb_pairs_workspace_bytes": (c_size, [c_i64]),
+    "a3d_aabb_clip_workspace_bytes": (c_size, [c_i64]),
+    "a3d_exclusive_scan_workspace_bytes": (c_size, [c_i64]),
+    "a3d_exclusive_scan_u32": (c_int, [c_vp, c_i64, c_vp, c_vp, c_size, c_vp]),
+    "a3d_sort_pairs_workspace_bytes": (c_size, [c_i64]),
+    "a3d_sort_pairs_u64": (c_int, [c_vp, c_vp, c_i64, c_int, c_int, c_vp, c_size, c_vp]),
     "a3d_aabb_pairs_count": (c_int, [ctypes.POINTER(BvhView), c_vp, c_vp, c_i64, c_int, c_vp, c_vp, c_size,
                                      ctypes.POINTER(c_i64), c_vp]),
-    "a3d_aabb_pairs_write": (c_int, [ctypes.POINTER(BvhView), c_vp, c_vp, c_i64, c_int, c_vp, c_size, c_vp, c_vp,
-                                     c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "a3d_aabb_pairs_clip": (c_int, [ctypes.POINTER(BvhView), c_vp, c_vp, c_i64, c_vp, c_size, c_vp, c_size, c_i64,
+                                    c_vp, ctypes.POINTER(c_i64), c_vp]),
+    "a3d_aabb_pairs_write": (c_int, [ctypes.POINTER(BvhView), c_vp, c_vp, c_i64, c_int, c_vp, c_size, c_vp, c_size,
+                                     c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "a3d_octree_workspace_bytes": (c_size, [c_int, c_int, c_i64]),
     "a3d_octree_traverse": (
         c_int,

@@ -286,12 +286,21 @@ class MeshBVH:
         lib = _lib.lib()
         ws = _lib.workspace(lib.a3d_aabb_pairs_workspace_bytes(n), dev)
         stream = _lib.stream_ptr(dev)
-        totals = (ctypes.c_int64 * 2)()
+        n_cand = ctypes.c_int64(0)
         _lib.call("a3d_aabb_pairs_count", ctypes.byref(self._bvh.view), mn.data_ptr(), mx.data_ptr(), n, mode,
-                  hit.data_ptr(), ws.data_ptr(), ws.numel(), totals, stream)
-        P, n_sat = int(totals[0]), int(totals[1])
-        if mode >= 2 and n_sat == 0:
+                  hit.data_ptr(), ws.data_ptr(), ws.numel(), ctypes.byref(n_cand), stream)
+        m = int(n_cand.value)
+        if mode >= 2 and m == 0:
             return AABBIntersectResult(hit=hit)  # no SAT candidate at all: the reference returns the mask alone
+        cws = None
+        P = m
+        if mode >= 2:
+            cws = _lib.workspace(lib.a3d_aabb_clip_workspace_bytes(m), dev)
+            n_pairs = ctypes.c_int64(0)
+            _lib.call("a3d_aabb_pairs_clip", ctypes.byref(self._bvh.view), mn.data_ptr(), mx.data_ptr(), n,
+                      ws.data_ptr(), ws.numel(), cws.data_ptr(), cws.numel(), m, hit.data_ptr(), ctypes.byref(n_pairs),
+                      stream)
+            P = int(n_pairs.value)
         a_ids = torch.empty(P, dtype=idt, device=dev)
         f_ids = torch.empty(P, dtype=idt, device=dev)
         pc = cen = ar = pv = None
@@ -304,8 +313,8 @@ class MeshBVH:
         if P:
             ptr = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
             _lib.call("a3d_aabb_pairs_write", ctypes.byref(self._bvh.view), mn.data_ptr(), mx.data_ptr(), n, mode,
-                      ws.data_ptr(), ws.numel(), a_ids.data_ptr(), f_ids.data_ptr(), ptr(pc), ptr(cen), ptr(ar),
-                      ptr(pv), stream)
+                      ws.data_ptr(), ws.numel(), ptr(cws), cws.numel() if cws is not None else 0, m,
+                      a_ids.data_ptr(), f_ids.data_ptr(), ptr(pc), ptr(cen), ptr(ar), ptr(pv), stream)
         return AABBIntersectResult(hit=hit, aabb_ids=a_ids, face_ids=f_ids, centroids=cen, areas=ar, poly_verts=pv,
                                    poly_counts=pc)
 

@@ -10,14 +10,18 @@
 //           centroid projected onto the triangle, and its fan area
 //   mode 3  mode 2 plus the polygon's vertices (8 slots, zero padded)
 //
-// Two passes over the boxes share one tree walk: the count pass counts per
-// box the pairs that survive (SAT, then the clip for modes 2-3), an
-// exclusive scan turns the counts into offsets, and the write pass walks
-// again and writes each pair's outputs straight into its compacted slot --
-// no candidate list, no truncation (the reference keeps at most
-// min(100 N, 5e7) candidates and drops the rest silently).  Pairs come
-// grouped by box in ascending order, in tree order within a box; the
-// reference's order is that of an atomic counter.
+// The tree walk finds the faces passing SAT, in two passes over the boxes:
+// a count pass, an exclusive scan of the counts, and a write pass that puts
+// each box's pairs at its offset -- exact-size outputs, no truncation (the
+// reference keeps at most min(100 N, 5e7) candidates and drops the rest
+// silently).  Mode 1 writes the pairs directly.  Modes 2-3 write them as a
+// candidate list (box, triangle slot) and clip it one thread per candidate,
+// converged: a flag pass (clip, hit mask), an exclusive scan of the flags,
+// and an emit pass that clips again and writes the outputs at their
+// compacted index.  (Clipping inside the divergent walk ran with one or two
+// active lanes per warp and was 10x slower.)  Pairs come grouped by box in
+// ascending order, in tree order within a box; the reference's order is
+// that of an atomic counter.
 //
 // The clip is restated operation by operation with round-to-nearest
 // intrinsics (IEEE divide and square root, no contraction), so the CPU
@@ -169,58 +173,113 @@ struct PairOut {
   float* poly_verts;  // mode 3
 };
 
-// Walks the tree for box i; counts (kWrite false) or writes (true) its
-// surviving pairs from slot base.  Returns the traversal status (2 =
-// overflow); *count = surviving pairs, *nsat = faces passing SAT.
-template <int kMode, bool kWrite, typename Stack>
-__device__ __forceinline__ int box_pairs(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
-                                         const float* __restrict__ bmin, const float* __restrict__ bmax, int64_t i,
-                                         Stack& st, int64_t base, const PairOut& out, uint32_t* count,
-                                         uint32_t* nsat) {
+// Clips candidate k (box cand_box[k], triangle record cand_slot[k]).
+template <bool kEmit, int kMode>
+__device__ __forceinline__ void clip_candidate(const TriRec* __restrict__ tris, const float* __restrict__ bmin,
+                                               const float* __restrict__ bmax, const uint32_t* __restrict__ cand_box,
+                                               const uint32_t* __restrict__ cand_slot, int64_t k,
+                                               uint32_t* __restrict__ flags, uint8_t* __restrict__ hit,
+                                               const int64_t* __restrict__ coffs, const PairOut& out,
+                                               int64_t n, int64_t num_slots, int64_t num_pairs,
+                                               unsigned long long* __restrict__ faults) {
+  const int64_t i = cand_box[k];
+  const uint32_t slot = cand_slot[k];
+  if (i >= n || slot >= num_slots) {  // never for a candidate list written by the walk
+    atomicAdd(faults, 1ull);
+    if (!kEmit) flags[k] = 0;
+    return;
+  }
+  const float4* p = reinterpret_cast<const float4*>(tris + slot);
+  TriRec t;
+  t.a = __ldg(p); t.b = __ldg(p + 1); t.c = __ldg(p + 2); t.r = make_float4(0.f, 0.f, 0.f, 0.f);
   const float mn[3] = {bmin[3 * i], bmin[3 * i + 1], bmin[3 * i + 2]};
   const float mx[3] = {bmax[3 * i], bmax[3 * i + 1], bmax[3 * i + 2]};
-  uint32_t k = 0, s = 0;
-  const int r = box_traverse(nodes, tris, mn[0], mn[1], mn[2], mx[0], mx[1], mx[2], st,
-                             [&](const TriRec& t, uint32_t) {
-    if (!sat_test(t, mn[0], mn[1], mn[2], mx[0], mx[1], mx[2])) return false;
-    ++s;
-    if (kMode >= 2) {
-      Poly pa, pb;
-      const int cnt = clip_tri(t, mn, mx, pa, pb);
-      if (!cnt) return false;
-      if (kWrite) {
-        const int64_t o = base + k;
-        const ClipOut c = clip_measure(t, mn, mx, pa, cnt);
-        reinterpret_cast<int64_t*>(out.aabb_ids)[o] = i;
-        reinterpret_cast<int64_t*>(out.face_ids)[o] = __float_as_int(t.a.w);
-        out.poly_counts[o] = c.count;
-        out.centroids[3 * o] = c.cx;
-        out.centroids[3 * o + 1] = c.cy;
-        out.centroids[3 * o + 2] = c.cz;
-        out.areas[o] = c.area;
-        if (kMode == 3) {
-          float4* pv = reinterpret_cast<float4*>(out.poly_verts + 24 * o);
+  Poly pa, pb;
+  const int cnt = clip_tri(t, mn, mx, pa, pb);
+  if (!kEmit) {
+    flags[k] = cnt > 0;
+    if (cnt > 0) hit[i] = 1;
+    return;
+  }
+  if (!cnt) return;
+  const int64_t o = coffs[k];
+  if (!flags[k] || o < 0 || o >= num_pairs) {  // the flag pass decided this clip differently
+    atomicAdd(faults, 1ull);
+    return;
+  }
+  const ClipOut c = clip_measure(t, mn, mx, pa, cnt);
+  reinterpret_cast<int64_t*>(out.aabb_ids)[o] = i;
+  reinterpret_cast<int64_t*>(out.face_ids)[o] = __float_as_int(t.a.w);
+  out.poly_counts[o] = c.count;
+  out.centroids[3 * o] = c.cx;
+  out.centroids[3 * o + 1] = c.cy;
+  out.centroids[3 * o + 2] = c.cz;
+  out.areas[o] = c.area;
+  if (kMode == 3) {
+    float4* pv = reinterpret_cast<float4*>(out.poly_verts + 24 * o);
 #pragma unroll
-          for (int q = 0; q < 6; ++q) {
-            float e[4];
+    for (int q = 0; q < 6; ++q) {
+      float e[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int f = 4 * q + u, vi = f / 3, ax = f % 3;
-              e[u] = vi < cnt ? pa.v[vi][ax] : 0.0f;
-            }
-            pv[q] = make_float4(e[0], e[1], e[2], e[3]);
-          }
-        }
+      for (int u = 0; u < 4; ++u) {
+        const int f = 4 * q + u, vi = f / 3, ax = f % 3;
+        e[u] = vi < cnt ? pa.v[vi][ax] : 0.0f;
       }
-    } else if (kWrite) {
-      reinterpret_cast<int32_t*>(out.aabb_ids)[base + k] = (int32_t)i;
-      reinterpret_cast<int32_t*>(out.face_ids)[base + k] = __float_as_int(t.a.w);
+      pv[q] = make_float4(e[0], e[1], e[2], e[3]);
+    }
+  }
+}
+
+__global__ void clip_flags_kernel(const TriRec* __restrict__ tris, const float* __restrict__ bmin,
+                                  const float* __restrict__ bmax, const uint32_t* __restrict__ cand_box,
+                                  const uint32_t* __restrict__ cand_slot, int64_t m, uint32_t* __restrict__ flags,
+                                  uint8_t* __restrict__ hit, int64_t n, int64_t num_slots,
+                                  unsigned long long* __restrict__ faults) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m)
+    clip_candidate<false, 2>(tris, bmin, bmax, cand_box, cand_slot, k, flags, hit, nullptr, PairOut{}, n, num_slots,
+                             0, faults);
+}
+
+template <int kMode>
+__global__ void clip_emit_kernel(const TriRec* __restrict__ tris, const float* __restrict__ bmin,
+                                 const float* __restrict__ bmax, const uint32_t* __restrict__ cand_box,
+                                 const uint32_t* __restrict__ cand_slot, int64_t m, uint32_t* __restrict__ flags,
+                                 const int64_t* __restrict__ coffs, PairOut out, int64_t n, int64_t num_slots,
+                                 unsigned long long* __restrict__ faults) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m)
+    clip_candidate<true, kMode>(tris, bmin, bmax, cand_box, cand_slot, k, flags, nullptr, coffs, out, n, num_slots,
+                                coffs[m], faults);
+}
+
+// Walks the tree for box i; counts (kWrite false) or writes (true) its
+// SAT pairs from slot base: kSlots false writes int32 (box, face id) pairs,
+// kSlots true the candidate list (box, triangle record slot).  Returns the
+// traversal status (2 = overflow); *count = pairs.
+template <bool kWrite, bool kSlots, typename Stack>
+__device__ __forceinline__ int box_pairs(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
+                                         const float* __restrict__ bmin, const float* __restrict__ bmax, int64_t i,
+                                         Stack& st, int64_t base, int64_t end, int32_t* __restrict__ out_box,
+                                         int32_t* __restrict__ out_face, uint32_t* count,
+                                         unsigned long long* __restrict__ faults) {
+  const float mnx = bmin[3 * i], mny = bmin[3 * i + 1], mnz = bmin[3 * i + 2];
+  const float mxx = bmax[3 * i], mxy = bmax[3 * i + 1], mxz = bmax[3 * i + 2];
+  uint32_t k = 0;
+  const int r = box_traverse(nodes, tris, mnx, mny, mnz, mxx, mxy, mxz, st, [&](const TriRec& t, uint32_t slot) {
+    if (!sat_test(t, mnx, mny, mnz, mxx, mxy, mxz)) return false;
+    if (kWrite) {
+      if (base + k < end) {  // the count pass found the same pairs
+        out_box[base + k] = (int32_t)i;
+        out_face[base + k] = kSlots ? (int32_t)slot : __float_as_int(t.a.w);
+      } else {
+        atomicAdd(faults, 1ull);
+      }
     }
     ++k;
     return false;
   });
   *count = k;
-  *nsat = s;
   return r;
 }
 
@@ -229,7 +288,7 @@ struct PairsWs {
   int64_t* offs;
   int64_t* scan_tmp;
   uint32_t* spill;
-  unsigned long long* misc;  // [0] spill count, [1] overflow, [2] SAT pairs
+  unsigned long long* misc;  // [0] spill count, [1] overflow, [2] guard faults
 };
 
 size_t carve_pairs(PairsWs& w, Workspace& ws, int64_t n) {
@@ -241,14 +300,23 @@ size_t carve_pairs(PairsWs& w, Workspace& ws, int64_t n) {
   return ws.used;
 }
 
-// one atomic per group of converged lanes; every lane is in exactly one group
-__device__ __forceinline__ void add_sat(unsigned long long* total, uint32_t s) {
-  const unsigned m = __activemask();
-  const uint32_t w = __reduce_add_sync(m, s);
-  if (w && (int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(total, (unsigned long long)w);
+struct ClipWs {
+  uint32_t* cand_box;
+  uint32_t* cand_slot;
+  uint32_t* flags;
+  int64_t* coffs;
+  int64_t* scan_tmp;
+};
+
+size_t carve_clip(ClipWs& w, Workspace& ws, int64_t m) {
+  w.cand_box = ws.take<uint32_t>(m);
+  w.cand_slot = ws.take<uint32_t>(m);
+  w.flags = ws.take<uint32_t>(m);
+  w.coffs = ws.take<int64_t>(m + 1);
+  w.scan_tmp = ws.take<int64_t>((int64_t)scan_workspace_elems(m));
+  return ws.used;
 }
 
-template <int kMode>
 __global__ void __launch_bounds__(kSatThreads)
     pairs_count_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
                        const float* __restrict__ bmin, const float* __restrict__ bmax, int64_t n,
@@ -258,19 +326,15 @@ __global__ void __launch_bounds__(kSatThreads)
   const int64_t i = (int64_t)blockIdx.x * kSatThreads + threadIdx.x;
   if (i >= n) return;
   ShStack st{s_stack + threadIdx.x, 0};
-  uint32_t c = 0, s = 0;
-  const int r = box_pairs<kMode, false>(nodes, tris, bmin, bmax, i, st, 0, PairOut{}, &c, &s);
-  if (r == 2) {
+  uint32_t c = 0;
+  if (box_pairs<false, false>(nodes, tris, bmin, bmax, i, st, 0, 0, nullptr, nullptr, &c, nullptr) == 2) {
     spill[atomicAdd(misc, 1ull)] = (uint32_t)i;
     c = 0;
-    s = 0;
   }
   counts[i] = c;
-  hit[i] = c > 0;
-  add_sat(misc + 2, s);
+  if (hit) hit[i] = c > 0;
 }
 
-template <int kMode>
 __global__ void pairs_count_spill_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
                                          const float* __restrict__ bmin, const float* __restrict__ bmax,
                                          uint32_t* __restrict__ counts, uint8_t* __restrict__ hit,
@@ -280,70 +344,59 @@ __global__ void pairs_count_spill_kernel(const WideNode* __restrict__ nodes, con
     const int64_t i = spill[t];
     LcStack st;
     st.sp = 0;
-    uint32_t c = 0, s = 0;
-    if (box_pairs<kMode, false>(nodes, tris, bmin, bmax, i, st, 0, PairOut{}, &c, &s) == 2) {
+    uint32_t c = 0;
+    if (box_pairs<false, false>(nodes, tris, bmin, bmax, i, st, 0, 0, nullptr, nullptr, &c, nullptr) == 2) {
       atomicExch(misc + 1, 1ull);
       c = 0;
-      s = 0;
     }
     counts[i] = c;
-    hit[i] = c > 0;
-    atomicAdd(misc + 2, (unsigned long long)s);
+    if (hit) hit[i] = c > 0;
   }
 }
 
-template <int kMode>
+template <bool kSlots>
 __global__ void __launch_bounds__(kSatThreads)
     pairs_write_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
                        const float* __restrict__ bmin, const float* __restrict__ bmax, int64_t n,
-                       const int64_t* __restrict__ offs, PairOut out) {
+                       const int64_t* __restrict__ offs, int32_t* __restrict__ out_box,
+                       int32_t* __restrict__ out_face, unsigned long long* __restrict__ misc) {
   __shared__ uint32_t s_stack[kSatDepth * kSatThreads];
   const int64_t i = (int64_t)blockIdx.x * kSatThreads + threadIdx.x;
   if (i >= n) return;
   ShStack st{s_stack + threadIdx.x, 0};
-  uint32_t c, s;
+  uint32_t c;
   // a box whose walk overflows here overflowed in the count pass too (same
   // walk): the spill kernel rewrites its whole segment
-  box_pairs<kMode, true>(nodes, tris, bmin, bmax, i, st, offs[i], out, &c, &s);
+  box_pairs<true, kSlots>(nodes, tris, bmin, bmax, i, st, offs[i], offs[i + 1], out_box, out_face, &c, misc + 2);
 }
 
-template <int kMode>
+template <bool kSlots>
 __global__ void pairs_write_spill_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
                                          const float* __restrict__ bmin, const float* __restrict__ bmax,
                                          const int64_t* __restrict__ offs, const uint32_t* __restrict__ spill,
-                                         const unsigned long long* __restrict__ misc, PairOut out) {
+                                         unsigned long long* __restrict__ misc, int32_t* __restrict__ out_box,
+                                         int32_t* __restrict__ out_face) {
   const uint64_t m = misc[0];
   for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (uint64_t)gridDim.x * blockDim.x) {
     const int64_t i = spill[t];
     LcStack st;
     st.sp = 0;
-    uint32_t c, s;
-    box_pairs<kMode, true>(nodes, tris, bmin, bmax, i, st, offs[i], out, &c, &s);
+    uint32_t c;
+    box_pairs<true, kSlots>(nodes, tris, bmin, bmax, i, st, offs[i], offs[i + 1], out_box, out_face, &c, misc + 2);
   }
 }
 
-template <int kMode>
-int launch_count(const a3d_bvh_view* bvh, const float* bmin, const float* bmax, int64_t n, uint8_t* hit,
-                 const PairsWs& w, cudaStream_t s) {
-  const WideNode* nodes = (const WideNode*)bvh->nodes;
-  const TriRec* tris = (const TriRec*)bvh->tris;
-  pairs_count_kernel<kMode><<<(unsigned)ceil_div(n, kSatThreads), kSatThreads, 0, s>>>(nodes, tris, bmin, bmax, n,
-                                                                                        w.counts, hit, w.spill, w.misc);
-  A3D_LAUNCH_CHECK();
-  pairs_count_spill_kernel<kMode><<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, bmin, bmax, w.counts, hit, w.spill, w.misc);
-  A3D_LAUNCH_CHECK();
-  return A3D_OK;
-}
-
-template <int kMode>
+template <bool kSlots>
 int launch_write(const a3d_bvh_view* bvh, const float* bmin, const float* bmax, int64_t n, const PairsWs& w,
-                 const PairOut& out, cudaStream_t s) {
+                 int32_t* out_box, int32_t* out_face, cudaStream_t s) {
   const WideNode* nodes = (const WideNode*)bvh->nodes;
   const TriRec* tris = (const TriRec*)bvh->tris;
-  pairs_write_kernel<kMode><<<(unsigned)ceil_div(n, kSatThreads), kSatThreads, 0, s>>>(nodes, tris, bmin, bmax, n,
-                                                                                        w.offs, out);
+  pairs_write_kernel<kSlots><<<(unsigned)ceil_div(n, kSatThreads), kSatThreads, 0, s>>>(nodes, tris, bmin, bmax, n,
+                                                                                        w.offs, out_box, out_face,
+                                                                                        w.misc);
   A3D_LAUNCH_CHECK();
-  pairs_write_spill_kernel<kMode><<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, bmin, bmax, w.offs, w.spill, w.misc, out);
+  pairs_write_spill_kernel<kSlots><<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, bmin, bmax, w.offs, w.spill, w.misc,
+                                                              out_box, out_face);
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
@@ -359,14 +412,28 @@ extern "C" size_t a3d_aabb_pairs_workspace_bytes(int64_t n) {
   return carve_pairs(w, ws, n > 0 ? n : 1) + 256;
 }
 
-extern "C" int a3d_aabb_pairs_count(const a3d_bvh_view* bvh, const float* box_min, const float* box_max, int64_t n,
-                                    int mode, uint8_t* hit, void* workspace, size_t workspace_bytes,
-                                    int64_t* totals_out, a3d_stream_t stream) {
-  cudaStream_t s = (cudaStream_t)stream;
+extern "C" size_t a3d_aabb_clip_workspace_bytes(int64_t num_candidates) {
+  Workspace ws(nullptr, 0);
+  ClipWs w;
+  return carve_clip(w, ws, num_candidates > 0 ? num_candidates : 1) + 256;
+}
+
+namespace {
+int check_pairs_args(const a3d_bvh_view* bvh, int mode, int64_t n) {
   A3D_REQUIRE(bvh && bvh->nodes && bvh->tris, A3D_ERR_ARGUMENT, "aabb_pairs: invalid bvh");
   A3D_REQUIRE(mode >= 1 && mode <= 3, A3D_ERR_ARGUMENT, "aabb_pairs: mode must be 1, 2 or 3");
-  A3D_REQUIRE(n >= 0 && n < (1ll << 31) && totals_out, A3D_ERR_ARGUMENT, "aabb_pairs: bad size");
-  totals_out[0] = totals_out[1] = 0;
+  A3D_REQUIRE(n >= 0 && n < (1ll << 31), A3D_ERR_ARGUMENT, "aabb_pairs: bad size");
+  return A3D_OK;
+}
+}  // namespace
+
+extern "C" int a3d_aabb_pairs_count(const a3d_bvh_view* bvh, const float* box_min, const float* box_max, int64_t n,
+                                    int mode, uint8_t* hit, void* workspace, size_t workspace_bytes,
+                                    int64_t* num_candidates_out, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_TRY(check_pairs_args(bvh, mode, n));
+  A3D_REQUIRE(num_candidates_out, A3D_ERR_ARGUMENT, "aabb_pairs: null count output");
+  *num_candidates_out = 0;
   if (n == 0) return A3D_OK;
   A3D_REQUIRE(box_min && box_max && hit, A3D_ERR_ARGUMENT, "aabb_pairs: null pointer");
   Workspace ws(workspace, workspace_bytes);
@@ -374,8 +441,15 @@ extern "C" int a3d_aabb_pairs_count(const a3d_bvh_view* bvh, const float* box_mi
   carve_pairs(w, ws, n);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "aabb_pairs: workspace too small");
   A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, 4 * sizeof(unsigned long long), s));
-  if (mode == 1) A3D_TRY(launch_count<1>(bvh, box_min, box_max, n, hit, w, s));
-  else A3D_TRY(launch_count<2>(bvh, box_min, box_max, n, hit, w, s));  // the count is the same for mode 3
+  // modes 2-3: the hit mask comes from the clip
+  uint8_t* h = mode == 1 ? hit : nullptr;
+  const WideNode* nodes = (const WideNode*)bvh->nodes;
+  const TriRec* tris = (const TriRec*)bvh->tris;
+  pairs_count_kernel<<<(unsigned)ceil_div(n, kSatThreads), kSatThreads, 0, s>>>(nodes, tris, box_min, box_max, n,
+                                                                                 w.counts, h, w.spill, w.misc);
+  A3D_LAUNCH_CHECK();
+  pairs_count_spill_kernel<<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, box_min, box_max, w.counts, h, w.spill, w.misc);
+  A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.counts, w.offs, n, w.scan_tmp, w.offs + n, s)));
   unsigned long long misc[4];
   int64_t total = 0;
@@ -383,30 +457,86 @@ extern "C" int a3d_aabb_pairs_count(const a3d_bvh_view* bvh, const float* box_mi
   A3D_CUDA_TRY(cudaMemcpyAsync(&total, w.offs + n, sizeof(total), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
   A3D_REQUIRE(misc[1] == 0, A3D_ERR_OVERFLOW, "aabb_pairs: traversal stack overflow");
-  totals_out[0] = total;
-  totals_out[1] = (int64_t)misc[2];
+  *num_candidates_out = total;
+  return A3D_OK;
+}
+
+extern "C" int a3d_aabb_pairs_clip(const a3d_bvh_view* bvh, const float* box_min, const float* box_max, int64_t n,
+                                   void* workspace, size_t workspace_bytes, void* clip_workspace,
+                                   size_t clip_workspace_bytes, int64_t num_candidates, uint8_t* hit,
+                                   int64_t* num_pairs_out, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_TRY(check_pairs_args(bvh, 2, n));
+  A3D_REQUIRE(num_pairs_out && num_candidates >= 0 && num_candidates < (1ll << 32), A3D_ERR_ARGUMENT,
+              "aabb_pairs_clip: bad argument");
+  *num_pairs_out = 0;
+  if (n == 0) return A3D_OK;
+  A3D_REQUIRE(box_min && box_max && hit, A3D_ERR_ARGUMENT, "aabb_pairs_clip: null pointer");
+  Workspace ws(workspace, workspace_bytes);
+  PairsWs w;
+  carve_pairs(w, ws, n);
+  Workspace cws(clip_workspace, clip_workspace_bytes);
+  ClipWs c;
+  carve_clip(c, cws, num_candidates);
+  A3D_REQUIRE(workspace && ws.ok() && clip_workspace && cws.ok(), A3D_ERR_WORKSPACE,
+              "aabb_pairs_clip: workspace too small");
+  A3D_CUDA_TRY(cudaMemsetAsync(hit, 0, n, s));
+  if (num_candidates == 0) return A3D_OK;
+  A3D_TRY(launch_write<true>(bvh, box_min, box_max, n, w, (int32_t*)c.cand_box, (int32_t*)c.cand_slot, s));
+  clip_flags_kernel<<<(unsigned)ceil_div(num_candidates, 256), 256, 0, s>>>(
+      (const TriRec*)bvh->tris, box_min, box_max, c.cand_box, c.cand_slot, num_candidates, c.flags, hit, n,
+      bvh->num_tris, w.misc + 2);
+  A3D_LAUNCH_CHECK();
+  A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(c.flags, c.coffs, num_candidates, c.scan_tmp,
+                                                     c.coffs + num_candidates, s)));
+  int64_t total = 0;
+  unsigned long long faults = 0;
+  A3D_CUDA_TRY(cudaMemcpyAsync(&total, c.coffs + num_candidates, sizeof(total), cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaMemcpyAsync(&faults, w.misc + 2, sizeof(faults), cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  A3D_REQUIRE(faults == 0, A3D_ERR_OVERFLOW, "aabb_pairs_clip: a candidate index guard fired");
+  *num_pairs_out = total;
   return A3D_OK;
 }
 
 extern "C" int a3d_aabb_pairs_write(const a3d_bvh_view* bvh, const float* box_min, const float* box_max, int64_t n,
-                                    int mode, void* workspace, size_t workspace_bytes, void* aabb_ids,
+                                    int mode, void* workspace, size_t workspace_bytes, void* clip_workspace,
+                                    size_t clip_workspace_bytes, int64_t num_candidates, void* aabb_ids,
                                     void* face_ids, int32_t* poly_counts, float* centroids, float* areas,
                                     float* poly_verts, a3d_stream_t stream) {
   cudaStream_t s = (cudaStream_t)stream;
-  A3D_REQUIRE(bvh && bvh->nodes && bvh->tris, A3D_ERR_ARGUMENT, "aabb_pairs: invalid bvh");
-  A3D_REQUIRE(mode >= 1 && mode <= 3, A3D_ERR_ARGUMENT, "aabb_pairs: mode must be 1, 2 or 3");
-  A3D_REQUIRE(n >= 0 && n < (1ll << 31), A3D_ERR_ARGUMENT, "aabb_pairs: bad size");
+  A3D_TRY(check_pairs_args(bvh, mode, n));
   if (n == 0) return A3D_OK;
   A3D_REQUIRE(box_min && box_max && aabb_ids && face_ids, A3D_ERR_ARGUMENT, "aabb_pairs: null output");
-  A3D_REQUIRE(mode == 1 || (poly_counts && centroids && areas), A3D_ERR_ARGUMENT, "aabb_pairs: null clip output");
-  A3D_REQUIRE(mode != 3 || (poly_verts && ((uintptr_t)poly_verts & 15) == 0), A3D_ERR_ARGUMENT,
-              "aabb_pairs: poly_verts must be a 16-byte aligned [P,8,3] buffer");
   Workspace ws(workspace, workspace_bytes);
   PairsWs w;
   carve_pairs(w, ws, n);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "aabb_pairs: workspace too small");
-  const PairOut out{aabb_ids, face_ids, poly_counts, centroids, areas, poly_verts};
-  if (mode == 1) return launch_write<1>(bvh, box_min, box_max, n, w, out, s);
-  if (mode == 2) return launch_write<2>(bvh, box_min, box_max, n, w, out, s);
-  return launch_write<3>(bvh, box_min, box_max, n, w, out, s);
+  if (mode == 1) {
+    A3D_TRY(launch_write<false>(bvh, box_min, box_max, n, w, (int32_t*)aabb_ids, (int32_t*)face_ids, s));
+  } else {
+    A3D_REQUIRE(poly_counts && centroids && areas, A3D_ERR_ARGUMENT, "aabb_pairs: null clip output");
+    A3D_REQUIRE(mode != 3 || (poly_verts && ((uintptr_t)poly_verts & 15) == 0), A3D_ERR_ARGUMENT,
+                "aabb_pairs: poly_verts must be a 16-byte aligned [P,8,3] buffer");
+    Workspace cws(clip_workspace, clip_workspace_bytes);
+    ClipWs c;
+    carve_clip(c, cws, num_candidates);
+    A3D_REQUIRE(clip_workspace && cws.ok() && num_candidates >= 0, A3D_ERR_WORKSPACE,
+                "aabb_pairs: clip workspace too small");
+    if (num_candidates == 0) return A3D_OK;
+    const PairOut out{aabb_ids, face_ids, poly_counts, centroids, areas, poly_verts};
+    const unsigned g = (unsigned)ceil_div(num_candidates, 256);
+    if (mode == 2)
+      clip_emit_kernel<2><<<g, 256, 0, s>>>((const TriRec*)bvh->tris, box_min, box_max, c.cand_box, c.cand_slot,
+                                            num_candidates, c.flags, c.coffs, out, n, bvh->num_tris, w.misc + 2);
+    else
+      clip_emit_kernel<3><<<g, 256, 0, s>>>((const TriRec*)bvh->tris, box_min, box_max, c.cand_box, c.cand_slot,
+                                            num_candidates, c.flags, c.coffs, out, n, bvh->num_tris, w.misc + 2);
+    A3D_LAUNCH_CHECK();
+  }
+  unsigned long long faults = 0;
+  A3D_CUDA_TRY(cudaMemcpyAsync(&faults, w.misc + 2, sizeof(faults), cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  A3D_REQUIRE(faults == 0, A3D_ERR_OVERFLOW, "aabb_pairs_write: an output index guard fired");
+  return A3D_OK;
 }

@@ -30,7 +30,11 @@ __device__ __forceinline__ T warp_reduce_sum(T v) {
 }
 
 // Block-wide exclusive scan for blockDim.x <= 1024 (multiple of 32).
-// s_warp must hold 32 elements.  Returns exclusive prefix; *total = block sum.
+// s_warp must hold kBlockScanSlots elements: one exclusive offset per warp
+// and, in its own slot, the block total (with 32 warps the last warp's
+// offset and the total would otherwise share a slot).  Returns the
+// exclusive prefix; *total = block sum.
+constexpr int kBlockScanSlots = 33;
 template <typename T>
 __device__ __forceinline__ T block_exclusive_scan(T v, T* s_warp, T* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -42,11 +46,11 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T* s_warp, T* total) {
     T w = lane < nwarps ? s_warp[lane] : T(0);
     T wi = warp_inclusive_scan(w);
     if (lane < nwarps) s_warp[lane] = wi - w;
-    if (lane == nwarps - 1) s_warp[31] = wi;
+    if (lane == nwarps - 1) s_warp[32] = wi;
   }
   __syncthreads();
   T res = inc - v + s_warp[warp];
-  if (total) *total = s_warp[31];
+  if (total) *total = s_warp[32];
   __syncthreads();
   return res;
 }
@@ -60,7 +64,7 @@ constexpr int kScanTile = kScanThreads * kScanItems;
 
 template <typename TIn, typename T>
 __global__ void scan_tile_reduce_kernel(const TIn* __restrict__ in, int64_t n, T* __restrict__ tile_sums) {
-  __shared__ T s_warp[32];
+  __shared__ T s_warp[kBlockScanSlots];
   const int64_t base = (int64_t)blockIdx.x * kScanTile;
   T acc = 0;
 #pragma unroll
@@ -76,7 +80,7 @@ __global__ void scan_tile_reduce_kernel(const TIn* __restrict__ in, int64_t n, T
 // Single block: exclusive scan of tile sums in place, total -> *total.
 template <typename T>
 __global__ void scan_tile_sums_kernel(T* __restrict__ sums, int64_t nb, T* __restrict__ total) {
-  __shared__ T s_warp[32];
+  __shared__ T s_warp[kBlockScanSlots];
   const int64_t per = ceil_div(nb, (int64_t)blockDim.x);
   const int64_t lo = (int64_t)threadIdx.x * per;
   const int64_t hi = lo + per < nb ? lo + per : nb;
@@ -95,7 +99,7 @@ __global__ void scan_tile_sums_kernel(T* __restrict__ sums, int64_t nb, T* __res
 template <typename TIn, typename T>
 __global__ void scan_tile_down_kernel(const TIn* __restrict__ in, T* __restrict__ out, int64_t n,
                                       const T* __restrict__ tile_offsets) {
-  __shared__ T s_warp[32];
+  __shared__ T s_warp[kBlockScanSlots];
   const int64_t base = (int64_t)blockIdx.x * kScanTile;
   // each thread owns kScanItems consecutive elements
   T vals[kScanItems];

@@ -559,6 +559,12 @@ def bench_dmc(dev, steps, warmup, cpu=True):
            "roofline_fwd": {"bound": "hbm", "achieved": alg / (fwd * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                             "frac": alg / (fwd * 1e-3) / 1e9 / peak, "peak_kind": kind,
                             "bytes": "108 B/active cube + 12 B/vertex + 24 B/face"}}
+    dmc_eval = SparseDiffDMC(device=str(dev)).eval()
+    with torch.no_grad():
+        eval_ms = _time_ms(lambda: dmc_eval(vd, sd, cd, 512), steps)
+        oe = dmc_eval(vd, sd, cd, 512)
+    out["eval_qef"] = {"ms": eval_ms, "vertices": int(oe.vertices.shape[0]), "faces": int(oe.faces.shape[0]),
+                       "note": "inference mode: corner gradients + QEF vertices + 2-triangle split, forward only"}
     if cpu:
         from oracle import dmc_oracle, orc
 
@@ -603,10 +609,62 @@ def bench_octree_flood(dev, steps, warmup):
     e1.record(stream)
     torch.cuda.synchronize()
     ff_ms = e0.elapsed_time(e1) / steps
-    return {"metric": "octree SAT 4->10 + sparse flood fill at 1024^3 (327,680 tris)", "unit": "ms",
-            "bvh_build_ms": build_ms, "octree_ms": oct_ms, "sparse_flood_fill_ms": ff_ms,
-            "candidate_voxels": int(cand.shape[0]),
-            "labels": {k: int(t.shape[0]) for k, t in out.items()}}
+    res = {"metric": "octree SAT 4->10 + sparse flood fill at 1024^3 (327,680 tris)", "unit": "ms",
+           "bvh_build_ms": build_ms, "octree_ms": oct_ms, "sparse_flood_fill_ms": ff_ms,
+           "candidate_voxels": int(cand.shape[0]),
+           "labels": {k: int(t.shape[0]) for k, t in out.items()}}
+    res["dual_graph"] = bench_dual(dev, oc, out, steps)
+    res["aabb_pairs"] = bench_pairs(dev, mesh, oc, cand, steps)
+    return res
+
+
+def bench_dual(dev, oc, labels, steps):
+    """construct_surface_dual_graph of the flood fill's dam + tide +
+    dry-adjacent cells at 1024^3, and the three dam wet masks.  Algorithmic
+    bytes: 12 B read per listed cell; 12 B cell + 64 B cube_idx + 48 B
+    adj_idx written per active cell, 24 B ijk + 12 B world per vertex."""
+    from atom3d_b200.apps import (construct_surface_dual_graph, get_dam_wet_corners, get_dam_wet_edges,
+                                  get_dam_wet_faces)
+
+    dam, tide, dry = labels["dam_ijk"], labels["tide_ijk"], labels["dry_adjacent_ijk"]
+    g_ms = _time_ms(lambda: construct_surface_dual_graph(dam, tide, dry, oc), steps)
+    w, vijk, ci, adj, cells = construct_surface_dual_graph(dam, tide, dry, oc)
+    n_in = dam.shape[0] + tide.shape[0] + dry.shape[0]
+    alg = 12.0 * n_in + 124.0 * cells.shape[0] + 36.0 * vijk.shape[0]
+    peak, kind = peaks()
+    wet_ms = _time_ms(lambda: (get_dam_wet_faces(dam, tide, 1024), get_dam_wet_edges(dam, tide, 1024),
+                               get_dam_wet_corners(dam, tide, 1024)), steps)
+    return {"ms": g_ms, "active_cells": int(cells.shape[0]), "vertices": int(vijk.shape[0]),
+            "listed_cells": int(n_in),
+            "roofline": {"bound": "hbm", "achieved": alg / (g_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (g_ms * 1e-3) / 1e9 / peak, "peak_kind": kind,
+                         "bytes": "12 B/listed cell + 124 B/active cell + 36 B/vertex (whole call, host syncs included)"},
+            "wet_masks_ms": wet_ms, "dam_cells": int(dam.shape[0])}
+
+
+def bench_pairs(dev, mesh, oc, cand, steps):
+    """MeshBVH.intersect_aabb on the level-10 octree candidates of the
+    327,680-triangle mesh (mode 1: SAT pairs; mode 3: clipped polygons), and
+    the reference demo's workload (80-face icosphere at 512^3, mode 3)."""
+    from atom3d_b200 import MeshBVH, OctreeIndexer, synthetic
+
+    mn, mx = oc.cube_aabb_level(cand, 10)
+    out = {"boxes": int(mn.shape[0])}
+    for mode in (1, 3):
+        ms = _time_ms(lambda: mesh.intersect_aabb(mn, mx, mode=mode), steps)
+        r = mesh.intersect_aabb(mn, mx, mode=mode)
+        out[f"mode{mode}"] = {"ms": ms, "pairs": int(r.aabb_ids.numel()), "mpairs_s": r.aabb_ids.numel() / ms / 1e3}
+    v, f = synthetic.icosphere(1)
+    ico = MeshBVH(v.to(dev), f.to(dev))
+    oc9 = OctreeIndexer(max_level=9, bounds=ico.get_bounds(), device=dev)
+    c9 = oc9.octree_traverse(ico)
+    a, b = oc9.cube_aabb_level(c9, 9)
+    ms = _time_ms(lambda: ico.intersect_aabb(a, b, mode=3), steps)
+    r = ico.intersect_aabb(a, b, mode=3)
+    out["demo_icosphere_512"] = {"boxes": int(a.shape[0]), "ms": ms, "polygons": int(r.poly_counts.numel()),
+                                 "reference_demo_polygons": 1172044,
+                                 "poly_counts_range": [int(r.poly_counts.min()), int(r.poly_counts.max())]}
+    return out
 
 
 def launches_per_udf():

@@ -169,19 +169,31 @@ int a3d_aabb_hit(const a3d_bvh_view* bvh, const float* box_min, const float* box
  * sat_clip_polygon_kernel (atom3d/kernels/cumtv_kernels.cu:209-460).
  *   mode 1: faces passing SAT;  modes 2, 3: faces passing SAT whose clip
  *   against the box (eps 1e-8) is non-empty.
- * Count pass: hit[n] (uint8) = box has a pair; totals_out (host, 2): [0]
- * pairs, [1] faces passing SAT over all boxes.  Synchronises.  The counts
- * stay in the workspace for the write pass, which writes the pairs grouped
- * by box (ascending), in tree order within a box:
- *   aabb_ids, face_ids  int32 [P] (mode 1) or int64 [P] (modes 2, 3)
- *   poly_counts int32 [P], centroids f32 [P,3], areas f32 [P]  (modes 2, 3)
- *   poly_verts f32 [P,8,3], 16-byte aligned, zero padded      (mode 3) */
+ * Protocol (each call synchronises once; the workspaces carry state from
+ * call to call):
+ *   1. a3d_aabb_pairs_count: per-box SAT counts; *num_candidates_out = the
+ *      number of SAT pairs.  Mode 1 also fills hit[n] (uint8).
+ *   2. modes 2, 3 only: a clip workspace of
+ *      a3d_aabb_clip_workspace_bytes(num_candidates) bytes, then
+ *      a3d_aabb_pairs_clip: hit[n] and *num_pairs_out (clip survivors).
+ *   3. a3d_aabb_pairs_write into outputs sized by the pair count, grouped
+ *      by box (ascending), in tree order within a box:
+ *        aabb_ids, face_ids  int32 [P] (mode 1) or int64 [P] (modes 2, 3)
+ *        poly_counts int32 [P], centroids f32 [P,3], areas f32 [P]  (2, 3)
+ *        poly_verts f32 [P,8,3], 16-byte aligned, zero padded       (3)
+ *      (mode 1 ignores the clip workspace). */
 size_t a3d_aabb_pairs_workspace_bytes(int64_t n);
+size_t a3d_aabb_clip_workspace_bytes(int64_t num_candidates);
 int a3d_aabb_pairs_count(const a3d_bvh_view* bvh, const float* box_min, const float* box_max,
                          int64_t n, int mode, uint8_t* hit, void* workspace,
-                         size_t workspace_bytes, int64_t* totals_out, a3d_stream_t stream);
+                         size_t workspace_bytes, int64_t* num_candidates_out, a3d_stream_t stream);
+int a3d_aabb_pairs_clip(const a3d_bvh_view* bvh, const float* box_min, const float* box_max,
+                        int64_t n, void* workspace, size_t workspace_bytes, void* clip_workspace,
+                        size_t clip_workspace_bytes, int64_t num_candidates, uint8_t* hit,
+                        int64_t* num_pairs_out, a3d_stream_t stream);
 int a3d_aabb_pairs_write(const a3d_bvh_view* bvh, const float* box_min, const float* box_max,
                          int64_t n, int mode, void* workspace, size_t workspace_bytes,
+                         void* clip_workspace, size_t clip_workspace_bytes, int64_t num_candidates,
                          void* aabb_ids, void* face_ids, int32_t* poly_counts, float* centroids,
                          float* areas, float* poly_verts, a3d_stream_t stream);
 
@@ -243,6 +255,18 @@ int a3d_flood_extract(const a3d_flood_geom* geom, void* workspace, size_t worksp
 /* out[i] = 1 when voxel ijk[i] carries the label. */
 int a3d_flood_test(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes,
                    int label, const int64_t* ijk, int64_t n, uint8_t* out, a3d_stream_t stream);
+
+/* ---- device-wide primitives (no reference counterpart) ------------------ */
+/* The library's own exclusive scan and stable LSD radix sort, for callers
+ * building their own compactions and orders.  out [n+1] int64: out[i] =
+ * sum of in[0..i), out[n] = total.  The sort orders (keys, vals) in place by
+ * key bits [begin_bit, end_bit), stably; n < 2^32. */
+size_t a3d_exclusive_scan_workspace_bytes(int64_t n);
+int a3d_exclusive_scan_u32(const uint32_t* in, int64_t n, int64_t* out, void* workspace,
+                           size_t workspace_bytes, a3d_stream_t stream);
+size_t a3d_sort_pairs_workspace_bytes(int64_t n);
+int a3d_sort_pairs_u64(uint64_t* keys, uint32_t* vals, int64_t n, int begin_bit, int end_bit,
+                       void* workspace, size_t workspace_bytes, a3d_stream_t stream);
 
 /* ---- surface dual graph and dam wet masks -------------------------------- */
 /* Replace construct_surface_dual_graph and get_dam_wet_faces / _edges /

@@ -969,3 +969,17 @@ void orc_aabb_pairs_fill(const float* V, const int32_t* F, int64_t nf, const flo
   par_for(n, 16, pairs_body, &c);
   free(tb);
 }
+
+typedef struct { const float* mn; const float* mx; const float* tri; float eps; int32_t* counts; } clipb_ctx;
+static void clipb_body(int64_t k, void* c_) {
+  clipb_ctx* c = (clipb_ctx*)c_;
+  float verts[24], cen[3], ar;
+  int cnt = 0;
+  orc_clip_pair(c->mn + 3 * k, c->mx + 3 * k, c->tri + 9 * k, c->eps, verts, &cnt, cen, &ar);
+  c->counts[k] = cnt;
+}
+/* clipped polygon vertex count of each (box k, triangle k) */
+void orc_clip_batch(const float* mn, const float* mx, const float* tri9, int64_t m, float eps, int32_t* counts) {
+  clipb_ctx c = {mn, mx, tri9, eps, counts};
+  par_for(m, 4096, clipb_body, &c);
+}

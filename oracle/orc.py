@@ -363,3 +363,11 @@ def aabb_pairs(V, F, bmin, bmax, mode=1, eps=1e-8):
     if mode == 3:
         out["poly_verts"] = pv
     return out
+
+
+def clip_counts(bmin, bmax, tri9, eps=1e-8):
+    """Clipped polygon vertex count for each row (box k, triangle k)."""
+    mn, mx, t = _f32(bmin).reshape(-1, 3), _f32(bmax).reshape(-1, 3), _f32(tri9).reshape(-1, 9)
+    out = np.empty(mn.shape[0], np.int32)
+    lib().orc_clip_batch(_p(mn), _p(mx), _p(t), I64(mn.shape[0]), ctypes.c_float(eps), _p(out))
+    return out
