@@ -40,6 +40,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 METRIC = "UDF Mqueries/s (plain traversal, 1.31M-triangle mesh, 16M queries)"
+# DRAM read + write of one udf_task_kernel launch per query, from the ncu
+# capture summarised in profiles/udf_task_kernel_full.md (4,194,304 queries:
+# 1.508 GB); traffic scales with the query count (the tree stays in L2)
+DRAM_BYTES_PER_QUERY = 1.507714e9 / 4194304
+TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, 4,194,304-query capture scaled per query"
 UNIT = "Mqueries/s"
 WORKLOAD = "udf_large: icosphere L8 (1,310,720 tris) + 16 sinusoids, 16,777,216 mixed queries"
 
@@ -299,8 +304,8 @@ def main():
         per_q = 32.0 + 24.0 * counts["nodes_per_query"] + 36.0 * counts["tris_per_query"]
         achieved = per_q * n / (kernel_ms * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "peak_kind": peak_kind, "bytes_per_query": per_q,
-                "kernel": "udf_kernel", "kernel_ms": kernel_ms}
+                "traffic": DRAM_BYTES_PER_QUERY * n, "traffic_source": TRAFFIC_SOURCE, "peak_kind": peak_kind,
+                "bytes_per_query": per_q, "kernel": "udf_task_kernel", "kernel_ms": kernel_ms}
     total_q = n * world
     line = {
         "metric": METRIC, "value": total_q / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world, "steps": args.steps,
