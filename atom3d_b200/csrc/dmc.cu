@@ -32,6 +32,11 @@ namespace {
 
 __constant__ unsigned char kCE[24] = {0, 1, 1, 5, 4, 5, 0, 4, 2, 3, 3, 7, 6, 7, 2, 6, 2, 0, 3, 1, 7, 5, 6, 4};
 
+// the packed edge list of dual vertex j of case c; edge k = (w >> 4k) & 15,
+// 15 = none
+__device__ __forceinline__ uint32_t vd_edges(int c, int j) { return __ldg(&kDmcPacked[c][j]); }
+__device__ __forceinline__ int vd_edge(uint32_t w, int k) { return (int)((w >> (4 * k)) & 15u); }
+
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fsb(float a, float b) { return __fsub_rn(a, b); }
@@ -108,11 +113,13 @@ __device__ __forceinline__ uint64_t hash64(uint64_t k) {
   return k;
 }
 
-__global__ void prob_insert_kernel(DmcIn in, int64_t ns, const uint32_t* __restrict__ list,
+// Stage-B kernels run over all N cubes and read the surface-cube count Ns
+// from the device (no host round trip before the crossing count).
+__global__ void prob_insert_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
                                    const uint8_t* __restrict__ cases, unsigned long long* __restrict__ table,
                                    uint64_t mask) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ns) return;
+  if (t >= (int64_t)*ns_dev) return;
   const uint32_t i = list[t];
   const int c = cases[i];
   if (kCheck[c][0] != 1) return;
@@ -126,11 +133,11 @@ __global__ void prob_insert_kernel(DmcIn in, int64_t ns, const uint32_t* __restr
   }
 }
 
-__global__ void case_fix_kernel(DmcIn in, int64_t ns, const uint32_t* __restrict__ list,
+__global__ void case_fix_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
                                 const uint8_t* __restrict__ cases, const unsigned long long* __restrict__ table,
                                 uint64_t mask, uint8_t* __restrict__ case_s) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ns) return;
+  if (t >= (int64_t)*ns_dev) return;
   const uint32_t i = list[t];
   const int c = cases[i];
   int out = c;
@@ -157,10 +164,14 @@ __device__ __forceinline__ void edge_ends(const DmcIn& in, uint32_t cube, int e,
   i1 = in.cidx[8 * (int64_t)cube + kCE[2 * e + 1]];
 }
 
-__global__ void cross_count_kernel(DmcIn in, int64_t ns, const uint32_t* __restrict__ list,
+__global__ void cross_count_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
                                    uint16_t* __restrict__ mask12, uint32_t* __restrict__ cnt) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ns) return;
+  if (t >= in.n) return;
+  if (t >= (int64_t)*ns_dev) {  // the scan runs over all N entries
+    cnt[t] = 0;
+    return;
+  }
   const uint32_t i = list[t];
   uint32_t m = 0;
 #pragma unroll
@@ -174,11 +185,11 @@ __global__ void cross_count_kernel(DmcIn in, int64_t ns, const uint32_t* __restr
   cnt[t] = (uint32_t)__popc(m);
 }
 
-__global__ void cross_write_kernel(DmcIn in, int64_t ns, const uint32_t* __restrict__ list,
+__global__ void cross_write_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
                                    const uint16_t* __restrict__ mask12, const uint32_t* __restrict__ off,
                                    uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ns) return;
+  if (t >= (int64_t)*ns_dev) return;
   const uint32_t i = list[t];
   uint32_t m = mask12[t];
   uint32_t o = off[t];
@@ -191,6 +202,52 @@ __global__ void cross_write_kernel(DmcIn in, int64_t ns, const uint32_t* __restr
     vals[o] = (uint32_t)(t * 12 + e);
     ++o;
   }
+}
+
+// Sort of the crossing entries by (key, val), key = i0 * M + i1 with i0 < i1,
+// as a counting sort on the lower endpoint i0: each corner is the lower
+// endpoint of at most 6 grid edges, each shared by at most 4 cubes, so a
+// group holds at most 24 entries and every entry finds its place by ranking
+// itself within its group.  vals grow with the input position, so the order
+// equals a stable sort by key.
+__global__ void edge_count_kernel(const uint64_t* __restrict__ keys, int64_t nc, uint64_t m,
+                                  uint32_t* __restrict__ lo_of, uint32_t* __restrict__ cnt) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nc) return;
+  const uint32_t i0 = (uint32_t)(keys[j] / m);
+  lo_of[j] = i0;
+  atomicAdd(&cnt[i0], 1u);
+}
+
+__global__ void edge_scatter_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals, int64_t nc,
+                                    const uint32_t* __restrict__ lo_of, const uint32_t* __restrict__ start,
+                                    uint32_t* __restrict__ fill, uint64_t* __restrict__ keys_g,
+                                    uint32_t* __restrict__ vals_g, uint32_t* __restrict__ lo_g) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nc) return;
+  const uint32_t i0 = lo_of[j];
+  const uint32_t p = start[i0] + atomicAdd(&fill[i0], 1u);
+  keys_g[p] = keys[j];
+  vals_g[p] = vals[j];
+  lo_g[p] = i0;
+}
+
+__global__ void edge_rank_kernel(const uint64_t* __restrict__ keys_g, const uint32_t* __restrict__ vals_g, int64_t nc,
+                                 const uint32_t* __restrict__ lo_g, const uint32_t* __restrict__ start,
+                                 uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nc) return;
+  const uint32_t i0 = lo_g[p];
+  const uint32_t b = start[i0], e = start[i0 + 1];
+  const uint64_t k = keys_g[p];
+  const uint32_t v = vals_g[p];
+  uint32_t rank = 0;
+  for (uint32_t q = b; q < e; ++q) {
+    const uint64_t kq = keys_g[q];
+    rank += (kq < k || (kq == k && vals_g[q] < v)) ? 1u : 0u;
+  }
+  keys[b + rank] = k;
+  vals[b + rank] = v;
 }
 
 __global__ void run_flag_kernel(const uint64_t* __restrict__ k, int64_t n, uint32_t* __restrict__ flag) {
@@ -215,10 +272,17 @@ __global__ void run_info_kernel(const uint64_t* __restrict__ k, const uint32_t* 
   }
 }
 
-__global__ void quad_flag_kernel(int64_t ne, int64_t nc, const uint32_t* __restrict__ rfirst,
+// runs over nc >= ne entries (ne, the unique-edge count, stays on the device);
+// flags beyond ne are zero so the scan can run over nc
+__global__ void quad_flag_kernel(const uint32_t* __restrict__ ne_dev, int64_t nc, const uint32_t* __restrict__ rfirst,
                                  uint32_t* __restrict__ qflag) {
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= ne) return;
+  if (r >= nc) return;
+  const int64_t ne = *ne_dev;
+  if (r >= ne) {
+    qflag[r] = 0;
+    return;
+  }
   const int64_t end = r + 1 < ne ? rfirst[r + 1] : nc;
   qflag[r] = (end - rfirst[r]) == 4 ? 1u : 0u;
 }
@@ -229,17 +293,21 @@ __global__ void vd_class_kernel(int64_t ns, const uint8_t* __restrict__ case_s, 
   if (t < ns) f[t] = kNumVd[case_s[t]] == cls ? 1u : 0u;
 }
 
+// class_totals[c-1] = number of surface cubes with c dual vertices (device)
 __global__ void vd_assign_kernel(int64_t ns, const uint8_t* __restrict__ case_s, int cls,
-                                 const uint32_t* __restrict__ f, const uint32_t* __restrict__ rank, uint32_t base,
-                                 uint32_t* __restrict__ vd_cube, uint8_t* __restrict__ vd_slot,
-                                 uint32_t* __restrict__ vd_ne) {
+                                 const uint32_t* __restrict__ f, const uint32_t* __restrict__ rank,
+                                 const uint32_t* __restrict__ class_totals, uint32_t* __restrict__ vd_cube,
+                                 uint8_t* __restrict__ vd_slot, uint32_t* __restrict__ vd_ne) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ns || !f[t]) return;
+  uint32_t base = 0;
+  for (int k = 1; k < cls; ++k) base += (uint32_t)k * class_totals[k - 1];
   const int c = case_s[t];
   const uint32_t v0 = base + rank[t] * (uint32_t)cls;
   for (int j = 0; j < cls; ++j) {
+    const uint32_t w = vd_edges(c, j);
     uint32_t ne = 0;
-    for (int k = 0; k < 7; ++k) ne += kDmcTable[c][j][k] != -1 ? 1u : 0u;
+    for (int k = 0; k < 7; ++k) ne += vd_edge(w, k) != 15 ? 1u : 0u;
     vd_cube[v0 + j] = (uint32_t)t;
     vd_slot[v0 + j] = (uint8_t)j;
     vd_ne[v0 + j] = ne;
@@ -289,13 +357,14 @@ __global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, con
   const uint32_t t = vd_cube[v];
   const int j = vd_slot[v];
   const int c = case_s[t];
+  const uint32_t vedges = vd_edges(c, j);
   const uint32_t cube = list[t];
   const int64_t g0 = goff[v];
   float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
   int64_t g = g0;
   for (int k = 0; k < 7; ++k) {
-    const int e = kDmcTable[c][j][k];
-    if (e < 0) continue;
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
     const int64_t flat = (int64_t)t * 12 + e;
     const int32_t r = ed.idx_map[flat];
     const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
@@ -333,8 +402,8 @@ __global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, con
   float dist[7];
   g = g0;
   for (int k = 0; k < 7; ++k) {
-    const int e = kDmcTable[c][j][k];
-    if (e < 0) continue;
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
     const int32_t r = ed.idx_map[(int64_t)t * 12 + e];
     const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
     const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
@@ -429,6 +498,7 @@ __global__ void vd_bwd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv,
   const uint32_t t = vd_cube[v];
   const int j = vd_slot[v];
   const int c = case_s[t];
+  const uint32_t vedges = vd_edges(c, j);
   const uint32_t cube = list[t];
   const int64_t g0 = goff[v];
   // recompute the forward quantities of this dual vertex
@@ -438,8 +508,8 @@ __global__ void vd_bwd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv,
   int ne = 0;
   float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
   for (int k = 0; k < 7; ++k) {
-    const int e = kDmcTable[c][j][k];
-    if (e < 0) continue;
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
     const int32_t r = ed.idx_map[(int64_t)t * 12 + e];
     const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
     I0[ne] = i0; I1[ne] = i1; E[ne] = e;
@@ -587,7 +657,6 @@ struct DmcWs {
   uint64_t* keys2;
   uint32_t* vals;
   uint32_t* vals2;
-  uint32_t* rs;
   uint32_t* rflag;     // [12N]
   uint32_t* rid;       // [12N]
   int32_t* idx_map;    // [12N]
@@ -607,6 +676,8 @@ struct DmcWs {
   float* g_vd;         // [4N,3]
   uint32_t* scan_tmp;
   uint32_t* misc;      // counters
+  uint32_t* ecnt;      // [M] edge-sort group sizes, then fill counters
+  uint32_t* estart;    // [M+1] edge-sort group starts
   uint64_t table_mask;
 };
 
@@ -634,7 +705,6 @@ size_t carve_dmc(DmcWs& w, Workspace& ws, int64_t n, int64_t m) {
   w.keys2 = ws.take<uint64_t>(n12);
   w.vals = ws.take<uint32_t>(n12);
   w.vals2 = ws.take<uint32_t>(n12);
-  w.rs = ws.take<uint32_t>((int64_t)radix_sort_scratch_elems(n12));
   w.rflag = ws.take<uint32_t>(n12);
   w.rid = ws.take<uint32_t>(n12);
   w.idx_map = ws.take<int32_t>(n12);
@@ -654,16 +724,12 @@ size_t carve_dmc(DmcWs& w, Workspace& ws, int64_t n, int64_t m) {
   w.g_vd = ws.take<float>(12 * n + 3);
   w.scan_tmp = ws.take<uint32_t>((int64_t)scan_workspace_elems(n12 > 4 * n ? n12 : 4 * n));
   w.misc = ws.take<uint32_t>(16);
+  w.ecnt = ws.take<uint32_t>(m);
+  w.estart = ws.take<uint32_t>(m + 1);
   return ws.used;
 }
 
 unsigned gsz(int64_t n, int b = 256) { return (unsigned)ceil_div(n > 0 ? n : 1, b); }
-
-int read_u32(const uint32_t* d, uint32_t* h, cudaStream_t s) {
-  A3D_CUDA_TRY(cudaMemcpyAsync(h, d, 4, cudaMemcpyDeviceToHost, s));
-  A3D_CUDA_TRY(cudaStreamSynchronize(s));
-  return A3D_OK;
-}
 
 DmcIn make_in(const a3d_dmc_inputs* p) {
   DmcIn in;
@@ -706,72 +772,72 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   case_kernel<<<gsz(n), 256, 0, s>>>(in, w.cases, w.flag);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flag, w.off, n, w.scan_tmp, w.off + n, s)));
-  uint32_t ns32 = 0;
-  A3D_TRY(read_u32(w.off + n, &ns32, s));
-  const int64_t ns = ns32;
-  counts[0] = ns;
-  if (ns == 0) return A3D_OK;
+  // stage B over all N cubes with the surface count on the device
+  const uint32_t* ns_dev = w.off + n;
   compact_kernel<<<gsz(n), 256, 0, s>>>(n, w.flag, w.off, w.list);
   A3D_LAUNCH_CHECK();
   A3D_CUDA_TRY(cudaMemsetAsync(w.table, 0xff, (w.table_mask + 1) * sizeof(unsigned long long), s));
-  prob_insert_kernel<<<gsz(ns), 256, 0, s>>>(in, ns, w.list, w.cases, w.table, w.table_mask);
+  prob_insert_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.cases, w.table, w.table_mask);
   A3D_LAUNCH_CHECK();
-  case_fix_kernel<<<gsz(ns), 256, 0, s>>>(in, ns, w.list, w.cases, w.table, w.table_mask, w.case_s);
+  case_fix_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.cases, w.table, w.table_mask, w.case_s);
   A3D_LAUNCH_CHECK();
-  cross_count_kernel<<<gsz(ns), 256, 0, s>>>(in, ns, w.list, w.mask12, w.ccnt);
+  cross_count_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.mask12, w.ccnt);
   A3D_LAUNCH_CHECK();
-  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ccnt, w.coff, ns, w.scan_tmp, w.coff + ns, s)));
-  uint32_t nc32 = 0;
-  A3D_TRY(read_u32(w.coff + ns, &nc32, s));
-  const int64_t nc = nc32;
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ccnt, w.coff, n, w.scan_tmp, w.coff + n, s)));
+  cross_write_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.mask12, w.coff, w.keys, w.vals);
+  A3D_LAUNCH_CHECK();
+  // the one round trip before the edge sort: surface cubes and crossings
+  uint32_t h2[2];
+  A3D_CUDA_TRY(cudaMemcpyAsync(h2, ns_dev, 4, cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaMemcpyAsync(h2 + 1, w.coff + n, 4, cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  const int64_t ns = h2[0], nc = h2[1];
+  counts[0] = ns;
   counts[1] = nc;  // crossing (cube, edge) entries == groups
-  cross_write_kernel<<<gsz(ns), 256, 0, s>>>(in, ns, w.list, w.mask12, w.coff, w.keys, w.vals);
+  if (ns == 0) return A3D_OK;
+  // counting sort of the crossings by (key, val); rid / rflag hold the
+  // lower endpoints until the run pass needs them
+  A3D_CUDA_TRY(cudaMemsetAsync(w.ecnt, 0, m * sizeof(uint32_t), s));
+  edge_count_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, nc, (uint64_t)m, w.rid, w.ecnt);
   A3D_LAUNCH_CHECK();
-  int bits = 1;
-  while (bits < 64 && ((unsigned __int128)1 << bits) < (unsigned __int128)m * (unsigned __int128)m) ++bits;
-  bool alt = false;
-  A3D_TRY(radix_sort_pairs<uint64_t>(w.keys, w.vals, w.keys2, w.vals2, nc, 0, ((bits + 7) / 8) * 8, w.rs, &alt, s));
-  const uint64_t* sk = alt ? w.keys2 : w.keys;
-  const uint32_t* sv = alt ? w.vals2 : w.vals;
-  if (alt) {
-    A3D_CUDA_TRY(cudaMemcpyAsync(w.keys, sk, nc * 8, cudaMemcpyDeviceToDevice, s));
-    A3D_CUDA_TRY(cudaMemcpyAsync(w.vals, sv, nc * 4, cudaMemcpyDeviceToDevice, s));
-  }
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ecnt, w.estart, m, w.scan_tmp, w.estart + m, s)));
+  A3D_CUDA_TRY(cudaMemsetAsync(w.ecnt, 0, m * sizeof(uint32_t), s));
+  edge_scatter_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, w.vals, nc, w.rid, w.estart, w.ecnt, w.keys2, w.vals2, w.rflag);
+  A3D_LAUNCH_CHECK();
+  edge_rank_kernel<<<gsz(nc), 256, 0, s>>>(w.keys2, w.vals2, nc, w.rflag, w.estart, w.keys, w.vals);
+  A3D_LAUNCH_CHECK();
   run_flag_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, nc, w.rflag);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.rflag, w.rid, nc, w.scan_tmp, w.misc, s)));
-  uint32_t ne32 = 0;
-  A3D_TRY(read_u32(w.misc, &ne32, s));
-  const int64_t ne = ne32;
-  counts[2] = ne;
   A3D_CUDA_TRY(cudaMemsetAsync(w.idx_map, 0xff, 12 * ns * sizeof(int32_t), s));
   A3D_CUDA_TRY(cudaMemsetAsync(w.vd_map, 0, 12 * ns * sizeof(int32_t), s));
   run_info_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, w.vals, nc, w.rflag, w.rid, m, w.idx_map, w.e0, w.e1, w.rfirst);
   A3D_LAUNCH_CHECK();
-  quad_flag_kernel<<<gsz(ne), 256, 0, s>>>(ne, nc, w.rfirst, w.qflag);
+  quad_flag_kernel<<<gsz(nc), 256, 0, s>>>(w.misc, nc, w.rfirst, w.qflag);
   A3D_LAUNCH_CHECK();
-  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.qflag, w.qoff, ne, w.scan_tmp, w.qoff + ne, s)));
-  uint32_t nq32 = 0;
-  A3D_TRY(read_u32(w.qoff + ne, &nq32, s));
-  counts[3] = nq32;
-  // dual vertices per vertex-count class 1..4
-  uint32_t base = 0;
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.qflag, w.qoff, nc, w.scan_tmp, w.qoff + nc, s)));
+  // dual vertices per vertex-count class 1..4; class totals in misc[4..7]
+  A3D_CUDA_TRY(cudaMemsetAsync(w.vd_ne, 0, (4 * ns + 1) * sizeof(uint32_t), s));
   for (int cls = 1; cls <= 4; ++cls) {
     vd_class_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, cls, w.cls_f);
     A3D_LAUNCH_CHECK();
-    A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.cls_f, w.cls_r, ns, w.scan_tmp, w.cls_r + ns, s)));
-    vd_assign_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, cls, w.cls_f, w.cls_r, base, w.vd_cube, w.vd_slot,
+    A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.cls_f, w.cls_r, ns, w.scan_tmp, w.misc + 3 + cls, s)));
+    vd_assign_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, cls, w.cls_f, w.cls_r, w.misc + 4, w.vd_cube, w.vd_slot,
                                              w.vd_ne);
     A3D_LAUNCH_CHECK();
-    uint32_t cnt = 0;
-    A3D_TRY(read_u32(w.cls_r + ns, &cnt, s));
-    base += cnt * (uint32_t)cls;
   }
-  const int64_t nv = base;
-  counts[4] = nv;
-  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.vd_ne, w.goff, nv, w.scan_tmp, w.goff + nv, s)));
-  uint32_t ng = 0;
-  A3D_TRY(read_u32(w.goff + nv, &ng, s));
+  // per-vertex edge offsets over the 4 Ns bound (entries past the last
+  // vertex are zero)
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.vd_ne, w.goff, 4 * ns, w.scan_tmp, w.goff + 4 * ns, s)));
+  uint32_t h8[8];
+  A3D_CUDA_TRY(cudaMemcpyAsync(h8, w.misc, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  uint32_t nq32 = 0, ng = 0;
+  A3D_CUDA_TRY(cudaMemcpyAsync(&nq32, w.qoff + nc, 4, cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaMemcpyAsync(&ng, w.goff + 4 * ns, 4, cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  counts[2] = h8[0];
+  counts[3] = nq32;
+  counts[4] = (int64_t)h8[4] + 2 * (int64_t)h8[5] + 3 * (int64_t)h8[6] + 4 * (int64_t)h8[7];
   counts[5] = ng;
   A3D_REQUIRE((int64_t)ng == nc, A3D_ERR_ARGUMENT, "dmc_prepare: crossing edges without a dual vertex (bad tables?)");
   return A3D_OK;
@@ -972,13 +1038,14 @@ __global__ void vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float
   const uint32_t t = vd_cube[v];
   const int j = vd_slot[v];
   const int c = case_s[t];
+  const uint32_t vedges = vd_edges(c, j);
   const uint32_t cube = list[t];
   const int64_t g0 = goff[v];
   float z[7][3], nn[7][3];
   int ne = 0;
   for (int k = 0; k < 7; ++k) {
-    const int e = kDmcTable[c][j][k];
-    if (e < 0) continue;
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
     const int64_t flat = (int64_t)t * 12 + e;
     const int32_t r = ed.idx_map[flat];
     const int64_t i0 = ed.e0[r], i1 = ed.e1[r];

@@ -42,15 +42,26 @@ def main(path: str) -> None:
         assert t[k].shape == s, (k, t[k].shape)
     # check_table's last column holds a case id (0..255): store it as uint8
     lines = ["// Generated by atom3d_b200/mesh_extractor/gen_tables.py -- DMC lookup tables.", "#pragma once", ""]
-    lines.append("__constant__ signed char kDmcTable[256][4][7] = {")
+    # Threads of one warp index these tables with different case ids, so they
+    # live in global memory (cached loads) rather than constant memory (one
+    # serialised access per distinct address).
+    lines.append("// kDmcPacked[c][j]: the up to 7 cube edges of dual vertex j of case c,")
+    lines.append("// edge k in bits 4k..4k+3, 0xF = no edge")
+    lines.append("__device__ const unsigned int kDmcPacked[256][4] = {")
     for c in range(256):
-        rows = ", ".join("{" + ", ".join(str(int(x)) for x in t["dmc_table"][c, j]) + "}" for j in range(4))
-        lines.append(f"  {{{rows}}},")
+        words = []
+        for j in range(4):
+            w = 0
+            for k in range(7):
+                e = int(t["dmc_table"][c, j, k])
+                w |= (0xF if e < 0 else e) << (4 * k)
+            words.append(f"0x{w:07x}u")
+        lines.append("  {" + ", ".join(words) + "},")
     lines.append("};")
-    lines.append("__constant__ unsigned char kNumVd[256] = {" +
+    lines.append("__device__ const unsigned char kNumVd[256] = {" +
                  ", ".join(str(int(x)) for x in t["num_vd_table"]) + "};")
     lines.append("// check: [flag, dx, dy, dz, replacement case]")
-    lines.append("__constant__ short kCheck[256][5] = {")
+    lines.append("__device__ const short kCheck[256][5] = {")
     for c in range(256):
         lines.append("  {" + ", ".join(str(int(x)) for x in t["check_table"][c]) + "},")
     lines.append("};")
