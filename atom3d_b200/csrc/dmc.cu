@@ -347,7 +347,9 @@ __device__ __forceinline__ void edge_normal(const float* x0, const float* x1, fl
 
 __device__ __forceinline__ float ldf(const float* p, int64_t i) { return __ldg(p + i); }
 
-// one thread per dual vertex: crossings, weighted average, L_dev
+// one thread per dual vertex: crossings, weighted average, L_dev.  The edge
+// loop is unrolled over the 7 table slots, so each edge's plain crossing
+// and distance stay in registers for the L_dev pass (one gather per edge).
 __global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, const uint32_t* __restrict__ list,
                           const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
                           const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
@@ -361,7 +363,9 @@ __global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, con
   const uint32_t cube = list[t];
   const int64_t g0 = goff[v];
   float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
+  float z[7][3];
   int64_t g = g0;
+#pragma unroll
   for (int k = 0; k < 7; ++k) {
     const int e = vd_edge(vedges, k);
     if (e == 15) continue;
@@ -374,6 +378,7 @@ __global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, con
     const float b = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
     const float w0 = fm(s1, a1), w1 = -fm(s0, a0);
     const float den = fa(w0, w1);
+    const float pw0 = s1, pw1 = -s0, pden = fa(pw0, pw1);
     float xa[3], xb[3], n[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) { xa[a] = ldf(x, 3 * i0 + a); xb[a] = ldf(x, 3 * i1 + a); }
@@ -384,6 +389,7 @@ __global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, con
       out.palpha[3 * g + a] = ue;
       out.nalpha[3 * g + a] = n[a];
       acc[a] = fa(acc[a], fm(ue, b));
+      z[k][a] = interp1(xa[a], xb[a], pw0, pw1, pden);  // the plain zero crossing
     }
     bsum = fa(bsum, b);
     out.vd_map[flat] = (int32_t)v;
@@ -400,27 +406,25 @@ __global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, con
   // L_dev: distances of the plain zero crossings to the dual vertex
   float msum = 0.f;
   float dist[7];
-  g = g0;
+#pragma unroll
   for (int k = 0; k < 7; ++k) {
-    const int e = vd_edge(vedges, k);
-    if (e == 15) continue;
-    const int32_t r = ed.idx_map[(int64_t)t * 12 + e];
-    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
-    const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
-    const float w0 = s1, w1 = -s0, dn = fa(w0, w1);
+    if (vd_edge(vedges, k) == 15) continue;
     float d2 = 0.f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float z = interp1(ldf(x, 3 * i0 + a), ldf(x, 3 * i1 + a), w0, w1, dn);
-      const float dd = fsb(z, vd[a]);
+      const float dd = fsb(z[k][a], vd[a]);
       d2 = fa(d2, fm(dd, dd));
     }
-    dist[g - g0] = sqrtf(d2);
-    msum = fa(msum, dist[g - g0]);
-    ++g;
+    dist[k] = sqrtf(d2);
+    msum = fa(msum, dist[k]);
   }
   const float mean = fd(msum, (float)ne);
-  for (int64_t q = 0; q < ne; ++q) out.ldev[g0 + q] = fabsf(fsb(dist[q], mean));
+  g = g0;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    if (vd_edge(vedges, k) == 15) continue;
+    out.ldev[g++] = fabsf(fsb(dist[k], mean));
+  }
 }
 
 __global__ void quad_kernel(int64_t ne, int64_t nc, const uint32_t* __restrict__ qflag, const uint32_t* __restrict__ qoff,
