@@ -471,6 +471,10 @@ constexpr int kTaskWarps = 2;
 constexpr int kTaskDepth = 32;
 constexpr int kSpillCap = 96;    // per-owner global overflow stack (entries)
 constexpr int kSpillChunk = 16;  // entries moved per spill / refill
+// A spill happens when a node's q <= 4 qualifying children do not fit, i.e.
+// with at least kTaskDepth - 2 entries on the stack, and moves a whole chunk:
+// the stack must then hold a chunk.
+static_assert(kTaskDepth - 2 >= kSpillChunk, "a spill needs a full chunk on the shared stack");
 constexpr int kTaskTriCap = 32 * kMaxLeafTris;
 constexpr int kTaskPool = 64;  // queries per pool taken from the global counter
 // register cap of the task kernel: each of the SM's four sub-partitions

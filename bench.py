@@ -217,10 +217,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip every measurement besides the main UDF line")
     ap.add_argument("--skip", default="", help="comma-separated extra sections to skip: learned,dmc,octree,rays,batch")
+    ap.add_argument("--section", default="", choices=["", "dmc", "octree", "rays", "batch"],
+                    help="run one extra section alone on cuda:0 and print its JSON (for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.section:
+        return run_section(args)
 
     rank, world, local = setup_dist(args.gpus)
     torch.cuda.set_device(local)
@@ -340,6 +344,25 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_section(args):
+    """One extra section alone (its own workload and timing), for profiling."""
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    steps = max(2, args.steps)
+    if args.section == "dmc":
+        out = bench_dmc(dev, steps, args.warmup, cpu=False)
+    elif args.section == "octree":
+        out = bench_octree_flood(dev, steps, args.warmup)
+    elif args.section == "batch":
+        out = bench_batch(dev, 2, 1, cpu=False)
+    else:
+        from atom3d_b200 import MeshBVH, synthetic
+
+        v, f, _ = synthetic.udf_large(n_queries=1)
+        out = bench_rays(dev, MeshBVH(v.to(dev), f.to(dev)), v, steps)
+    print(json.dumps({"section": args.section, **out}), flush=True)
 
 
 def _time_ms(fn, steps, warmup=2):
