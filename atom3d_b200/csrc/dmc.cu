@@ -910,46 +910,55 @@ namespace a3d {
 namespace {
 
 struct GradWs {
-  float* x;         // [M,3]
-  uint64_t* keys;   // [12N]
-  uint64_t* keys2;
-  uint32_t* vals;
-  uint32_t* vals2;
-  uint32_t* rs;
-  double* acc;      // [M][9]: DtD xx xy xz yy yz zz, Dtb x y z
+  float* x;          // [M,3]
+  uint32_t* cnt;     // [2M] edges per corner as first endpoint (0..M-1), as second (M..2M-1)
+  uint32_t* start;   // [2M+1]
+  uint32_t* other;   // [24N] the other endpoint of each cube edge, grouped by corner slot
+  uint32_t* scan_tmp;
 };
 
 size_t carve_grad(GradWs& w, Workspace& ws, int64_t n, int64_t m) {
-  const int64_t n12 = 12 * n;
   w.x = ws.take<float>(3 * m);
-  w.keys = ws.take<uint64_t>(n12);
-  w.keys2 = ws.take<uint64_t>(n12);
-  w.vals = ws.take<uint32_t>(n12);
-  w.vals2 = ws.take<uint32_t>(n12);
-  w.rs = ws.take<uint32_t>((int64_t)radix_sort_scratch_elems(n12));
-  w.acc = ws.take<double>(9 * m);
+  w.cnt = ws.take<uint32_t>(2 * m);
+  w.start = ws.take<uint32_t>(2 * m + 1);
+  w.other = ws.take<uint32_t>(24 * n);
+  w.scan_tmp = ws.take<uint32_t>((int64_t)scan_workspace_elems(2 * m));
   return ws.used;
 }
 
-__global__ void all_edge_keys_kernel(DmcIn in, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+// Corner-gradient least squares (atom3d/mesh_extractor/sparse_diffdmc.py:
+// 451-513): every unique grid edge (a, b) -- cube edge e runs from corner
+// kCE[2e] to kCE[2e+1], so a shared edge has the same orientation in each of
+// its cubes -- adds d d^T to both ends and (s_b - s_a)/|x_b - x_a| d to a and
+// its negative to b, d = (x_b - x_a)/|x_b - x_a|.  Instead of sorting the
+// 12 N edge keys to find the unique ones, each corner gathers its own edges
+// from two adjacency lists (as first and as second endpoint), skips repeats
+// of the same neighbour (an edge is listed once per cube holding it) and
+// sums in ascending neighbour order: deterministic FP64 sums, no atomics.
+__global__ void edge_adj_count_kernel(DmcIn in, uint32_t* __restrict__ cnt) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= in.n * 12) return;
   const int64_t i = t / 12;
   const int e = (int)(t % 12);
-  const uint64_t a = (uint64_t)in.cidx[8 * i + kCE[2 * e]], b = (uint64_t)in.cidx[8 * i + kCE[2 * e + 1]];
-  keys[t] = a * (uint64_t)in.m + b;
-  vals[t] = (uint32_t)t;
+  const int64_t a = in.cidx[8 * i + kCE[2 * e]], b = in.cidx[8 * i + kCE[2 * e + 1]];
+  atomicAdd(&cnt[a], 1u);
+  atomicAdd(&cnt[in.m + b], 1u);
 }
 
-// each unique (ordered) corner pair once: d (x) d to both ends, the edge's
-// gradient projection times d to the first and its negative to the second
-__global__ void edge_lsq_kernel(DmcIn in, const uint64_t* __restrict__ keys, int64_t nk, const float* __restrict__ x,
-                                double* __restrict__ acc) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nk) return;
-  const uint64_t k = keys[r];
-  if (r > 0 && keys[r - 1] == k) return;
-  const int64_t i0 = (int64_t)(k / (uint64_t)in.m), i1 = (int64_t)(k % (uint64_t)in.m);
+__global__ void edge_adj_fill_kernel(DmcIn in, const uint32_t* __restrict__ start, uint32_t* __restrict__ fill,
+                                     uint32_t* __restrict__ other) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= in.n * 12) return;
+  const int64_t i = t / 12;
+  const int e = (int)(t % 12);
+  const int64_t a = in.cidx[8 * i + kCE[2 * e]], b = in.cidx[8 * i + kCE[2 * e + 1]];
+  other[start[a] + atomicAdd(&fill[a], 1u)] = (uint32_t)b;
+  other[start[in.m + b] + atomicAdd(&fill[in.m + b], 1u)] = (uint32_t)a;
+}
+
+// contribution of edge (i0 -> i1): d d^T in o, the gradient projection in f
+__device__ __forceinline__ void edge_terms(const DmcIn& in, const float* __restrict__ x, int64_t i0, int64_t i1,
+                                           double o[6], double f[3]) {
   float ev[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) ev[a] = fsb(ldf(x, 3 * i1 + a), ldf(x, 3 * i0 + a));
@@ -959,21 +968,52 @@ __global__ void edge_lsq_kernel(DmcIn in, const uint64_t* __restrict__ keys, int
   for (int a = 0; a < 3; ++a) d[a] = fd(ev[a], el);
   const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
   const float gp = fd(fsb(s1, s0), el);
-  const double o[6] = {(double)fm(d[0], d[0]), (double)fm(d[0], d[1]), (double)fm(d[0], d[2]),
-                       (double)fm(d[1], d[1]), (double)fm(d[1], d[2]), (double)fm(d[2], d[2])};
-  double* a0 = acc + 9 * i0;
-  double* a1 = acc + 9 * i1;
+  o[0] = (double)fm(d[0], d[0]); o[1] = (double)fm(d[0], d[1]); o[2] = (double)fm(d[0], d[2]);
+  o[3] = (double)fm(d[1], d[1]); o[4] = (double)fm(d[1], d[2]); o[5] = (double)fm(d[2], d[2]);
 #pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    atomicAdd(a0 + q, o[q]);
-    atomicAdd(a1 + q, o[q]);
-  }
+  for (int a = 0; a < 3; ++a) f[a] = (double)fm(gp, d[a]);
+}
+
+__device__ __forceinline__ void solve_sym3(const double* a, const double* b, double* xo);
+
+// one thread per corner: gather, regularise (1e-4 I), solve
+__global__ void corner_gradient_kernel(DmcIn in, const float* __restrict__ x, const uint32_t* __restrict__ start,
+                                       const uint32_t* __restrict__ other, float* __restrict__ grad) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= in.m) return;
+  double A[6] = {0, 0, 0, 0, 0, 0}, B[3] = {0, 0, 0};
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const double f = (double)fm(gp, d[a]);
-    atomicAdd(a0 + 6 + a, f);
-    atomicAdd(a1 + 6 + a, -f);
+  for (int side = 0; side < 2; ++side) {  // 0: c is the first endpoint, 1: the second
+    const uint32_t b = start[side * in.m + c], e = start[side * in.m + c + 1];
+    bool any = false;
+    uint32_t last = 0;
+    for (;;) {  // the distinct neighbours in ascending order
+      bool found = false;
+      uint32_t nxt = 0xffffffffu;
+      for (uint32_t q = b; q < e; ++q) {
+        const uint32_t v = other[q];
+        if ((!any || v > last) && v <= nxt) { nxt = v; found = true; }
+      }
+      if (!found) break;
+      double o[6], f[3];
+      if (side == 0) edge_terms(in, x, c, nxt, o, f);
+      else edge_terms(in, x, nxt, c, o, f);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) A[q] += o[q];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) B[a] += side == 0 ? f[a] : -f[a];
+      any = true;
+      last = nxt;
+    }
   }
+  A[0] += 1e-4;
+  A[3] += 1e-4;
+  A[5] += 1e-4;
+  double g[3];
+  solve_sym3(A, B, g);
+  const bool bad = isnan(g[0]) || isnan(g[1]) || isnan(g[2]);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) grad[3 * c + q] = bad ? 0.f : (float)g[q];
 }
 
 // solves the symmetric 3x3 system (a: xx xy xz yy yz zz) by cofactors
@@ -985,23 +1025,6 @@ __device__ __forceinline__ void solve_sym3(const double* a, const double* b, dou
   xo[0] = (c00 * b[0] + c01 * b[1] + c02 * b[2]) * inv;
   xo[1] = (c01 * b[0] + c11 * b[1] + c12 * b[2]) * inv;
   xo[2] = (c02 * b[0] + c12 * b[1] + c22 * b[2]) * inv;
-}
-
-__global__ void corner_solve_kernel(int64_t m, const double* __restrict__ acc, float* __restrict__ grad) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
-  double a[6], b[3], g[3];
-#pragma unroll
-  for (int q = 0; q < 6; ++q) a[q] = acc[9 * i + q];
-  a[0] += 1e-4;
-  a[3] += 1e-4;
-  a[5] += 1e-4;
-#pragma unroll
-  for (int q = 0; q < 3; ++q) b[q] = acc[9 * i + 6 + q];
-  solve_sym3(a, b, g);
-  const bool bad = isnan(g[0]) || isnan(g[1]) || isnan(g[2]);
-#pragma unroll
-  for (int q = 0; q < 3; ++q) grad[3 * i + q] = bad ? 0.f : (float)g[q];
 }
 
 // crossing normal from the corner gradients, confidence-weighted by their
@@ -1217,17 +1240,14 @@ extern "C" int a3d_dmc_corner_gradients(const a3d_dmc_inputs* p, void* workspace
   corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, 2.0f / (float)p->resolution, w.x);
   A3D_LAUNCH_CHECK();
   const int64_t nk = 12 * n;
-  all_edge_keys_kernel<<<gsz(nk), 256, 0, s>>>(in, w.keys, w.vals);
+  A3D_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, sizeof(uint32_t) * 2 * m, s));
+  edge_adj_count_kernel<<<gsz(nk), 256, 0, s>>>(in, w.cnt);
   A3D_LAUNCH_CHECK();
-  int bits = 1;
-  while (bits < 64 && ((uint64_t)1 << bits) <= (uint64_t)m * (uint64_t)m) ++bits;
-  bool alt = false;
-  A3D_TRY(radix_sort_pairs<uint64_t>(w.keys, w.vals, w.keys2, w.vals2, nk, 0, bits, w.rs, &alt, s));
-  const uint64_t* keys = alt ? w.keys2 : w.keys;
-  A3D_CUDA_TRY(cudaMemsetAsync(w.acc, 0, sizeof(double) * 9 * m, s));
-  edge_lsq_kernel<<<gsz(nk), 256, 0, s>>>(in, keys, nk, w.x, w.acc);
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.cnt, w.start, 2 * m, w.scan_tmp, w.start + 2 * m, s)));
+  A3D_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, sizeof(uint32_t) * 2 * m, s));
+  edge_adj_fill_kernel<<<gsz(nk), 256, 0, s>>>(in, w.start, w.cnt, w.other);
   A3D_LAUNCH_CHECK();
-  corner_solve_kernel<<<gsz(m), 256, 0, s>>>(m, w.acc, gradients);
+  corner_gradient_kernel<<<gsz(m), 256, 0, s>>>(in, w.x, w.start, w.other, gradients);
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }

@@ -73,10 +73,33 @@ __global__ void bbox32_kernel(const int32_t* __restrict__ ijk, int64_t n, int* _
       hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
     }
   }
-  if ((threadIdx.x & 31) == 0) {
+  // one atomic per block and bound: warps meet in shared memory first
+  __shared__ int s_b[6][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  if (lane == 0) {
     for (int a = 0; a < 3; ++a) {
-      atomicMin(&bb[a], lo[a]);
-      atomicMax(&bb[3 + a], hi[a]);
+      s_b[a][warp] = lo[a];
+      s_b[3 + a][warp] = hi[a];
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = lane < nwarps ? s_b[a][lane] : INT_MAX;
+      hi[a] = lane < nwarps ? s_b[3 + a][lane] : INT_MIN;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const int l = __shfl_xor_sync(0xffffffffu, lo[a], o), h = __shfl_xor_sync(0xffffffffu, hi[a], o);
+        lo[a] = l < lo[a] ? l : lo[a];
+        hi[a] = h > hi[a] ? h : hi[a];
+      }
+    }
+    if (lane == 0) {
+      for (int a = 0; a < 3; ++a) {
+        atomicMin(&bb[a], lo[a]);
+        atomicMax(&bb[3 + a], hi[a]);
+      }
     }
   }
 }
