@@ -40,7 +40,7 @@ def _rank_main(rank, world, port, out):
 
 def test_replicas_max_over_ranks_and_throughput():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
         res = dict(out)
