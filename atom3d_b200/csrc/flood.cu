@@ -480,21 +480,27 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
   const uint8_t one = 1;
   A3D_CUDA_TRY(cudaMemcpyAsync(w.dirty + sb, &one, 1, cudaMemcpyHostToDevice, s));
   uint8_t *cur = w.dirty, *nxt = w.dirty2;
+  // Rounds are queued kRoundsPerCheck at a time and the "changed" flag of the
+  // last one is read once per group: a round with no dirty brick does
+  // nothing, so the rounds past convergence only cost their launch.
+  constexpr int kRoundsPerCheck = 4;
   int rounds = 0;
   const int max_rounds = 1 << 20;
-  for (; rounds < max_rounds; ++rounds) {
-    A3D_CUDA_TRY(cudaMemsetAsync(nxt, 0, nbricks, s));
-    A3D_CUDA_TRY(cudaMemsetAsync(w.misc + 1, 0, 4, s));
-    flood_brick_kernel<<<(unsigned)nbricks, kBX * kBY, 0, s>>>(g, w.occ, w.water, cur, nxt, nbx, nby, 4 * (kBX + kBY),
-                                                                w.misc + 1);
-    A3D_LAUNCH_CHECK();
+  while (rounds < max_rounds) {
+    for (int k = 0; k < kRoundsPerCheck; ++k, ++rounds) {
+      A3D_CUDA_TRY(cudaMemsetAsync(nxt, 0, nbricks, s));
+      A3D_CUDA_TRY(cudaMemsetAsync(w.misc + 1, 0, 4, s));
+      flood_brick_kernel<<<(unsigned)nbricks, kBX * kBY, 0, s>>>(g, w.occ, w.water, cur, nxt, nbx, nby,
+                                                                  4 * (kBX + kBY), w.misc + 1);
+      A3D_LAUNCH_CHECK();
+      uint8_t* t = cur; cur = nxt; nxt = t;
+    }
     uint32_t any = 0;
     A3D_CUDA_TRY(cudaMemcpyAsync(&any, w.misc + 1, 4, cudaMemcpyDeviceToHost, s));
     A3D_CUDA_TRY(cudaStreamSynchronize(s));
-    uint8_t* t = cur; cur = nxt; nxt = t;
     if (!any) break;
   }
-  if (rounds_out) *rounds_out = rounds + 1;
+  if (rounds_out) *rounds_out = rounds;
   const unsigned gw = (unsigned)ceil_div(nwords, 256);
   labels_kernel<<<gw, 256, 0, s>>>(g, w.occ, w.water, w.lab, nwords);
   A3D_LAUNCH_CHECK();
