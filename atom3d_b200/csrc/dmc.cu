@@ -288,22 +288,38 @@ __global__ void quad_flag_kernel(const uint32_t* __restrict__ ne_dev, int64_t nc
 }
 
 // per-surface-cube dual-vertex bookkeeping (vertex count class 1..4)
-__global__ void vd_class_kernel(int64_t ns, const uint8_t* __restrict__ case_s, int cls, uint32_t* __restrict__ f) {
+// Dual-vertex numbering by vertex-count class (1..4), then cube order, then
+// slot.  One pass flags each surface cube's class in two 64-bit words --
+// classes 1 and 2 in the low and high halves of one, 3 and 4 of the other --
+// so two scans give every cube its rank within its class and the class
+// totals at once (counts stay below 2^28: no carry crosses a half).
+__global__ void vd_class_kernel(int64_t ns, const uint8_t* __restrict__ case_s, uint64_t* __restrict__ fa,
+                                uint64_t* __restrict__ fb) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < ns) f[t] = kNumVd[case_s[t]] == cls ? 1u : 0u;
+  if (t >= ns) return;
+  const int cls = kNumVd[case_s[t]];
+  fa[t] = (uint64_t)(cls == 1) | ((uint64_t)(cls == 2) << 32);
+  fb[t] = (uint64_t)(cls == 3) | ((uint64_t)(cls == 4) << 32);
 }
 
-// class_totals[c-1] = number of surface cubes with c dual vertices (device)
-__global__ void vd_assign_kernel(int64_t ns, const uint8_t* __restrict__ case_s, int cls,
-                                 const uint32_t* __restrict__ f, const uint32_t* __restrict__ rank,
-                                 const uint32_t* __restrict__ class_totals, uint32_t* __restrict__ vd_cube,
+__device__ __forceinline__ uint32_t class_field(uint64_t a, uint64_t b, int cls) {
+  const uint64_t w = cls <= 2 ? a : b;
+  return (uint32_t)((cls & 1) ? (w & 0xffffffffull) : (w >> 32));
+}
+
+// ra / rb: exclusive scans of the class words, totals at [ns]
+__global__ void vd_assign_kernel(int64_t ns, const uint8_t* __restrict__ case_s, const uint64_t* __restrict__ ra,
+                                 const uint64_t* __restrict__ rb, uint32_t* __restrict__ vd_cube,
                                  uint8_t* __restrict__ vd_slot, uint32_t* __restrict__ vd_ne) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ns || !f[t]) return;
-  uint32_t base = 0;
-  for (int k = 1; k < cls; ++k) base += (uint32_t)k * class_totals[k - 1];
+  if (t >= ns) return;
   const int c = case_s[t];
-  const uint32_t v0 = base + rank[t] * (uint32_t)cls;
+  const int cls = kNumVd[c];
+  if (cls < 1 || cls > 4) return;
+  const uint64_t ta = ra[ns], tb = rb[ns];
+  uint32_t base = 0;
+  for (int k = 1; k < cls; ++k) base += (uint32_t)k * class_field(ta, tb, k);
+  const uint32_t v0 = base + class_field(ra[t], rb[t], cls) * (uint32_t)cls;
   for (int j = 0; j < cls; ++j) {
     const uint32_t w = vd_edges(c, j);
     uint32_t ne = 0;
@@ -480,15 +496,16 @@ __device__ __forceinline__ void scatter_interp_grad(const DmcIn& in, const float
                                                     float ue[3], float w0, float w1, float den, int64_t i0, int64_t i1,
                                                     float& gw0, float& gw1, DmcGrad& gr) {
   // ue = (xa w0 + xb w1) / den: d/dxa = w0/den, d/dxb = w1/den,
-  // d/dw0 = (xa - ue)/den, d/dw1 = (xb - ue)/den
+  // d/dw0 = (xa - ue)/den, d/dw1 = (xb - ue)/den (one division per edge)
+  const float inv = 1.0f / den;
   gw0 = 0.f;
   gw1 = 0.f;
   for (int a = 0; a < 3; ++a) {
-    gw0 += gue[a] * (xa[a] - ue[a]) / den;
-    gw1 += gue[a] * (xb[a] - ue[a]) / den;
+    gw0 += gue[a] * (xa[a] - ue[a]) * inv;
+    gw1 += gue[a] * (xb[a] - ue[a]) * inv;
     if (gr.g_deform) {
-      atomicAdd(&gr.g_deform[3 * i0 + a], gue[a] * w0 / den);
-      atomicAdd(&gr.g_deform[3 * i1 + a], gue[a] * w1 / den);
+      atomicAdd(&gr.g_deform[3 * i0 + a], gue[a] * w0 * inv);
+      atomicAdd(&gr.g_deform[3 * i1 + a], gue[a] * w1 * inv);
     }
   }
 }
@@ -561,29 +578,32 @@ __global__ void vd_bwd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv,
       gD[q] += gl * sg;
       gmean -= gl * sg;
     }
-    for (int q = 0; q < ne; ++q) gD[q] += gmean / (float)ne;
+    const float gm = gmean / (float)ne;
+    for (int q = 0; q < ne; ++q) gD[q] += gm;
   }
   // dist -> crossing z and dual vertex
   float gZ[7][3];
   for (int q = 0; q < ne; ++q) {
+    const float invd = D[q] > 0.f ? 1.0f / D[q] : 0.f;
     for (int a = 0; a < 3; ++a) {
-      const float u = D[q] > 0.f ? (Z[q][a] - vd[a]) / D[q] : 0.f;
+      const float u = (Z[q][a] - vd[a]) * invd;
       gZ[q][a] = gD[q] * u;
       gvd[a] -= gD[q] * u;
     }
   }
   // vd = sum(b ue) / (sum b + 1e-8)
+  const float inv_bden = 1.0f / bden;
   float gB = 0.f;
-  for (int a = 0; a < 3; ++a) gB -= gvd[a] * vd[a] / bden;
+  for (int a = 0; a < 3; ++a) gB -= gvd[a] * vd[a] * inv_bden;
   for (int q = 0; q < ne; ++q) {
     const int e = E[q];
     const int64_t i0 = I0[q], i1 = I1[q];
     float gue[3];
     float gb = gB;
     for (int a = 0; a < 3; ++a) {
-      gue[a] = gvd[a] * B[q] / bden;
+      gue[a] = gvd[a] * B[q] * inv_bden;
       if (gr.g_palpha) gue[a] += gr.g_palpha[3 * (g0 + q) + a];
-      gb += gvd[a] * UE[q][a] / bden;
+      gb += gvd[a] * UE[q][a] * inv_bden;
     }
     float xa[3], xb[3];
     for (int a = 0; a < 3; ++a) { xa[a] = x[3 * i0 + a]; xb[a] = x[3 * i1 + a]; }
@@ -674,8 +694,11 @@ struct DmcWs {
   uint8_t* vd_slot;    // [4N]
   uint32_t* vd_ne;     // [4N]
   uint32_t* goff;      // [4N]
-  uint32_t* cls_f;     // [N]
-  uint32_t* cls_r;     // [N]
+  uint64_t* cls_a;     // [N] class words (classes 1, 2) and their scan [N+1]
+  uint64_t* cls_ra;
+  uint64_t* cls_b;     // classes 3, 4
+  uint64_t* cls_rb;
+  uint64_t* scan_tmp64;
   int32_t* quads;      // [12N/4*4]
   float* g_vd;         // [4N,3]
   uint32_t* scan_tmp;
@@ -722,8 +745,11 @@ size_t carve_dmc(DmcWs& w, Workspace& ws, int64_t n, int64_t m) {
   w.vd_slot = ws.take<uint8_t>(4 * n + 1);
   w.vd_ne = ws.take<uint32_t>(4 * n + 1);
   w.goff = ws.take<uint32_t>(4 * n + 2);
-  w.cls_f = ws.take<uint32_t>(n);
-  w.cls_r = ws.take<uint32_t>(n + 1);
+  w.cls_a = ws.take<uint64_t>(n);
+  w.cls_ra = ws.take<uint64_t>(n + 1);
+  w.cls_b = ws.take<uint64_t>(n);
+  w.cls_rb = ws.take<uint64_t>(n + 1);
+  w.scan_tmp64 = ws.take<uint64_t>((int64_t)scan_workspace_elems(n));
   w.quads = ws.take<int32_t>(n12);
   w.g_vd = ws.take<float>(12 * n + 3);
   w.scan_tmp = ws.take<uint32_t>((int64_t)scan_workspace_elems(n12 > 4 * n ? n12 : 4 * n));
@@ -820,28 +846,29 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   quad_flag_kernel<<<gsz(nc), 256, 0, s>>>(w.misc, nc, w.rfirst, w.qflag);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.qflag, w.qoff, nc, w.scan_tmp, w.qoff + nc, s)));
-  // dual vertices per vertex-count class 1..4; class totals in misc[4..7]
+  // dual vertices numbered per vertex-count class (two packed scans)
   A3D_CUDA_TRY(cudaMemsetAsync(w.vd_ne, 0, (4 * ns + 1) * sizeof(uint32_t), s));
-  for (int cls = 1; cls <= 4; ++cls) {
-    vd_class_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, cls, w.cls_f);
-    A3D_LAUNCH_CHECK();
-    A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.cls_f, w.cls_r, ns, w.scan_tmp, w.misc + 3 + cls, s)));
-    vd_assign_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, cls, w.cls_f, w.cls_r, w.misc + 4, w.vd_cube, w.vd_slot,
-                                             w.vd_ne);
-    A3D_LAUNCH_CHECK();
-  }
+  vd_class_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, w.cls_a, w.cls_b);
+  A3D_LAUNCH_CHECK();
+  A3D_TRY((device_exclusive_scan<uint64_t, uint64_t>(w.cls_a, w.cls_ra, ns, w.scan_tmp64, w.cls_ra + ns, s)));
+  A3D_TRY((device_exclusive_scan<uint64_t, uint64_t>(w.cls_b, w.cls_rb, ns, w.scan_tmp64, w.cls_rb + ns, s)));
+  vd_assign_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, w.cls_ra, w.cls_rb, w.vd_cube, w.vd_slot, w.vd_ne);
+  A3D_LAUNCH_CHECK();
   // per-vertex edge offsets over the 4 Ns bound (entries past the last
   // vertex are zero)
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.vd_ne, w.goff, 4 * ns, w.scan_tmp, w.goff + 4 * ns, s)));
-  uint32_t h8[8];
-  A3D_CUDA_TRY(cudaMemcpyAsync(h8, w.misc, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  uint32_t nq32 = 0, ng = 0;
+  uint32_t ne32 = 0, nq32 = 0, ng = 0;
+  uint64_t tot[2] = {0, 0};
+  A3D_CUDA_TRY(cudaMemcpyAsync(&ne32, w.misc, 4, cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaMemcpyAsync(&nq32, w.qoff + nc, 4, cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaMemcpyAsync(&ng, w.goff + 4 * ns, 4, cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaMemcpyAsync(tot, w.cls_ra + ns, 8, cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaMemcpyAsync(tot + 1, w.cls_rb + ns, 8, cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
-  counts[2] = h8[0];
+  counts[2] = ne32;
   counts[3] = nq32;
-  counts[4] = (int64_t)h8[4] + 2 * (int64_t)h8[5] + 3 * (int64_t)h8[6] + 4 * (int64_t)h8[7];
+  counts[4] = (int64_t)(tot[0] & 0xffffffffull) + 2 * (int64_t)(tot[0] >> 32) + 3 * (int64_t)(tot[1] & 0xffffffffull) +
+              4 * (int64_t)(tot[1] >> 32);
   counts[5] = ng;
   A3D_REQUIRE((int64_t)ng == nc, A3D_ERR_ARGUMENT, "dmc_prepare: crossing edges without a dual vertex (bad tables?)");
   return A3D_OK;
