@@ -92,14 +92,35 @@ __global__ void corner_pos_kernel(DmcIn in, float ws, float* __restrict__ x) {
   }
 }
 
-__global__ void case_kernel(DmcIn in, uint8_t* __restrict__ cases, uint32_t* __restrict__ flag) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= in.n) return;
-  uint32_t c = 0;
+// corner positions and case ids in one pass over cube_idx: thread (cube,
+// corner) writes its corner's position and its sign bit; the 8 lanes of a
+// cube (aligned groups of 8) OR their bits into the case id
+__global__ void corner_case_kernel(DmcIn in, float ws, float* __restrict__ x, uint8_t* __restrict__ cases,
+                                   uint32_t* __restrict__ flag) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = t < in.n * 8;
+  const int c = (int)(t & 7);
+  uint32_t bit = 0;
+  if (valid) {
+    const int64_t i = t >> 3;
+    const int64_t mi = in.cidx[t];
+    const int off[3] = {c & 1, (c >> 1) & 1, (c >> 2) & 1};
 #pragma unroll
-  for (int k = 0; k < 8; ++k) c |= (fsb(in.sdf[in.cidx[8 * i + k]], in.iso) < 0.f ? 1u : 0u) << k;
-  cases[i] = (uint8_t)c;
-  flag[i] = (c != 0u && c != 255u) ? 1u : 0u;
+    for (int a = 0; a < 3; ++a) {
+      const float g = fa((float)in.vox[3 * i + a], (float)off[a]);
+      float v = fsb(fm(g, ws), 1.0f);
+      if (in.deform) v = fa(v, in.deform[3 * mi + a]);
+      x[3 * mi + a] = v;
+    }
+    bit = (fsb(in.sdf[mi], in.iso) < 0.f ? 1u : 0u) << c;
+  }
+  bit |= __shfl_xor_sync(0xffffffffu, bit, 1);
+  bit |= __shfl_xor_sync(0xffffffffu, bit, 2);
+  bit |= __shfl_xor_sync(0xffffffffu, bit, 4);
+  if (valid && c == 0) {
+    cases[t >> 3] = (uint8_t)bit;
+    flag[t >> 3] = (bit != 0u && bit != 255u) ? 1u : 0u;
+  }
 }
 
 __global__ void compact_kernel(int64_t n, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off,
@@ -797,9 +818,7 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   const float wsc = (float)(2.0 / (double)p->resolution);
   init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x);
   A3D_LAUNCH_CHECK();
-  corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, wsc, w.x);
-  A3D_LAUNCH_CHECK();
-  case_kernel<<<gsz(n), 256, 0, s>>>(in, w.cases, w.flag);
+  corner_case_kernel<<<gsz(8 * n), 256, 0, s>>>(in, wsc, w.x, w.cases, w.flag);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flag, w.off, n, w.scan_tmp, w.off + n, s)));
   // stage B over all N cubes with the surface count on the device
