@@ -638,11 +638,17 @@ def bench_octree_flood(dev, steps, warmup):
     e1.record(stream)
     torch.cuda.synchronize()
     oct_ms = e0.elapsed_time(e1) / steps
-    for _ in range(max(1, warmup - 2)):
+    # each call returns ~4.8 GB of label coordinates: the previous result is
+    # released before the next call, so the timed calls reuse its memory
+    # instead of timing fresh device allocations
+    out = None
+    for _ in range(max(2, warmup - 1)):
+        out = None
         out = sparse_flood_fill(mesh, 1024, min_level=4, bounds=bounds, verbose=False)
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(steps):
+        out = None
         out = sparse_flood_fill(mesh, 1024, min_level=4, bounds=bounds, verbose=False)
     e1.record(stream)
     torch.cuda.synchronize()
