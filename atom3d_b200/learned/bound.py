@@ -6,7 +6,7 @@ from samples produced by the plain traversal itself; a calibrated margin
 turns its prediction into a per-query upper bound that seeds the traversal's
 pruning radius (``MeshBVH.udf(points, bound=...)``).  Queries whose bound
 turns out too small are re-run without it, so results are identical with or
-without the network; the plain method is the judge of the bound's misses.
+without the network; the plain method decides which bounds missed.
 
 Training and inference run in hand-written BF16 tensor-core kernels
 (a3d_gemm_bf16, a3d_mlp_* in csrc/mlp.cu); PyTorch only holds the buffers.

@@ -9,7 +9,7 @@ Gradients flow to sdf, deform, alpha and beta like the reference's autograd
 graph.  The QEF inference mode (a module in eval mode, or inference_mode
 "qef") runs a3d_dmc_corner_gradients (unless corner_gradients are given)
 and a3d_dmc_emit_qef; it is forward-only.  Per-vertex features are not
-provided by this build and raise NotImplementedError.
+provided and raise NotImplementedError.
 """
 
 from __future__ import annotations

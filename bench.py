@@ -10,8 +10,9 @@ queries (distance, face id, closest point) through the C ABI.
   e2e    : queries/s through MeshBVH.udf with pinned host buffers, H2D of
            the queries and D2H of the results inside the timed region
   roofline.achieved : algorithmic bytes of the traversal kernel per launch
-           (per-query reference-layout bytes) / its average
-           CUDA-event duration
+           (32 B of I/O + 24 B per node box + 36 B per triangle test of the
+           plain method on the reference's binary tree, per query) / its
+           average CUDA-event duration
   cpu_baseline : the CPU brute-force port of the reference's closest-point
            maths on a bounded query sample, all host threads
 
