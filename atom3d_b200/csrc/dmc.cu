@@ -55,6 +55,15 @@ struct DmcIn {
   float wscale;           // weight_scale
 };
 
+// Corner id of entry t of cube_idx.  An id outside [0, m) reads as corner 0,
+// so no kernel dereferences it; corner_case_kernel flags it and
+// a3d_dmc_prepare reports it as an argument error at its first host read
+// (the reference's torch indexing raises for such an index).
+__device__ __forceinline__ int64_t corner_at(const DmcIn& in, int64_t t) {
+  const int64_t v = in.cidx[t];
+  return (uint64_t)v < (uint64_t)in.m ? v : 0;
+}
+
 // interpolation of one edge: (x0*w0 + x1*w1) / (w0 + w1), w0 = s1, w1 = -s0
 __device__ __forceinline__ float interp1(float x0, float x1, float w0, float w1, float den) {
   return fd(fa(fm(x0, w0), fm(x1, w1)), den);
@@ -65,8 +74,12 @@ __device__ __forceinline__ float norm_w(float v, float ws, bool given) {
 }
 
 // ---- stage A ---------------------------------------------------------------
-__global__ void init_pos_kernel(int64_t m, const float* __restrict__ deform, float* __restrict__ x) {
+// also clears the word corner_case_kernel flags out-of-range corner ids in
+// (when given)
+__global__ void init_pos_kernel(int64_t m, const float* __restrict__ deform, float* __restrict__ x,
+                                uint32_t* __restrict__ bad_index) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (bad_index && i == 0) *bad_index = 0u;
   if (i >= m) return;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -81,7 +94,7 @@ __global__ void corner_pos_kernel(DmcIn in, float ws, float* __restrict__ x) {
   if (t >= in.n * 8) return;
   const int64_t i = t >> 3;
   const int c = (int)(t & 7);
-  const int64_t mi = in.cidx[t];
+  const int64_t mi = corner_at(in, t);
   const int off[3] = {c & 1, (c >> 1) & 1, (c >> 2) & 1};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -96,14 +109,15 @@ __global__ void corner_pos_kernel(DmcIn in, float ws, float* __restrict__ x) {
 // corner) writes its corner's position and its sign bit; the 8 lanes of a
 // cube (aligned groups of 8) OR their bits into the case id
 __global__ void corner_case_kernel(DmcIn in, float ws, float* __restrict__ x, uint8_t* __restrict__ cases,
-                                   uint32_t* __restrict__ flag) {
+                                   uint32_t* __restrict__ flag, uint32_t* __restrict__ bad_index) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = t < in.n * 8;
   const int c = (int)(t & 7);
   uint32_t bit = 0;
   if (valid) {
     const int64_t i = t >> 3;
-    const int64_t mi = in.cidx[t];
+    if ((uint64_t)in.cidx[t] >= (uint64_t)in.m) *bad_index = 1u;
+    const int64_t mi = corner_at(in, t);
     const int off[3] = {c & 1, (c >> 1) & 1, (c >> 2) & 1};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -121,6 +135,18 @@ __global__ void corner_case_kernel(DmcIn in, float ws, float* __restrict__ x, ui
     cases[t >> 3] = (uint8_t)bit;
     flag[t >> 3] = (bit != 0u && bit != 255u) ? 1u : 0u;
   }
+}
+
+// copies scattered device words into one block, so that the host reads
+// them with one copy instead of one copy each
+struct WordList {
+  const uint32_t* src[8];
+  int n;
+};
+
+__global__ void gather_words_kernel(WordList l, uint32_t* __restrict__ out) {
+  const int k = (int)threadIdx.x;
+  if (k < l.n) out[k] = *l.src[k];
 }
 
 __global__ void compact_kernel(int64_t n, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off,
@@ -181,8 +207,8 @@ __global__ void case_fix_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, c
 }
 
 __device__ __forceinline__ void edge_ends(const DmcIn& in, uint32_t cube, int e, int64_t& i0, int64_t& i1) {
-  i0 = in.cidx[8 * (int64_t)cube + kCE[2 * e]];
-  i1 = in.cidx[8 * (int64_t)cube + kCE[2 * e + 1]];
+  i0 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e]);
+  i1 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e + 1]);
 }
 
 __global__ void cross_count_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
@@ -816,9 +842,12 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   if (n == 0 || m == 0) return A3D_OK;
   DmcIn in = make_in(p);
   const float wsc = (float)(2.0 / (double)p->resolution);
-  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x);
+  // misc[1]: out-of-range corner ids; misc[4..6] and misc[8..14]: the words
+  // the two host reads take
+  uint32_t* bad_index = w.misc + 1;
+  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x, bad_index);
   A3D_LAUNCH_CHECK();
-  corner_case_kernel<<<gsz(8 * n), 256, 0, s>>>(in, wsc, w.x, w.cases, w.flag);
+  corner_case_kernel<<<gsz(8 * n), 256, 0, s>>>(in, wsc, w.x, w.cases, w.flag, bad_index);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flag, w.off, n, w.scan_tmp, w.off + n, s)));
   // stage B over all N cubes with the surface count on the device
@@ -835,12 +864,15 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ccnt, w.coff, n, w.scan_tmp, w.coff + n, s)));
   cross_write_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.mask12, w.coff, w.keys, w.vals);
   A3D_LAUNCH_CHECK();
-  // the one round trip before the edge sort: surface cubes and crossings
-  uint32_t h2[2];
-  A3D_CUDA_TRY(cudaMemcpyAsync(h2, ns_dev, 4, cudaMemcpyDeviceToHost, s));
-  A3D_CUDA_TRY(cudaMemcpyAsync(h2 + 1, w.coff + n, 4, cudaMemcpyDeviceToHost, s));
+  // the one round trip before the edge sort: surface cubes, crossings and
+  // the out-of-range flag
+  uint32_t h3[3];
+  gather_words_kernel<<<1, 32, 0, s>>>(WordList{{ns_dev, w.coff + n, bad_index}, 3}, w.misc + 4);
+  A3D_LAUNCH_CHECK();
+  A3D_CUDA_TRY(cudaMemcpyAsync(h3, w.misc + 4, sizeof(h3), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
-  const int64_t ns = h2[0], nc = h2[1];
+  A3D_REQUIRE(h3[2] == 0u, A3D_ERR_ARGUMENT, "dmc_prepare: cube_idx holds a corner id outside [0, num_corners)");
+  const int64_t ns = h3[0], nc = h3[1];
   counts[0] = ns;
   counts[1] = nc;  // crossing (cube, edge) entries == groups
   if (ns == 0) return A3D_OK;
@@ -876,14 +908,18 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   // per-vertex edge offsets over the 4 Ns bound (entries past the last
   // vertex are zero)
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.vd_ne, w.goff, 4 * ns, w.scan_tmp, w.goff + 4 * ns, s)));
-  uint32_t ne32 = 0, nq32 = 0, ng = 0;
-  uint64_t tot[2] = {0, 0};
-  A3D_CUDA_TRY(cudaMemcpyAsync(&ne32, w.misc, 4, cudaMemcpyDeviceToHost, s));
-  A3D_CUDA_TRY(cudaMemcpyAsync(&nq32, w.qoff + nc, 4, cudaMemcpyDeviceToHost, s));
-  A3D_CUDA_TRY(cudaMemcpyAsync(&ng, w.goff + 4 * ns, 4, cudaMemcpyDeviceToHost, s));
-  A3D_CUDA_TRY(cudaMemcpyAsync(tot, w.cls_ra + ns, 8, cudaMemcpyDeviceToHost, s));
-  A3D_CUDA_TRY(cudaMemcpyAsync(tot + 1, w.cls_rb + ns, 8, cudaMemcpyDeviceToHost, s));
+  // unique edges, quads, edge groups and the two packed class totals (64-bit,
+  // low word first)
+  const uint32_t* ra = reinterpret_cast<const uint32_t*>(w.cls_ra + ns);
+  const uint32_t* rb = reinterpret_cast<const uint32_t*>(w.cls_rb + ns);
+  gather_words_kernel<<<1, 32, 0, s>>>(WordList{{w.misc, w.qoff + nc, w.goff + 4 * ns, ra, ra + 1, rb, rb + 1}, 7},
+                                       w.misc + 8);
+  A3D_LAUNCH_CHECK();
+  uint32_t h7[7];
+  A3D_CUDA_TRY(cudaMemcpyAsync(h7, w.misc + 8, sizeof(h7), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  const uint32_t ne32 = h7[0], nq32 = h7[1], ng = h7[2];
+  const uint64_t tot[2] = {(uint64_t)h7[3] | ((uint64_t)h7[4] << 32), (uint64_t)h7[5] | ((uint64_t)h7[6] << 32)};
   counts[2] = ne32;
   counts[3] = nq32;
   counts[4] = (int64_t)(tot[0] & 0xffffffffull) + 2 * (int64_t)(tot[0] >> 32) + 3 * (int64_t)(tot[1] & 0xffffffffull) +
@@ -986,7 +1022,7 @@ __global__ void edge_adj_count_kernel(DmcIn in, uint32_t* __restrict__ cnt) {
   if (t >= in.n * 12) return;
   const int64_t i = t / 12;
   const int e = (int)(t % 12);
-  const int64_t a = in.cidx[8 * i + kCE[2 * e]], b = in.cidx[8 * i + kCE[2 * e + 1]];
+  const int64_t a = corner_at(in, 8 * i + kCE[2 * e]), b = corner_at(in, 8 * i + kCE[2 * e + 1]);
   atomicAdd(&cnt[a], 1u);
   atomicAdd(&cnt[in.m + b], 1u);
 }
@@ -997,7 +1033,7 @@ __global__ void edge_adj_fill_kernel(DmcIn in, const uint32_t* __restrict__ star
   if (t >= in.n * 12) return;
   const int64_t i = t / 12;
   const int e = (int)(t % 12);
-  const int64_t a = in.cidx[8 * i + kCE[2 * e]], b = in.cidx[8 * i + kCE[2 * e + 1]];
+  const int64_t a = corner_at(in, 8 * i + kCE[2 * e]), b = corner_at(in, 8 * i + kCE[2 * e + 1]);
   other[start[a] + atomicAdd(&fill[a], 1u)] = (uint32_t)b;
   other[start[in.m + b] + atomicAdd(&fill[in.m + b], 1u)] = (uint32_t)a;
 }
@@ -1155,7 +1191,7 @@ __global__ void vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float
   for (int a = 0; a < 3; ++a) {
     float sacc = 0.f, lo = INFINITY, hi = -INFINITY;
     for (int k = 0; k < 8; ++k) {
-      const float p = ldf(x, 3 * in.cidx[8 * (int64_t)cube + k] + a);
+      const float p = ldf(x, 3 * corner_at(in, 8 * (int64_t)cube + k) + a);
       sacc = fa(sacc, p);
       lo = fminf(lo, p);
       hi = fmaxf(hi, p);
@@ -1281,7 +1317,7 @@ extern "C" int a3d_dmc_corner_gradients(const a3d_dmc_inputs* p, void* workspace
   A3D_CUDA_TRY(cudaMemsetAsync(gradients, 0, sizeof(float) * 3 * m, s));
   if (n == 0) return A3D_OK;
   DmcIn in = make_in(p);
-  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x);
+  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x, nullptr);
   A3D_LAUNCH_CHECK();
   corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, 2.0f / (float)p->resolution, w.x);
   A3D_LAUNCH_CHECK();

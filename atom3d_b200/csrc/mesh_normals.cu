@@ -19,10 +19,17 @@ namespace {
 
 __global__ void face_kernel(const float* __restrict__ V, const int32_t* __restrict__ F, int64_t nf, int64_t nv,
                             float* __restrict__ fn_sign, float* __restrict__ fn_unit, float* __restrict__ ang,
-                            float* __restrict__ vacc, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                            float* __restrict__ vacc, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                            uint32_t* __restrict__ bad_face) {
   const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nf) return;
-  const int64_t id[3] = {F[3 * f], F[3 * f + 1], F[3 * f + 2]};
+  int64_t id[3] = {F[3 * f], F[3 * f + 1], F[3 * f + 2]};
+  // a face index outside [0, nv) is reported after the edge count is read;
+  // until then the face reads as a point at vertex 0
+  if (id[0] < 0 || id[1] < 0 || id[2] < 0 || id[0] >= nv || id[1] >= nv || id[2] >= nv) {
+    *bad_face = 1u;
+    id[0] = id[1] = id[2] = 0;
+  }
   float p[3][3];
 #pragma unroll
   for (int k = 0; k < 3; ++k)
@@ -118,7 +125,7 @@ struct NrmWs {
   uint32_t* flag;
   uint32_t* eid;
   uint32_t* scan_tmp;
-  uint32_t* total;
+  uint32_t* total;  // [0] unique edges, [1] out-of-range face flag
 };
 size_t carve_nrm(NrmWs& w, Workspace& ws, int64_t nv, int64_t nf) {
   const int64_t nh = 3 * nf;
@@ -155,15 +162,19 @@ extern "C" int a3d_mesh_normals(const float* vertices, int64_t num_vertices, con
   A3D_REQUIRE(num_vertices > 0 && num_faces > 0, A3D_ERR_ARGUMENT, "mesh_normals: empty mesh");
   A3D_REQUIRE(num_faces < (1ll << 30), A3D_ERR_ARGUMENT, "mesh_normals: too many faces");
   A3D_REQUIRE(num_vertices < (1ll << 31), A3D_ERR_ARGUMENT, "mesh_normals: too many vertices");
+  A3D_REQUIRE(vertices && faces && face_normals_sign && face_angles && vertex_pn && he_edge_idx &&
+                  (edge_pn || edge_capacity == 0),
+              A3D_ERR_ARGUMENT, "mesh_normals: null pointer");
   Workspace ws(workspace, workspace_bytes);
   NrmWs w;
   carve_nrm(w, ws, num_vertices, num_faces);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "mesh_normals: workspace too small");
   const int64_t nh = 3 * num_faces;
   A3D_CUDA_TRY(cudaMemsetAsync(w.vacc, 0, sizeof(float) * 3 * num_vertices, s));
+  A3D_CUDA_TRY(cudaMemsetAsync(w.total, 0, sizeof(uint32_t) * 2, s));
   face_kernel<<<(unsigned)ceil_div(num_faces, 256), 256, 0, s>>>(vertices, faces, num_faces, num_vertices,
                                                                  face_normals_sign, w.fn_unit, face_angles, w.vacc,
-                                                                 w.keys, w.vals);
+                                                                 w.keys, w.vals, w.total + 1);
   A3D_LAUNCH_CHECK();
   normalize_rows_kernel<<<(unsigned)ceil_div(num_vertices, 256), 256, 0, s>>>(w.vacc, vertex_pn, num_vertices);
   A3D_LAUNCH_CHECK();
@@ -178,9 +189,11 @@ extern "C" int a3d_mesh_normals(const float* vertices, int64_t num_vertices, con
   run_start_kernel<<<(unsigned)ceil_div(nh, 256), 256, 0, s>>>(k, nh, w.flag);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flag, w.eid, nh, w.scan_tmp, w.total, s)));
-  uint32_t ne = 0;
-  A3D_CUDA_TRY(cudaMemcpyAsync(&ne, w.total, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  uint32_t h[2] = {0, 0};
+  A3D_CUDA_TRY(cudaMemcpyAsync(h, w.total, sizeof(h), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  A3D_REQUIRE(h[1] == 0u, A3D_ERR_ARGUMENT, "mesh_normals: face index outside [0, num_vertices)");
+  const uint32_t ne = h[0];
   if (num_edges_out) *num_edges_out = ne;
   A3D_REQUIRE((int64_t)ne <= edge_capacity, A3D_ERR_WORKSPACE, "mesh_normals: edge capacity too small");
   edge_kernel<<<(unsigned)ceil_div(nh, 256), 256, 0, s>>>(k, he, nh, w.flag, w.eid, w.fn_unit, edge_pn,

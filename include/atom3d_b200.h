@@ -74,7 +74,9 @@ int a3d_bvh_build(const float* vertices, int64_t num_vertices,
  * Outputs: face_normals_sign [F,3] (n/(|n|+1e-8), used by the sign test),
  * face_angles [F,3], vertex_pn [V,3], edge_pn [edge_capacity,3],
  * he_edge_idx [3F] int64 (half-edge -> edge id, edges numbered in ascending
- * key lo*V+hi order like torch.unique). *num_edges_out receives E. */
+ * key lo*V+hi order like torch.unique). *num_edges_out receives E.
+ * A face index outside [0, num_vertices) returns A3D_ERR_ARGUMENT (no kernel
+ * reads or writes through it). */
 size_t a3d_mesh_normals_workspace_bytes(int64_t num_vertices, int64_t num_faces);
 int a3d_mesh_normals(const float* vertices, int64_t num_vertices,
                      const int32_t* faces, int64_t num_faces,
@@ -340,7 +342,10 @@ typedef struct a3d_dmc_inputs {
 size_t a3d_dmc_workspace_bytes(int64_t num_cubes, int64_t num_corners);
 /* Topology pass.  counts (host, 6): surface cubes, groups G (crossing
  * cube-edges == L_dev/p_alpha/n_alpha rows), surface edges, quads Q, dual
- * vertices V; the workspace keeps the topology for _emit and _backward. */
+ * vertices V; the workspace keeps the topology for _emit and _backward.
+ * A cube_idx entry outside [0, num_corners) returns A3D_ERR_ARGUMENT (no
+ * kernel reads or writes through it; the other DMC entry points read such
+ * an entry as corner 0 and report nothing, so call this one first). */
 int a3d_dmc_prepare(const a3d_dmc_inputs* in, void* workspace, size_t workspace_bytes,
                     int64_t* counts, a3d_stream_t stream);
 /* Geometry pass: vertices [V+Q,3], faces [4Q,3] int64, L_dev [G],

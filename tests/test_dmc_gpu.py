@@ -167,3 +167,25 @@ def test_dmc_qef_mode_is_forward_only():
     o = SparseDiffDMC(device="cuda").eval()(vox.cuda(), s, cidx.cuda(), 32)
     with pytest.raises(NotImplementedError):
         (o.vertices ** 2).sum().backward()
+
+
+@pytest.mark.parametrize("mode", ["train", "eval"])
+def test_dmc_cube_idx_out_of_range_raises(golden, mode):
+    """A cube_idx entry outside [0, M) is an argument error: every kernel reads
+    such an entry as corner 0 and the topology pass reports it at its first
+    host read, before any output is written."""
+    g = golden("dmc_small.npz")
+    dmc = SparseDiffDMC(device="cuda")
+    if mode == "eval":
+        dmc = dmc.eval()
+    vox, sdf = torch.from_numpy(g["vox"]).cuda(), torch.from_numpy(g["sdf"]).cuda()
+    deform = torch.from_numpy(g["deform"]).cuda()
+    for bad in (sdf.shape[0], -1):
+        cidx = torch.from_numpy(g["cidx"]).cuda().clone()
+        cidx[cidx.shape[0] // 2, 5] = bad
+        with pytest.raises(RuntimeError, match="outside"):
+            dmc(vox, sdf, cidx, int(g["res"]), deform=deform)
+    # the next valid call is unaffected
+    o = dmc(vox, sdf, torch.from_numpy(g["cidx"]).cuda(), int(g["res"]), deform=deform)
+    key = "train_faces" if mode == "train" else "eval_faces"
+    assert np.array_equal(o.faces.cpu().numpy(), g[key])

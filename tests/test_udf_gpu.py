@@ -229,3 +229,16 @@ def test_cpu_device_raises():
     v, f = synthetic.icosphere(1)
     with pytest.raises(RuntimeError):
         MeshBVH(v, f, device="cpu")
+
+
+@pytest.mark.parametrize("bad", [-1, "nv"])
+def test_face_index_out_of_range_raises(bad):
+    """A face index outside [0, V) is an argument error (the normals pass and
+    the build clamp it before any access), and the device stays usable."""
+    v, f = synthetic.icosphere(2)
+    fb = f.clone()
+    fb[7, 1] = v.shape[0] if bad == "nv" else bad
+    with pytest.raises(RuntimeError, match="face index"):
+        MeshBVH(v.cuda(), fb.cuda())
+    d = MeshBVH(v.cuda(), f.cuda()).udf(torch.zeros(4, 3, device="cuda"))
+    assert bool(torch.isfinite(d).all()) and bool((d == d[0]).all()) and 0.5 < float(d[0]) <= 1.0
