@@ -22,8 +22,10 @@
 //     the brick is stable, then marks its neighbours dirty if it changed.
 //     Bits only ever get set, so reading a neighbour's word while it is
 //     being updated is safe; rounds repeat until no brick is dirty;
-//   * labels, k-ring dilation and counts are word-parallel passes; the
-//     coordinates are written after an exclusive scan of per-word counts.
+//   * labels and the k-ring dilation are word-parallel passes; one pass
+//     counts every label per tile of kTileWords words (and in total), and a
+//     label's coordinates are written by one block per tile after a scan of
+//     that label's tile counts (words are ranked inside the tile).
 #include <limits.h>
 
 #include "primitives.cuh"
@@ -303,37 +305,99 @@ __global__ void ring_classify_kernel(const uint32_t* __restrict__ ring, uint32_t
   lab[kDryAdj * nwords + i] = n & dry & ~dam;
 }
 
-__global__ void popc_kernel(const uint32_t* __restrict__ v, int64_t n, uint32_t* __restrict__ c) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) c[i] = (uint32_t)__popc(v[i]);
+// A tile is kTileWords consecutive words: 256 threads, each warp owning
+// kTileWords / 8 consecutive words in chunks of 32 (one word per lane).
+constexpr int kTileThreads = 256;
+constexpr int kTileWords = 2048;
+constexpr int kTileChunks = kTileWords / kTileThreads;  // chunks of 32 words per warp
+
+// set voxels of every label per tile (label-major [kRing][ntiles]) and per
+// label in total
+__global__ void __launch_bounds__(kTileThreads) tile_counts_kernel(const uint32_t* __restrict__ lab, int64_t nwords,
+                                                                   int64_t ntiles, uint32_t* __restrict__ tcnt,
+                                                                   unsigned long long* __restrict__ tot) {
+  __shared__ uint32_t s_part[kRing][kTileThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t base = (int64_t)blockIdx.x * kTileWords;
+#pragma unroll 1
+  for (int k = 0; k < kRing; ++k) {
+    const uint32_t* v = lab + (int64_t)k * nwords;
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < kTileChunks; ++j) {
+      const int64_t i = base + (int64_t)j * kTileThreads + threadIdx.x;
+      if (i < nwords) c += (uint32_t)__popc(v[i]);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) c += __shfl_xor_sync(0xffffffffu, c, d);
+    if (lane == 0) s_part[k][warp] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x < kRing) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int w = 0; w < kTileThreads / 32; ++w) c += s_part[threadIdx.x][w];
+    tcnt[threadIdx.x * ntiles + blockIdx.x] = c;
+    if (c) atomicAdd(&tot[threadIdx.x], (unsigned long long)c);
+  }
 }
 
-// One warp per 32 consecutive words; for each word the 32 lanes take its 32
-// bits, so the set voxels' coordinates are written as one contiguous run
-// (coalesced) in the word's bit order -- lexicographic (x, y, z) overall.
-__global__ void extract_kernel(Geom g, const uint32_t* __restrict__ v, const int64_t* __restrict__ offs,
-                               int64_t nwords, int32_t* __restrict__ out) {
+// One block per tile.  Each lane takes one word per chunk and ranks it in
+// the tile (warp scans of popcounts, then the warps' totals); then, for each
+// non-empty word of a chunk, the 32 lanes take its 32 bits, so the set
+// voxels' coordinates are written as one contiguous run in the word's bit
+// order -- lexicographic (x, y, z) overall.  Positions at or past `count`
+// are not written.  Needs nwords < 2^32 (word coordinates in 32 bits).
+__global__ void __launch_bounds__(kTileThreads) extract_tile_kernel(Geom g, const uint32_t* __restrict__ v,
+                                                                    const int64_t* __restrict__ toff, int64_t nwords,
+                                                                    int64_t count, int32_t* __restrict__ out) {
+  __shared__ uint32_t s_warp[kTileThreads / 32];
   const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
-  if (w0 >= nwords) return;
-  const int nw = nwords - w0 < 32 ? (int)(nwords - w0) : 32;
-  const uint32_t mine = lane < nw ? v[w0 + lane] : 0u;
-  const int64_t my_off = lane < nw ? offs[w0 + lane] : 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  for (int j = 0; j < nw; ++j) {
-    const uint32_t m = __shfl_sync(FULL, mine, j);
-    if (m == 0u) continue;
-    const int64_t o = __shfl_sync(FULL, my_off, j);
-    const int64_t i = w0 + j;
-    const int w = (int)(i % g.nw);
-    const int64_t row = i / g.nw;
-    const int y = (int)(row % g.ny), x = (int)(row / g.ny);
-    if ((m >> lane) & 1u) {
-      int32_t* p = out + 3 * (o + __popc(m & lt));
-      p[0] = x + g.vx;
-      p[1] = y + g.vy;
-      p[2] = w * 32 + lane + g.vz;
+  const int64_t base = (int64_t)blockIdx.x * kTileWords + (int64_t)warp * (kTileChunks * 32);
+  uint32_t word[kTileChunks], incl[kTileChunks];
+  uint32_t run = 0;
+#pragma unroll
+  for (int c = 0; c < kTileChunks; ++c) {
+    const int64_t i = base + c * 32 + lane;
+    word[c] = i < nwords ? v[i] : 0u;
+    uint32_t p = (uint32_t)__popc(word[c]);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, p, d);
+      if (lane >= d) p += t;
+    }
+    incl[c] = run + p;
+    run += __shfl_sync(FULL, p, 31);
+  }
+  if (lane == 0) s_warp[warp] = run;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int w = 0; w < warp; ++w) before += s_warp[w];
+  const int64_t start = toff[blockIdx.x] + before;
+#pragma unroll
+  for (int c = 0; c < kTileChunks; ++c) {
+    unsigned nz = __ballot_sync(FULL, word[c] != 0u);
+    if (!nz) continue;
+    const uint32_t i = (uint32_t)(base + c * 32 + lane);
+    const uint32_t row = i / (uint32_t)g.nw;
+    const int wz = (int)(i - row * (uint32_t)g.nw);
+    const int y = (int)(row % (uint32_t)g.ny), x = (int)(row / (uint32_t)g.ny);
+    const uint32_t excl = incl[c] - (uint32_t)__popc(word[c]);
+    while (nz) {
+      const int j = __ffs(nz) - 1;
+      nz &= nz - 1u;
+      const uint32_t m = __shfl_sync(FULL, word[c], j);
+      const uint32_t e = __shfl_sync(FULL, excl, j);
+      const int xx = __shfl_sync(FULL, x, j), yy = __shfl_sync(FULL, y, j), ww = __shfl_sync(FULL, wz, j);
+      const int64_t pos = start + e + __popc(m & lt);
+      if (((m >> lane) & 1u) && pos < count) {
+        int32_t* p = out + 3 * pos;
+        p[0] = xx + g.vx;
+        p[1] = yy + g.vy;
+        p[2] = ww * 32 + lane + g.vz;
+      }
     }
   }
 }
@@ -387,11 +451,13 @@ struct FloodWs {
   uint32_t* ring2;   // second ring buffer
   uint8_t* dirty;
   uint8_t* dirty2;
-  uint32_t* cnt;     // per-word counts
-  int64_t* offs;
+  uint32_t* tcnt;    // [kRing][ntiles] voxels per label and tile
+  int64_t* toff;     // [ntiles + 1] one label's tile offsets
   int64_t* scan_tmp;
-  uint32_t* misc;    // [0] seed status [1] any dirty
+  uint32_t* misc;    // [0] seed status [1] any dirty [8..21] label totals (u64)
 };
+
+int64_t tiles_of(const Geom& g) { return ceil_div((int64_t)g.nx * g.ny * g.nw, kTileWords); }
 
 size_t carve_flood(FloodWs& w, Workspace& ws, const Geom& g) {
   const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
@@ -402,10 +468,11 @@ size_t carve_flood(FloodWs& w, Workspace& ws, const Geom& g) {
   w.ring2 = ws.take<uint32_t>(nwords);
   w.dirty = ws.take<uint8_t>(nbricks);
   w.dirty2 = ws.take<uint8_t>(nbricks);
-  w.cnt = ws.take<uint32_t>(nwords);
-  w.offs = ws.take<int64_t>(nwords + 1);
-  w.scan_tmp = ws.take<int64_t>((int64_t)scan_workspace_elems(nwords));
-  w.misc = ws.take<uint32_t>(8);
+  const int64_t ntiles = tiles_of(g);
+  w.tcnt = ws.take<uint32_t>(kRing * ntiles);
+  w.toff = ws.take<int64_t>(ntiles + 1);
+  w.scan_tmp = ws.take<int64_t>((int64_t)scan_workspace_elems(ntiles));
+  w.misc = ws.take<uint32_t>(32);
   return ws.used;
 }
 }  // namespace
@@ -445,6 +512,8 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
   A3D_REQUIRE(geom->k_ring >= 0, A3D_ERR_ARGUMENT, "flood_fill: k_ring must be >= 0");
   Geom g = to_geom(geom);
   A3D_REQUIRE(g.nx > 0 && g.ny > 0 && g.nz > 0, A3D_ERR_ARGUMENT, "flood_fill: empty volume");
+  A3D_REQUIRE((int64_t)g.nx * g.ny * g.nw < (1ll << 32), A3D_ERR_ARGUMENT,
+              "flood_fill: volume above 2^37 voxels (2^32 words)");
   Workspace ws(workspace, workspace_bytes);
   FloodWs w;
   carve_flood(w, ws, g);
@@ -455,7 +524,7 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
   for (int k = 0; k < kLabels; ++k) counts_out[k] = 0;
   A3D_CUDA_TRY(cudaMemsetAsync(w.occ, 0, nwords * 4, s));
   A3D_CUDA_TRY(cudaMemsetAsync(w.water, 0, nwords * 4, s));
-  A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, 32, s));
+  A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, 32 * sizeof(uint32_t), s));
   if (n > 0) {
     set_bits_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(dam_ijk, n, g, w.occ);
     A3D_LAUNCH_CHECK();
@@ -515,16 +584,15 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
   }
   ring_classify_kernel<<<gw, 256, 0, s>>>(ring_a, w.lab, nwords);
   A3D_LAUNCH_CHECK();
-  // counts per label
-  for (int k = 0; k < kRing; ++k) {
-    popc_kernel<<<gw, 256, 0, s>>>(w.lab + (int64_t)k * nwords, nwords, w.cnt);
-    A3D_LAUNCH_CHECK();
-    A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.cnt, w.offs, nwords, w.scan_tmp, w.offs + nwords, s)));
-    int64_t c = 0;
-    A3D_CUDA_TRY(cudaMemcpyAsync(&c, w.offs + nwords, 8, cudaMemcpyDeviceToHost, s));
-    A3D_CUDA_TRY(cudaStreamSynchronize(s));
-    counts_out[k] = c;
-  }
+  // counts per label and tile, one pass and one host read
+  const int64_t ntiles = tiles_of(g);
+  unsigned long long* tot = reinterpret_cast<unsigned long long*>(w.misc + 8);
+  tile_counts_kernel<<<(unsigned)ntiles, kTileThreads, 0, s>>>(w.lab, nwords, ntiles, w.tcnt, tot);
+  A3D_LAUNCH_CHECK();
+  unsigned long long h[kRing];
+  A3D_CUDA_TRY(cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int k = 0; k < kRing; ++k) counts_out[k] = (int64_t)h[k];
   return A3D_OK;
 }
 
@@ -540,12 +608,11 @@ extern "C" int a3d_flood_extract(const a3d_flood_geom* geom, void* workspace, si
   if (count == 0) return A3D_OK;
   A3D_REQUIRE(out_ijk, A3D_ERR_ARGUMENT, "flood_extract: null output");
   const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
-  const unsigned gw = (unsigned)ceil_div(nwords, 256);
+  const int64_t ntiles = tiles_of(g);
   const uint32_t* v = w.lab + (int64_t)label * nwords;
-  popc_kernel<<<gw, 256, 0, s>>>(v, nwords, w.cnt);
-  A3D_LAUNCH_CHECK();
-  A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.cnt, w.offs, nwords, w.scan_tmp, w.offs + nwords, s)));
-  extract_kernel<<<gw, 256, 0, s>>>(g, v, w.offs, nwords, out_ijk);
+  A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.tcnt + (int64_t)label * ntiles, w.toff, ntiles, w.scan_tmp,
+                                                     w.toff + ntiles, s)));
+  extract_tile_kernel<<<(unsigned)ntiles, kTileThreads, 0, s>>>(g, v, w.toff, nwords, count, out_ijk);
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
