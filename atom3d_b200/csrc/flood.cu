@@ -147,79 +147,95 @@ __global__ void set_bits_kernel(const int64_t* __restrict__ ijk, int64_t n, Geom
   atomicOr(&vol[widx(g, x, y, z >> 5)], 1u << (z & 31));
 }
 
-// one relaxation round over the dirty bricks
+// One relaxation round over the bricks queued for it: list `cur` with
+// cnt[round % 3] entries, which the blocks stride over.  A brick whose water
+// changed queues its 27 neighbours (itself included) for the next round,
+// each once: mark[b] is the last round b was queued for, raised with
+// atomicMax, and the first raiser appends b to `nxt` (count cnt[(round + 1)
+// % 3]).  Block 0 clears cnt[(round + 2) % 3], the input count of the
+// previous round, for the round after this one.
 __global__ void __launch_bounds__(kBX * kBY) flood_brick_kernel(Geom g, const uint32_t* __restrict__ occ,
-                                                              uint32_t* water, const uint8_t* __restrict__ dirty,
-                                                              uint8_t* __restrict__ next_dirty, int nbx, int nby,
-                                                              int max_iters, uint32_t* __restrict__ any_dirty) {
-  const int bid = blockIdx.x;
-  if (!dirty[bid]) return;
-  const int bw = bid / (nbx * nby);
-  const int rem = bid % (nbx * nby);
-  const int bxi = rem / nby, byi = rem % nby;
-  const int x0 = bxi * kBX, y0 = byi * kBY;
+                                                              uint32_t* water, const uint32_t* __restrict__ cur,
+                                                              uint32_t* __restrict__ nxt, uint32_t* __restrict__ mark,
+                                                              uint32_t* __restrict__ cnt, int round, int nbx, int nby,
+                                                              int max_iters) {
+  const uint32_t nbricks = (uint32_t)nbx * (uint32_t)nby * (uint32_t)g.nw;
+  const uint32_t n_cur = min(cnt[round % 3], nbricks);
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt[(round + 2) % 3] = 0u;
+  const uint32_t next_round = (uint32_t)round + 1u;
   __shared__ uint32_t s_r[3][kBX + 2][kBY + 2];  // words w-1, w, w+1 of the rows with halo
-  const int tx = threadIdx.x / kBY, ty = threadIdx.x % kBY;
-  // load the halo'd water words (monotone: a racing update is harmless)
-  for (int i = threadIdx.x; i < 3 * (kBX + 2) * (kBY + 2); i += blockDim.x) {
-    const int k = i / ((kBX + 2) * (kBY + 2));
-    const int r2 = i % ((kBX + 2) * (kBY + 2));
-    const int hx = r2 / (kBY + 2), hy = r2 % (kBY + 2);
-    const int x = x0 + hx - 1, y = y0 + hy - 1, w = bw + k - 1;
-    uint32_t v = 0;
-    if (x >= 0 && x < g.nx && y >= 0 && y < g.ny && w >= 0 && w < g.nw) v = __ldcg(&water[widx(g, x, y, w)]);
-    s_r[k][hx][hy] = v;
-  }
-  const int x = x0 + tx, y = y0 + ty;
-  const bool inside = x < g.nx && y < g.ny;
-  uint32_t f = 0;
-  if (inside) f = ~occ[widx(g, x, y, bw)] & crop_mask(g, x, y, bw);
-  __syncthreads();
-  const uint32_t orig = s_r[1][tx + 1][ty + 1];
-  bool changed_any = false;
-  for (int it = 0; it < max_iters; ++it) {
-    uint32_t acc = 0;
-    const uint32_t self = s_r[1][tx + 1][ty + 1];
-    // neighbours along z of this row (words of the adjacent bricks)
-    acc |= (s_r[0][tx + 1][ty + 1] >> 31) | (s_r[2][tx + 1][ty + 1] << 31);
-#pragma unroll
-    for (int dx = -1; dx <= 1; ++dx) {
-#pragma unroll
-      for (int dy = -1; dy <= 1; ++dy) {
-        if (dx == 0 && dy == 0) continue;
-        const int l1 = (dx != 0) + (dy != 0);
-        const uint32_t a = s_r[0][tx + 1 + dx][ty + 1 + dy];
-        const uint32_t c = s_r[1][tx + 1 + dx][ty + 1 + dy];
-        const uint32_t b = s_r[2][tx + 1 + dx][ty + 1 + dy];
-        if (g.conn == 6) {
-          if (l1 == 1) acc |= c;
-        } else if (g.conn == 18) {
-          acc |= (l1 == 1) ? zdil(a, c, b) : c;
-        } else {
-          acc |= zdil(a, c, b);
+  for (uint32_t item = blockIdx.x; item < n_cur; item += gridDim.x) {
+    const int bid = (int)cur[item];
+    const int bw = bid / (nbx * nby);
+    const int rem = bid % (nbx * nby);
+    const int bxi = rem / nby, byi = rem % nby;
+    const int x0 = bxi * kBX, y0 = byi * kBY;
+    const int tx = threadIdx.x / kBY, ty = threadIdx.x % kBY;
+    // load the halo'd water words (monotone: a racing update is harmless)
+    for (int i = threadIdx.x; i < 3 * (kBX + 2) * (kBY + 2); i += blockDim.x) {
+      const int k = i / ((kBX + 2) * (kBY + 2));
+      const int r2 = i % ((kBX + 2) * (kBY + 2));
+      const int hx = r2 / (kBY + 2), hy = r2 % (kBY + 2);
+      const int x = x0 + hx - 1, y = y0 + hy - 1, w = bw + k - 1;
+      uint32_t v = 0;
+      if (x >= 0 && x < g.nx && y >= 0 && y < g.ny && w >= 0 && w < g.nw) v = __ldcg(&water[widx(g, x, y, w)]);
+      s_r[k][hx][hy] = v;
+    }
+    const int x = x0 + tx, y = y0 + ty;
+    const bool inside = x < g.nx && y < g.ny;
+    uint32_t f = 0;
+    if (inside) f = ~occ[widx(g, x, y, bw)] & crop_mask(g, x, y, bw);
+    __syncthreads();
+    const uint32_t orig = s_r[1][tx + 1][ty + 1];
+    bool changed_any = false;
+    for (int it = 0; it < max_iters; ++it) {
+      uint32_t acc = 0;
+      const uint32_t self = s_r[1][tx + 1][ty + 1];
+      // neighbours along z of this row (words of the adjacent bricks)
+      acc |= (s_r[0][tx + 1][ty + 1] >> 31) | (s_r[2][tx + 1][ty + 1] << 31);
+  #pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+  #pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+          if (dx == 0 && dy == 0) continue;
+          const int l1 = (dx != 0) + (dy != 0);
+          const uint32_t a = s_r[0][tx + 1 + dx][ty + 1 + dy];
+          const uint32_t c = s_r[1][tx + 1 + dx][ty + 1 + dy];
+          const uint32_t b = s_r[2][tx + 1 + dx][ty + 1 + dy];
+          if (g.conn == 6) {
+            if (l1 == 1) acc |= c;
+          } else if (g.conn == 18) {
+            acc |= (l1 == 1) ? zdil(a, c, b) : c;
+          } else {
+            acc |= zdil(a, c, b);
+          }
+        }
+      }
+      const uint32_t nw = inside ? fill_runs(self | (acc & f), f) | self : self;
+      const bool ch = nw != self;
+      if (ch) s_r[1][tx + 1][ty + 1] = nw;
+      changed_any |= ch;
+      if (!__syncthreads_or(ch)) break;
+    }
+    const uint32_t fin = s_r[1][tx + 1][ty + 1];
+    if (inside && fin != orig) water[widx(g, x, y, bw)] = fin;
+    // the barrier also ends this brick's reads of s_r before the next item's
+    // halo load
+    if (__syncthreads_or(inside && fin != orig)) {
+      if (threadIdx.x < 27) {
+        const int dz = threadIdx.x / 9 - 1, dxx = (threadIdx.x / 3) % 3 - 1, dyy = threadIdx.x % 3 - 1;
+        const int nbw = bw + dz, nbxx = bxi + dxx, nbyy = byi + dyy;
+        if (nbw >= 0 && nbw < g.nw && nbxx >= 0 && nbxx < nbx && nbyy >= 0 && nbyy < nby) {
+          const uint32_t nb = (uint32_t)((nbw * nbx + nbxx) * nby + nbyy);
+          if (atomicMax(&mark[nb], next_round) < next_round) {
+            const uint32_t slot = atomicAdd(&cnt[(round + 1) % 3], 1u);
+            if (slot < nbricks) nxt[slot] = nb;
+          }
         }
       }
     }
-    const uint32_t nw = inside ? fill_runs(self | (acc & f), f) | self : self;
-    const bool ch = nw != self;
-    if (ch) s_r[1][tx + 1][ty + 1] = nw;
-    changed_any |= ch;
-    if (!__syncthreads_or(ch)) break;
+    (void)changed_any;
   }
-  const uint32_t fin = s_r[1][tx + 1][ty + 1];
-  if (inside && fin != orig) water[widx(g, x, y, bw)] = fin;
-  if (__syncthreads_or(inside && fin != orig)) {
-    if (threadIdx.x < 27) {
-      const int dz = threadIdx.x / 9 - 1, dxx = (threadIdx.x / 3) % 3 - 1, dyy = threadIdx.x % 3 - 1;
-      const int nbw = bw + dz, nbxx = bxi + dxx, nbyy = byi + dyy;
-      const int nbz = (g.nw + 0);
-      if (nbw >= 0 && nbw < nbz && nbxx >= 0 && nbxx < nbx && nbyy >= 0 && nbyy < nby) {
-        next_dirty[(nbw * nbx + nbxx) * nby + nbyy] = 1;
-        *any_dirty = 1u;
-      }
-    }
-  }
-  (void)changed_any;
 }
 
 // label volumes.  slot order: 0 water(pure) 1 dry 2 tide(collision) 3 dam
@@ -413,14 +429,19 @@ __global__ void test_bits_kernel(Geom g, const uint32_t* __restrict__ v, const i
   out[i] = r;
 }
 
+// plants the seed voxel and queues its brick for round 0 (list[0], cnt[0]);
+// status: 1 when the seed is occupied
 __global__ void seed_kernel(Geom g, const uint32_t* __restrict__ occ, uint32_t* __restrict__ water, int sx, int sy,
-                            int sz, uint32_t* __restrict__ status) {
+                            int sz, uint32_t seed_brick, uint32_t* __restrict__ list, uint32_t* __restrict__ cnt,
+                            uint32_t* __restrict__ status) {
   const int64_t i = widx(g, sx, sy, sz >> 5);
   const uint32_t bit = 1u << (sz & 31);
   if (occ[i] & bit) {
     status[0] = 1u;  // seed occupied
   } else {
     water[i] |= bit;
+    list[0] = seed_brick;
+    cnt[0] = 1u;
     status[0] = 0u;
   }
 }
@@ -449,12 +470,13 @@ struct FloodWs {
   uint32_t* water;
   uint32_t* lab;     // kLabels volumes
   uint32_t* ring2;   // second ring buffer
-  uint8_t* dirty;
-  uint8_t* dirty2;
+  uint32_t* mark;    // [nbricks] last round each brick was queued for
+  uint32_t* list_a;  // [nbricks] bricks queued for even rounds
+  uint32_t* list_b;  // [nbricks] odd rounds
   uint32_t* tcnt;    // [kRing][ntiles] voxels per label and tile
   int64_t* toff;     // [ntiles + 1] one label's tile offsets
   int64_t* scan_tmp;
-  uint32_t* misc;    // [0] seed status [1] any dirty [8..21] label totals (u64)
+  uint32_t* misc;    // [0] seed status [2..4] queue counts (round % 3) [8..21] label totals (u64)
 };
 
 int64_t tiles_of(const Geom& g) { return ceil_div((int64_t)g.nx * g.ny * g.nw, kTileWords); }
@@ -466,8 +488,9 @@ size_t carve_flood(FloodWs& w, Workspace& ws, const Geom& g) {
   w.water = ws.take<uint32_t>(nwords);
   w.lab = ws.take<uint32_t>(kLabels * nwords);
   w.ring2 = ws.take<uint32_t>(nwords);
-  w.dirty = ws.take<uint8_t>(nbricks);
-  w.dirty2 = ws.take<uint8_t>(nbricks);
+  w.mark = ws.take<uint32_t>(nbricks);
+  w.list_a = ws.take<uint32_t>(nbricks);
+  w.list_b = ws.take<uint32_t>(nbricks);
   const int64_t ntiles = tiles_of(g);
   w.tcnt = ws.take<uint32_t>(kRing * ntiles);
   w.toff = ws.take<int64_t>(ntiles + 1);
@@ -533,7 +556,12 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
             sz = (int)(geom->seed[2] - geom->vol_lo[2]);
   A3D_REQUIRE(sx >= g.cx0 && sx <= g.cx1 && sy >= g.cy0 && sy <= g.cy1 && sz >= g.cz0 && sz <= g.cz1,
               A3D_ERR_ARGUMENT, "flood_fill: seed outside the crop");
-  seed_kernel<<<1, 1, 0, s>>>(g, w.occ, w.water, sx, sy, sz, w.misc);
+  // the queue of round 0 is the seed's brick; misc (queue counts included)
+  // was cleared above and mark starts at round 0 for every brick
+  const int64_t sb = ((int64_t)(sz >> 5) * nbx + sx / kBX) * nby + sy / kBY;
+  uint32_t* qcnt = w.misc + 2;
+  A3D_CUDA_TRY(cudaMemsetAsync(w.mark, 0, nbricks * sizeof(uint32_t), s));
+  seed_kernel<<<1, 1, 0, s>>>(g, w.occ, w.water, sx, sy, sz, (uint32_t)sb, w.list_a, qcnt, w.misc);
   A3D_LAUNCH_CHECK();
   uint32_t seed_status = 0;
   A3D_CUDA_TRY(cudaMemcpyAsync(&seed_status, w.misc, 4, cudaMemcpyDeviceToHost, s));
@@ -543,31 +571,32 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
     return A3D_OK;
   }
   counts_out[kLabels] = 0;
-  // relaxation rounds over dirty bricks
-  A3D_CUDA_TRY(cudaMemsetAsync(w.dirty, 0, nbricks, s));
-  const int64_t sb = ((int64_t)(sz >> 5) * nbx + sx / kBX) * nby + sy / kBY;
-  const uint8_t one = 1;
-  A3D_CUDA_TRY(cudaMemcpyAsync(w.dirty + sb, &one, 1, cudaMemcpyHostToDevice, s));
-  uint8_t *cur = w.dirty, *nxt = w.dirty2;
-  // Rounds are queued kRoundsPerCheck at a time and the "changed" flag of the
-  // last one is read once per group: a round with no dirty brick does
-  // nothing, so the rounds past convergence only cost their launch.
+  // Relaxation rounds over queued bricks.  A grid of the resident blocks
+  // strides over each round's queue, so a round costs what its queue holds,
+  // not one block per brick of the volume.  Rounds are launched
+  // kRoundsPerCheck at a time and the next round's queue length is read
+  // once per group: a round with an empty queue only costs its launch.
+  int dev = 0, sms = 0, per_sm = 0;
+  A3D_CUDA_TRY(cudaGetDevice(&dev));
+  A3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, flood_brick_kernel, kBX * kBY, 0));
+  const int64_t resident = (int64_t)(sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
+  const unsigned grid = (unsigned)(nbricks < resident ? nbricks : resident);
   constexpr int kRoundsPerCheck = 4;
   int rounds = 0;
   const int max_rounds = 1 << 20;
   while (rounds < max_rounds) {
     for (int k = 0; k < kRoundsPerCheck; ++k, ++rounds) {
-      A3D_CUDA_TRY(cudaMemsetAsync(nxt, 0, nbricks, s));
-      A3D_CUDA_TRY(cudaMemsetAsync(w.misc + 1, 0, 4, s));
-      flood_brick_kernel<<<(unsigned)nbricks, kBX * kBY, 0, s>>>(g, w.occ, w.water, cur, nxt, nbx, nby,
-                                                                  4 * (kBX + kBY), w.misc + 1);
+      const uint32_t* cur = (rounds & 1) ? w.list_b : w.list_a;
+      uint32_t* nxt = (rounds & 1) ? w.list_a : w.list_b;
+      flood_brick_kernel<<<grid, kBX * kBY, 0, s>>>(g, w.occ, w.water, cur, nxt, w.mark, qcnt, rounds, nbx, nby,
+                                                    4 * (kBX + kBY));
       A3D_LAUNCH_CHECK();
-      uint8_t* t = cur; cur = nxt; nxt = t;
     }
-    uint32_t any = 0;
-    A3D_CUDA_TRY(cudaMemcpyAsync(&any, w.misc + 1, 4, cudaMemcpyDeviceToHost, s));
+    uint32_t queued = 0;
+    A3D_CUDA_TRY(cudaMemcpyAsync(&queued, qcnt + rounds % 3, 4, cudaMemcpyDeviceToHost, s));
     A3D_CUDA_TRY(cudaStreamSynchronize(s));
-    if (!any) break;
+    if (!queued) break;
   }
   if (rounds_out) *rounds_out = rounds;
   const unsigned gw = (unsigned)ceil_div(nwords, 256);
