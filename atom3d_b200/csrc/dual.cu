@@ -138,8 +138,10 @@ __global__ void corners_kernel(VGeom g, const uint32_t* __restrict__ cells, uint
   ccnt[i] = (uint32_t)__popc(__ldg(cells + i));
 }
 
-// One warp per 32 consecutive words; the 32 lanes take the bits of each word
-// in turn, so the set voxels are written as contiguous runs in word order.
+// One warp per 32 consecutive words; the 32 lanes take the bits of each
+// non-empty word in turn, so the set voxels are written as contiguous runs in
+// word order.  Each lane reads the offset and computes the coordinates of
+// its own word; the warp visits only the non-empty words.
 // Cells (kVerts false): int32 grid coordinates.  Vertices: int64 grid
 // coordinates and world positions origin + ijk * cell (a product, then a
 // sum: the reference's two separate tensor operations, no contraction).
@@ -151,19 +153,23 @@ __global__ void extract_kernel(VGeom g, const uint32_t* __restrict__ v, const in
   const int lane = threadIdx.x & 31;
   const int64_t w0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
   if (w0 >= nwords) return;
-  const int nw = nwords - w0 < 32 ? (int)(nwords - w0) : 32;
-  const uint32_t mine = lane < nw ? v[w0 + lane] : 0u;
-  const int64_t my_off = lane < nw ? offs[w0 + lane] : 0;
+  const int64_t i = w0 + lane;
+  const uint32_t mine = i < nwords ? v[i] : 0u;
+  unsigned nz = __ballot_sync(FULL, mine != 0u);
+  if (!nz) return;
+  const int64_t my_off = mine ? offs[i] : 0;
+  const int64_t row = i / g.nw;
+  const int my_z = (int)(i - row * g.nw) * 32 + g.lz;
+  const int my_y = (int)(row % g.ny) + g.ly, my_x = (int)(row / g.ny) + g.lx;
   const unsigned lt = (1u << lane) - 1u;
-  for (int j = 0; j < nw; ++j) {
+  while (nz) {
+    const int j = __ffs(nz) - 1;
+    nz &= nz - 1u;
     const uint32_t m = __shfl_sync(FULL, mine, j);
-    if (m == 0u) continue;
     const int64_t o = __shfl_sync(FULL, my_off, j);
+    const int gx = __shfl_sync(FULL, my_x, j), gy = __shfl_sync(FULL, my_y, j);
+    const int gz = __shfl_sync(FULL, my_z, j) + lane;
     if (!((m >> lane) & 1u)) continue;
-    const int64_t i = w0 + j;
-    const int w = (int)(i % g.nw);
-    const int64_t row = i / g.nw;
-    const int gy = (int)(row % g.ny) + g.ly, gx = (int)(row / g.ny) + g.lx, gz = w * 32 + lane + g.lz;
     const int64_t r = o + __popc(m & lt);
     if (kVerts) {
       out_verts[3 * r] = gx;
