@@ -993,6 +993,8 @@ namespace {
 
 struct GradWs {
   float* x;          // [M,3]
+  uint32_t* slots;   // [6M] grid adjacency: per corner, the neighbour along x, y, z as first endpoint, then as second
+  uint32_t* misc;    // [0] slot conflict flag
   uint32_t* cnt;     // [2M] edges per corner as first endpoint (0..M-1), as second (M..2M-1)
   uint32_t* start;   // [2M+1]
   uint32_t* other;   // [24N] the other endpoint of each cube edge, grouped by corner slot
@@ -1001,6 +1003,8 @@ struct GradWs {
 
 size_t carve_grad(GradWs& w, Workspace& ws, int64_t n, int64_t m) {
   w.x = ws.take<float>(3 * m);
+  w.slots = ws.take<uint32_t>(6 * m);
+  w.misc = ws.take<uint32_t>(8);
   w.cnt = ws.take<uint32_t>(2 * m);
   w.start = ws.take<uint32_t>(2 * m + 1);
   w.other = ws.take<uint32_t>(24 * n);
@@ -1014,9 +1018,28 @@ size_t carve_grad(GradWs& w, Workspace& ws, int64_t n, int64_t m) {
 // its cubes -- adds d d^T to both ends and (s_b - s_a)/|x_b - x_a| d to a and
 // its negative to b, d = (x_b - x_a)/|x_b - x_a|.  Instead of sorting the
 // 12 N edge keys to find the unique ones, each corner gathers its own edges
-// from two adjacency lists (as first and as second endpoint), skips repeats
-// of the same neighbour (an edge is listed once per cube holding it) and
-// sums in ascending neighbour order: deterministic FP64 sums, no atomics.
+// (as first and as second endpoint), skips repeats of the same neighbour (an
+// edge is listed once per cube holding it) and sums in ascending neighbour
+// order: deterministic FP64 sums.  Cube indices from one grid give a corner
+// at most one neighbour per axis and side, kept in 6 slots per corner
+// (edge_slot_kernel); when some slot is claimed by two different corners the
+// neighbours are gathered from two adjacency lists instead (count, scan,
+// fill).  Both gathers give the same neighbours in the same order.
+constexpr uint32_t kNoCorner = 0xffffffffu;
+
+__global__ void edge_slot_kernel(DmcIn in, uint32_t* __restrict__ slots, uint32_t* __restrict__ conflict) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= in.n * 12) return;
+  const int64_t i = t / 12;
+  const int e = (int)(t % 12);
+  const int d = kCE[2 * e] ^ kCE[2 * e + 1];
+  const int axis = d == 1 ? 0 : (d == 2 ? 1 : 2);
+  const int64_t a = corner_at(in, 8 * i + kCE[2 * e]), b = corner_at(in, 8 * i + kCE[2 * e + 1]);
+  const uint32_t oa = atomicCAS(&slots[6 * a + axis], kNoCorner, (uint32_t)b);
+  const uint32_t ob = atomicCAS(&slots[6 * b + 3 + axis], kNoCorner, (uint32_t)a);
+  if ((oa != kNoCorner && oa != (uint32_t)b) || (ob != kNoCorner && ob != (uint32_t)a)) *conflict = 1u;
+}
+
 __global__ void edge_adj_count_kernel(DmcIn in, uint32_t* __restrict__ cnt) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= in.n * 12) return;
@@ -1058,7 +1081,51 @@ __device__ __forceinline__ void edge_terms(const DmcIn& in, const float* __restr
 
 __device__ __forceinline__ void solve_sym3(const double* a, const double* b, double* xo);
 
-// one thread per corner: gather, regularise (1e-4 I), solve
+// regularise (1e-4 I), solve, write (zeros for a singular system)
+__device__ __forceinline__ void finish_corner(double A[6], const double B[3], float* __restrict__ grad, int64_t c) {
+  A[0] += 1e-4;
+  A[3] += 1e-4;
+  A[5] += 1e-4;
+  double g[3];
+  solve_sym3(A, B, g);
+  const bool bad = isnan(g[0]) || isnan(g[1]) || isnan(g[2]);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) grad[3 * c + q] = bad ? 0.f : (float)g[q];
+}
+
+__device__ __forceinline__ void add_edge(const DmcIn& in, const float* __restrict__ x, int64_t c, uint32_t nb,
+                                         int side, double A[6], double B[3]) {
+  double o[6], f[3];
+  if (side == 0) edge_terms(in, x, c, nb, o, f);
+  else edge_terms(in, x, nb, c, o, f);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) A[q] += o[q];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) B[a] += side == 0 ? f[a] : -f[a];
+}
+
+// one thread per corner from its 6 grid slots: per side the (at most 3)
+// neighbours sorted ascending, repeats skipped
+__global__ void corner_gradient_slots_kernel(DmcIn in, const float* __restrict__ x, const uint32_t* __restrict__ slots,
+                                             float* __restrict__ grad) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= in.m) return;
+  double A[6] = {0, 0, 0, 0, 0, 0}, B[3] = {0, 0, 0};
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    uint32_t v0 = slots[6 * c + 3 * side], v1 = slots[6 * c + 3 * side + 1], v2 = slots[6 * c + 3 * side + 2];
+    uint32_t t;
+    if (v0 > v1) { t = v0; v0 = v1; v1 = t; }
+    if (v1 > v2) { t = v1; v1 = v2; v2 = t; }
+    if (v0 > v1) { t = v0; v0 = v1; v1 = t; }
+    if (v0 != kNoCorner) add_edge(in, x, c, v0, side, A, B);
+    if (v1 != kNoCorner && v1 != v0) add_edge(in, x, c, v1, side, A, B);
+    if (v2 != kNoCorner && v2 != v1) add_edge(in, x, c, v2, side, A, B);
+  }
+  finish_corner(A, B, grad, c);
+}
+
+// one thread per corner from the adjacency lists: gather, regularise (1e-4 I), solve
 __global__ void corner_gradient_kernel(DmcIn in, const float* __restrict__ x, const uint32_t* __restrict__ start,
                                        const uint32_t* __restrict__ other, float* __restrict__ grad) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1077,25 +1144,12 @@ __global__ void corner_gradient_kernel(DmcIn in, const float* __restrict__ x, co
         if ((!any || v > last) && v <= nxt) { nxt = v; found = true; }
       }
       if (!found) break;
-      double o[6], f[3];
-      if (side == 0) edge_terms(in, x, c, nxt, o, f);
-      else edge_terms(in, x, nxt, c, o, f);
-#pragma unroll
-      for (int q = 0; q < 6; ++q) A[q] += o[q];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) B[a] += side == 0 ? f[a] : -f[a];
+      add_edge(in, x, c, nxt, side, A, B);
       any = true;
       last = nxt;
     }
   }
-  A[0] += 1e-4;
-  A[3] += 1e-4;
-  A[5] += 1e-4;
-  double g[3];
-  solve_sym3(A, B, g);
-  const bool bad = isnan(g[0]) || isnan(g[1]) || isnan(g[2]);
-#pragma unroll
-  for (int q = 0; q < 3; ++q) grad[3 * c + q] = bad ? 0.f : (float)g[q];
+  finish_corner(A, B, grad, c);
 }
 
 // solves the symmetric 3x3 system (a: xx xy xz yy yz zz) by cofactors
@@ -1322,6 +1376,18 @@ extern "C" int a3d_dmc_corner_gradients(const a3d_dmc_inputs* p, void* workspace
   corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, 2.0f / (float)p->resolution, w.x);
   A3D_LAUNCH_CHECK();
   const int64_t nk = 12 * n;
+  A3D_CUDA_TRY(cudaMemsetAsync(w.slots, 0xff, sizeof(uint32_t) * 6 * m, s));
+  A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, sizeof(uint32_t), s));
+  edge_slot_kernel<<<gsz(nk), 256, 0, s>>>(in, w.slots, w.misc);
+  A3D_LAUNCH_CHECK();
+  uint32_t conflict = 0;
+  A3D_CUDA_TRY(cudaMemcpyAsync(&conflict, w.misc, sizeof(conflict), cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  if (!conflict) {
+    corner_gradient_slots_kernel<<<gsz(m), 256, 0, s>>>(in, w.x, w.slots, gradients);
+    A3D_LAUNCH_CHECK();
+    return A3D_OK;
+  }
   A3D_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, sizeof(uint32_t) * 2 * m, s));
   edge_adj_count_kernel<<<gsz(nk), 256, 0, s>>>(in, w.cnt);
   A3D_LAUNCH_CHECK();

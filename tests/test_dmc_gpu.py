@@ -189,3 +189,41 @@ def test_dmc_cube_idx_out_of_range_raises(golden, mode):
     o = dmc(vox, sdf, torch.from_numpy(g["cidx"]).cuda(), int(g["res"]), deform=deform)
     key = "train_faces" if mode == "train" else "eval_faces"
     assert np.array_equal(o.faces.cpu().numpy(), g[key])
+
+
+def test_dmc_corner_gradients_non_grid_indices():
+    """Cube indices that are not one grid's (a corner with two different +x
+    neighbours: one cube uses a duplicate of a shared corner) take the
+    adjacency-list gather; it matches the oracle like the grid gather."""
+    import ctypes
+
+    from oracle import dmc_oracle as D
+    from atom3d_b200 import _lib
+    from atom3d_b200.mesh_extractor import sparse_diffdmc as M
+
+    vox, sdf, cidx, _ = synthetic.dmc_spheres(res=64, seed=8, n_spheres=6)
+    ci = cidx.numpy().copy()
+    # an x-edge (corner slots (0,1), (2,3), (4,5) or (6,7)) held by two cubes
+    pairs = [(0, 1), (2, 3), (4, 5), (6, 7)]
+    keys = np.concatenate([ci[:, p] for p in pairs])
+    _, first, counts = np.unique(keys, axis=0, return_index=True, return_counts=True)
+    k = int(first[np.argmax(counts >= 2)])
+    assert counts.max() >= 2
+    cube, (p0, p1) = k % ci.shape[0], pairs[k // ci.shape[0]]
+    m = sdf.shape[0]
+    b = int(ci[cube, p1])
+    ci[cube, p1] = m  # this cube's copy of corner b
+    sdf2 = np.concatenate([sdf.numpy(), sdf.numpy()[b:b + 1]])
+    x = D.CUBE_CORNERS
+    pos = np.zeros((m + 1, 3), np.float32)
+    pos[ci.reshape(-1)] = (vox.numpy()[:, None, :] + x[None]).reshape(-1, 3)
+    world = pos * np.float32(2.0 / 64) - np.float32(1.0)
+    G = D.corner_gradients(world, sdf2, ci)
+    c = M._DmcContext(vox.cuda(), torch.from_numpy(sdf2).cuda(), torch.from_numpy(ci).cuda(), 64, None, None, None,
+                      0.0, 0.99)
+    got = torch.empty(m + 1, 3, device="cuda")
+    lib = M._bind()
+    ws = _lib.workspace(lib.a3d_dmc_corner_gradients_workspace_bytes(vox.shape[0], m + 1), "cuda")
+    _lib.check("a3d_dmc_corner_gradients", lib.a3d_dmc_corner_gradients(
+        ctypes.byref(c.inp), ws.data_ptr(), ws.numel(), got.data_ptr(), c.stream))
+    assert np.allclose(got.cpu().numpy(), G, rtol=1e-5, atol=1e-5)
