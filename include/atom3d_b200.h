@@ -243,15 +243,19 @@ typedef struct a3d_flood_geom {
 int a3d_flood_bbox(const int64_t* ijk, int64_t n, int64_t* bbox_out,
                    void* workspace, size_t workspace_bytes, a3d_stream_t stream);
 size_t a3d_flood_workspace_bytes(const a3d_flood_geom* geom);
-/* Floods and labels; counts_out (host, 9): voxel count per label slot 0..7
- * and [8] = 1 when the seed is occupied (then nothing else is computed,
- * like the reference's empty result).  The labelled volumes stay in the
- * workspace for a3d_flood_extract / a3d_flood_test.  rounds_out (nullable):
- * relaxation rounds used. */
+/* Floods and labels; counts_out (host, 9): voxel count per label slot 0..6,
+ * [7] = 0 and [8] = 1 when the seed is occupied (then nothing else is
+ * computed, like the reference's empty result).  The labelled volumes and
+ * their per-tile counts stay in the workspace for a3d_flood_extract /
+ * a3d_flood_test.  rounds_out (nullable): relaxation rounds launched (a
+ * multiple of 4).  The volume must hold fewer than 2^37 voxels (2^32
+ * words). */
 int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood_geom* geom,
                    void* workspace, size_t workspace_bytes, int64_t* counts_out,
                    int* rounds_out, a3d_stream_t stream);
-/* Writes the voxels of one label as int32 [count,3] in lexicographic order. */
+/* Writes the voxels of one label as int32 [count,3] in lexicographic order;
+ * count is the label's count from a3d_flood_fill (no position at or past
+ * count is written). */
 int a3d_flood_extract(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes,
                       int label, int32_t* out_ijk, int64_t count, a3d_stream_t stream);
 /* out[i] = 1 when voxel ijk[i] carries the label. */
