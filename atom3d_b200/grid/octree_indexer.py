@@ -29,6 +29,7 @@ class OctreeIndexer(CubeGrid):
         self._level_resolutions = [2 ** lv for lv in range(max_level + 1)]
         # float32 (hi - lo) / res, the reference's per-level cell size
         self._level_cell_sizes = [(self.bounds[1] - self.bounds[0]) / r for r in self._level_resolutions]
+        self._descent_args = None
 
     def get_resolution(self, level: int) -> int:
         return self._level_resolutions[level]
@@ -94,13 +95,21 @@ class OctreeIndexer(CubeGrid):
         return torch.stack([xx.flatten(), yy.flatten(), zz.flatten()], dim=1)
 
     # -------------------------------------------------------------- traversal
+    def _host_descent_args(self):
+        """Grid origin and per-level cell sizes as C float arrays, read back
+        with one device-to-host copy per indexer (both are fixed when the
+        indexer is built)."""
+        if self._descent_args is None:
+            parts = [self.bounds[0].detach().float().reshape(3)]
+            parts += [c.detach().float().reshape(3) for c in self._level_cell_sizes]
+            v = torch.cat(parts).cpu().tolist()
+            self._descent_args = ((ctypes.c_float * 3)(*v[:3]), (ctypes.c_float * (len(v) - 3))(*v[3:]))
+        return self._descent_args
+
     def octree_traverse(self, bvh, min_level: int = 2) -> torch.Tensor:
         """Active cubes [K, 3] int64 at max_level, coarse-to-fine from min_level."""
         dev = bvh.device
-        lo = self.bounds[0].detach().float().cpu()
-        cells = torch.stack([c.detach().float().cpu() for c in self._level_cell_sizes]).contiguous()
-        lo_c = (ctypes.c_float * 3)(*lo.tolist())
-        cell_c = (ctypes.c_float * cells.numel())(*cells.flatten().tolist())
+        lo_c, cell_c = self._host_descent_args()
         cap = max(1 << (3 * min_level), 6 * (4 ** self.max_level), 1024)
         for _ in range(6):
             out = torch.empty(cap, 3, dtype=torch.int64, device=dev)
