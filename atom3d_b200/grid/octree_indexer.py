@@ -47,15 +47,61 @@ class OctreeIndexer(CubeGrid):
         return (grid_coords.float() + 0.5) * self.get_cell_size(level) + self.bounds[0]
 
     def cube_aabb_level(self, cubes: torch.Tensor, level: Optional[int] = None) -> Tuple[torch.Tensor, torch.Tensor]:
+        """AABBs of cubes given as [B, 3] ijk or [B] linear indices at `level`
+        (default max_level)."""
         level = self.max_level if level is None else level
         if cubes.dim() == 1:
-            r = self.get_resolution(level)
-            cubes = self.unravel_idx(cubes, (r, r, r))
+            cubes = self.cube_to_ijk_level(cubes, level)
+        elif cubes.dim() != 2 or cubes.shape[1] != 3:
+            raise ValueError(f"cubes must be [B, 3] ijk or [B] linear idx, got shape {cubes.shape}")
         cell = self.get_cell_size(level)
         mn = cubes.float() * cell + self.bounds[0]
         return mn, mn + cell
 
-    get_cell_aabb_level = cube_aabb_level
+    def get_cell_aabb_level(self, grid_coords: torch.Tensor, level: int) -> Tuple[torch.Tensor, torch.Tensor]:
+        """Cell AABB with the upper corner computed as (ijk + 1) * cell + lo,
+        which can differ in the last bit from cube_aabb_level's min + cell."""
+        cell = self.get_cell_size(level)
+        return grid_coords.float() * cell + self.bounds[0], (grid_coords.float() + 1) * cell + self.bounds[0]
+
+    def get_root_coords(self) -> torch.Tensor:
+        return torch.zeros(1, 3, dtype=self.index_dtype, device=self.device)
+
+    def cube_to_ijk_level(self, cube_idx: torch.Tensor, level: Optional[int] = None) -> torch.Tensor:
+        r = self.get_resolution(self.max_level if level is None else level)
+        return self.unravel_idx(cube_idx, (r, r, r))
+
+    def ijk_to_cube_level(self, ijk: torch.Tensor, level: Optional[int] = None) -> torch.Tensor:
+        r = self.get_resolution(self.max_level if level is None else level)
+        return self.ravel_ijk(ijk, (r, r, r))
+
+    def cube_corner_coords_level(self, cube_ijk: torch.Tensor, level: int) -> torch.Tensor:
+        """World positions [B, 8, 3] of the cubes' corners in CUBE_CORNERS order."""
+        corners = cube_ijk[:, None, :] + self.CUBE_CORNERS[None]
+        return corners.float() * self.get_cell_size(level) + self.bounds[0]
+
+    def cube_edge_endpoints_level(self, cube_ijk: torch.Tensor, level: int) -> torch.Tensor:
+        """Endpoints [B, 12, 2, 3] of the cubes' edges in CUBE_EDGES order."""
+        w = self.cube_corner_coords_level(cube_ijk, level)
+        return torch.stack([w[:, self.CUBE_EDGES[:, 0]], w[:, self.CUBE_EDGES[:, 1]]], dim=2)
+
+    def filter_active_cubes(self, cube_ijk: torch.Tensor, level: int, mesh_aabb_min: torch.Tensor,
+                            mesh_aabb_max: torch.Tensor) -> torch.Tensor:
+        """Cubes whose AABB overlaps some mesh AABB (closed intervals on every
+        axis), in input order (reference: atom3d/grid/octree_indexer.py:
+        441-468).  The cube x box test runs over chunks of cubes, so its
+        temporary stays near 64M entries whatever the sizes."""
+        cmin, cmax = self.cube_aabb_level(cube_ijk, level)
+        amin = mesh_aabb_min.to(device=cmin.device, dtype=cmin.dtype)
+        amax = mesh_aabb_max.to(device=cmin.device, dtype=cmin.dtype)
+        n = int(cube_ijk.shape[0])
+        keep = torch.zeros(n, dtype=torch.bool, device=cmin.device)
+        step = max(1, (1 << 26) // max(3 * int(amin.shape[0]), 1))
+        for s in range(0, n, step):
+            e = min(n, s + step)
+            ov = (cmin[s:e, None, :] <= amax[None]) & (cmax[s:e, None, :] >= amin[None])
+            keep[s:e] = ov.all(dim=2).any(dim=1)
+        return cube_ijk[keep]
 
     # ---------------------------------------------------------------- Morton
     def _ijk_to_morton(self, ijk: torch.Tensor) -> torch.Tensor:
