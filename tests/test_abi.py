@@ -53,3 +53,35 @@ def test_library_has_no_cuda_runtime_dependency():
     ctypes.CDLL(path)
     data = open("/proc/self/maps").read()
     assert path in data
+
+
+def _call(lib, name, *args):
+    fn = getattr(lib, name)
+    st = fn(*args)
+    return st, lib.a3d_last_error()
+
+
+def test_entry_points_reject_bad_arguments_before_any_device_work(lib):
+    """Argument errors come back as A3D_ERR_ARGUMENT with a message, before
+    any CUDA call (so they hold on a host without a GPU), the C-ABI
+    counterpart of the reference's TORCH_CHECK errors."""
+    i64, sz, ci = ctypes.c_int64, ctypes.c_size_t, ctypes.c_int
+    cases = [
+        ("a3d_udf", (None, None, i64(4), None, None, None, None, None, None, None, ctypes.c_uint32(0), None, sz(0),
+                     None), b"invalid bvh"),
+        ("a3d_udf_noalloc", (None, None, i64(-1), None, None, None, None, None), b"negative"),
+        ("a3d_udf_noalloc", (None, None, i64((1 << 20) + 1), None, None, None, None, None), b"1048576"),
+        ("a3d_mesh_normals", (None, i64(0), None, i64(0), None, None, None, None, i64(0), None, None, None, sz(0),
+                              None), b"empty mesh"),
+        ("a3d_octree_traverse", (None, None, None, ci(0), ci(0), None, i64(0), None, None, sz(0), None),
+         b"invalid bvh"),
+        ("a3d_flood_fill", (None, i64(0), None, None, sz(0), None, None, None), b"null argument"),
+        ("a3d_dmc_prepare", (None, None, sz(0), None, None), b"null argument"),
+        ("a3d_dual_graph_count", (None, None, ci(-1), None, None, sz(0), None, None), b"bad argument"),
+        ("a3d_ray_nearest", (None, None, None, i64(1), ctypes.c_float(1.0), None, None, None, None, None, None, None,
+                             None, sz(0), None), b"invalid bvh"),
+    ]
+    for name, args, msg in cases:
+        st, err = _call(lib, name, *args)
+        assert st == 1, (name, st, err)  # A3D_ERR_ARGUMENT
+        assert msg in err, (name, err)
