@@ -585,6 +585,7 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
   constexpr int kRoundsPerCheck = 4;
   int rounds = 0;
   const int max_rounds = 1 << 20;
+  uint32_t queued = 1;
   while (rounds < max_rounds) {
     for (int k = 0; k < kRoundsPerCheck; ++k, ++rounds) {
       const uint32_t* cur = (rounds & 1) ? w.list_b : w.list_a;
@@ -593,11 +594,12 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
                                                     4 * (kBX + kBY));
       A3D_LAUNCH_CHECK();
     }
-    uint32_t queued = 0;
     A3D_CUDA_TRY(cudaMemcpyAsync(&queued, qcnt + rounds % 3, 4, cudaMemcpyDeviceToHost, s));
     A3D_CUDA_TRY(cudaStreamSynchronize(s));
     if (!queued) break;
   }
+  // bricks still queued after the round cap: the water is incomplete
+  A3D_REQUIRE(queued == 0, A3D_ERR_OVERFLOW, "a3d_flood_fill: relaxation did not converge within 2^20 rounds");
   if (rounds_out) *rounds_out = rounds;
   const unsigned gw = (unsigned)ceil_div(nwords, 256);
   labels_kernel<<<gw, 256, 0, s>>>(g, w.occ, w.water, w.lab, nwords);

@@ -248,7 +248,8 @@ size_t a3d_flood_workspace_bytes(const a3d_flood_geom* geom);
  * computed, like the reference's empty result).  The labelled volumes and
  * their per-tile counts stay in the workspace for a3d_flood_extract /
  * a3d_flood_test.  rounds_out (nullable): relaxation rounds launched (a
- * multiple of 4).  The volume must hold fewer than 2^37 voxels (2^32
+ * multiple of 4).  A3D_ERR_OVERFLOW when bricks are still queued after 2^20
+ * rounds (the water would be incomplete).  The volume must hold fewer than 2^37 voxels (2^32
  * words). */
 int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood_geom* geom,
                    void* workspace, size_t workspace_bytes, int64_t* counts_out,

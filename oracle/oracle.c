@@ -474,7 +474,85 @@ void orc_ref_bvh_aabb_hit(const float* nodes, const float* tris, const float* bm
   par_for(n, 64, rah_body, &c);
 }
 
-typedef struct { const float* V; const int32_t* F; int64_t nf; const float* tb; const int64_t* cur; const float* cell; const float* lo; uint8_t* h; } oct_ctx;
+/* Uniform-grid broadphase over the grown triangle boxes: a triangle is listed
+ * in every cell its box overlaps, a query box visits every cell it overlaps
+ * (one cell of slack per side), so a triangle whose box overlaps the query's
+ * is always met.  The decision per triangle is box_hits' (pre-reject, then
+ * SAT), so the result equals the brute-force scan; only the cost changes. */
+typedef struct { double lo[3], inv[3]; int g; int64_t* start; int32_t* items; } tgrid_t;
+
+static inline int tgrid_cell(const tgrid_t* G, int a, double x) {
+  double t = floor((x - G->lo[a]) * G->inv[a]);
+  if (t < 0) t = 0;
+  if (t > G->g - 1) t = G->g - 1;
+  return (int)t;
+}
+
+static void tgrid_build(tgrid_t* G, const float* tb, int64_t nf, const float* lo, const float* ext) {
+  int g = (int)(2.0 * cbrt((double)(nf > 1 ? nf : 1)));
+  if (g < 4) g = 4;
+  if (g > 256) g = 256;
+  G->g = g;
+  for (int a = 0; a < 3; ++a) {
+    G->lo[a] = lo[a];
+    G->inv[a] = ext[a] > 0 ? g / (double)ext[a] : 0.0;
+  }
+  int64_t nc = (int64_t)g * g * g;
+  G->start = (int64_t*)calloc((size_t)nc + 1, sizeof(int64_t));
+  for (int pass = 0; pass < 2; ++pass) {
+    int64_t* fill = NULL;
+    if (pass == 1) {
+      for (int64_t c = 0; c < nc; ++c) G->start[c + 1] += G->start[c];
+      G->items = (int32_t*)malloc(sizeof(int32_t) * (size_t)(G->start[nc] > 0 ? G->start[nc] : 1));
+      fill = (int64_t*)malloc(sizeof(int64_t) * (size_t)nc);
+      memcpy(fill, G->start, sizeof(int64_t) * (size_t)nc);
+    }
+    for (int64_t f = 0; f < nf; ++f) {
+      const float* b = tb + 6 * f;
+      int i0[3], i1[3];
+      for (int a = 0; a < 3; ++a) {
+        i0[a] = tgrid_cell(G, a, b[a]);
+        i1[a] = tgrid_cell(G, a, b[3 + a]);
+      }
+      for (int x = i0[0]; x <= i1[0]; ++x)
+        for (int y = i0[1]; y <= i1[1]; ++y)
+          for (int z = i0[2]; z <= i1[2]; ++z) {
+            int64_t c = ((int64_t)x * g + y) * g + z;
+            if (pass == 0) G->start[c + 1]++;
+            else G->items[fill[c]++] = (int32_t)f;
+          }
+    }
+    free(fill);
+  }
+}
+
+static int tgrid_box_hits(const tgrid_t* G, const float* V, const int32_t* F, const float* tb, const float* mn,
+                          const float* mx) {
+  int i0[3], i1[3];
+  for (int a = 0; a < 3; ++a) {
+    i0[a] = tgrid_cell(G, a, mn[a]) - 1;
+    i1[a] = tgrid_cell(G, a, mx[a]) + 1;
+    if (i0[a] < 0) i0[a] = 0;
+    if (i1[a] > G->g - 1) i1[a] = G->g - 1;
+  }
+  int g = G->g;
+  for (int x = i0[0]; x <= i1[0]; ++x)
+    for (int y = i0[1]; y <= i1[1]; ++y)
+      for (int z = i0[2]; z <= i1[2]; ++z) {
+        int64_t c = ((int64_t)x * g + y) * g + z;
+        for (int64_t k = G->start[c]; k < G->start[c + 1]; ++k) {
+          int64_t f = G->items[k];
+          const float* b = tb + 6 * f;
+          if (b[0] > mx[0] || b[3] < mn[0] || b[1] > mx[1] || b[4] < mn[1] || b[2] > mx[2] || b[5] < mn[2]) continue;
+          float t[9];
+          gather_tri(V, F, f, t);
+          if (orc_sat(t, mn, mx)) return 1;
+        }
+      }
+  return 0;
+}
+
+typedef struct { const float* V; const int32_t* F; const tgrid_t* G; const float* tb; const int64_t* cur; const float* cell; const float* lo; uint8_t* h; } oct_ctx;
 static void oct_body(int64_t k, void* c_) {
   oct_ctx* c = (oct_ctx*)c_;
   float mn[3], mx[3];
@@ -482,13 +560,15 @@ static void oct_body(int64_t k, void* c_) {
     mn[a] = (float)c->cur[3 * k + a] * c->cell[a] + c->lo[a];
     mx[a] = mn[a] + c->cell[a];
   }
-  c->h[k] = (uint8_t)box_hits(c->V, c->F, c->nf, c->tb, mn, mx);
+  c->h[k] = (uint8_t)tgrid_box_hits(c->G, c->V, c->F, c->tb, mn, mx);
 }
 
 /* returns K (>= 0), or -(needed) when out_cap is too small */
 int64_t orc_octree_traverse(const float* V, const int32_t* F, int64_t nf, const float* lo, const float* cells,
                             int min_level, int max_level, int64_t* out, int64_t out_cap) {
   float* tb = tri_boxes(V, F, nf);
+  tgrid_t G;
+  tgrid_build(&G, tb, nf, lo, cells); /* cells[0..2] = the level-0 cell = the whole grid */
   int64_t n = (int64_t)1 << (3 * min_level);
   int64_t* cur = (int64_t*)malloc(sizeof(int64_t) * 3 * n);
   int r = 1 << min_level;
@@ -501,18 +581,20 @@ int64_t orc_octree_traverse(const float* V, const int32_t* F, int64_t nf, const 
   for (int level = min_level; level <= max_level; ++level) {
     const float* cell = cells + 3 * level;
     uint8_t* h = (uint8_t*)malloc(ncur > 0 ? ncur : 1);
-    oct_ctx oc = {V, F, nf, tb, cur, cell, lo, h};
+    oct_ctx oc = {V, F, &G, tb, cur, cell, lo, h};
     par_for(ncur, 64, oct_body, &oc);
     int64_t m = 0;
     for (int64_t k = 0; k < ncur; ++k) m += h[k];
     if (level == max_level) {
-      if (m > out_cap) { free(h); free(cur); free(tb); return -m; }
+      if (m > out_cap) { free(h); free(cur); free(tb); free(G.start); free(G.items); return -m; }
       int64_t o = 0;
       for (int64_t k = 0; k < ncur; ++k)
         if (h[k]) { memcpy(out + 3 * o, cur + 3 * k, 3 * sizeof(int64_t)); ++o; }
       free(h);
       free(cur);
       free(tb);
+      free(G.start);
+      free(G.items);
       return m;
     }
     int64_t* nxt = (int64_t*)malloc(sizeof(int64_t) * 3 * 8 * (m > 0 ? m : 1));
@@ -534,6 +616,8 @@ int64_t orc_octree_traverse(const float* V, const int32_t* F, int64_t nf, const 
   }
   free(cur);
   free(tb);
+  free(G.start);
+  free(G.items);
   return 0;
 }
 

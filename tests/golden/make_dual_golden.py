@@ -11,7 +11,7 @@ Cases:
           grid's y and z faces, where the reference's linear key wraps
   nodry   the shell case with dry_adjacent_ijk = None
 
-Usage:  python tests/golden/make_dual_golden.py [--reference /root/reference]
+Usage:  python tests/golden/make_dual_golden.py --reference <Atom3d checkout>
 """
 
 from __future__ import annotations
@@ -45,7 +45,7 @@ def cases():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of the Atom3d checkout (read only)")
     args = ap.parse_args()
     import_reference(args.reference)
     from atom3d.apps.sparse_flood_fill import (construct_surface_dual_graph, get_dam_wet_corners,

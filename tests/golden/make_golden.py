@@ -19,7 +19,7 @@ pure-PyTorch parts are recorded:
   dmc_small.npz     SparseDiffDMC forward (train and eval) and autograd
                     gradients w.r.t. sdf and deform on a small sphere union
 
-Usage:  python tests/golden/make_golden.py [--reference /root/reference]
+Usage:  python tests/golden/make_golden.py --reference <Atom3d checkout>
 """
 
 from __future__ import annotations
@@ -53,7 +53,7 @@ def import_reference(path: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of the Atom3d checkout (read only)")
     args = ap.parse_args()
     atom3d = import_reference(args.reference)
     from atom3d.grid.octree_indexer import OctreeIndexer

@@ -6,7 +6,7 @@ Only the reference's grid modules and the two small modules they import
 (constants, core/device_utils) are loaded, from a scratch copy arranged as
 a minimal package, so no CUDA extension of the reference is built.
 
-Usage:  python tests/golden/make_grid_golden.py [--reference /root/reference]
+Usage:  python tests/golden/make_grid_golden.py --reference <Atom3d checkout>
 """
 
 from __future__ import annotations
@@ -113,7 +113,7 @@ def outputs(CubeGrid, OctreeIndexer, inp):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of the Atom3d checkout (read only)")
     args = ap.parse_args()
     CubeGrid, OctreeIndexer = import_reference_grid(args.reference)
     inp = inputs()

@@ -7,7 +7,7 @@ the same Moller-Trumbore maths as its GPU kernel with a 1e-6 instead of 1e-8
 lower bound on t and inf instead of max_t for a miss.  The fixture pins the
 oracle's restatement of that maths (hit flags, t, face ids, hit points).
 
-Usage:  python tests/golden/make_ray_golden.py [--reference /root/reference]
+Usage:  python tests/golden/make_ray_golden.py --reference <Atom3d checkout>
 """
 
 from __future__ import annotations
@@ -47,7 +47,7 @@ def rays(seed: int = 21, n: int = 1500):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of the Atom3d checkout (read only)")
     args = ap.parse_args()
     import_reference(args.reference)
     from atom3d.core.mesh_bvh import MeshBVH

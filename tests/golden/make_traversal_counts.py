@@ -27,7 +27,11 @@ from oracle import orc  # noqa: E402
 
 
 def main():
-    import_reference(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", required=True, help="path of the Atom3d checkout (read only)")
+    import_reference(ap.parse_args().reference)
     from atom3d.kernels.bvh import get_bvh_kernels
 
     v, f, q = synthetic.udf_large()

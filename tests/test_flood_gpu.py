@@ -88,3 +88,78 @@ def test_flood_partition_properties_large():
     # the sphere's centre is dry, the crop corner is water
     c = torch.tensor([256, 256, 256], device="cuda", dtype=torch.int32)
     assert (out["dry_ijk"] == c).all(1).any()
+
+
+def serpentine_dam(lo=20, hi=179, fine=True):
+    """A closed box shell [lo, hi]^3 whose inside is a serpentine: walls at
+    every other y, spanning x and z, each open at alternating x ends, so the
+    water entering through one opening in the -x face walks every corridor
+    across all bricks (many relaxation rounds).  With ``fine`` the walls of
+    the corridors inside the first 32 x 32 rows also open at alternating ends
+    of that brick, a path of about 16 x 32 steps inside one brick: longer than
+    a brick's per-round iteration cap, so the brick has to queue itself again."""
+    n = hi - lo + 1
+    ax = np.arange(lo, hi + 1)
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    shell = (X == lo) | (X == hi) | (Y == lo) | (Y == hi) | (Z == lo) | (Z == hi)
+    shell &= ~((X == lo) & (Y == lo + 1) & (Z > lo) & (Z < hi))  # the inlet
+    inner = (X > lo) & (X < hi) & (Y > lo) & (Y < hi) & (Z > lo) & (Z < hi)
+    wall = inner & ((Y - lo) % 2 == 0)
+    k = (Y - lo) // 2
+    gap_x = np.where(k % 2 == 1, lo + 1, hi - 1)
+    wall &= X != gap_x
+    if fine:
+        b0 = (lo // 32 + 1) * 32  # a brick fully inside the box
+        inb = (X >= b0) & (X < b0 + 32) & (Y >= b0) & (Y < b0 + 32)
+        # inside that brick the corridor walls open at alternating brick ends
+        fine_gap = np.where(k % 2 == 1, b0, b0 + 31)
+        wall &= ~(inb & (X == fine_gap))
+    assert n > 64
+    maze = np.argwhere(shell | wall).astype(np.int64) + lo
+    # a sealed hollow box beside the maze: its inside stays dry
+    b = np.arange(hi + 6, hi + 17)
+    B = np.stack(np.meshgrid(b, b, b, indexing="ij"), -1).reshape(-1, 3)
+    edge = ((B == b[0]) | (B == b[-1])).any(1)
+    return np.concatenate([maze, B[edge]])
+
+
+@pytest.mark.parametrize("conn", [6, 26])
+def test_flood_serpentine_many_rounds_matches_oracle(orc, conn):
+    from atom3d_b200.apps.sparse_flood_fill import _Flood
+
+    dam = serpentine_dam()
+    got = flood_fill_3d_sparse(torch.from_numpy(dam).cuda(), 256, padding=2, connectivity=conn)
+    ref = orc.flood_fill_3d_sparse(dam, 256, padding=2, connectivity=conn)
+    for g, r, name in zip(got, ref, ["water", "dry", "tide", "dam", "dam_mask", "ext"]):
+        assert eq(g, r), (conn, name)
+    assert ref[0].shape[0] + ref[2].shape[0] > 2_000_000  # the water did walk the maze
+    assert ref[1].shape[0] >= 9 ** 3  # the sealed box
+    fl = _Flood(torch.from_numpy(dam).cuda(), 256, (0, 0, 0), 2, conn, 0)
+    assert fl.rounds > 100, fl.rounds
+
+
+def test_flood_closure_512():
+    """At 512^3: no free crop voxel outside the water touches the water
+    (conn 26), i.e. the relaxation reached its fixed point."""
+    v, f = synthetic.octree_mesh()
+    bounds = torch.tensor([[-1.5] * 3, [1.5] * 3], device="cuda")
+    mesh = MeshBVH(v.cuda(), f.cuda())
+    out = sparse_flood_fill(mesh, 512, connectivity=26, min_level=4, bounds=bounds, verbose=False)
+    oc = OctreeIndexer(max_level=9, bounds=bounds, device="cuda")
+    dam = oc.octree_traverse(mesh, min_level=4)
+    lo = (dam.min(0).values - 10).clamp(min=0)
+    hi = (dam.max(0).values + 10).clamp(max=511)
+    size = (hi - lo + 1).tolist()
+
+    def vol(t):
+        m = torch.zeros(size, dtype=torch.bool, device="cuda")
+        if t.shape[0]:
+            c = t.long() - lo
+            m[c[:, 0], c[:, 1], c[:, 2]] = True
+        return m
+
+    wet = vol(out["water_ijk"]) | vol(out["tide_ijk"])
+    occ = vol(dam)
+    grown = torch.nn.functional.max_pool3d(wet.float()[None, None], 3, 1, 1)[0, 0] > 0.5
+    leak = grown & ~wet & ~occ
+    assert int(leak.sum()) == 0

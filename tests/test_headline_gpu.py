@@ -1,0 +1,242 @@
+"""Parity at the full workload sizes the benchmarks time.
+
+  * 100,000 queries on the 20,480-triangle noisy sphere: every query against
+    the FP64 brute force, and against the reference's own bvh_udf_kernel;
+  * the 327,680-triangle sphere, octree 4 -> 10 (1024^3) with bounds
+    [-1.5, 1.5]^3: candidate voxels bit-exact in values and order against the
+    oracle and against the reference's own SAT kernel on its own tree; all six
+    sparse_flood_fill label sets at 1024^3 bit-exact against the reference's
+    own BFS kernel and host glue;
+  * 16,777,216 queries on the 1,310,720-triangle sphere: a stratified 4,096
+    query sample against the FP64 brute force, every query against the
+    reference's bvh_udf_kernel, and the UDF gradient of 1,048,576 points;
+  * SparseDiffDMC at 512^3 (2.2M active cubes): topology digest, a vertex
+    sample and 1,000 sdf gradients against the reference's own CPU outputs
+    (tests/golden/dmc512.npz), and the same 1,000 gradients against FP64
+    central differences.
+
+Tolerances: integer outputs bit-exact; distances, closest points and DMC
+vertices within 1e-6 of the bounding-box diagonal; face ids exact except at
+ties (the returned face's FP64 distance is within that tolerance of the FP64
+minimum, or, against the reference kernel, of the reference's face).
+"""
+
+import hashlib
+
+import numpy as np
+import pytest
+import torch
+
+from atom3d_b200 import MeshBVH, OctreeIndexer, SparseDiffDMC, sparse_flood_fill, synthetic
+
+pytestmark = pytest.mark.gpu
+
+BOUNDS = [[-1.5] * 3, [1.5] * 3]
+
+
+@pytest.fixture(scope="module")
+def ref():
+    from oracle import ref_gpu
+
+    if not ref_gpu.available():
+        pytest.skip("oracle/_ref is not built (oracle/build_ref.py --reference <checkout>)")
+    return ref_gpu
+
+
+def diag_of(v):
+    v = v.double()
+    return float((v.max(0).values - v.min(0).values).norm())
+
+
+def faces_vs_fp64(orc, v, f, q, dist, fid, cp, tol):
+    d64, f64, _ = orc.udf_exact(v.numpy(), f.numpy(), q.numpy())
+    err = np.abs(dist.astype(np.float64) - d64)
+    assert err.max() <= tol, f"max distance error {err.max():.3e} > {tol:.3e}"
+    dmine = orc.tri_dist(v.numpy(), f.numpy(), q.numpy(), fid)
+    ok = (fid == f64) | (np.abs(dmine - d64) <= tol)
+    assert ok.all(), f"{int((~ok).sum())} face ids are neither exact nor ties"
+    cerr = np.abs(np.linalg.norm(cp.astype(np.float64) - q.numpy().astype(np.float64), axis=1) - d64)
+    assert cerr.max() <= tol
+    return float(err.max()), float((fid == f64).mean())
+
+
+def faces_vs_reference_kernel(orc, v, f, q, dist, fid, rd, rfid, tol):
+    """Every query: our face equals the reference kernel's, or both faces are
+    at the same FP64 distance within tol; distances agree within tol."""
+    dd = np.abs(dist.astype(np.float64) - rd.astype(np.float64))
+    assert dd.max() <= tol, f"distance vs reference kernel {dd.max():.3e} > {tol:.3e}"
+    diff = np.nonzero(fid != rfid)[0]
+    if diff.shape[0]:
+        qd = q.numpy()[diff]
+        a = orc.tri_dist(v.numpy(), f.numpy(), qd, fid[diff])
+        b = orc.tri_dist(v.numpy(), f.numpy(), qd, rfid[diff])
+        bad = np.abs(a - b) > tol
+        assert not bad.any(), f"{int(bad.sum())} of {diff.shape[0]} differing face ids are not ties"
+    return 1.0 - diff.shape[0] / fid.shape[0]
+
+
+def test_udf_100k_vs_fp64_and_reference_kernel(orc, ref):
+    v, f, q = synthetic.udf_small()
+    assert q.shape[0] == 100_000
+    mesh = MeshBVH(v.cuda(), f.cuda())
+    r = mesh.udf(q.cuda(), return_closest=True, return_face_ids=True)
+    dist, fid, cp = r.distances.cpu().numpy(), r.face_ids.cpu().numpy(), r.closest_points.cpu().numpy()
+    tol = 1e-6 * diag_of(v)
+    faces_vs_fp64(orc, v, f, q, dist, fid, cp, tol)
+    rb = ref.RefBVH(v.cuda(), f.cuda())
+    rd, rfid, _, _ = rb.udf(q.cuda())
+    same = faces_vs_reference_kernel(orc, v, f, q, dist, fid, rd.cpu().numpy(), rfid.cpu().numpy(), tol)
+    assert same > 0.1
+
+
+@pytest.fixture(scope="module")
+def octree_case():
+    v, f = synthetic.octree_mesh()
+    assert f.shape[0] == 327_680
+    mesh = MeshBVH(v.cuda(), f.cuda())
+    oc = OctreeIndexer(max_level=10, bounds=torch.tensor(BOUNDS), device="cuda")
+    dam = oc.octree_traverse(mesh, min_level=4)
+    return v, f, mesh, dam
+
+
+def test_octree_4_to_10_bit_exact(orc, ref, octree_case):
+    v, f, _, dam = octree_case
+    got = dam.cpu().numpy()
+    assert got.dtype == np.int64 and got.shape[0] > 1_000_000
+    exp = orc.octree_traverse(v.numpy(), f.numpy(), BOUNDS[0], BOUNDS[1], 4, 10)
+    assert np.array_equal(got, exp), "octree candidates differ from the oracle"
+    rb = ref.RefBVH(v.cuda(), f.cuda())
+    rdam = ref.octree_traverse(rb, torch.tensor(BOUNDS), 4, 10)
+    assert torch.equal(dam, rdam), (
+        f"octree candidates differ from the reference kernels: {dam.shape[0]} vs {rdam.shape[0]}")
+
+
+def test_flood_labels_1024_bit_exact_vs_reference_kernel(ref, octree_case):
+    _, _, mesh, dam = octree_case
+    got = sparse_flood_fill(mesh, 1024, connectivity=26, min_level=4, bounds=torch.tensor(BOUNDS).cuda(),
+                            verbose=False)
+    water, dry, coll, tdam, _, _ = ref.flood_fill_3d_sparse(dam, 1024, padding=10, connectivity=26)
+    nb, signs = ref.dam_neighborhood_signs(tdam, water, dry, 1024, 1)
+    exp = {"dam_ijk": tdam, "water_ijk": water, "dry_ijk": dry, "tide_ijk": coll,
+           "extended_tide_ijk": nb[signs == 1], "dry_adjacent_ijk": nb[signs == -1]}
+    del water, dry, coll, tdam, nb, signs
+    for k, e in exp.items():
+        g = got[k]
+        assert g.dtype == torch.int32 and g.shape == e.shape, (k, tuple(g.shape), tuple(e.shape))
+        assert torch.equal(g, e), k
+    assert got["water_ijk"].shape[0] > 100_000_000 and got["dry_ijk"].shape[0] > 10_000_000
+
+
+@pytest.fixture(scope="module")
+def large_case():
+    v, f, q = synthetic.udf_large()
+    assert f.shape[0] == 1_310_720 and q.shape[0] == 16_777_216
+    mesh = MeshBVH(v.cuda(), f.cuda())
+    qd = q.cuda()
+    r = mesh.udf(qd, return_closest=True, return_face_ids=True)
+    return v, f, q, mesh, r
+
+
+def test_udf_16m_sample_vs_fp64(orc, large_case):
+    v, f, q, _, r = large_case
+    n = q.shape[0]
+    g = np.random.default_rng(16)
+    pick = np.sort(np.concatenate([g.choice(n // 2, 2048, replace=False),
+                                   n // 2 + g.choice(n - n // 2, 2048, replace=False)]))
+    pt = torch.from_numpy(pick).cuda()
+    dist = r.distances[pt].cpu().numpy()
+    fid = r.face_ids[pt].cpu().numpy()
+    cp = r.closest_points[pt].cpu().numpy()
+    err, exact = faces_vs_fp64(orc, v, f, q[pick], dist, fid, cp, 1e-6 * diag_of(v))
+    assert exact > 0.5
+
+
+def test_udf_16m_vs_reference_kernel(orc, ref, large_case):
+    v, f, q, _, r = large_case
+    rb = ref.RefBVH(v.cuda(), f.cuda())
+    rd, rfid, _, _ = rb.udf(q.cuda())
+    same = faces_vs_reference_kernel(orc, v, f, q, r.distances.cpu().numpy(), r.face_ids.cpu().numpy(),
+                                     rd.cpu().numpy(), rfid.cpu().numpy(), 1e-6 * diag_of(v))
+    assert same > 0.5
+
+
+def test_udf_gradient_1m_points(orc, large_case):
+    v, f, q, mesh, _ = large_case
+    g = torch.Generator().manual_seed(17)
+    idx = torch.randperm(q.shape[0], generator=g)[: 1 << 20]
+    p = q[idx].cuda().requires_grad_(True)
+    r = mesh.udf(p, return_grad=True)
+    r.distances.sum().backward()
+    grad = p.grad.double()
+    away = r.distances.detach() > 1e-4
+    # unit length, and along (p - c) for the closest point the call returned
+    n = grad.norm(dim=1)
+    assert (n[away] - 1).abs().max().item() < 1e-5
+    u = (p.detach().double() - r.closest_points.detach().double())
+    u = u / u.norm(dim=1, keepdim=True)
+    assert ((grad * u).sum(1)[away] - 1).abs().max().item() < 1e-5
+    # against the FP64 closest point on a sample
+    s = np.random.default_rng(18).choice(p.shape[0], 4096, replace=False)
+    ps = p.detach()[torch.from_numpy(s).cuda()].cpu()
+    d64, _, c64 = orc.udf_exact(v.numpy(), f.numpy(), ps.numpy())
+    keep = d64 > 1e-3
+    u64 = (ps.double().numpy() - c64) / d64[:, None]
+    gs = grad[torch.from_numpy(s).cuda()].cpu().numpy()
+    assert np.abs(gs - u64)[keep].max() < 1e-3
+
+
+def _local_loss(D, vox, vijk, sdf, cidx, cube_of, corner, s_val, res):
+    """Sum of squared vertex norms over the cubes within 3 cells of ``corner``
+    (FP64 DMC), with that corner's sdf set to ``s_val``.  Vertices outside the
+    reach of the corner appear on both sides of a difference and cancel."""
+    c = vijk[corner]
+    rng = np.arange(-3, 3)
+    cand = (c[None, None, None, :] + np.stack(np.meshgrid(rng, rng, rng, indexing="ij"), -1)).reshape(-1, 3)
+    keys = (cand[:, 0] * res + cand[:, 1]) * res + cand[:, 2]
+    pos = np.searchsorted(cube_of[0], keys)
+    pos = np.clip(pos, 0, cube_of[0].shape[0] - 1)
+    cubes = np.sort(cube_of[1][pos[cube_of[0][pos] == keys]])
+    ci = cidx[cubes]
+    uniq, inv = np.unique(ci.reshape(-1), return_inverse=True)
+    s = sdf[uniq].astype(np.float64)
+    s[np.searchsorted(uniq, corner)] = s_val
+    return D.loss_vertices_sq(vox[cubes], s, inv.reshape(-1, 8), res, dtype=np.float64)
+
+
+def test_dmc_512_vs_reference_and_fp64_differences(golden):
+    from oracle import dmc_oracle as D
+
+    gd = golden("dmc512.npz")
+    vox, sdf, cidx, vijk = synthetic.dmc_spheres(512)
+    assert abs(float(sdf.double().sum()) - float(gd["sdf_sum"])) == 0.0, "regenerated input differs"
+    s = sdf.cuda().requires_grad_(True)
+    out = SparseDiffDMC(device="cuda")(vox.cuda(), s, cidx.cuda(), 512)
+    (out.vertices ** 2).sum().backward()
+    faces = out.faces.cpu().numpy()
+    assert out.vertices.shape[0] == int(gd["n_vertices"]) and faces.shape[0] == int(gd["n_faces"])
+    assert hashlib.sha256(np.ascontiguousarray(faces.astype(np.int64)).tobytes()).hexdigest() == str(
+        gd["faces_sha256"]), "faces differ from the reference's"
+    tol = 1e-6 * 2 * np.sqrt(3)
+    vs = out.vertices.detach()[torch.from_numpy(gd["vert_idx"]).cuda()].cpu().numpy()
+    assert np.abs(vs - gd["vertices"]).max() <= tol
+    ld = out.L_dev.detach()[torch.from_numpy(gd["ldev_idx"]).cuda()].cpu().numpy()
+    assert np.abs(ld - gd["L_dev"]).max() <= tol
+    idx = gd["grad_idx"]
+    g = s.grad[torch.from_numpy(idx).cuda()].cpu().double().numpy()
+    gref = gd["grad_sdf"].astype(np.float64)
+    assert np.abs(g - gref).max() <= 1e-4 * max(1.0, np.abs(gref).max())
+    # FP64 central differences, evaluated on the cubes around each corner
+    voxn, cidxn, sdfn, vijkn = vox.numpy(), cidx.numpy(), sdf.numpy(), vijk.numpy()
+    keys = (voxn[:, 0] * 512 + voxn[:, 1]) * 512 + voxn[:, 2]
+    order = np.argsort(keys)
+    cube_of = (keys[order], order)
+    worst = 0.0
+    for i, gi in zip(idx, g):
+        s0 = float(sdfn[i])
+        assert s0 != 0.0
+        h = min(1e-6, abs(s0) / 4)
+        fp = _local_loss(D, voxn, vijkn, sdfn, cidxn, cube_of, i, s0 + h, 512)
+        fm = _local_loss(D, voxn, vijkn, sdfn, cidxn, cube_of, i, s0 - h, 512)
+        fd = (fp - fm) / (2 * h)
+        worst = max(worst, abs(fd - gi) / max(1.0, abs(fd)))
+    assert worst <= 2e-3, worst
