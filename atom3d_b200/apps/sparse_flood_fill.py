@@ -57,6 +57,11 @@ _SIGS = {
                                          ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     "a3d_flood_test": (ctypes.c_int, [ctypes.POINTER(FloodGeom), ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
                                       ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
+    "a3d_ring_signs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                      ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(FloodGeom), ctypes.c_void_p,
+                                      ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]),
+    "a3d_ring_signs_emit": (ctypes.c_int, [ctypes.POINTER(FloodGeom), ctypes.c_void_p, ctypes.c_size_t,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     "a3d_cells_bbox": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64), ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, ctypes.c_size_t,
                                       ctypes.c_void_p]),
@@ -179,6 +184,72 @@ def flood_fill_3d_sparse(
     water = fl.extract(WATER) if return_water_dry else _empty3(dev)
     dry = fl.extract(DRY) if return_water_dry else _empty3(dev)
     return water, dry, fl.extract(TIDE), fl.extract(DAM), fl.test(DAM, dam_coords), fl.extract(EXT_DAM)
+
+
+def get_dam_neighborhood_signs(
+    dam_ijk: torch.Tensor,
+    water_ijk: torch.Tensor,
+    dry_ijk: torch.Tensor,
+    resolution: int,
+    k_ring: int = 1,
+) -> Tuple[torch.Tensor, torch.Tensor]:
+    """k-ring neighbourhood of the dam cells and its signs (reference:
+    atom3d/apps/sparse_flood_fill.py:34-100).
+
+    Returns (neighbor_ijk int32 [K,3], signs int8 [K]): the dam grown by
+    ``k_ring`` 26-neighbourhood rings inside [0, resolution)^3, unique and in
+    lexicographic order, with sign 0 for dam cells, else +1 (SIGN_WATER) for
+    water cells, else -1 (SIGN_DRY) for dry cells, else +1.  With k_ring = 0
+    the dam list comes back as given (every sign 0), like the reference's
+    empty expansion loop.  Runs on bit volumes over the dam's bounding box
+    (a3d_ring_signs); dam cells must lie in [0, resolution).
+    """
+    dev = dam_ijk.device
+    if len(dam_ijk) == 0:
+        return torch.empty(0, 3, dtype=torch.int32, device=dev), torch.empty(0, dtype=torch.int8, device=dev)
+    k_ring = int(k_ring)
+    if k_ring < 0:
+        raise ValueError(f"k_ring must be >= 0, got {k_ring}")
+    if k_ring == 0:
+        return dam_ijk.int(), torch.zeros(dam_ijk.shape[0], dtype=torch.int8, device=dev)
+    lib = _bind()
+    _lib.require_cuda(dam_ijk, "dam_ijk")
+    R = int(resolution)
+
+    def lst(t, what):
+        if t is None or len(t) == 0:
+            return torch.empty(0, 3, dtype=torch.int64, device=dev)
+        if t.dim() != 2 or t.shape[1] != 3:
+            raise ValueError(f"{what} must be [K,3], got {tuple(t.shape)}")
+        return t.to(device=dev, dtype=torch.int64).contiguous()
+
+    dam, water, dry = lst(dam_ijk, "dam_ijk"), lst(water_ijk, "water_ijk"), lst(dry_ijk, "dry_ijk")
+    stream = _lib.stream_ptr(dev)
+    ws0 = _lib.workspace(64, dev)
+    bb = (ctypes.c_int64 * 6)()
+    _lib.check("a3d_flood_bbox", lib.a3d_flood_bbox(dam.data_ptr(), dam.shape[0], bb, ws0.data_ptr(), ws0.numel(),
+                                                    stream))
+    if min(bb[:3]) < 0 or max(bb[3:]) >= R:
+        raise ValueError(f"dam_ijk: coordinates must lie in [0, {R}), got range {list(bb[:3])}..{list(bb[3:])}")
+    g = FloodGeom()
+    for a in range(3):
+        lo, hi = max(bb[a] - k_ring, 0), min(bb[3 + a] + k_ring, R - 1)
+        g.vol_lo[a] = g.crop_lo[a] = g.seed[a] = lo
+        g.crop_hi[a] = hi
+        g.vol_dims[a] = hi - lo + 1
+    g.connectivity = 26
+    g.k_ring = k_ring
+    ws = _lib.workspace(lib.a3d_flood_workspace_bytes(ctypes.byref(g)), dev)
+    count = ctypes.c_int64(0)
+    _lib.check("a3d_ring_signs", lib.a3d_ring_signs(
+        dam.data_ptr(), dam.shape[0], water.data_ptr(), water.shape[0], dry.data_ptr(), dry.shape[0], ctypes.byref(g),
+        ws.data_ptr(), ws.numel(), ctypes.byref(count), stream))
+    k = int(count.value)
+    ijk = torch.empty(k, 3, dtype=torch.int32, device=dev)
+    signs = torch.empty(k, dtype=torch.int8, device=dev)
+    _lib.check("a3d_ring_signs_emit", lib.a3d_ring_signs_emit(ctypes.byref(g), ws.data_ptr(), ws.numel(),
+                                                              ijk.data_ptr(), signs.data_ptr(), k, stream))
+    return ijk, signs
 
 
 def sparse_flood_fill(

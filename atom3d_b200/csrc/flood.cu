@@ -446,6 +446,25 @@ __global__ void seed_kernel(Geom g, const uint32_t* __restrict__ occ, uint32_t* 
   }
 }
 
+// sign of each listed voxel (get_dam_neighborhood_signs priority: dam 0,
+// then water +1, then dry -1, else +1), read from the membership volumes
+__global__ void ring_sign_kernel(Geom g, const uint32_t* __restrict__ dam, const uint32_t* __restrict__ water,
+                                 const uint32_t* __restrict__ dry, const int32_t* __restrict__ ijk, int64_t n,
+                                 int8_t* __restrict__ sign) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int x = ijk[3 * i] - g.vx, y = ijk[3 * i + 1] - g.vy, z = ijk[3 * i + 2] - g.vz;
+  int8_t r = 1;
+  if (x >= 0 && y >= 0 && z >= 0 && x < g.nx && y < g.ny && z < g.nz) {
+    const int64_t k = widx(g, x, y, z >> 5);
+    const uint32_t bit = 1u << (z & 31);
+    if (dam[k] & bit) r = 0;
+    else if (water[k] & bit) r = 1;
+    else if (dry[k] & bit) r = -1;
+  }
+  sign[i] = r;
+}
+
 }  // namespace
 }  // namespace a3d
 
@@ -660,6 +679,82 @@ extern "C" int a3d_flood_test(const a3d_flood_geom* geom, void* workspace, size_
   if (n == 0) return A3D_OK;
   const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
   test_bits_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(g, w.lab + (int64_t)label * nwords, ijk, n, out);
+  A3D_LAUNCH_CHECK();
+  return A3D_OK;
+}
+
+// ---- dam neighbourhood signs for caller-given lists -------------------------
+// Volumes of the flood workspace reused: lab[kDam], lab[kWater], lab[kDry]
+// hold the three lists' voxels inside the volume, lab[kExtTide] the dam grown
+// by k_ring 3x3x3 dilations (clamped to the volume, which the caller clamps
+// to the grid), lab[kRing] and ring2 are the dilation's ping-pong buffers.
+extern "C" int a3d_ring_signs(const int64_t* dam_ijk, int64_t n_dam, const int64_t* water_ijk, int64_t n_water,
+                              const int64_t* dry_ijk, int64_t n_dry, const a3d_flood_geom* geom, void* workspace,
+                              size_t workspace_bytes, int64_t* count_out, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(geom && count_out && dam_ijk && n_dam > 0, A3D_ERR_ARGUMENT, "ring_signs: null argument or no dam");
+  A3D_REQUIRE(geom->k_ring >= 0, A3D_ERR_ARGUMENT, "ring_signs: k_ring must be >= 0");
+  A3D_REQUIRE((n_water == 0 || water_ijk) && (n_dry == 0 || dry_ijk), A3D_ERR_ARGUMENT, "ring_signs: null list");
+  Geom g = to_geom(geom);
+  A3D_REQUIRE(g.nx > 0 && g.ny > 0 && g.nz > 0, A3D_ERR_ARGUMENT, "ring_signs: empty volume");
+  A3D_REQUIRE((int64_t)g.nx * g.ny * g.nw < (1ll << 32), A3D_ERR_ARGUMENT, "ring_signs: volume above 2^32 words");
+  Workspace ws(workspace, workspace_bytes);
+  FloodWs w;
+  carve_flood(w, ws, g);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "ring_signs: workspace too small");
+  const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
+  A3D_CUDA_TRY(cudaMemsetAsync(w.lab, 0, (size_t)kLabels * nwords * 4, s));
+  A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, 32 * sizeof(uint32_t), s));
+  uint32_t* v_dam = w.lab + (int64_t)kDam * nwords;
+  set_bits_kernel<<<(unsigned)ceil_div(n_dam, 256), 256, 0, s>>>(dam_ijk, n_dam, g, v_dam);
+  A3D_LAUNCH_CHECK();
+  if (n_water > 0) {
+    set_bits_kernel<<<(unsigned)ceil_div(n_water, 256), 256, 0, s>>>(water_ijk, n_water, g,
+                                                                     w.lab + (int64_t)kWater * nwords);
+    A3D_LAUNCH_CHECK();
+  }
+  if (n_dry > 0) {
+    set_bits_kernel<<<(unsigned)ceil_div(n_dry, 256), 256, 0, s>>>(dry_ijk, n_dry, g, w.lab + (int64_t)kDry * nwords);
+    A3D_LAUNCH_CHECK();
+  }
+  const unsigned gw = (unsigned)ceil_div(nwords, 256);
+  uint32_t* ring_out = w.lab + (int64_t)kExtTide * nwords;
+  const uint32_t* src = v_dam;
+  uint32_t* bufs[2] = {w.lab + (int64_t)kRing * nwords, w.ring2};
+  for (int k = 0; k < geom->k_ring; ++k) {
+    uint32_t* dst = (k == geom->k_ring - 1) ? ring_out : bufs[k & 1];
+    box_dilate_kernel<<<gw, 256, 0, s>>>(g, src, dst, nwords);
+    A3D_LAUNCH_CHECK();
+    src = dst;
+  }
+  if (geom->k_ring == 0)
+    A3D_CUDA_TRY(cudaMemcpyAsync(ring_out, v_dam, nwords * 4, cudaMemcpyDeviceToDevice, s));
+  const int64_t ntiles = tiles_of(g);
+  unsigned long long* tot = reinterpret_cast<unsigned long long*>(w.misc + 8);
+  tile_counts_kernel<<<(unsigned)ntiles, kTileThreads, 0, s>>>(w.lab, nwords, ntiles, w.tcnt, tot);
+  A3D_LAUNCH_CHECK();
+  unsigned long long h = 0;
+  A3D_CUDA_TRY(cudaMemcpyAsync(&h, tot + kExtTide, sizeof(h), cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  *count_out = (int64_t)h;
+  return A3D_OK;
+}
+
+extern "C" int a3d_ring_signs_emit(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes,
+                                   int32_t* out_ijk, int8_t* out_signs, int64_t count, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(geom, A3D_ERR_ARGUMENT, "ring_signs_emit: null geometry");
+  if (count == 0) return A3D_OK;
+  A3D_REQUIRE(out_ijk && out_signs, A3D_ERR_ARGUMENT, "ring_signs_emit: null output");
+  A3D_TRY(a3d_flood_extract(geom, workspace, workspace_bytes, kExtTide, out_ijk, count, stream));
+  Geom g = to_geom(geom);
+  Workspace ws(workspace, workspace_bytes);
+  FloodWs w;
+  carve_flood(w, ws, g);
+  const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
+  ring_sign_kernel<<<(unsigned)ceil_div(count, 256), 256, 0, s>>>(
+      g, w.lab + (int64_t)kDam * nwords, w.lab + (int64_t)kWater * nwords, w.lab + (int64_t)kDry * nwords, out_ijk,
+      count, out_signs);
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }

@@ -263,6 +263,22 @@ int a3d_flood_extract(const a3d_flood_geom* geom, void* workspace, size_t worksp
 int a3d_flood_test(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes,
                    int label, const int64_t* ijk, int64_t n, uint8_t* out, a3d_stream_t stream);
 
+/* Replaces get_dam_neighborhood_signs (atom3d/apps/sparse_flood_fill.py:
+ * 34-100) for caller-given lists (sparse_flood_fill's fused pass covers its
+ * own).  geom: vol_lo/vol_dims = the dam's bounding box grown by k_ring and
+ * clamped to [0, resolution), crop = the volume, k_ring >= 1 (seed and
+ * connectivity unused); workspace: a3d_flood_workspace_bytes(geom).
+ * a3d_ring_signs marks the three lists (voxels outside the volume are
+ * ignored), grows the dam by k_ring 3x3x3 dilations and returns the number
+ * of ring voxels (one host read); a3d_ring_signs_emit writes them as int32
+ * [count,3] in lexicographic order (torch.unique(dim=0) order) and their
+ * signs: 0 dam, else +1 water, else -1 dry, else +1. */
+int a3d_ring_signs(const int64_t* dam_ijk, int64_t n_dam, const int64_t* water_ijk, int64_t n_water,
+                   const int64_t* dry_ijk, int64_t n_dry, const a3d_flood_geom* geom, void* workspace,
+                   size_t workspace_bytes, int64_t* count_out, a3d_stream_t stream);
+int a3d_ring_signs_emit(const a3d_flood_geom* geom, void* workspace, size_t workspace_bytes, int32_t* out_ijk,
+                        int8_t* out_signs, int64_t count, a3d_stream_t stream);
+
 /* ---- device-wide primitives (no reference counterpart) ------------------ */
 /* The library's own exclusive scan and stable LSD radix sort, for callers
  * building their own compactions and orders.  out [n+1] int64: out[i] =

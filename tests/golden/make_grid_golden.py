@@ -57,6 +57,9 @@ def inputs():
         "idx4": torch.randint(0, 16 ** 3, (30,), generator=g),
         "ijk5": torch.randint(0, 32, (30, 3), generator=g),
     }
+    ne = 3 * RES * (RES + 1) ** 2
+    inp["eidx"] = torch.cat([torch.randint(0, ne, (60,), generator=g), torch.tensor([0, ne - 1, ne // 3, 2 * ne // 3])])
+    inp["edir"] = torch.where(torch.rand(64, generator=g) < 0.5, -1, 1)
     c = lo + (hi - lo) * torch.rand(25, 3, generator=g)
     half = 0.02 + 0.1 * torch.rand(25, 3, generator=g)
     inp["amin"], inp["amax"] = c - half, c + half
@@ -85,6 +88,15 @@ def outputs(CubeGrid, OctreeIndexer, inp):
         "generate_all_cells": cg.generate_all_cells(),
     }
     out["cube_aabb_min"], out["cube_aabb_max"] = cg.cube_aabb(inp["idx"])
+    # edge / face topology: every edge of the listed cubes, plus edges on the
+    # grid's faces (incident cubes partly outside the grid)
+    out["cube_edge_indices"] = cg.cube_edge_indices(inp["idx"])
+    out["voxel_unique_edges_0"], out["voxel_unique_edges_1"] = cg.voxel_unique_edges(inp["voxels"])
+    out["voxel_unique_edges_idx_0"], out["voxel_unique_edges_idx_1"] = cg.voxel_unique_edges(inp["idx"])
+    out["edge_endpoints"] = cg.edge_endpoints(inp["eidx"])
+    out["cube_face_indices"] = cg.cube_face_indices(inp["idx"])
+    out["edge_incident_cubes"] = cg.edge_incident_cubes(inp["eidx"])
+    out["edge_incident_cubes_dir"] = cg.edge_incident_cubes(inp["eidx"], inp["edir"])
     for k, t in enumerate(cg.voxel_unique_vertices(inp["voxels"])):
         out[f"voxel_unique_vertices_{k}"] = t
     oc = OctreeIndexer(MAX_LEVEL, bounds=b, device="cpu")

@@ -163,3 +163,35 @@ def test_flood_closure_512():
     grown = torch.nn.functional.max_pool3d(wet.float()[None, None], 3, 1, 1)[0, 0] > 0.5
     leak = grown & ~wet & ~occ
     assert int(leak.sum()) == 0
+
+
+@pytest.mark.parametrize("k_ring", [0, 1, 2, 3])
+def test_get_dam_neighborhood_signs_matches_oracle(orc, k_ring):
+    from atom3d_b200.apps import get_dam_neighborhood_signs
+
+    g = np.random.default_rng(k_ring)
+    dam = shell(24, 8.0) + 3
+    # the grid's faces are reached too: a dam blob against coordinate 0 and R-1
+    dam = np.concatenate([dam, [[0, 5, 5], [0, 6, 5], [31, 31, 31], [30, 31, 0]]])
+    dam = dam[g.permutation(dam.shape[0])]
+    box = np.argwhere(np.ones((32, 32, 32), bool))
+    water = box[g.random(box.shape[0]) < 0.4]
+    dry = box[g.random(box.shape[0]) < 0.3]
+    got_ijk, got_s = get_dam_neighborhood_signs(torch.from_numpy(dam).cuda(), torch.from_numpy(water).cuda(),
+                                                torch.from_numpy(dry).cuda().int(), 32, k_ring=k_ring)
+    ref_ijk, ref_s = orc.dam_neighborhood_signs(dam, water, dry, 32, k_ring)
+    assert got_ijk.dtype == torch.int32 and got_s.dtype == torch.int8
+    assert eq(got_ijk, ref_ijk.astype(np.int32)) and eq(got_s, ref_s)
+    assert (got_s == 0).sum().item() == np.unique(dam, axis=0).shape[0] if k_ring else True
+
+
+def test_get_dam_neighborhood_signs_edge_cases():
+    from atom3d_b200.apps import get_dam_neighborhood_signs
+
+    e = torch.zeros(0, 3, dtype=torch.int64, device="cuda")
+    a, b = get_dam_neighborhood_signs(e, e, e, 16)
+    assert a.shape == (0, 3) and b.shape == (0,)
+    with pytest.raises(ValueError):
+        get_dam_neighborhood_signs(torch.tensor([[16, 0, 0]], device="cuda"), e, e, 16)
+    a, b = get_dam_neighborhood_signs(torch.tensor([[0, 0, 0]], device="cuda"), e, e, 16, k_ring=1)
+    assert a.shape == (8, 3) and int((b == 0).sum()) == 1 and int((b == 1).sum()) == 7
