@@ -391,6 +391,39 @@ int orc_sat(const float* t /* 9 */, const float* mn, const float* mx) {
   return 1;
 }
 
+static void gather_tri(const float* V, const int32_t* F, int64_t f, float* t);
+
+/* "Some triangle hits" per box with the stricter rule of the reference's BVH
+ * cull applied per triangle: the triangle's own box must overlap the query
+ * box exactly (aabb_overlap, bvh_kernels.cu:241-245, :583) before SAT.  The
+ * reference applies that cull to node boxes (unions of up to 4 triangle
+ * boxes), so its result lies between this and orc_boxes_hit; the tests use
+ * it to show that a voxel the product keeps and the reference drops is hit
+ * only within sat_eps outside the triangles' own boxes. */
+typedef struct { const float* V; const int32_t* F; int64_t nf; const float* bmin; const float* bmax; uint8_t* hit; } bhx_ctx;
+static void bhx_body(int64_t i, void* c_) {
+  bhx_ctx* c = (bhx_ctx*)c_;
+  const float* mn = c->bmin + 3 * i;
+  const float* mx = c->bmax + 3 * i;
+  uint8_t h = 0;
+  for (int64_t f = 0; f < c->nf && !h; ++f) {
+    float t[9];
+    gather_tri(c->V, c->F, f, t);
+    int ov = 1;
+    for (int a = 0; a < 3; ++a) {
+      const float lo = fminf(fminf(t[a], t[3 + a]), t[6 + a]), hi = fmaxf(fmaxf(t[a], t[3 + a]), t[6 + a]);
+      if (lo > mx[a] || hi < mn[a]) ov = 0;
+    }
+    if (ov && orc_sat(t, mn, mx)) h = 1;
+  }
+  c->hit[i] = h;
+}
+void orc_boxes_hit_exact_box(const float* V, const int32_t* F, int64_t nf, const float* bmin, const float* bmax,
+                             int64_t n, uint8_t* hit) {
+  bhx_ctx c = {V, F, nf, bmin, bmax, hit};
+  par_for(n, 1, bhx_body, &c);
+}
+
 static void gather_tri(const float* V, const int32_t* F, int64_t f, float* t) {
   for (int k = 0; k < 3; ++k)
     for (int a = 0; a < 3; ++a) t[3 * k + a] = V[3 * (int64_t)F[3 * f + k] + a];

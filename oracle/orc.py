@@ -124,6 +124,37 @@ def boxes_hit(V, F, bmin, bmax):
     return h.astype(bool)
 
 
+def boxes_hit_exact_box(V, F, bmin, bmax):
+    """Per box: some triangle whose own box overlaps it exactly passes SAT."""
+    V, F, bmin, bmax = _f32(V), _i32(F), _f32(bmin), _f32(bmax)
+    h = np.empty(bmin.shape[0], np.uint8)
+    lib().orc_boxes_hit_exact_box(_p(V), _p(F), I64(F.shape[0]), _p(bmin), _p(bmax), I64(bmin.shape[0]), _p(h))
+    return h.astype(bool)
+
+
+def ref_octree_traverse(nodes, tris, lo, hi, min_level, max_level):
+    """octree_traverse with bvh_aabb_intersect_kernel restated over a reference
+    build_bvh tree as the per-level test (tree-dependent, like the reference)."""
+    cells = level_cells(lo, hi, max_level)
+    lo32 = _f32(lo)
+    corners = np.array([[i & 1, (i >> 1) & 1, (i >> 2) & 1] for i in range(8)], np.int64)
+
+    def boxes(ijk, lv):
+        mn = (ijk.astype(np.float32) * cells[lv] + lo32).astype(np.float32)
+        return mn, (mn + cells[lv]).astype(np.float32)
+
+    r = 1 << min_level
+    x = np.arange(r, dtype=np.int64)
+    cur = np.stack(np.meshgrid(x, x, x, indexing="ij"), -1).reshape(-1, 3)
+    cur = cur[ref_bvh_aabb_hit(nodes, tris, *boxes(cur, min_level))]
+    for lv in range(min_level + 1, max_level + 1):
+        if cur.shape[0] == 0:
+            break
+        cur = ((cur * 2)[:, None, :] + corners[None]).reshape(-1, 3)
+        cur = cur[ref_bvh_aabb_hit(nodes, tris, *boxes(cur, lv))]
+    return cur
+
+
 def ref_bvh_aabb_hit(nodes, tris, bmin, bmax):
     nodes, tris, bmin, bmax = _f32(nodes), _f32(tris), _f32(bmin), _f32(bmax)
     h = np.empty(bmin.shape[0], np.uint8)

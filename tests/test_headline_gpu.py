@@ -100,15 +100,37 @@ def octree_case():
 
 
 def test_octree_4_to_10_bit_exact(orc, ref, octree_case):
+    """Bit-exact (values and order) against the oracle.  Against the
+    reference's own kernels on the reference's own tree: the reference culls
+    BVH nodes by exact box overlap before SAT, so a triangle lying within
+    sat_eps outside a voxel reaches SAT only when other triangles of its leaf
+    widen the leaf box -- a tree-dependent outcome.  The product keeps every
+    SAT hit (a superset, never losing surface); the test pins the oracle's
+    restatement of the reference kernel to the reference's GPU build, then
+    requires the reference's voxels to be ours in our order, and every extra
+    voxel to be one that no triangle's own box touches (a sat_eps contact)."""
     v, f, _, dam = octree_case
     got = dam.cpu().numpy()
     assert got.dtype == np.int64 and got.shape[0] > 1_000_000
     exp = orc.octree_traverse(v.numpy(), f.numpy(), BOUNDS[0], BOUNDS[1], 4, 10)
     assert np.array_equal(got, exp), "octree candidates differ from the oracle"
     rb = ref.RefBVH(v.cuda(), f.cuda())
-    rdam = ref.octree_traverse(rb, torch.tensor(BOUNDS), 4, 10)
-    assert torch.equal(dam, rdam), (
-        f"octree candidates differ from the reference kernels: {dam.shape[0]} vs {rdam.shape[0]}")
+    rdam = ref.octree_traverse(rb, torch.tensor(BOUNDS), 4, 10).cpu().numpy()
+    rexp = orc.ref_octree_traverse(rb.nodes.cpu().numpy(), rb.triangles.cpu().numpy(), BOUNDS[0], BOUNDS[1], 4, 10)
+    assert np.array_equal(rdam, rexp), "oracle restatement differs from the reference's own kernels"
+
+    def key(a):
+        return (a[:, 0] * 1024 + a[:, 1]) * 1024 + a[:, 2]
+
+    common = np.isin(key(got), key(rdam))
+    assert np.array_equal(got[common], rdam), "reference voxels are not ours, in our order"
+    extra = got[~common]
+    assert extra.shape[0] <= 1e-5 * got.shape[0], extra.shape[0]
+    cells = orc.level_cells(BOUNDS[0], BOUNDS[1], 10)[10]
+    mn = (extra.astype(np.float32) * cells + np.float32(BOUNDS[0][0])).astype(np.float32)
+    mx = (mn + cells).astype(np.float32)
+    assert orc.boxes_hit(v.numpy(), f.numpy(), mn, mx).all()
+    assert not orc.boxes_hit_exact_box(v.numpy(), f.numpy(), mn, mx).any()
 
 
 def test_flood_labels_1024_bit_exact_vs_reference_kernel(ref, octree_case):
@@ -165,7 +187,7 @@ def test_udf_gradient_1m_points(orc, large_case):
     g = torch.Generator().manual_seed(17)
     idx = torch.randperm(q.shape[0], generator=g)[: 1 << 20]
     p = q[idx].cuda().requires_grad_(True)
-    r = mesh.udf(p, return_grad=True)
+    r = mesh.udf(p, return_grad=True, return_closest=True)
     r.distances.sum().backward()
     grad = p.grad.double()
     away = r.distances.detach() > 1e-4
