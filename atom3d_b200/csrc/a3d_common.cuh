@@ -46,7 +46,10 @@ void a3d_set_error(const char* msg, const char* file, int line);
 
 namespace a3d {
 
-constexpr int kNumSMs = 148;
+// streaming multiprocessors of the current device (queried once per device;
+// 148 on B200), for sizing persistent and grid-stride launches
+int num_sms();
+constexpr int kMaxDevices = 64;
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 

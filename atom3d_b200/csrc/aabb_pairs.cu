@@ -395,7 +395,7 @@ int launch_write(const a3d_bvh_view* bvh, const float* bmin, const float* bmax, 
                                                                                         w.offs, out_box, out_face,
                                                                                         w.misc);
   A3D_LAUNCH_CHECK();
-  pairs_write_spill_kernel<kSlots><<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, bmin, bmax, w.offs, w.spill, w.misc,
+  pairs_write_spill_kernel<kSlots><<<num_sms() * 4, 64, 0, s>>>(nodes, tris, bmin, bmax, w.offs, w.spill, w.misc,
                                                               out_box, out_face);
   A3D_LAUNCH_CHECK();
   return A3D_OK;
@@ -448,7 +448,7 @@ extern "C" int a3d_aabb_pairs_count(const a3d_bvh_view* bvh, const float* box_mi
   pairs_count_kernel<<<(unsigned)ceil_div(n, kSatThreads), kSatThreads, 0, s>>>(nodes, tris, box_min, box_max, n,
                                                                                  w.counts, h, w.spill, w.misc);
   A3D_LAUNCH_CHECK();
-  pairs_count_spill_kernel<<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, box_min, box_max, w.counts, h, w.spill, w.misc);
+  pairs_count_spill_kernel<<<num_sms() * 4, 64, 0, s>>>(nodes, tris, box_min, box_max, w.counts, h, w.spill, w.misc);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.counts, w.offs, n, w.scan_tmp, w.offs + n, s)));
   unsigned long long misc[4];

@@ -14,6 +14,9 @@
 //   4. one binary radix tree per mesh over its sorted range [s, e): internal
 //      nodes s..e-2 with root s, leaf j at N + j (duplicate codes
 //      disambiguated by index)
+//   4b. SAH refinement: every subtree of at most 1024 triangles below the
+//      top of the tree is rebuilt top-down with binned SAH by one thread
+//      block (bvh_sah.cuh), in place and within its own index range
 //   5. bottom-up refit (second arriving child computes the union box)
 //   6. surface-area-guided collapse into 4-wide quantised nodes: starting
 //      from a binary node, the child with the largest surface area is opened
@@ -29,6 +32,7 @@
 #include <string.h>
 
 #include "bvh_layout.cuh"
+#include "bvh_sah.cuh"
 #include "primitives.cuh"
 
 namespace a3d {
@@ -37,7 +41,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxLevels = 64;  // wide levels; deeper trees report A3D_ERR_OVERFLOW
-constexpr int kLevelBlocks = kNumSMs * 8;
 constexpr uint32_t kNoLevel = 255u;
 // leaves of up to 8 triangles: fewer, larger leaves trade node tests for
 // cheaper triangle tests (16M-query closest-point workload on a 1.31M-
@@ -76,6 +79,8 @@ struct BuildWs {
   uint32_t* slot_alt;
   uint32_t* newidx;     // [N] slot -> final node index
   int64_t* count;       // single-mesh builds: node count
+  int32_t* clusters;    // [N] roots of the subtrees the SAH pass rebuilds
+  uint32_t* ncl;        // their count
 };
 
 size_t carve(BuildWs& w, Workspace& ws, int64_t n, int64_t m) {
@@ -110,6 +115,8 @@ size_t carve(BuildWs& w, Workspace& ws, int64_t n, int64_t m) {
   w.slot_alt = ws.take<uint32_t>(n);
   w.newidx = ws.take<uint32_t>(n);
   w.count = ws.take<int64_t>(1);
+  w.clusters = ws.take<int32_t>(n);
+  w.ncl = ws.take<uint32_t>(1);
   return ws.used;
 }
 
@@ -532,6 +539,28 @@ __global__ void write_tris_kernel(const float* __restrict__ V, const int64_t* __
   tris[j] = r;
 }
 
+// resident blocks of the SAH kernel on the current device (its shared
+// memory needs the opt-in above 48 KB), set up once per device
+int sah_grid_size(int* grid) {
+  static int cached[kMaxDevices] = {0};
+  int dev = 0;
+  A3D_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < kMaxDevices && cached[dev] > 0) {
+    *grid = cached[dev];
+    return A3D_OK;
+  }
+  A3D_CUDA_TRY(cudaFuncSetAttribute(sah_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(SahSmem)));
+  int sms = 0, per_sm = 0;
+  A3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sah_cluster_kernel, kSahThreads,
+                                                             sizeof(SahSmem)));
+  const int g = (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
+  if (dev >= 0 && dev < kMaxDevices) cached[dev] = g;
+  *grid = g;
+  return A3D_OK;
+}
+
 int mesh_bits_of(int nmesh) {
   int mbits = 0;
   while ((1ll << mbits) < nmesh) ++mbits;
@@ -562,6 +591,17 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
 
   radix_tree_kernel<<<g, kThreads, 0, s>>>(keys, face_off, nmesh, n, w.left, w.right, w.parent, w.first, w.last);
   A3D_LAUNCH_CHECK();
+  // SAH refinement of every subtree of <= kSahMax triangles below the top
+  A3D_CUDA_TRY(cudaMemsetAsync(w.ncl, 0, sizeof(uint32_t), s));
+  sah_find_kernel<<<g, kThreads, 0, s>>>(face_off, nmesh, n, w.parent, w.first, w.last, w.clusters, w.ncl);
+  A3D_LAUNCH_CHECK();
+  int sah_grid = 0;
+  A3D_TRY(sah_grid_size(&sah_grid));
+  const int64_t max_clusters = n / 3 + 1;
+  sah_cluster_kernel<<<(unsigned)(max_clusters < sah_grid ? max_clusters : sah_grid), kSahThreads, sizeof(SahSmem),
+                       s>>>(w.clusters, w.ncl, SahTree{w.left, w.right, w.parent, w.first, w.last, n},
+                            const_cast<uint32_t*>(order), w.tri_lo, w.tri_hi, w.centroid);
+  A3D_LAUNCH_CHECK();
   A3D_CUDA_TRY(cudaMemsetAsync(w.visit, 0, sizeof(uint32_t) * n, s));
   refit_kernel<<<g, kThreads, 0, s>>>(order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.box_lo, w.box_hi,
                                       w.visit);
@@ -571,7 +611,8 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
 
   // collapse: a fixed number of level launches (empty levels return at once)
   A3D_CUDA_TRY(cudaMemsetAsync(w.lvl, 0xff, sizeof(uint32_t) * n, s));
-  const int64_t lb = ceil_div(n, kThreads) < kLevelBlocks ? ceil_div(n, kThreads) : kLevelBlocks;
+  const int64_t level_blocks = (int64_t)num_sms() * 8;
+  const int64_t lb = ceil_div(n, kThreads) < level_blocks ? ceil_div(n, kThreads) : level_blocks;
   int32_t *cur = w.work_a, *nxt = w.work_b;
   for (int level = 0; level < kMaxLevels; ++level) {
     collapse_level_kernel<<<(unsigned)lb, kThreads, 0, s>>>(level, w.counters, cur, nxt, n, leaf_max, w.left,

@@ -383,8 +383,9 @@ extern "C" int a3d_gemm_bf16(const a3d_gemm_args* a, a3d_stream_t stream) {
   // into Cf atomically; only for a plain accumulate into Cf
   const bool plain_acc = a->Cf && a->accumulate && !a->Cb && !a->bias && !a->mask && !a->relu;
   const int64_t tiles = (int64_t)grid.x * grid.y;
-  if (plain_acc && tiles < a3d::kNumSMs && a->k >= 4 * kBK) {
-    const int64_t want = (2 * a3d::kNumSMs + tiles - 1) / tiles;
+  const int sms = a3d::num_sms();
+  if (plain_acc && tiles < sms && a->k >= 4 * kBK) {
+    const int64_t want = (2 * (int64_t)sms + tiles - 1) / tiles;
     grid.z = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, a->k / (2 * kBK)));
   }
   A3D_REQUIRE(grid.y < 65536, A3D_ERR_ARGUMENT, "gemm_bf16: m too large for one launch");
@@ -451,14 +452,15 @@ extern "C" int a3d_mlp_bound(const a3d_mlp_weights* wts, const float* x, int64_t
   p.nz = Normalise{wts->norm[0], wts->norm[1], wts->norm[2], wts->norm[3]};
   p.scale = wts->scale; p.margin = wts->margin;
   const size_t smem = sizeof(InfSmem);
-  static bool attr_set = false;
-  if (!attr_set) {
-    A3D_CUDA_TRY(cudaFuncSetAttribute(mlp_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
-  int dev = 0, sms = kNumSMs;
+  // the shared-memory opt-in is a per-device setting
+  static bool attr_set[kMaxDevices] = {false};
+  int dev = 0;
   A3D_CUDA_TRY(cudaGetDevice(&dev));
-  A3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (dev < 0 || dev >= kMaxDevices || !attr_set[dev]) {
+    A3D_CUDA_TRY(cudaFuncSetAttribute(mlp_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (dev >= 0 && dev < kMaxDevices) attr_set[dev] = true;
+  }
+  const int sms = num_sms();
   const int64_t tiles = ceil_div(n, kRows);
   const int64_t grid = tiles < (int64_t)sms ? tiles : (int64_t)sms;
   mlp_bound_kernel<<<(unsigned)grid, kInfWarps * 32, smem, (cudaStream_t)stream>>>(x, n, p, bound);

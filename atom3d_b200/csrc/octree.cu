@@ -202,7 +202,7 @@ extern "C" int a3d_aabb_hit(const a3d_bvh_view* bvh, const float* box_min, const
   aabb_hit_kernel<<<(unsigned)ceil_div(n, kSatThreads), kSatThreads, 0, s>>>(
       (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, box_min, box_max, n, hit, spill, nspill);
   A3D_LAUNCH_CHECK();
-  aabb_hit_spill_kernel<<<kNumSMs * 4, 64, 0, s>>>((const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, box_min,
+  aabb_hit_spill_kernel<<<num_sms() * 4, 64, 0, s>>>((const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, box_min,
                                                    box_max, hit, spill, nspill, (int*)(nspill + 1));
   A3D_LAUNCH_CHECK();
   int ov = 0;
@@ -282,7 +282,7 @@ extern "C" int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo
     octree_level_kernel<<<gk, kSatThreads, 0, s>>>(nodes, tris, ncand, first_level, res, parents, g, w.flags, w.spill,
                                                    w.misc + 1);
     A3D_LAUNCH_CHECK();
-    octree_spill_kernel<<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, first_level, res, parents, g, w.flags, w.spill,
+    octree_spill_kernel<<<num_sms() * 4, 64, 0, s>>>(nodes, tris, first_level, res, parents, g, w.flags, w.spill,
                                                    w.misc + 1, (int*)(w.misc + 2));
     A3D_LAUNCH_CHECK();
     flags_to_u8_kernel<<<(unsigned)ceil_div(ncand, 256), 256, 0, s>>>(w.flags, ncand, w.hit);

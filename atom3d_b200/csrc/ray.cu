@@ -509,7 +509,7 @@ extern "C" int a3d_ray_nearest(const a3d_bvh_view* bvh, const float* rays_o, con
   ray_nearest_kernel<<<(unsigned)ceil_div(num_rays, kRayThreads), kRayThreads, 0, s>>>(
       nodes, tris, face_normals, rays_o, rays_d, num_rays, max_t, out, w.rerun, w.status);
   A3D_LAUNCH_CHECK();
-  ray_nearest_rerun_kernel<<<kNumSMs * 4, 64, 0, s>>>(nodes, tris, face_normals, rays_o, rays_d, max_t, out, w.rerun,
+  ray_nearest_rerun_kernel<<<num_sms() * 4, 64, 0, s>>>(nodes, tris, face_normals, rays_o, rays_d, max_t, out, w.rerun,
                                                       w.status, w.status + 1);
   A3D_LAUNCH_CHECK();
   return A3D_OK;

@@ -865,7 +865,7 @@ size_t carve_udf(UdfWs& w, Workspace& ws, int64_t n, uint32_t flags) {
 // owners of the persistent traversal that get an overflow stack when the
 // workspace has room for it (bounded: 148 SMs x 10 blocks x 64 lanes)
 int64_t spill_owner_bound(int64_t n) {
-  const int64_t cap = (int64_t)kNumSMs * 10 * 64;
+  const int64_t cap = (int64_t)148 * 10 * 64;  // overflow stacks for the resident owners of a 148-SM part
   return n + 128 < cap ? n + 128 : cap;
 }
 
@@ -878,14 +878,20 @@ struct TaskShape {
 
 template <bool kSign, bool kStats, bool kBatch>
 int task_blocks_per_sm(int* out) {
-  static int cached = 0;
-  if (cached == 0) {
-    int b = 0;
-    A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, udf_task_kernel<kSign, kStats, kBatch>,
-                                                               kTaskWarps * 32, 0));
-    cached = b < 1 ? 1 : b;
+  // per device: a process may drive GPUs of different kinds
+  static int cached[kMaxDevices] = {0};
+  int dev = 0;
+  A3D_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < kMaxDevices && cached[dev] > 0) {
+    *out = cached[dev];
+    return A3D_OK;
   }
-  *out = cached;
+  int b = 0;
+  A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, udf_task_kernel<kSign, kStats, kBatch>,
+                                                             kTaskWarps * 32, 0));
+  b = b < 1 ? 1 : b;
+  if (dev >= 0 && dev < kMaxDevices) cached[dev] = b;
+  *out = b;
   return A3D_OK;
 }
 
@@ -898,9 +904,7 @@ int launch_udf(const TreeT<kBatch>& T, const float* pts, int64_t n, const uint32
     A3D_TRY((task_blocks_per_sm<kSign, kStats, kBatch>(&bps)));
     if (shape.blocks_per_sm > 0 && shape.blocks_per_sm < bps) bps = shape.blocks_per_sm;
     const int pool = shape.pool > 0 ? shape.pool : kTaskPool;
-    int dev = 0, sms = kNumSMs;
-    A3D_CUDA_TRY(cudaGetDevice(&dev));
-    A3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int sms = num_sms();
     const int64_t pools = ceil_div(n, pool);
     const int64_t want_blocks = ceil_div(pools, kTaskWarps);
     const int64_t grid = want_blocks < (int64_t)sms * bps ? want_blocks : (int64_t)sms * bps;
@@ -918,7 +922,8 @@ int launch_udf(const TreeT<kBatch>& T, const float* pts, int64_t n, const uint32
   A3D_LAUNCH_CHECK();
   // the re-run list length is only known on the device: launch enough
   // threads for a few percent of the queries, each thread strides
-  const int64_t rr_threads = n / 16 > (int64_t)kNumSMs * 256 ? n / 16 : (int64_t)kNumSMs * 256;
+  const int64_t rr_min = (int64_t)num_sms() * 256;
+  const int64_t rr_threads = n / 16 > rr_min ? n / 16 : rr_min;
   udf_rerun_kernel<kSign, kStats, kBatch><<<(unsigned)ceil_div(rr_threads, 64), 64, 0, s>>>(
       T, pts, w.rerun, w.nrerun, out, sg, stats, w.nrerun + 1, w.nrerun + 4, sel);
   A3D_LAUNCH_CHECK();

@@ -73,3 +73,10 @@ extern "C" int a3d_udf_noalloc(const a3d_bvh_view* bvh, const float* points, int
   return a3d_udf(bvh, points, num_points, distances, face_ids, closest_points, uvw, nullptr, nullptr, nullptr,
                  A3D_UDF_SORT_QUERIES, scratch, kNoAllocScratchBytes, stream);
 }
+
+extern "C" int a3d_udf_noalloc_status(uint32_t* status_out, a3d_stream_t stream) {
+  A3D_REQUIRE(status_out, A3D_ERR_ARGUMENT, "udf_noalloc_status: null output");
+  void* scratch = nullptr;
+  A3D_TRY(scratch_address(&scratch));
+  return a3d_udf_status(scratch, status_out, stream);
+}

@@ -135,6 +135,12 @@ int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num_points,
 int a3d_udf_noalloc(const a3d_bvh_view* bvh, const float* points, int64_t num_points,
                     float* distances, int32_t* face_ids, float* closest_points,
                     float* uvw, a3d_stream_t stream);
+/* Status words of the last a3d_udf_noalloc call on the current device, in
+ * a3d_udf_status's layout (re-runs, deep-stack overflow, 0, guard faults),
+ * read from the shared static scratch after `stream` drains; a call that
+ * overlapped on the GPU with another a3d_udf_noalloc call reads a mix of
+ * both.  No counterpart in the reference. */
+int a3d_udf_noalloc_status(uint32_t* status_out, a3d_stream_t stream);
 
 /* Adjoint of the unsigned distance with respect to the mesh vertices:
  * grad_vertices[V,3] += sum_q grad_dist[q] * d dist_q / d vertex.
@@ -400,8 +406,8 @@ int a3d_dmc_emit_qef(const a3d_dmc_inputs* in, void* workspace, size_t workspace
                      float* vertices, int64_t* faces, float* l_dev, float* p_alpha, float* n_alpha,
                      a3d_stream_t stream);
 
-/* Status words of the last a3d_udf / a3d_batch_udf / a3d_udf_noalloc call
- * that used `workspace`, copied to the host after the stream drains:
+/* Status words of the last a3d_udf / a3d_batch_udf call that used
+ * `workspace`, copied to the host after the stream drains:
  * [0] queries re-run by the deep-stack kernel, [1] deep-stack overflow (a
  * re-run query's result may be inexact), [2] 0, [3] guard faults of batch
  * queries (bit 0: a node index outside the node array, bit 1: a triangle

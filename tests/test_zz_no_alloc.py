@@ -57,6 +57,22 @@ def test_noalloc_matches_regular_entry_point_twice():
         assert np.isfinite(d.cpu().numpy()).all()
 
 
+def test_noalloc_status_words_readable():
+    """A caller without the scratch address still reads the last call's
+    status words (re-runs, overflow, faults) through the accessor."""
+    v, f, _ = synthetic.udf_small(n_queries=1)
+    mesh = MeshBVH(v.cuda(), f.cuda())
+    q = (torch.rand(50_000, 3, generator=torch.Generator().manual_seed(3)) * 3.0 - 1.5).cuda()
+    call_noalloc(mesh, q)
+    fn = _lib.lib().a3d_udf_noalloc_status
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    st = (ctypes.c_uint32 * 4)(7, 7, 7, 7)
+    _lib.check("a3d_udf_noalloc_status", fn(ctypes.addressof(st), _lib.stream_ptr(q.device)))
+    assert st[1] == 0 and st[2] == 0 and st[3] == 0
+    assert st[0] < q.shape[0]
+
+
 def test_noalloc_rejects_oversized_batches():
     v, f, _ = synthetic.udf_small(n_queries=1)
     mesh = MeshBVH(v.cuda(), f.cuda())
