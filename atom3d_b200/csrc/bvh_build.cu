@@ -14,7 +14,7 @@
 //   4. one binary radix tree per mesh over its sorted range [s, e): internal
 //      nodes s..e-2 with root s, leaf j at N + j (duplicate codes
 //      disambiguated by index)
-//   4b. SAH refinement: every subtree of at most 1024 triangles below the
+//   4b. SAH refinement: every subtree of at most 16384 triangles below the
 //      top of the tree is rebuilt top-down with binned SAH by one thread
 //      block (bvh_sah.cuh), in place and within its own index range
 //   5. bottom-up refit (second arriving child computes the union box)
@@ -81,6 +81,8 @@ struct BuildWs {
   int64_t* count;       // single-mesh builds: node count
   int32_t* clusters;    // [N] roots of the subtrees the SAH pass rebuilds
   uint32_t* ncl;        // their count
+  uint32_t* sah_tmp;    // [N] partition scratch of the SAH pass
+  SahNode* sah_small;   // [N] its lists of small nodes
 };
 
 size_t carve(BuildWs& w, Workspace& ws, int64_t n, int64_t m) {
@@ -117,6 +119,8 @@ size_t carve(BuildWs& w, Workspace& ws, int64_t n, int64_t m) {
   w.count = ws.take<int64_t>(1);
   w.clusters = ws.take<int32_t>(n);
   w.ncl = ws.take<uint32_t>(1);
+  w.sah_tmp = ws.take<uint32_t>(n);
+  w.sah_small = ws.take<SahNode>(n);
   return ws.used;
 }
 
@@ -600,7 +604,8 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
   const int64_t max_clusters = n / 3 + 1;
   sah_cluster_kernel<<<(unsigned)(max_clusters < sah_grid ? max_clusters : sah_grid), kSahThreads, sizeof(SahSmem),
                        s>>>(w.clusters, w.ncl, SahTree{w.left, w.right, w.parent, w.first, w.last, n},
-                            const_cast<uint32_t*>(order), w.tri_lo, w.tri_hi, w.centroid);
+                            const_cast<uint32_t*>(order), w.sah_tmp, w.sah_small,
+                            SahPrims{w.centroid, w.tri_lo, w.tri_hi});
   A3D_LAUNCH_CHECK();
   A3D_CUDA_TRY(cudaMemsetAsync(w.visit, 0, sizeof(uint32_t) * n, s));
   refit_kernel<<<g, kThreads, 0, s>>>(order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.box_lo, w.box_hi,

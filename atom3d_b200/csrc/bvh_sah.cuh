@@ -10,8 +10,10 @@
 //     (shared-memory bins, block scans for a stable partition);
 //   * smaller nodes are handed to the block's warps, each building its
 //     subtrees alone (warp shuffles and ballots, per-warp bins).
-// Partitions are stable, reductions are min/max/integer sums, so the result
-// is deterministic.  A node with no valid split (coincident centroids) or
+// The triangles' centroids and boxes are read from global memory (L2
+// resident); the cluster's slice of the sorted face order is partitioned in
+// place.  Partitions are stable, reductions are min/max/integer sums, so the
+// result is deterministic.  A node with no valid split (coincident centroids) or
 // deeper than kSahMaxDepth inside its cluster is split at its median position.
 //
 // Node numbering stays within the cluster's own index set.  A radix-tree
@@ -30,40 +32,32 @@
 namespace a3d {
 namespace {
 
-constexpr int kSahMax = 1024;
+constexpr int kSahMax = 16384;
 constexpr int kSahBins = 16;
 constexpr int kSahWarpMax = 128;
 constexpr int kSahThreads = 256;
 constexpr int kSahWarps = kSahThreads / 32;
-constexpr int kSahMaxDepth = 40;
+constexpr int kSahMaxDepth = 48;
 constexpr int kSahCand = 3 * (kSahBins - 1);            // 45 split candidates
 constexpr int kBinWords = 3 * kSahBins * 7;              // count, lo xyz, hi xyz
 constexpr int kSahWarpStack = kSahWarpMax / 2;           // disjoint ranges of >= 2
 constexpr int kSahBlockStack = kSahMax / (kSahWarpMax + 1) + 2;
 
+// a node to split: local range [b, e) of its cluster, parent index (-1 for
+// the cluster root), side in the parent, depth inside the cluster
+struct SahNode {
+  int b, e, parent, sd;  // sd = side | depth << 1
+};
+
 struct SahSmem {
-  float c[3][kSahMax];
-  float lo[3][kSahMax];
-  float hi[3][kSahMax];
-  uint32_t face[kSahMax];
-  uint16_t ord[kSahMax];
-  uint16_t tmp[kSahMax];
   uint32_t bins[kSahWarps + 1][kBinWords];  // per warp, then the block's
-  uint2 wstack[kSahWarps][kSahWarpStack];
-  uint2 bstack[kSahBlockStack];
-  uint2 small[kSahMax / 2];
+  SahNode wstack[kSahWarps][kSahWarpStack];
+  SahNode bstack[kSahBlockStack];
   float red[kSahWarps][6];
   uint32_t wsum[kSahWarps];
   float cb[6];
-  int nsmall, nb, m, root_nat;
+  int nsmall, nb, m, axis, kk, root_nat;
 };
-
-// stack entry: x = b | e << 11 | side << 22 | depth << 23, y = parent index
-// (-1 for the cluster root)
-__device__ __forceinline__ uint2 sah_entry(int b, int e, int side, int depth, int parent) {
-  return make_uint2((uint32_t)b | ((uint32_t)e << 11) | ((uint32_t)side << 22) | ((uint32_t)depth << 23),
-                    (uint32_t)parent);
-}
 
 struct SahTree {
   int32_t* left;
@@ -139,19 +133,29 @@ __device__ __forceinline__ int sah_pick(const uint32_t* bins, const float* cb, i
   return bn;
 }
 
-__device__ __forceinline__ void sah_bin_prim(uint32_t* bins, const SahSmem& S, int p, const float* cb,
+// the triangles' centroids and boxes, indexed by face id
+struct SahPrims {
+  const float4* __restrict__ cen;
+  const float4* __restrict__ lo;
+  const float4* __restrict__ hi;
+};
+
+__device__ __forceinline__ float sah_c(const float4& c, int a) { return a == 0 ? c.x : (a == 1 ? c.y : c.z); }
+
+__device__ __forceinline__ void sah_bin_prim(uint32_t* bins, const SahPrims& P, uint32_t face, const float* cb,
                                              const float* scale) {
+  const float4 c = __ldg(P.cen + face), lo = __ldg(P.lo + face), hi = __ldg(P.hi + face);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     if (!(cb[3 + a] > cb[a])) continue;
-    uint32_t* w = bins + (a * kSahBins + sah_bin(S.c[a][p], cb[a], scale[a])) * 7;
+    uint32_t* w = bins + (a * kSahBins + sah_bin(sah_c(c, a), cb[a], scale[a])) * 7;
     atomicAdd(&w[0], 1u);
-    atomicMin(&w[1], float_flip(S.lo[0][p]));
-    atomicMin(&w[2], float_flip(S.lo[1][p]));
-    atomicMin(&w[3], float_flip(S.lo[2][p]));
-    atomicMax(&w[4], float_flip(S.hi[0][p]));
-    atomicMax(&w[5], float_flip(S.hi[1][p]));
-    atomicMax(&w[6], float_flip(S.hi[2][p]));
+    atomicMin(&w[1], float_flip(lo.x));
+    atomicMin(&w[2], float_flip(lo.y));
+    atomicMin(&w[3], float_flip(lo.z));
+    atomicMax(&w[4], float_flip(hi.x));
+    atomicMax(&w[5], float_flip(hi.y));
+    atomicMax(&w[6], float_flip(hi.z));
   }
 }
 
@@ -198,10 +202,14 @@ __device__ __forceinline__ void sah_emit(const SahTree& T, int f, int b, int m, 
 }
 
 // One block per cluster (grid-stride over the device-side cluster list).
+// The cluster's slice of the sorted face order is partitioned in place
+// (tmp: a scratch slice of the same positions); small nodes waiting for the
+// warps are listed in `small` at the cluster's positions (a cluster of n
+// triangles has fewer than n of them).
 __global__ void __launch_bounds__(kSahThreads)
     sah_cluster_kernel(const int32_t* __restrict__ clusters, const uint32_t* __restrict__ ncl, SahTree T,
-                       uint32_t* __restrict__ order, const float4* __restrict__ tri_lo,
-                       const float4* __restrict__ tri_hi, const float4* __restrict__ cen) {
+                       uint32_t* __restrict__ order, uint32_t* __restrict__ tmp_all, SahNode* __restrict__ small_all,
+                       SahPrims P) {
   extern __shared__ __align__(16) unsigned char sah_raw[];
   SahSmem& S = *reinterpret_cast<SahSmem*>(sah_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -212,20 +220,15 @@ __global__ void __launch_bounds__(kSahThreads)
     const int f = T.first[R], l = T.last[R];
     const int n = l - f + 1;
     const int shift = (R == l) ? 1 : 0;
-    for (int p = tid; p < n; p += kSahThreads) {
-      const uint32_t fc = order[f + p];
-      S.face[p] = fc;
-      S.ord[p] = (uint16_t)p;
-      const float4 c = cen[fc], a = tri_lo[fc], z = tri_hi[fc];
-      S.c[0][p] = c.x; S.c[1][p] = c.y; S.c[2][p] = c.z;
-      S.lo[0][p] = a.x; S.lo[1][p] = a.y; S.lo[2][p] = a.z;
-      S.hi[0][p] = z.x; S.hi[1][p] = z.y; S.hi[2][p] = z.z;
-    }
+    uint32_t* ord = order + f;
+    uint32_t* tmp = tmp_all + f;
+    SahNode* small = small_all + f;
     if (tid == 0) {
       S.nsmall = 0;
       S.nb = 0;
-      if (n > kSahWarpMax) S.bstack[S.nb++] = sah_entry(0, n, 0, 0, -1);
-      else S.small[S.nsmall++] = sah_entry(0, n, 0, 0, -1);
+      const SahNode root{0, n, -1, 0};
+      if (n > kSahWarpMax) S.bstack[S.nb++] = root;
+      else small[S.nsmall++] = root;
     }
     __syncthreads();
     // ---- stage A: nodes above kSahWarpMax, split by the whole block
@@ -233,16 +236,16 @@ __global__ void __launch_bounds__(kSahThreads)
       __syncthreads();
       const int nb = S.nb;
       if (nb == 0) break;
-      const uint2 en = S.bstack[nb - 1];
-      const int b = en.x & 2047, e = (en.x >> 11) & 2047, side = (en.x >> 22) & 1, depth = (int)(en.x >> 23);
-      const int plabel = (int)en.y;
+      const SahNode en = S.bstack[nb - 1];
+      const int b = en.b, e = en.e, side = en.sd & 1, depth = en.sd >> 1;
+      const int plabel = en.parent;
       const bool is_root = plabel < 0;
       // centroid bounds
       float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
       for (int i = b + tid; i < e; i += kSahThreads) {
-        const int p = S.ord[i];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) { mn[a] = fminf(mn[a], S.c[a][p]); mx[a] = fmaxf(mx[a], S.c[a][p]); }
+        const float4 c = __ldg(P.cen + ord[i]);
+        mn[0] = fminf(mn[0], c.x); mn[1] = fminf(mn[1], c.y); mn[2] = fminf(mn[2], c.z);
+        mx[0] = fmaxf(mx[0], c.x); mx[1] = fmaxf(mx[1], c.y); mx[2] = fmaxf(mx[2], c.z);
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1)
@@ -268,29 +271,29 @@ __global__ void __launch_bounds__(kSahThreads)
       for (int a = 0; a < 3; ++a) scale[a] = cb[3 + a] > cb[a] ? (float)kSahBins / (cb[3 + a] - cb[a]) : 0.f;
       const bool median = depth >= kSahMaxDepth;
       if (!median)
-        for (int i = b + tid; i < e; i += kSahThreads) sah_bin_prim(S.bins[kSahWarps], S, S.ord[i], cb, scale);
+        for (int i = b + tid; i < e; i += kSahThreads) sah_bin_prim(S.bins[kSahWarps], P, ord[i], cb, scale);
       __syncthreads();
       if (warp == 0) {
         int axis = 0, kk = 0, nl = 0;
         if (!median) nl = sah_pick(S.bins[kSahWarps], cb, lane, axis, kk);
         if (lane == 0) {
           S.m = nl > 0 ? b + nl : b + (e - b) / 2;
-          S.red[0][0] = __int_as_float(nl > 0 ? axis : -1);
-          S.red[0][1] = __int_as_float(kk);
+          S.axis = nl > 0 ? axis : -1;
+          S.kk = kk;
         }
       }
       __syncthreads();
-      const int m = S.m, axis = __float_as_int(S.red[0][0]), kk = __float_as_int(S.red[0][1]);
+      const int m = S.m, axis = S.axis, kk = S.kk;
       if (axis >= 0) {
         // stable partition: block-wide ranks of the left flags, chunk by chunk
         int lbase = b, rbase = m;
         for (int i0 = b; i0 < e; i0 += kSahThreads) {
           const int i = i0 + tid;
-          int p = 0;
+          uint32_t p = 0;
           bool lft = false;
           if (i < e) {
-            p = S.ord[i];
-            lft = sah_bin(S.c[axis][p], cb[axis], scale[axis]) < kk;
+            p = ord[i];
+            lft = sah_bin(sah_c(__ldg(P.cen + p), axis), cb[axis], scale[axis]) < kk;
           }
           const unsigned bl = __ballot_sync(FULL, lft), br = __ballot_sync(FULL, i < e && !lft);
           __syncthreads();
@@ -305,14 +308,14 @@ __global__ void __launch_bounds__(kSahThreads)
           }
           const unsigned below = (1u << lane) - 1u;
           if (i < e) {
-            if (lft) S.tmp[lbase + lb + __popc(bl & below)] = (uint16_t)p;
-            else S.tmp[rbase + rb + __popc(br & below)] = (uint16_t)p;
+            if (lft) tmp[lbase + lb + __popc(bl & below)] = p;
+            else tmp[rbase + rb + __popc(br & below)] = p;
           }
           lbase += lt;
           rbase += rt;
         }
         __syncthreads();
-        for (int i = b + tid; i < e; i += kSahThreads) S.ord[i] = S.tmp[i];
+        for (int i = b + tid; i < e; i += kSahThreads) ord[i] = tmp[i];
       }
       __syncthreads();
       if (tid == 0) {
@@ -320,37 +323,37 @@ __global__ void __launch_bounds__(kSahThreads)
         if (is_root) S.root_nat = f + m - 1 + shift;
         const int label = sah_label(f, m, shift, R, S.root_nat, is_root);
         sah_emit(T, f, b, m, e, label, plabel, side, [&](int cb0, int ce0, int cs) {
-          const uint2 ch = sah_entry(cb0, ce0, cs, depth + 1, label);
+          const SahNode ch{cb0, ce0, label, cs | ((depth + 1) << 1)};
           if (ce0 - cb0 > kSahWarpMax) S.bstack[S.nb++] = ch;
-          else S.small[S.nsmall++] = ch;
+          else small[S.nsmall++] = ch;
         });
       }
     }
+    __syncthreads();
     // ---- stage B: each warp builds the subtrees of its small nodes
     uint32_t* wb = S.bins[warp];
-    uint2* ws = S.wstack[warp];
+    SahNode* ws = S.wstack[warp];
     const int nsmall = S.nsmall;
     for (int si = warp; si < nsmall; si += kSahWarps) {
-      int sp = 0;
-      if (lane == 0) ws[0] = S.small[si];
-      sp = 1;
+      if (lane == 0) ws[0] = small[si];
+      int sp = 1;
       __syncwarp();
       while (sp > 0) {
-        const uint2 en = ws[sp - 1];
+        const SahNode en = ws[sp - 1];
         --sp;
         __syncwarp();
-        const int b = en.x & 2047, e = (en.x >> 11) & 2047, side = (en.x >> 22) & 1, depth = (int)(en.x >> 23);
-        const int plabel = (int)en.y;
+        const int b = en.b, e = en.e, side = en.sd & 1, depth = en.sd >> 1;
+        const int plabel = en.parent;
         const bool is_root = plabel < 0;
-        int m = b + 1, axis = -1, kk = 0;
-        float cb[6], scale[3];
+        int m = b + 1;
         if (e - b > 2) {
           float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
           for (int i = b + lane; i < e; i += 32) {
-            const int p = S.ord[i];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) { mn[a] = fminf(mn[a], S.c[a][p]); mx[a] = fmaxf(mx[a], S.c[a][p]); }
+            const float4 c = __ldg(P.cen + ord[i]);
+            mn[0] = fminf(mn[0], c.x); mn[1] = fminf(mn[1], c.y); mn[2] = fminf(mn[2], c.z);
+            mx[0] = fmaxf(mx[0], c.x); mx[1] = fmaxf(mx[1], c.y); mx[2] = fmaxf(mx[2], c.z);
           }
+          float cb[6], scale[3];
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
@@ -364,11 +367,11 @@ __global__ void __launch_bounds__(kSahThreads)
             cb[3 + a] = mx[a];
             scale[a] = mx[a] > mn[a] ? (float)kSahBins / (mx[a] - mn[a]) : 0.f;
           }
-          int nl = 0;
+          int nl = 0, axis = 0, kk = 0;
           if (depth < kSahMaxDepth) {
             sah_clear_bins(wb, lane, 32);
             __syncwarp();
-            for (int i = b + lane; i < e; i += 32) sah_bin_prim(wb, S, S.ord[i], cb, scale);
+            for (int i = b + lane; i < e; i += 32) sah_bin_prim(wb, P, ord[i], cb, scale);
             __syncwarp();
             nl = sah_pick(wb, cb, lane, axis, kk);
             __syncwarp();
@@ -378,23 +381,23 @@ __global__ void __launch_bounds__(kSahThreads)
             int lbase = b, rbase = m;
             for (int i0 = b; i0 < e; i0 += 32) {
               const int i = i0 + lane;
-              int p = 0;
+              uint32_t p = 0;
               bool lft = false;
               if (i < e) {
-                p = S.ord[i];
-                lft = sah_bin(S.c[axis][p], cb[axis], scale[axis]) < kk;
+                p = ord[i];
+                lft = sah_bin(sah_c(__ldg(P.cen + p), axis), cb[axis], scale[axis]) < kk;
               }
               const unsigned bl = __ballot_sync(FULL, lft), br = __ballot_sync(FULL, i < e && !lft);
               const unsigned below = (1u << lane) - 1u;
               if (i < e) {
-                if (lft) S.tmp[lbase + __popc(bl & below)] = (uint16_t)p;
-                else S.tmp[rbase + __popc(br & below)] = (uint16_t)p;
+                if (lft) tmp[lbase + __popc(bl & below)] = p;
+                else tmp[rbase + __popc(br & below)] = p;
               }
               lbase += __popc(bl);
               rbase += __popc(br);
             }
             __syncwarp();
-            for (int i = b + lane; i < e; i += 32) S.ord[i] = S.tmp[i];
+            for (int i = b + lane; i < e; i += 32) ord[i] = tmp[i];
             __syncwarp();
           } else {
             m = b + (e - b) / 2;
@@ -404,15 +407,13 @@ __global__ void __launch_bounds__(kSahThreads)
           if (is_root) S.root_nat = f + m - 1 + shift;
           const int label = sah_label(f, m, shift, R, S.root_nat, is_root);
           sah_emit(T, f, b, m, e, label, plabel, side, [&](int cb0, int ce0, int cs) {
-            ws[sp++] = sah_entry(cb0, ce0, cs, depth + 1, label);
+            ws[sp++] = SahNode{cb0, ce0, label, cs | ((depth + 1) << 1)};
           });
         }
         sp = __shfl_sync(FULL, sp, 0);
         __syncwarp();
       }
     }
-    __syncthreads();
-    for (int p = tid; p < n; p += kSahThreads) order[f + p] = S.face[S.ord[p]];
     __syncthreads();
   }
 }
