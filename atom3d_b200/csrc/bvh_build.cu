@@ -18,10 +18,11 @@
 //      top of the tree is rebuilt top-down with binned SAH by one thread
 //      block (bvh_sah.cuh), in place and within its own index range
 //   5. bottom-up refit (second arriving child computes the union box)
-//   6. surface-area-guided collapse into 4-wide quantised nodes: starting
-//      from a binary node, the child with the largest surface area is opened
-//      until four slots are used; subtrees of <= leaf_max triangles become
-//      leaves.  Level-synchronous over device-side worklists; a wide node is
+//   6. SAH-optimal collapse into 4-wide quantised nodes: the refit also
+//      computes, bottom-up, the cheapest cover of every subtree by 1..4 wide
+//      slots (leaf or wide node, weighted by surface area); a wide node's
+//      children are the subtrees that cover chose, leaves hold at most
+//      leaf_max triangles.  Level-synchronous over device-side worklists; a wide node is
 //      written at the slot of its binary node, so the order in which a
 //      level's work is done does not matter
 //   7. layout: wide nodes stably sorted by level -- breadth first, each
@@ -81,6 +82,8 @@ struct BuildWs {
   int64_t* count;       // single-mesh builds: node count
   int32_t* clusters;    // [N] roots of the subtrees the SAH pass rebuilds
   uint32_t* ncl;        // their count
+  float4* dp_cost;      // [N] collapse cost of each internal node spread over 1..4 wide slots
+  uint32_t* dp_dec;     // [N] the decisions behind dp_cost (see refit_kernel)
   uint32_t* sah_tmp;    // [N] partition scratch of the SAH pass
   SahNode* sah_small;   // [N] its lists of small nodes
 };
@@ -119,6 +122,8 @@ size_t carve(BuildWs& w, Workspace& ws, int64_t n, int64_t m) {
   w.count = ws.take<int64_t>(1);
   w.clusters = ws.take<int32_t>(n);
   w.ncl = ws.take<uint32_t>(1);
+  w.dp_cost = ws.take<float4>(n);
+  w.dp_dec = ws.take<uint32_t>(n);
   w.sah_tmp = ws.take<uint32_t>(n);
   w.sah_small = ws.take<SahNode>(n);
   return ws.used;
@@ -320,11 +325,42 @@ __global__ void radix_tree_kernel(const uint64_t* __restrict__ keys, const int64
   if (ii == s) parent[i] = -1;
 }
 
-// 5. refit: leaf boxes from sorted triangles, unions bottom-up
+__device__ __forceinline__ float half_area(float4 lo, float4 hi) {
+  const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+  return dx * dy + dy * dz + dz * dx;
+}
+
+// Cost weights of the SAH-optimal collapse: a wide-node visit against one
+// triangle test, as measured on the closest-point traversal (a 4-box node
+// visit costs about 6.7 triangle tests: 16M-query workload, leaves of 4 vs 8)
+constexpr float kCostNode = 6.7f, kCostTri = 1.0f;
+
+// 5. refit: leaf boxes from sorted triangles, unions bottom-up; and, at each
+// internal node, the SAH-optimal collapse costs.  cost[i] (i = 1..4) is the
+// cheapest way to cover the node's subtree with i slots of a wide node:
+//   cost[1] = min(leaf: kCostTri * A * count   (count <= leaf_max, not a root),
+//                 wide node: kCostNode * A + min over j = 2..4 of split[j])
+//   split[j] = min over k of cost_left[k] + cost_right[j - k]
+//   cost[i > 1] = min(cost[i - 1], split[i])
+// with A the node's half surface area (a binary leaf costs kCostTri * A for
+// any i).  dec bytes: [0] = 0 for a leaf, else (slots << 2) | k of the best
+// wide node; [i-1] (i = 2..4) = k of split[i], or 0xff when cost[i-1] wins.
+__device__ __forceinline__ void child_costs(int c, int64_t n, const float4* box_lo, const float4* box_hi,
+                                            const float4* cost, float out[5]) {
+  if (c >= n) {
+    const float a = kCostTri * half_area(__ldcg(&box_lo[c]), __ldcg(&box_hi[c]));
+    out[1] = out[2] = out[3] = out[4] = a;
+  } else {
+    const float4 v = __ldcg(&cost[c]);
+    out[1] = v.x; out[2] = v.y; out[3] = v.z; out[4] = v.w;
+  }
+}
+
 __global__ void refit_kernel(const uint32_t* __restrict__ order, const float4* __restrict__ tri_lo,
                              const float4* __restrict__ tri_hi, int64_t n, const int32_t* __restrict__ left,
                              const int32_t* __restrict__ right, const int32_t* __restrict__ parent,
-                             float4* box_lo, float4* box_hi, uint32_t* visit) {
+                             const int32_t* __restrict__ first, const int32_t* __restrict__ last, int leaf_max,
+                             float4* box_lo, float4* box_hi, float4* cost, uint32_t* dec, uint32_t* visit) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const int64_t leaf = n + j;
@@ -339,16 +375,50 @@ __global__ void refit_kernel(const uint32_t* __restrict__ order, const float4* _
     const int l = left[p], r = right[p];
     const float4 al = __ldcg(&box_lo[l]), ah = __ldcg(&box_hi[l]);
     const float4 bl = __ldcg(&box_lo[r]), bh = __ldcg(&box_hi[r]);
-    __stcg(&box_lo[p], make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.f));
-    __stcg(&box_hi[p], make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.f));
+    const float4 lo = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.f);
+    const float4 hi = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.f);
+    __stcg(&box_lo[p], lo);
+    __stcg(&box_hi[p], hi);
+    // collapse costs
+    float cl[5], cr[5];
+    child_costs(l, n, box_lo, box_hi, cost, cl);
+    child_costs(r, n, box_lo, box_hi, cost, cr);
+    float split[5] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY};
+    int sk[5] = {0, 0, 0, 0, 0};
+    for (int i = 2; i <= 4; ++i)
+      for (int k = 1; k < i; ++k) {
+        const float c = cl[k] + cr[i - k];
+        if (c < split[i]) { split[i] = c; sk[i] = k; }
+      }
+    const float area = half_area(lo, hi);
+    int wi = 2;
+    for (int i = 3; i <= 4; ++i)
+      if (split[i] < split[wi]) wi = i;
+    const float wide = kCostNode * area + split[wi];
+    const int count = last[p] - first[p] + 1;
+    const float leafc = (count <= leaf_max && parent[p] >= 0) ? kCostTri * area * (float)count : INFINITY;
+    float c[5];
+    uint32_t d = 0;
+    if (leafc <= wide) {
+      c[1] = leafc;
+    } else {
+      c[1] = wide;
+      d = (uint32_t)((wi << 2) | sk[wi]);
+    }
+    for (int i = 2; i <= 4; ++i) {
+      if (c[i - 1] <= split[i]) {
+        c[i] = c[i - 1];
+        d |= 0xffu << (8 * (i - 1));
+      } else {
+        c[i] = split[i];
+        d |= (uint32_t)sk[i] << (8 * (i - 1));
+      }
+    }
+    __stcg(&cost[p], make_float4(c[1], c[2], c[3], c[4]));
+    __stcg(&dec[p], d);
     __threadfence();
     p = parent[p];
   }
-}
-
-__device__ __forceinline__ float half_area(float4 lo, float4 hi) {
-  const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
-  return dx * dy + dy * dz + dz * dx;
 }
 
 __device__ __forceinline__ uint32_t scale_exponent(float ext) {
@@ -381,7 +451,8 @@ __global__ void __launch_bounds__(kThreads)
                           int32_t* __restrict__ nxt, int64_t n, int leaf_max, const int32_t* __restrict__ left,
                           const int32_t* __restrict__ right, const int32_t* __restrict__ first,
                           const int32_t* __restrict__ last, const float4* __restrict__ box_lo,
-                          const float4* __restrict__ box_hi, WideNode* __restrict__ tmp, uint32_t* __restrict__ lvl) {
+                          const float4* __restrict__ box_hi, const uint32_t* __restrict__ dec,
+                          WideNode* __restrict__ tmp, uint32_t* __restrict__ lvl) {
   const uint32_t cnt = counters[level];
   const int nn = (int)n;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += (int64_t)gridDim.x * blockDim.x) {
@@ -392,24 +463,36 @@ __global__ void __launch_bounds__(kThreads)
       c[0] = b;
       nc = 1;
     } else {
-      c[0] = left[b];
-      c[1] = right[b];
-      nc = 2;
-      while (nc < 4) {
-        int best = -1;
-        float best_a = -1.f;
-        for (int j = 0; j < nc; ++j) {
-          if (c[j] < nn) {
-            const float a = half_area(box_lo[c[j]], box_hi[c[j]]);
-            if (a > best_a) { best_a = a; best = j; }
-          }
+      // the subtrees the SAH-optimal collapse chose for this node's slots,
+      // expanded left to right (a pending (node, slots) pair per entry)
+      const uint32_t d0 = dec[b];
+      int pn[4], ps[4], np = 0;
+      const int slots = (int)((d0 & 0xffu) >> 2), k0 = (int)(d0 & 3u);
+      if (slots >= 2 && k0 >= 1 && k0 < slots) {
+        pn[0] = right[b]; ps[0] = slots - k0;  // stack: right pushed first
+        pn[1] = left[b]; ps[1] = k0;
+        np = 2;
+      } else {  // a root the cost model would have made a leaf: two slots
+        pn[0] = right[b]; ps[0] = 1;
+        pn[1] = left[b]; ps[1] = 1;
+        np = 2;
+      }
+      nc = 0;
+      while (np > 0 && nc < 4) {
+        --np;
+        const int x = pn[np];
+        int i = ps[np];
+        if (x < nn) {
+          const uint32_t dx = dec[x];
+          while (i > 1 && ((dx >> (8 * (i - 1))) & 0xffu) == 0xffu) --i;
         }
-        if (best < 0) break;
-        const int x = c[best];
-        for (int j = nc; j > best + 1; --j) c[j] = c[j - 1];
-        c[best] = left[x];
-        c[best + 1] = right[x];
-        ++nc;
+        if (i <= 1 || x >= nn) {
+          c[nc++] = x;
+        } else {
+          const int k = (int)((dec[x] >> (8 * (i - 1))) & 0xffu);
+          pn[np] = right[x]; ps[np] = i - k; ++np;
+          pn[np] = left[x]; ps[np] = k; ++np;
+        }
       }
     }
     const float4 plo = box_lo[b], phi = box_hi[b];
@@ -438,7 +521,7 @@ __global__ void __launch_bounds__(kThreads)
       quantize_axis(nd.oy, sy, lo.y, hi.y, a0, a1); nd.q[1] |= a0 << (8 * j); nd.q[4] |= a1 << (8 * j);
       quantize_axis(nd.oz, sz, lo.z, hi.z, a0, a1); nd.q[2] |= a0 << (8 * j); nd.q[5] |= a1 << (8 * j);
       const int count = cj >= nn ? 1 : last[cj] - first[cj] + 1;
-      if (count <= leaf_max) {
+      if (cj >= nn || (dec[cj] & 0xffu) == 0u) {
         const uint32_t f0 = cj >= nn ? (uint32_t)(cj - nn) : (uint32_t)first[cj];
         nd.ref[j] = make_leaf_ref(f0, (uint32_t)count);
       } else {
@@ -608,8 +691,8 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
                             SahPrims{w.centroid, w.tri_lo, w.tri_hi});
   A3D_LAUNCH_CHECK();
   A3D_CUDA_TRY(cudaMemsetAsync(w.visit, 0, sizeof(uint32_t) * n, s));
-  refit_kernel<<<g, kThreads, 0, s>>>(order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.box_lo, w.box_hi,
-                                      w.visit);
+  refit_kernel<<<g, kThreads, 0, s>>>(order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.first, w.last,
+                                      leaf_max, w.box_lo, w.box_hi, w.dp_cost, w.dp_dec, w.visit);
   A3D_LAUNCH_CHECK();
   write_tris_kernel<<<g, kThreads, 0, s>>>(V, vert_off, F, face_off, w.mesh_of, order, n, tris_out);
   A3D_LAUNCH_CHECK();
@@ -622,7 +705,7 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
   for (int level = 0; level < kMaxLevels; ++level) {
     collapse_level_kernel<<<(unsigned)lb, kThreads, 0, s>>>(level, w.counters, cur, nxt, n, leaf_max, w.left,
                                                             w.right, w.first, w.last, w.box_lo, w.box_hi,
-                                                            w.tmp_nodes, w.lvl);
+                                                            w.dp_dec, w.tmp_nodes, w.lvl);
     A3D_LAUNCH_CHECK();
     int32_t* t = cur;
     cur = nxt;
