@@ -186,6 +186,85 @@ def cpu_baseline(v, f, q, budget_s=15.0):
             "sample": f"{n} of the 16,777,216 queries (brute force over all 1,310,720 triangles)"}
 
 
+def fp64_check(v, f, q, dist_d, fid_d, n_sample=1024):
+    """Error of the device results against the oracle's FP64 brute force on a
+    stratified sample (half surface-band, half box queries): max distance
+    error (absolute and over the box diagonal) and face ids exact or tied."""
+    from oracle import orc
+
+    n = q.shape[0]
+    g = np.random.default_rng(2024)
+    h = n_sample // 2
+    pick = np.sort(np.concatenate([g.choice(n // 2, h, replace=False), n // 2 + g.choice(n - n // 2, h, replace=False)]))
+    pt = torch.from_numpy(pick).to(dist_d.device)
+    d = dist_d[pt].double().cpu().numpy()
+    fid = fid_d[pt].cpu().numpy()
+    qs = q[pick].numpy()
+    t0 = time.perf_counter()
+    d64, f64, _ = orc.udf_exact(v.numpy(), f.numpy(), qs)
+    diag = float((v.double().max(0).values - v.double().min(0).values).norm())
+    err = float(np.abs(d - d64).max())
+    dm = orc.tri_dist(v.numpy(), f.numpy(), qs, fid)
+    tie = np.abs(dm - d64) <= 1e-6 * diag
+    return {"sample": int(pick.shape[0]), "max_abs_err": err, "max_err_over_diag": err / diag,
+            "face_ids_exact": float((fid == f64).mean()), "face_ids_exact_or_tie": float(((fid == f64) | tie).mean()),
+            "oracle": "FP64 brute force over all triangles", "oracle_s": time.perf_counter() - t0}
+
+
+def reference_gpu_bar(steps=3):
+    """The reference's own CUDA kernels (compiled from its sources into
+    oracle/_ref with its flags) on this GPU: its host SAH build, bvh_udf on
+    the 16,777,216-query workload, and octree_traverse 4 -> 10 plus
+    sparse_flood_fill at 1024^3 (the 327,680-triangle sphere) driven by the
+    restated host glue.  Wall-clock with synchronisation (the reference's
+    flood fill runs on the legacy default stream with a host loop)."""
+    from oracle import ref_gpu
+
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref not built (oracle/build_ref.py needs the reference checkout)"}
+    from atom3d_b200 import synthetic
+
+    dev = torch.device("cuda", 0)
+    out = {"build": "reference sources, -O3 --use_fast_math, sm_100a (oracle/build_ref.py)"}
+
+    def wall(fn, k):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(k):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts) * 1e3
+
+    v, f, q = synthetic.udf_large()
+    t0 = time.perf_counter()
+    rb = ref_gpu.RefBVH(v.to(dev), f.to(dev))
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    qd = q.to(dev)
+    ms = wall(lambda: rb.udf(qd), steps)
+    out["udf"] = {"queries": int(q.shape[0]), "ms": ms, "Mqueries_per_s": q.shape[0] / ms / 1e3,
+                  "host_sah_build_s": build_s}
+    del qd, rb
+    v2, f2 = synthetic.octree_mesh()
+    rb2 = ref_gpu.RefBVH(v2.to(dev), f2.to(dev))
+    bounds = torch.tensor([[-1.5] * 3, [1.5] * 3])
+    oct_ms = wall(lambda: ref_gpu.octree_traverse(rb2, bounds, 4, 10), steps)
+    dam = ref_gpu.octree_traverse(rb2, bounds, 4, 10)
+
+    def flood():
+        water, dry, coll, tdam, _, _ = ref_gpu.flood_fill_3d_sparse(dam, 1024, padding=10, connectivity=26)
+        ref_gpu.dam_neighborhood_signs(tdam, water, dry, 1024, 1)
+
+    flood_ms = wall(flood, max(1, steps - 1))
+    out["octree_flood_1024"] = {"octree_ms": oct_ms, "flood_fill_ms": flood_ms, "candidates": int(dam.shape[0])}
+    return out
+
+
 def run_reference(args):
     rank, world, local = setup_dist(args.gpus)
     if rank != 0:
@@ -212,6 +291,17 @@ def run_reference(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "sample_queries": n},
             "cpu_baseline": base, "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        line["reference_gpu"] = reference_gpu_bar()
+    except Exception as e:  # the reference's GPU bar is a reported extra
+        line["reference_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    dmc_golden = os.path.join(HERE, "tests", "golden", "dmc512.npz")
+    if os.path.exists(dmc_golden):
+        g = np.load(dmc_golden)
+        line["reference_cpu_dmc_512"] = {
+            "forward_s": float(g["ref_cpu_s"][0]), "backward_s": float(g["ref_cpu_s"][1]),
+            "cubes": int(g["n_cubes"]), "where": "build container, 8 threads (tests/golden/make_dmc512_golden.py); "
+            "the reference's SparseDiffDMC is Python and is not on the GPU machine"}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -349,6 +439,9 @@ def main():
             line["batch"] = bench_batch(dev, 2, 1, cpu=cpu)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(v, f, q)
+        step()
+        torch.cuda.synchronize()
+        line["fp64_check"] = fp64_check(v, f, q, dist_o, fid_o)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
