@@ -712,6 +712,159 @@ __global__ void vd_bwd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv,
   }
 }
 
+// ---- vertex features (v_features) ---------------------------------------------
+// Per dual vertex v and channel c:
+//   feat[v, c] = sum_k b_k uf_k[c] / (sum_k b_k + 1e-8),
+//   uf_k[c]    = (f[i0, c] w0 + f[i1, c] w1) / (w0 + w1), w0 = s1 a1, w1 = -s0 a0
+// the weights of p_alpha (atom3d/mesh_extractor/sparse_diffdmc.py:658-663,
+// :762-770); the training split appends each quad's mean feature (:815-818).
+__global__ void vd_feat_kernel(DmcIn in, int64_t nv, int C, const float* __restrict__ feat,
+                               const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
+                               const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot, EdgeData ed,
+                               float* __restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nv * C) return;
+  const int64_t v = t / C;
+  const int c = (int)(t - v * C);
+  const uint32_t cs = vd_cube[v];
+  const uint32_t vedges = vd_edges(case_s[cs], vd_slot[v]);
+  const uint32_t cube = list[cs];
+  float acc = 0.f, bsum = 0.f;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
+    const int32_t r = ed.idx_map[(int64_t)cs * 12 + e];
+    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
+    const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
+    const float a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
+    const float a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
+    const float b = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
+    const float w0 = fm(s1, a1), w1 = -fm(s0, a0);
+    const float uf = interp1(ldf(feat, i0 * C + c), ldf(feat, i1 * C + c), w0, w1, fa(w0, w1));
+    acc = fa(acc, fm(uf, b));
+    bsum = fa(bsum, b);
+  }
+  out[v * C + c] = fd(acc, fa(bsum, 1e-8f));
+}
+
+__global__ void quad_feat_kernel(int64_t nq, int64_t nv, int C, const int32_t* __restrict__ quads,
+                                 float* __restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nq * C) return;
+  const int64_t q = t / C;
+  const int c = (int)(t - q * C);
+  float s = 0.f;
+  for (int k = 0; k < 4; ++k) s = fa(s, out[(int64_t)quads[4 * q + k] * C + c]);
+  out[(nv + q) * C + c] = fm(s, 0.25f);
+}
+
+__global__ void quad_feat_bwd_kernel(int64_t nq, int64_t nv, int C, const int32_t* __restrict__ quads,
+                                     const float* __restrict__ g_out, float* __restrict__ scratch) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nq * C) return;
+  const int64_t q = t / C;
+  const int c = (int)(t - q * C);
+  const float g = g_out[(nv + q) * C + c] * 0.25f;
+  for (int k = 0; k < 4; ++k) atomicAdd(&scratch[(int64_t)quads[4 * q + k] * C + c], g);
+}
+
+struct FeatGrad {
+  const float* g_out;  // [V(+Q), C]
+  const float* extra;  // [V, C] the quad centres' share, or null
+  float* g_feat;       // [M, C] or null
+  float* g_sdf;        // [M] or null
+  float* g_alpha;      // [N, 8] raw or null
+  float* g_beta;       // [N, 12] raw or null
+};
+
+// one thread per dual vertex, channels looped (the edge weights' gradients
+// sum over the channels)
+__global__ void vd_feat_bwd_kernel(DmcIn in, int64_t nv, int C, const float* __restrict__ feat,
+                                   const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
+                                   const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
+                                   EdgeData ed, FeatGrad gr) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const uint32_t cs = vd_cube[v];
+  const uint32_t vedges = vd_edges(case_s[cs], vd_slot[v]);
+  const uint32_t cube = list[cs];
+  int64_t I0[7], I1[7];
+  int E[7];
+  float S0[7], S1[7], A0[7], A1[7], B[7];
+  int ne = 0;
+  float bsum = 0.f;
+  for (int k = 0; k < 7; ++k) {
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
+    const int32_t r = ed.idx_map[(int64_t)cs * 12 + e];
+    I0[ne] = ed.e0[r];
+    I1[ne] = ed.e1[r];
+    E[ne] = e;
+    S0[ne] = fsb(in.sdf[I0[ne]], in.iso);
+    S1[ne] = fsb(in.sdf[I1[ne]], in.iso);
+    A0[ne] = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
+    A1[ne] = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
+    B[ne] = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
+    bsum = fa(bsum, B[ne]);
+    ++ne;
+  }
+  const float bden = fa(bsum, 1e-8f);
+  const float inv_bden = 1.0f / bden;
+  auto gvf = [&](int c) {
+    float g = gr.g_out[v * C + c];
+    if (gr.extra) g += gr.extra[v * C + c];
+    return g;
+  };
+  // dL/dbden through feat[c] = acc[c] / bden
+  float gB = 0.f;
+  for (int c = 0; c < C; ++c) {
+    const float g = gvf(c);
+    if (g == 0.f) continue;
+    float acc = 0.f;
+    for (int q = 0; q < ne; ++q) {
+      const float w0 = fm(S1[q], A1[q]), w1 = -fm(S0[q], A0[q]);
+      const float uf = interp1(feat[I0[q] * C + c], feat[I1[q] * C + c], w0, w1, fa(w0, w1));
+      acc = fa(acc, fm(uf, B[q]));
+    }
+    gB -= g * fd(acc, bden) * inv_bden;
+  }
+  for (int q = 0; q < ne; ++q) {
+    const float w0 = S1[q] * A1[q], w1 = -(S0[q] * A0[q]), den = w0 + w1;
+    const float inv = 1.0f / den;
+    float gw0 = 0.f, gw1 = 0.f, gb = gB;
+    for (int c = 0; c < C; ++c) {
+      const float g = gvf(c);
+      if (g == 0.f) continue;
+      const float f0 = feat[I0[q] * C + c], f1 = feat[I1[q] * C + c];
+      const float uf = (f0 * w0 + f1 * w1) * inv;
+      const float guf = g * B[q] * inv_bden;
+      gb += g * uf * inv_bden;
+      gw0 += guf * (f0 - uf) * inv;
+      gw1 += guf * (f1 - uf) * inv;
+      if (gr.g_feat) {
+        atomicAdd(&gr.g_feat[I0[q] * C + c], guf * w0 * inv);
+        atomicAdd(&gr.g_feat[I1[q] * C + c], guf * w1 * inv);
+      }
+    }
+    if (gr.g_sdf) {
+      atomicAdd(&gr.g_sdf[I1[q]], gw0 * A1[q]);
+      atomicAdd(&gr.g_sdf[I0[q]], -gw1 * A0[q]);
+    }
+    const int e = E[q];
+    if (gr.g_alpha && in.alpha) {
+      const int c0 = kCE[2 * e], c1 = kCE[2 * e + 1];
+      const float t0 = tanhf(in.alpha[8 * (int64_t)cube + c0]), t1 = tanhf(in.alpha[8 * (int64_t)cube + c1]);
+      atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c1], gw0 * S1[q] * in.wscale * (1.f - t1 * t1));
+      atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c0], -gw1 * S0[q] * in.wscale * (1.f - t0 * t0));
+    }
+    if (gr.g_beta && in.beta) {
+      const float tb = tanhf(in.beta[12 * (int64_t)cube + e]);
+      gr.g_beta[12 * (int64_t)cube + e] += gb * in.wscale * (1.f - tb * tb);
+    }
+  }
+}
+
 // ---- workspace ------------------------------------------------------------------
 struct DmcWs {
   float* x;            // [M,3]
@@ -977,6 +1130,61 @@ extern "C" int a3d_dmc_backward(const a3d_dmc_inputs* p, void* workspace, size_t
   }
   EdgeData ed{w.e0, w.e1, w.idx_map};
   vd_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, w.x, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, gr);
+  A3D_LAUNCH_CHECK();
+  return A3D_OK;
+}
+
+extern "C" int a3d_dmc_features(const a3d_dmc_inputs* p, void* workspace, size_t workspace_bytes,
+                                const int64_t* counts, const float* features, int32_t channels,
+                                int32_t with_centres, float* out, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(p && counts && features && out && channels > 0, A3D_ERR_ARGUMENT, "dmc_features: null argument");
+  const int64_t n = p->num_cubes, m = p->num_corners;
+  Workspace ws(workspace, workspace_bytes);
+  DmcWs w;
+  carve_dmc(w, ws, n > 0 ? n : 1, m > 0 ? m : 1);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "dmc_features: workspace too small");
+  const int64_t ns = counts[0], nq = counts[3], nv = counts[4];
+  if (ns == 0 || nv == 0) return A3D_OK;
+  DmcIn in = make_in(p);
+  EdgeData ed{w.e0, w.e1, w.idx_map};
+  const int C = channels;
+  vd_feat_kernel<<<gsz(nv * C), 256, 0, s>>>(in, nv, C, features, w.list, w.case_s, w.vd_cube, w.vd_slot, ed, out);
+  A3D_LAUNCH_CHECK();
+  if (with_centres && nq > 0) {
+    quad_feat_kernel<<<gsz(nq * C), 256, 0, s>>>(nq, nv, C, w.quads, out);
+    A3D_LAUNCH_CHECK();
+  }
+  return A3D_OK;
+}
+
+extern "C" int a3d_dmc_features_backward(const a3d_dmc_inputs* p, void* workspace, size_t workspace_bytes,
+                                         const int64_t* counts, const float* features, int32_t channels,
+                                         int32_t with_centres, const float* g_out, float* scratch,
+                                         float* g_features, float* g_sdf, float* g_alpha, float* g_beta,
+                                         a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(p && counts && features && g_out && channels > 0, A3D_ERR_ARGUMENT,
+              "dmc_features_backward: null argument");
+  const int64_t n = p->num_cubes, m = p->num_corners;
+  Workspace ws(workspace, workspace_bytes);
+  DmcWs w;
+  carve_dmc(w, ws, n > 0 ? n : 1, m > 0 ? m : 1);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "dmc_features_backward: workspace too small");
+  const int64_t ns = counts[0], nq = counts[3], nv = counts[4];
+  if (ns == 0 || nv == 0) return A3D_OK;
+  DmcIn in = make_in(p);
+  EdgeData ed{w.e0, w.e1, w.idx_map};
+  const int C = channels;
+  const bool centres = with_centres && nq > 0;
+  A3D_REQUIRE(!centres || scratch, A3D_ERR_ARGUMENT, "dmc_features_backward: the centres need a scratch [V, C]");
+  if (centres) {
+    quad_feat_bwd_kernel<<<gsz(nq * C), 256, 0, s>>>(nq, nv, C, w.quads, g_out, scratch);
+    A3D_LAUNCH_CHECK();
+  }
+  FeatGrad gr{g_out, centres ? scratch : nullptr, g_features, g_sdf, g_alpha, g_beta};
+  vd_feat_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, nv, C, features, w.list, w.case_s, w.vd_cube, w.vd_slot, ed,
+                                                   gr);
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }

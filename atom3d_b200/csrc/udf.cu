@@ -634,6 +634,19 @@ __global__ void __maxnreg__(kTaskMaxRegs)
       }
       done = !have;
     }
+    if (done && best_tri == 0xffffffffu && bsq < INFINITY) {
+      // the caller's bound excluded every triangle: run the query again in
+      // place, unbounded (a greedy probe seeds it), instead of handing it to
+      // the deep-stack re-run kernel
+      bsq = INFINITY;
+      best_sq = INFINITY;
+      sp = 0;
+      gsp = 0;
+      phase = kProbe;
+      ref = root;
+      have = true;
+      done = false;
+    }
     if (phase == kAbandon) done = true;
     const bool found = done && phase != kAbandon && best_tri != 0xffffffffu;
     if (done && !found) {

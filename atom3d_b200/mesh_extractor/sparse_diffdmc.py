@@ -8,8 +8,15 @@ adjoint behind torch.autograd.Function that recomputes per-edge quantities.
 Gradients flow to sdf, deform, alpha and beta like the reference's autograd
 graph.  The QEF inference mode (a module in eval mode, or inference_mode
 "qef") runs a3d_dmc_corner_gradients (unless corner_gradients are given)
-and a3d_dmc_emit_qef; it is forward-only.  Per-vertex features are not
-provided and raise NotImplementedError.
+and a3d_dmc_emit_qef; it is forward-only.  Per-corner features
+(v_features [M, C]) are interpolated to the dual vertices by
+a3d_dmc_features (training mode also appends each quad centre's mean) and
+are differentiable in training mode (a3d_dmc_features_backward).
+
+The kernels compute in float32.  float64 inputs raise TypeError unless the
+caller asks for float32 arithmetic with dtype=torch.float32 (the reference
+computes in the input dtype); other floating dtypes are cast to float32 and
+the outputs back to the input dtype.
 """
 
 from __future__ import annotations
@@ -58,6 +65,12 @@ _SIGS = {
                                     ctypes.POINTER(ctypes.c_int64)] + [ctypes.c_void_p] * 6),
     "a3d_dmc_backward": (ctypes.c_int, [ctypes.POINTER(DmcInputs), ctypes.c_void_p, ctypes.c_size_t,
                                         ctypes.POINTER(ctypes.c_int64)] + [ctypes.c_void_p] * 9),
+    "a3d_dmc_features": (ctypes.c_int, [ctypes.POINTER(DmcInputs), ctypes.c_void_p, ctypes.c_size_t,
+                                        ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
+    "a3d_dmc_features_backward": (ctypes.c_int, [ctypes.POINTER(DmcInputs), ctypes.c_void_p, ctypes.c_size_t,
+                                                 ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, ctypes.c_int32,
+                                                 ctypes.c_int32] + [ctypes.c_void_p] * 7),
     "a3d_dmc_corner_gradients_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int64, ctypes.c_int64]),
     "a3d_dmc_corner_gradients": (ctypes.c_int, [ctypes.POINTER(DmcInputs), ctypes.c_void_p, ctypes.c_size_t,
                                                 ctypes.c_void_p, ctypes.c_void_p]),
@@ -99,9 +112,23 @@ class _DmcContext:
         return ns, ng, nq, nv
 
 
+def _features(c, feat, with_centres, rows):
+    """Dual-vertex features [rows, C] (a3d_dmc_features); an empty tensor
+    when there are none."""
+    if feat is None:
+        return torch.empty(0, device=c.dev)
+    C = feat.shape[1]
+    out = torch.empty(rows, C, dtype=torch.float32, device=c.dev)
+    if c.counts[0] > 0 and c.counts[4] > 0:
+        _lib.check("a3d_dmc_features", _bind().a3d_dmc_features(
+            ctypes.byref(c.inp), c.ws.data_ptr(), c.ws.numel(), c.counts, feat.data_ptr(), C, int(with_centres),
+            out.data_ptr(), c.stream))
+    return out
+
+
 class _DmcFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, sdf, deform, alpha, beta, vox, cidx, res, iso, wscale):
+    def forward(ctx, sdf, deform, alpha, beta, vfeat, vox, cidx, res, iso, wscale):
         c = _DmcContext(vox, sdf, cidx, res, deform, alpha, beta, iso, wscale)
         ns, ng, nq, nv = c.sizes
         dev = sdf.device
@@ -114,13 +141,15 @@ class _DmcFn(torch.autograd.Function):
             _lib.check("a3d_dmc_emit", _bind().a3d_dmc_emit(
                 ctypes.byref(c.inp), c.ws.data_ptr(), c.ws.numel(), c.counts, verts.data_ptr(), faces.data_ptr(),
                 ldev.data_ptr(), pa.data_ptr(), na.data_ptr(), c.stream))
+        vf = _features(c, vfeat, True, nv + nq)
         ctx.dmc = c
+        ctx.vfeat = vfeat
         ctx.has = (deform is not None, alpha is not None, beta is not None)
         ctx.mark_non_differentiable(faces)
-        return verts, faces, ldev, pa, na
+        return verts, faces, ldev, pa, na, vf
 
     @staticmethod
-    def backward(ctx, g_verts, g_faces, g_ldev, g_pa, g_na):
+    def backward(ctx, g_verts, g_faces, g_ldev, g_pa, g_na, g_vf):
         c = ctx.dmc
         need = ctx.needs_input_grad
         dev = c.dev
@@ -139,15 +168,26 @@ class _DmcFn(torch.autograd.Function):
                 ctypes.byref(c.inp), c.ws.data_ptr(), c.ws.numel(), c.counts, _lib.ptr(gv), _lib.ptr(gl),
                 _lib.ptr(gp), _lib.ptr(gn), _lib.ptr(g_sdf), _lib.ptr(g_def), _lib.ptr(g_alpha), _lib.ptr(g_beta),
                 c.stream))
-        return g_sdf, g_def, g_alpha, g_beta, None, None, None, None, None
+        g_feat = None
+        vfeat = ctx.vfeat
+        if vfeat is not None and g_vf is not None and g_vf.numel() > 0 and c.counts[0] > 0 and c.counts[4] > 0:
+            C = vfeat.shape[1]
+            nv = int(c.counts[4])
+            g_feat = torch.zeros_like(vfeat) if need[4] else None
+            scratch = torch.zeros(nv, C, dtype=torch.float32, device=dev)
+            _lib.check("a3d_dmc_features_backward", _bind().a3d_dmc_features_backward(
+                ctypes.byref(c.inp), c.ws.data_ptr(), c.ws.numel(), c.counts, vfeat.data_ptr(), C, 1,
+                cont(g_vf).data_ptr(), scratch.data_ptr(), _lib.ptr(g_feat), _lib.ptr(g_sdf), _lib.ptr(g_alpha),
+                _lib.ptr(g_beta), c.stream))
+        return g_sdf, g_def, g_alpha, g_beta, g_feat, None, None, None, None, None
 
 
 class _DmcQefFn(torch.autograd.Function):
     """QEF inference mode: forward only."""
 
     @staticmethod
-    def forward(ctx, sdf, deform, vox, cidx, res, iso, wscale, reg, corner_gradients):
-        c = _DmcContext(vox, sdf, cidx, res, deform, None, None, iso, wscale)
+    def forward(ctx, sdf, deform, alpha, beta, vfeat, vox, cidx, res, iso, wscale, reg, corner_gradients):
+        c = _DmcContext(vox, sdf, cidx, res, deform, alpha, beta, iso, wscale)
         ns, ng, nq, nv = c.sizes
         dev = sdf.device
         lib = _bind()
@@ -167,8 +207,9 @@ class _DmcQefFn(torch.autograd.Function):
                 ctypes.byref(c.inp), c.ws.data_ptr(), c.ws.numel(), c.counts, corner_gradients.data_ptr(),
                 float(reg), verts.data_ptr(), faces.data_ptr(), ldev.data_ptr(), pa.data_ptr(), na.data_ptr(),
                 c.stream))
+        vf = _features(c, vfeat, False, nv)
         ctx.mark_non_differentiable(faces)
-        return verts, faces, ldev, pa, na
+        return verts, faces, ldev, pa, na, vf
 
     @staticmethod
     def backward(ctx, *grads):
@@ -224,11 +265,12 @@ class SparseDiffDMC(nn.Module):
         mode = ("weighted_avg" if self.training else "qef") if inference_mode == "auto" else inference_mode
         if mode not in ("weighted_avg", "qef"):
             raise ValueError(f"SparseDiffDMC: unknown inference_mode {inference_mode!r}")
-        if v_features is not None:
-            raise NotImplementedError("SparseDiffDMC: vertex features are not provided")
         _lib.require_cuda(sdf, "sdf")
         dev = sdf.device
         out_dtype = dtype or (sdf.dtype if sdf.dtype.is_floating_point else torch.float32)
+        if out_dtype == torch.float64:
+            raise TypeError("SparseDiffDMC computes in float32 on the GPU; pass float32 inputs, or "
+                            "dtype=torch.float32 to accept float32 arithmetic on float64 inputs")
 
         def f32(t, shape_last=None):
             if t is None:
@@ -238,16 +280,25 @@ class SparseDiffDMC(nn.Module):
         vox = voxel_coords.to(device=dev, dtype=torch.int64).contiguous()
         cidx = cube_idx.to(device=dev, dtype=torch.int64).contiguous()
         s = f32(sdf)
+        vf_in = None
+        if v_features is not None:
+            if v_features.dim() != 2 or v_features.shape[0] != sdf.shape[0]:
+                raise ValueError(f"v_features must be [M, C] with M = {sdf.shape[0]}, got {tuple(v_features.shape)}")
+            vf_in = f32(v_features)
         if mode == "qef":
-            # alpha only moves p_alpha; beta and gamma do not enter this mode
+            # alpha moves p_alpha (and the features' interpolation), not the
+            # QEF vertices; beta weighs the features; gamma does not enter
             cg = f32(corner_gradients)
-            verts, faces, ldev, pa, na = _DmcQefFn.apply(s, f32(deform), vox, cidx, int(resolution), float(isovalue),
-                                                         float(weight_scale), float(qef_reg_scale), cg)
-            if alpha is not None:
-                raise NotImplementedError("SparseDiffDMC: alpha weights in the QEF inference mode are not provided")
+            verts, faces, ldev, pa, na, vf = _DmcQefFn.apply(
+                s, f32(deform), f32(alpha), f32(beta), vf_in, vox, cidx, int(resolution), float(isovalue),
+                float(weight_scale), float(qef_reg_scale), cg)
         else:
-            verts, faces, ldev, pa, na = _DmcFn.apply(s, f32(deform), f32(alpha), f32(beta), vox, cidx,
-                                                      int(resolution), float(isovalue), float(weight_scale))
+            verts, faces, ldev, pa, na, vf = _DmcFn.apply(s, f32(deform), f32(alpha), f32(beta), vf_in, vox, cidx,
+                                                          int(resolution), float(isovalue), float(weight_scale))
+        if vf_in is None:
+            vf = None
         if out_dtype != torch.float32:
             verts, ldev, pa, na = (t.to(out_dtype) for t in (verts, ldev, pa, na))
-        return SparseDiffDMCOutput(vertices=verts, faces=faces, L_dev=ldev, p_alpha=pa, n_alpha=na, v_features=None)
+            if vf is not None:
+                vf = vf.to(out_dtype)
+        return SparseDiffDMCOutput(vertices=verts, faces=faces, L_dev=ldev, p_alpha=pa, n_alpha=na, v_features=vf)

@@ -388,6 +388,24 @@ int a3d_dmc_backward(const a3d_dmc_inputs* in, void* workspace, size_t workspace
                      const int64_t* counts, const float* g_vertices, const float* g_l_dev,
                      const float* g_p_alpha, const float* g_n_alpha, float* g_sdf,
                      float* g_deform, float* g_alpha, float* g_beta, a3d_stream_t stream);
+/* Vertex features (SparseDiffDMC's v_features,
+ * atom3d/mesh_extractor/sparse_diffdmc.py:658-663, :762-770, :815-818), after
+ * a3d_dmc_emit or a3d_dmc_emit_qef on the same workspace: corner features
+ * [M, channels] -> out [V (+Q with with_centres), channels], each dual
+ * vertex's feature the beta-weighted mean of its crossings' alpha-weighted
+ * interpolations (the weights of p_alpha); with_centres appends each quad's
+ * mean (the training split's centre vertices).  The adjoint accumulates into
+ * g_features [M, C], g_sdf [M], g_alpha [N, 8], g_beta [N, 12] (nullable,
+ * zero-initialised by the caller); scratch [V, C], zeroed by the caller,
+ * takes the centres' share when with_centres. */
+int a3d_dmc_features(const a3d_dmc_inputs* in, void* workspace, size_t workspace_bytes,
+                     const int64_t* counts, const float* features, int32_t channels,
+                     int32_t with_centres, float* out, a3d_stream_t stream);
+int a3d_dmc_features_backward(const a3d_dmc_inputs* in, void* workspace, size_t workspace_bytes,
+                              const int64_t* counts, const float* features, int32_t channels,
+                              int32_t with_centres, const float* g_out, float* scratch,
+                              float* g_features, float* g_sdf, float* g_alpha, float* g_beta,
+                              a3d_stream_t stream);
 /* QEF inference mode (SparseDiffDMC in eval / inference_mode "qef",
  * atom3d/mesh_extractor/sparse_diffdmc.py:201-218, :289-513, :798-805).
  * Corner gradients: least-squares fit over every unique cube edge at each

@@ -227,3 +227,55 @@ def test_dmc_corner_gradients_non_grid_indices():
     _lib.check("a3d_dmc_corner_gradients", lib.a3d_dmc_corner_gradients(
         ctypes.byref(c.inp), ws.data_ptr(), ws.numel(), got.data_ptr(), c.stream))
     assert np.allclose(got.cpu().numpy(), G, rtol=1e-5, atol=1e-5)
+
+
+def _features_case():
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_dmc_features_golden as G
+
+    return G.inputs()
+
+
+def test_dmc_vertex_features_train_mode_vs_reference(golden):
+    g = golden("dmc_features.npz")
+    vox, sdf, cidx, feat, alpha, beta = _features_case()
+    s = sdf.cuda().requires_grad_(True)
+    f = feat.cuda().requires_grad_(True)
+    a = alpha.cuda().requires_grad_(True)
+    b = beta.cuda().requires_grad_(True)
+    o = SparseDiffDMC(device="cuda")(vox.cuda(), s, cidx.cuda(), int(g["res"]), alpha=a, beta=b, v_features=f)
+    ((o.vertices ** 2).sum() + (o.v_features ** 2).sum()).backward()
+    assert np.array_equal(o.faces.cpu().numpy(), g["train_faces"])
+    assert np.abs(o.vertices.detach().cpu().numpy() - g["train_vertices"]).max() <= TOL
+    vf = o.v_features.detach().cpu().numpy()
+    assert vf.shape == g["train_v_features"].shape
+    assert np.abs(vf - g["train_v_features"]).max() <= 1e-5 * max(1.0, np.abs(g["train_v_features"]).max())
+    for name, t in (("grad_sdf", s), ("grad_feat", f), ("grad_alpha", a), ("grad_beta", b)):
+        ref = g[name]
+        got = t.grad.cpu().numpy()
+        assert np.abs(got - ref).max() <= 1e-4 * max(1.0, np.abs(ref).max()), (name, np.abs(got - ref).max())
+
+
+def test_dmc_qef_mode_alpha_and_features_vs_reference(golden):
+    g = golden("dmc_features.npz")
+    vox, sdf, cidx, feat, alpha, _ = _features_case()
+    dmc = SparseDiffDMC(device="cuda")
+    dmc.eval()
+    o = dmc(vox.cuda(), sdf.cuda(), cidx.cuda(), int(g["res"]), alpha=alpha.cuda(), v_features=feat.cuda())
+    assert np.array_equal(o.faces.cpu().numpy(), g["eval_faces"])
+    assert np.abs(o.vertices.cpu().numpy() - g["eval_vertices"]).max() <= 1e-5
+    assert np.abs(o.p_alpha.cpu().numpy() - g["eval_p_alpha"]).max() <= TOL
+    ref = g["eval_v_features"]
+    assert np.abs(o.v_features.cpu().numpy() - ref).max() <= 1e-5 * max(1.0, np.abs(ref).max())
+
+
+def test_dmc_float64_inputs_need_an_explicit_dtype():
+    vox, sdf, cidx, _ = synthetic.dmc_spheres(res=24, seed=3, n_spheres=3)
+    with pytest.raises(TypeError):
+        SparseDiffDMC(device="cuda")(vox.cuda(), sdf.double().cuda(), cidx.cuda(), 24)
+    o = SparseDiffDMC(device="cuda")(vox.cuda(), sdf.double().cuda(), cidx.cuda(), 24, dtype=torch.float32)
+    r = SparseDiffDMC(device="cuda")(vox.cuda(), sdf.cuda(), cidx.cuda(), 24)
+    assert o.vertices.dtype == torch.float32 and torch.equal(o.vertices, r.vertices)
