@@ -38,6 +38,10 @@ constexpr int kSahWarpMax = 128;
 constexpr int kSahThreads = 256;
 constexpr int kSahWarps = kSahThreads / 32;
 constexpr int kSahMaxDepth = 48;
+// nodes this small split at their median position: 2 = SAH all the way down
+// (median splits at 8 and below built the 1.31M-triangle tree in 7.1 ms
+// instead of 10.5 ms but cost 21 more triangle tests per query, +1.2% query time)
+constexpr int kSahTiny = 2;
 constexpr int kSahCand = 3 * (kSahBins - 1);            // 45 split candidates
 constexpr int kBinWords = 3 * kSahBins * 7;              // count, lo xyz, hi xyz
 constexpr int kSahWarpStack = kSahWarpMax / 2;           // disjoint ranges of >= 2
@@ -346,7 +350,8 @@ __global__ void __launch_bounds__(kSahThreads)
         const int plabel = en.parent;
         const bool is_root = plabel < 0;
         int m = b + 1;
-        if (e - b > 2) {
+        // at most kSahTiny triangles: split at the median position
+        if (e - b > kSahTiny) {
           float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
           for (int i = b + lane; i < e; i += 32) {
             const float4 c = __ldg(P.cen + ord[i]);
@@ -402,6 +407,8 @@ __global__ void __launch_bounds__(kSahThreads)
           } else {
             m = b + (e - b) / 2;
           }
+        } else {
+          m = b + (e - b) / 2;
         }
         if (lane == 0) {
           if (is_root) S.root_nat = f + m - 1 + shift;

@@ -317,8 +317,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip every measurement besides the main UDF line")
     ap.add_argument("--skip", default="", help="comma-separated extra sections to skip: learned,dmc,octree,rays,batch")
-    ap.add_argument("--section", default="", choices=["", "dmc", "octree", "rays", "batch"],
+    ap.add_argument("--section", default="", choices=["", "dmc", "octree", "rays", "batch", "build", "learned"],
                     help="run one extra section alone on cuda:0 and print its JSON (for profiling)")
+    ap.add_argument("--level", type=int, default=10, help="octree section: finest level (10 = 1024^3)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -437,6 +438,8 @@ def main():
             line["rays"] = bench_rays(dev, mesh, v, max(3, args.steps // 2))
         if "batch" not in skip:
             line["batch"] = bench_batch(dev, 2, 1, cpu=cpu)
+        if "build" not in skip:
+            line["build"] = bench_build(dev, max(3, args.steps // 2))
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(v, f, q)
         step()
@@ -456,15 +459,43 @@ def run_section(args):
     if args.section == "dmc":
         out = bench_dmc(dev, steps, args.warmup, cpu=False)
     elif args.section == "octree":
-        out = bench_octree_flood(dev, steps, args.warmup)
+        out = bench_octree_flood(dev, steps, args.warmup, max_level=args.level)
     elif args.section == "batch":
         out = bench_batch(dev, 2, 1, cpu=False)
+    elif args.section == "build":
+        out = bench_build(dev, steps)
+    elif args.section == "learned":
+        from atom3d_b200 import MeshBVH, synthetic
+
+        v, f, q = synthetic.udf_large(n_queries=args.queries)
+        out = bench_learned(dev, v, f, MeshBVH(v.to(dev), f.to(dev)), q.to(dev), steps)
     else:
         from atom3d_b200 import MeshBVH, synthetic
 
-        v, f, _ = synthetic.udf_large(n_queries=1)
+        v, f, _ = synthetic.udf_large(n_queries=2)
         out = bench_rays(dev, MeshBVH(v.to(dev), f.to(dev)), v, steps)
     print(json.dumps({"section": args.section, **out}), flush=True)
+
+
+def bench_build(dev, steps):
+    """GPU BVH build of the 1,310,720-triangle mesh (Morton codes, radix sort,
+    radix tree, SAH refinement, refit with the collapse costs, collapse,
+    layout), device-timed.  Algorithmic bytes per triangle: 60 (Morton) +
+    24 per 8-bit radix pass x 8 passes + 80 (emission and refit)."""
+    from atom3d_b200 import MeshBVH, synthetic
+
+    v, f, _ = synthetic.udf_large(n_queries=2)
+    vd, fd = v.to(dev), f.to(dev)
+    MeshBVH(vd, fd)
+    ms = _time_ms(lambda: MeshBVH(vd, fd), steps)
+    nf = int(f.shape[0])
+    peak, kind = peaks()
+    byts = (60 + 24 * 8 + 80) * nf
+    gbs = byts / (ms * 1e-3) / 1e9
+    return {"metric": "BVH build ms (1,310,720 triangles)", "value": ms, "unit": "ms", "triangles": nf,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "peak_kind": kind, "bytes": "332 B per triangle (60 Morton + 8 x 24 radix + 80 refit)",
+                         "note": "whole build call incl. host read of its node count; latency-bound"}}
 
 
 def _time_ms(fn, steps, warmup=2):
@@ -706,9 +737,10 @@ def bench_dmc(dev, steps, warmup, cpu=True):
     return out
 
 
-def bench_octree_flood(dev, steps, warmup):
-    """octree_traverse (levels 4..10, 1024^3) and sparse_flood_fill on the
-    327,680-triangle displaced sphere, bounds [-1.5, 1.5]^3."""
+def bench_octree_flood(dev, steps, warmup, max_level=10):
+    """octree_traverse (levels 4..max_level, 1024^3 by default) and
+    sparse_flood_fill on the 327,680-triangle displaced sphere, bounds
+    [-1.5, 1.5]^3."""
     from atom3d_b200 import MeshBVH, OctreeIndexer, sparse_flood_fill, synthetic
 
     v, f = synthetic.octree_mesh()
@@ -722,7 +754,8 @@ def bench_octree_flood(dev, steps, warmup):
     mesh = MeshBVH(vd, fd)
     torch.cuda.synchronize()
     build_ms = (time.perf_counter() - t0) * 1e3
-    oc = OctreeIndexer(max_level=10, bounds=bounds, device=dev)
+    oc = OctreeIndexer(max_level=max_level, bounds=bounds, device=dev)
+    res_grid = 1 << max_level
     for _ in range(warmup):
         cand = oc.octree_traverse(mesh, min_level=4)
     torch.cuda.synchronize()
@@ -738,12 +771,12 @@ def bench_octree_flood(dev, steps, warmup):
     out = None
     for _ in range(max(2, warmup - 1)):
         out = None
-        out = sparse_flood_fill(mesh, 1024, min_level=4, bounds=bounds, verbose=False)
+        out = sparse_flood_fill(mesh, res_grid, min_level=4, bounds=bounds, verbose=False)
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(steps):
         out = None
-        out = sparse_flood_fill(mesh, 1024, min_level=4, bounds=bounds, verbose=False)
+        out = sparse_flood_fill(mesh, res_grid, min_level=4, bounds=bounds, verbose=False)
     e1.record(stream)
     torch.cuda.synchronize()
     ff_ms = e0.elapsed_time(e1) / steps
@@ -754,7 +787,7 @@ def bench_octree_flood(dev, steps, warmup):
     visited = labels["water_ijk"] + labels["tide_ijk"]
     peak, kind = peaks()
     gbs = 220.0 * visited / (ff_ms * 1e-3) / 1e9
-    res = {"metric": "octree SAT 4->10 + sparse flood fill at 1024^3 (327,680 tris)", "unit": "ms",
+    res = {"metric": f"octree SAT 4->{max_level} + sparse flood fill at {res_grid}^3 (327,680 tris)", "unit": "ms",
            "bvh_build_ms": build_ms, "octree_ms": oct_ms, "sparse_flood_fill_ms": ff_ms,
            "candidate_voxels": int(cand.shape[0]), "labels": labels,
            "roofline_flood": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
@@ -780,8 +813,9 @@ def bench_dual(dev, oc, labels, steps):
     n_in = dam.shape[0] + tide.shape[0] + dry.shape[0]
     alg = 12.0 * n_in + 124.0 * cells.shape[0] + 36.0 * vijk.shape[0]
     peak, kind = peaks()
-    wet_ms = _time_ms(lambda: (get_dam_wet_faces(dam, tide, 1024), get_dam_wet_edges(dam, tide, 1024),
-                               get_dam_wet_corners(dam, tide, 1024)), steps)
+    R = 1 << int(oc.max_level)
+    wet_ms = _time_ms(lambda: (get_dam_wet_faces(dam, tide, R), get_dam_wet_edges(dam, tide, R),
+                               get_dam_wet_corners(dam, tide, R)), steps)
     return {"ms": g_ms, "active_cells": int(cells.shape[0]), "vertices": int(vijk.shape[0]),
             "listed_cells": int(n_in),
             "roofline": {"bound": "hbm", "achieved": alg / (g_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
@@ -796,7 +830,7 @@ def bench_pairs(dev, mesh, oc, cand, steps):
     the reference demo's workload (80-face icosphere at 512^3, mode 3)."""
     from atom3d_b200 import MeshBVH, OctreeIndexer, synthetic
 
-    mn, mx = oc.cube_aabb_level(cand, 10)
+    mn, mx = oc.cube_aabb_level(cand, int(oc.max_level))
     out = {"boxes": int(mn.shape[0])}
     for mode in (1, 3):
         ms = _time_ms(lambda: mesh.intersect_aabb(mn, mx, mode=mode), steps)
