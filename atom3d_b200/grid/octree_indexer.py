@@ -1,5 +1,7 @@
 """OctreeIndexer: multi-level cube grid with the coarse-to-fine SAT descent
-(drop-in for atom3d/grid/octree_indexer.py:17-509).
+(drop-in for atom3d/grid/octree_indexer.py:17-509 except three Python-loop
+helpers that are not ported: expand_nodes (:371-420), mark_active_nodes and
+get_node_neighbors, none of them on the descent's path).
 
 ``octree_traverse`` runs the whole descent in one native call
 (a3d_octree_traverse): per level, one SAT any-hit query per candidate cube

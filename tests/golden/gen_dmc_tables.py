@@ -8,11 +8,11 @@ table; the tetrahedra table kept for state-dict compatibility).  They are
 data, not code: this script reads them from a reference checkout once and
 writes two compact encodings:
 
-  ../csrc/dmc_tables.inc   int8 C arrays for the CUDA kernels
-  dmc_tables.py            hex strings decoded into torch tensors
+  atom3d_b200/csrc/dmc_tables.inc            int8 C arrays for the CUDA kernels
+  atom3d_b200/mesh_extractor/dmc_tables.py   hex strings decoded into torch tensors
 
-Usage: python -m atom3d_b200.mesh_extractor.gen_tables <path to the
-reference's atom3d/mesh_extractor/tables.py>
+Usage: python tests/golden/gen_dmc_tables.py <path to the reference's
+atom3d/mesh_extractor/tables.py>
 """
 
 from __future__ import annotations
@@ -23,7 +23,8 @@ import sys
 
 import numpy as np
 
-HERE = os.path.dirname(os.path.abspath(__file__))
+HERE = os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))), "atom3d_b200",
+                    "mesh_extractor")
 
 
 def load(path: str) -> dict:
@@ -41,7 +42,7 @@ def main(path: str) -> None:
     for k, s in shapes.items():
         assert t[k].shape == s, (k, t[k].shape)
     # check_table's last column holds a case id (0..255): store it as uint8
-    lines = ["// Generated by atom3d_b200/mesh_extractor/gen_tables.py -- DMC lookup tables.", "#pragma once", ""]
+    lines = ["// Generated by tests/golden/gen_dmc_tables.py -- DMC lookup tables.", "#pragma once", ""]
     # Threads of one warp index these tables with different case ids, so they
     # live in global memory (cached loads) rather than constant memory (one
     # serialised access per distinct address).
@@ -67,7 +68,7 @@ def main(path: str) -> None:
     lines.append("};")
     with open(os.path.join(HERE, "..", "csrc", "dmc_tables.inc"), "w") as f:
         f.write("\n".join(lines) + "\n")
-    py = ['"""DMC lookup tables (generated by gen_tables.py; hex-encoded int16 data)."""', "",
+    py = ['"""DMC lookup tables (generated by tests/golden/gen_dmc_tables.py; hex-encoded int16 data)."""', "",
           "import numpy as np", "", "_SHAPES = " + repr(shapes), "", "_HEX = {"]
     for k in shapes:
         py.append(f"    {k!r}: {t[k].astype('<i2').tobytes().hex()!r},")

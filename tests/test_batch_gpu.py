@@ -118,7 +118,7 @@ def test_graph_replay_and_tuned_shapes_give_identical_results():
         assert torch.equal(d2, dist) and torch.equal(f2, fid) and torch.equal(c2, cp)
 
 
-def test_more_queries_than_one_launch():
+def test_more_queries_than_one_launch(orc):
     # two launches of the traversal (the second one partial), queries of one
     # mesh split between them
     v, f = synthetic.displaced_sphere(3, 8, 0.05, 7)
@@ -133,7 +133,15 @@ def test_more_queries_than_one_launch():
     for vm, q, sl in ((v, q1, slice(0, n1)), (v2, q2, slice(n1, n1 + n2))):
         ref = MeshBVH(vm.cuda(), f.cuda()).udf(q, return_face_ids=True)
         assert torch.equal(dist[sl], ref.distances)
-        assert float((fid[sl].long() != ref.face_ids.long()).float().mean()) < 0.01
+        # face ids equal, or tied: both faces at the same FP64 distance within
+        # 1e-6 of the box diagonal (the batched tree differs from the single one)
+        diff = torch.nonzero(fid[sl].long() != ref.face_ids.long()).flatten()
+        if diff.numel():
+            qd = q[diff].cpu().numpy()
+            a = orc.tri_dist(vm.numpy(), f.numpy(), qd, fid[sl][diff].cpu().numpy())
+            b = orc.tri_dist(vm.numpy(), f.numpy(), qd, ref.face_ids[diff].cpu().numpy())
+            diag = float((vm.double().max(0).values - vm.double().min(0).values).norm())
+            assert np.abs(a - b).max() <= 1e-6 * diag, (diff.numel(), np.abs(a - b).max())
 
 
 def test_bad_face_index_is_reported():

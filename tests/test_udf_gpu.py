@@ -197,7 +197,8 @@ def test_udf_grad_points_and_vertices_fd(orc):
     (d * w).sum().backward()
     gp = p.grad.cpu().double().numpy()
     gv = vv.grad.cpu().double().numpy()
-    # FP64 central differences of sum_i w_i * dist_i through the oracle
+    # FP64 central differences of sum_i w_i * dist_i through the oracle (with
+    # h = 1e-3 they agree with the analytic FP64 gradient to 2e-5 here)
     V = v.double().numpy()
     Fn = f.numpy()
     Q = q.double().numpy()
@@ -214,7 +215,7 @@ def test_udf_grad_points_and_vertices_fd(orc):
             Qp[i, a] += h
             Qm[i, a] -= h
             fd = (energy(V, Qp) - energy(V, Qm)) / (2 * h)
-            assert abs(fd - gp[i, a]) < 2e-2 * max(1.0, abs(fd)), (i, a, fd, gp[i, a])
+            assert abs(fd - gp[i, a]) < 1e-3 * max(1.0, abs(fd)), (i, a, fd, gp[i, a])
     touched = np.argsort(-np.abs(gv).sum(1))[:6]
     for vi in touched:
         for a in range(3):
@@ -222,7 +223,7 @@ def test_udf_grad_points_and_vertices_fd(orc):
             Vp[vi, a] += h
             Vm[vi, a] -= h
             fd = (energy(Vp, Q) - energy(Vm, Q)) / (2 * h)
-            assert abs(fd - gv[vi, a]) < 3e-2 * max(1.0, abs(fd)), (vi, a, fd, gv[vi, a])
+            assert abs(fd - gv[vi, a]) < 2e-3 * max(1.0, abs(fd)), (vi, a, fd, gv[vi, a])
 
 
 def test_cpu_device_raises():
