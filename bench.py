@@ -42,9 +42,9 @@ sys.path.insert(0, HERE)
 
 METRIC = "UDF Mqueries/s (plain traversal, 1.31M-triangle mesh, 16M queries)"
 # DRAM read + write of one udf_task_kernel launch per query, measured by an
-# ncu capture of a 4,194,304-query launch on this mesh (1.508 GB); traffic
+# ncu capture of a 4,194,304-query launch on this mesh (1.471 GB); traffic
 # scales with the query count (the tree stays in L2)
-DRAM_BYTES_PER_QUERY = 1.507714e9 / 4194304
+DRAM_BYTES_PER_QUERY = 1.471343e9 / 4194304
 TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, 4,194,304-query capture scaled per query"
 UNIT = "Mqueries/s"
 WORKLOAD = "udf_large: icosphere L8 (1,310,720 tris) + 16 sinusoids, 16,777,216 mixed queries"
