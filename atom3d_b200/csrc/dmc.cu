@@ -73,6 +73,27 @@ __device__ __forceinline__ float norm_w(float v, float ws, bool given) {
   return given ? fa(fm(tanhf(v), ws), 1.0f) : 1.0f;
 }
 
+// World position of local corner c of a cube whose voxel coordinates are
+// vx (corner id gid): the reference's grid -> world map,
+// (voxel + corner offset) * 2/res - 1, then + deform
+// (atom3d/mesh_extractor/sparse_diffdmc.py:151-168)
+__device__ __forceinline__ void corner_world(const DmcIn& in, float ws, const float* vx, int c, int64_t gid, float* p) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float v = fsb(fm(fa(vx[a], (float)((c >> a) & 1)), ws), 1.0f);
+    if (in.deform) v = fa(v, __ldg(in.deform + 3 * gid + a));
+    p[a] = v;
+  }
+}
+
+__device__ __forceinline__ void load_voxel(const DmcIn& in, int64_t cube, float* vx) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) vx[a] = (float)__ldg(in.vox + 3 * cube + a);
+}
+
+__device__ __forceinline__ float world_scale(const DmcIn& in) { return (float)(2.0 / (double)in.res); }
+inline float world_scale_host(int res) { return (float)(2.0 / (double)res); }
+
 // ---- stage A ---------------------------------------------------------------
 // also clears the word corner_case_kernel flags out-of-range corner ids in
 // (when given)
@@ -105,28 +126,21 @@ __global__ void corner_pos_kernel(DmcIn in, float ws, float* __restrict__ x) {
   }
 }
 
-// corner positions and case ids in one pass over cube_idx: thread (cube,
-// corner) writes its corner's position and its sign bit; the 8 lanes of a
-// cube (aligned groups of 8) OR their bits into the case id
-__global__ void corner_case_kernel(DmcIn in, float ws, float* __restrict__ x, uint8_t* __restrict__ cases,
-                                   uint32_t* __restrict__ flag, uint32_t* __restrict__ bad_index) {
+// case ids in one pass over cube_idx: thread (cube, corner) takes its
+// corner's sign bit; the 8 lanes of a cube (aligned groups of 8) OR their
+// bits into the case id.  Corner positions are not materialised: the kernels
+// that need them compute them from the cube (corner_world).
+__global__ void corner_case_kernel(DmcIn in, uint8_t* __restrict__ cases, uint32_t* __restrict__ flag,
+                                   uint32_t* __restrict__ bad_index) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = t < in.n * 8;
   const int c = (int)(t & 7);
   uint32_t bit = 0;
   if (valid) {
-    const int64_t i = t >> 3;
-    if ((uint64_t)in.cidx[t] >= (uint64_t)in.m) *bad_index = 1u;
-    const int64_t mi = corner_at(in, t);
-    const int off[3] = {c & 1, (c >> 1) & 1, (c >> 2) & 1};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float g = fa((float)in.vox[3 * i + a], (float)off[a]);
-      float v = fsb(fm(g, ws), 1.0f);
-      if (in.deform) v = fa(v, in.deform[3 * mi + a]);
-      x[3 * mi + a] = v;
-    }
-    bit = (fsb(in.sdf[mi], in.iso) < 0.f ? 1u : 0u) << c;
+    const int64_t v = in.cidx[t];
+    if ((uint64_t)v >= (uint64_t)in.m) *bad_index = 1u;
+    const int64_t mi = (uint64_t)v < (uint64_t)in.m ? v : 0;
+    bit = (fsb(__ldg(in.sdf + mi), in.iso) < 0.f ? 1u : 0u) << c;
   }
   bit |= __shfl_xor_sync(0xffffffffu, bit, 1);
   bit |= __shfl_xor_sync(0xffffffffu, bit, 2);
@@ -211,23 +225,34 @@ __device__ __forceinline__ void edge_ends(const DmcIn& in, uint32_t cube, int e,
   i1 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e + 1]);
 }
 
+// positions of the ends of cube edge e of a cube at voxel vx.  A unique
+// edge's corner ids (i0, i1) come from the key (cube_idx[c0], cube_idx[c1])
+// of the cube's own local corners c0 = kCE[2e], c1 = kCE[2e+1] (a cube whose
+// ids run the other way along the edge makes a different key), so i0 is
+// always local corner c0 here
+__device__ __forceinline__ void edge_world(const DmcIn& in, float ws, const float* vx, int e, int64_t i0, int64_t i1,
+                                           float* xa, float* xb) {
+  corner_world(in, ws, vx, kCE[2 * e], i0, xa);
+  corner_world(in, ws, vx, kCE[2 * e + 1], i1, xb);
+}
+
+// crossing edges of each surface cube from its sign bits (the raw case id:
+// an edge crosses when its two corners' bits differ, the test the case id
+// was made with)
 __global__ void cross_count_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
-                                   uint16_t* __restrict__ mask12, uint32_t* __restrict__ cnt) {
+                                   const uint8_t* __restrict__ cases, uint16_t* __restrict__ mask12,
+                                   uint32_t* __restrict__ cnt) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= in.n) return;
   if (t >= (int64_t)*ns_dev) {  // the scan runs over all N entries
     cnt[t] = 0;
     return;
   }
-  const uint32_t i = list[t];
+  const uint32_t c = cases[list[t]];
   uint32_t m = 0;
 #pragma unroll
-  for (int e = 0; e < 12; ++e) {
-    int64_t i0, i1;
-    edge_ends(in, i, e, i0, i1);
-    const bool n0 = fsb(in.sdf[i0], in.iso) < 0.f, n1 = fsb(in.sdf[i1], in.iso) < 0.f;
-    if (n0 != n1) m |= 1u << e;
-  }
+  for (int e = 0; e < 12; ++e)
+    if (((c >> kCE[2 * e]) ^ (c >> kCE[2 * e + 1])) & 1u) m |= 1u << e;
   mask12[t] = (uint16_t)m;
   cnt[t] = (uint32_t)__popc(m);
 }
@@ -413,7 +438,7 @@ __device__ __forceinline__ float ldf(const float* p, int64_t i) { return __ldg(p
 // one thread per dual vertex: crossings, weighted average, L_dev.  The edge
 // loop is unrolled over the 7 table slots, so each edge's plain crossing
 // and distance stay in registers for the L_dev pass (one gather per edge).
-__global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, const uint32_t* __restrict__ list,
+__global__ void vd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
                           const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
                           const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
                           VdOut out) {
@@ -424,6 +449,9 @@ __global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, con
   const int c = case_s[t];
   const uint32_t vedges = vd_edges(c, j);
   const uint32_t cube = list[t];
+  const float ws = world_scale(in);
+  float vx[3];
+  load_voxel(in, cube, vx);
   const int64_t g0 = goff[v];
   float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
   float z[7][3];
@@ -443,8 +471,7 @@ __global__ void vd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, con
     const float den = fa(w0, w1);
     const float pw0 = s1, pw1 = -s0, pden = fa(pw0, pw1);
     float xa[3], xb[3], n[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) { xa[a] = ldf(x, 3 * i0 + a); xb[a] = ldf(x, 3 * i1 + a); }
+    edge_world(in, ws, vx, e, i0, i1, xa, xb);
     edge_normal(xa, xb, s0, s1, n);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -557,7 +584,7 @@ __device__ __forceinline__ void scatter_interp_grad(const DmcIn& in, const float
   }
 }
 
-__global__ void vd_bwd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv, const uint32_t* __restrict__ list,
+__global__ void vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
                               const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
                               const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
                               DmcGrad gr) {
@@ -568,6 +595,9 @@ __global__ void vd_bwd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv,
   const int c = case_s[t];
   const uint32_t vedges = vd_edges(c, j);
   const uint32_t cube = list[t];
+  const float ws = world_scale(in);
+  float vx[3];
+  load_voxel(in, cube, vx);
   const int64_t g0 = goff[v];
   // recompute the forward quantities of this dual vertex
   int64_t I0[7], I1[7];
@@ -586,8 +616,10 @@ __global__ void vd_bwd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv,
     A[ne][1] = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
     B[ne] = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
     const float w0 = fm(S[ne][1], A[ne][1]), w1 = -fm(S[ne][0], A[ne][0]), den = fa(w0, w1);
+    float pa[3], pb[3];
+    edge_world(in, ws, vx, e, i0, i1, pa, pb);
     for (int a = 0; a < 3; ++a) {
-      UE[ne][a] = interp1(x[3 * i0 + a], x[3 * i1 + a], w0, w1, den);
+      UE[ne][a] = interp1(pa[a], pb[a], w0, w1, den);
       acc[a] = fa(acc[a], fm(UE[ne][a], B[ne]));
     }
     bsum = fa(bsum, B[ne]);
@@ -606,8 +638,10 @@ __global__ void vd_bwd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv,
   for (int q = 0; q < ne; ++q) {
     const float w0 = S[q][1], w1 = -S[q][0], dn = fa(w0, w1);
     float d2 = 0.f;
+    float pa[3], pb[3];
+    edge_world(in, ws, vx, E[q], I0[q], I1[q], pa, pb);
     for (int a = 0; a < 3; ++a) {
-      Z[q][a] = interp1(x[3 * I0[q] + a], x[3 * I1[q] + a], w0, w1, dn);
+      Z[q][a] = interp1(pa[a], pb[a], w0, w1, dn);
       const float dd = fsb(Z[q][a], vd[a]);
       d2 = fa(d2, fm(dd, dd));
     }
@@ -653,7 +687,7 @@ __global__ void vd_bwd_kernel(DmcIn in, const float* __restrict__ x, int64_t nv,
       gb += gvd[a] * UE[q][a] * inv_bden;
     }
     float xa[3], xb[3];
-    for (int a = 0; a < 3; ++a) { xa[a] = x[3 * i0 + a]; xb[a] = x[3 * i1 + a]; }
+    edge_world(in, ws, vx, e, i0, i1, xa, xb);
     // ue through w0 = s1 a1, w1 = -s0 a0
     {
       const float w0 = S[q][1] * A[q][1], w1 = -(S[q][0] * A[q][0]), den = w0 + w1;
@@ -994,13 +1028,11 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   for (int k = 0; k < 6; ++k) counts[k] = 0;
   if (n == 0 || m == 0) return A3D_OK;
   DmcIn in = make_in(p);
-  const float wsc = (float)(2.0 / (double)p->resolution);
   // misc[1]: out-of-range corner ids; misc[4..6] and misc[8..14]: the words
   // the two host reads take
   uint32_t* bad_index = w.misc + 1;
-  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x, bad_index);
-  A3D_LAUNCH_CHECK();
-  corner_case_kernel<<<gsz(8 * n), 256, 0, s>>>(in, wsc, w.x, w.cases, w.flag, bad_index);
+  A3D_CUDA_TRY(cudaMemsetAsync(bad_index, 0, sizeof(uint32_t), s));
+  corner_case_kernel<<<gsz(8 * n), 256, 0, s>>>(in, w.cases, w.flag, bad_index);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flag, w.off, n, w.scan_tmp, w.off + n, s)));
   // stage B over all N cubes with the surface count on the device
@@ -1012,7 +1044,7 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   A3D_LAUNCH_CHECK();
   case_fix_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.cases, w.table, w.table_mask, w.case_s);
   A3D_LAUNCH_CHECK();
-  cross_count_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.mask12, w.ccnt);
+  cross_count_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.cases, w.mask12, w.ccnt);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ccnt, w.coff, n, w.scan_tmp, w.coff + n, s)));
   cross_write_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.mask12, w.coff, w.keys, w.vals);
@@ -1044,7 +1076,6 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.rflag, w.rid, nc, w.scan_tmp, w.misc, s)));
   A3D_CUDA_TRY(cudaMemsetAsync(w.idx_map, 0xff, 12 * ns * sizeof(int32_t), s));
-  A3D_CUDA_TRY(cudaMemsetAsync(w.vd_map, 0, 12 * ns * sizeof(int32_t), s));
   run_info_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, w.vals, nc, w.rflag, w.rid, m, w.idx_map, w.e0, w.e1, w.rfirst);
   A3D_LAUNCH_CHECK();
   quad_flag_kernel<<<gsz(nc), 256, 0, s>>>(w.misc, nc, w.rfirst, w.qflag);
@@ -1097,7 +1128,7 @@ extern "C" int a3d_dmc_emit(const a3d_dmc_inputs* p, void* workspace, size_t wor
   DmcIn in = make_in(p);
   EdgeData ed{w.e0, w.e1, w.idx_map};
   VdOut out{vertices, l_dev, p_alpha, n_alpha, w.vd_map};
-  vd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, w.x, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, out);
+  vd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, out);
   A3D_LAUNCH_CHECK();
   (void)nc;
   if (nq > 0) {
@@ -1129,7 +1160,7 @@ extern "C" int a3d_dmc_backward(const a3d_dmc_inputs* p, void* workspace, size_t
     A3D_LAUNCH_CHECK();
   }
   EdgeData ed{w.e0, w.e1, w.idx_map};
-  vd_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, w.x, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, gr);
+  vd_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, gr);
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
@@ -1624,6 +1655,11 @@ extern "C" int a3d_dmc_emit_qef(const a3d_dmc_inputs* p, void* workspace, size_t
   DmcIn in = make_in(p);
   EdgeData ed{w.e0, w.e1, w.idx_map};
   VdOut out{vertices, l_dev, p_alpha, n_alpha, w.vd_map};
+  // corner world positions (the training path computes them per edge)
+  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x, nullptr);
+  A3D_LAUNCH_CHECK();
+  corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, world_scale_host(p->resolution), w.x);
+  A3D_LAUNCH_CHECK();
   vd_qef_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, w.x, corner_gradients, qef_reg_scale, nv, w.list, w.case_s,
                                              w.vd_cube, w.vd_slot, w.goff, ed, out);
   A3D_LAUNCH_CHECK();

@@ -685,7 +685,6 @@ def bench_dmc(dev, steps, warmup, cpu=True):
     vox, sdf, cidx, _ = synthetic.dmc_spheres(res=512)
     vd, sd, cd = vox.to(dev), sdf.to(dev), cidx.to(dev)
     dmc = SparseDiffDMC(device=str(dev))
-    stream = torch.cuda.current_stream(dev)
 
     def fwd_bwd():
         s_ = sd.detach().requires_grad_(True)
@@ -693,29 +692,19 @@ def bench_dmc(dev, steps, warmup, cpu=True):
         (o.vertices ** 2).sum().backward()
         return o
 
-    for _ in range(warmup):
-        o = fwd_bwd()
-    torch.cuda.synchronize()
-    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-    fwd_ms = bwd_ms = 0.0
-    tot = 0.0
-    for _ in range(steps):
-        s_ = sd.detach().requires_grad_(True)
-        e0.record(stream)
-        o = dmc(vd, s_, cd, 512)
-        e1.record(stream)
-        (o.vertices ** 2).sum().backward()
-        e2.record(stream)
-        torch.cuda.synchronize()
-        fwd_ms += e0.elapsed_time(e1)
-        bwd_ms += e1.elapsed_time(e2)
-        tot += e0.elapsed_time(e2)
+    def fwd_only():
+        return dmc(vd, sd.detach().requires_grad_(True), cd, 512)
+
+    # steps back to back between two events on the stream (the forward's two
+    # host reads of counts stay inside each step); backward = the difference
+    o = fwd_bwd()
+    tot = _time_ms(fwd_bwd, steps, warmup)
+    fwd = _time_ms(fwd_only, steps, warmup)
     n_cubes, n_v, n_f = vox.shape[0], o.vertices.shape[0], o.faces.shape[0]
     peak, kind = peaks()
-    fwd = fwd_ms / steps
     alg = 108.0 * n_cubes + 12.0 * n_v + 24.0 * n_f
-    out = {"metric": "DMC fwd+bwd ms (32-sphere SDF, 512^3, 2.2M active cubes)", "value": tot / steps, "unit": "ms",
-           "higher_is_better": False, "fwd_ms": fwd, "bwd_ms": bwd_ms / steps, "active_cubes": int(n_cubes),
+    out = {"metric": "DMC fwd+bwd ms (32-sphere SDF, 512^3, 2.2M active cubes)", "value": tot, "unit": "ms",
+           "higher_is_better": False, "fwd_ms": fwd, "bwd_ms": tot - fwd, "active_cubes": int(n_cubes),
            "vertices": int(n_v), "faces": int(n_f),
            "roofline_fwd": {"bound": "hbm", "achieved": alg / (fwd * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                             "frac": alg / (fwd * 1e-3) / 1e9 / peak, "peak_kind": kind,
