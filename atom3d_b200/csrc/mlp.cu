@@ -1,21 +1,24 @@
 // Learned distance bound: a Fourier-feature MLP (3 -> 64 Fourier features
-// -> 128 -> 128 -> 128 -> 1, ReLU) evaluated and trained with hand-written
-// BF16 tensor-core kernels (mma.sync m16n8k16, FP32 accumulation).
+// -> 128 -> 128 -> 128 -> 1, ReLU) with BF16 operands and FP32
+// accumulation: inference on the tcgen05 tensor cores (accumulators in
+// tensor memory), training with mma.sync GEMM kernels.
 //
 // No counterpart in the reference.  The network predicts the unsigned
-// distance of a query; a calibrated margin turns the prediction into a
-// per-query upper bound that seeds the closest-point traversal's pruning
-// radius (a3d_udf's `bound` argument).  The traversal re-runs any query
-// whose bound proves too small, so results never depend on the network.
+// distance of a query (or its logarithm); a calibrated scale and margin turn
+// the prediction into a per-query upper bound that seeds the closest-point
+// traversal's pruning radius (a3d_udf's `bound` argument).  The traversal
+// re-runs any query whose bound proves too small, so results never depend
+// on the network.
 //
 // Kernels:
-//   mlp_bound_kernel   fused inference: features, three hidden layers and
-//                      the head for 128 queries per CTA, weights and
-//                      activations in shared memory
-//   gemm_bf16_kernel   C = op(A) op(B) (+bias)(relu)(mask) for training,
-//                      arbitrary strides, 64x64 tiles, 4 warps
-//   small kernels      Fourier features, head forward/backward, column
-//                      sums, Adam
+//   mlp_bound_tc_kernel  fused inference: Fourier features, three hidden
+//                        layers as tcgen05.mma (M = 128 queries, N = 128,
+//                        K = 16 per instruction, weights staged once per
+//                        CTA), epilogues from tensor memory, head
+//   gemm_bf16_kernel     C = op(A) op(B) (+bias)(relu)(mask) for training,
+//                        arbitrary strides, 64x64 tiles, 4 warps
+//   small kernels        Fourier features, head forward/backward, column
+//                        sums, Adam
 #include <math.h>
 
 #include <algorithm>
@@ -221,21 +224,36 @@ __global__ void f32_to_bf16_kernel(const float* __restrict__ in, int64_t n, __nv
 }
 
 // ---------------------------------------------------------------------------
-// fused inference
+// fused inference on the fifth-generation tensor cores (tcgen05 + TMEM)
 // ---------------------------------------------------------------------------
-constexpr int kInfWarps = 4;
-constexpr int kRowsPerWarp = 32;
-constexpr int kRows = kInfWarps * kRowsPerWarp;  // 128 queries per CTA
-constexpr int kLd1 = kIn + 8;                    // padded row strides (bf16)
-constexpr int kLdH = kHid + 8;
+// One CTA per SM, four warpgroups.  The three hidden-layer weight matrices
+// are staged once per CTA in shared memory (W^T, K-major, 128-B swizzle:
+// 80 KB); each warpgroup owns a tile of 128 queries at a time: its threads
+// write the tile's Fourier features (one query row per thread) into the
+// group's A operand, one thread issues the layer's tcgen05.mma.kind::f16
+// (M = 128 queries, N = 128 outputs, K = 16 per instruction) into the
+// group's 128 TMEM columns and commits to the group's mbarrier; the 128
+// threads then read their own row back with tcgen05.ld (warp w of the group
+// owns TMEM lanes 32w..32w+31), add the bias, apply ReLU, round to bf16 and
+// write the next layer's A operand in place.  The last layer folds into the
+// head dot product in registers.  The groups run independently (named
+// barriers), so one group's MMAs overlap another group's epilogue.
+constexpr int kTcGroups = 4;
+constexpr int kTcThreads = kTcGroups * 128;
+constexpr int kTcRows = 128;                   // queries per tile (MMA M)
+constexpr uint32_t kAtom = kTcRows * 128u;     // 128 rows x 128 B: one swizzle column of K = 64 bf16
+constexpr uint32_t kTmemCols = 512;            // 4 groups x 128 fp32 columns
+constexpr uint32_t kWaitLimit = 1u << 22;      // mbarrier polls before a group gives up
 
-struct InfSmem {
-  __nv_bfloat16 w1t[kHid][kLd1];   // W1 transposed: [out][in]
-  __nv_bfloat16 w2t[kHid][kLdH];
-  __nv_bfloat16 w3t[kHid][kLdH];
+struct TcSmem {  // placed at a 1024-B aligned address (the 128-B swizzle repeats every 1 KB)
+  uint8_t w1[kAtom];                  // W1^T: N = 128, K = 64
+  uint8_t w2[2 * kAtom];              // W2^T: K = 128 as two 64-wide columns
+  uint8_t w3[2 * kAtom];
+  uint8_t act[kTcGroups][2 * kAtom];  // per-group A operand (features, then hidden activations)
   float b1[kHid], b2[kHid], b3[kHid], w4[kHid];
   float freq[kIn / 2 * 3];
-  __nv_bfloat16 act[kInfWarps][2][kRowsPerWarp][kLdH];  // ping-pong activations per warp
+  unsigned long long mbar[kTcGroups];
+  uint32_t tmem_base;
 };
 
 struct InfParams {
@@ -249,122 +267,243 @@ struct InfParams {
   float b4;
   const float* freq;  // [32][3]
   Normalise nz;
-  float scale, margin;  // bound = max(y, 0) * scale + margin
+  float scale, margin;  // bound = max(y, 0) * scale + margin, or exp(y) * scale + margin
+  int log_space;        // the network predicts log(distance)
 };
 
-// one warp: out[32 x 128] = relu(in[32 x K] W + b), written as bf16 to `out`
-// (or, for the last layer, folded into the head dot product)
-template <int K, int LDA, int LDW>
-__device__ __forceinline__ void warp_layer(const __nv_bfloat16 (*in)[kLdH], const __nv_bfloat16 (*w)[LDW],
-                                           const float* b, __nv_bfloat16 (*out)[kLdH], const float* w4,
-                                           float* head_rows, int lane) {
-  const int gid = lane >> 2, tig = lane & 3;
-  const __nv_bfloat16* inb = &in[0][0];
+// byte offset of 16-B chunk c (0..7) of row r inside one K-major 128-B
+// swizzle column: 8-row groups 1 KB apart, rows 128 B apart, the chunk index
+// XORed with the row's position in its 8-row group
+__device__ __forceinline__ uint32_t sw128(uint32_t r, uint32_t c) {
+  return (r >> 3) * 1024u + (r & 7u) * 128u + ((c ^ (r & 7u)) << 4);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// shared-memory matrix descriptor: K-major, 128-B swizzle, 8-row groups
+// 1024 B apart (stride byte offset), leading byte offset unused (1),
+// descriptor version 1
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) |
+         ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
+}
+
+// instruction descriptor: BF16 x BF16 -> FP32, A and B K-major, M = 128, N = 128
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(128) : "memory");
+}
+
+// AND of a predicate over the 128 threads of warpgroup g (a named barrier)
+__device__ __forceinline__ bool group_all(int g, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.and.pred p, %2, %3, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(1 + g), "r"(128)
+      : "memory");
+  return r != 0;
+}
+
+// bounded wait for the mbarrier phase with the given parity; false when the
+// poll limit ran out
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// 32 consecutive fp32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int half = 0; half < 2; ++half) {
-    float acc[2][8][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 8; ++j)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
-#pragma unroll
-    for (int k0 = 0; k0 < K; k0 += 16) {
-      uint32_t a[2][4];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int r = i * 16 + gid;
-        a[i][0] = *reinterpret_cast<const uint32_t*>(inb + r * LDA + k0 + 2 * tig);
-        a[i][1] = *reinterpret_cast<const uint32_t*>(inb + (r + 8) * LDA + k0 + 2 * tig);
-        a[i][2] = *reinterpret_cast<const uint32_t*>(inb + r * LDA + k0 + 2 * tig + 8);
-        a[i][3] = *reinterpret_cast<const uint32_t*>(inb + (r + 8) * LDA + k0 + 2 * tig + 8);
-      }
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int c = half * 64 + j * 8 + gid;
-        uint32_t bb[2];
-        bb[0] = *reinterpret_cast<const uint32_t*>(&w[c][k0 + 2 * tig]);
-        bb[1] = *reinterpret_cast<const uint32_t*>(&w[c][k0 + 2 * tig + 8]);
-        mma_bf16(acc[0][j], a[0], bb);
-        mma_bf16(acc[1][j], a[1], bb);
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int c = half * 64 + j * 8 + 2 * tig;
-        const float v0 = fmaxf(acc[i][j][0] + b[c], 0.f), v1 = fmaxf(acc[i][j][1] + b[c + 1], 0.f);
-        const float v2 = fmaxf(acc[i][j][2] + b[c], 0.f), v3 = fmaxf(acc[i][j][3] + b[c + 1], 0.f);
-        const int r = i * 16 + gid;
-        if (head_rows) {
-          // last hidden layer: fold into the head, h rounded to bf16 like training
-          const float h0 = __bfloat162float(__float2bfloat16(v0)), h1 = __bfloat162float(__float2bfloat16(v1));
-          const float h2 = __bfloat162float(__float2bfloat16(v2)), h3 = __bfloat162float(__float2bfloat16(v3));
-          head_rows[i * 2] += h0 * w4[c] + h1 * w4[c + 1];
-          head_rows[i * 2 + 1] += h2 * w4[c] + h3 * w4[c + 1];
-        } else {
-          *reinterpret_cast<uint32_t*>(&out[r][c]) = pack_bf16(v0, v1);
-          *reinterpret_cast<uint32_t*>(&out[r + 8][c]) = pack_bf16(v2, v3);
-        }
-      }
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// stage W^T ([128 out][K] bf16, out-major) into K-major 128-B swizzle columns
+__device__ __forceinline__ void stage_weights(uint8_t* dst, const __nv_bfloat16* src, int K, int tid) {
+  const int chunks = K / 8;  // 16-B chunks per row
+  for (int e = tid; e < kHid * chunks; e += kTcThreads) {
+    const int n = e / chunks, c = e % chunks;
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(src + (size_t)n * K) + c);
+    *reinterpret_cast<uint4*>(dst + (c >> 3) * kAtom + sw128(n, c & 7)) = v;
   }
 }
 
-__global__ void __launch_bounds__(kInfWarps * 32) mlp_bound_kernel(const float* __restrict__ x, int64_t n,
-                                                                 InfParams p, float* __restrict__ bound) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  InfSmem& S = *reinterpret_cast<InfSmem*>(smem_raw);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // weights into shared memory (padded rows)
-  for (int e = tid; e < kHid * kIn; e += blockDim.x) S.w1t[e / kIn][e % kIn] = p.w1t[e];
-  for (int e = tid; e < kHid * kHid; e += blockDim.x) {
-    S.w2t[e / kHid][e % kHid] = p.w2t[e];
-    S.w3t[e / kHid][e % kHid] = p.w3t[e];
+// one layer's epilogue: relu(acc + b) -> bf16 -> this thread's row of the
+// next A operand (K = 128: two swizzle columns)
+__device__ __forceinline__ void epilogue_to_act(uint32_t tmem_row, const float* b, uint8_t* act, uint32_t row) {
+#pragma unroll
+  for (int cb = 0; cb < kHid / 32; ++cb) {
+    float v[32];
+    tmem_ld32(tmem_row + cb * 32, v);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c0 = cb * 32 + q * 8;
+      uint4 w;
+      w.x = pack_bf16(fmaxf(v[q * 8 + 0] + b[c0 + 0], 0.f), fmaxf(v[q * 8 + 1] + b[c0 + 1], 0.f));
+      w.y = pack_bf16(fmaxf(v[q * 8 + 2] + b[c0 + 2], 0.f), fmaxf(v[q * 8 + 3] + b[c0 + 3], 0.f));
+      w.z = pack_bf16(fmaxf(v[q * 8 + 4] + b[c0 + 4], 0.f), fmaxf(v[q * 8 + 5] + b[c0 + 5], 0.f));
+      w.w = pack_bf16(fmaxf(v[q * 8 + 6] + b[c0 + 6], 0.f), fmaxf(v[q * 8 + 7] + b[c0 + 7], 0.f));
+      *reinterpret_cast<uint4*>(act + (c0 >> 6) * kAtom + sw128(row, (c0 & 63) >> 3)) = w;
+    }
   }
-  for (int e = tid; e < kHid; e += blockDim.x) {
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    mlp_bound_tc_kernel(const float* __restrict__ x, int64_t n, InfParams p, float* __restrict__ bound,
+                        unsigned int* __restrict__ status) {
+  extern __shared__ unsigned char smem_raw[];
+  TcSmem& S = *reinterpret_cast<TcSmem*>(smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u));
+  const int tid = threadIdx.x, g = tid >> 7, t = tid & 127, wg = t >> 5;
+
+  stage_weights(S.w1, p.w1t, kIn, tid);
+  stage_weights(S.w2, p.w2t, kHid, tid);
+  stage_weights(S.w3, p.w3t, kHid, tid);
+  for (int e = tid; e < kHid; e += kTcThreads) {
     S.b1[e] = p.b1[e]; S.b2[e] = p.b2[e]; S.b3[e] = p.b3[e]; S.w4[e] = p.w4[e];
   }
-  for (int e = tid; e < kIn / 2 * 3; e += blockDim.x) S.freq[e] = p.freq[e];
+  for (int e = tid; e < kIn / 2 * 3; e += kTcThreads) S.freq[e] = p.freq[e];
+  if (tid < kTcGroups) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&S.mbar[tid])), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (tid < 32) {  // warp 0 allocates the CTA's TMEM columns
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  proxy_fence();  // staged weights visible to the tensor cores
+  tc_fence_before();
   __syncthreads();
-  const int64_t tiles = ceil_div(n, kRows);
-  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const int64_t r0 = tile * kRows + warp * kRowsPerWarp;
-    // Fourier features of this warp's 32 queries (lane = query)
+  tc_fence_after();
+
+  const uint32_t tmem_group = S.tmem_base + (uint32_t)g * kHid;        // this group's 128 columns
+  const uint32_t tmem_row = tmem_group + ((uint32_t)(wg * 32) << 16);  // this warp's 32 lanes
+  uint8_t* act = S.act[g];
+  const uint32_t act_a = smem_u32(act), w1_a = smem_u32(S.w1), w2_a = smem_u32(S.w2), w3_a = smem_u32(S.w3);
+  const uint32_t mbar = smem_u32(&S.mbar[g]);
+  uint32_t parity = 0;
+  bool ok = true;
+
+  const int64_t tiles = ceil_div(n, (int64_t)kTcRows);
+  for (int64_t tile = (int64_t)blockIdx.x * kTcGroups + g; tile < tiles && ok;
+       tile += (int64_t)gridDim.x * kTcGroups) {
+    const int64_t q = tile * kTcRows + t;
+    // Fourier features of query q -> row t (K = 64: one swizzle column)
     {
-      const int64_t q = r0 + lane;
       float px = 0.f, py = 0.f, pz = 0.f;
       if (q < n) { px = x[3 * q]; py = x[3 * q + 1]; pz = x[3 * q + 2]; }
-      for (int j = 0; j < kIn / 2; ++j) {
-        float s, c;
-        fourier(px, py, pz, p.nz, S.freq, j, s, c);
-        *reinterpret_cast<uint32_t*>(&S.act[warp][0][lane][2 * j]) = pack_bf16(s, c);
+#pragma unroll
+      for (int c = 0; c < kIn / 8; ++c) {
+        uint32_t w[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          float s, co;
+          fourier(px, py, pz, p.nz, S.freq, 4 * c + k, s, co);
+          w[k] = pack_bf16(s, co);
+        }
+        *reinterpret_cast<uint4*>(act + sw128(t, c)) = make_uint4(w[0], w[1], w[2], w[3]);
       }
     }
-    __syncwarp();
-    warp_layer<kIn, kLdH, kLd1>(S.act[warp][0], S.w1t, S.b1, S.act[warp][1], nullptr, nullptr, lane);
-    __syncwarp();
-    warp_layer<kHid, kLdH, kLdH>(S.act[warp][1], S.w2t, S.b2, S.act[warp][0], nullptr, nullptr, lane);
-    __syncwarp();
-    float head[4] = {0.f, 0.f, 0.f, 0.f};  // rows gid, gid+8, 16+gid, 24+gid
-    warp_layer<kHid, kLdH, kLdH>(S.act[warp][0], S.w3t, S.b3, nullptr, S.w4, head, lane);
-    // reduce the head's partial sums over the 4 lanes of a row group
+    float y = 0.f;
+#pragma unroll 1
+    for (int layer = 0; layer < 3 && ok; ++layer) {
+      proxy_fence();       // this thread's A-operand row visible to the tensor cores
+      tc_fence_before();   // and its earlier TMEM reads ordered before the barrier
+      group_sync(g);
+      if (t == 0) {
+        tc_fence_after();
+        const int ksteps = layer == 0 ? kIn / 16 : kHid / 16;
+        const uint32_t w_a = layer == 0 ? w1_a : (layer == 1 ? w2_a : w3_a);
+        for (int j = 0; j < ksteps; ++j) {
+          const uint32_t off = (uint32_t)(j >> 2) * kAtom + (uint32_t)(j & 3) * 32u;
+          umma_bf16(tmem_group, sw128_desc(act_a + off), sw128_desc(w_a + off), j > 0 ? 1u : 0u);
+        }
+        umma_commit(mbar);
+      }
+      // the group goes on only if every thread saw the phase complete, so
+      // its named barriers stay matched when a wait runs out
+      ok = group_all(g, mbar_wait(mbar, parity));
+      parity ^= 1u;
+      if (!ok) break;
+      tc_fence_after();
+      if (layer < 2) {
+        epilogue_to_act(tmem_row, layer == 0 ? S.b1 : S.b2, act, (uint32_t)t);
+      } else {
+        // last hidden layer: h rounded to bf16 like training, folded into the head
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      head[r] += __shfl_xor_sync(0xffffffffu, head[r], 1);
-      head[r] += __shfl_xor_sync(0xffffffffu, head[r], 2);
-    }
-    if ((lane & 3) == 0) {
-      const int gid = lane >> 2;
-      const int rows[4] = {gid, gid + 8, 16 + gid, 24 + gid};
+        for (int cb = 0; cb < kHid / 32; ++cb) {
+          float v[32];
+          tmem_ld32(tmem_row + cb * 32, v);
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int64_t q = r0 + rows[r];
-        if (q < n) bound[q] = fmaxf(head[r] + p.b4, 0.f) * p.scale + p.margin;
+          for (int i = 0; i < 32; ++i) {
+            const int c = cb * 32 + i;
+            const float h = __bfloat162float(__float2bfloat16(fmaxf(v[i] + S.b3[c], 0.f)));
+            y += h * S.w4[c];
+          }
+        }
       }
     }
-    __syncwarp();
+    if (ok && q < n) {
+      const float z = y + p.b4;
+      bound[q] = (p.log_space ? expf(z) : fmaxf(z, 0.f)) * p.scale + p.margin;
+    }
+  }
+  if (!ok) {
+    atomicOr(status, 1u);
+    // a group that gave up may still have MMAs in flight: wait once more
+    // (bounded) for its last commit before the columns are released
+    mbar_wait(mbar, parity ^ 1u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (tid < 32) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(S.tmem_base), "r"(kTmemCols)
+                 : "memory");
   }
 }
 
@@ -372,6 +511,10 @@ __global__ void __launch_bounds__(kInfWarps * 32) mlp_bound_kernel(const float* 
 }  // namespace a3d
 
 using namespace a3d;
+
+// status word of the inference kernel, per device (bit 0: a warpgroup's
+// tensor-core wait ran out and its remaining tiles were left unwritten)
+__device__ unsigned int g_mlp_status;
 
 extern "C" int a3d_gemm_bf16(const a3d_gemm_args* a, a3d_stream_t stream) {
   A3D_REQUIRE(a && a->A && a->B && (a->Cf || a->Cb), A3D_ERR_ARGUMENT, "gemm_bf16: null operand");
@@ -451,19 +594,37 @@ extern "C" int a3d_mlp_bound(const a3d_mlp_weights* wts, const float* x, int64_t
   p.freq = wts->freq;
   p.nz = Normalise{wts->norm[0], wts->norm[1], wts->norm[2], wts->norm[3]};
   p.scale = wts->scale; p.margin = wts->margin;
-  const size_t smem = sizeof(InfSmem);
-  // the shared-memory opt-in is a per-device setting
+  p.log_space = wts->log_space;
+  // the staged weight rows are read as 16-B vectors
+  A3D_REQUIRE(((uintptr_t)p.w1t | (uintptr_t)p.w2t | (uintptr_t)p.w3t) % 16 == 0, A3D_ERR_ARGUMENT,
+              "mlp_bound: weight matrices must be 16-byte aligned");
+  const size_t smem = sizeof(TcSmem) + 1024;  // + alignment of the swizzled operands
+  // the shared-memory opt-in and the status word's address are per device
   static bool attr_set[kMaxDevices] = {false};
+  static unsigned int* status_ptr[kMaxDevices] = {nullptr};
   int dev = 0;
   A3D_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices || !attr_set[dev]) {
-    A3D_CUDA_TRY(cudaFuncSetAttribute(mlp_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (dev >= 0 && dev < kMaxDevices) attr_set[dev] = true;
+  A3D_REQUIRE(dev >= 0 && dev < kMaxDevices, A3D_ERR_ARGUMENT, "mlp_bound: device ordinal out of range");
+  if (!attr_set[dev]) {
+    A3D_CUDA_TRY(cudaFuncSetAttribute(mlp_bound_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    A3D_CUDA_TRY(cudaGetSymbolAddress((void**)&status_ptr[dev], g_mlp_status));
+    attr_set[dev] = true;
   }
+  A3D_CUDA_TRY(cudaMemsetAsync(status_ptr[dev], 0, sizeof(unsigned int), (cudaStream_t)stream));
   const int sms = num_sms();
-  const int64_t tiles = ceil_div(n, kRows);
-  const int64_t grid = tiles < (int64_t)sms ? tiles : (int64_t)sms;
-  mlp_bound_kernel<<<(unsigned)grid, kInfWarps * 32, smem, (cudaStream_t)stream>>>(x, n, p, bound);
+  const int64_t tiles = ceil_div(n, (int64_t)kTcRows);
+  const int64_t want = ceil_div(tiles, (int64_t)kTcGroups);
+  const int64_t grid = want < (int64_t)sms ? want : (int64_t)sms;
+  mlp_bound_tc_kernel<<<(unsigned)grid, kTcThreads, smem, (cudaStream_t)stream>>>(x, n, p, bound,
+                                                                                 status_ptr[dev]);
   A3D_LAUNCH_CHECK();
+  return A3D_OK;
+}
+
+extern "C" int a3d_mlp_bound_status(unsigned int* status, a3d_stream_t stream) {
+  A3D_REQUIRE(status, A3D_ERR_ARGUMENT, "mlp_bound_status: null argument");
+  A3D_CUDA_TRY(cudaMemcpyFromSymbolAsync(status, g_mlp_status, sizeof(unsigned int), 0, cudaMemcpyDeviceToHost,
+                                         (cudaStream_t)stream));
+  A3D_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
   return A3D_OK;
 }

@@ -538,6 +538,7 @@ __global__ void __maxnreg__(kTaskMaxRegs)
   uint32_t ref = 0, prev = 0xffffffffu, best_tri = 0xffffffffu, root = 0u, prev_root = 0u;
   float best_sq = INFINITY, px = 0.f, py = 0.f, pz = 0.f, bsq = INFINITY;
   bool have = false;
+  bool reused = false;  // the query's radius is seeded by the previous query's triangle
   int sp = 0;
   // overflow stack in global memory (the workspace's spill region), used
   // when the shared stack is full; owners beyond the region have none
@@ -571,6 +572,7 @@ __global__ void __maxnreg__(kTaskMaxRegs)
     // a finite caller bound alone seeds the radius when asked to (no probe
     // descent); else the previous result seeds it for a nearby query in the
     // sorted order; otherwise a greedy probe does
+    reused = false;
     if ((seeding & kSeedBoundOnly) && bsq < INFINITY) {
       best_sq = bsq;
       phase = kTrav;
@@ -579,6 +581,7 @@ __global__ void __maxnreg__(kTaskMaxRegs)
     } else if ((seeding & kSeedReuse) && prev != 0xffffffffu && (!kBatch || root == prev_root) &&
                k - kprev <= 64 && k > kprev) {
       phase = kSeed;
+      reused = true;
     } else {
       prev = 0xffffffffu;
       phase = kProbe;
@@ -636,15 +639,21 @@ __global__ void __maxnreg__(kTaskMaxRegs)
     }
     if (done && best_tri == 0xffffffffu && bsq < INFINITY) {
       // the caller's bound excluded every triangle: run the query again in
-      // place, unbounded (a greedy probe seeds it), instead of handing it to
-      // the deep-stack re-run kernel
+      // place, unbounded, seeded as the plain method seeds it (the previous
+      // query's triangle when that seeded it, else a greedy probe), instead
+      // of handing it to the deep-stack re-run kernel
       bsq = INFINITY;
       best_sq = INFINITY;
       sp = 0;
       gsp = 0;
-      phase = kProbe;
-      ref = root;
-      have = true;
+      if (reused) {
+        phase = kSeed;
+        have = false;
+      } else {
+        phase = kProbe;
+        ref = root;
+        have = true;
+      }
       done = false;
     }
     if (phase == kAbandon) done = true;

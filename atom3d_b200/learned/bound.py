@@ -9,7 +9,9 @@ turns out too small are re-run without it, so results are identical with or
 without the network; the plain method decides which bounds missed.
 
 Training and inference run in hand-written BF16 tensor-core kernels
-(a3d_gemm_bf16, a3d_mlp_* in csrc/mlp.cu); PyTorch only holds the buffers.
+(csrc/mlp.cu): inference in one tcgen05 kernel with its accumulators in
+tensor memory (a3d_mlp_bound), training in mma.sync GEMMs (a3d_gemm_bf16,
+a3d_mlp_*); PyTorch only holds the buffers.
 """
 
 from __future__ import annotations
@@ -29,6 +31,7 @@ class MlpWeights(ctypes.Structure):
         ("b1", ctypes.c_void_p), ("b2", ctypes.c_void_p), ("b3", ctypes.c_void_p),
         ("w4", ctypes.c_void_p), ("b4", ctypes.c_float), ("freq", ctypes.c_void_p),
         ("norm", ctypes.c_float * 4), ("scale", ctypes.c_float), ("margin", ctypes.c_float),
+        ("log_space", ctypes.c_int32),
     ]
 
 
@@ -45,6 +48,7 @@ class GemmArgs(ctypes.Structure):
 _SIGS = {
     "a3d_mlp_bound": (ctypes.c_int, [ctypes.POINTER(MlpWeights), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                      ctypes.c_void_p]),
+    "a3d_mlp_bound_status": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint), ctypes.c_void_p]),
     "a3d_gemm_bf16": (ctypes.c_int, [ctypes.POINTER(GemmArgs), ctypes.c_void_p]),
     "a3d_mlp_fourier": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_float), ctypes.c_void_p,
                                        ctypes.c_void_p, ctypes.c_void_p]),
@@ -79,8 +83,14 @@ _SHAPES = [("W1", (N_IN, N_HID)), ("W2", (N_HID, N_HID)), ("W3", (N_HID, N_HID))
 class LearnedBound:
     """Per-mesh learned upper bound on the unsigned distance."""
 
-    def __init__(self, lo, hi, device="cuda", sigma: float = 1.5, seed: int = 0):
+    def __init__(self, lo, hi, device="cuda", sigma: float = 1.5, seed: int = 0, log_space: bool = False):
+        """``log_space``: the network learns log(distance + eps) instead of the
+        distance, so its error is relative (near-surface queries get tight
+        bounds) and the bound is exp(y) * scale + margin."""
         self.dev = torch.device(device)
+        self.log_space = bool(log_space)
+        self.eps = 1e-4
+        self.coverage = None
         lo = torch.as_tensor(lo, dtype=torch.float32)
         hi = torch.as_tensor(hi, dtype=torch.float32)
         c = (lo + hi) * 0.5
@@ -192,6 +202,8 @@ class LearnedBound:
         """Train on (points, plain-traversal distances); returns the loss history."""
         x = x.to(self.dev, torch.float32).contiguous()
         dist = dist.to(self.dev, torch.float32).contiguous()
+        if self.log_space:
+            dist = torch.log(dist + self.eps)
         n = x.shape[0]
         g = torch.Generator(device=self.dev).manual_seed(seed)
         hist = []
@@ -209,12 +221,14 @@ class LearnedBound:
         return torch.cat(hist).cpu() if hist else torch.zeros(0)
 
     def predict(self, x: torch.Tensor) -> torch.Tensor:
+        """The network's output through the training kernels (log(distance +
+        eps) in log space)."""
         y, _ = self.forward_backward(x.to(self.dev, torch.float32).contiguous(), None)
         return y
 
     def calibrate(self, x: torch.Tensor, dist: torch.Tensor, coverage: float = 0.995, slack: float = 1.02):
         """Choose scale/margin so that ``coverage`` of the samples satisfy
-        dist <= max(y, 0) * scale + margin."""
+        dist <= max(y, 0) * scale + margin (exp(y) in log space)."""
         raw = self._raw_bound(x)
         self.scale = float(slack)
         excess = dist.to(self.dev).float() - raw * self.scale
@@ -234,10 +248,10 @@ class LearnedBound:
         return MlpWeights(self._t["W1"].data_ptr(), self._t["W2"].data_ptr(), self._t["W3"].data_ptr(),
                           V["b1"].data_ptr(), V["b2"].data_ptr(), V["b3"].data_ptr(), V["w4"].data_ptr(),
                           float(V["b4"].item()), self.freq.data_ptr(), (ctypes.c_float * 4)(*self.norm),
-                          float(self.scale), float(self.margin))
+                          float(self.scale), float(self.margin), int(self.log_space))
 
     def __call__(self, x: torch.Tensor, out: Optional[torch.Tensor] = None, weights: Optional[MlpWeights] = None):
-        """Per-query bound (fused BF16 tensor-core inference kernel)."""
+        """Per-query bound (fused tcgen05 inference kernel)."""
         x = x.to(self.dev, torch.float32).contiguous()
         out = torch.empty(x.shape[0], dtype=torch.float32, device=self.dev) if out is None else out
         w = self.weights() if weights is None else weights
@@ -246,14 +260,69 @@ class LearnedBound:
         return out
 
 
-def train_for_mesh(mesh, samples: torch.Tensor, epochs: int = 8, coverage: float = 0.995, seed: int = 0):
-    """Fit a LearnedBound on plain-traversal distances of ``samples``."""
+    def status(self) -> int:
+        """Status word of the last inference launch on this device (waits
+        for it): bit 0 when a tile's tensor-core wait ran out."""
+        st = ctypes.c_uint(0)
+        _lib.check("a3d_mlp_bound_status", _bind().a3d_mlp_bound_status(ctypes.byref(st), self.stream))
+        return int(st.value)
+
+
+def _time_query(mesh, x, bound, reps: int = 3) -> float:
+    bvh = mesh._bvh
+    bvh.query(x, bound=bound, want_uvw=False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        bvh.query(x, bound=bound, want_uvw=False)
+    e1.record()
+    torch.cuda.synchronize(mesh.device)
+    return e0.elapsed_time(e1) / reps
+
+
+def tune_coverage(lb: "LearnedBound", mesh, x: torch.Tensor, dist: torch.Tensor,
+                  coverages=(0.97, 0.99, 0.997, 0.999), scales=(1.0, 1.1, 1.25, 1.5)) -> float:
+    """Choose the bound's scale and calibration coverage whose bound makes the
+    traversal of the held-out samples fastest (CUDA events on the held-out
+    set only; results never depend on the choice).  A looser bound prunes
+    less, a tighter one makes more queries restart; the trade-off depends on
+    the mesh and the query distribution, so it is measured rather than
+    fixed."""
+    x = x.to(lb.dev, torch.float32).contiguous()
+    d = dist.to(lb.dev).float()
+    raw = lb._raw_bound(x)
+    best = (float("inf"), coverages[0], 1.0, 0.0)
+    for sc in scales:
+        excess = (d - raw * sc)[:1 << 24]
+        for c in coverages:
+            margin = max(0.0, float(torch.quantile(excess, c)))
+            ms = _time_query(mesh, x, raw * sc + margin)
+            if ms < best[0]:
+                best = (ms, c, sc, margin)
+    lb.coverage, lb.scale, lb.margin = best[1], best[2], best[3]
+    return lb.coverage
+
+
+def train_for_mesh(mesh, samples: torch.Tensor, epochs: int = 8, coverage: float = 0.995, seed: int = 0,
+                   tune: bool = False, log_space: bool = False):
+    """Fit a LearnedBound on plain-traversal distances of ``samples``: a
+    random 90% trains it, the other 10% sets its margin.  With ``tune`` the
+    bound's scale and the margin's coverage are picked by timing the
+    traversal on the held-out samples."""
     lo = mesh.get_bounds()[0].cpu()
     hi = mesh.get_bounds()[1].cpu()
-    lb = LearnedBound(lo, hi, device=mesh.device, seed=seed)
+    lb = LearnedBound(lo, hi, device=mesh.device, seed=seed, log_space=log_space)
     n = samples.shape[0]
     ntr = int(n * 0.9)
-    d = mesh.udf(samples.to(mesh.device))
-    lb.fit(samples[:ntr], d[:ntr], epochs=epochs, seed=seed)
-    lb.calibrate(samples[ntr:], d[ntr:], coverage=coverage)
+    x = samples.to(mesh.device, torch.float32)
+    d = mesh.udf(x)
+    # a random split: the held-out tenth follows the samples' distribution
+    # whatever order they come in
+    perm = torch.randperm(n, generator=torch.Generator().manual_seed(seed + 1)).to(mesh.device)
+    tr, ho = perm[:ntr], perm[ntr:]
+    lb.fit(x[tr], d[tr], epochs=epochs, seed=seed)
+    lb.calibrate(x[ho], d[ho], coverage=coverage)
+    lb.coverage = coverage
+    if tune:
+        tune_coverage(lb, mesh, x[ho], d[ho])
     return lb

@@ -411,6 +411,12 @@ def main():
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": DRAM_BYTES_PER_QUERY * n, "traffic_source": TRAFFIC_SOURCE, "peak_kind": peak_kind,
                 "bytes_per_query": per_q, "kernel": "udf_task_kernel", "kernel_ms": kernel_ms}
+        # the tree (nodes + triangles, ~91 MB) stays in L2: the same bytes
+        # against the L2 read bandwidth measured on this GPU
+        l2 = l2_read_peak(dev)
+        roof["l2"] = {"peak": l2, "unit": "GB/s", "frac": achieved / l2,
+                      "how": "a3d_read_probe: 48 MiB buffer read 40 times through L2 (16-B ld.global.cg), "
+                             "CUDA events, best of 5"}
     line = {
         "metric": METRIC, "value": replica_throughput(n, world, ms), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -524,7 +530,7 @@ def bench_learned(dev, v, f, mesh, qd, steps):
     train = synthetic.mixed_queries(v, f, 1 << 22, g)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    lb = train_for_mesh(mesh, train, epochs=8, coverage=0.99)
+    lb = train_for_mesh(mesh, train, epochs=8, coverage=0.99, tune=True, log_space=True)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     bvh = mesh._bvh
@@ -542,15 +548,22 @@ def bench_learned(dev, v, f, mesh, qd, steps):
         "exact_bound_seeds": (exact, NR | BS),
     }
     out = {"metric": "UDF Mqueries/s, learned bound vs plain (same 16M queries)", "unit": UNIT,
-           "train_s": train_s, "train_samples": 1 << 22, "margin": lb.margin, "infer_ms": infer_ms,
+           "train_s": train_s, "train_samples": 1 << 22, "margin": lb.margin, "scale": lb.scale,
+           "coverage": lb.coverage, "log_space": lb.log_space,
+           "infer_ms": infer_ms, "infer_tflops": 82176 * n / (infer_ms * 1e-3) / 1e12,
            "bound_covers": float((ref[0] <= bound).float().mean())}
     for name, (b, flags) in variants.items():
-        r = bvh.query(qd, bound=b, seeding=flags)
+        st = torch.zeros(4, dtype=torch.int64, device=dev)
+        r = bvh.query(qd, bound=b, seeding=flags, stats=st)
         same = bool(torch.equal(r[0], ref[0]) and torch.equal(r[1], ref[1]))
+        nodes, tris, reruns, _ = (int(x) for x in st.cpu())
         ms = _time_ms(lambda: bvh.query(qd, bound=b, seeding=flags), steps)
         if name.startswith("learned"):
             ms += infer_ms  # the bound's inference is part of the learned path
-        out[name] = {"ms": ms, "mqs": n / ms / 1e3, "identical": same}
+        # per-query node visits and triangle tests (a query whose bound
+        # excluded every triangle counts both of its passes)
+        out[name] = {"ms": ms, "mqs": n / ms / 1e3, "identical": same, "nodes_per_query": nodes / n,
+                     "tris_per_query": tris / n, "deep_stack_reruns": reruns}
     out["speedup_learned_vs_plain"] = out["plain"]["ms"] / min(out["learned_cap"]["ms"], out["learned_seeds"]["ms"])
     out["speedup_exact_bound_vs_plain"] = out["plain"]["ms"] / min(out["exact_bound_cap"]["ms"],
                                                                      out["exact_bound_seeds"]["ms"])
@@ -836,6 +849,36 @@ def bench_pairs(dev, mesh, oc, cand, steps):
                                  "reference_demo_polygons": 1172044,
                                  "poly_counts_range": [int(r.poly_counts.min()), int(r.poly_counts.max())]}
     return out
+
+
+def l2_read_peak(dev, mib=48, passes=40, reps=5):
+    """Read bandwidth of a buffer that stays in L2 (GB/s): a3d_read_probe
+    streams it `passes` times; best of `reps` CUDA-event timings."""
+    import ctypes
+
+    from atom3d_b200 import _lib
+
+    fn = _lib.lib().a3d_read_probe
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    buf = torch.ones(mib << 20, dtype=torch.uint8, device=dev)
+    sink = torch.zeros(1, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    nbytes = buf.numel()
+
+    def run():
+        _lib.check("a3d_read_probe", fn(buf.data_ptr(), nbytes, passes, sink.data_ptr(), stream.cuda_stream))
+
+    run()
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1))
+    return nbytes * passes / (best * 1e-3) / 1e9
 
 
 def launches_per_udf():

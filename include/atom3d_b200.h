@@ -296,6 +296,11 @@ int a3d_exclusive_scan_u32(const uint32_t* in, int64_t n, int64_t* out, void* wo
 size_t a3d_sort_pairs_workspace_bytes(int64_t n);
 int a3d_sort_pairs_u64(uint64_t* keys, uint32_t* vals, int64_t n, int begin_bit, int end_bit,
                        void* workspace, size_t workspace_bytes, a3d_stream_t stream);
+/* Streams `bytes` (a multiple of 16) of `buf` `passes` times through L2 with
+ * 16-byte loads from 4 blocks of 512 threads per SM; `sink` (device, one
+ * word) keeps the loads live.  Timed with events on a buffer that fits in L2
+ * it measures the L2 read bandwidth (the bench's L2 roofline denominator). */
+int a3d_read_probe(const void* buf, int64_t bytes, int passes, uint32_t* sink, a3d_stream_t stream);
 
 /* ---- surface dual graph and dam wet masks -------------------------------- */
 /* Replace construct_surface_dual_graph and get_dam_wet_faces / _edges /
@@ -519,9 +524,12 @@ int a3d_batch_autotune(const a3d_bvh_batch* bvh, const float* points, const int6
 
 /* ---- learned distance bound (no counterpart in the reference) ----------- */
 /* A Fourier-feature MLP (3 -> 64 -> 128 -> 128 -> 128 -> 1, ReLU) predicts
- * a query's unsigned distance; bound = max(y, 0) * scale + margin seeds
- * a3d_udf's pruning radius (results never depend on it).  Inference is one
- * fused BF16 tensor-core kernel; training uses the kernels below. */
+ * a query's unsigned distance (or its logarithm); bound = max(y, 0) * scale
+ * + margin (exp(y) * scale + margin in log space) seeds a3d_udf's pruning
+ * radius (results never depend on it).  Inference is one fused kernel on the
+ * tcgen05 tensor cores (BF16 operands in shared memory, FP32 accumulators in
+ * tensor memory, one CTA per SM, 128 queries per warpgroup tile); the weight
+ * matrices must be 16-byte aligned.  Training uses the kernels below. */
 typedef struct a3d_mlp_weights {
   const void* w1t;   /* bf16 [128][64]  (W1 transposed, out-major) */
   const void* w2t;   /* bf16 [128][128] */
@@ -535,10 +543,16 @@ typedef struct a3d_mlp_weights {
   float norm[4];     /* x_hat = (x - norm[0..2]) * norm[3] */
   float scale;
   float margin;
+  int32_t log_space; /* nonzero: y predicts log(distance), bound = exp(y) * scale + margin */
 } a3d_mlp_weights;
 
 int a3d_mlp_bound(const a3d_mlp_weights* w, const float* x, int64_t n, float* bound,
                   a3d_stream_t stream);
+/* Status of the last a3d_mlp_bound launch on the current device (waits for
+ * `stream`): bit 0 set when a tile's tensor-core wait ran out, in which case
+ * bounds of the tiles not reached were left unwritten.  Calls that overlap
+ * on the GPU share the word. */
+int a3d_mlp_bound_status(unsigned int* status, a3d_stream_t stream);
 
 /* training building blocks (BF16 operands, FP32 accumulation) */
 typedef struct a3d_gemm_args {

@@ -47,7 +47,35 @@ def test_inference_kernel_matches_training_forward():
     x = (torch.rand(10000, 3, generator=torch.Generator().manual_seed(1)) * 3 - 1.5).cuda()
     y = lb.predict(x)
     b = lb(x)
+    assert lb.status() == 0
     assert torch.allclose(b, torch.clamp(y, min=0), atol=2e-3, rtol=2e-2)
+
+
+@pytest.mark.parametrize("n,log_space", [(1, False), (127, False), (128, True), (129, False), (4096 + 77, True),
+                                         (600_000, False)])
+def test_tensor_core_inference_matches_training_kernels(n, log_space):
+    """The tcgen05 inference kernel (tensor-memory accumulators, swizzled
+    shared-memory operands) against the training path's mma.sync GEMMs on the
+    same BF16 weights and features: the same roundings, so only the FP32
+    summation order differs; ragged tails, many tiles per warpgroup, both
+    output spaces."""
+    lb = LearnedBound([-1.5] * 3, [1.5] * 3, seed=7, log_space=log_space)
+    g = torch.Generator().manual_seed(3)
+    xt = (torch.rand(8192, 3, generator=g) * 3 - 1.5).cuda()
+    lb.fit(xt, xt.norm(dim=1) * 0.5, epochs=2, batch=1024)  # a trained spread of weights
+    x = (torch.rand(n, 3, generator=g) * 3 - 1.5).cuda()
+    y = lb.predict(x)
+    y = torch.exp(y) if log_space else torch.clamp(y, min=0)
+    b = lb(x)
+    assert lb.status() == 0
+    d = (b - y).abs()
+    scale = float(y.abs().max()) + 1e-6
+    assert float(d.max()) <= 2e-2 * scale, float(d.max())
+    assert float(d.median()) <= 1e-3 * scale, float(d.median())
+    # every query written (no tile skipped), deterministically
+    out = torch.full((n,), float("nan"), device="cuda")
+    lb(x, out=out)
+    assert torch.equal(out, b)
 
 
 def test_trained_bound_against_the_plain_method():
