@@ -126,29 +126,40 @@ __global__ void corner_pos_kernel(DmcIn in, float ws, float* __restrict__ x) {
   }
 }
 
-// case ids in one pass over cube_idx: thread (cube, corner) takes its
-// corner's sign bit; the 8 lanes of a cube (aligned groups of 8) OR their
-// bits into the case id.  Corner positions are not materialised: the kernels
-// that need them compute them from the cube (corner_world).
+// case ids in one pass over cube_idx: one thread per cube reads its 8
+// corner ids (four 16-B loads when cube_idx is 16-B aligned) and gathers the
+// 8 corner signs independently, so each thread has 64 B and 8 gathers in
+// flight.  Corner positions are not materialised: the kernels that need them
+// compute them from the cube (corner_world).
+template <bool kVec>
 __global__ void corner_case_kernel(DmcIn in, uint8_t* __restrict__ cases, uint32_t* __restrict__ flag,
                                    uint32_t* __restrict__ bad_index) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = t < in.n * 8;
-  const int c = (int)(t & 7);
-  uint32_t bit = 0;
-  if (valid) {
-    const int64_t v = in.cidx[t];
-    if ((uint64_t)v >= (uint64_t)in.m) *bad_index = 1u;
-    const int64_t mi = (uint64_t)v < (uint64_t)in.m ? v : 0;
-    bit = (fsb(__ldg(in.sdf + mi), in.iso) < 0.f ? 1u : 0u) << c;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= in.n) return;
+  int64_t v[8];
+  if (kVec) {
+    const longlong2* p = reinterpret_cast<const longlong2*>(in.cidx + 8 * i);
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const longlong2 q = __ldg(p + h);
+      v[2 * h] = q.x;
+      v[2 * h + 1] = q.y;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[c] = __ldg(in.cidx + 8 * i + c);
   }
-  bit |= __shfl_xor_sync(0xffffffffu, bit, 1);
-  bit |= __shfl_xor_sync(0xffffffffu, bit, 2);
-  bit |= __shfl_xor_sync(0xffffffffu, bit, 4);
-  if (valid && c == 0) {
-    cases[t >> 3] = (uint8_t)bit;
-    flag[t >> 3] = (bit != 0u && bit != 255u) ? 1u : 0u;
+  bool bad = false;
+  uint32_t bits = 0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const bool ok = (uint64_t)v[c] < (uint64_t)in.m;
+    bad = bad || !ok;
+    bits |= (fsb(__ldg(in.sdf + (ok ? v[c] : 0)), in.iso) < 0.f ? 1u : 0u) << c;
   }
+  if (bad) *bad_index = 1u;
+  cases[i] = (uint8_t)bits;
+  flag[i] = (bits != 0u && bits != 255u) ? 1u : 0u;
 }
 
 // copies scattered device words into one block, so that the host reads
@@ -456,14 +467,34 @@ __global__ void vd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ lis
   float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
   float z[7][3];
   int64_t g = g0;
+  // the dependent gathers level by level over the slots, so each level's
+  // loads of all edges are in flight together
+  int32_t R[7], I0[7], I1[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const int e = vd_edge(vedges, k);
+    R[k] = e == 15 ? 0 : ed.idx_map[(int64_t)t * 12 + e];
+  }
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const bool has = vd_edge(vedges, k) != 15;
+    I0[k] = has ? (int32_t)ed.e0[R[k]] : 0;
+    I1[k] = has ? (int32_t)ed.e1[R[k]] : 0;
+  }
+  float S0[7], S1[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const bool has = vd_edge(vedges, k) != 15;
+    S0[k] = has ? fsb(ldf(in.sdf, I0[k]), in.iso) : 0.f;
+    S1[k] = has ? fsb(ldf(in.sdf, I1[k]), in.iso) : 0.f;
+  }
 #pragma unroll
   for (int k = 0; k < 7; ++k) {
     const int e = vd_edge(vedges, k);
     if (e == 15) continue;
     const int64_t flat = (int64_t)t * 12 + e;
-    const int32_t r = ed.idx_map[flat];
-    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
-    const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
+    const int64_t i0 = I0[k], i1 = I1[k];
+    const float s0 = S0[k], s1 = S1[k];
     const float a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
     const float a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
     const float b = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
@@ -584,6 +615,12 @@ __device__ __forceinline__ void scatter_interp_grad(const DmcIn& in, const float
   }
 }
 
+// One thread per dual vertex.  The forward quantities are recomputed per
+// table slot k (0..6, unrolled, so every per-edge value lives in a register
+// indexed by a compile-time slot instead of a local-memory array); slots
+// without an edge are skipped.  Gradient order per edge as the forward's
+// reverse: L_dev -> distances -> plain crossings and the dual vertex ->
+// weighted average -> interpolation weights -> sdf, deform, alpha, beta.
 __global__ void vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
                               const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
                               const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
@@ -599,116 +636,155 @@ __global__ void vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__
   float vx[3];
   load_voxel(in, cube, vx);
   const int64_t g0 = goff[v];
-  // recompute the forward quantities of this dual vertex
-  int64_t I0[7], I1[7];
-  int E[7];
-  float A[7][2], S[7][2], B[7], UE[7][3];
-  int ne = 0;
+  // gathers level by level over the slots (independent loads in flight)
+  int32_t R[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const int e = vd_edge(vedges, k);
+    R[k] = e == 15 ? 0 : ed.idx_map[(int64_t)t * 12 + e];
+  }
+  int32_t I0[7], I1[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const bool has = vd_edge(vedges, k) != 15;
+    I0[k] = has ? (int32_t)ed.e0[R[k]] : 0;
+    I1[k] = has ? (int32_t)ed.e1[R[k]] : 0;
+  }
+  float S0[7], S1[7], A0[7], A1[7], B[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const int e = vd_edge(vedges, k);
+    const bool has = e != 15;
+    const int ee = has ? e : 0;  // a valid table index for the empty slots
+    S0[k] = has ? fsb(ldf(in.sdf, I0[k]), in.iso) : 0.f;
+    S1[k] = has ? fsb(ldf(in.sdf, I1[k]), in.iso) : 0.f;
+    A0[k] = (has && in.alpha) ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * ee]], in.wscale, true) : 1.f;
+    A1[k] = (has && in.alpha) ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * ee + 1]], in.wscale, true) : 1.f;
+    B[k] = (has && in.beta) ? norm_w(in.beta[12 * (int64_t)cube + ee], in.wscale, true) : 1.f;
+  }
+  // forward: weighted average of the alpha-weighted crossings
+  float UE[7][3], Z[7][3];
   float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
+  int ne = 0;
+#pragma unroll
   for (int k = 0; k < 7; ++k) {
     const int e = vd_edge(vedges, k);
     if (e == 15) continue;
-    const int32_t r = ed.idx_map[(int64_t)t * 12 + e];
-    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
-    I0[ne] = i0; I1[ne] = i1; E[ne] = e;
-    S[ne][0] = fsb(in.sdf[i0], in.iso); S[ne][1] = fsb(in.sdf[i1], in.iso);
-    A[ne][0] = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
-    A[ne][1] = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
-    B[ne] = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
-    const float w0 = fm(S[ne][1], A[ne][1]), w1 = -fm(S[ne][0], A[ne][0]), den = fa(w0, w1);
+    const float w0 = fm(S1[k], A1[k]), w1 = -fm(S0[k], A0[k]), den = fa(w0, w1);
+    const float pw0 = S1[k], pw1 = -S0[k], pden = fa(pw0, pw1);
     float pa[3], pb[3];
-    edge_world(in, ws, vx, e, i0, i1, pa, pb);
+    edge_world(in, ws, vx, e, I0[k], I1[k], pa, pb);
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
-      UE[ne][a] = interp1(pa[a], pb[a], w0, w1, den);
-      acc[a] = fa(acc[a], fm(UE[ne][a], B[ne]));
+      UE[k][a] = interp1(pa[a], pb[a], w0, w1, den);
+      Z[k][a] = interp1(pa[a], pb[a], pw0, pw1, pden);
+      acc[a] = fa(acc[a], fm(UE[k][a], B[k]));
     }
-    bsum = fa(bsum, B[ne]);
+    bsum = fa(bsum, B[k]);
     ++ne;
   }
   const float bden = fa(bsum, 1e-8f);
   float vd[3];
+#pragma unroll
   for (int a = 0; a < 3; ++a) vd[a] = fd(acc[a], bden);
   // incoming gradient of the dual vertex
   float gvd[3] = {0.f, 0.f, 0.f};
   if (gr.g_verts)
+#pragma unroll
     for (int a = 0; a < 3; ++a) gvd[a] = gr.g_verts[3 * v + a] + gr.g_vd[3 * v + a];
   // L_dev backward (mad = |dist - mean|, mean = sum(dist)/ne)
-  float Z[7][3], D[7], gD[7];
+  float D[7], gD[7];
   float msum = 0.f;
-  for (int q = 0; q < ne; ++q) {
-    const float w0 = S[q][1], w1 = -S[q][0], dn = fa(w0, w1);
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    D[k] = 0.f;
+    gD[k] = 0.f;
+    if (vd_edge(vedges, k) == 15) continue;
     float d2 = 0.f;
-    float pa[3], pb[3];
-    edge_world(in, ws, vx, E[q], I0[q], I1[q], pa, pb);
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
-      Z[q][a] = interp1(pa[a], pb[a], w0, w1, dn);
-      const float dd = fsb(Z[q][a], vd[a]);
+      const float dd = fsb(Z[k][a], vd[a]);
       d2 = fa(d2, fm(dd, dd));
     }
-    D[q] = sqrtf(d2);
-    msum = fa(msum, D[q]);
-    gD[q] = 0.f;
+    D[k] = sqrtf(d2);
+    msum = fa(msum, D[k]);
   }
   const float mean = fd(msum, (float)ne);
   if (gr.g_ldev) {
     float gmean = 0.f;
-    for (int q = 0; q < ne; ++q) {
+    int q = 0;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      if (vd_edge(vedges, k) == 15) continue;
       const float gl = gr.g_ldev[g0 + q];
-      const float df = D[q] - mean;
+      const float df = D[k] - mean;
       const float sg = df > 0.f ? 1.f : (df < 0.f ? -1.f : 0.f);
-      gD[q] += gl * sg;
+      gD[k] += gl * sg;
       gmean -= gl * sg;
+      ++q;
     }
     const float gm = gmean / (float)ne;
-    for (int q = 0; q < ne; ++q) gD[q] += gm;
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+      if (vd_edge(vedges, k) != 15) gD[k] += gm;
   }
-  // dist -> crossing z and dual vertex
+  // dist -> crossing z (gZ, kept in Z's registers' place) and the dual vertex
   float gZ[7][3];
-  for (int q = 0; q < ne; ++q) {
-    const float invd = D[q] > 0.f ? 1.0f / D[q] : 0.f;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) gZ[k][a] = 0.f;
+    if (vd_edge(vedges, k) == 15) continue;
+    const float invd = D[k] > 0.f ? 1.0f / D[k] : 0.f;
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float u = (Z[q][a] - vd[a]) * invd;
-      gZ[q][a] = gD[q] * u;
-      gvd[a] -= gD[q] * u;
+      const float u = (Z[k][a] - vd[a]) * invd;
+      gZ[k][a] = gD[k] * u;
+      gvd[a] -= gD[k] * u;
     }
   }
   // vd = sum(b ue) / (sum b + 1e-8)
   const float inv_bden = 1.0f / bden;
   float gB = 0.f;
+#pragma unroll
   for (int a = 0; a < 3; ++a) gB -= gvd[a] * vd[a] * inv_bden;
-  for (int q = 0; q < ne; ++q) {
-    const int e = E[q];
-    const int64_t i0 = I0[q], i1 = I1[q];
+  int q = 0;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
+    const int64_t i0 = I0[k], i1 = I1[k];
     float gue[3];
     float gb = gB;
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
-      gue[a] = gvd[a] * B[q] * inv_bden;
+      gue[a] = gvd[a] * B[k] * inv_bden;
       if (gr.g_palpha) gue[a] += gr.g_palpha[3 * (g0 + q) + a];
-      gb += gvd[a] * UE[q][a] * inv_bden;
+      gb += gvd[a] * UE[k][a] * inv_bden;
     }
     float xa[3], xb[3];
     edge_world(in, ws, vx, e, i0, i1, xa, xb);
     // ue through w0 = s1 a1, w1 = -s0 a0
     {
-      const float w0 = S[q][1] * A[q][1], w1 = -(S[q][0] * A[q][0]), den = w0 + w1;
+      const float w0 = S1[k] * A1[k], w1 = -(S0[k] * A0[k]), den = w0 + w1;
       float gw0, gw1;
-      scatter_interp_grad(in, gue, xa, xb, UE[q], w0, w1, den, i0, i1, gw0, gw1, gr);
+      scatter_interp_grad(in, gue, xa, xb, UE[k], w0, w1, den, i0, i1, gw0, gw1, gr);
       if (gr.g_sdf) {
-        atomicAdd(&gr.g_sdf[i1], gw0 * A[q][1]);
-        atomicAdd(&gr.g_sdf[i0], -gw1 * A[q][0]);
+        atomicAdd(&gr.g_sdf[i1], gw0 * A1[k]);
+        atomicAdd(&gr.g_sdf[i0], -gw1 * A0[k]);
       }
       if (gr.g_alpha && in.alpha) {
         const int c0 = kCE[2 * e], c1 = kCE[2 * e + 1];
         const float t0 = tanhf(in.alpha[8 * (int64_t)cube + c0]), t1 = tanhf(in.alpha[8 * (int64_t)cube + c1]);
-        atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c1], gw0 * S[q][1] * in.wscale * (1.f - t1 * t1));
-        atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c0], -gw1 * S[q][0] * in.wscale * (1.f - t0 * t0));
+        atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c1], gw0 * S1[k] * in.wscale * (1.f - t1 * t1));
+        atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c0], -gw1 * S0[k] * in.wscale * (1.f - t0 * t0));
       }
     }
     // plain crossing z through w0 = s1, w1 = -s0
     {
-      const float w0 = S[q][1], w1 = -S[q][0], den = w0 + w1;
+      const float w0 = S1[k], w1 = -S0[k], den = w0 + w1;
       float gw0, gw1;
-      scatter_interp_grad(in, gZ[q], xa, xb, Z[q], w0, w1, den, i0, i1, gw0, gw1, gr);
+      scatter_interp_grad(in, gZ[k], xa, xb, Z[k], w0, w1, den, i0, i1, gw0, gw1, gr);
       if (gr.g_sdf) {
         atomicAdd(&gr.g_sdf[i1], gw0);
         atomicAdd(&gr.g_sdf[i0], -gw1);
@@ -717,21 +793,26 @@ __global__ void vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__
     // edge normal (n_alpha) through the edge vector
     if (gr.g_nalpha && gr.g_deform) {
       float ev[3];
+#pragma unroll
       for (int a = 0; a < 3; ++a) ev[a] = xb[a] - xa[a];
       const float el = sqrtf(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
       const float L = el + 1e-8f;
-      const float ds = S[q][1] - S[q][0];
+      const float ds = S1[k] - S0[k];
       const float sg = ds > 0.f ? 1.f : (ds < 0.f ? -1.f : 0.f);
       float u[3], n[3];
+#pragma unroll
       for (int a = 0; a < 3; ++a) u[a] = ev[a] / L * sg;
       const float ul = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
       const float* gn = gr.g_nalpha + 3 * (g0 + q);
       if (ul > 1e-12f && el > 0.f) {
+#pragma unroll
         for (int a = 0; a < 3; ++a) n[a] = u[a] / ul;
         const float ndg = n[0] * gn[0] + n[1] * gn[1] + n[2] * gn[2];
         float ged[3];
+#pragma unroll
         for (int a = 0; a < 3; ++a) ged[a] = sg * (gn[a] - n[a] * ndg) / ul;
         const float gdot = ged[0] * ev[0] + ged[1] * ev[1] + ged[2] * ev[2];
+#pragma unroll
         for (int a = 0; a < 3; ++a) {
           const float gev = ged[a] / L - ev[a] * gdot / (L * L * el);
           atomicAdd(&gr.g_deform[3 * i1 + a], gev);
@@ -743,6 +824,7 @@ __global__ void vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__
       const float tb = tanhf(in.beta[12 * (int64_t)cube + e]);
       gr.g_beta[12 * (int64_t)cube + e] += gb * in.wscale * (1.f - tb * tb);
     }
+    ++q;
   }
 }
 
@@ -1032,7 +1114,10 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   // the two host reads take
   uint32_t* bad_index = w.misc + 1;
   A3D_CUDA_TRY(cudaMemsetAsync(bad_index, 0, sizeof(uint32_t), s));
-  corner_case_kernel<<<gsz(8 * n), 256, 0, s>>>(in, w.cases, w.flag, bad_index);
+  if (((uintptr_t)in.cidx & 15u) == 0)
+    corner_case_kernel<true><<<gsz(n), 256, 0, s>>>(in, w.cases, w.flag, bad_index);
+  else
+    corner_case_kernel<false><<<gsz(n), 256, 0, s>>>(in, w.cases, w.flag, bad_index);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flag, w.off, n, w.scan_tmp, w.off + n, s)));
   // stage B over all N cubes with the surface count on the device

@@ -304,14 +304,14 @@ def tune_coverage(lb: "LearnedBound", mesh, x: torch.Tensor, dist: torch.Tensor,
 
 
 def train_for_mesh(mesh, samples: torch.Tensor, epochs: int = 8, coverage: float = 0.995, seed: int = 0,
-                   tune: bool = False, log_space: bool = False):
+                   tune: bool = False, log_space: bool = False, sigma: float = 1.5, lr: float = 2e-3):
     """Fit a LearnedBound on plain-traversal distances of ``samples``: a
     random 90% trains it, the other 10% sets its margin.  With ``tune`` the
     bound's scale and the margin's coverage are picked by timing the
     traversal on the held-out samples."""
     lo = mesh.get_bounds()[0].cpu()
     hi = mesh.get_bounds()[1].cpu()
-    lb = LearnedBound(lo, hi, device=mesh.device, seed=seed, log_space=log_space)
+    lb = LearnedBound(lo, hi, device=mesh.device, seed=seed, log_space=log_space, sigma=sigma)
     n = samples.shape[0]
     ntr = int(n * 0.9)
     x = samples.to(mesh.device, torch.float32)
@@ -320,7 +320,7 @@ def train_for_mesh(mesh, samples: torch.Tensor, epochs: int = 8, coverage: float
     # whatever order they come in
     perm = torch.randperm(n, generator=torch.Generator().manual_seed(seed + 1)).to(mesh.device)
     tr, ho = perm[:ntr], perm[ntr:]
-    lb.fit(x[tr], d[tr], epochs=epochs, seed=seed)
+    lb.fit(x[tr], d[tr], epochs=epochs, seed=seed, lr=lr)
     lb.calibrate(x[ho], d[ho], coverage=coverage)
     lb.coverage = coverage
     if tune:

@@ -146,6 +146,9 @@ class _DmcFn(torch.autograd.Function):
         ctx.vfeat = vfeat
         ctx.has = (deform is not None, alpha is not None, beta is not None)
         ctx.mark_non_differentiable(faces)
+        # outputs the loss does not use arrive as None (null pointers to the
+        # backward kernels) instead of zero tensors filled per call
+        ctx.set_materialize_grads(False)
         return verts, faces, ldev, pa, na, vf
 
     @staticmethod
