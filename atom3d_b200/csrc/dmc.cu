@@ -281,13 +281,14 @@ __global__ void cross_write_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev
     m &= m - 1;
     int64_t i0, i1;
     edge_ends(in, i, e, i0, i1);
-    keys[o] = (uint64_t)i0 * (uint64_t)in.m + (uint64_t)i1;
+    keys[o] = ((uint64_t)i0 << 32) | (uint64_t)i1;
     vals[o] = (uint32_t)(t * 12 + e);
     ++o;
   }
 }
 
-// Sort of the crossing entries by (key, val), key = i0 * M + i1 with i0 < i1,
+// Sort of the crossing entries by (key, val), key = i0 << 32 | i1 with i0 < i1
+// (corner ids are below 2^31, so the order is that of the pair (i0, i1)),
 // as a counting sort on the lower endpoint i0: each corner is the lower
 // endpoint of at most 6 grid edges, each shared by at most 4 cubes, so a
 // group holds at most 24 entries and every entry finds its place by ranking
@@ -297,7 +298,7 @@ __global__ void edge_count_kernel(const uint64_t* __restrict__ keys, int64_t nc,
                                   uint32_t* __restrict__ lo_of, uint32_t* __restrict__ cnt) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nc) return;
-  const uint32_t i0 = (uint32_t)(keys[j] / m);
+  const uint32_t i0 = (uint32_t)(keys[j] >> 32);
   lo_of[j] = i0;
   atomicAdd(&cnt[i0], 1u);
 }
@@ -349,8 +350,8 @@ __global__ void run_info_kernel(const uint64_t* __restrict__ k, const uint32_t* 
   const uint32_t r = rid[j] + flag[j] - 1u;
   idx_map[v[j]] = (int32_t)r;
   if (flag[j]) {
-    e0[r] = (int64_t)(k[j] / (uint64_t)m);
-    e1[r] = (int64_t)(k[j] % (uint64_t)m);
+    e0[r] = (int64_t)(k[j] >> 32);
+    e1[r] = (int64_t)(k[j] & 0xffffffffull);
     rfirst[r] = (uint32_t)j;
   }
 }
@@ -446,132 +447,169 @@ __device__ __forceinline__ void edge_normal(const float* x0, const float* x1, fl
 
 __device__ __forceinline__ float ldf(const float* p, int64_t i) { return __ldg(p + i); }
 
-// one thread per dual vertex: crossings, weighted average, L_dev.  The edge
-// loop is unrolled over the 7 table slots, so each edge's plain crossing
-// and distance stay in registers for the L_dev pass (one gather per edge).
-__global__ void vd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
-                          const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
-                          const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
-                          VdOut out) {
-  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= nv) return;
-  const uint32_t t = vd_cube[v];
-  const int j = vd_slot[v];
-  const int c = case_s[t];
-  const uint32_t vedges = vd_edges(c, j);
-  const uint32_t cube = list[t];
-  const float ws = world_scale(in);
-  float vx[3];
-  load_voxel(in, cube, vx);
-  const int64_t g0 = goff[v];
-  float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
-  float z[7][3];
-  int64_t g = g0;
-  // the dependent gathers level by level over the slots, so each level's
-  // loads of all edges are in flight together
-  int32_t R[7], I0[7], I1[7];
+// Eight lanes per dual vertex, lane k owning table slot k (lane 7 idle): a
+// vertex's up to 7 crossings are gathered and evaluated on separate lanes,
+// and the per-vertex sums (weighted average, mean crossing distance) are
+// folded through shuffles in slot order, so their roundings are those of a
+// sequential loop over the slots.  A vertex's crossings are consecutive in
+// the per-crossing outputs, so its lanes write consecutive entries.
+constexpr int kVdThreads = 256;  // 32 dual vertices per block
+
+// sum of x over the slots of this lane's 8-lane group that hold an edge, in
+// slot order; every lane of the group gets the sum
+__device__ __forceinline__ float slot_sum(float x, uint32_t emask, int base) {
+  float acc = 0.f;
 #pragma unroll
   for (int k = 0; k < 7; ++k) {
-    const int e = vd_edge(vedges, k);
-    R[k] = e == 15 ? 0 : ed.idx_map[(int64_t)t * 12 + e];
+    const float y = __shfl_sync(0xffffffffu, x, base + k);
+    if ((emask >> k) & 1u) acc = fa(acc, y);
   }
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    const bool has = vd_edge(vedges, k) != 15;
-    I0[k] = has ? (int32_t)ed.e0[R[k]] : 0;
-    I1[k] = has ? (int32_t)ed.e1[R[k]] : 0;
+  return acc;
+}
+
+// the setup a vertex's 8 lanes share: its cube, case slot and edge list
+struct VdLane {
+  int64_t v, g;       // dual vertex; this lane's crossing index
+  uint32_t t, cube;   // surface-cube rank and cube index
+  uint32_t emask;     // slots that hold an edge
+  int e;              // this lane's cube edge, 15 = none
+  int base;           // first lane of the group in the warp
+  bool live;
+};
+
+__device__ __forceinline__ VdLane vd_lane(int64_t nv, const uint32_t* __restrict__ list,
+                                          const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
+                                          const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff) {
+  VdLane L;
+  const int lane = threadIdx.x & 31, k = lane & 7;
+  L.base = lane & ~7;
+  L.v = ((int64_t)blockIdx.x * kVdThreads + threadIdx.x) >> 3;
+  L.live = L.v < nv;
+  uint32_t vedges = 0xffffffffu;
+  L.t = 0;
+  L.cube = 0;
+  int64_t g0 = 0;
+  if (L.live) {
+    L.t = vd_cube[L.v];
+    vedges = vd_edges(case_s[L.t], vd_slot[L.v]);
+    L.cube = list[L.t];
+    g0 = goff[L.v];
   }
-  float S0[7], S1[7];
+  L.emask = 0;
 #pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    const bool has = vd_edge(vedges, k) != 15;
-    S0[k] = has ? fsb(ldf(in.sdf, I0[k]), in.iso) : 0.f;
-    S1[k] = has ? fsb(ldf(in.sdf, I1[k]), in.iso) : 0.f;
-  }
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    const int e = vd_edge(vedges, k);
-    if (e == 15) continue;
-    const int64_t flat = (int64_t)t * 12 + e;
-    const int64_t i0 = I0[k], i1 = I1[k];
-    const float s0 = S0[k], s1 = S1[k];
-    const float a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
-    const float a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
-    const float b = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
+  for (int q = 0; q < 7; ++q)
+    if (vd_edge(vedges, q) != 15) L.emask |= 1u << q;
+  L.e = k < 7 ? vd_edge(vedges, k) : 15;
+  L.g = g0 + __popc(L.emask & ((1u << k) - 1u));
+  return L;
+}
+
+__global__ void __launch_bounds__(kVdThreads)
+    vd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
+              const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
+              const uint32_t* __restrict__ goff, EdgeData ed, VdOut out) {
+  const VdLane L = vd_lane(nv, list, case_s, vd_cube, vd_slot, goff);
+  const bool has = L.e != 15;
+  float ue[3] = {0.f, 0.f, 0.f}, z[3] = {0.f, 0.f, 0.f}, b = 0.f;
+  if (has) {
+    const int e = L.e;
+    const int64_t flat = (int64_t)L.t * 12 + e;
+    const int32_t r = ed.idx_map[flat];
+    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
+    const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
+    const float a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)L.cube + kCE[2 * e]], in.wscale, true) : 1.f;
+    const float a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)L.cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
+    b = in.beta ? norm_w(in.beta[12 * (int64_t)L.cube + e], in.wscale, true) : 1.f;
     const float w0 = fm(s1, a1), w1 = -fm(s0, a0);
     const float den = fa(w0, w1);
     const float pw0 = s1, pw1 = -s0, pden = fa(pw0, pw1);
-    float xa[3], xb[3], n[3];
-    edge_world(in, ws, vx, e, i0, i1, xa, xb);
+    float vx[3], xa[3], xb[3], n[3];
+    load_voxel(in, L.cube, vx);
+    edge_world(in, world_scale(in), vx, e, i0, i1, xa, xb);
     edge_normal(xa, xb, s0, s1, n);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float ue = interp1(xa[a], xb[a], w0, w1, den);
-      out.palpha[3 * g + a] = ue;
-      out.nalpha[3 * g + a] = n[a];
-      acc[a] = fa(acc[a], fm(ue, b));
-      z[k][a] = interp1(xa[a], xb[a], pw0, pw1, pden);  // the plain zero crossing
+      ue[a] = interp1(xa[a], xb[a], w0, w1, den);
+      out.palpha[3 * L.g + a] = ue[a];
+      out.nalpha[3 * L.g + a] = n[a];
+      z[a] = interp1(xa[a], xb[a], pw0, pw1, pden);  // the plain zero crossing
     }
-    bsum = fa(bsum, b);
-    out.vd_map[flat] = (int32_t)v;
-    ++g;
+    out.vd_map[flat] = (int32_t)L.v;
   }
-  const int64_t ne = g - g0;
   float vd[3];
-  const float den = fa(bsum, 1e-8f);
+  const float bden = fa(slot_sum(b, L.emask, L.base), 1e-8f);
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    vd[a] = fd(acc[a], den);
-    out.verts[3 * v + a] = vd[a];
-  }
+  for (int a = 0; a < 3; ++a) vd[a] = fd(slot_sum(fm(ue[a], b), L.emask, L.base), bden);
+  const int k = threadIdx.x & 7;
+  if (L.live && k < 3) out.verts[3 * L.v + k] = k == 0 ? vd[0] : (k == 1 ? vd[1] : vd[2]);
   // L_dev: distances of the plain zero crossings to the dual vertex
-  float msum = 0.f;
-  float dist[7];
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    if (vd_edge(vedges, k) == 15) continue;
+  float dist = 0.f;
+  if (has) {
     float d2 = 0.f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float dd = fsb(z[k][a], vd[a]);
+      const float dd = fsb(z[a], vd[a]);
       d2 = fa(d2, fm(dd, dd));
     }
-    dist[k] = sqrtf(d2);
-    msum = fa(msum, dist[k]);
+    dist = sqrtf(d2);
   }
-  const float mean = fd(msum, (float)ne);
-  g = g0;
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    if (vd_edge(vedges, k) == 15) continue;
-    out.ldev[g++] = fabsf(fsb(dist[k], mean));
+  const float msum = slot_sum(dist, L.emask, L.base);
+  if (has) {
+    const float mean = fd(msum, (float)__popc(L.emask));
+    out.ldev[L.g] = fabsf(fsb(dist, mean));
   }
 }
 
-__global__ void quad_kernel(int64_t ne, int64_t nc, const uint32_t* __restrict__ qflag, const uint32_t* __restrict__ qoff,
-                            const uint32_t* __restrict__ rfirst, const uint32_t* __restrict__ vals,
-                            const int32_t* __restrict__ vd_map, const int64_t* __restrict__ e0,
-                            const float* __restrict__ sdf, float iso, int64_t nvd, float* __restrict__ verts,
-                            int64_t* __restrict__ faces, int32_t* __restrict__ quads) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= ne || !qflag[r]) return;
-  const int64_t q = qoff[r];
-  int32_t v[4];
-  for (int k = 0; k < 4; ++k) v[k] = vd_map[vals[rfirst[r] + k]];
-  const bool flip = fsb(sdf[e0[r]], iso) > 0.f;
-  int32_t o[4];
-  if (flip) { o[0] = v[0]; o[1] = v[1]; o[2] = v[3]; o[3] = v[2]; }
-  else { o[0] = v[2]; o[1] = v[3]; o[2] = v[1]; o[3] = v[0]; }
-  const int64_t cidx = nvd + q;
-  float s[3] = {0.f, 0.f, 0.f};
-  for (int k = 0; k < 4; ++k) {
-    quads[4 * q + k] = o[k];
-    for (int a = 0; a < 3; ++a) s[a] = fa(s[a], verts[3 * (int64_t)o[k] + a]);
-    faces[3 * (4 * q + k)] = o[k];
-    faces[3 * (4 * q + k) + 1] = o[(k + 1) & 3];
-    faces[3 * (4 * q + k) + 2] = cidx;
+// Quads from the unique edges shared by four surface cubes, one thread per
+// unique edge.  A block's quads occupy one contiguous range of the outputs
+// (qoff is the exclusive scan of the quad flags), so the block stages its
+// faces, quad corners and centre vertices in shared memory and writes each
+// range with consecutive threads on consecutive words.
+constexpr int kQuadThreads = 256;
+__global__ void __launch_bounds__(kQuadThreads)
+    quad_kernel(int64_t ne, int64_t nc, const uint32_t* __restrict__ qflag, const uint32_t* __restrict__ qoff,
+                const uint32_t* __restrict__ rfirst, const uint32_t* __restrict__ vals,
+                const int32_t* __restrict__ vd_map, const int64_t* __restrict__ e0, const float* __restrict__ sdf,
+                float iso, int64_t nvd, float* __restrict__ verts, int64_t* __restrict__ faces,
+                int32_t* __restrict__ quads) {
+  __shared__ int32_t s_quad[kQuadThreads][4];
+  __shared__ float s_ctr[kQuadThreads * 3];
+  const int64_t r0 = (int64_t)blockIdx.x * kQuadThreads;
+  const int64_t r = r0 + threadIdx.x;
+  const int64_t r_end = r0 + kQuadThreads < ne ? r0 + kQuadThreads : ne;
+  const int64_t q0 = qoff[r0];
+  const int cnt = (int)(qoff[r_end] - q0);  // quads of this block
+  if (r < ne && qflag[r]) {
+    const int l = (int)(qoff[r] - q0);
+    int32_t v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = vd_map[vals[rfirst[r] + k]];
+    const bool flip = fsb(sdf[e0[r]], iso) > 0.f;
+    int32_t o[4];
+    if (flip) { o[0] = v[0]; o[1] = v[1]; o[2] = v[3]; o[3] = v[2]; }
+    else { o[0] = v[2]; o[1] = v[3]; o[2] = v[1]; o[3] = v[0]; }
+    float sacc[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      s_quad[l][k] = o[k];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) sacc[a] = fa(sacc[a], verts[3 * (int64_t)o[k] + a]);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) s_ctr[3 * l + a] = fm(sacc[a], 0.25f);
   }
-  for (int a = 0; a < 3; ++a) verts[3 * cidx + a] = fm(s[a], 0.25f);
+  __syncthreads();
+  // quad corners [cnt][4] int32
+  for (int i = threadIdx.x; i < 4 * cnt; i += kQuadThreads) quads[4 * q0 + i] = s_quad[i >> 2][i & 3];
+  // faces [4 cnt][3] int64: triangle k of quad l = (o[k], o[k+1], centre)
+  for (int i = threadIdx.x; i < 12 * cnt; i += kQuadThreads) {
+    const int l = i / 12, rem = i - 12 * l, k = rem / 3, col = rem - 3 * k;
+    const int64_t val = col == 0 ? (int64_t)s_quad[l][k]
+                                 : (col == 1 ? (int64_t)s_quad[l][(k + 1) & 3] : nvd + q0 + l);
+    faces[12 * q0 + i] = val;
+  }
+  // centre vertices [cnt][3] after the dual vertices
+  for (int i = threadIdx.x; i < 3 * cnt; i += kQuadThreads) verts[3 * (nvd + q0) + i] = s_ctr[i];
 }
 
 // ---- adjoint ------------------------------------------------------------------
@@ -615,216 +653,176 @@ __device__ __forceinline__ void scatter_interp_grad(const DmcIn& in, const float
   }
 }
 
-// One thread per dual vertex.  The forward quantities are recomputed per
-// table slot k (0..6, unrolled, so every per-edge value lives in a register
-// indexed by a compile-time slot instead of a local-memory array); slots
-// without an edge are skipped.  Gradient order per edge as the forward's
-// reverse: L_dev -> distances -> plain crossings and the dual vertex ->
-// weighted average -> interpolation weights -> sdf, deform, alpha, beta.
-__global__ void vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
-                              const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
-                              const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
-                              DmcGrad gr) {
-  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= nv) return;
-  const uint32_t t = vd_cube[v];
-  const int j = vd_slot[v];
-  const int c = case_s[t];
-  const uint32_t vedges = vd_edges(c, j);
-  const uint32_t cube = list[t];
+// Eight lanes per dual vertex as in vd_kernel: lane k recomputes the
+// forward quantities of slot k's crossing; the per-vertex reductions (dual
+// vertex, mean distance, the L_dev and distance adjoints folded into the
+// vertex's gradient) run through shuffles in slot order; each lane then
+// scatters its own crossing's adjoint into sdf, deform, alpha and beta.
+// Gradient order as the forward's reverse: L_dev -> distances -> plain
+// crossings and the dual vertex -> weighted average -> interpolation weights.
+__global__ void __launch_bounds__(kVdThreads)
+    vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
+                  const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
+                  const uint32_t* __restrict__ goff, EdgeData ed, DmcGrad gr) {
+  const VdLane L = vd_lane(nv, list, case_s, vd_cube, vd_slot, goff);
+  const bool has = L.e != 15;
+  const int e = has ? L.e : 0;
+  const uint32_t FULL = 0xffffffffu;
+  int64_t i0 = 0, i1 = 0;
+  float S0 = 0.f, S1 = 0.f, A0 = 1.f, A1 = 1.f, B = 0.f;
+  float UE[3] = {0.f, 0.f, 0.f}, Z[3] = {0.f, 0.f, 0.f}, vx[3] = {0.f, 0.f, 0.f};
   const float ws = world_scale(in);
-  float vx[3];
-  load_voxel(in, cube, vx);
-  const int64_t g0 = goff[v];
-  // gathers level by level over the slots (independent loads in flight)
-  int32_t R[7];
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    const int e = vd_edge(vedges, k);
-    R[k] = e == 15 ? 0 : ed.idx_map[(int64_t)t * 12 + e];
-  }
-  int32_t I0[7], I1[7];
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    const bool has = vd_edge(vedges, k) != 15;
-    I0[k] = has ? (int32_t)ed.e0[R[k]] : 0;
-    I1[k] = has ? (int32_t)ed.e1[R[k]] : 0;
-  }
-  float S0[7], S1[7], A0[7], A1[7], B[7];
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    const int e = vd_edge(vedges, k);
-    const bool has = e != 15;
-    const int ee = has ? e : 0;  // a valid table index for the empty slots
-    S0[k] = has ? fsb(ldf(in.sdf, I0[k]), in.iso) : 0.f;
-    S1[k] = has ? fsb(ldf(in.sdf, I1[k]), in.iso) : 0.f;
-    A0[k] = (has && in.alpha) ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * ee]], in.wscale, true) : 1.f;
-    A1[k] = (has && in.alpha) ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * ee + 1]], in.wscale, true) : 1.f;
-    B[k] = (has && in.beta) ? norm_w(in.beta[12 * (int64_t)cube + ee], in.wscale, true) : 1.f;
-  }
-  // forward: weighted average of the alpha-weighted crossings
-  float UE[7][3], Z[7][3];
-  float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
-  int ne = 0;
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    const int e = vd_edge(vedges, k);
-    if (e == 15) continue;
-    const float w0 = fm(S1[k], A1[k]), w1 = -fm(S0[k], A0[k]), den = fa(w0, w1);
-    const float pw0 = S1[k], pw1 = -S0[k], pden = fa(pw0, pw1);
+  if (has) {
+    const int32_t r = ed.idx_map[(int64_t)L.t * 12 + e];
+    i0 = ed.e0[r];
+    i1 = ed.e1[r];
+    S0 = fsb(ldf(in.sdf, i0), in.iso);
+    S1 = fsb(ldf(in.sdf, i1), in.iso);
+    A0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)L.cube + kCE[2 * e]], in.wscale, true) : 1.f;
+    A1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)L.cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
+    B = in.beta ? norm_w(in.beta[12 * (int64_t)L.cube + e], in.wscale, true) : 1.f;
+    const float w0 = fm(S1, A1), w1 = -fm(S0, A0), den = fa(w0, w1);
+    const float pw0 = S1, pw1 = -S0, pden = fa(pw0, pw1);
     float pa[3], pb[3];
-    edge_world(in, ws, vx, e, I0[k], I1[k], pa, pb);
+    load_voxel(in, L.cube, vx);
+    edge_world(in, ws, vx, e, i0, i1, pa, pb);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      UE[k][a] = interp1(pa[a], pb[a], w0, w1, den);
-      Z[k][a] = interp1(pa[a], pb[a], pw0, pw1, pden);
-      acc[a] = fa(acc[a], fm(UE[k][a], B[k]));
+      UE[a] = interp1(pa[a], pb[a], w0, w1, den);
+      Z[a] = interp1(pa[a], pb[a], pw0, pw1, pden);
     }
-    bsum = fa(bsum, B[k]);
-    ++ne;
   }
-  const float bden = fa(bsum, 1e-8f);
+  const float bden = fa(slot_sum(B, L.emask, L.base), 1e-8f);
   float vd[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) vd[a] = fd(acc[a], bden);
+  for (int a = 0; a < 3; ++a) vd[a] = fd(slot_sum(fm(UE[a], B), L.emask, L.base), bden);
   // incoming gradient of the dual vertex
   float gvd[3] = {0.f, 0.f, 0.f};
-  if (gr.g_verts)
+  if (gr.g_verts && L.live)
 #pragma unroll
-    for (int a = 0; a < 3; ++a) gvd[a] = gr.g_verts[3 * v + a] + gr.g_vd[3 * v + a];
+    for (int a = 0; a < 3; ++a) gvd[a] = gr.g_verts[3 * L.v + a] + gr.g_vd[3 * L.v + a];
   // L_dev backward (mad = |dist - mean|, mean = sum(dist)/ne)
-  float D[7], gD[7];
-  float msum = 0.f;
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    D[k] = 0.f;
-    gD[k] = 0.f;
-    if (vd_edge(vedges, k) == 15) continue;
+  float D = 0.f;
+  if (has) {
     float d2 = 0.f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float dd = fsb(Z[k][a], vd[a]);
+      const float dd = fsb(Z[a], vd[a]);
       d2 = fa(d2, fm(dd, dd));
     }
-    D[k] = sqrtf(d2);
-    msum = fa(msum, D[k]);
+    D = sqrtf(d2);
   }
-  const float mean = fd(msum, (float)ne);
+  const int ne = __popc(L.emask);
+  const float mean = fd(slot_sum(D, L.emask, L.base), (float)ne);
+  float gD = 0.f;
   if (gr.g_ldev) {
+    float x = 0.f;
+    if (has) {
+      const float gl = gr.g_ldev[L.g];
+      const float df = D - mean;
+      const float sg = df > 0.f ? 1.f : (df < 0.f ? -1.f : 0.f);
+      x = gl * sg;
+    }
+    gD = x;
     float gmean = 0.f;
-    int q = 0;
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
-      if (vd_edge(vedges, k) == 15) continue;
-      const float gl = gr.g_ldev[g0 + q];
-      const float df = D[k] - mean;
-      const float sg = df > 0.f ? 1.f : (df < 0.f ? -1.f : 0.f);
-      gD[k] += gl * sg;
-      gmean -= gl * sg;
-      ++q;
+      const float y = __shfl_sync(FULL, x, L.base + k);
+      if ((L.emask >> k) & 1u) gmean -= y;
     }
-    const float gm = gmean / (float)ne;
-#pragma unroll
-    for (int k = 0; k < 7; ++k)
-      if (vd_edge(vedges, k) != 15) gD[k] += gm;
+    gD += gmean / (float)ne;
   }
-  // dist -> crossing z (gZ, kept in Z's registers' place) and the dual vertex
-  float gZ[7][3];
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) gZ[k][a] = 0.f;
-    if (vd_edge(vedges, k) == 15) continue;
-    const float invd = D[k] > 0.f ? 1.0f / D[k] : 0.f;
+  // dist -> crossing z and the dual vertex
+  float gZ[3];
+  {
+    const float invd = D > 0.f ? 1.0f / D : 0.f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float u = (Z[k][a] - vd[a]) * invd;
-      gZ[k][a] = gD[k] * u;
-      gvd[a] -= gD[k] * u;
+      const float u = (Z[a] - vd[a]) * invd;
+      gZ[a] = has ? gD * u : 0.f;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) {
+        const float y = __shfl_sync(FULL, gZ[a], L.base + k);
+        if ((L.emask >> k) & 1u) gvd[a] -= y;
+      }
     }
   }
+  if (!has) return;  // no shuffles below
   // vd = sum(b ue) / (sum b + 1e-8)
   const float inv_bden = 1.0f / bden;
   float gB = 0.f;
 #pragma unroll
   for (int a = 0; a < 3; ++a) gB -= gvd[a] * vd[a] * inv_bden;
-  int q = 0;
+  float gue[3];
+  float gb = gB;
 #pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    const int e = vd_edge(vedges, k);
-    if (e == 15) continue;
-    const int64_t i0 = I0[k], i1 = I1[k];
-    float gue[3];
-    float gb = gB;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      gue[a] = gvd[a] * B[k] * inv_bden;
-      if (gr.g_palpha) gue[a] += gr.g_palpha[3 * (g0 + q) + a];
-      gb += gvd[a] * UE[k][a] * inv_bden;
+  for (int a = 0; a < 3; ++a) {
+    gue[a] = gvd[a] * B * inv_bden;
+    if (gr.g_palpha) gue[a] += gr.g_palpha[3 * L.g + a];
+    gb += gvd[a] * UE[a] * inv_bden;
+  }
+  float xa[3], xb[3];
+  edge_world(in, ws, vx, e, i0, i1, xa, xb);
+  // ue through w0 = s1 a1, w1 = -s0 a0
+  {
+    const float w0 = S1 * A1, w1 = -(S0 * A0), den = w0 + w1;
+    float gw0, gw1;
+    scatter_interp_grad(in, gue, xa, xb, UE, w0, w1, den, i0, i1, gw0, gw1, gr);
+    if (gr.g_sdf) {
+      atomicAdd(&gr.g_sdf[i1], gw0 * A1);
+      atomicAdd(&gr.g_sdf[i0], -gw1 * A0);
     }
-    float xa[3], xb[3];
-    edge_world(in, ws, vx, e, i0, i1, xa, xb);
-    // ue through w0 = s1 a1, w1 = -s0 a0
-    {
-      const float w0 = S1[k] * A1[k], w1 = -(S0[k] * A0[k]), den = w0 + w1;
-      float gw0, gw1;
-      scatter_interp_grad(in, gue, xa, xb, UE[k], w0, w1, den, i0, i1, gw0, gw1, gr);
-      if (gr.g_sdf) {
-        atomicAdd(&gr.g_sdf[i1], gw0 * A1[k]);
-        atomicAdd(&gr.g_sdf[i0], -gw1 * A0[k]);
-      }
-      if (gr.g_alpha && in.alpha) {
-        const int c0 = kCE[2 * e], c1 = kCE[2 * e + 1];
-        const float t0 = tanhf(in.alpha[8 * (int64_t)cube + c0]), t1 = tanhf(in.alpha[8 * (int64_t)cube + c1]);
-        atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c1], gw0 * S1[k] * in.wscale * (1.f - t1 * t1));
-        atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c0], -gw1 * S0[k] * in.wscale * (1.f - t0 * t0));
-      }
+    if (gr.g_alpha && in.alpha) {
+      const int c0 = kCE[2 * e], c1 = kCE[2 * e + 1];
+      const float t0 = tanhf(in.alpha[8 * (int64_t)L.cube + c0]), t1 = tanhf(in.alpha[8 * (int64_t)L.cube + c1]);
+      atomicAdd(&gr.g_alpha[8 * (int64_t)L.cube + c1], gw0 * S1 * in.wscale * (1.f - t1 * t1));
+      atomicAdd(&gr.g_alpha[8 * (int64_t)L.cube + c0], -gw1 * S0 * in.wscale * (1.f - t0 * t0));
     }
-    // plain crossing z through w0 = s1, w1 = -s0
-    {
-      const float w0 = S1[k], w1 = -S0[k], den = w0 + w1;
-      float gw0, gw1;
-      scatter_interp_grad(in, gZ[k], xa, xb, Z[k], w0, w1, den, i0, i1, gw0, gw1, gr);
-      if (gr.g_sdf) {
-        atomicAdd(&gr.g_sdf[i1], gw0);
-        atomicAdd(&gr.g_sdf[i0], -gw1);
-      }
+  }
+  // plain crossing z through w0 = s1, w1 = -s0 (nothing to add without an
+  // L_dev gradient: gZ is zero)
+  if (gr.g_ldev) {
+    const float w0 = S1, w1 = -S0, den = w0 + w1;
+    float gw0, gw1;
+    scatter_interp_grad(in, gZ, xa, xb, Z, w0, w1, den, i0, i1, gw0, gw1, gr);
+    if (gr.g_sdf) {
+      atomicAdd(&gr.g_sdf[i1], gw0);
+      atomicAdd(&gr.g_sdf[i0], -gw1);
     }
-    // edge normal (n_alpha) through the edge vector
-    if (gr.g_nalpha && gr.g_deform) {
-      float ev[3];
+  }
+  // edge normal (n_alpha) through the edge vector
+  if (gr.g_nalpha && gr.g_deform) {
+    float ev[3];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) ev[a] = xb[a] - xa[a];
-      const float el = sqrtf(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
-      const float L = el + 1e-8f;
-      const float ds = S1[k] - S0[k];
-      const float sg = ds > 0.f ? 1.f : (ds < 0.f ? -1.f : 0.f);
-      float u[3], n[3];
+    for (int a = 0; a < 3; ++a) ev[a] = xb[a] - xa[a];
+    const float el = sqrtf(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+    const float Ln = el + 1e-8f;
+    const float ds = S1 - S0;
+    const float sg = ds > 0.f ? 1.f : (ds < 0.f ? -1.f : 0.f);
+    float u[3], n[3];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) u[a] = ev[a] / L * sg;
-      const float ul = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-      const float* gn = gr.g_nalpha + 3 * (g0 + q);
-      if (ul > 1e-12f && el > 0.f) {
+    for (int a = 0; a < 3; ++a) u[a] = ev[a] / Ln * sg;
+    const float ul = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const float* gn = gr.g_nalpha + 3 * L.g;
+    if (ul > 1e-12f && el > 0.f) {
 #pragma unroll
-        for (int a = 0; a < 3; ++a) n[a] = u[a] / ul;
-        const float ndg = n[0] * gn[0] + n[1] * gn[1] + n[2] * gn[2];
-        float ged[3];
+      for (int a = 0; a < 3; ++a) n[a] = u[a] / ul;
+      const float ndg = n[0] * gn[0] + n[1] * gn[1] + n[2] * gn[2];
+      float ged[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) ged[a] = sg * (gn[a] - n[a] * ndg) / ul;
-        const float gdot = ged[0] * ev[0] + ged[1] * ev[1] + ged[2] * ev[2];
+      for (int a = 0; a < 3; ++a) ged[a] = sg * (gn[a] - n[a] * ndg) / ul;
+      const float gdot = ged[0] * ev[0] + ged[1] * ev[1] + ged[2] * ev[2];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const float gev = ged[a] / L - ev[a] * gdot / (L * L * el);
-          atomicAdd(&gr.g_deform[3 * i1 + a], gev);
-          atomicAdd(&gr.g_deform[3 * i0 + a], -gev);
-        }
+      for (int a = 0; a < 3; ++a) {
+        const float gev = ged[a] / Ln - ev[a] * gdot / (Ln * Ln * el);
+        atomicAdd(&gr.g_deform[3 * i1 + a], gev);
+        atomicAdd(&gr.g_deform[3 * i0 + a], -gev);
       }
     }
-    if (gr.g_beta && in.beta) {
-      const float tb = tanhf(in.beta[12 * (int64_t)cube + e]);
-      gr.g_beta[12 * (int64_t)cube + e] += gb * in.wscale * (1.f - tb * tb);
-    }
-    ++q;
+  }
+  if (gr.g_beta && in.beta) {
+    const float tb = tanhf(in.beta[12 * (int64_t)L.cube + e]);
+    gr.g_beta[12 * (int64_t)L.cube + e] += gb * in.wscale * (1.f - tb * tb);
   }
 }
 
@@ -1213,11 +1211,12 @@ extern "C" int a3d_dmc_emit(const a3d_dmc_inputs* p, void* workspace, size_t wor
   DmcIn in = make_in(p);
   EdgeData ed{w.e0, w.e1, w.idx_map};
   VdOut out{vertices, l_dev, p_alpha, n_alpha, w.vd_map};
-  vd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, out);
+  vd_kernel<<<gsz(8 * nv, kVdThreads), kVdThreads, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff,
+                                                           ed, out);
   A3D_LAUNCH_CHECK();
   (void)nc;
   if (nq > 0) {
-    quad_kernel<<<gsz(ne), 256, 0, s>>>(ne, nc, w.qflag, w.qoff, w.rfirst, w.vals, w.vd_map, w.e0, p->sdf, p->isovalue,
+    quad_kernel<<<gsz(ne, kQuadThreads), kQuadThreads, 0, s>>>(ne, nc, w.qflag, w.qoff, w.rfirst, w.vals, w.vd_map, w.e0, p->sdf, p->isovalue,
                                         nv, vertices, faces, w.quads);
     A3D_LAUNCH_CHECK();
   }
@@ -1245,7 +1244,8 @@ extern "C" int a3d_dmc_backward(const a3d_dmc_inputs* p, void* workspace, size_t
     A3D_LAUNCH_CHECK();
   }
   EdgeData ed{w.e0, w.e1, w.idx_map};
-  vd_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, gr);
+  vd_bwd_kernel<<<gsz(8 * nv, kVdThreads), kVdThreads, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot,
+                                                               w.goff, ed, gr);
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
@@ -1644,31 +1644,44 @@ __global__ void vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float
 }
 
 // 2 triangles per quad along the shorter diagonal
-__global__ void quad_eval_kernel(int64_t ne, const uint32_t* __restrict__ qflag, const uint32_t* __restrict__ qoff,
-                                 const uint32_t* __restrict__ rfirst, const uint32_t* __restrict__ vals,
-                                 const int32_t* __restrict__ vd_map, const int64_t* __restrict__ e0,
-                                 const float* __restrict__ sdf, float iso, const float* __restrict__ verts,
-                                 int64_t* __restrict__ faces) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= ne || !qflag[r]) return;
-  const int64_t q = qoff[r];
-  int32_t v[4];
-  for (int k = 0; k < 4; ++k) v[k] = vd_map[vals[rfirst[r] + k]];
-  const bool flip = fsb(sdf[e0[r]], iso) > 0.f;
-  int32_t o[4];
-  if (flip) { o[0] = v[0]; o[1] = v[1]; o[2] = v[3]; o[3] = v[2]; }
-  else { o[0] = v[2]; o[1] = v[3]; o[2] = v[1]; o[3] = v[0]; }
-  float l02 = 0.f, l13 = 0.f;
+// (one thread per unique edge; a block's faces form one contiguous range,
+// staged in shared memory and written coalesced, as in quad_kernel)
+__global__ void __launch_bounds__(kQuadThreads)
+    quad_eval_kernel(int64_t ne, const uint32_t* __restrict__ qflag, const uint32_t* __restrict__ qoff,
+                     const uint32_t* __restrict__ rfirst, const uint32_t* __restrict__ vals,
+                     const int32_t* __restrict__ vd_map, const int64_t* __restrict__ e0,
+                     const float* __restrict__ sdf, float iso, const float* __restrict__ verts,
+                     int64_t* __restrict__ faces) {
+  __shared__ int32_t s_tri[kQuadThreads][6];
+  const int64_t r0 = (int64_t)blockIdx.x * kQuadThreads;
+  const int64_t r = r0 + threadIdx.x;
+  const int64_t r_end = r0 + kQuadThreads < ne ? r0 + kQuadThreads : ne;
+  const int64_t q0 = qoff[r0];
+  const int cnt = (int)(qoff[r_end] - q0);
+  if (r < ne && qflag[r]) {
+    const int l = (int)(qoff[r] - q0);
+    int32_t v[4];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float d02 = fsb(verts[3 * (int64_t)o[0] + a], verts[3 * (int64_t)o[2] + a]);
-    const float d13 = fsb(verts[3 * (int64_t)o[1] + a], verts[3 * (int64_t)o[3] + a]);
-    l02 = fa(l02, fm(d02, d02));
-    l13 = fa(l13, fm(d13, d13));
+    for (int k = 0; k < 4; ++k) v[k] = vd_map[vals[rfirst[r] + k]];
+    const bool flip = fsb(sdf[e0[r]], iso) > 0.f;
+    int32_t o[4];
+    if (flip) { o[0] = v[0]; o[1] = v[1]; o[2] = v[3]; o[3] = v[2]; }
+    else { o[0] = v[2]; o[1] = v[3]; o[2] = v[1]; o[3] = v[0]; }
+    float l02 = 0.f, l13 = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float d02 = fsb(verts[3 * (int64_t)o[0] + a], verts[3 * (int64_t)o[2] + a]);
+      const float d13 = fsb(verts[3 * (int64_t)o[1] + a], verts[3 * (int64_t)o[3] + a]);
+      l02 = fa(l02, fm(d02, d02));
+      l13 = fa(l13, fm(d13, d13));
+    }
+    const bool m = sqrtf(l02) < sqrtf(l13);
+    const int s1[6] = {0, 1, 2, 0, 2, 3}, s2[6] = {0, 1, 3, 3, 1, 2};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s_tri[l][k] = o[m ? s1[k] : s2[k]];
   }
-  const bool m = sqrtf(l02) < sqrtf(l13);
-  const int s1[6] = {0, 1, 2, 0, 2, 3}, s2[6] = {0, 1, 3, 3, 1, 2};
-  for (int k = 0; k < 6; ++k) faces[6 * q + k] = o[m ? s1[k] : s2[k]];
+  __syncthreads();
+  for (int i = threadIdx.x; i < 6 * cnt; i += kQuadThreads) faces[6 * q0 + i] = (int64_t)s_tri[i / 6][i % 6];
 }
 
 }  // namespace
@@ -1749,7 +1762,7 @@ extern "C" int a3d_dmc_emit_qef(const a3d_dmc_inputs* p, void* workspace, size_t
                                              w.vd_cube, w.vd_slot, w.goff, ed, out);
   A3D_LAUNCH_CHECK();
   if (nq > 0) {
-    quad_eval_kernel<<<gsz(ne), 256, 0, s>>>(ne, w.qflag, w.qoff, w.rfirst, w.vals, w.vd_map, w.e0, p->sdf,
+    quad_eval_kernel<<<gsz(ne, kQuadThreads), kQuadThreads, 0, s>>>(ne, w.qflag, w.qoff, w.rfirst, w.vals, w.vd_map, w.e0, p->sdf,
                                              p->isovalue, vertices, faces);
     A3D_LAUNCH_CHECK();
   }

@@ -96,26 +96,46 @@ __global__ void scan_tile_sums_kernel(T* __restrict__ sums, int64_t nb, T* __res
   if (threadIdx.x == 0 && total) *total = tot;
 }
 
+// The tile passes through shared memory: loaded and stored with consecutive
+// threads on consecutive elements (coalesced), scanned with each thread
+// owning kScanItems consecutive elements (one padding slot per 32 keeps the
+// per-thread reads off a single bank).  out may alias in: a block reads its
+// whole tile before writing it.
+__host__ __device__ constexpr int scan_pad(int i) { return i + (i >> 5); }
+
 template <typename TIn, typename T>
 __global__ void scan_tile_down_kernel(const TIn* __restrict__ in, T* __restrict__ out, int64_t n,
                                       const T* __restrict__ tile_offsets) {
   __shared__ T s_warp[kBlockScanSlots];
+  __shared__ T s_tile[scan_pad(kScanTile)];
   const int64_t base = (int64_t)blockIdx.x * kScanTile;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int li = i * kScanThreads + threadIdx.x;
+    const int64_t idx = base + li;
+    s_tile[scan_pad(li)] = idx < n ? (T)in[idx] : T(0);
+  }
+  __syncthreads();
   // each thread owns kScanItems consecutive elements
   T vals[kScanItems];
   T acc = 0;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    int64_t idx = base + (int64_t)threadIdx.x * kScanItems + i;
-    vals[i] = idx < n ? (T)in[idx] : T(0);
+    vals[i] = s_tile[scan_pad(threadIdx.x * kScanItems + i)];
     acc += vals[i];
   }
   T run = block_exclusive_scan<T>(acc, s_warp, (T*)nullptr) + tile_offsets[blockIdx.x];
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    int64_t idx = base + (int64_t)threadIdx.x * kScanItems + i;
-    if (idx < n) out[idx] = run;
+    s_tile[scan_pad(threadIdx.x * kScanItems + i)] = run;
     run += vals[i];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int li = i * kScanThreads + threadIdx.x;
+    const int64_t idx = base + li;
+    if (idx < n) out[idx] = s_tile[scan_pad(li)];
   }
 }
 
