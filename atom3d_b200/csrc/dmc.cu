@@ -231,11 +231,6 @@ __global__ void case_fix_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, c
   case_s[t] = (uint8_t)out;
 }
 
-__device__ __forceinline__ void edge_ends(const DmcIn& in, uint32_t cube, int e, int64_t& i0, int64_t& i1) {
-  i0 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e]);
-  i1 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e + 1]);
-}
-
 // positions of the ends of cube edge e of a cube at voxel vx.  A unique
 // edge's corner ids (i0, i1) come from the key (cube_idx[c0], cube_idx[c1])
 // of the cube's own local corners c0 = kCE[2e], c1 = kCE[2e+1] (a cube whose
@@ -268,22 +263,45 @@ __global__ void cross_count_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev
   cnt[t] = (uint32_t)__popc(m);
 }
 
-__global__ void cross_write_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
-                                   const uint16_t* __restrict__ mask12, const uint32_t* __restrict__ off,
-                                   uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)*ns_dev) return;
-  const uint32_t i = list[t];
-  uint32_t m = mask12[t];
-  uint32_t o = off[t];
-  while (m) {
-    const int e = __ffs(m) - 1;
-    m &= m - 1;
-    int64_t i0, i1;
-    edge_ends(in, i, e, i0, i1);
-    keys[o] = ((uint64_t)i0 << 32) | (uint64_t)i1;
-    vals[o] = (uint32_t)(t * 12 + e);
-    ++o;
+// Crossing entries (key, val) of the surface cubes, val = t * 12 + e in edge
+// order.  A block's entries form one contiguous range of the output (off is
+// the exclusive scan of the per-cube counts), so they are staged in shared
+// memory and written with consecutive threads on consecutive entries.
+constexpr int kCrossThreads = 128;
+__global__ void __launch_bounds__(kCrossThreads)
+    cross_write_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
+                       const uint16_t* __restrict__ mask12, const uint32_t* __restrict__ off,
+                       uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  __shared__ uint64_t s_key[kCrossThreads * 12];
+  __shared__ uint32_t s_val[kCrossThreads * 12];
+  const int64_t ns = (int64_t)*ns_dev;
+  const int64_t t0 = (int64_t)blockIdx.x * kCrossThreads, t = t0 + threadIdx.x;
+  if (t0 >= ns) return;  // the whole block is past the surface cubes
+  const int64_t t_end = t0 + kCrossThreads < ns ? t0 + kCrossThreads : ns;
+  const uint32_t o0 = off[t0];
+  const int cnt = (int)(off[t_end] - o0);
+  if (t < ns) {
+    const uint32_t i = list[t];
+    const uint32_t m = mask12[t];
+    int64_t id[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) id[c] = corner_at(in, 8 * (int64_t)i + c);
+    // the cube edge table (kCE) as a compile-time array, so the unrolled
+    // loop indexes the corner ids in registers
+    constexpr unsigned char ce[24] = {0, 1, 1, 5, 4, 5, 0, 4, 2, 3, 3, 7, 6, 7, 2, 6, 2, 0, 3, 1, 7, 5, 6, 4};
+    int o = (int)(off[t] - o0);
+#pragma unroll
+    for (int e = 0; e < 12; ++e) {
+      if (!((m >> e) & 1u)) continue;
+      s_key[o] = ((uint64_t)id[ce[2 * e]] << 32) | (uint64_t)id[ce[2 * e + 1]];
+      s_val[o] = (uint32_t)(t * 12 + e);
+      ++o;
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < cnt; k += kCrossThreads) {
+    keys[o0 + k] = s_key[k];
+    vals[o0 + k] = s_val[k];
   }
 }
 
@@ -414,6 +432,34 @@ __global__ void vd_assign_kernel(int64_t ns, const uint8_t* __restrict__ case_s,
   }
 }
 
+// Dual vertex of crossing entry val = t * 12 + e (surface cube t, cube edge
+// e): the cube's first vertex in the class numbering of vd_assign_kernel
+// plus the slot of the cube's case whose edge list holds e.  Computed where
+// it is needed instead of stored per (cube, edge).
+struct VdNumbering {
+  const uint8_t* case_s;
+  const uint64_t* ra;  // exclusive scans of the class words, totals at [ns]
+  const uint64_t* rb;
+  int64_t ns;
+  __device__ __forceinline__ int32_t vertex_of(uint32_t val) const {
+    const uint32_t t = val / 12u, e = val - 12u * t;
+    const int c = case_s[t];
+    const int cls = kNumVd[c];
+    const uint64_t ta = ra[ns], tb = rb[ns];
+    uint32_t base = 0;
+    for (int k = 1; k < cls; ++k) base += (uint32_t)k * class_field(ta, tb, k);
+    const uint32_t v0 = base + class_field(ra[t], rb[t], cls) * (uint32_t)cls;
+    int slot = 0;
+    for (int j = 0; j < cls; ++j) {
+      const uint32_t w = vd_edges(c, j);
+#pragma unroll
+      for (int k = 0; k < 7; ++k)
+        if (vd_edge(w, k) == (int)e) slot = j;
+    }
+    return (int32_t)(v0 + (uint32_t)slot);
+  }
+};
+
 struct EdgeData {
   const int64_t* e0;
   const int64_t* e1;
@@ -425,7 +471,6 @@ struct VdOut {
   float* ldev;       // [G]
   float* palpha;     // [G,3]
   float* nalpha;     // [G,3]
-  int32_t* vd_map;   // [12*Ns]
 };
 
 // edge normal of the training mode: normalize(edge_dir * sign(s1 - s0))
@@ -447,116 +492,87 @@ __device__ __forceinline__ void edge_normal(const float* x0, const float* x1, fl
 
 __device__ __forceinline__ float ldf(const float* p, int64_t i) { return __ldg(p + i); }
 
-// Eight lanes per dual vertex, lane k owning table slot k (lane 7 idle): a
-// vertex's up to 7 crossings are gathered and evaluated on separate lanes,
-// and the per-vertex sums (weighted average, mean crossing distance) are
-// folded through shuffles in slot order, so their roundings are those of a
-// sequential loop over the slots.  A vertex's crossings are consecutive in
-// the per-crossing outputs, so its lanes write consecutive entries.
-constexpr int kVdThreads = 256;  // 32 dual vertices per block
-
-// sum of x over the slots of this lane's 8-lane group that hold an edge, in
-// slot order; every lane of the group gets the sum
-__device__ __forceinline__ float slot_sum(float x, uint32_t emask, int base) {
-  float acc = 0.f;
+// one thread per dual vertex: crossings, weighted average, L_dev.  The edge
+// loop is unrolled over the 7 table slots, so each edge's plain crossing
+// and distance stay in registers for the L_dev pass (one gather per edge).
+// An edge's corner ids are the cube's own corner ids at the edge's two local
+// corners (the unique-edge key was made from them), read from the cube's
+// 64-B row of cube_idx, which stays in L1 for the vertex's edges, instead
+// of through the crossing's unique-edge index.
+__global__ void vd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
+                          const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
+                          const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
+                          VdOut out) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const uint32_t t = vd_cube[v];
+  const int j = vd_slot[v];
+  const int c = case_s[t];
+  const uint32_t vedges = vd_edges(c, j);
+  const uint32_t cube = list[t];
+  const float ws = world_scale(in);
+  float vx[3];
+  load_voxel(in, cube, vx);
+  const int64_t g0 = goff[v];
+  float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
+  float z[7][3];
+  int64_t g = g0;
 #pragma unroll
   for (int k = 0; k < 7; ++k) {
-    const float y = __shfl_sync(0xffffffffu, x, base + k);
-    if ((emask >> k) & 1u) acc = fa(acc, y);
-  }
-  return acc;
-}
-
-// the setup a vertex's 8 lanes share: its cube, case slot and edge list
-struct VdLane {
-  int64_t v, g;       // dual vertex; this lane's crossing index
-  uint32_t t, cube;   // surface-cube rank and cube index
-  uint32_t emask;     // slots that hold an edge
-  int e;              // this lane's cube edge, 15 = none
-  int base;           // first lane of the group in the warp
-  bool live;
-};
-
-__device__ __forceinline__ VdLane vd_lane(int64_t nv, const uint32_t* __restrict__ list,
-                                          const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
-                                          const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff) {
-  VdLane L;
-  const int lane = threadIdx.x & 31, k = lane & 7;
-  L.base = lane & ~7;
-  L.v = ((int64_t)blockIdx.x * kVdThreads + threadIdx.x) >> 3;
-  L.live = L.v < nv;
-  uint32_t vedges = 0xffffffffu;
-  L.t = 0;
-  L.cube = 0;
-  int64_t g0 = 0;
-  if (L.live) {
-    L.t = vd_cube[L.v];
-    vedges = vd_edges(case_s[L.t], vd_slot[L.v]);
-    L.cube = list[L.t];
-    g0 = goff[L.v];
-  }
-  L.emask = 0;
-#pragma unroll
-  for (int q = 0; q < 7; ++q)
-    if (vd_edge(vedges, q) != 15) L.emask |= 1u << q;
-  L.e = k < 7 ? vd_edge(vedges, k) : 15;
-  L.g = g0 + __popc(L.emask & ((1u << k) - 1u));
-  return L;
-}
-
-__global__ void __launch_bounds__(kVdThreads)
-    vd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
-              const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
-              const uint32_t* __restrict__ goff, EdgeData ed, VdOut out) {
-  const VdLane L = vd_lane(nv, list, case_s, vd_cube, vd_slot, goff);
-  const bool has = L.e != 15;
-  float ue[3] = {0.f, 0.f, 0.f}, z[3] = {0.f, 0.f, 0.f}, b = 0.f;
-  if (has) {
-    const int e = L.e;
-    const int64_t flat = (int64_t)L.t * 12 + e;
-    const int32_t r = ed.idx_map[flat];
-    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
+    const int64_t i0 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e]);
+    const int64_t i1 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e + 1]);
     const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
-    const float a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)L.cube + kCE[2 * e]], in.wscale, true) : 1.f;
-    const float a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)L.cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
-    b = in.beta ? norm_w(in.beta[12 * (int64_t)L.cube + e], in.wscale, true) : 1.f;
+    const float a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
+    const float a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
+    const float b = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
     const float w0 = fm(s1, a1), w1 = -fm(s0, a0);
     const float den = fa(w0, w1);
     const float pw0 = s1, pw1 = -s0, pden = fa(pw0, pw1);
-    float vx[3], xa[3], xb[3], n[3];
-    load_voxel(in, L.cube, vx);
-    edge_world(in, world_scale(in), vx, e, i0, i1, xa, xb);
+    float xa[3], xb[3], n[3];
+    edge_world(in, ws, vx, e, i0, i1, xa, xb);
     edge_normal(xa, xb, s0, s1, n);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      ue[a] = interp1(xa[a], xb[a], w0, w1, den);
-      out.palpha[3 * L.g + a] = ue[a];
-      out.nalpha[3 * L.g + a] = n[a];
-      z[a] = interp1(xa[a], xb[a], pw0, pw1, pden);  // the plain zero crossing
+      const float ue = interp1(xa[a], xb[a], w0, w1, den);
+      out.palpha[3 * g + a] = ue;
+      out.nalpha[3 * g + a] = n[a];
+      acc[a] = fa(acc[a], fm(ue, b));
+      z[k][a] = interp1(xa[a], xb[a], pw0, pw1, pden);  // the plain zero crossing
     }
-    out.vd_map[flat] = (int32_t)L.v;
+    bsum = fa(bsum, b);
+    ++g;
   }
+  const int64_t ne = g - g0;
   float vd[3];
-  const float bden = fa(slot_sum(b, L.emask, L.base), 1e-8f);
+  const float den = fa(bsum, 1e-8f);
 #pragma unroll
-  for (int a = 0; a < 3; ++a) vd[a] = fd(slot_sum(fm(ue[a], b), L.emask, L.base), bden);
-  const int k = threadIdx.x & 7;
-  if (L.live && k < 3) out.verts[3 * L.v + k] = k == 0 ? vd[0] : (k == 1 ? vd[1] : vd[2]);
+  for (int a = 0; a < 3; ++a) {
+    vd[a] = fd(acc[a], den);
+    out.verts[3 * v + a] = vd[a];
+  }
   // L_dev: distances of the plain zero crossings to the dual vertex
-  float dist = 0.f;
-  if (has) {
+  float msum = 0.f;
+  float dist[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    if (vd_edge(vedges, k) == 15) continue;
     float d2 = 0.f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float dd = fsb(z[a], vd[a]);
+      const float dd = fsb(z[k][a], vd[a]);
       d2 = fa(d2, fm(dd, dd));
     }
-    dist = sqrtf(d2);
+    dist[k] = sqrtf(d2);
+    msum = fa(msum, dist[k]);
   }
-  const float msum = slot_sum(dist, L.emask, L.base);
-  if (has) {
-    const float mean = fd(msum, (float)__popc(L.emask));
-    out.ldev[L.g] = fabsf(fsb(dist, mean));
+  const float mean = fd(msum, (float)ne);
+  g = g0;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    if (vd_edge(vedges, k) == 15) continue;
+    out.ldev[g++] = fabsf(fsb(dist[k], mean));
   }
 }
 
@@ -569,7 +585,7 @@ constexpr int kQuadThreads = 256;
 __global__ void __launch_bounds__(kQuadThreads)
     quad_kernel(int64_t ne, int64_t nc, const uint32_t* __restrict__ qflag, const uint32_t* __restrict__ qoff,
                 const uint32_t* __restrict__ rfirst, const uint32_t* __restrict__ vals,
-                const int32_t* __restrict__ vd_map, const int64_t* __restrict__ e0, const float* __restrict__ sdf,
+                VdNumbering vn, const int64_t* __restrict__ e0, const float* __restrict__ sdf,
                 float iso, int64_t nvd, float* __restrict__ verts, int64_t* __restrict__ faces,
                 int32_t* __restrict__ quads) {
   __shared__ int32_t s_quad[kQuadThreads][4];
@@ -583,7 +599,7 @@ __global__ void __launch_bounds__(kQuadThreads)
     const int l = (int)(qoff[r] - q0);
     int32_t v[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = vd_map[vals[rfirst[r] + k]];
+    for (int k = 0; k < 4; ++k) v[k] = vn.vertex_of(vals[rfirst[r] + k]);
     const bool flip = fsb(sdf[e0[r]], iso) > 0.f;
     int32_t o[4];
     if (flip) { o[0] = v[0]; o[1] = v[1]; o[2] = v[3]; o[3] = v[2]; }
@@ -653,176 +669,224 @@ __device__ __forceinline__ void scatter_interp_grad(const DmcIn& in, const float
   }
 }
 
-// Eight lanes per dual vertex as in vd_kernel: lane k recomputes the
-// forward quantities of slot k's crossing; the per-vertex reductions (dual
-// vertex, mean distance, the L_dev and distance adjoints folded into the
-// vertex's gradient) run through shuffles in slot order; each lane then
-// scatters its own crossing's adjoint into sdf, deform, alpha and beta.
+// One thread per dual vertex.  The slot loops are not unrolled (the kernel
+// stays small enough for the instruction cache): each pass reloads a slot's
+// corner ids, signs and weights (the cube's 64-B row of cube_idx, sdf and the
+// weights stay in L1 across the passes) and recomputes its crossings.  An
+// edge's corner ids are the cube's own ids at its two local corners.  Without
+// an L_dev gradient two passes suffice (dual vertex, then the scatter).
 // Gradient order as the forward's reverse: L_dev -> distances -> plain
-// crossings and the dual vertex -> weighted average -> interpolation weights.
-__global__ void __launch_bounds__(kVdThreads)
-    vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
-                  const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
-                  const uint32_t* __restrict__ goff, EdgeData ed, DmcGrad gr) {
-  const VdLane L = vd_lane(nv, list, case_s, vd_cube, vd_slot, goff);
-  const bool has = L.e != 15;
-  const int e = has ? L.e : 0;
-  const uint32_t FULL = 0xffffffffu;
-  int64_t i0 = 0, i1 = 0;
-  float S0 = 0.f, S1 = 0.f, A0 = 1.f, A1 = 1.f, B = 0.f;
-  float UE[3] = {0.f, 0.f, 0.f}, Z[3] = {0.f, 0.f, 0.f}, vx[3] = {0.f, 0.f, 0.f};
-  const float ws = world_scale(in);
-  if (has) {
-    const int32_t r = ed.idx_map[(int64_t)L.t * 12 + e];
-    i0 = ed.e0[r];
-    i1 = ed.e1[r];
-    S0 = fsb(ldf(in.sdf, i0), in.iso);
-    S1 = fsb(ldf(in.sdf, i1), in.iso);
-    A0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)L.cube + kCE[2 * e]], in.wscale, true) : 1.f;
-    A1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)L.cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
-    B = in.beta ? norm_w(in.beta[12 * (int64_t)L.cube + e], in.wscale, true) : 1.f;
-    const float w0 = fm(S1, A1), w1 = -fm(S0, A0), den = fa(w0, w1);
-    const float pw0 = S1, pw1 = -S0, pden = fa(pw0, pw1);
-    float pa[3], pb[3];
-    load_voxel(in, L.cube, vx);
-    edge_world(in, ws, vx, e, i0, i1, pa, pb);
+// crossings and the dual vertex -> weighted average -> interpolation
+// weights -> sdf, deform, alpha, beta.
+struct BwdSlot {
+  int64_t i0, i1;
+  float s0, s1, a0, a1, b;
+  float ue[3], z[3], xa[3], xb[3];
+};
+
+__device__ __forceinline__ void bwd_slot(const DmcIn& in, float ws, const float* vx, uint32_t cube, int e,
+                                         BwdSlot& q) {
+  q.i0 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e]);
+  q.i1 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e + 1]);
+  q.s0 = fsb(ldf(in.sdf, q.i0), in.iso);
+  q.s1 = fsb(ldf(in.sdf, q.i1), in.iso);
+  q.a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
+  q.a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
+  q.b = in.beta ? norm_w(in.beta[12 * (int64_t)cube + e], in.wscale, true) : 1.f;
+  const float w0 = fm(q.s1, q.a1), w1 = -fm(q.s0, q.a0), den = fa(w0, w1);
+  const float pw0 = q.s1, pw1 = -q.s0, pden = fa(pw0, pw1);
+  edge_world(in, ws, vx, e, q.i0, q.i1, q.xa, q.xb);
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      UE[a] = interp1(pa[a], pb[a], w0, w1, den);
-      Z[a] = interp1(pa[a], pb[a], pw0, pw1, pden);
-    }
+  for (int a = 0; a < 3; ++a) {
+    q.ue[a] = interp1(q.xa[a], q.xb[a], w0, w1, den);
+    q.z[a] = interp1(q.xa[a], q.xb[a], pw0, pw1, pden);
   }
-  const float bden = fa(slot_sum(B, L.emask, L.base), 1e-8f);
+}
+
+// distance of slot q's plain crossing to the dual vertex
+__device__ __forceinline__ float bwd_dist(const BwdSlot& q, const float* vd) {
+  float d2 = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float dd = fsb(q.z[a], vd[a]);
+    d2 = fa(d2, fm(dd, dd));
+  }
+  return sqrtf(d2);
+}
+
+__global__ void __launch_bounds__(128) vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
+                                                     const uint8_t* __restrict__ case_s,
+                                                     const uint32_t* __restrict__ vd_cube,
+                                                     const uint8_t* __restrict__ vd_slot,
+                                                     const uint32_t* __restrict__ goff, EdgeData ed, DmcGrad gr) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  (void)ed;
+  const uint32_t t = vd_cube[v];
+  const int c = case_s[t];
+  const uint32_t vedges = vd_edges(c, vd_slot[v]);
+  const uint32_t cube = list[t];
+  const float ws = world_scale(in);
+  float vx[3];
+  load_voxel(in, cube, vx);
+  const int64_t g0 = goff[v];
+  BwdSlot q;
+  // forward: weighted average of the alpha-weighted crossings
+  float acc[3] = {0.f, 0.f, 0.f}, bsum = 0.f;
+  int ne = 0;
+#pragma unroll 1
+  for (int k = 0; k < 7; ++k) {
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
+    bwd_slot(in, ws, vx, cube, e, q);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) acc[a] = fa(acc[a], fm(q.ue[a], q.b));
+    bsum = fa(bsum, q.b);
+    ++ne;
+  }
+  const float bden = fa(bsum, 1e-8f);
   float vd[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) vd[a] = fd(slot_sum(fm(UE[a], B), L.emask, L.base), bden);
+  for (int a = 0; a < 3; ++a) vd[a] = fd(acc[a], bden);
   // incoming gradient of the dual vertex
   float gvd[3] = {0.f, 0.f, 0.f};
-  if (gr.g_verts && L.live)
+  if (gr.g_verts)
 #pragma unroll
-    for (int a = 0; a < 3; ++a) gvd[a] = gr.g_verts[3 * L.v + a] + gr.g_vd[3 * L.v + a];
-  // L_dev backward (mad = |dist - mean|, mean = sum(dist)/ne)
-  float D = 0.f;
-  if (has) {
-    float d2 = 0.f;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float dd = fsb(Z[a], vd[a]);
-      d2 = fa(d2, fm(dd, dd));
+    for (int a = 0; a < 3; ++a) gvd[a] = gr.g_verts[3 * v + a] + gr.g_vd[3 * v + a];
+  // L_dev backward (mad = |dist - mean|, mean = sum(dist)/ne): gD of slot
+  // k = gl_k sign(D_k - mean) + gm, gm = -sum_k gl_k sign(D_k - mean) / ne
+  const bool with_ldev = gr.g_ldev != nullptr;
+  float mean = 0.f, gm = 0.f;
+  if (with_ldev) {
+    float msum = 0.f;
+#pragma unroll 1
+    for (int k = 0; k < 7; ++k) {
+      const int e = vd_edge(vedges, k);
+      if (e == 15) continue;
+      bwd_slot(in, ws, vx, cube, e, q);
+      msum = fa(msum, bwd_dist(q, vd));
     }
-    D = sqrtf(d2);
-  }
-  const int ne = __popc(L.emask);
-  const float mean = fd(slot_sum(D, L.emask, L.base), (float)ne);
-  float gD = 0.f;
-  if (gr.g_ldev) {
-    float x = 0.f;
-    if (has) {
-      const float gl = gr.g_ldev[L.g];
+    mean = fd(msum, (float)ne);
+    float gmean = 0.f;
+    int r = 0;
+#pragma unroll 1
+    for (int k = 0; k < 7; ++k) {
+      const int e = vd_edge(vedges, k);
+      if (e == 15) continue;
+      bwd_slot(in, ws, vx, cube, e, q);
+      const float df = bwd_dist(q, vd) - mean;
+      const float sg = df > 0.f ? 1.f : (df < 0.f ? -1.f : 0.f);
+      gmean -= gr.g_ldev[g0 + r] * sg;
+      ++r;
+    }
+    gm = gmean / (float)ne;
+    // dist -> crossing z and the dual vertex
+    r = 0;
+#pragma unroll 1
+    for (int k = 0; k < 7; ++k) {
+      const int e = vd_edge(vedges, k);
+      if (e == 15) continue;
+      bwd_slot(in, ws, vx, cube, e, q);
+      const float D = bwd_dist(q, vd);
       const float df = D - mean;
       const float sg = df > 0.f ? 1.f : (df < 0.f ? -1.f : 0.f);
-      x = gl * sg;
-    }
-    gD = x;
-    float gmean = 0.f;
+      const float gD = gr.g_ldev[g0 + r] * sg + gm;
+      const float invd = D > 0.f ? 1.0f / D : 0.f;
 #pragma unroll
-    for (int k = 0; k < 7; ++k) {
-      const float y = __shfl_sync(FULL, x, L.base + k);
-      if ((L.emask >> k) & 1u) gmean -= y;
-    }
-    gD += gmean / (float)ne;
-  }
-  // dist -> crossing z and the dual vertex
-  float gZ[3];
-  {
-    const float invd = D > 0.f ? 1.0f / D : 0.f;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float u = (Z[a] - vd[a]) * invd;
-      gZ[a] = has ? gD * u : 0.f;
-#pragma unroll
-      for (int k = 0; k < 7; ++k) {
-        const float y = __shfl_sync(FULL, gZ[a], L.base + k);
-        if ((L.emask >> k) & 1u) gvd[a] -= y;
-      }
+      for (int a = 0; a < 3; ++a) gvd[a] -= gD * ((q.z[a] - vd[a]) * invd);
+      ++r;
     }
   }
-  if (!has) return;  // no shuffles below
   // vd = sum(b ue) / (sum b + 1e-8)
   const float inv_bden = 1.0f / bden;
   float gB = 0.f;
 #pragma unroll
   for (int a = 0; a < 3; ++a) gB -= gvd[a] * vd[a] * inv_bden;
-  float gue[3];
-  float gb = gB;
+  int r = 0;
+#pragma unroll 1
+  for (int k = 0; k < 7; ++k) {
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
+    bwd_slot(in, ws, vx, cube, e, q);
+    const int64_t i0 = q.i0, i1 = q.i1;
+    float gue[3];
+    float gb = gB;
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    gue[a] = gvd[a] * B * inv_bden;
-    if (gr.g_palpha) gue[a] += gr.g_palpha[3 * L.g + a];
-    gb += gvd[a] * UE[a] * inv_bden;
-  }
-  float xa[3], xb[3];
-  edge_world(in, ws, vx, e, i0, i1, xa, xb);
-  // ue through w0 = s1 a1, w1 = -s0 a0
-  {
-    const float w0 = S1 * A1, w1 = -(S0 * A0), den = w0 + w1;
-    float gw0, gw1;
-    scatter_interp_grad(in, gue, xa, xb, UE, w0, w1, den, i0, i1, gw0, gw1, gr);
-    if (gr.g_sdf) {
-      atomicAdd(&gr.g_sdf[i1], gw0 * A1);
-      atomicAdd(&gr.g_sdf[i0], -gw1 * A0);
+    for (int a = 0; a < 3; ++a) {
+      gue[a] = gvd[a] * q.b * inv_bden;
+      if (gr.g_palpha) gue[a] += gr.g_palpha[3 * (g0 + r) + a];
+      gb += gvd[a] * q.ue[a] * inv_bden;
     }
-    if (gr.g_alpha && in.alpha) {
-      const int c0 = kCE[2 * e], c1 = kCE[2 * e + 1];
-      const float t0 = tanhf(in.alpha[8 * (int64_t)L.cube + c0]), t1 = tanhf(in.alpha[8 * (int64_t)L.cube + c1]);
-      atomicAdd(&gr.g_alpha[8 * (int64_t)L.cube + c1], gw0 * S1 * in.wscale * (1.f - t1 * t1));
-      atomicAdd(&gr.g_alpha[8 * (int64_t)L.cube + c0], -gw1 * S0 * in.wscale * (1.f - t0 * t0));
-    }
-  }
-  // plain crossing z through w0 = s1, w1 = -s0 (nothing to add without an
-  // L_dev gradient: gZ is zero)
-  if (gr.g_ldev) {
-    const float w0 = S1, w1 = -S0, den = w0 + w1;
-    float gw0, gw1;
-    scatter_interp_grad(in, gZ, xa, xb, Z, w0, w1, den, i0, i1, gw0, gw1, gr);
-    if (gr.g_sdf) {
-      atomicAdd(&gr.g_sdf[i1], gw0);
-      atomicAdd(&gr.g_sdf[i0], -gw1);
-    }
-  }
-  // edge normal (n_alpha) through the edge vector
-  if (gr.g_nalpha && gr.g_deform) {
-    float ev[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) ev[a] = xb[a] - xa[a];
-    const float el = sqrtf(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
-    const float Ln = el + 1e-8f;
-    const float ds = S1 - S0;
-    const float sg = ds > 0.f ? 1.f : (ds < 0.f ? -1.f : 0.f);
-    float u[3], n[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) u[a] = ev[a] / Ln * sg;
-    const float ul = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-    const float* gn = gr.g_nalpha + 3 * L.g;
-    if (ul > 1e-12f && el > 0.f) {
-#pragma unroll
-      for (int a = 0; a < 3; ++a) n[a] = u[a] / ul;
-      const float ndg = n[0] * gn[0] + n[1] * gn[1] + n[2] * gn[2];
-      float ged[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) ged[a] = sg * (gn[a] - n[a] * ndg) / ul;
-      const float gdot = ged[0] * ev[0] + ged[1] * ev[1] + ged[2] * ev[2];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float gev = ged[a] / Ln - ev[a] * gdot / (Ln * Ln * el);
-        atomicAdd(&gr.g_deform[3 * i1 + a], gev);
-        atomicAdd(&gr.g_deform[3 * i0 + a], -gev);
+    // ue through w0 = s1 a1, w1 = -s0 a0
+    {
+      const float w0 = q.s1 * q.a1, w1 = -(q.s0 * q.a0), den = w0 + w1;
+      float gw0, gw1;
+      scatter_interp_grad(in, gue, q.xa, q.xb, q.ue, w0, w1, den, i0, i1, gw0, gw1, gr);
+      if (gr.g_sdf) {
+        atomicAdd(&gr.g_sdf[i1], gw0 * q.a1);
+        atomicAdd(&gr.g_sdf[i0], -gw1 * q.a0);
+      }
+      if (gr.g_alpha && in.alpha) {
+        const int c0 = kCE[2 * e], c1 = kCE[2 * e + 1];
+        const float t0 = tanhf(in.alpha[8 * (int64_t)cube + c0]), t1 = tanhf(in.alpha[8 * (int64_t)cube + c1]);
+        atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c1], gw0 * q.s1 * in.wscale * (1.f - t1 * t1));
+        atomicAdd(&gr.g_alpha[8 * (int64_t)cube + c0], -gw1 * q.s0 * in.wscale * (1.f - t0 * t0));
       }
     }
-  }
-  if (gr.g_beta && in.beta) {
-    const float tb = tanhf(in.beta[12 * (int64_t)L.cube + e]);
-    gr.g_beta[12 * (int64_t)L.cube + e] += gb * in.wscale * (1.f - tb * tb);
+    // plain crossing z through w0 = s1, w1 = -s0 (zero without an L_dev
+    // gradient)
+    if (with_ldev) {
+      const float D = bwd_dist(q, vd);
+      const float df = D - mean;
+      const float sg = df > 0.f ? 1.f : (df < 0.f ? -1.f : 0.f);
+      const float gD = gr.g_ldev[g0 + r] * sg + gm;
+      const float invd = D > 0.f ? 1.0f / D : 0.f;
+      float gZ[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) gZ[a] = gD * ((q.z[a] - vd[a]) * invd);
+      const float w0 = q.s1, w1 = -q.s0, den = w0 + w1;
+      float gw0, gw1;
+      scatter_interp_grad(in, gZ, q.xa, q.xb, q.z, w0, w1, den, i0, i1, gw0, gw1, gr);
+      if (gr.g_sdf) {
+        atomicAdd(&gr.g_sdf[i1], gw0);
+        atomicAdd(&gr.g_sdf[i0], -gw1);
+      }
+    }
+    // edge normal (n_alpha) through the edge vector
+    if (gr.g_nalpha && gr.g_deform) {
+      float ev[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) ev[a] = q.xb[a] - q.xa[a];
+      const float el = sqrtf(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+      const float L = el + 1e-8f;
+      const float ds = q.s1 - q.s0;
+      const float sg = ds > 0.f ? 1.f : (ds < 0.f ? -1.f : 0.f);
+      float u[3], n[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) u[a] = ev[a] / L * sg;
+      const float ul = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+      const float* gn = gr.g_nalpha + 3 * (g0 + r);
+      if (ul > 1e-12f && el > 0.f) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) n[a] = u[a] / ul;
+        const float ndg = n[0] * gn[0] + n[1] * gn[1] + n[2] * gn[2];
+        float ged[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ged[a] = sg * (gn[a] - n[a] * ndg) / ul;
+        const float gdot = ged[0] * ev[0] + ged[1] * ev[1] + ged[2] * ev[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float gev = ged[a] / L - ev[a] * gdot / (L * L * el);
+          atomicAdd(&gr.g_deform[3 * i1 + a], gev);
+          atomicAdd(&gr.g_deform[3 * i0 + a], -gev);
+        }
+      }
+    }
+    if (gr.g_beta && in.beta) {
+      const float tb = tanhf(in.beta[12 * (int64_t)cube + e]);
+      gr.g_beta[12 * (int64_t)cube + e] += gb * in.wscale * (1.f - tb * tb);
+    }
+    ++r;
   }
 }
 
@@ -998,7 +1062,6 @@ struct DmcWs {
   uint32_t* rflag;     // [12N]
   uint32_t* rid;       // [12N]
   int32_t* idx_map;    // [12N]
-  int32_t* vd_map;     // [12N]
   int64_t* e0;         // [12N]
   int64_t* e1;
   uint32_t* rfirst;    // [12N]
@@ -1049,7 +1112,6 @@ size_t carve_dmc(DmcWs& w, Workspace& ws, int64_t n, int64_t m) {
   w.rflag = ws.take<uint32_t>(n12);
   w.rid = ws.take<uint32_t>(n12);
   w.idx_map = ws.take<int32_t>(n12);
-  w.vd_map = ws.take<int32_t>(n12);
   w.e0 = ws.take<int64_t>(n12);
   w.e1 = ws.take<int64_t>(n12);
   w.rfirst = ws.take<uint32_t>(n12);
@@ -1130,7 +1192,8 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   cross_count_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.cases, w.mask12, w.ccnt);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ccnt, w.coff, n, w.scan_tmp, w.coff + n, s)));
-  cross_write_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.mask12, w.coff, w.keys, w.vals);
+  cross_write_kernel<<<gsz(n, kCrossThreads), kCrossThreads, 0, s>>>(in, ns_dev, w.list, w.mask12, w.coff, w.keys,
+                                                                     w.vals);
   A3D_LAUNCH_CHECK();
   // the one round trip before the edge sort: surface cubes, crossings and
   // the out-of-range flag
@@ -1158,7 +1221,8 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   run_flag_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, nc, w.rflag);
   A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.rflag, w.rid, nc, w.scan_tmp, w.misc, s)));
-  A3D_CUDA_TRY(cudaMemsetAsync(w.idx_map, 0xff, 12 * ns * sizeof(int32_t), s));
+  // idx_map is read only at crossing (cube, edge) pairs, all of which
+  // run_info_kernel writes: no clear
   run_info_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, w.vals, nc, w.rflag, w.rid, m, w.idx_map, w.e0, w.e1, w.rfirst);
   A3D_LAUNCH_CHECK();
   quad_flag_kernel<<<gsz(nc), 256, 0, s>>>(w.misc, nc, w.rfirst, w.qflag);
@@ -1210,13 +1274,12 @@ extern "C" int a3d_dmc_emit(const a3d_dmc_inputs* p, void* workspace, size_t wor
   if (ns == 0 || nv == 0) return A3D_OK;
   DmcIn in = make_in(p);
   EdgeData ed{w.e0, w.e1, w.idx_map};
-  VdOut out{vertices, l_dev, p_alpha, n_alpha, w.vd_map};
-  vd_kernel<<<gsz(8 * nv, kVdThreads), kVdThreads, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff,
-                                                           ed, out);
+  VdOut out{vertices, l_dev, p_alpha, n_alpha};
+  vd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, out);
   A3D_LAUNCH_CHECK();
   (void)nc;
   if (nq > 0) {
-    quad_kernel<<<gsz(ne, kQuadThreads), kQuadThreads, 0, s>>>(ne, nc, w.qflag, w.qoff, w.rfirst, w.vals, w.vd_map, w.e0, p->sdf, p->isovalue,
+    quad_kernel<<<gsz(ne, kQuadThreads), kQuadThreads, 0, s>>>(ne, nc, w.qflag, w.qoff, w.rfirst, w.vals, VdNumbering{w.case_s, w.cls_ra, w.cls_rb, ns}, w.e0, p->sdf, p->isovalue,
                                         nv, vertices, faces, w.quads);
     A3D_LAUNCH_CHECK();
   }
@@ -1244,8 +1307,7 @@ extern "C" int a3d_dmc_backward(const a3d_dmc_inputs* p, void* workspace, size_t
     A3D_LAUNCH_CHECK();
   }
   EdgeData ed{w.e0, w.e1, w.idx_map};
-  vd_bwd_kernel<<<gsz(8 * nv, kVdThreads), kVdThreads, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot,
-                                                               w.goff, ed, gr);
+  vd_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, gr);
   A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
@@ -1533,9 +1595,9 @@ __global__ void vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float
   for (int k = 0; k < 7; ++k) {
     const int e = vd_edge(vedges, k);
     if (e == 15) continue;
-    const int64_t flat = (int64_t)t * 12 + e;
-    const int32_t r = ed.idx_map[flat];
-    const int64_t i0 = ed.e0[r], i1 = ed.e1[r];
+    // the edge's corner ids are the cube's own ids at its local corners
+    const int64_t i0 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e]);
+    const int64_t i1 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e + 1]);
     const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
     const float a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
     const float a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
@@ -1553,7 +1615,6 @@ __global__ void vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float
       out.nalpha[3 * g + a] = nn[ne][a];
       z[ne][a] = interp1(xa[a], xb[a], s1, -s0, zd);
     }
-    out.vd_map[flat] = (int32_t)v;
     ++ne;
   }
   // centroid of the crossings; cell centre and bounds
@@ -1649,7 +1710,7 @@ __global__ void vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float
 __global__ void __launch_bounds__(kQuadThreads)
     quad_eval_kernel(int64_t ne, const uint32_t* __restrict__ qflag, const uint32_t* __restrict__ qoff,
                      const uint32_t* __restrict__ rfirst, const uint32_t* __restrict__ vals,
-                     const int32_t* __restrict__ vd_map, const int64_t* __restrict__ e0,
+                     VdNumbering vn, const int64_t* __restrict__ e0,
                      const float* __restrict__ sdf, float iso, const float* __restrict__ verts,
                      int64_t* __restrict__ faces) {
   __shared__ int32_t s_tri[kQuadThreads][6];
@@ -1662,7 +1723,7 @@ __global__ void __launch_bounds__(kQuadThreads)
     const int l = (int)(qoff[r] - q0);
     int32_t v[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = vd_map[vals[rfirst[r] + k]];
+    for (int k = 0; k < 4; ++k) v[k] = vn.vertex_of(vals[rfirst[r] + k]);
     const bool flip = fsb(sdf[e0[r]], iso) > 0.f;
     int32_t o[4];
     if (flip) { o[0] = v[0]; o[1] = v[1]; o[2] = v[3]; o[3] = v[2]; }
@@ -1752,7 +1813,7 @@ extern "C" int a3d_dmc_emit_qef(const a3d_dmc_inputs* p, void* workspace, size_t
   if (ns == 0 || nv == 0) return A3D_OK;
   DmcIn in = make_in(p);
   EdgeData ed{w.e0, w.e1, w.idx_map};
-  VdOut out{vertices, l_dev, p_alpha, n_alpha, w.vd_map};
+  VdOut out{vertices, l_dev, p_alpha, n_alpha};
   // corner world positions (the training path computes them per edge)
   init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x, nullptr);
   A3D_LAUNCH_CHECK();
@@ -1762,7 +1823,7 @@ extern "C" int a3d_dmc_emit_qef(const a3d_dmc_inputs* p, void* workspace, size_t
                                              w.vd_cube, w.vd_slot, w.goff, ed, out);
   A3D_LAUNCH_CHECK();
   if (nq > 0) {
-    quad_eval_kernel<<<gsz(ne, kQuadThreads), kQuadThreads, 0, s>>>(ne, w.qflag, w.qoff, w.rfirst, w.vals, w.vd_map, w.e0, p->sdf,
+    quad_eval_kernel<<<gsz(ne, kQuadThreads), kQuadThreads, 0, s>>>(ne, w.qflag, w.qoff, w.rfirst, w.vals, VdNumbering{w.case_s, w.cls_ra, w.cls_rb, ns}, w.e0, p->sdf,
                                              p->isovalue, vertices, faces);
     A3D_LAUNCH_CHECK();
   }
