@@ -1704,6 +1704,378 @@ __global__ void vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float
   for (int q = 0; q < ne; ++q) out.ldev[g0 + q] = fabsf(fsb(dist[q], mean));
 }
 
+// ---- QEF-mode adjoint -----------------------------------------------------------
+// The reference differentiates its QEF vertices through torch.linalg.lstsq
+// and the crossing normals (atom3d/mesh_extractor/sparse_diffdmc.py:289-389,
+// :610-650); the corner gradients it estimates itself carry no gradient
+// (_estimate_corner_gradients runs under no_grad, :451), those a caller
+// passes do.  One thread per dual vertex recomputes the forward of
+// vd_qef_kernel (same roundings, the same FP64 normal equations and the same
+// fallback decision) and backpropagates:
+//   L_dev -> crossing distances -> crossings z and the dual vertex;
+//   vd = dl + cen (or cen on fallback); dl = M^-1 m, M = sum r r^T,
+//   m = sum r rhs: with y = M^-1 g_dl, g_r = y (rhs - r.dl) - dl (y.r),
+//   g_rhs = y.r;
+//   rows -> normals, crossings, centroid cen = mean z, cell centre
+//   ctr = mean of the 8 corner positions;
+//   normals n = g / |g|, g = (w0 g0 + w1 g1) / (w0 + w1), w0 = |g0| (1 - t),
+//   w1 = |g1| t, t = clamp(s0 / (s0 - s1 + 1e-8), 0, 1) -> sdf through t,
+//   corner gradients, or the edge direction (positions) on its fallback;
+//   z and p_alpha -> sdf, alpha, positions (deform).
+struct QefGrad {
+  const float* g_verts;   // [V,3] or null
+  const float* g_ldev;    // [G] or null
+  const float* g_palpha;  // [G,3] or null
+  const float* g_nalpha;  // [G,3] or null
+  float* g_sdf;           // [M] or null
+  float* g_deform;        // [M,3] or null
+  float* g_alpha;         // [N,8] raw or null
+  float* g_grad;          // [M,3] or null: gradient w.r.t. the corner gradients
+};
+
+// adjoint of edge_normal(xa, xb, s0, s1) for an output gradient gn, into the
+// end positions (the sign of s1 - s0 is piecewise constant)
+__device__ __forceinline__ void edge_normal_bwd(const float* xa, const float* xb, float s0, float s1, const float* gn,
+                                                float* g_xa, float* g_xb) {
+  float ev[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) ev[a] = xb[a] - xa[a];
+  const float el = sqrtf(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+  const float L = el + 1e-8f;
+  const float ds = s1 - s0;
+  const float sg = ds > 0.f ? 1.f : (ds < 0.f ? -1.f : 0.f);
+  float u[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) u[a] = ev[a] / L * sg;
+  const float ul = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+  if (!(ul > 1e-12f && el > 0.f)) return;
+  float n[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) n[a] = u[a] / ul;
+  const float ndg = n[0] * gn[0] + n[1] * gn[1] + n[2] * gn[2];
+  float ged[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) ged[a] = sg * (gn[a] - n[a] * ndg) / ul;
+  const float gdot = ged[0] * ev[0] + ged[1] * ev[1] + ged[2] * ev[2];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float gev = ged[a] / L - ev[a] * gdot / (L * L * el);
+    g_xb[a] += gev;
+    g_xa[a] -= gev;
+  }
+}
+
+__global__ void vd_qef_bwd_kernel(DmcIn in, const float* __restrict__ x, const float* __restrict__ grad, float lam,
+                                  int64_t nv, const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
+                                  const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
+                                  const uint32_t* __restrict__ goff, QefGrad gq) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const uint32_t t = vd_cube[v];
+  const uint32_t vedges = vd_edges(case_s[t], vd_slot[v]);
+  const uint32_t cube = list[t];
+  const int64_t g0 = goff[v];
+  // ---- forward, as vd_qef_kernel
+  int64_t I0[7], I1[7];
+  int E[7];
+  float S0[7], S1[7], z[7][3], nn[7][3];
+  int ne = 0;
+  for (int k = 0; k < 7; ++k) {
+    const int e = vd_edge(vedges, k);
+    if (e == 15) continue;
+    const int64_t i0 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e]);
+    const int64_t i1 = corner_at(in, 8 * (int64_t)cube + kCE[2 * e + 1]);
+    const float s0 = fsb(ldf(in.sdf, i0), in.iso), s1 = fsb(ldf(in.sdf, i1), in.iso);
+    const float zd = fa(s1, -s0);
+    float xa[3], xb[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { xa[a] = ldf(x, 3 * i0 + a); xb[a] = ldf(x, 3 * i1 + a); }
+    crossing_normal(grad, i0, i1, s0, s1, xa, xb, nn[ne]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) z[ne][a] = interp1(xa[a], xb[a], s1, -s0, zd);
+    I0[ne] = i0; I1[ne] = i1; E[ne] = e; S0[ne] = s0; S1[ne] = s1;
+    ++ne;
+  }
+  float cen[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float sacc = 0.f;
+    for (int q = 0; q < ne; ++q) sacc = fa(sacc, z[q][a]);
+    cen[a] = fd(sacc, (float)(ne > 0 ? ne : 1));
+  }
+  float ctr[3], cmin[3], cmax[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float sacc = 0.f, lo = INFINITY, hi = -INFINITY;
+    for (int k = 0; k < 8; ++k) {
+      const float pp = ldf(x, 3 * corner_at(in, 8 * (int64_t)cube + k) + a);
+      sacc = fa(sacc, pp);
+      lo = fminf(lo, pp);
+      hi = fmaxf(hi, pp);
+    }
+    ctr[a] = fd(sacc, 8.f);
+    cmin[a] = lo;
+    cmax[a] = hi;
+  }
+  const double sl = sqrt((double)lam);
+  // row q of the system: (r, rhs); reg_row: the cell-centre row of axis a
+  auto row_of = [&](int q, double* rv, double& rhs, int& reg_axis) {
+    const int row = (q - (ne - 1) + 10) % 10;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) rv[a] = (double)nn[q][a];
+    rhs = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) rhs += (double)nn[q][a] * ((double)z[q][a] - (double)cen[a]);
+    reg_axis = -1;
+    if (row >= 7) {
+      reg_axis = row - 7;
+      rv[reg_axis] = sl;
+      rhs = sl * ((double)ctr[reg_axis] - (double)cen[reg_axis]);
+    }
+  };
+  double ata[6] = {0, 0, 0, 0, 0, 0}, atb[3] = {0, 0, 0};
+  auto add_row = [&](const double* rv, double rhs) {
+    ata[0] += rv[0] * rv[0]; ata[1] += rv[0] * rv[1]; ata[2] += rv[0] * rv[2];
+    ata[3] += rv[1] * rv[1]; ata[4] += rv[1] * rv[2]; ata[5] += rv[2] * rv[2];
+    atb[0] += rv[0] * rhs; atb[1] += rv[1] * rhs; atb[2] += rv[2] * rhs;
+  };
+  bool reg_used[3] = {false, false, false};
+  for (int q = 0; q < ne; ++q) {
+    double rv[3], rhs;
+    int ra;
+    row_of(q, rv, rhs, ra);
+    if (ra >= 0) reg_used[ra] = true;
+    add_row(rv, rhs);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (reg_used[a]) continue;
+    double rv[3] = {0.0, 0.0, 0.0};
+    rv[a] = sl;
+    add_row(rv, sl * ((double)ctr[a] - (double)cen[a]));
+  }
+  double dl[3];
+  solve_sym3(ata, atb, dl);
+  float vd[3];
+  bool bad = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    vd[a] = fa((float)dl[a], cen[a]);
+    bad = bad || isnan(vd[a]);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float mg = fsb(cmax[a], cmin[a]);
+    bad = bad || vd[a] < fsb(cmin[a], mg) || vd[a] > fa(cmax[a], mg);
+  }
+  if (bad)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) vd[a] = cen[a];
+  // ---- adjoint
+  float gvd[3] = {0.f, 0.f, 0.f};
+  if (gq.g_verts)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) gvd[a] = gq.g_verts[3 * v + a];
+  float gz[7][3], gn[7][3];
+  for (int q = 0; q < ne; ++q)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      gz[q][a] = 0.f;
+      gn[q][a] = gq.g_nalpha ? gq.g_nalpha[3 * (g0 + q) + a] : 0.f;
+    }
+  if (gq.g_ldev) {
+    // mad = |dist - mean|, mean = sum(dist)/ne (distances as the forward)
+    float D[7], msum = 0.f;
+    for (int q = 0; q < ne; ++q) {
+      float d2 = 0.f;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float dd = fsb(z[q][a], vd[a]);
+        d2 = fa(d2, fm(dd, dd));
+      }
+      D[q] = sqrtf(d2);
+      msum = fa(msum, D[q]);
+    }
+    const float mean = fd(msum, (float)ne);
+    float gmean = 0.f, gD[7];
+    for (int q = 0; q < ne; ++q) {
+      const float gl = gq.g_ldev[g0 + q];
+      const float df = D[q] - mean;
+      const float sg = df > 0.f ? 1.f : (df < 0.f ? -1.f : 0.f);
+      gD[q] = gl * sg;
+      gmean -= gl * sg;
+    }
+    const float gm = gmean / (float)ne;
+    for (int q = 0; q < ne; ++q) {
+      const float gdq = gD[q] + gm;
+      const float invd = D[q] > 0.f ? 1.0f / D[q] : 0.f;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float u = (z[q][a] - vd[a]) * invd;
+        gz[q][a] += gdq * u;
+        gvd[a] -= gdq * u;
+      }
+    }
+  }
+  float gcen[3] = {gvd[0], gvd[1], gvd[2]}, gctr[3] = {0.f, 0.f, 0.f};
+  if (!bad) {
+    // vd = dl + cen: through the solve and the rows
+    double y[3];
+    const double gdl[3] = {(double)gvd[0], (double)gvd[1], (double)gvd[2]};
+    solve_sym3(ata, gdl, y);
+    for (int q = 0; q < ne; ++q) {
+      double rv[3], rhs;
+      int ra;
+      row_of(q, rv, rhs, ra);
+      const double res = rhs - (rv[0] * dl[0] + rv[1] * dl[1] + rv[2] * dl[2]);
+      const double yr = y[0] * rv[0] + y[1] * rv[1] + y[2] * rv[2];
+      double gr_[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) gr_[a] = y[a] * res - dl[a] * yr;
+      if (ra < 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          gn[q][a] += (float)(gr_[a] + yr * ((double)z[q][a] - (double)cen[a]));
+          gz[q][a] += (float)(yr * (double)nn[q][a]);
+          gcen[a] -= (float)(yr * (double)nn[q][a]);
+        }
+      } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          if (a != ra) gn[q][a] += (float)gr_[a];
+        gctr[ra] += (float)(sl * yr);
+        gcen[ra] -= (float)(sl * yr);
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (reg_used[a]) continue;
+      const double yr = y[a] * sl;
+      gctr[a] += (float)(sl * yr);
+      gcen[a] -= (float)(sl * yr);
+    }
+  }
+  // cen = mean of the crossings
+  for (int q = 0; q < ne; ++q)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) gz[q][a] += gcen[a] / (float)ne;
+  // ctr = mean of the 8 corner positions (positions = grid map + deform)
+  if (gq.g_deform && (gctr[0] != 0.f || gctr[1] != 0.f || gctr[2] != 0.f))
+    for (int k = 0; k < 8; ++k) {
+      const int64_t ck = corner_at(in, 8 * (int64_t)cube + k);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) atomicAdd(&gq.g_deform[3 * ck + a], gctr[a] * 0.125f);
+    }
+  DmcGrad gr{nullptr, nullptr, nullptr, nullptr, nullptr, gq.g_deform, nullptr, nullptr, nullptr};
+  for (int q = 0; q < ne; ++q) {
+    const int64_t i0 = I0[q], i1 = I1[q];
+    const float s0 = S0[q], s1 = S1[q];
+    const int e = E[q];
+    float xa[3], xb[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { xa[a] = ldf(x, 3 * i0 + a); xb[a] = ldf(x, 3 * i1 + a); }
+    float gs0 = 0.f, gs1 = 0.f;
+    float gxa[3] = {0.f, 0.f, 0.f}, gxb[3] = {0.f, 0.f, 0.f};
+    // normal: n = g / max(|g|, 1e-12)
+    {
+      const float Dt = fa(fsb(s0, s1), 1e-8f);
+      const float traw = fd(s0, Dt);
+      const float tt = fminf(fmaxf(traw, 0.f), 1.f);
+      float g0v[3], g1v[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) { g0v[a] = ldf(grad, 3 * i0 + a); g1v[a] = ldf(grad, 3 * i1 + a); }
+      const float n0 = sqrtf(fa(fa(fm(g0v[0], g0v[0]), fm(g0v[1], g0v[1])), fm(g0v[2], g0v[2])));
+      const float n1 = sqrtf(fa(fa(fm(g1v[0], g1v[0]), fm(g1v[1], g1v[1])), fm(g1v[2], g1v[2])));
+      const float w0 = fm(n0, fsb(1.f, tt)), w1 = fm(n1, tt);
+      const float den = fa(w0, w1);
+      float gv[3];
+      if (den > 1e-6f) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) gv[a] = fd(fa(fm(w0, g0v[a]), fm(w1, g1v[a])), den);
+      } else {
+        edge_normal(xa, xb, s0, s1, gv);
+      }
+      const float glen = sqrtf(fa(fa(fm(gv[0], gv[0]), fm(gv[1], gv[1])), fm(gv[2], gv[2])));
+      float ggv[3];
+      if (glen > 1e-12f) {
+        const float nd = (gv[0] * gn[q][0] + gv[1] * gn[q][1] + gv[2] * gn[q][2]) / glen;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ggv[a] = (gn[q][a] - gv[a] / glen * nd) / glen;
+      } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ggv[a] = gn[q][a] / 1e-12f;
+      }
+      if (den > 1e-6f) {
+        float gN[3];
+        float gden = 0.f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          gN[a] = ggv[a] / den;
+          gden -= ggv[a] * gv[a] / den;
+        }
+        const float gw0 = gN[0] * g0v[0] + gN[1] * g0v[1] + gN[2] * g0v[2] + gden;
+        const float gw1 = gN[0] * g1v[0] + gN[1] * g1v[1] + gN[2] * g1v[2] + gden;
+        if (gq.g_grad) {
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const float d0 = w0 * gN[a] + (n0 > 0.f ? gw0 * (1.f - tt) * g0v[a] / n0 : 0.f);
+            const float d1 = w1 * gN[a] + (n1 > 0.f ? gw1 * tt * g1v[a] / n1 : 0.f);
+            atomicAdd(&gq.g_grad[3 * i0 + a], d0);
+            atomicAdd(&gq.g_grad[3 * i1 + a], d1);
+          }
+        }
+        const float gt = -n0 * gw0 + n1 * gw1;
+        if (traw > 0.f && traw < 1.f) {
+          gs0 += gt * (1e-8f - s1) / (Dt * Dt);
+          gs1 += gt * s0 / (Dt * Dt);
+        }
+      } else {
+        edge_normal_bwd(xa, xb, s0, s1, ggv, gxa, gxb);
+      }
+    }
+    // plain crossing z = (xa s1 - xb s0) / (s1 - s0)
+    {
+      const float w0 = s1, w1 = -s0, den = w0 + w1;
+      float gw0, gw1;
+      scatter_interp_grad(in, gz[q], xa, xb, z[q], w0, w1, den, i0, i1, gw0, gw1, gr);
+      gs1 += gw0;
+      gs0 -= gw1;
+    }
+    // p_alpha = (xa s1 a1 - xb s0 a0) / (s1 a1 - s0 a0)
+    if (gq.g_palpha) {
+      const float a0 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e]], in.wscale, true) : 1.f;
+      const float a1 = in.alpha ? norm_w(in.alpha[8 * (int64_t)cube + kCE[2 * e + 1]], in.wscale, true) : 1.f;
+      const float w0 = fm(s1, a1), w1 = -fm(s0, a0), den = fa(w0, w1);
+      float ue[3], gue[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        ue[a] = interp1(xa[a], xb[a], w0, w1, den);
+        gue[a] = gq.g_palpha[3 * (g0 + q) + a];
+      }
+      float gw0, gw1;
+      scatter_interp_grad(in, gue, xa, xb, ue, s1 * a1, -(s0 * a0), s1 * a1 - s0 * a0, i0, i1, gw0, gw1, gr);
+      gs1 += gw0 * a1;
+      gs0 -= gw1 * a0;
+      if (gq.g_alpha && in.alpha) {
+        const int c0 = kCE[2 * e], c1 = kCE[2 * e + 1];
+        const float t0 = tanhf(in.alpha[8 * (int64_t)cube + c0]), t1 = tanhf(in.alpha[8 * (int64_t)cube + c1]);
+        atomicAdd(&gq.g_alpha[8 * (int64_t)cube + c1], gw0 * s1 * in.wscale * (1.f - t1 * t1));
+        atomicAdd(&gq.g_alpha[8 * (int64_t)cube + c0], -gw1 * s0 * in.wscale * (1.f - t0 * t0));
+      }
+    }
+    if (gq.g_sdf) {
+      atomicAdd(&gq.g_sdf[i0], gs0);
+      atomicAdd(&gq.g_sdf[i1], gs1);
+    }
+    if (gq.g_deform)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (gxa[a] != 0.f) atomicAdd(&gq.g_deform[3 * i0 + a], gxa[a]);
+        if (gxb[a] != 0.f) atomicAdd(&gq.g_deform[3 * i1 + a], gxb[a]);
+      }
+  }
+}
+
 // 2 triangles per quad along the shorter diagonal
 // (one thread per unique edge; a block's faces form one contiguous range,
 // staged in shared memory and written coalesced, as in quad_kernel)
@@ -1827,5 +2199,32 @@ extern "C" int a3d_dmc_emit_qef(const a3d_dmc_inputs* p, void* workspace, size_t
                                              p->isovalue, vertices, faces);
     A3D_LAUNCH_CHECK();
   }
+  return A3D_OK;
+}
+
+extern "C" int a3d_dmc_backward_qef(const a3d_dmc_inputs* p, void* workspace, size_t workspace_bytes,
+                                    const int64_t* counts, const float* corner_gradients, float qef_reg_scale,
+                                    const float* g_vertices, const float* g_l_dev, const float* g_p_alpha,
+                                    const float* g_n_alpha, float* g_sdf, float* g_deform, float* g_alpha,
+                                    float* g_corner_gradients, a3d_stream_t stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  A3D_REQUIRE(p && counts && corner_gradients, A3D_ERR_ARGUMENT, "dmc_backward_qef: null argument");
+  const int64_t n = p->num_cubes, m = p->num_corners;
+  Workspace ws(workspace, workspace_bytes);
+  DmcWs w;
+  carve_dmc(w, ws, n > 0 ? n : 1, m > 0 ? m : 1);
+  A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "dmc_backward_qef: workspace too small");
+  const int64_t ns = counts[0], nv = counts[4];
+  if (ns == 0 || nv == 0) return A3D_OK;
+  DmcIn in = make_in(p);
+  // corner world positions, as the forward computed them
+  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x, nullptr);
+  A3D_LAUNCH_CHECK();
+  corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, world_scale_host(p->resolution), w.x);
+  A3D_LAUNCH_CHECK();
+  QefGrad gq{g_vertices, g_l_dev, g_p_alpha, g_n_alpha, g_sdf, g_deform, g_alpha, g_corner_gradients};
+  vd_qef_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, w.x, corner_gradients, qef_reg_scale, nv, w.list, w.case_s,
+                                                 w.vd_cube, w.vd_slot, w.goff, gq);
+  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }

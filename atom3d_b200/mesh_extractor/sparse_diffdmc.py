@@ -77,6 +77,9 @@ _SIGS = {
     "a3d_dmc_emit_qef": (ctypes.c_int, [ctypes.POINTER(DmcInputs), ctypes.c_void_p, ctypes.c_size_t,
                                         ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, ctypes.c_float]
                          + [ctypes.c_void_p] * 6),
+    "a3d_dmc_backward_qef": (ctypes.c_int, [ctypes.POINTER(DmcInputs), ctypes.c_void_p, ctypes.c_size_t,
+                                            ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, ctypes.c_float]
+                             + [ctypes.c_void_p] * 9),
 }
 
 
@@ -186,7 +189,10 @@ class _DmcFn(torch.autograd.Function):
 
 
 class _DmcQefFn(torch.autograd.Function):
-    """QEF inference mode: forward only."""
+    """QEF inference mode.  Differentiable like the reference's eval mode:
+    vertices, L_dev, p_alpha and n_alpha w.r.t. sdf, deform, alpha, the
+    vertex features and caller-given corner gradients (gradients the library
+    estimates carry none, as in the reference)."""
 
     @staticmethod
     def forward(ctx, sdf, deform, alpha, beta, vfeat, vox, cidx, res, iso, wscale, reg, corner_gradients):
@@ -211,13 +217,49 @@ class _DmcQefFn(torch.autograd.Function):
                 float(reg), verts.data_ptr(), faces.data_ptr(), ldev.data_ptr(), pa.data_ptr(), na.data_ptr(),
                 c.stream))
         vf = _features(c, vfeat, False, nv)
+        ctx.dmc = c
+        ctx.vfeat = vfeat
+        ctx.reg = float(reg)
+        ctx.cg = corner_gradients.detach()
+        ctx.has = (deform is not None, alpha is not None, beta is not None)
         ctx.mark_non_differentiable(faces)
+        ctx.set_materialize_grads(False)
         return verts, faces, ldev, pa, na, vf
 
     @staticmethod
-    def backward(ctx, *grads):
-        raise NotImplementedError("SparseDiffDMC: gradients through the QEF inference mode are not provided; "
-                                  "use the weighted-average (training) mode for optimisation")
+    def backward(ctx, g_verts, g_faces, g_ldev, g_pa, g_na, g_vf):
+        c = ctx.dmc
+        need = ctx.needs_input_grad
+        dev = c.dev
+        n, m = c.inp.num_cubes, c.inp.num_corners
+
+        def cont(t):
+            return None if t is None else t.contiguous().float()
+
+        g_sdf = torch.zeros(m, dtype=torch.float32, device=dev) if need[0] else None
+        g_def = torch.zeros(m, 3, dtype=torch.float32, device=dev) if (need[1] and ctx.has[0]) else None
+        g_alpha = torch.zeros(n, 8, dtype=torch.float32, device=dev) if (need[2] and ctx.has[1]) else None
+        g_beta = torch.zeros(n, 12, dtype=torch.float32, device=dev) if (need[3] and ctx.has[2]) else None
+        g_cg = torch.zeros(m, 3, dtype=torch.float32, device=dev) if need[11] else None
+        gv, gl, gp, gn = cont(g_verts), cont(g_ldev), cont(g_pa), cont(g_na)
+        outs = (g_sdf, g_def, g_alpha, g_cg)
+        if c.counts[0] > 0 and any(x is not None for x in outs) and any(x is not None for x in (gv, gl, gp, gn)):
+            _lib.check("a3d_dmc_backward_qef", _bind().a3d_dmc_backward_qef(
+                ctypes.byref(c.inp), c.ws.data_ptr(), c.ws.numel(), c.counts, ctx.cg.data_ptr(), ctx.reg,
+                _lib.ptr(gv), _lib.ptr(gl), _lib.ptr(gp), _lib.ptr(gn), _lib.ptr(g_sdf), _lib.ptr(g_def),
+                _lib.ptr(g_alpha), _lib.ptr(g_cg), c.stream))
+        g_feat = None
+        vfeat = ctx.vfeat
+        if vfeat is not None and g_vf is not None and g_vf.numel() > 0 and c.counts[0] > 0 and c.counts[4] > 0:
+            C = vfeat.shape[1]
+            nv = int(c.counts[4])
+            g_feat = torch.zeros_like(vfeat) if need[4] else None
+            scratch = torch.zeros(nv, C, dtype=torch.float32, device=dev)
+            _lib.check("a3d_dmc_features_backward", _bind().a3d_dmc_features_backward(
+                ctypes.byref(c.inp), c.ws.data_ptr(), c.ws.numel(), c.counts, vfeat.data_ptr(), C, 0,
+                cont(g_vf).data_ptr(), scratch.data_ptr(), _lib.ptr(g_feat), _lib.ptr(g_sdf), _lib.ptr(g_alpha),
+                _lib.ptr(g_beta), c.stream))
+        return g_sdf, g_def, g_alpha, g_beta, g_feat, None, None, None, None, None, None, g_cg
 
 
 class SparseDMC(nn.Module):

@@ -711,8 +711,10 @@ def bench_dmc(dev, steps, warmup, cpu=True):
     # steps back to back between two events on the stream (the forward's two
     # host reads of counts stay inside each step); backward = the difference
     o = fwd_bwd()
-    tot = _time_ms(fwd_bwd, steps, warmup)
-    fwd = _time_ms(fwd_only, steps, warmup)
+    # each step is about a millisecond: time at least 20 of them after 5
+    # warm-up steps so allocator and clock effects average out
+    tot = _time_ms(fwd_bwd, max(20, steps), max(5, warmup))
+    fwd = _time_ms(fwd_only, max(20, steps), max(5, warmup))
     n_cubes, n_v, n_f = vox.shape[0], o.vertices.shape[0], o.faces.shape[0]
     peak, kind = peaks()
     alg = 108.0 * n_cubes + 12.0 * n_v + 24.0 * n_f

@@ -428,6 +428,21 @@ int a3d_dmc_emit_qef(const a3d_dmc_inputs* in, void* workspace, size_t workspace
                      const int64_t* counts, const float* corner_gradients, float qef_reg_scale,
                      float* vertices, int64_t* faces, float* l_dev, float* p_alpha, float* n_alpha,
                      a3d_stream_t stream);
+/* Adjoint of a3d_dmc_emit_qef on the same workspace and the same corner
+ * gradients: the reference differentiates the QEF vertices through
+ * torch.linalg.lstsq, the crossings and the interpolated crossing normals
+ * (atom3d/mesh_extractor/sparse_diffdmc.py:289-389, :610-650).  Gradients
+ * w.r.t. vertices [V,3], L_dev [G], p_alpha [G,3], n_alpha [G,3] (each
+ * nullable) are accumulated into g_sdf [M], g_deform [M,3], g_alpha [N,8]
+ * and g_corner_gradients [M,3] (each nullable; the caller zeroes them).
+ * Corner gradients the library estimated carry no gradient, as in the
+ * reference (_estimate_corner_gradients runs under no_grad); pass
+ * g_corner_gradients for gradients the caller supplied. */
+int a3d_dmc_backward_qef(const a3d_dmc_inputs* in, void* workspace, size_t workspace_bytes,
+                         const int64_t* counts, const float* corner_gradients, float qef_reg_scale,
+                         const float* g_vertices, const float* g_l_dev, const float* g_p_alpha,
+                         const float* g_n_alpha, float* g_sdf, float* g_deform, float* g_alpha,
+                         float* g_corner_gradients, a3d_stream_t stream);
 
 /* Status words of the last a3d_udf / a3d_batch_udf call that used
  * `workspace`, copied to the host after the stream drains:

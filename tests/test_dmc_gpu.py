@@ -160,13 +160,94 @@ def test_dmc_corner_gradients_and_given_gradients():
     assert np.abs(o.vertices.cpu().numpy() - r["vertices"]).max() <= TOL
 
 
-def test_dmc_qef_mode_is_forward_only():
-    g = synthetic.dmc_spheres(res=32, seed=9, n_spheres=3)
-    vox, sdf, cidx, _ = g
-    s = sdf.cuda().requires_grad_(True)
-    o = SparseDiffDMC(device="cuda").eval()(vox.cuda(), s, cidx.cuda(), 32)
-    with pytest.raises(NotImplementedError):
-        (o.vertices ** 2).sum().backward()
+def test_dmc_qef_grad_matches_reference_autograd(golden):
+    """QEF (eval) mode gradients of sum |v|^2 w.r.t. sdf and deform against
+    the reference's own autograd (torch.linalg.lstsq in FP32 QR; this build
+    solves the same system through FP64 normal equations, so the vertices
+    differ by up to ~4.4e-6 and the gradients by a few 1e-4 of their scale)."""
+    g = golden("dmc_small.npz")
+    dmc = SparseDiffDMC(device="cuda").eval()
+    s = torch.from_numpy(g["sdf"]).cuda().requires_grad_(True)
+    de = torch.from_numpy(g["deform"]).cuda().requires_grad_(True)
+    o = dmc(torch.from_numpy(g["vox"]).cuda(), s, torch.from_numpy(g["cidx"]).cuda(), int(g["res"]), deform=de)
+    (o.vertices ** 2).sum().backward()
+    for got, ref in ((s.grad, g["eval_grad_sdf"]), (de.grad, g["eval_grad_deform"])):
+        got = got.cpu().numpy()
+        scale = max(1.0, np.abs(ref).max())
+        err = np.abs(got - ref)
+        assert err.max() <= 2e-3 * scale, (err.max(), scale)
+        assert np.median(err[np.abs(ref) > 0]) <= 1e-5 * scale
+
+
+def _qef_loss(out, w):
+    return ((out["vertices"] ** 2).sum() + (w["L_dev"] * out["L_dev"]).sum() + (w["p_alpha"] * out["p_alpha"]).sum()
+            + (w["n_alpha"] * out["n_alpha"]).sum())
+
+
+def test_dmc_qef_grad_vs_fp64_central_differences():
+    """Every output of the QEF mode (vertices, L_dev, p_alpha, n_alpha) in one
+    seeded linear functional; its gradient w.r.t. sdf, deform and caller-given
+    corner gradients against FP64 central differences of the oracle's QEF
+    forward (the corner gradients held fixed, as the reference's are)."""
+    from oracle import dmc_oracle as D
+
+    vox, sdf, cidx, _ = synthetic.dmc_spheres(res=24, seed=3, n_spheres=3, noise=0.0)
+    s = sdf.double().numpy()
+    rng = np.random.default_rng(1)
+    deform = rng.normal(0, 1e-3, (s.shape[0], 3))
+    G = D.corner_gradients(_corner_positions(vox.numpy(), cidx.numpy(), 24, deform), s, cidx.numpy(),
+                           dtype=np.float64)
+    ref0 = D.forward(vox.numpy(), s, cidx.numpy(), 24, deform=deform, dtype=np.float64, mode="qef", corner_grads=G)
+    w = {k: rng.normal(0, 1, ref0[k].shape) for k in ("L_dev", "p_alpha", "n_alpha")}
+
+    st = torch.from_numpy(s).float().cuda().requires_grad_(True)
+    dt = torch.from_numpy(deform).float().cuda().requires_grad_(True)
+    gt = torch.from_numpy(G).float().cuda().requires_grad_(True)
+    o = SparseDiffDMC(device="cuda").eval()(vox.cuda(), st, cidx.cuda(), 24, deform=dt, corner_gradients=gt)
+    assert np.array_equal(o.faces.cpu().numpy(), ref0["faces"])
+    wt = {k: torch.from_numpy(v).float().cuda() for k, v in w.items()}
+    loss = ((o.vertices ** 2).sum() + (wt["L_dev"] * o.L_dev).sum() + (wt["p_alpha"] * o.p_alpha).sum()
+            + (wt["n_alpha"] * o.n_alpha).sum())
+    loss.backward()
+    gs, gd, gg = (t.grad.cpu().double().numpy() for t in (st, dt, gt))
+
+    def f(ss=s, dd=deform, gg_=G):
+        return _qef_loss(D.forward(vox.numpy(), ss, cidx.numpy(), 24, deform=dd, dtype=np.float64, mode="qef",
+                                   corner_grads=gg_), w)
+
+    h = 1e-6
+    active = np.nonzero(np.abs(gs) > 1e-6)[0]
+    pick = rng.choice(active, size=min(30, active.shape[0]), replace=False)
+    for i in pick:
+        sp, sm = s.copy(), s.copy()
+        sp[i] += h
+        sm[i] -= h
+        fdv = (f(ss=sp) - f(ss=sm)) / (2 * h)
+        assert abs(fdv - gs[i]) <= 2e-3 * max(1.0, abs(fdv)), ("sdf", i, fdv, gs[i])
+    for i in pick[:10]:
+        for a in range(3):
+            dp, dm = deform.copy(), deform.copy()
+            dp[i, a] += h
+            dm[i, a] -= h
+            fdv = (f(dd=dp) - f(dd=dm)) / (2 * h)
+            assert abs(fdv - gd[i, a]) <= 2e-3 * max(1.0, abs(fdv)), ("deform", i, a, fdv, gd[i, a])
+    gact = np.nonzero(np.abs(gg).sum(1) > 1e-6)[0]
+    for i in rng.choice(gact, size=min(10, gact.shape[0]), replace=False):
+        for a in range(3):
+            gp, gm = G.copy(), G.copy()
+            gp[i, a] += h
+            gm[i, a] -= h
+            fdv = (f(gg_=gp) - f(gg_=gm)) / (2 * h)
+            assert abs(fdv - gg[i, a]) <= 2e-3 * max(1.0, abs(fdv)), ("corner gradient", i, a, fdv, gg[i, a])
+
+
+def _corner_positions(vox, cidx, res, deform):
+    from oracle import dmc_oracle as D
+
+    M = deform.shape[0]
+    pos = np.zeros((M, 3))
+    pos[cidx.reshape(-1)] = (vox[:, None, :] + D.CUBE_CORNERS[None]).reshape(-1, 3)
+    return pos * (2.0 / res) - 1.0 + deform
 
 
 @pytest.mark.parametrize("mode", ["train", "eval"])
