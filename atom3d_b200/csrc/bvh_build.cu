@@ -618,11 +618,24 @@ __global__ void write_tris_kernel(const float* __restrict__ V, const int64_t* __
   const float e1 = v32x * v32x + v32y * v32y + v32z * v32z;
   const float e2 = v13x * v13x + v13y * v13y + v13z * v13z;
   const int local = (int)((int64_t)f - face_off[m]);
+  // dual-basis coefficients of the barycentric projection (e0 = b - a,
+  // e1 = c - a): u = A (v.e0) - B (v.e1), w = C (v.e1) - B (v.e0) with
+  // A = d11 / |n|^2, B = d01 / |n|^2, C = d00 / |n|^2 (|n|^2 = d00 d11 - d01^2),
+  // from the FP32 edge vectors the test forms, divided in FP64
+  const float f0x = b.x - a.x, f0y = b.y - a.y, f0z = b.z - a.z;
+  const float f1x = c.x - a.x, f1y = c.y - a.y, f1z = c.z - a.z;
+  const double d00 = (double)f0x * f0x + (double)f0y * f0y + (double)f0z * f0z;
+  const double d01 = (double)f0x * f1x + (double)f0y * f1y + (double)f0z * f1z;
+  const double d11 = (double)f1x * f1x + (double)f1y * f1y + (double)f1z * f1z;
+  const double den = (double)nsqf > 0.0 ? (double)nsqf : 1.0;
+  const bool near_degenerate = (flags & kTriFlagNearDegenerate) != 0;
   TriRec r;
   r.a = make_float4(a.x, a.y, a.z, __int_as_float(local));
-  r.b = make_float4(b.x, b.y, b.z, __uint_as_float(flags));
-  r.c = make_float4(c.x, c.y, c.z, nsqf > 0.f ? 1.0f / nsqf : 0.f);
-  r.r = make_float4(1.0f / fmaxf(e0, 1e-12f), 1.0f / fmaxf(e1, 1e-12f), 1.0f / fmaxf(e2, 1e-12f), 0.f);
+  r.b = make_float4(b.x, b.y, b.z, (float)(d01 / den));
+  // a negative c.w marks a near-degenerate triangle (evaluated in FP64)
+  r.c = make_float4(c.x, c.y, c.z, near_degenerate ? -1.0f : (float)(d11 / den));
+  r.r = make_float4(1.0f / fmaxf(e0, 1e-12f), 1.0f / fmaxf(e1, 1e-12f), 1.0f / fmaxf(e2, 1e-12f),
+                    (float)(d00 / den));
   tris[j] = r;
 }
 

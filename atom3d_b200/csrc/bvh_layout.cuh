@@ -16,11 +16,16 @@
 // so the decoded box always contains the exact one.
 //
 // TriRec (64 B): float4 a (xyz, w = original face id as int bits),
-//                float4 b (xyz, w = flag bits),
-//                float4 c (xyz, w = 1 / |n|^2 with n = (b - a) x (a - c)),
+//                float4 b (xyz, w = B = d01 / |n|^2),
+//                float4 c (xyz, w = A = d11 / |n|^2, or -1 for a
+//                          near-degenerate triangle, evaluated in FP64),
 //                float4 r (1 / max(|b-a|^2, 1e-12), 1 / max(|c-b|^2, 1e-12),
-//                          1 / max(|a-c|^2, 1e-12), 0)
-// The reciprocals let the per-triangle distance test run without a divide.
+//                          1 / max(|a-c|^2, 1e-12), C = d00 / |n|^2)
+// with e0 = b - a, e1 = c - a, d00 = e0.e0, d01 = e0.e1, d11 = e1.e1 and
+// |n|^2 = d00 d11 - d01^2: the dual-basis coefficients of the barycentric
+// projection and the edge reciprocals let the per-triangle distance test run
+// without a cross product or a divide.  a, b, c are the mesh's own vertex
+// coordinates (the bit-exact ray, SAT and clip tests read only them).
 #pragma once
 
 #include <stdint.h>

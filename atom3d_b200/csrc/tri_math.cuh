@@ -98,27 +98,31 @@ struct TriEval {
   }
 };
 
-// FP32 squared distance with the triangle's precomputed reciprocals (no
-// divide): same branch structure and products as TriEval<float>::dist_sq.
-__device__ __forceinline__ float dist_sq_rcp(V3<float> p, V3<float> a, V3<float> b, V3<float> c, float inv_nsq,
-                                             float inv_e0, float inv_e1, float inv_e2) {
-  const V3<float> v21 = sub(b, a), v32 = sub(c, b), v13 = sub(a, c);
-  const V3<float> p1 = sub(p, a), p2 = sub(p, b), p3 = sub(p, c);
-  const V3<float> nor = cross(v21, v13);
-  const float nsq = dot(nor, nor);
-  const bool inside = nsq >= 1e-12f && dot(cross(v21, nor), p1) >= 0.f && dot(cross(v32, nor), p2) >= 0.f &&
-                      dot(cross(v13, nor), p3) >= 0.f;
-  if (inside) {
-    const float d = dot(nor, p1);
-    return d * d * inv_nsq;
+// FP32 squared distance by barycentric projection.  p - a projects onto the
+// plane at a + u e0 + w e1 (e0 = b - a, e1 = c - a) with u = A d1 - B d2,
+// w = C d2 - B d1, d1 = (p - a).e0, d2 = (p - a).e1 and the triangle's
+// precomputed dual-basis coefficients A, B, C; inside the triangle
+// (u, w >= 0, u + w <= 1) the distance is that to the projection, else the
+// nearest of the three clamped edge distances (edges a-b and a-c reuse d1
+// and d2).  The same point-triangle distance as TriEval::dist_sq: the
+// region test is made on the barycentrics instead of the three edge-plane
+// signs, so the two agree to rounding where a point sits on a region border.
+__device__ __forceinline__ float dist_sq_bary(V3<float> p, V3<float> a, V3<float> b, V3<float> c, float A, float B,
+                                              float C, float inv_ab, float inv_bc, float inv_ca) {
+  const V3<float> e0 = sub(b, a), e1 = sub(c, a), v = sub(p, a);
+  const float d1 = dot(v, e0), d2 = dot(v, e1);
+  const float u = A * d1 - B * d2, w = C * d2 - B * d1;
+  if (u >= 0.f && w >= 0.f && u + w <= 1.f) {
+    const V3<float> q = sub(v, add(scl(e0, u), scl(e1, w)));
+    return dot(q, q);
   }
-  auto edge = [](V3<float> v, V3<float> q, float inv) {
-    const float t = clamp01(dot(v, q) * inv);
-    const V3<float> e = sub(scl(v, t), q);
-    return dot(e, e);
-  };
-  const float e1 = edge(v21, p1, inv_e0), e2 = edge(v32, p2, inv_e1), e3 = edge(v13, p3, inv_e2);
-  return e1 < e2 ? (e1 < e3 ? e1 : e3) : (e2 < e3 ? e2 : e3);
+  const float t0 = clamp01(d1 * inv_ab), t2 = clamp01(d2 * inv_ca);
+  const V3<float> r0 = sub(v, scl(e0, t0)), r2 = sub(v, scl(e1, t2));
+  const V3<float> vb = sub(v, e0), ebc = sub(e1, e0);
+  const float t1 = clamp01(dot(vb, ebc) * inv_bc);
+  const V3<float> r1 = sub(vb, scl(ebc, t1));
+  const float q0 = dot(r0, r0), q1 = dot(r1, r1), q2 = dot(r2, r2);
+  return q0 < q1 ? (q0 < q2 ? q0 : q2) : (q1 < q2 ? q1 : q2);
 }
 
 }  // namespace a3d

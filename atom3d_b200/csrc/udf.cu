@@ -102,10 +102,10 @@ __device__ __noinline__ float tri_dist_sq_f64(float ax, float ay, float az, floa
 }
 
 __device__ __forceinline__ float tri_dist_sq(const TriRec& t, float px, float py, float pz) {
-  if (__float_as_uint(t.b.w) & kTriFlagNearDegenerate)
+  if (t.c.w < 0.f)  // near-degenerate
     return tri_dist_sq_f64(t.a.x, t.a.y, t.a.z, t.b.x, t.b.y, t.b.z, t.c.x, t.c.y, t.c.z, px, py, pz);
-  return dist_sq_rcp(mk(px, py, pz), mk(t.a.x, t.a.y, t.a.z), mk(t.b.x, t.b.y, t.b.z), mk(t.c.x, t.c.y, t.c.z),
-                     t.c.w, t.r.x, t.r.y, t.r.z);
+  return dist_sq_bary(mk(px, py, pz), mk(t.a.x, t.a.y, t.a.z), mk(t.b.x, t.b.y, t.b.z), mk(t.c.x, t.c.y, t.c.z),
+                      t.c.w, t.b.w, t.r.w, t.r.x, t.r.y, t.r.z);
 }
 
 __device__ __forceinline__ TriRec load_tri(const TriRec* tris, uint32_t i) {
@@ -260,7 +260,7 @@ __device__ __noinline__ void finish_query(const TriRec* __restrict__ tris, uint3
     const V3<float> a = mk(t.a.x, t.a.y, t.a.z), b = mk(t.b.x, t.b.y, t.b.z), c = mk(t.c.x, t.c.y, t.c.z);
     const V3<float> p = mk(px, py, pz);
     V3<float> cp;
-    if (__float_as_uint(t.b.w) & kTriFlagNearDegenerate) {
+    if (t.c.w < 0.f) {  // near-degenerate
       const V3<double> cd = TriEval<double>::closest(mk<double>(px, py, pz), mk<double>(a.x, a.y, a.z),
                                                      mk<double>(b.x, b.y, b.z), mk<double>(c.x, c.y, c.z));
       cp = mk((float)cd.x, (float)cd.y, (float)cd.z);
