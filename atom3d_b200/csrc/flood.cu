@@ -153,19 +153,20 @@ __global__ void set_bits_kernel(const int64_t* __restrict__ ijk, int64_t n, Geom
 // each once: mark[b] is the last round b was queued for, raised with
 // atomicMax, and the first raiser appends b to `nxt` (count cnt[(round + 1)
 // % 3]).  Block 0 clears cnt[(round + 2) % 3], the input count of the
-// previous round, for the round after this one.
-__global__ void __launch_bounds__(kBX * kBY) flood_brick_kernel(Geom g, const uint32_t* __restrict__ occ,
-                                                              uint32_t* water, const uint32_t* __restrict__ cur,
-                                                              uint32_t* __restrict__ nxt, uint32_t* __restrict__ mark,
-                                                              uint32_t* __restrict__ cnt, int round, int nbx, int nby,
-                                                              int max_iters) {
+// previous round, for the round after this one.  Rounds run back to back
+// inside one kernel, so everything another block may have written in an
+// earlier round (queue, counts, water) is read through L2 (ld.global.cg),
+// never from a stale L1 line.
+__device__ __forceinline__ void relax_round(const Geom& g, const uint32_t* __restrict__ occ, uint32_t* water,
+                                            const uint32_t* cur, uint32_t* nxt, uint32_t* __restrict__ mark,
+                                            uint32_t* cnt, int round, int nbx, int nby, int max_iters,
+                                            uint32_t (*s_r)[kBX + 2][kBY + 2]) {
   const uint32_t nbricks = (uint32_t)nbx * (uint32_t)nby * (uint32_t)g.nw;
-  const uint32_t n_cur = min(cnt[round % 3], nbricks);
+  const uint32_t n_cur = min(__ldcg(cnt + round % 3), nbricks);
   if (blockIdx.x == 0 && threadIdx.x == 0) cnt[(round + 2) % 3] = 0u;
   const uint32_t next_round = (uint32_t)round + 1u;
-  __shared__ uint32_t s_r[3][kBX + 2][kBY + 2];  // words w-1, w, w+1 of the rows with halo
   for (uint32_t item = blockIdx.x; item < n_cur; item += gridDim.x) {
-    const int bid = (int)cur[item];
+    const int bid = (int)__ldcg(cur + item);
     const int bw = bid / (nbx * nby);
     const int rem = bid % (nbx * nby);
     const int bxi = rem / nby, byi = rem % nby;
@@ -187,7 +188,6 @@ __global__ void __launch_bounds__(kBX * kBY) flood_brick_kernel(Geom g, const ui
     if (inside) f = ~occ[widx(g, x, y, bw)] & crop_mask(g, x, y, bw);
     __syncthreads();
     const uint32_t orig = s_r[1][tx + 1][ty + 1];
-    bool changed_any = false;
     for (int it = 0; it < max_iters; ++it) {
       uint32_t acc = 0;
       const uint32_t self = s_r[1][tx + 1][ty + 1];
@@ -214,7 +214,6 @@ __global__ void __launch_bounds__(kBX * kBY) flood_brick_kernel(Geom g, const ui
       const uint32_t nw = inside ? fill_runs(self | (acc & f), f) | self : self;
       const bool ch = nw != self;
       if (ch) s_r[1][tx + 1][ty + 1] = nw;
-      changed_any |= ch;
       if (!__syncthreads_or(ch)) break;
     }
     const uint32_t fin = s_r[1][tx + 1][ty + 1];
@@ -234,8 +233,72 @@ __global__ void __launch_bounds__(kBX * kBY) flood_brick_kernel(Geom g, const ui
         }
       }
     }
-    (void)changed_any;
   }
+}
+
+// Grid-wide barrier of a cooperative launch (every block resident): bar[0]
+// counts arrivals, bar[1] is the generation the last arrival advances.  A
+// block reads the generation before it arrives, so the advance cannot be
+// missed; the waiting spins are bounded (about a second), after which the
+// barrier reports failure instead of waiting on.
+constexpr uint32_t kBarrierSpins = 1u << 24;
+__device__ __forceinline__ bool grid_barrier(uint32_t* bar) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t* vgen = bar + 1;
+    const uint32_t gen = *vgen;
+    __threadfence();
+    bool ok = true;
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      for (uint32_t spins = 0; *vgen == gen; ++spins) {
+        if (spins >= kBarrierSpins) {
+          ok = false;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok ? 1 : 0;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// All relaxation rounds in one cooperative launch of the resident blocks:
+// round r relaxes the bricks queued for it, a grid barrier closes the round,
+// and every block reads the next queue's length after the barrier, so all
+// blocks stop together when it is empty.  sync: [0..1] barrier words, [2]
+// status (bit 0: the round cap was reached with bricks still queued, bit 1:
+// a barrier wait ran out), [3] the number of rounds run.
+__global__ void __launch_bounds__(kBX * kBY)
+    flood_rounds_kernel(Geom g, const uint32_t* __restrict__ occ, uint32_t* water, uint32_t* list_a, uint32_t* list_b,
+                        uint32_t* __restrict__ mark, uint32_t* cnt, int nbx, int nby, int max_iters, int max_rounds,
+                        uint32_t* sync) {
+  __shared__ uint32_t s_r[3][kBX + 2][kBY + 2];  // words w-1, w, w+1 of the rows with halo
+  int round = 0;
+  for (;;) {
+    const uint32_t* cur = (round & 1) ? list_b : list_a;
+    uint32_t* nxt = (round & 1) ? list_a : list_b;
+    relax_round(g, occ, water, cur, nxt, mark, cnt, round, nbx, nby, max_iters, s_r);
+    const bool ok = grid_barrier(sync);
+    ++round;
+    if (!ok) {
+      if (threadIdx.x == 0) atomicOr(sync + 2, 2u);
+      break;
+    }
+    if (__ldcg(cnt + round % 3) == 0u) break;
+    if (round >= max_rounds) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(sync + 2, 1u);
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) sync[3] = (uint32_t)round;
 }
 
 // label volumes.  slot order: 0 water(pure) 1 dry 2 tide(collision) 3 dam
@@ -590,35 +653,34 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
     return A3D_OK;
   }
   counts_out[kLabels] = 0;
-  // Relaxation rounds over queued bricks.  A grid of the resident blocks
-  // strides over each round's queue, so a round costs what its queue holds,
-  // not one block per brick of the volume.  Rounds are launched
-  // kRoundsPerCheck at a time and the next round's queue length is read
-  // once per group: a round with an empty queue only costs its launch.
-  int dev = 0, sms = 0, per_sm = 0;
+  // Relaxation rounds over queued bricks, all in one cooperative launch of
+  // the resident blocks (they stride over each round's queue, so a round
+  // costs what its queue holds); the rounds end on the device when the next
+  // queue is empty, and one host read takes the status and the round count.
+  int dev = 0, sms = 0, per_sm = 0, coop = 0;
   A3D_CUDA_TRY(cudaGetDevice(&dev));
   A3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, flood_brick_kernel, kBX * kBY, 0));
+  A3D_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  A3D_REQUIRE(coop != 0, A3D_ERR_CUDA, "a3d_flood_fill: the device does not support cooperative launches");
+  A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, flood_rounds_kernel, kBX * kBY, 0));
   const int64_t resident = (int64_t)(sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
   const unsigned grid = (unsigned)(nbricks < resident ? nbricks : resident);
-  constexpr int kRoundsPerCheck = 4;
-  int rounds = 0;
-  const int max_rounds = 1 << 20;
-  uint32_t queued = 1;
-  while (rounds < max_rounds) {
-    for (int k = 0; k < kRoundsPerCheck; ++k, ++rounds) {
-      const uint32_t* cur = (rounds & 1) ? w.list_b : w.list_a;
-      uint32_t* nxt = (rounds & 1) ? w.list_a : w.list_b;
-      flood_brick_kernel<<<grid, kBX * kBY, 0, s>>>(g, w.occ, w.water, cur, nxt, w.mark, qcnt, rounds, nbx, nby,
-                                                    4 * (kBX + kBY));
-      A3D_LAUNCH_CHECK();
-    }
-    A3D_CUDA_TRY(cudaMemcpyAsync(&queued, qcnt + rounds % 3, 4, cudaMemcpyDeviceToHost, s));
-    A3D_CUDA_TRY(cudaStreamSynchronize(s));
-    if (!queued) break;
-  }
+  // barrier, status and round words: misc[24..27] (cleared with misc
+  // above; misc[8..21] collects the label totals below)
+  uint32_t* sync = w.misc + 24;
+  int max_rounds = 1 << 20;
+  int max_iters = 4 * (kBX + kBY);
+  void* args[] = {(void*)&g, (void*)&w.occ, (void*)&w.water, (void*)&w.list_a, (void*)&w.list_b, (void*)&w.mark,
+                  (void*)&qcnt, (void*)&nbx, (void*)&nby, (void*)&max_iters, (void*)&max_rounds, (void*)&sync};
+  A3D_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)flood_rounds_kernel, dim3(grid), dim3(kBX * kBY), args, 0,
+                                           s));
+  uint32_t hs[2] = {0, 0};
+  A3D_CUDA_TRY(cudaMemcpyAsync(hs, sync + 2, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  A3D_CUDA_TRY(cudaStreamSynchronize(s));
+  A3D_REQUIRE(!(hs[0] & 2u), A3D_ERR_TIMEOUT, "a3d_flood_fill: a grid barrier of the relaxation timed out");
   // bricks still queued after the round cap: the water is incomplete
-  A3D_REQUIRE(queued == 0, A3D_ERR_OVERFLOW, "a3d_flood_fill: relaxation did not converge within 2^20 rounds");
+  A3D_REQUIRE(!(hs[0] & 1u), A3D_ERR_OVERFLOW, "a3d_flood_fill: relaxation did not converge within 2^20 rounds");
+  const int rounds = (int)hs[1];
   if (rounds_out) *rounds_out = rounds;
   const unsigned gw = (unsigned)ceil_div(nwords, 256);
   labels_kernel<<<gw, 256, 0, s>>>(g, w.occ, w.water, w.lab, nwords);

@@ -253,9 +253,12 @@ size_t a3d_flood_workspace_bytes(const a3d_flood_geom* geom);
  * [7] = 0 and [8] = 1 when the seed is occupied (then nothing else is
  * computed, like the reference's empty result).  The labelled volumes and
  * their per-tile counts stay in the workspace for a3d_flood_extract /
- * a3d_flood_test.  rounds_out (nullable): relaxation rounds launched (a
- * multiple of 4).  A3D_ERR_OVERFLOW when bricks are still queued after 2^20
- * rounds (the water would be incomplete).  The volume must hold fewer than 2^37 voxels (2^32
+ * a3d_flood_test.  rounds_out (nullable): relaxation rounds run; all rounds
+ * run in one cooperative launch of the resident blocks, separated by grid
+ * barriers and ended on the device when the next round's queue is empty (one
+ * host read per call).  A3D_ERR_OVERFLOW when bricks are still queued after
+ * 2^20 rounds (the water would be incomplete); A3D_ERR_TIMEOUT when a grid
+ * barrier waited about a second.  The volume must hold fewer than 2^37 voxels (2^32
  * words). */
 int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood_geom* geom,
                    void* workspace, size_t workspace_bytes, int64_t* counts_out,
