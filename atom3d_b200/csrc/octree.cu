@@ -60,6 +60,8 @@ __device__ __forceinline__ void cube_box(int x, int y, int z, const LevelGeom& g
   }
 }
 
+constexpr uint32_t kNoHint = 0xffffffffu;  // no triangle to try first
+
 // candidate k of this level: either cube k of the full min_level grid
 // (meshgrid 'ij': x slowest, z fastest) or child (k & 7) of parent k >> 3
 __device__ __forceinline__ void candidate_ijk(int64_t k, bool first_level, int res, const int32_t* parents, int& x,
@@ -77,10 +79,38 @@ __device__ __forceinline__ void candidate_ijk(int64_t k, bool first_level, int r
   }
 }
 
+// A candidate's hit decision: the triangle that hit its parent first (most
+// children of a hit voxel meet the same triangle, which is several voxels
+// wide at the finest levels), else an any-hit walk from the root.  The SAT
+// predicate does not depend on the tree (the walk's pruning box is grown to
+// cover sat_eps and rounding), so a hint that hits gives the decision the
+// walk would give.  The hitting triangle's slot goes to ctri for the
+// candidate's own children.
+template <typename Stack>
+__device__ __forceinline__ int candidate_hit(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
+                                             const float* mn, const float* mx, uint32_t hint, Stack& st,
+                                             uint32_t& hit_slot) {
+  if (hint != kNoHint) {
+    const float4* p = reinterpret_cast<const float4*>(tris + hint);
+    TriRec t;
+    t.a = __ldg(p); t.b = __ldg(p + 1); t.c = __ldg(p + 2); t.r = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (sat_test(t, mn[0], mn[1], mn[2], mx[0], mx[1], mx[2])) {
+      hit_slot = hint;
+      return 1;
+    }
+  }
+  return box_traverse(nodes, tris, mn[0], mn[1], mn[2], mx[0], mx[1], mx[2], st, [&](const TriRec& t, uint32_t slot) {
+    if (!sat_test(t, mn[0], mn[1], mn[2], mx[0], mx[1], mx[2])) return false;
+    hit_slot = slot;
+    return true;
+  });
+}
+
 __global__ void __launch_bounds__(kSatThreads)
     octree_level_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris, int64_t ncand,
-                        bool first_level, int res, const int32_t* __restrict__ parents, LevelGeom g,
-                        uint32_t* __restrict__ flags, uint32_t* __restrict__ spill, uint32_t* __restrict__ nspill) {
+                        bool first_level, int res, const int32_t* __restrict__ parents,
+                        const uint32_t* __restrict__ parent_hint, LevelGeom g, uint32_t* __restrict__ flags,
+                        uint32_t* __restrict__ ctri, uint32_t* __restrict__ spill, uint32_t* __restrict__ nspill) {
   __shared__ uint32_t s_stack[kSatDepth * kSatThreads];
   const int64_t k = (int64_t)blockIdx.x * kSatThreads + threadIdx.x;
   if (k >= ncand) return;
@@ -89,19 +119,24 @@ __global__ void __launch_bounds__(kSatThreads)
   float mn[3], mx[3];
   cube_box(x, y, z, g, mn, mx);
   ShStack st{s_stack + threadIdx.x, 0};
-  const int r = box_any_hit(nodes, tris, mn[0], mn[1], mn[2], mx[0], mx[1], mx[2], st);
+  uint32_t slot = kNoHint;
+  const uint32_t hint = parent_hint ? parent_hint[k >> 3] : kNoHint;
+  const int r = candidate_hit(nodes, tris, mn, mx, hint, st, slot);
   if (r == 2) {
     flags[k] = 0;
     spill[atomicAdd(nspill, 1u)] = (uint32_t)k;
   } else {
     flags[k] = (uint32_t)r;
+    ctri[k] = slot;
   }
 }
 
 __global__ void octree_spill_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
-                                    bool first_level, int res, const int32_t* __restrict__ parents, LevelGeom g,
-                                    uint32_t* __restrict__ flags, const uint32_t* __restrict__ spill,
-                                    const uint32_t* __restrict__ nspill, int* __restrict__ overflow) {
+                                    bool first_level, int res, const int32_t* __restrict__ parents,
+                                    const uint32_t* __restrict__ parent_hint, LevelGeom g,
+                                    uint32_t* __restrict__ flags, uint32_t* __restrict__ ctri,
+                                    const uint32_t* __restrict__ spill, const uint32_t* __restrict__ nspill,
+                                    int* __restrict__ overflow) {
   const uint32_t m = *nspill;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t k = spill[t];
@@ -111,9 +146,13 @@ __global__ void octree_spill_kernel(const WideNode* __restrict__ nodes, const Tr
     cube_box(x, y, z, g, mn, mx);
     LcStack st;
     st.sp = 0;
-    const int r = box_any_hit(nodes, tris, mn[0], mn[1], mn[2], mx[0], mx[1], mx[2], st);
+    uint32_t slot = kNoHint;
+    // the hint was tested in the level kernel; the walk decides
+    const int r = candidate_hit(nodes, tris, mn, mx, kNoHint, st, slot);
+    (void)parent_hint;
     if (r == 2) atomicExch(overflow, 1);
     flags[k] = r == 1 ? 1u : 0u;
+    ctri[k] = slot;
   }
 }
 
@@ -121,7 +160,8 @@ __global__ void octree_spill_kernel(const WideNode* __restrict__ nodes, const Tr
 // after the scan pass; hit tested again from the candidate's own flag copy)
 __global__ void octree_compact_kernel(int64_t ncand, bool first_level, int res, const int32_t* __restrict__ parents,
                                       const uint8_t* __restrict__ hit, const uint32_t* __restrict__ offs,
-                                      int32_t* __restrict__ out32, int64_t* __restrict__ out64) {
+                                      const uint32_t* __restrict__ ctri, int32_t* __restrict__ out32,
+                                      uint32_t* __restrict__ hint_out, int64_t* __restrict__ out64) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ncand || !hit[k]) return;
   int x, y, z;
@@ -131,6 +171,7 @@ __global__ void octree_compact_kernel(int64_t ncand, bool first_level, int res, 
     out64[3 * o] = x; out64[3 * o + 1] = y; out64[3 * o + 2] = z;
   } else {
     out32[3 * o] = x; out32[3 * o + 1] = y; out32[3 * o + 2] = z;
+    hint_out[o] = ctri[k];
   }
 }
 
@@ -216,6 +257,9 @@ namespace {
 struct OctWs {
   int32_t* list_a;
   int32_t* list_b;
+  uint32_t* hint_a;  // per entry of list_a: the triangle that hit it
+  uint32_t* hint_b;
+  uint32_t* ctri;    // per candidate: the triangle that hit it
   uint32_t* flags;
   uint8_t* hit;
   uint32_t* scan_tmp;
@@ -226,6 +270,9 @@ size_t carve_oct(OctWs& w, Workspace& ws, int64_t cap) {
   const int64_t ncap = 8 * cap;
   w.list_a = ws.take<int32_t>(3 * cap);
   w.list_b = ws.take<int32_t>(3 * cap);
+  w.hint_a = ws.take<uint32_t>(cap);
+  w.hint_b = ws.take<uint32_t>(cap);
+  w.ctri = ws.take<uint32_t>(ncap);
   w.flags = ws.take<uint32_t>(ncap);
   w.hit = ws.take<uint8_t>(ncap);
   w.scan_tmp = ws.take<uint32_t>((int64_t)scan_workspace_elems(ncap));
@@ -263,7 +310,9 @@ extern "C" int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo
   const TriRec* tris = (const TriRec*)bvh->tris;
   int64_t ncand = first;
   const int32_t* parents = nullptr;
+  const uint32_t* parent_hint = nullptr;
   int32_t* next = w.list_a;
+  uint32_t* next_hint = w.hint_a;
   *count_out = 0;
   for (int level = min_level; level <= max_level; ++level) {
     const bool first_level = level == min_level;
@@ -279,11 +328,11 @@ extern "C" int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo
     }
     A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, 8 * sizeof(uint32_t), s));
     const unsigned gk = (unsigned)ceil_div(ncand, kSatThreads);
-    octree_level_kernel<<<gk, kSatThreads, 0, s>>>(nodes, tris, ncand, first_level, res, parents, g, w.flags, w.spill,
-                                                   w.misc + 1);
+    octree_level_kernel<<<gk, kSatThreads, 0, s>>>(nodes, tris, ncand, first_level, res, parents, parent_hint, g,
+                                                   w.flags, w.ctri, w.spill, w.misc + 1);
     A3D_LAUNCH_CHECK();
-    octree_spill_kernel<<<num_sms() * 4, 64, 0, s>>>(nodes, tris, first_level, res, parents, g, w.flags, w.spill,
-                                                   w.misc + 1, (int*)(w.misc + 2));
+    octree_spill_kernel<<<num_sms() * 4, 64, 0, s>>>(nodes, tris, first_level, res, parents, parent_hint, g, w.flags,
+                                                   w.ctri, w.spill, w.misc + 1, (int*)(w.misc + 2));
     A3D_LAUNCH_CHECK();
     flags_to_u8_kernel<<<(unsigned)ceil_div(ncand, 256), 256, 0, s>>>(w.flags, ncand, w.hit);
     A3D_LAUNCH_CHECK();
@@ -304,7 +353,8 @@ extern "C" int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo
       A3D_REQUIRE(false, A3D_ERR_WORKSPACE, "octree: level capacity exceeded");
     }
     octree_compact_kernel<<<(unsigned)ceil_div(ncand, 256), 256, 0, s>>>(ncand, first_level, res, parents, w.hit,
-                                                                         w.flags, last ? nullptr : next,
+                                                                         w.flags, w.ctri, last ? nullptr : next,
+                                                                         last ? nullptr : next_hint,
                                                                          last ? out_ijk : nullptr);
     A3D_LAUNCH_CHECK();
     if (last || total == 0) {
@@ -312,7 +362,9 @@ extern "C" int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo
       break;
     }
     parents = next;
+    parent_hint = next_hint;
     next = (next == w.list_a) ? w.list_b : w.list_a;
+    next_hint = (next_hint == w.hint_a) ? w.hint_b : w.hint_a;
     ncand = total * 8;
   }
   return A3D_OK;

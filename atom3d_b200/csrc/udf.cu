@@ -496,14 +496,13 @@ constexpr int kFinCap = 64;
 
 struct TaskSmem {
   uint2 stack[kTaskDepth][32];
-  float px[32], py[32], pz[32];
+  float4 p[32];  // owners' query points (w unused): one 16-B read per task
   uint32_t nref[32];
   uint8_t nown[32];
   float boxd[32 * kBoxStride];
   uint32_t boxr[32 * kBoxStride];
   uint32_t tidx[kTaskTriCap];
-  uint8_t town[kTaskTriCap];
-  uint8_t tpos[kTaskTriCap];
+  uint8_t town[kTaskTriCap];  // owner lane | position in its leaf << 5
   float trid[kMaxLeafTris * kTriRow];
   uint32_t fin_q[kFinCap];
   uint32_t fin_tri[kFinCap];
@@ -559,7 +558,7 @@ __global__ void __maxnreg__(kTaskMaxRegs)
     qi = perm ? (int64_t)perm[k] : k;
     root = kBatch ? sel.root_of(qi) : 0u;
     px = pts[3 * qi]; py = pts[3 * qi + 1]; pz = pts[3 * qi + 2];
-    S.px[lane] = px; S.py[lane] = py; S.pz[lane] = pz;
+    S.p[lane] = make_float4(px, py, pz, 0.f);
     bsq = INFINITY;
     if (bound) {
       const float b = bound[qi];
@@ -707,8 +706,7 @@ __global__ void __maxnreg__(kTaskMaxRegs)
     if (tcnt > 0) {
       for (int i = 0; i < tcnt; ++i) {
         S.tidx[toff + i] = f0 + i;
-        S.town[toff + i] = (uint8_t)lane;
-        S.tpos[toff + i] = (uint8_t)i;
+        S.town[toff + i] = (uint8_t)(lane | (i << 5));
       }
       if (kStats) ctr.tris += tcnt;
     }
@@ -719,13 +717,16 @@ __global__ void __maxnreg__(kTaskMaxRegs)
       const int o = S.nown[r];
       float d;
       uint32_t cr;
-      quad_child_box(T, S.nref[r], c, S.px[o], S.py[o], S.pz[o], d, cr);
+      const float4 q = S.p[o];
+      quad_child_box(T, S.nref[r], c, q.x, q.y, q.z, d, cr);
       S.boxd[r * kBoxStride + c] = d;
       S.boxr[r * kBoxStride + c] = cr;
     }
     for (int t = lane; t < ttotal; t += 32) {
-      const int o = S.town[t];
-      S.trid[S.tpos[t] * kTriRow + o] = tri_dist_sq(T.tri(S.tidx[t]), S.px[o], S.py[o], S.pz[o]);
+      const uint32_t op = S.town[t];
+      const int o = (int)(op & 31u);
+      const float4 q = S.p[o];
+      S.trid[(op >> 5) * kTriRow + o] = tri_dist_sq(T.tri(S.tidx[t]), q.x, q.y, q.z);
     }
     __syncwarp();
     // (d) owners consume their results
