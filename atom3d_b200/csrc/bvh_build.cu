@@ -331,9 +331,15 @@ __device__ __forceinline__ float half_area(float4 lo, float4 hi) {
 }
 
 // Cost weights of the SAH-optimal collapse: a wide-node visit against one
-// triangle test, as measured on the closest-point traversal (a 4-box node
-// visit costs about 6.7 triangle tests: 16M-query workload, leaves of 4 vs 8)
-constexpr float kCostNode = 6.7f, kCostTri = 1.0f;
+// triangle test, as measured on the closest-point traversal.  With the
+// barycentric triangle test a 4-box node visit costs more triangle tests than
+// before: on the 16M-query workload the traversal time is flat for weights
+// 12-24 and lowest near 16 (148.4 ms; 150.6 ms at the 6.7 fitted for the
+// cross-product test, 156.3 ms at 5)
+#ifndef A3D_SAH_NODE_COST
+#define A3D_SAH_NODE_COST 16.0f
+#endif
+constexpr float kCostNode = A3D_SAH_NODE_COST, kCostTri = 1.0f;
 
 // 5. refit: leaf boxes from sorted triangles, unions bottom-up; and, at each
 // internal node, the SAH-optimal collapse costs.  cost[i] (i = 1..4) is the

@@ -499,8 +499,7 @@ struct TaskSmem {
   float4 p[32];  // owners' query points (w unused): one 16-B read per task
   uint32_t nref[32];
   uint8_t nown[32];
-  float boxd[32 * kBoxStride];
-  uint32_t boxr[32 * kBoxStride];
+  uint2 box[32 * kBoxStride];  // (distance bits, child ref) per child-box task
   uint32_t tidx[kTaskTriCap];
   uint8_t town[kTaskTriCap];  // owner lane | position in its leaf << 5
   float trid[kMaxLeafTris * kTriRow];
@@ -719,8 +718,7 @@ __global__ void __maxnreg__(kTaskMaxRegs)
       uint32_t cr;
       const float4 q = S.p[o];
       quad_child_box(T, S.nref[r], c, q.x, q.y, q.z, d, cr);
-      S.boxd[r * kBoxStride + c] = d;
-      S.boxr[r * kBoxStride + c] = cr;
+      S.box[r * kBoxStride + c] = make_uint2(__float_as_uint(d), cr);
     }
     for (int t = lane; t < ttotal; t += 32) {
       const uint32_t op = S.town[t];
@@ -735,8 +733,9 @@ __global__ void __maxnreg__(kTaskMaxRegs)
       uint32_t r[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        d[c] = S.boxd[kBoxStride * nrank + c];
-        r[c] = S.boxr[kBoxStride * nrank + c];
+        const uint2 e = S.box[kBoxStride * nrank + c];
+        d[c] = __uint_as_float(e.x);
+        r[c] = e.y;
       }
       if (phase == kProbe) {
         // greedy: the (distance, ref)-smallest child
