@@ -33,6 +33,10 @@
     if (_s != A3D_OK) return _s;                            \
   } while (0)
 
+// launch `kernel` with programmatic dependent launch (see launch_pdl)
+#define A3D_PDL(kernel, grid, block, smem, stream, ...) \
+  A3D_CUDA_TRY(::a3d::launch_pdl(kernel, grid, block, smem, stream, __VA_ARGS__))
+
 #define A3D_REQUIRE(cond, code, msg)                        \
   do {                                                      \
     if (!(cond)) {                                          \
@@ -52,6 +56,31 @@ int num_sms();
 constexpr int kMaxDevices = 64;
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Programmatic dependent launch.  A kernel started with launch_pdl may be
+// scheduled while the previous kernel on the stream is still draining, which
+// hides the launch gap between dependent kernels; it must call pdl_wait()
+// (griddepcontrol.wait) before it touches memory, which returns once the
+// previous kernel has completed and its writes are visible, so the effects
+// keep the stream order.  pdl_wait() is a no-op in a kernel launched
+// without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 
 // Bump allocator over a caller-provided workspace.  Every sub-buffer is
 // 256-byte aligned so that vector loads and bulk copies stay aligned.

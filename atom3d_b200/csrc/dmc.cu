@@ -99,6 +99,7 @@ inline float world_scale_host(int res) { return (float)(2.0 / (double)res); }
 // (when given)
 __global__ void init_pos_kernel(int64_t m, const float* __restrict__ deform, float* __restrict__ x,
                                 uint32_t* __restrict__ bad_index) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (bad_index && i == 0) *bad_index = 0u;
   if (i >= m) return;
@@ -111,6 +112,7 @@ __global__ void init_pos_kernel(int64_t m, const float* __restrict__ deform, flo
 }
 
 __global__ void corner_pos_kernel(DmcIn in, float ws, float* __restrict__ x) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= in.n * 8) return;
   const int64_t i = t >> 3;
@@ -134,6 +136,7 @@ __global__ void corner_pos_kernel(DmcIn in, float ws, float* __restrict__ x) {
 template <bool kVec>
 __global__ void corner_case_kernel(DmcIn in, uint8_t* __restrict__ cases, uint32_t* __restrict__ flag,
                                    uint32_t* __restrict__ bad_index) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= in.n) return;
   int64_t v[8];
@@ -170,12 +173,14 @@ struct WordList {
 };
 
 __global__ void gather_words_kernel(WordList l, uint32_t* __restrict__ out) {
+  pdl_wait();
   const int k = (int)threadIdx.x;
   if (k < l.n) out[k] = *l.src[k];
 }
 
 __global__ void compact_kernel(int64_t n, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off,
                                uint32_t* __restrict__ list) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n && flag[i]) list[off[i]] = (uint32_t)i;
 }
@@ -190,6 +195,7 @@ __device__ __forceinline__ uint64_t hash64(uint64_t k) {
 __global__ void prob_insert_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
                                    const uint8_t* __restrict__ cases, unsigned long long* __restrict__ table,
                                    uint64_t mask) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)*ns_dev) return;
   const uint32_t i = list[t];
@@ -208,6 +214,7 @@ __global__ void prob_insert_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev
 __global__ void case_fix_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
                                 const uint8_t* __restrict__ cases, const unsigned long long* __restrict__ table,
                                 uint64_t mask, uint8_t* __restrict__ case_s) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)*ns_dev) return;
   const uint32_t i = list[t];
@@ -248,6 +255,7 @@ __device__ __forceinline__ void edge_world(const DmcIn& in, float ws, const floa
 __global__ void cross_count_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
                                    const uint8_t* __restrict__ cases, uint16_t* __restrict__ mask12,
                                    uint32_t* __restrict__ cnt) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= in.n) return;
   if (t >= (int64_t)*ns_dev) {  // the scan runs over all N entries
@@ -272,6 +280,7 @@ __global__ void __launch_bounds__(kCrossThreads)
     cross_write_kernel(DmcIn in, const uint32_t* __restrict__ ns_dev, const uint32_t* __restrict__ list,
                        const uint16_t* __restrict__ mask12, const uint32_t* __restrict__ off,
                        uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  pdl_wait();
   __shared__ uint64_t s_key[kCrossThreads * 12];
   __shared__ uint32_t s_val[kCrossThreads * 12];
   const int64_t ns = (int64_t)*ns_dev;
@@ -314,6 +323,7 @@ __global__ void __launch_bounds__(kCrossThreads)
 // equals a stable sort by key.
 __global__ void edge_count_kernel(const uint64_t* __restrict__ keys, int64_t nc, uint64_t m,
                                   uint32_t* __restrict__ lo_of, uint32_t* __restrict__ cnt) {
+  pdl_wait();
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nc) return;
   const uint32_t i0 = (uint32_t)(keys[j] >> 32);
@@ -325,6 +335,7 @@ __global__ void edge_scatter_kernel(const uint64_t* __restrict__ keys, const uin
                                     const uint32_t* __restrict__ lo_of, const uint32_t* __restrict__ start,
                                     uint32_t* __restrict__ fill, uint64_t* __restrict__ keys_g,
                                     uint32_t* __restrict__ vals_g, uint32_t* __restrict__ lo_g) {
+  pdl_wait();
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nc) return;
   const uint32_t i0 = lo_of[j];
@@ -337,6 +348,7 @@ __global__ void edge_scatter_kernel(const uint64_t* __restrict__ keys, const uin
 __global__ void edge_rank_kernel(const uint64_t* __restrict__ keys_g, const uint32_t* __restrict__ vals_g, int64_t nc,
                                  const uint32_t* __restrict__ lo_g, const uint32_t* __restrict__ start,
                                  uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  pdl_wait();
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nc) return;
   const uint32_t i0 = lo_g[p];
@@ -353,6 +365,7 @@ __global__ void edge_rank_kernel(const uint64_t* __restrict__ keys_g, const uint
 }
 
 __global__ void run_flag_kernel(const uint64_t* __restrict__ k, int64_t n, uint32_t* __restrict__ flag) {
+  pdl_wait();
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j < n) flag[j] = (j == 0 || k[j] != k[j - 1]) ? 1u : 0u;
 }
@@ -361,6 +374,7 @@ __global__ void run_info_kernel(const uint64_t* __restrict__ k, const uint32_t* 
                                 const uint32_t* __restrict__ flag, const uint32_t* __restrict__ rid, int64_t m,
                                 int32_t* __restrict__ idx_map, int64_t* __restrict__ e0, int64_t* __restrict__ e1,
                                 uint32_t* __restrict__ rfirst) {
+  pdl_wait();
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   // rid holds the exclusive scan of the run-start flags: the run of entry j
@@ -378,6 +392,7 @@ __global__ void run_info_kernel(const uint64_t* __restrict__ k, const uint32_t* 
 // flags beyond ne are zero so the scan can run over nc
 __global__ void quad_flag_kernel(const uint32_t* __restrict__ ne_dev, int64_t nc, const uint32_t* __restrict__ rfirst,
                                  uint32_t* __restrict__ qflag) {
+  pdl_wait();
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nc) return;
   const int64_t ne = *ne_dev;
@@ -397,6 +412,7 @@ __global__ void quad_flag_kernel(const uint32_t* __restrict__ ne_dev, int64_t nc
 // totals at once (counts stay below 2^28: no carry crosses a half).
 __global__ void vd_class_kernel(int64_t ns, const uint8_t* __restrict__ case_s, uint64_t* __restrict__ fa,
                                 uint64_t* __restrict__ fb) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ns) return;
   const int cls = kNumVd[case_s[t]];
@@ -413,6 +429,7 @@ __device__ __forceinline__ uint32_t class_field(uint64_t a, uint64_t b, int cls)
 __global__ void vd_assign_kernel(int64_t ns, const uint8_t* __restrict__ case_s, const uint64_t* __restrict__ ra,
                                  const uint64_t* __restrict__ rb, uint32_t* __restrict__ vd_cube,
                                  uint8_t* __restrict__ vd_slot, uint32_t* __restrict__ vd_ne) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ns) return;
   const int c = case_s[t];
@@ -503,6 +520,7 @@ __global__ void vd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ lis
                           const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
                           const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
                           VdOut out) {
+  pdl_wait();
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const uint32_t t = vd_cube[v];
@@ -588,6 +606,7 @@ __global__ void __launch_bounds__(kQuadThreads)
                 VdNumbering vn, const int64_t* __restrict__ e0, const float* __restrict__ sdf,
                 float iso, int64_t nvd, float* __restrict__ verts, int64_t* __restrict__ faces,
                 int32_t* __restrict__ quads) {
+  pdl_wait();
   __shared__ int32_t s_quad[kQuadThreads][4];
   __shared__ float s_ctr[kQuadThreads * 3];
   const int64_t r0 = (int64_t)blockIdx.x * kQuadThreads;
@@ -642,6 +661,7 @@ struct DmcGrad {
 };
 
 __global__ void quad_bwd_kernel(int64_t nq, int64_t nvd, const int32_t* __restrict__ quads, DmcGrad gr) {
+  pdl_wait();
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nq || !gr.g_verts) return;
   const float* gc = gr.g_verts + 3 * (nvd + q);
@@ -719,6 +739,7 @@ __global__ void __launch_bounds__(128) vd_bwd_kernel(DmcIn in, int64_t nv, const
                                                      const uint32_t* __restrict__ vd_cube,
                                                      const uint8_t* __restrict__ vd_slot,
                                                      const uint32_t* __restrict__ goff, EdgeData ed, DmcGrad gr) {
+  pdl_wait();
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   (void)ed;
@@ -900,6 +921,7 @@ __global__ void vd_feat_kernel(DmcIn in, int64_t nv, int C, const float* __restr
                                const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
                                const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot, EdgeData ed,
                                float* __restrict__ out) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nv * C) return;
   const int64_t v = t / C;
@@ -928,6 +950,7 @@ __global__ void vd_feat_kernel(DmcIn in, int64_t nv, int C, const float* __restr
 
 __global__ void quad_feat_kernel(int64_t nq, int64_t nv, int C, const int32_t* __restrict__ quads,
                                  float* __restrict__ out) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq * C) return;
   const int64_t q = t / C;
@@ -939,6 +962,7 @@ __global__ void quad_feat_kernel(int64_t nq, int64_t nv, int C, const int32_t* _
 
 __global__ void quad_feat_bwd_kernel(int64_t nq, int64_t nv, int C, const int32_t* __restrict__ quads,
                                      const float* __restrict__ g_out, float* __restrict__ scratch) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq * C) return;
   const int64_t q = t / C;
@@ -962,6 +986,7 @@ __global__ void vd_feat_bwd_kernel(DmcIn in, int64_t nv, int C, const float* __r
                                    const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
                                    const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
                                    EdgeData ed, FeatGrad gr) {
+  pdl_wait();
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const uint32_t cs = vd_cube[v];
@@ -1173,33 +1198,26 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   // misc[1]: out-of-range corner ids; misc[4..6] and misc[8..14]: the words
   // the two host reads take
   uint32_t* bad_index = w.misc + 1;
-  A3D_CUDA_TRY(cudaMemsetAsync(bad_index, 0, sizeof(uint32_t), s));
+  A3D_TRY(fill_async<uint32_t>(bad_index, 1, 0u, s));
   if (((uintptr_t)in.cidx & 15u) == 0)
-    corner_case_kernel<true><<<gsz(n), 256, 0, s>>>(in, w.cases, w.flag, bad_index);
+    A3D_PDL(corner_case_kernel<true>, dim3(gsz(n)), dim3(256), 0, s, in, w.cases, w.flag, bad_index);
   else
-    corner_case_kernel<false><<<gsz(n), 256, 0, s>>>(in, w.cases, w.flag, bad_index);
-  A3D_LAUNCH_CHECK();
+    A3D_PDL(corner_case_kernel<false>, dim3(gsz(n)), dim3(256), 0, s, in, w.cases, w.flag, bad_index);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flag, w.off, n, w.scan_tmp, w.off + n, s)));
   // stage B over all N cubes with the surface count on the device
   const uint32_t* ns_dev = w.off + n;
-  compact_kernel<<<gsz(n), 256, 0, s>>>(n, w.flag, w.off, w.list);
-  A3D_LAUNCH_CHECK();
-  A3D_CUDA_TRY(cudaMemsetAsync(w.table, 0xff, (w.table_mask + 1) * sizeof(unsigned long long), s));
-  prob_insert_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.cases, w.table, w.table_mask);
-  A3D_LAUNCH_CHECK();
-  case_fix_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.cases, w.table, w.table_mask, w.case_s);
-  A3D_LAUNCH_CHECK();
-  cross_count_kernel<<<gsz(n), 256, 0, s>>>(in, ns_dev, w.list, w.cases, w.mask12, w.ccnt);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(compact_kernel, dim3(gsz(n)), dim3(256), 0, s, n, w.flag, w.off, w.list);
+  A3D_TRY(fill_async<unsigned long long>(w.table, (int64_t)(w.table_mask + 1), ~0ull, s));
+  A3D_PDL(prob_insert_kernel, dim3(gsz(n)), dim3(256), 0, s, in, ns_dev, w.list, w.cases, w.table, w.table_mask);
+  A3D_PDL(case_fix_kernel, dim3(gsz(n)), dim3(256), 0, s, in, ns_dev, w.list, w.cases, w.table, w.table_mask, w.case_s);
+  A3D_PDL(cross_count_kernel, dim3(gsz(n)), dim3(256), 0, s, in, ns_dev, w.list, w.cases, w.mask12, w.ccnt);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ccnt, w.coff, n, w.scan_tmp, w.coff + n, s)));
-  cross_write_kernel<<<gsz(n, kCrossThreads), kCrossThreads, 0, s>>>(in, ns_dev, w.list, w.mask12, w.coff, w.keys,
+  A3D_PDL(cross_write_kernel, dim3(gsz(n, kCrossThreads)), dim3(kCrossThreads), 0, s, in, ns_dev, w.list, w.mask12, w.coff, w.keys,
                                                                      w.vals);
-  A3D_LAUNCH_CHECK();
   // the one round trip before the edge sort: surface cubes, crossings and
   // the out-of-range flag
   uint32_t h3[3];
-  gather_words_kernel<<<1, 32, 0, s>>>(WordList{{ns_dev, w.coff + n, bad_index}, 3}, w.misc + 4);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(gather_words_kernel, dim3(1), dim3(32), 0, s, WordList{{ns_dev, w.coff + n, bad_index}, 3}, w.misc + 4);
   A3D_CUDA_TRY(cudaMemcpyAsync(h3, w.misc + 4, sizeof(h3), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
   A3D_REQUIRE(h3[2] == 0u, A3D_ERR_ARGUMENT, "dmc_prepare: cube_idx holds a corner id outside [0, num_corners)");
@@ -1209,33 +1227,25 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   if (ns == 0) return A3D_OK;
   // counting sort of the crossings by (key, val); rid / rflag hold the
   // lower endpoints until the run pass needs them
-  A3D_CUDA_TRY(cudaMemsetAsync(w.ecnt, 0, m * sizeof(uint32_t), s));
-  edge_count_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, nc, (uint64_t)m, w.rid, w.ecnt);
-  A3D_LAUNCH_CHECK();
+  A3D_TRY(fill_async<uint32_t>(w.ecnt, m, 0u, s));
+  A3D_PDL(edge_count_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, nc, (uint64_t)m, w.rid, w.ecnt);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ecnt, w.estart, m, w.scan_tmp, w.estart + m, s)));
-  A3D_CUDA_TRY(cudaMemsetAsync(w.ecnt, 0, m * sizeof(uint32_t), s));
-  edge_scatter_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, w.vals, nc, w.rid, w.estart, w.ecnt, w.keys2, w.vals2, w.rflag);
-  A3D_LAUNCH_CHECK();
-  edge_rank_kernel<<<gsz(nc), 256, 0, s>>>(w.keys2, w.vals2, nc, w.rflag, w.estart, w.keys, w.vals);
-  A3D_LAUNCH_CHECK();
-  run_flag_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, nc, w.rflag);
-  A3D_LAUNCH_CHECK();
+  A3D_TRY(fill_async<uint32_t>(w.ecnt, m, 0u, s));
+  A3D_PDL(edge_scatter_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.rid, w.estart, w.ecnt, w.keys2, w.vals2, w.rflag);
+  A3D_PDL(edge_rank_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys2, w.vals2, nc, w.rflag, w.estart, w.keys, w.vals);
+  A3D_PDL(run_flag_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, nc, w.rflag);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.rflag, w.rid, nc, w.scan_tmp, w.misc, s)));
   // idx_map is read only at crossing (cube, edge) pairs, all of which
   // run_info_kernel writes: no clear
-  run_info_kernel<<<gsz(nc), 256, 0, s>>>(w.keys, w.vals, nc, w.rflag, w.rid, m, w.idx_map, w.e0, w.e1, w.rfirst);
-  A3D_LAUNCH_CHECK();
-  quad_flag_kernel<<<gsz(nc), 256, 0, s>>>(w.misc, nc, w.rfirst, w.qflag);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(run_info_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.rflag, w.rid, m, w.idx_map, w.e0, w.e1, w.rfirst);
+  A3D_PDL(quad_flag_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.misc, nc, w.rfirst, w.qflag);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.qflag, w.qoff, nc, w.scan_tmp, w.qoff + nc, s)));
   // dual vertices numbered per vertex-count class (two packed scans)
-  A3D_CUDA_TRY(cudaMemsetAsync(w.vd_ne, 0, (4 * ns + 1) * sizeof(uint32_t), s));
-  vd_class_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, w.cls_a, w.cls_b);
-  A3D_LAUNCH_CHECK();
+  A3D_TRY(fill_async<uint32_t>(w.vd_ne, 4 * ns + 1, 0u, s));
+  A3D_PDL(vd_class_kernel, dim3(gsz(ns)), dim3(256), 0, s, ns, w.case_s, w.cls_a, w.cls_b);
   A3D_TRY((device_exclusive_scan<uint64_t, uint64_t>(w.cls_a, w.cls_ra, ns, w.scan_tmp64, w.cls_ra + ns, s)));
   A3D_TRY((device_exclusive_scan<uint64_t, uint64_t>(w.cls_b, w.cls_rb, ns, w.scan_tmp64, w.cls_rb + ns, s)));
-  vd_assign_kernel<<<gsz(ns), 256, 0, s>>>(ns, w.case_s, w.cls_ra, w.cls_rb, w.vd_cube, w.vd_slot, w.vd_ne);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(vd_assign_kernel, dim3(gsz(ns)), dim3(256), 0, s, ns, w.case_s, w.cls_ra, w.cls_rb, w.vd_cube, w.vd_slot, w.vd_ne);
   // per-vertex edge offsets over the 4 Ns bound (entries past the last
   // vertex are zero)
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.vd_ne, w.goff, 4 * ns, w.scan_tmp, w.goff + 4 * ns, s)));
@@ -1243,9 +1253,8 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   // low word first)
   const uint32_t* ra = reinterpret_cast<const uint32_t*>(w.cls_ra + ns);
   const uint32_t* rb = reinterpret_cast<const uint32_t*>(w.cls_rb + ns);
-  gather_words_kernel<<<1, 32, 0, s>>>(WordList{{w.misc, w.qoff + nc, w.goff + 4 * ns, ra, ra + 1, rb, rb + 1}, 7},
+  A3D_PDL(gather_words_kernel, dim3(1), dim3(32), 0, s, WordList{{w.misc, w.qoff + nc, w.goff + 4 * ns, ra, ra + 1, rb, rb + 1}, 7},
                                        w.misc + 8);
-  A3D_LAUNCH_CHECK();
   uint32_t h7[7];
   A3D_CUDA_TRY(cudaMemcpyAsync(h7, w.misc + 8, sizeof(h7), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1275,13 +1284,11 @@ extern "C" int a3d_dmc_emit(const a3d_dmc_inputs* p, void* workspace, size_t wor
   DmcIn in = make_in(p);
   EdgeData ed{w.e0, w.e1, w.idx_map};
   VdOut out{vertices, l_dev, p_alpha, n_alpha};
-  vd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, out);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(vd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, out);
   (void)nc;
   if (nq > 0) {
-    quad_kernel<<<gsz(ne, kQuadThreads), kQuadThreads, 0, s>>>(ne, nc, w.qflag, w.qoff, w.rfirst, w.vals, VdNumbering{w.case_s, w.cls_ra, w.cls_rb, ns}, w.e0, p->sdf, p->isovalue,
+    A3D_PDL(quad_kernel, dim3(gsz(ne, kQuadThreads)), dim3(kQuadThreads), 0, s, ne, nc, w.qflag, w.qoff, w.rfirst, w.vals, VdNumbering{w.case_s, w.cls_ra, w.cls_rb, ns}, w.e0, p->sdf, p->isovalue,
                                         nv, vertices, faces, w.quads);
-    A3D_LAUNCH_CHECK();
   }
   return A3D_OK;
 }
@@ -1301,14 +1308,12 @@ extern "C" int a3d_dmc_backward(const a3d_dmc_inputs* p, void* workspace, size_t
   if (ns == 0 || nv == 0) return A3D_OK;
   DmcIn in = make_in(p);
   DmcGrad gr{g_vertices, g_l_dev, g_p_alpha, g_n_alpha, g_sdf, g_deform, g_alpha, g_beta, w.g_vd};
-  A3D_CUDA_TRY(cudaMemsetAsync(w.g_vd, 0, 3 * nv * sizeof(float), s));
+  A3D_TRY(fill_async<float>(w.g_vd, 3 * nv, 0.f, s));
   if (nq > 0 && g_vertices) {
-    quad_bwd_kernel<<<gsz(nq), 256, 0, s>>>(nq, nv, w.quads, gr);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(quad_bwd_kernel, dim3(gsz(nq)), dim3(256), 0, s, nq, nv, w.quads, gr);
   }
   EdgeData ed{w.e0, w.e1, w.idx_map};
-  vd_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, gr);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(vd_bwd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, gr);
   return A3D_OK;
 }
 
@@ -1327,11 +1332,9 @@ extern "C" int a3d_dmc_features(const a3d_dmc_inputs* p, void* workspace, size_t
   DmcIn in = make_in(p);
   EdgeData ed{w.e0, w.e1, w.idx_map};
   const int C = channels;
-  vd_feat_kernel<<<gsz(nv * C), 256, 0, s>>>(in, nv, C, features, w.list, w.case_s, w.vd_cube, w.vd_slot, ed, out);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(vd_feat_kernel, dim3(gsz(nv * C)), dim3(256), 0, s, in, nv, C, features, w.list, w.case_s, w.vd_cube, w.vd_slot, ed, out);
   if (with_centres && nq > 0) {
-    quad_feat_kernel<<<gsz(nq * C), 256, 0, s>>>(nq, nv, C, w.quads, out);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(quad_feat_kernel, dim3(gsz(nq * C)), dim3(256), 0, s, nq, nv, C, w.quads, out);
   }
   return A3D_OK;
 }
@@ -1357,13 +1360,11 @@ extern "C" int a3d_dmc_features_backward(const a3d_dmc_inputs* p, void* workspac
   const bool centres = with_centres && nq > 0;
   A3D_REQUIRE(!centres || scratch, A3D_ERR_ARGUMENT, "dmc_features_backward: the centres need a scratch [V, C]");
   if (centres) {
-    quad_feat_bwd_kernel<<<gsz(nq * C), 256, 0, s>>>(nq, nv, C, w.quads, g_out, scratch);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(quad_feat_bwd_kernel, dim3(gsz(nq * C)), dim3(256), 0, s, nq, nv, C, w.quads, g_out, scratch);
   }
   FeatGrad gr{g_out, centres ? scratch : nullptr, g_features, g_sdf, g_alpha, g_beta};
-  vd_feat_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, nv, C, features, w.list, w.case_s, w.vd_cube, w.vd_slot, ed,
+  A3D_PDL(vd_feat_bwd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, nv, C, features, w.list, w.case_s, w.vd_cube, w.vd_slot, ed,
                                                    gr);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
 
@@ -1414,6 +1415,7 @@ size_t carve_grad(GradWs& w, Workspace& ws, int64_t n, int64_t m) {
 constexpr uint32_t kNoCorner = 0xffffffffu;
 
 __global__ void edge_slot_kernel(DmcIn in, uint32_t* __restrict__ slots, uint32_t* __restrict__ conflict) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= in.n * 12) return;
   const int64_t i = t / 12;
@@ -1427,6 +1429,7 @@ __global__ void edge_slot_kernel(DmcIn in, uint32_t* __restrict__ slots, uint32_
 }
 
 __global__ void edge_adj_count_kernel(DmcIn in, uint32_t* __restrict__ cnt) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= in.n * 12) return;
   const int64_t i = t / 12;
@@ -1438,6 +1441,7 @@ __global__ void edge_adj_count_kernel(DmcIn in, uint32_t* __restrict__ cnt) {
 
 __global__ void edge_adj_fill_kernel(DmcIn in, const uint32_t* __restrict__ start, uint32_t* __restrict__ fill,
                                      uint32_t* __restrict__ other) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= in.n * 12) return;
   const int64_t i = t / 12;
@@ -1494,6 +1498,7 @@ __device__ __forceinline__ void add_edge(const DmcIn& in, const float* __restric
 // neighbours sorted ascending, repeats skipped
 __global__ void corner_gradient_slots_kernel(DmcIn in, const float* __restrict__ x, const uint32_t* __restrict__ slots,
                                              float* __restrict__ grad) {
+  pdl_wait();
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= in.m) return;
   double A[6] = {0, 0, 0, 0, 0, 0}, B[3] = {0, 0, 0};
@@ -1514,6 +1519,7 @@ __global__ void corner_gradient_slots_kernel(DmcIn in, const float* __restrict__
 // one thread per corner from the adjacency lists: gather, regularise (1e-4 I), solve
 __global__ void corner_gradient_kernel(DmcIn in, const float* __restrict__ x, const uint32_t* __restrict__ start,
                                        const uint32_t* __restrict__ other, float* __restrict__ grad) {
+  pdl_wait();
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= in.m) return;
   double A[6] = {0, 0, 0, 0, 0, 0}, B[3] = {0, 0, 0};
@@ -1582,6 +1588,7 @@ __global__ void vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float
                               int64_t nv, const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
                               const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
                               const uint32_t* __restrict__ goff, EdgeData ed, VdOut out) {
+  pdl_wait();
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const uint32_t t = vd_cube[v];
@@ -1769,6 +1776,7 @@ __global__ void vd_qef_bwd_kernel(DmcIn in, const float* __restrict__ x, const f
                                   int64_t nv, const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
                                   const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
                                   const uint32_t* __restrict__ goff, QefGrad gq) {
+  pdl_wait();
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const uint32_t t = vd_cube[v];
@@ -2085,6 +2093,7 @@ __global__ void __launch_bounds__(kQuadThreads)
                      VdNumbering vn, const int64_t* __restrict__ e0,
                      const float* __restrict__ sdf, float iso, const float* __restrict__ verts,
                      int64_t* __restrict__ faces) {
+  pdl_wait();
   __shared__ int32_t s_tri[kQuadThreads][6];
   const int64_t r0 = (int64_t)blockIdx.x * kQuadThreads;
   const int64_t r = r0 + threadIdx.x;
@@ -2138,35 +2147,28 @@ extern "C" int a3d_dmc_corner_gradients(const a3d_dmc_inputs* p, void* workspace
   carve_grad(w, ws, n > 0 ? n : 1, m > 0 ? m : 1);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "dmc_corner_gradients: workspace too small");
   if (m == 0) return A3D_OK;
-  A3D_CUDA_TRY(cudaMemsetAsync(gradients, 0, sizeof(float) * 3 * m, s));
+  A3D_TRY(fill_async<float>(gradients, 3 * m, 0.f, s));
   if (n == 0) return A3D_OK;
   DmcIn in = make_in(p);
-  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x, nullptr);
-  A3D_LAUNCH_CHECK();
-  corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, 2.0f / (float)p->resolution, w.x);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(init_pos_kernel, dim3(gsz(m)), dim3(256), 0, s, m, p->deform, w.x, nullptr);
+  A3D_PDL(corner_pos_kernel, dim3(gsz(8 * n)), dim3(256), 0, s, in, 2.0f / (float)p->resolution, w.x);
   const int64_t nk = 12 * n;
-  A3D_CUDA_TRY(cudaMemsetAsync(w.slots, 0xff, sizeof(uint32_t) * 6 * m, s));
-  A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, sizeof(uint32_t), s));
-  edge_slot_kernel<<<gsz(nk), 256, 0, s>>>(in, w.slots, w.misc);
-  A3D_LAUNCH_CHECK();
+  A3D_TRY(fill_async<uint32_t>(w.slots, 6 * m, 0xffffffffu, s));
+  A3D_TRY(fill_async<uint32_t>(w.misc, 1, 0u, s));
+  A3D_PDL(edge_slot_kernel, dim3(gsz(nk)), dim3(256), 0, s, in, w.slots, w.misc);
   uint32_t conflict = 0;
   A3D_CUDA_TRY(cudaMemcpyAsync(&conflict, w.misc, sizeof(conflict), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
   if (!conflict) {
-    corner_gradient_slots_kernel<<<gsz(m), 256, 0, s>>>(in, w.x, w.slots, gradients);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(corner_gradient_slots_kernel, dim3(gsz(m)), dim3(256), 0, s, in, w.x, w.slots, gradients);
     return A3D_OK;
   }
-  A3D_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, sizeof(uint32_t) * 2 * m, s));
-  edge_adj_count_kernel<<<gsz(nk), 256, 0, s>>>(in, w.cnt);
-  A3D_LAUNCH_CHECK();
+  A3D_TRY(fill_async<uint32_t>(w.cnt, 2 * m, 0u, s));
+  A3D_PDL(edge_adj_count_kernel, dim3(gsz(nk)), dim3(256), 0, s, in, w.cnt);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.cnt, w.start, 2 * m, w.scan_tmp, w.start + 2 * m, s)));
-  A3D_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, sizeof(uint32_t) * 2 * m, s));
-  edge_adj_fill_kernel<<<gsz(nk), 256, 0, s>>>(in, w.start, w.cnt, w.other);
-  A3D_LAUNCH_CHECK();
-  corner_gradient_kernel<<<gsz(m), 256, 0, s>>>(in, w.x, w.start, w.other, gradients);
-  A3D_LAUNCH_CHECK();
+  A3D_TRY(fill_async<uint32_t>(w.cnt, 2 * m, 0u, s));
+  A3D_PDL(edge_adj_fill_kernel, dim3(gsz(nk)), dim3(256), 0, s, in, w.start, w.cnt, w.other);
+  A3D_PDL(corner_gradient_kernel, dim3(gsz(m)), dim3(256), 0, s, in, w.x, w.start, w.other, gradients);
   return A3D_OK;
 }
 
@@ -2187,17 +2189,13 @@ extern "C" int a3d_dmc_emit_qef(const a3d_dmc_inputs* p, void* workspace, size_t
   EdgeData ed{w.e0, w.e1, w.idx_map};
   VdOut out{vertices, l_dev, p_alpha, n_alpha};
   // corner world positions (the training path computes them per edge)
-  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x, nullptr);
-  A3D_LAUNCH_CHECK();
-  corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, world_scale_host(p->resolution), w.x);
-  A3D_LAUNCH_CHECK();
-  vd_qef_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, w.x, corner_gradients, qef_reg_scale, nv, w.list, w.case_s,
+  A3D_PDL(init_pos_kernel, dim3(gsz(m)), dim3(256), 0, s, m, p->deform, w.x, nullptr);
+  A3D_PDL(corner_pos_kernel, dim3(gsz(8 * n)), dim3(256), 0, s, in, world_scale_host(p->resolution), w.x);
+  A3D_PDL(vd_qef_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, w.x, corner_gradients, qef_reg_scale, nv, w.list, w.case_s,
                                              w.vd_cube, w.vd_slot, w.goff, ed, out);
-  A3D_LAUNCH_CHECK();
   if (nq > 0) {
-    quad_eval_kernel<<<gsz(ne, kQuadThreads), kQuadThreads, 0, s>>>(ne, w.qflag, w.qoff, w.rfirst, w.vals, VdNumbering{w.case_s, w.cls_ra, w.cls_rb, ns}, w.e0, p->sdf,
+    A3D_PDL(quad_eval_kernel, dim3(gsz(ne, kQuadThreads)), dim3(kQuadThreads), 0, s, ne, w.qflag, w.qoff, w.rfirst, w.vals, VdNumbering{w.case_s, w.cls_ra, w.cls_rb, ns}, w.e0, p->sdf,
                                              p->isovalue, vertices, faces);
-    A3D_LAUNCH_CHECK();
   }
   return A3D_OK;
 }
@@ -2218,13 +2216,10 @@ extern "C" int a3d_dmc_backward_qef(const a3d_dmc_inputs* p, void* workspace, si
   if (ns == 0 || nv == 0) return A3D_OK;
   DmcIn in = make_in(p);
   // corner world positions, as the forward computed them
-  init_pos_kernel<<<gsz(m), 256, 0, s>>>(m, p->deform, w.x, nullptr);
-  A3D_LAUNCH_CHECK();
-  corner_pos_kernel<<<gsz(8 * n), 256, 0, s>>>(in, world_scale_host(p->resolution), w.x);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(init_pos_kernel, dim3(gsz(m)), dim3(256), 0, s, m, p->deform, w.x, nullptr);
+  A3D_PDL(corner_pos_kernel, dim3(gsz(8 * n)), dim3(256), 0, s, in, world_scale_host(p->resolution), w.x);
   QefGrad gq{g_vertices, g_l_dev, g_p_alpha, g_n_alpha, g_sdf, g_deform, g_alpha, g_corner_gradients};
-  vd_qef_bwd_kernel<<<gsz(nv, 128), 128, 0, s>>>(in, w.x, corner_gradients, qef_reg_scale, nv, w.list, w.case_s,
+  A3D_PDL(vd_qef_bwd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, w.x, corner_gradients, qef_reg_scale, nv, w.list, w.case_s,
                                                  w.vd_cube, w.vd_slot, w.goff, gq);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }

@@ -64,6 +64,7 @@ constexpr int kScanTile = kScanThreads * kScanItems;
 
 template <typename TIn, typename T>
 __global__ void scan_tile_reduce_kernel(const TIn* __restrict__ in, int64_t n, T* __restrict__ tile_sums) {
+  pdl_wait();
   __shared__ T s_warp[kBlockScanSlots];
   const int64_t base = (int64_t)blockIdx.x * kScanTile;
   T acc = 0;
@@ -80,6 +81,7 @@ __global__ void scan_tile_reduce_kernel(const TIn* __restrict__ in, int64_t n, T
 // Single block: exclusive scan of tile sums in place, total -> *total.
 template <typename T>
 __global__ void scan_tile_sums_kernel(T* __restrict__ sums, int64_t nb, T* __restrict__ total) {
+  pdl_wait();
   __shared__ T s_warp[kBlockScanSlots];
   const int64_t per = ceil_div(nb, (int64_t)blockDim.x);
   const int64_t lo = (int64_t)threadIdx.x * per;
@@ -106,6 +108,7 @@ __host__ __device__ constexpr int scan_pad(int i) { return i + (i >> 5); }
 template <typename TIn, typename T>
 __global__ void scan_tile_down_kernel(const TIn* __restrict__ in, T* __restrict__ out, int64_t n,
                                       const T* __restrict__ tile_offsets) {
+  pdl_wait();
   __shared__ T s_warp[kBlockScanSlots];
   __shared__ T s_tile[scan_pad(kScanTile)];
   const int64_t base = (int64_t)blockIdx.x * kScanTile;
@@ -153,12 +156,28 @@ int device_exclusive_scan(const TIn* in, T* out, int64_t n, T* tmp, T* total_dev
   const int64_t nb = ceil_div(n, kScanTile);
   // The down pass reads thread-contiguous items, the reduce pass strided
   // items: both cover the same tile so tile sums agree.
-  scan_tile_reduce_kernel<TIn, T><<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, tmp);
-  A3D_LAUNCH_CHECK();
-  scan_tile_sums_kernel<T><<<1, 1024, 0, s>>>(tmp, nb, total_dev ? total_dev : tmp + nb);
-  A3D_LAUNCH_CHECK();
-  scan_tile_down_kernel<TIn, T><<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, tmp);
-  A3D_LAUNCH_CHECK();
+  // the three passes back to back with programmatic dependent launch
+  A3D_PDL(scan_tile_reduce_kernel<TIn, T>, dim3((unsigned)nb), dim3(kScanThreads), 0, s, in, n, tmp);
+  A3D_PDL(scan_tile_sums_kernel<T>, dim3(1), dim3(1024), 0, s, tmp, nb, total_dev ? total_dev : tmp + nb);
+  A3D_PDL(scan_tile_down_kernel<TIn, T>, dim3((unsigned)nb), dim3(kScanThreads), 0, s, in, out, n, tmp);
+  return A3D_OK;
+}
+
+// n copies of v at p, a grid-stride kernel launched with programmatic
+// dependent launch (a memset between two kernels would break the chain)
+template <typename T>
+__global__ void fill_kernel(T* __restrict__ p, int64_t n, T v) {
+  pdl_wait();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+template <typename T>
+int fill_async(T* p, int64_t n, T v, cudaStream_t s) {
+  if (n <= 0) return A3D_OK;
+  const int64_t want = ceil_div(n, 256);
+  const int64_t cap = (int64_t)num_sms() * 8;
+  A3D_PDL(fill_kernel<T>, dim3((unsigned)(want < cap ? want : cap)), dim3(256), 0, s, p, n, v);
   return A3D_OK;
 }
 
