@@ -235,6 +235,7 @@ __global__ void clip_flags_kernel(const TriRec* __restrict__ tris, const float* 
                                   const uint32_t* __restrict__ cand_slot, int64_t m, uint32_t* __restrict__ flags,
                                   uint8_t* __restrict__ hit, int64_t n, int64_t num_slots,
                                   unsigned long long* __restrict__ faults) {
+  pdl_wait();
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < m)
     clip_candidate<false, 2>(tris, bmin, bmax, cand_box, cand_slot, k, flags, hit, nullptr, PairOut{}, n, num_slots,
@@ -247,6 +248,7 @@ __global__ void clip_emit_kernel(const TriRec* __restrict__ tris, const float* _
                                  const uint32_t* __restrict__ cand_slot, int64_t m, uint32_t* __restrict__ flags,
                                  const int64_t* __restrict__ coffs, PairOut out, int64_t n, int64_t num_slots,
                                  unsigned long long* __restrict__ faults) {
+  pdl_wait();
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < m)
     clip_candidate<true, kMode>(tris, bmin, bmax, cand_box, cand_slot, k, flags, nullptr, coffs, out, n, num_slots,
@@ -322,6 +324,7 @@ __global__ void __launch_bounds__(kSatThreads)
                        const float* __restrict__ bmin, const float* __restrict__ bmax, int64_t n,
                        uint32_t* __restrict__ counts, uint8_t* __restrict__ hit, uint32_t* __restrict__ spill,
                        unsigned long long* __restrict__ misc) {
+  pdl_wait();
   __shared__ uint32_t s_stack[kSatDepth * kSatThreads];
   const int64_t i = (int64_t)blockIdx.x * kSatThreads + threadIdx.x;
   if (i >= n) return;
@@ -339,6 +342,7 @@ __global__ void pairs_count_spill_kernel(const WideNode* __restrict__ nodes, con
                                          const float* __restrict__ bmin, const float* __restrict__ bmax,
                                          uint32_t* __restrict__ counts, uint8_t* __restrict__ hit,
                                          const uint32_t* __restrict__ spill, unsigned long long* __restrict__ misc) {
+  pdl_wait();
   const uint64_t m = misc[0];
   for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (uint64_t)gridDim.x * blockDim.x) {
     const int64_t i = spill[t];
@@ -360,6 +364,7 @@ __global__ void __launch_bounds__(kSatThreads)
                        const float* __restrict__ bmin, const float* __restrict__ bmax, int64_t n,
                        const int64_t* __restrict__ offs, int32_t* __restrict__ out_box,
                        int32_t* __restrict__ out_face, unsigned long long* __restrict__ misc) {
+  pdl_wait();
   __shared__ uint32_t s_stack[kSatDepth * kSatThreads];
   const int64_t i = (int64_t)blockIdx.x * kSatThreads + threadIdx.x;
   if (i >= n) return;
@@ -376,6 +381,7 @@ __global__ void pairs_write_spill_kernel(const WideNode* __restrict__ nodes, con
                                          const int64_t* __restrict__ offs, const uint32_t* __restrict__ spill,
                                          unsigned long long* __restrict__ misc, int32_t* __restrict__ out_box,
                                          int32_t* __restrict__ out_face) {
+  pdl_wait();
   const uint64_t m = misc[0];
   for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (uint64_t)gridDim.x * blockDim.x) {
     const int64_t i = spill[t];
@@ -391,13 +397,11 @@ int launch_write(const a3d_bvh_view* bvh, const float* bmin, const float* bmax, 
                  int32_t* out_box, int32_t* out_face, cudaStream_t s) {
   const WideNode* nodes = (const WideNode*)bvh->nodes;
   const TriRec* tris = (const TriRec*)bvh->tris;
-  pairs_write_kernel<kSlots><<<(unsigned)ceil_div(n, kSatThreads), kSatThreads, 0, s>>>(nodes, tris, bmin, bmax, n,
+  A3D_PDL(pairs_write_kernel<kSlots>, dim3((unsigned)ceil_div(n, kSatThreads)), dim3(kSatThreads), 0, s, nodes, tris, bmin, bmax, n,
                                                                                         w.offs, out_box, out_face,
                                                                                         w.misc);
-  A3D_LAUNCH_CHECK();
-  pairs_write_spill_kernel<kSlots><<<num_sms() * 4, 64, 0, s>>>(nodes, tris, bmin, bmax, w.offs, w.spill, w.misc,
+  A3D_PDL(pairs_write_spill_kernel<kSlots>, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, bmin, bmax, w.offs, w.spill, w.misc,
                                                               out_box, out_face);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
 
@@ -445,11 +449,9 @@ extern "C" int a3d_aabb_pairs_count(const a3d_bvh_view* bvh, const float* box_mi
   uint8_t* h = mode == 1 ? hit : nullptr;
   const WideNode* nodes = (const WideNode*)bvh->nodes;
   const TriRec* tris = (const TriRec*)bvh->tris;
-  pairs_count_kernel<<<(unsigned)ceil_div(n, kSatThreads), kSatThreads, 0, s>>>(nodes, tris, box_min, box_max, n,
+  A3D_PDL(pairs_count_kernel, dim3((unsigned)ceil_div(n, kSatThreads)), dim3(kSatThreads), 0, s, nodes, tris, box_min, box_max, n,
                                                                                  w.counts, h, w.spill, w.misc);
-  A3D_LAUNCH_CHECK();
-  pairs_count_spill_kernel<<<num_sms() * 4, 64, 0, s>>>(nodes, tris, box_min, box_max, w.counts, h, w.spill, w.misc);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(pairs_count_spill_kernel, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, box_min, box_max, w.counts, h, w.spill, w.misc);
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.counts, w.offs, n, w.scan_tmp, w.offs + n, s)));
   unsigned long long misc[4];
   int64_t total = 0;
@@ -483,10 +485,9 @@ extern "C" int a3d_aabb_pairs_clip(const a3d_bvh_view* bvh, const float* box_min
   A3D_CUDA_TRY(cudaMemsetAsync(hit, 0, n, s));
   if (num_candidates == 0) return A3D_OK;
   A3D_TRY(launch_write<true>(bvh, box_min, box_max, n, w, (int32_t*)c.cand_box, (int32_t*)c.cand_slot, s));
-  clip_flags_kernel<<<(unsigned)ceil_div(num_candidates, 256), 256, 0, s>>>(
+  A3D_PDL(clip_flags_kernel, dim3((unsigned)ceil_div(num_candidates, 256)), dim3(256), 0, s, 
       (const TriRec*)bvh->tris, box_min, box_max, c.cand_box, c.cand_slot, num_candidates, c.flags, hit, n,
       bvh->num_tris, w.misc + 2);
-  A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(c.flags, c.coffs, num_candidates, c.scan_tmp,
                                                      c.coffs + num_candidates, s)));
   int64_t total = 0;
@@ -527,12 +528,11 @@ extern "C" int a3d_aabb_pairs_write(const a3d_bvh_view* bvh, const float* box_mi
     const PairOut out{aabb_ids, face_ids, poly_counts, centroids, areas, poly_verts};
     const unsigned g = (unsigned)ceil_div(num_candidates, 256);
     if (mode == 2)
-      clip_emit_kernel<2><<<g, 256, 0, s>>>((const TriRec*)bvh->tris, box_min, box_max, c.cand_box, c.cand_slot,
-                                            num_candidates, c.flags, c.coffs, out, n, bvh->num_tris, w.misc + 2);
+      A3D_PDL(clip_emit_kernel<2>, dim3(g), dim3(256), 0, s, (const TriRec*)bvh->tris, box_min, box_max, c.cand_box,
+              c.cand_slot, num_candidates, c.flags, c.coffs, out, n, bvh->num_tris, w.misc + 2);
     else
-      clip_emit_kernel<3><<<g, 256, 0, s>>>((const TriRec*)bvh->tris, box_min, box_max, c.cand_box, c.cand_slot,
-                                            num_candidates, c.flags, c.coffs, out, n, bvh->num_tris, w.misc + 2);
-    A3D_LAUNCH_CHECK();
+      A3D_PDL(clip_emit_kernel<3>, dim3(g), dim3(256), 0, s, (const TriRec*)bvh->tris, box_min, box_max, c.cand_box,
+              c.cand_slot, num_candidates, c.flags, c.coffs, out, n, bvh->num_tris, w.misc + 2);
   }
   unsigned long long faults = 0;
   A3D_CUDA_TRY(cudaMemcpyAsync(&faults, w.misc + 2, sizeof(faults), cudaMemcpyDeviceToHost, s));

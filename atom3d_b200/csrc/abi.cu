@@ -29,6 +29,7 @@ int num_sms() {
 }
 
 __global__ void iota_u32_kernel(uint32_t* out, int64_t n) {
+  pdl_wait();
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (uint32_t)i;
 }

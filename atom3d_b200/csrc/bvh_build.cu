@@ -145,6 +145,7 @@ __device__ __forceinline__ int segment_of(const int64_t* __restrict__ off, int n
 }
 
 __global__ void single_offsets_kernel(int64_t* face_off, int64_t* vert_off, int64_t nf, int64_t nv) {
+  pdl_wait();
   if (threadIdx.x == 0) {
     face_off[0] = 0;
     face_off[1] = nf;
@@ -157,6 +158,7 @@ __global__ void single_offsets_kernel(int64_t* face_off, int64_t* vert_off, int6
 // (the mesh roots: internal node s, or the lone leaf N + s)
 __global__ void init_kernel(const int64_t* __restrict__ face_off, int nmesh, int64_t n, uint32_t* bounds,
                             int32_t* err, uint32_t* counters, int32_t* work0) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < 12 * (int64_t)nmesh) bounds[t] = (((t % 12) / 3) % 2 == 0) ? 0xffffffffu : 0u;
   if (t < 4) err[t] = 0;
@@ -186,6 +188,7 @@ __global__ void __launch_bounds__(kThreads)
                     const int64_t* __restrict__ face_off, int nmesh, int64_t nf, float4* __restrict__ tri_lo,
                     float4* __restrict__ tri_hi, float4* __restrict__ cen, uint32_t* __restrict__ mesh_of,
                     uint32_t* __restrict__ bounds, int32_t* __restrict__ err) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i0b = (int64_t)blockIdx.x * blockDim.x;
   __shared__ int s_m0;
@@ -252,6 +255,7 @@ __global__ void __launch_bounds__(kThreads)
 __global__ void morton_kernel(const float4* __restrict__ cen, const uint32_t* __restrict__ mesh_of, int64_t n,
                               const uint32_t* __restrict__ bounds, int bits, uint64_t* __restrict__ keys,
                               uint32_t* __restrict__ vals) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t m = mesh_of[i];
@@ -286,6 +290,7 @@ __global__ void radix_tree_kernel(const uint64_t* __restrict__ keys, const int64
                                   int64_t n, int32_t* __restrict__ left, int32_t* __restrict__ right,
                                   int32_t* __restrict__ parent, int32_t* __restrict__ first,
                                   int32_t* __restrict__ last) {
+  pdl_wait();
   const int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ii >= n) return;
   const int i = (int)ii;
@@ -367,6 +372,7 @@ __global__ void refit_kernel(const uint32_t* __restrict__ order, const float4* _
                              const int32_t* __restrict__ right, const int32_t* __restrict__ parent,
                              const int32_t* __restrict__ first, const int32_t* __restrict__ last, int leaf_max,
                              float4* box_lo, float4* box_hi, float4* cost, uint32_t* dec, uint32_t* visit) {
+  pdl_wait();
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const int64_t leaf = n + j;
@@ -459,6 +465,7 @@ __global__ void __launch_bounds__(kThreads)
                           const int32_t* __restrict__ last, const float4* __restrict__ box_lo,
                           const float4* __restrict__ box_hi, const uint32_t* __restrict__ dec,
                           WideNode* __restrict__ tmp, uint32_t* __restrict__ lvl) {
+  pdl_wait();
   const uint32_t cnt = counters[level];
   const int nn = (int)n;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += (int64_t)gridDim.x * blockDim.x) {
@@ -542,12 +549,14 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 __global__ void depth_check_kernel(const uint32_t* counters, int32_t* err) {
+  pdl_wait();
   if (threadIdx.x == 0 && counters[kMaxLevels] != 0u) err[1] = 1;
 }
 
 // 7a. final index of each wide node
 __global__ void layout_index_kernel(const uint32_t* __restrict__ sorted_lvl, const uint32_t* __restrict__ sorted_slot,
                                     int64_t n, uint32_t* __restrict__ newidx) {
+  pdl_wait();
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
   if ((sorted_lvl[r] & 0xffu) != kNoLevel) newidx[sorted_slot[r]] = (uint32_t)r;
@@ -557,6 +566,7 @@ __global__ void layout_index_kernel(const uint32_t* __restrict__ sorted_lvl, con
 __global__ void layout_copy_kernel(const uint32_t* __restrict__ sorted_lvl, const uint32_t* __restrict__ sorted_slot,
                                    int64_t n, const uint32_t* __restrict__ newidx, const WideNode* __restrict__ tmp,
                                    WideNode* __restrict__ out) {
+  pdl_wait();
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
   if ((sorted_lvl[r] & 0xffu) == kNoLevel) return;
@@ -574,6 +584,7 @@ __global__ void finish_kernel(const int64_t* __restrict__ face_off, int nmesh, c
                               const uint32_t* __restrict__ newidx, const uint32_t* __restrict__ bounds,
                               uint32_t* __restrict__ roots, float* __restrict__ bounds_out,
                               int64_t* __restrict__ num_nodes) {
+  pdl_wait();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0 && num_nodes) {
     int64_t total = 0;
@@ -593,6 +604,7 @@ __global__ void write_tris_kernel(const float* __restrict__ V, const int64_t* __
                                   const int32_t* __restrict__ F, const int64_t* __restrict__ face_off,
                                   const uint32_t* __restrict__ mesh_of, const uint32_t* __restrict__ order, int64_t n,
                                   TriRec* __restrict__ tris) {
+  pdl_wait();
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const uint32_t f = order[j];
@@ -680,41 +692,32 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
   const int mbits = mesh_bits_of(nmesh);
   const int bits = (64 - mbits) / 3 < 21 ? (64 - mbits) / 3 : 21;
   const int64_t init_threads = 12ll * nmesh > kMaxLevels + 1 ? 12ll * nmesh : kMaxLevels + 1;
-  init_kernel<<<(unsigned)ceil_div(init_threads, kThreads), kThreads, 0, s>>>(face_off, nmesh, n, w.bounds, w.err,
+  A3D_PDL(init_kernel, dim3((unsigned)ceil_div(init_threads, kThreads)), dim3(kThreads), 0, s, face_off, nmesh, n, w.bounds, w.err,
                                                                               w.counters, w.work_a);
-  A3D_LAUNCH_CHECK();
   const unsigned g = (unsigned)ceil_div(n, kThreads);
-  tri_prep_kernel<<<g, kThreads, 0, s>>>(V, vert_off, F, face_off, nmesh, n, w.tri_lo, w.tri_hi, w.centroid,
+  A3D_PDL(tri_prep_kernel, dim3(g), dim3(kThreads), 0, s, V, vert_off, F, face_off, nmesh, n, w.tri_lo, w.tri_hi, w.centroid,
                                          w.mesh_of, w.bounds, w.err);
-  A3D_LAUNCH_CHECK();
-  morton_kernel<<<g, kThreads, 0, s>>>(w.centroid, w.mesh_of, n, w.bounds, bits, w.keys, w.vals);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(morton_kernel, dim3(g), dim3(kThreads), 0, s, w.centroid, w.mesh_of, n, w.bounds, bits, w.keys, w.vals);
   bool alt = false;
   A3D_TRY(radix_sort_pairs<uint64_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, n, 0, 3 * bits + mbits, w.rs_scratch,
                                      &alt, s));
   const uint64_t* keys = alt ? w.keys_alt : w.keys;
   const uint32_t* order = alt ? w.vals_alt : w.vals;
 
-  radix_tree_kernel<<<g, kThreads, 0, s>>>(keys, face_off, nmesh, n, w.left, w.right, w.parent, w.first, w.last);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(radix_tree_kernel, dim3(g), dim3(kThreads), 0, s, keys, face_off, nmesh, n, w.left, w.right, w.parent, w.first, w.last);
   // SAH refinement of every subtree of <= kSahMax triangles below the top
   A3D_CUDA_TRY(cudaMemsetAsync(w.ncl, 0, sizeof(uint32_t), s));
-  sah_find_kernel<<<g, kThreads, 0, s>>>(face_off, nmesh, n, w.parent, w.first, w.last, w.clusters, w.ncl);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(sah_find_kernel, dim3(g), dim3(kThreads), 0, s, face_off, nmesh, n, w.parent, w.first, w.last, w.clusters, w.ncl);
   int sah_grid = 0;
   A3D_TRY(sah_grid_size(&sah_grid));
   const int64_t max_clusters = n / 3 + 1;
-  sah_cluster_kernel<<<(unsigned)(max_clusters < sah_grid ? max_clusters : sah_grid), kSahThreads, sizeof(SahSmem),
-                       s>>>(w.clusters, w.ncl, SahTree{w.left, w.right, w.parent, w.first, w.last, n},
+  A3D_PDL(sah_cluster_kernel, dim3((unsigned)(max_clusters < sah_grid ? max_clusters : sah_grid)), dim3(kSahThreads), sizeof(SahSmem), s, w.clusters, w.ncl, SahTree{w.left, w.right, w.parent, w.first, w.last, n},
                             const_cast<uint32_t*>(order), w.sah_tmp, w.sah_small,
                             SahPrims{w.centroid, w.tri_lo, w.tri_hi});
-  A3D_LAUNCH_CHECK();
   A3D_CUDA_TRY(cudaMemsetAsync(w.visit, 0, sizeof(uint32_t) * n, s));
-  refit_kernel<<<g, kThreads, 0, s>>>(order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.first, w.last,
+  A3D_PDL(refit_kernel, dim3(g), dim3(kThreads), 0, s, order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.first, w.last,
                                       leaf_max, w.box_lo, w.box_hi, w.dp_cost, w.dp_dec, w.visit);
-  A3D_LAUNCH_CHECK();
-  write_tris_kernel<<<g, kThreads, 0, s>>>(V, vert_off, F, face_off, w.mesh_of, order, n, tris_out);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(write_tris_kernel, dim3(g), dim3(kThreads), 0, s, V, vert_off, F, face_off, w.mesh_of, order, n, tris_out);
 
   // collapse: a fixed number of level launches (empty levels return at once)
   A3D_CUDA_TRY(cudaMemsetAsync(w.lvl, 0xff, sizeof(uint32_t) * n, s));
@@ -722,31 +725,25 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
   const int64_t lb = ceil_div(n, kThreads) < level_blocks ? ceil_div(n, kThreads) : level_blocks;
   int32_t *cur = w.work_a, *nxt = w.work_b;
   for (int level = 0; level < kMaxLevels; ++level) {
-    collapse_level_kernel<<<(unsigned)lb, kThreads, 0, s>>>(level, w.counters, cur, nxt, n, leaf_max, w.left,
+    A3D_PDL(collapse_level_kernel, dim3((unsigned)lb), dim3(kThreads), 0, s, level, w.counters, cur, nxt, n, leaf_max, w.left,
                                                             w.right, w.first, w.last, w.box_lo, w.box_hi,
                                                             w.dp_dec, w.tmp_nodes, w.lvl);
-    A3D_LAUNCH_CHECK();
     int32_t* t = cur;
     cur = nxt;
     nxt = t;
   }
-  depth_check_kernel<<<1, 32, 0, s>>>(w.counters, w.err);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(depth_check_kernel, dim3(1), dim3(32), 0, s, w.counters, w.err);
   // breadth-first layout: stable sort of the slots by level
-  iota_u32_kernel<<<g, kThreads, 0, s>>>(w.slot, n);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(iota_u32_kernel, dim3(g), dim3(kThreads), 0, s, w.slot, n);
   bool lalt = false;
   A3D_TRY(radix_sort_pairs<uint32_t>(w.lvl, w.slot, w.lvl_alt, w.slot_alt, n, 0, 8, w.rs_scratch, &lalt, s));
   const uint32_t* slvl = lalt ? w.lvl_alt : w.lvl;
   const uint32_t* sslot = lalt ? w.slot_alt : w.slot;
-  layout_index_kernel<<<g, kThreads, 0, s>>>(slvl, sslot, n, w.newidx);
-  A3D_LAUNCH_CHECK();
-  layout_copy_kernel<<<g, kThreads, 0, s>>>(slvl, sslot, n, w.newidx, w.tmp_nodes, nodes_out);
-  A3D_LAUNCH_CHECK();
-  finish_kernel<<<(unsigned)ceil_div(nmesh, kThreads), kThreads, 0, s>>>(face_off, nmesh, w.counters, w.newidx,
+  A3D_PDL(layout_index_kernel, dim3(g), dim3(kThreads), 0, s, slvl, sslot, n, w.newidx);
+  A3D_PDL(layout_copy_kernel, dim3(g), dim3(kThreads), 0, s, slvl, sslot, n, w.newidx, w.tmp_nodes, nodes_out);
+  A3D_PDL(finish_kernel, dim3((unsigned)ceil_div(nmesh, kThreads)), dim3(kThreads), 0, s, face_off, nmesh, w.counters, w.newidx,
                                                                          w.bounds, roots_out, bounds_out,
                                                                          num_nodes_out);
-  A3D_LAUNCH_CHECK();
   if (status_out) A3D_CUDA_TRY(cudaMemcpyAsync(status_out, w.err, 2 * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
   return A3D_OK;
 }
@@ -782,8 +779,7 @@ extern "C" int a3d_bvh_build(const float* vertices, int64_t num_vertices, const 
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "bvh_build: workspace too small");
   if (leaf_max == 0) leaf_max = kDefaultLeafMax;
   A3D_REQUIRE(leaf_max >= 1 && leaf_max <= kMaxLeafTris, A3D_ERR_ARGUMENT, "bvh_build: leaf_max must be in 1..8");
-  single_offsets_kernel<<<1, 32, 0, s>>>(w.face_off, w.vert_off, n, num_vertices);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(single_offsets_kernel, dim3(1), dim3(32), 0, s, w.face_off, w.vert_off, n, num_vertices);
   A3D_TRY(build_wide_bvh(vertices, w.vert_off, faces, w.face_off, 1, n, leaf_max, (WideNode*)nodes_out,
                          (TriRec*)tris_out, nullptr, nullptr, w.count, nullptr, w, s));
   uint32_t hb[12];

@@ -214,6 +214,7 @@ __global__ void __launch_bounds__(kSahThreads)
     sah_cluster_kernel(const int32_t* __restrict__ clusters, const uint32_t* __restrict__ ncl, SahTree T,
                        uint32_t* __restrict__ order, uint32_t* __restrict__ tmp_all, SahNode* __restrict__ small_all,
                        SahPrims P) {
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char sah_raw[];
   SahSmem& S = *reinterpret_cast<SahSmem*>(sah_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -431,6 +432,7 @@ __global__ void sah_find_kernel(const int64_t* __restrict__ face_off, int nmesh,
                                 const int32_t* __restrict__ parent, const int32_t* __restrict__ first,
                                 const int32_t* __restrict__ last, int32_t* __restrict__ clusters,
                                 uint32_t* __restrict__ ncl) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int lo = 0, hi = nmesh - 1;

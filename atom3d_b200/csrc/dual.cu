@@ -56,6 +56,7 @@ __device__ __forceinline__ int64_t vrank(const VGeom& g, const uint32_t* __restr
 }
 
 __global__ void bbox32_kernel(const int32_t* __restrict__ ijk, int64_t n, int* __restrict__ bb) {
+  pdl_wait();
   int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
@@ -105,6 +106,7 @@ __global__ void bbox32_kernel(const int32_t* __restrict__ ijk, int64_t n, int* _
 }
 
 __global__ void set_cells_kernel(const int32_t* __restrict__ ijk, int64_t n, VGeom g, uint32_t* __restrict__ vol) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int x = ijk[3 * i] - g.lx, y = ijk[3 * i + 1] - g.ly, z = ijk[3 * i + 2] - g.lz;
@@ -116,6 +118,7 @@ __global__ void set_cells_kernel(const int32_t* __restrict__ ijk, int64_t n, VGe
 // one-bit z shift; also the per-word popcounts of both volumes
 __global__ void corners_kernel(VGeom g, const uint32_t* __restrict__ cells, uint32_t* __restrict__ verts,
                                uint32_t* __restrict__ ccnt, uint32_t* __restrict__ vcnt, int64_t nwords) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nwords) return;
   const int w = (int)(i % g.nw);
@@ -149,6 +152,7 @@ template <bool kVerts>
 __global__ void extract_kernel(VGeom g, const uint32_t* __restrict__ v, const int64_t* __restrict__ offs,
                                int64_t nwords, int32_t* __restrict__ out_cells, int64_t* __restrict__ out_verts,
                                float* __restrict__ out_world, float3 origin, float3 cell) {
+  pdl_wait();
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int64_t w0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
@@ -209,6 +213,7 @@ __global__ void links_kernel(VGeom g, int64_t R, const int32_t* __restrict__ cel
                              const uint32_t* __restrict__ cells, const int64_t* __restrict__ coffs,
                              const uint32_t* __restrict__ verts, const int64_t* __restrict__ voffs,
                              int64_t* __restrict__ cube_idx, int64_t* __restrict__ adj_idx) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ncells) return;
   const int gx = cells_ijk[3 * i], gy = cells_ijk[3 * i + 1], gz = cells_ijk[3 * i + 2];
@@ -280,6 +285,7 @@ WetMasks make_wet_masks() {
 __global__ void dam_wet_kernel(VGeom g, const uint32_t* __restrict__ coll, const int32_t* __restrict__ dam, int64_t n,
                                WetMasks wm, uint8_t* __restrict__ faces, uint8_t* __restrict__ edges,
                                uint8_t* __restrict__ corners) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   // grid coordinates outside [0, R) are never in the collision volume, so
@@ -376,8 +382,7 @@ extern "C" int a3d_cells_bbox(const int32_t* const* lists, const int64_t* counts
     A3D_REQUIRE(counts[l] >= 0 && (counts[l] == 0 || lists[l]), A3D_ERR_ARGUMENT, "cells_bbox: bad list");
     if (counts[l] == 0) continue;
     const int64_t blocks = ceil_div(counts[l], 256) < 4096 ? ceil_div(counts[l], 256) : 4096;
-    bbox32_kernel<<<(unsigned)blocks, 256, 0, s>>>(lists[l], counts[l], bb);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(bbox32_kernel, dim3((unsigned)blocks), dim3(256), 0, s, lists[l], counts[l], bb);
   }
   int h[6];
   A3D_CUDA_TRY(cudaMemcpyAsync(h, bb, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -411,11 +416,9 @@ extern "C" int a3d_dual_graph_count(const int32_t* const* lists, const int64_t* 
   for (int l = 0; l < num_lists; ++l) {
     A3D_REQUIRE(counts[l] >= 0 && (counts[l] == 0 || lists[l]), A3D_ERR_ARGUMENT, "dual_graph_count: bad list");
     if (counts[l] == 0) continue;
-    set_cells_kernel<<<(unsigned)ceil_div(counts[l], 256), 256, 0, s>>>(lists[l], counts[l], g, w.cells);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(set_cells_kernel, dim3((unsigned)ceil_div(counts[l], 256)), dim3(256), 0, s, lists[l], counts[l], g, w.cells);
   }
-  corners_kernel<<<(unsigned)ceil_div(nwords, 256), 256, 0, s>>>(g, w.cells, w.verts, w.ccnt, w.vcnt, nwords);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(corners_kernel, dim3((unsigned)ceil_div(nwords, 256)), dim3(256), 0, s, g, w.cells, w.verts, w.ccnt, w.vcnt, nwords);
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.ccnt, w.coffs, nwords, w.scan_tmp, w.coffs + nwords, s)));
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.vcnt, w.voffs, nwords, w.scan_tmp, w.voffs + nwords, s)));
   A3D_CUDA_TRY(cudaMemcpyAsync(counts_out, w.coffs + nwords, 8, cudaMemcpyDeviceToHost, s));
@@ -444,13 +447,10 @@ extern "C" int a3d_dual_graph_emit(const a3d_dual_geom* geom, void* workspace, s
   const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
   const unsigned gw = (unsigned)ceil_div(nwords, 256);
   const float3 o = make_float3(origin[0], origin[1], origin[2]), c = make_float3(cell[0], cell[1], cell[2]);
-  extract_kernel<false><<<gw, 256, 0, s>>>(g, w.cells, w.coffs, nwords, cells_ijk, nullptr, nullptr, o, c);
-  A3D_LAUNCH_CHECK();
-  extract_kernel<true><<<gw, 256, 0, s>>>(g, w.verts, w.voffs, nwords, nullptr, vertices_ijk, vertices_world, o, c);
-  A3D_LAUNCH_CHECK();
-  links_kernel<<<(unsigned)ceil_div(num_cells, 256), 256, 0, s>>>(g, geom->resolution, cells_ijk, num_cells, w.cells,
+  A3D_PDL(extract_kernel<false>, dim3(gw), dim3(256), 0, s, g, w.cells, w.coffs, nwords, cells_ijk, nullptr, nullptr, o, c);
+  A3D_PDL(extract_kernel<true>, dim3(gw), dim3(256), 0, s, g, w.verts, w.voffs, nwords, nullptr, vertices_ijk, vertices_world, o, c);
+  A3D_PDL(links_kernel, dim3((unsigned)ceil_div(num_cells, 256)), dim3(256), 0, s, g, geom->resolution, cells_ijk, num_cells, w.cells,
                                                                    w.coffs, w.verts, w.voffs, cube_idx, adj_idx);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
 
@@ -486,10 +486,8 @@ extern "C" int a3d_dam_wet(const int32_t* dam_ijk, int64_t n, const int32_t* col
   A3D_REQUIRE(workspace && workspace_bytes >= (size_t)nwords * 4, A3D_ERR_WORKSPACE, "dam_wet: workspace too small");
   uint32_t* vol = (uint32_t*)workspace;
   A3D_CUDA_TRY(cudaMemsetAsync(vol, 0, nwords * 4, s));
-  set_cells_kernel<<<(unsigned)ceil_div(m, 256), 256, 0, s>>>(collision_ijk, m, g, vol);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(set_cells_kernel, dim3((unsigned)ceil_div(m, 256)), dim3(256), 0, s, collision_ijk, m, g, vol);
   static const WetMasks wm = make_wet_masks();
-  dam_wet_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(g, vol, dam_ijk, n, wm, wet_faces, wet_edges, wet_corners);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(dam_wet_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, s, g, vol, dam_ijk, n, wm, wet_faces, wet_edges, wet_corners);
   return A3D_OK;
 }

@@ -90,6 +90,7 @@ __device__ __forceinline__ uint32_t zdil(uint32_t a, uint32_t c, uint32_t b) {
 }
 
 __global__ void bbox_kernel(const int64_t* __restrict__ ijk, int64_t n, long long* __restrict__ bb) {
+  pdl_wait();
   long long lo[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, hi[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
@@ -140,6 +141,7 @@ __global__ void bbox_kernel(const int64_t* __restrict__ ijk, int64_t n, long lon
 }
 
 __global__ void set_bits_kernel(const int64_t* __restrict__ ijk, int64_t n, Geom g, uint32_t* __restrict__ vol) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int x = (int)(ijk[3 * i] - g.vx), y = (int)(ijk[3 * i + 1] - g.vy), z = (int)(ijk[3 * i + 2] - g.vz);
@@ -280,6 +282,7 @@ __global__ void __launch_bounds__(kBX * kBY)
     flood_rounds_kernel(Geom g, const uint32_t* __restrict__ occ, uint32_t* water, uint32_t* list_a, uint32_t* list_b,
                         uint32_t* __restrict__ mark, uint32_t* cnt, int nbx, int nby, int max_iters, int max_rounds,
                         uint32_t* sync) {
+  pdl_wait();
   __shared__ uint32_t s_r[3][kBX + 2][kBY + 2];  // words w-1, w, w+1 of the rows with halo
   int round = 0;
   for (;;) {
@@ -333,6 +336,7 @@ __device__ __forceinline__ uint32_t dil_conn(const uint32_t* __restrict__ v, con
 
 __global__ void labels_kernel(Geom g, const uint32_t* __restrict__ occ, const uint32_t* __restrict__ water,
                               uint32_t* __restrict__ lab, int64_t nwords) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nwords) return;
   const int w = (int)(i % g.nw);
@@ -367,6 +371,7 @@ __global__ void labels_kernel(Geom g, const uint32_t* __restrict__ occ, const ui
 // 3x3x3 box dilation of src into dst (one ring of get_dam_neighborhood_signs)
 __global__ void box_dilate_kernel(Geom g, const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
                                   int64_t nwords) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nwords) return;
   const int w = (int)(i % g.nw);
@@ -376,6 +381,7 @@ __global__ void box_dilate_kernel(Geom g, const uint32_t* __restrict__ src, uint
 }
 
 __global__ void ring_classify_kernel(const uint32_t* __restrict__ ring, uint32_t* __restrict__ lab, int64_t nwords) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nwords) return;
   const uint32_t n = ring[i];
@@ -395,6 +401,7 @@ constexpr int kTileChunks = kTileWords / kTileThreads;  // chunks of 32 words pe
 __global__ void __launch_bounds__(kTileThreads) tile_counts_kernel(const uint32_t* __restrict__ lab, int64_t nwords,
                                                                    int64_t ntiles, uint32_t* __restrict__ tcnt,
                                                                    unsigned long long* __restrict__ tot) {
+  pdl_wait();
   __shared__ uint32_t s_part[kRing][kTileThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * kTileWords;
@@ -430,6 +437,7 @@ __global__ void __launch_bounds__(kTileThreads) tile_counts_kernel(const uint32_
 __global__ void __launch_bounds__(kTileThreads) extract_tile_kernel(Geom g, const uint32_t* __restrict__ v,
                                                                     const int64_t* __restrict__ toff, int64_t nwords,
                                                                     int64_t count, int32_t* __restrict__ out) {
+  pdl_wait();
   __shared__ uint32_t s_warp[kTileThreads / 32];
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -483,6 +491,7 @@ __global__ void __launch_bounds__(kTileThreads) extract_tile_kernel(Geom g, cons
 
 __global__ void test_bits_kernel(Geom g, const uint32_t* __restrict__ v, const int64_t* __restrict__ ijk, int64_t n,
                                  uint8_t* __restrict__ out) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int x = (int)(ijk[3 * i] - g.vx), y = (int)(ijk[3 * i + 1] - g.vy), z = (int)(ijk[3 * i + 2] - g.vz);
@@ -497,6 +506,7 @@ __global__ void test_bits_kernel(Geom g, const uint32_t* __restrict__ v, const i
 __global__ void seed_kernel(Geom g, const uint32_t* __restrict__ occ, uint32_t* __restrict__ water, int sx, int sy,
                             int sz, uint32_t seed_brick, uint32_t* __restrict__ list, uint32_t* __restrict__ cnt,
                             uint32_t* __restrict__ status) {
+  pdl_wait();
   const int64_t i = widx(g, sx, sy, sz >> 5);
   const uint32_t bit = 1u << (sz & 31);
   if (occ[i] & bit) {
@@ -514,6 +524,7 @@ __global__ void seed_kernel(Geom g, const uint32_t* __restrict__ occ, uint32_t* 
 __global__ void ring_sign_kernel(Geom g, const uint32_t* __restrict__ dam, const uint32_t* __restrict__ water,
                                  const uint32_t* __restrict__ dry, const int32_t* __restrict__ ijk, int64_t n,
                                  int8_t* __restrict__ sign) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int x = ijk[3 * i] - g.vx, y = ijk[3 * i + 1] - g.vy, z = ijk[3 * i + 2] - g.vz;
@@ -591,8 +602,7 @@ extern "C" int a3d_flood_bbox(const int64_t* ijk, int64_t n, int64_t* bbox_out, 
   long long* bb = (long long*)workspace;
   A3D_CUDA_TRY(cudaMemcpyAsync(bb, init, sizeof(init), cudaMemcpyHostToDevice, s));
   const int64_t blocks = ceil_div(n, 256) < 4096 ? ceil_div(n, 256) : 4096;
-  bbox_kernel<<<(unsigned)blocks, 256, 0, s>>>(ijk, n, bb);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(bbox_kernel, dim3((unsigned)blocks), dim3(256), 0, s, ijk, n, bb);
   long long h[6];
   A3D_CUDA_TRY(cudaMemcpyAsync(h, bb, sizeof(h), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
@@ -631,8 +641,7 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
   A3D_CUDA_TRY(cudaMemsetAsync(w.water, 0, nwords * 4, s));
   A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, 32 * sizeof(uint32_t), s));
   if (n > 0) {
-    set_bits_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(dam_ijk, n, g, w.occ);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(set_bits_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, s, dam_ijk, n, g, w.occ);
   }
   const int sx = (int)(geom->seed[0] - geom->vol_lo[0]), sy = (int)(geom->seed[1] - geom->vol_lo[1]),
             sz = (int)(geom->seed[2] - geom->vol_lo[2]);
@@ -643,8 +652,7 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
   const int64_t sb = ((int64_t)(sz >> 5) * nbx + sx / kBX) * nby + sy / kBY;
   uint32_t* qcnt = w.misc + 2;
   A3D_CUDA_TRY(cudaMemsetAsync(w.mark, 0, nbricks * sizeof(uint32_t), s));
-  seed_kernel<<<1, 1, 0, s>>>(g, w.occ, w.water, sx, sy, sz, (uint32_t)sb, w.list_a, qcnt, w.misc);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(seed_kernel, dim3(1), dim3(1), 0, s, g, w.occ, w.water, sx, sy, sz, (uint32_t)sb, w.list_a, qcnt, w.misc);
   uint32_t seed_status = 0;
   A3D_CUDA_TRY(cudaMemcpyAsync(&seed_status, w.misc, 4, cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
@@ -683,24 +691,20 @@ extern "C" int a3d_flood_fill(const int64_t* dam_ijk, int64_t n, const a3d_flood
   const int rounds = (int)hs[1];
   if (rounds_out) *rounds_out = rounds;
   const unsigned gw = (unsigned)ceil_div(nwords, 256);
-  labels_kernel<<<gw, 256, 0, s>>>(g, w.occ, w.water, w.lab, nwords);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(labels_kernel, dim3(gw), dim3(256), 0, s, g, w.occ, w.water, w.lab, nwords);
   // k-ring box dilation of the dam, ping-ponging ring buffers
   uint32_t* ring_a = w.lab + (int64_t)kRing * nwords;
   A3D_CUDA_TRY(cudaMemcpyAsync(ring_a, w.lab + (int64_t)kDam * nwords, nwords * 4, cudaMemcpyDeviceToDevice, s));
   uint32_t* ring_b = w.ring2;
   for (int k = 0; k < geom->k_ring; ++k) {
-    box_dilate_kernel<<<gw, 256, 0, s>>>(g, ring_a, ring_b, nwords);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(box_dilate_kernel, dim3(gw), dim3(256), 0, s, g, ring_a, ring_b, nwords);
     uint32_t* t = ring_a; ring_a = ring_b; ring_b = t;
   }
-  ring_classify_kernel<<<gw, 256, 0, s>>>(ring_a, w.lab, nwords);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(ring_classify_kernel, dim3(gw), dim3(256), 0, s, ring_a, w.lab, nwords);
   // counts per label and tile, one pass and one host read
   const int64_t ntiles = tiles_of(g);
   unsigned long long* tot = reinterpret_cast<unsigned long long*>(w.misc + 8);
-  tile_counts_kernel<<<(unsigned)ntiles, kTileThreads, 0, s>>>(w.lab, nwords, ntiles, w.tcnt, tot);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(tile_counts_kernel, dim3((unsigned)ntiles), dim3(kTileThreads), 0, s, w.lab, nwords, ntiles, w.tcnt, tot);
   unsigned long long h[kRing];
   A3D_CUDA_TRY(cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
@@ -724,8 +728,7 @@ extern "C" int a3d_flood_extract(const a3d_flood_geom* geom, void* workspace, si
   const uint32_t* v = w.lab + (int64_t)label * nwords;
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.tcnt + (int64_t)label * ntiles, w.toff, ntiles, w.scan_tmp,
                                                      w.toff + ntiles, s)));
-  extract_tile_kernel<<<(unsigned)ntiles, kTileThreads, 0, s>>>(g, v, w.toff, nwords, count, out_ijk);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(extract_tile_kernel, dim3((unsigned)ntiles), dim3(kTileThreads), 0, s, g, v, w.toff, nwords, count, out_ijk);
   return A3D_OK;
 }
 
@@ -740,8 +743,7 @@ extern "C" int a3d_flood_test(const a3d_flood_geom* geom, void* workspace, size_
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "flood_test: workspace too small");
   if (n == 0) return A3D_OK;
   const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
-  test_bits_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(g, w.lab + (int64_t)label * nwords, ijk, n, out);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(test_bits_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, s, g, w.lab + (int64_t)label * nwords, ijk, n, out);
   return A3D_OK;
 }
 
@@ -768,16 +770,13 @@ extern "C" int a3d_ring_signs(const int64_t* dam_ijk, int64_t n_dam, const int64
   A3D_CUDA_TRY(cudaMemsetAsync(w.lab, 0, (size_t)kLabels * nwords * 4, s));
   A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, 32 * sizeof(uint32_t), s));
   uint32_t* v_dam = w.lab + (int64_t)kDam * nwords;
-  set_bits_kernel<<<(unsigned)ceil_div(n_dam, 256), 256, 0, s>>>(dam_ijk, n_dam, g, v_dam);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(set_bits_kernel, dim3((unsigned)ceil_div(n_dam, 256)), dim3(256), 0, s, dam_ijk, n_dam, g, v_dam);
   if (n_water > 0) {
-    set_bits_kernel<<<(unsigned)ceil_div(n_water, 256), 256, 0, s>>>(water_ijk, n_water, g,
+    A3D_PDL(set_bits_kernel, dim3((unsigned)ceil_div(n_water, 256)), dim3(256), 0, s, water_ijk, n_water, g,
                                                                      w.lab + (int64_t)kWater * nwords);
-    A3D_LAUNCH_CHECK();
   }
   if (n_dry > 0) {
-    set_bits_kernel<<<(unsigned)ceil_div(n_dry, 256), 256, 0, s>>>(dry_ijk, n_dry, g, w.lab + (int64_t)kDry * nwords);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(set_bits_kernel, dim3((unsigned)ceil_div(n_dry, 256)), dim3(256), 0, s, dry_ijk, n_dry, g, w.lab + (int64_t)kDry * nwords);
   }
   const unsigned gw = (unsigned)ceil_div(nwords, 256);
   uint32_t* ring_out = w.lab + (int64_t)kExtTide * nwords;
@@ -785,16 +784,14 @@ extern "C" int a3d_ring_signs(const int64_t* dam_ijk, int64_t n_dam, const int64
   uint32_t* bufs[2] = {w.lab + (int64_t)kRing * nwords, w.ring2};
   for (int k = 0; k < geom->k_ring; ++k) {
     uint32_t* dst = (k == geom->k_ring - 1) ? ring_out : bufs[k & 1];
-    box_dilate_kernel<<<gw, 256, 0, s>>>(g, src, dst, nwords);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(box_dilate_kernel, dim3(gw), dim3(256), 0, s, g, src, dst, nwords);
     src = dst;
   }
   if (geom->k_ring == 0)
     A3D_CUDA_TRY(cudaMemcpyAsync(ring_out, v_dam, nwords * 4, cudaMemcpyDeviceToDevice, s));
   const int64_t ntiles = tiles_of(g);
   unsigned long long* tot = reinterpret_cast<unsigned long long*>(w.misc + 8);
-  tile_counts_kernel<<<(unsigned)ntiles, kTileThreads, 0, s>>>(w.lab, nwords, ntiles, w.tcnt, tot);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(tile_counts_kernel, dim3((unsigned)ntiles), dim3(kTileThreads), 0, s, w.lab, nwords, ntiles, w.tcnt, tot);
   unsigned long long h = 0;
   A3D_CUDA_TRY(cudaMemcpyAsync(&h, tot + kExtTide, sizeof(h), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
@@ -814,9 +811,8 @@ extern "C" int a3d_ring_signs_emit(const a3d_flood_geom* geom, void* workspace, 
   FloodWs w;
   carve_flood(w, ws, g);
   const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
-  ring_sign_kernel<<<(unsigned)ceil_div(count, 256), 256, 0, s>>>(
+  A3D_PDL(ring_sign_kernel, dim3((unsigned)ceil_div(count, 256)), dim3(256), 0, s, 
       g, w.lab + (int64_t)kDam * nwords, w.lab + (int64_t)kWater * nwords, w.lab + (int64_t)kDry * nwords, out_ijk,
       count, out_signs);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }

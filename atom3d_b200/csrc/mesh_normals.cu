@@ -21,6 +21,7 @@ __global__ void face_kernel(const float* __restrict__ V, const int32_t* __restri
                             float* __restrict__ fn_sign, float* __restrict__ fn_unit, float* __restrict__ ang,
                             float* __restrict__ vacc, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
                             uint32_t* __restrict__ bad_face) {
+  pdl_wait();
   const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nf) return;
   int64_t id[3] = {F[3 * f], F[3 * f + 1], F[3 * f + 2]};
@@ -78,6 +79,7 @@ __global__ void face_kernel(const float* __restrict__ V, const int32_t* __restri
 }
 
 __global__ void normalize_rows_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t n) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float x = in[3 * i], y = in[3 * i + 1], z = in[3 * i + 2];
@@ -86,6 +88,7 @@ __global__ void normalize_rows_kernel(const float* __restrict__ in, float* __res
 }
 
 __global__ void run_start_kernel(const uint64_t* __restrict__ k, int64_t n, uint32_t* __restrict__ flag) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   flag[i] = (i == 0 || k[i] != k[i - 1]) ? 1u : 0u;
@@ -98,6 +101,7 @@ __global__ void edge_kernel(const uint64_t* __restrict__ k, const uint32_t* __re
                             const uint32_t* __restrict__ start_flag, const uint32_t* __restrict__ edge_id,
                             const float* __restrict__ fn_unit, float* __restrict__ edge_pn,
                             int64_t* __restrict__ he_edge_idx) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !start_flag[i]) return;
   const uint32_t e = edge_id[i];
@@ -172,12 +176,10 @@ extern "C" int a3d_mesh_normals(const float* vertices, int64_t num_vertices, con
   const int64_t nh = 3 * num_faces;
   A3D_CUDA_TRY(cudaMemsetAsync(w.vacc, 0, sizeof(float) * 3 * num_vertices, s));
   A3D_CUDA_TRY(cudaMemsetAsync(w.total, 0, sizeof(uint32_t) * 2, s));
-  face_kernel<<<(unsigned)ceil_div(num_faces, 256), 256, 0, s>>>(vertices, faces, num_faces, num_vertices,
+  A3D_PDL(face_kernel, dim3((unsigned)ceil_div(num_faces, 256)), dim3(256), 0, s, vertices, faces, num_faces, num_vertices,
                                                                  face_normals_sign, w.fn_unit, face_angles, w.vacc,
                                                                  w.keys, w.vals, w.total + 1);
-  A3D_LAUNCH_CHECK();
-  normalize_rows_kernel<<<(unsigned)ceil_div(num_vertices, 256), 256, 0, s>>>(w.vacc, vertex_pn, num_vertices);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(normalize_rows_kernel, dim3((unsigned)ceil_div(num_vertices, 256)), dim3(256), 0, s, w.vacc, vertex_pn, num_vertices);
   // key bits: lo*V+hi < V^2
   int bits = 1;
   while (bits < 64 && ((unsigned __int128)1 << bits) < (unsigned __int128)num_vertices * num_vertices) ++bits;
@@ -186,8 +188,7 @@ extern "C" int a3d_mesh_normals(const float* vertices, int64_t num_vertices, con
   A3D_TRY(radix_sort_pairs<uint64_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, nh, 0, end_bit, w.rs, &alt, s));
   const uint64_t* k = alt ? w.keys_alt : w.keys;
   const uint32_t* he = alt ? w.vals_alt : w.vals;
-  run_start_kernel<<<(unsigned)ceil_div(nh, 256), 256, 0, s>>>(k, nh, w.flag);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(run_start_kernel, dim3((unsigned)ceil_div(nh, 256)), dim3(256), 0, s, k, nh, w.flag);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flag, w.eid, nh, w.scan_tmp, w.total, s)));
   uint32_t h[2] = {0, 0};
   A3D_CUDA_TRY(cudaMemcpyAsync(h, w.total, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -196,8 +197,7 @@ extern "C" int a3d_mesh_normals(const float* vertices, int64_t num_vertices, con
   const uint32_t ne = h[0];
   if (num_edges_out) *num_edges_out = ne;
   A3D_REQUIRE((int64_t)ne <= edge_capacity, A3D_ERR_WORKSPACE, "mesh_normals: edge capacity too small");
-  edge_kernel<<<(unsigned)ceil_div(nh, 256), 256, 0, s>>>(k, he, nh, w.flag, w.eid, w.fn_unit, edge_pn,
+  A3D_PDL(edge_kernel, dim3((unsigned)ceil_div(nh, 256)), dim3(256), 0, s, k, he, nh, w.flag, w.eid, w.fn_unit, edge_pn,
                                                           he_edge_idx);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }

@@ -15,6 +15,7 @@ __global__ void __launch_bounds__(kSatThreads)
     aabb_hit_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
                     const float* __restrict__ bmin, const float* __restrict__ bmax, int64_t n,
                     uint8_t* __restrict__ hit, uint32_t* __restrict__ spill, uint32_t* __restrict__ nspill) {
+  pdl_wait();
   __shared__ uint32_t s_stack[kSatDepth * kSatThreads];
   const int64_t i = (int64_t)blockIdx.x * kSatThreads + threadIdx.x;
   if (i >= n) return;
@@ -32,6 +33,7 @@ __global__ void aabb_hit_spill_kernel(const WideNode* __restrict__ nodes, const 
                                       const float* __restrict__ bmin, const float* __restrict__ bmax,
                                       uint8_t* __restrict__ hit, const uint32_t* __restrict__ spill,
                                       const uint32_t* __restrict__ nspill, int* __restrict__ overflow) {
+  pdl_wait();
   const uint32_t m = *nspill;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = spill[t];
@@ -111,6 +113,7 @@ __global__ void __launch_bounds__(kSatThreads)
                         bool first_level, int res, const int32_t* __restrict__ parents,
                         const uint32_t* __restrict__ parent_hint, LevelGeom g, uint32_t* __restrict__ flags,
                         uint32_t* __restrict__ ctri, uint32_t* __restrict__ spill, uint32_t* __restrict__ nspill) {
+  pdl_wait();
   __shared__ uint32_t s_stack[kSatDepth * kSatThreads];
   const int64_t k = (int64_t)blockIdx.x * kSatThreads + threadIdx.x;
   if (k >= ncand) return;
@@ -137,6 +140,7 @@ __global__ void octree_spill_kernel(const WideNode* __restrict__ nodes, const Tr
                                     uint32_t* __restrict__ flags, uint32_t* __restrict__ ctri,
                                     const uint32_t* __restrict__ spill, const uint32_t* __restrict__ nspill,
                                     int* __restrict__ overflow) {
+  pdl_wait();
   const uint32_t m = *nspill;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t k = spill[t];
@@ -162,6 +166,7 @@ __global__ void octree_compact_kernel(int64_t ncand, bool first_level, int res, 
                                       const uint8_t* __restrict__ hit, const uint32_t* __restrict__ offs,
                                       const uint32_t* __restrict__ ctri, int32_t* __restrict__ out32,
                                       uint32_t* __restrict__ hint_out, int64_t* __restrict__ out64) {
+  pdl_wait();
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ncand || !hit[k]) return;
   int x, y, z;
@@ -176,12 +181,14 @@ __global__ void octree_compact_kernel(int64_t ncand, bool first_level, int res, 
 }
 
 __global__ void flags_to_u8_kernel(const uint32_t* __restrict__ f, int64_t n, uint8_t* __restrict__ h) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) h[i] = (uint8_t)f[i];
 }
 
 // ---- Morton ------------------------------------------------------------------
 __global__ void morton_encode_kernel(const int64_t* __restrict__ ijk, int64_t n, int64_t* __restrict__ out) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   // bits 0..20 of each coordinate (two's complement bits, like the
@@ -191,6 +198,7 @@ __global__ void morton_encode_kernel(const int64_t* __restrict__ ijk, int64_t n,
 }
 
 __global__ void morton_decode_kernel(const int64_t* __restrict__ m, int64_t n, int level, int64_t* __restrict__ ijk) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint64_t v = (uint64_t)m[i];
@@ -209,16 +217,14 @@ using namespace a3d;
 extern "C" int a3d_morton_encode(const int64_t* ijk, int64_t n, int64_t* morton, a3d_stream_t stream) {
   A3D_REQUIRE(n >= 0, A3D_ERR_ARGUMENT, "morton_encode: bad size");
   if (n == 0) return A3D_OK;
-  morton_encode_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, (cudaStream_t)stream>>>(ijk, n, morton);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(morton_encode_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, (cudaStream_t)stream, ijk, n, morton);
   return A3D_OK;
 }
 
 extern "C" int a3d_morton_decode(const int64_t* morton, int64_t n, int level, int64_t* ijk, a3d_stream_t stream) {
   A3D_REQUIRE(n >= 0 && level >= 0, A3D_ERR_ARGUMENT, "morton_decode: bad argument");
   if (n == 0) return A3D_OK;
-  morton_decode_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, (cudaStream_t)stream>>>(morton, n, level, ijk);
-  A3D_LAUNCH_CHECK();
+  A3D_PDL(morton_decode_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, (cudaStream_t)stream, morton, n, level, ijk);
   return A3D_OK;
 }
 
@@ -240,12 +246,10 @@ extern "C" int a3d_aabb_hit(const a3d_bvh_view* bvh, const float* box_min, const
   uint32_t* nspill = ws.take<uint32_t>(4);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "aabb_hit: workspace too small");
   A3D_CUDA_TRY(cudaMemsetAsync(nspill, 0, 4 * sizeof(uint32_t), s));
-  aabb_hit_kernel<<<(unsigned)ceil_div(n, kSatThreads), kSatThreads, 0, s>>>(
+  A3D_PDL(aabb_hit_kernel, dim3((unsigned)ceil_div(n, kSatThreads)), dim3(kSatThreads), 0, s, 
       (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, box_min, box_max, n, hit, spill, nspill);
-  A3D_LAUNCH_CHECK();
-  aabb_hit_spill_kernel<<<num_sms() * 4, 64, 0, s>>>((const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, box_min,
+  A3D_PDL(aabb_hit_spill_kernel, dim3(num_sms() * 4), dim3(64), 0, s, (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, box_min,
                                                    box_max, hit, spill, nspill, (int*)(nspill + 1));
-  A3D_LAUNCH_CHECK();
   int ov = 0;
   A3D_CUDA_TRY(cudaMemcpyAsync(&ov, nspill + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
@@ -328,14 +332,11 @@ extern "C" int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo
     }
     A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, 8 * sizeof(uint32_t), s));
     const unsigned gk = (unsigned)ceil_div(ncand, kSatThreads);
-    octree_level_kernel<<<gk, kSatThreads, 0, s>>>(nodes, tris, ncand, first_level, res, parents, parent_hint, g,
+    A3D_PDL(octree_level_kernel, dim3(gk), dim3(kSatThreads), 0, s, nodes, tris, ncand, first_level, res, parents, parent_hint, g,
                                                    w.flags, w.ctri, w.spill, w.misc + 1);
-    A3D_LAUNCH_CHECK();
-    octree_spill_kernel<<<num_sms() * 4, 64, 0, s>>>(nodes, tris, first_level, res, parents, parent_hint, g, w.flags,
+    A3D_PDL(octree_spill_kernel, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, first_level, res, parents, parent_hint, g, w.flags,
                                                    w.ctri, w.spill, w.misc + 1, (int*)(w.misc + 2));
-    A3D_LAUNCH_CHECK();
-    flags_to_u8_kernel<<<(unsigned)ceil_div(ncand, 256), 256, 0, s>>>(w.flags, ncand, w.hit);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(flags_to_u8_kernel, dim3((unsigned)ceil_div(ncand, 256)), dim3(256), 0, s, w.flags, ncand, w.hit);
     A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flags, w.flags, ncand, w.scan_tmp, w.misc, s)));
     uint32_t hm[3];
     A3D_CUDA_TRY(cudaMemcpyAsync(hm, w.misc, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
@@ -352,11 +353,10 @@ extern "C" int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo
       *count_out = -1;
       A3D_REQUIRE(false, A3D_ERR_WORKSPACE, "octree: level capacity exceeded");
     }
-    octree_compact_kernel<<<(unsigned)ceil_div(ncand, 256), 256, 0, s>>>(ncand, first_level, res, parents, w.hit,
+    A3D_PDL(octree_compact_kernel, dim3((unsigned)ceil_div(ncand, 256)), dim3(256), 0, s, ncand, first_level, res, parents, w.hit,
                                                                          w.flags, w.ctri, last ? nullptr : next,
                                                                          last ? nullptr : next_hint,
                                                                          last ? out_ijk : nullptr);
-    A3D_LAUNCH_CHECK();
     if (last || total == 0) {
       if (!last) *count_out = 0;
       break;

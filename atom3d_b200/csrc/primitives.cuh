@@ -191,6 +191,7 @@ constexpr int kRsTile = kRsThreads * kRsItems;
 template <typename K>
 __global__ void __launch_bounds__(kRsThreads) rs_upsweep_kernel(const K* __restrict__ keys, int64_t n, int shift,
                                                                 uint32_t* __restrict__ hist, int64_t num_tiles) {
+  pdl_wait();
   __shared__ uint32_t s_hist[256];
   s_hist[threadIdx.x] = 0;
   __syncthreads();
@@ -212,6 +213,7 @@ __global__ void __launch_bounds__(kRsThreads)
     rs_downsweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, K* __restrict__ keys_out,
                         uint32_t* __restrict__ vals_out, int64_t n, int shift, const uint32_t* __restrict__ offsets,
                         int64_t num_tiles) {
+  pdl_wait();
   __shared__ uint32_t s_base[256];
   __shared__ uint32_t s_warp[kRsThreads / 32][256];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -274,11 +276,10 @@ int radix_sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, i
   K *kin = keys, *kout = keys_alt;
   uint32_t *vin = vals, *vout = vals_alt;
   for (int shift = begin_bit; shift < end_bit; shift += 8) {
-    rs_upsweep_kernel<K><<<(unsigned)nt, kRsThreads, 0, s>>>(kin, n, shift, hist, nt);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(rs_upsweep_kernel<K>, dim3((unsigned)nt), dim3(kRsThreads), 0, s, (const K*)kin, n, shift, hist, nt);
     A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(hist, hist, 256 * nt, tmp, (uint32_t*)nullptr, s)));
-    rs_downsweep_kernel<K><<<(unsigned)nt, kRsThreads, 0, s>>>(kin, vin, kout, vout, n, shift, hist, nt);
-    A3D_LAUNCH_CHECK();
+    A3D_PDL(rs_downsweep_kernel<K>, dim3((unsigned)nt), dim3(kRsThreads), 0, s, (const K*)kin, (const uint32_t*)vin,
+            kout, vout, n, shift, (const uint32_t*)hist, nt);
     K* tk = kin; kin = kout; kout = tk;
     uint32_t* tv = vin; vin = vout; vout = tv;
     *result_in_alt = !*result_in_alt;

@@ -279,6 +279,7 @@ __global__ void __launch_bounds__(kRayThreads)
                        const float* __restrict__ face_normals, const float* __restrict__ ro,
                        const float* __restrict__ rd, int64_t n, float max_t, RayOut out, uint32_t* __restrict__ rerun,
                        uint32_t* __restrict__ nrerun) {
+  pdl_wait();
   __shared__ uint2 s_stack[kRayShared * kRayThreads];
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -299,6 +300,7 @@ __global__ void __launch_bounds__(64)
                              const float* __restrict__ rd, float max_t, RayOut out,
                              const uint32_t* __restrict__ rerun, const uint32_t* __restrict__ nrerun,
                              uint32_t* __restrict__ overflow) {
+  pdl_wait();
   const uint32_t m = *nrerun;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = rerun[k];
@@ -354,6 +356,7 @@ __device__ bool all_hits(const WideNode* __restrict__ nodes, const TriRec* __res
 __global__ void ray_all_count_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
                                      const float* __restrict__ ro, const float* __restrict__ rd, int64_t n,
                                      float max_t, int32_t* __restrict__ counts, uint32_t* __restrict__ overflow) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Ray r = make_ray(ld3(ro, i), ld3(rd, i));
@@ -374,6 +377,7 @@ struct AllOut {
 __global__ void ray_all_collect_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
                                        const float* __restrict__ ro, const float* __restrict__ rd, int64_t n,
                                        float max_t, const int64_t* __restrict__ offsets, AllOut out) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Ray r = make_ray(ld3(ro, i), ld3(rd, i));
@@ -409,6 +413,7 @@ __global__ void __launch_bounds__(64)
     ray_parity_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
                       const float* __restrict__ pts, int64_t n, const float* __restrict__ dirs, int ndir, float max_t,
                       float coalesce, int32_t* __restrict__ votes, uint32_t* __restrict__ overflow) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const V3 o = ld3(pts, i);
@@ -506,12 +511,10 @@ extern "C" int a3d_ray_nearest(const a3d_bvh_view* bvh, const float* rays_o, con
   const WideNode* nodes = (const WideNode*)bvh->nodes;
   const TriRec* tris = (const TriRec*)bvh->tris;
   const RayOut out{hit, t, face_ids, hit_points, normals, uvw};
-  ray_nearest_kernel<<<(unsigned)ceil_div(num_rays, kRayThreads), kRayThreads, 0, s>>>(
+  A3D_PDL(ray_nearest_kernel, dim3((unsigned)ceil_div(num_rays, kRayThreads)), dim3(kRayThreads), 0, s, 
       nodes, tris, face_normals, rays_o, rays_d, num_rays, max_t, out, w.rerun, w.status);
-  A3D_LAUNCH_CHECK();
-  ray_nearest_rerun_kernel<<<num_sms() * 4, 64, 0, s>>>(nodes, tris, face_normals, rays_o, rays_d, max_t, out, w.rerun,
+  A3D_PDL(ray_nearest_rerun_kernel, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, face_normals, rays_o, rays_d, max_t, out, w.rerun,
                                                       w.status, w.status + 1);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
 
@@ -526,9 +529,8 @@ extern "C" int a3d_ray_all_count(const a3d_bvh_view* bvh, const float* rays_o, c
   A3D_CUDA_TRY(cudaMemsetAsync(w.status, 0, 4 * sizeof(uint32_t), s));
   if (num_rays == 0) return cudaMemsetAsync(offsets_out, 0, sizeof(int64_t), s) == cudaSuccess ? A3D_OK : A3D_ERR_CUDA;
   A3D_REQUIRE(rays_o && rays_d, A3D_ERR_ARGUMENT, "ray_all: null pointer");
-  ray_all_count_kernel<<<(unsigned)ceil_div(num_rays, 128), 128, 0, s>>>(
+  A3D_PDL(ray_all_count_kernel, dim3((unsigned)ceil_div(num_rays, 128)), dim3(128), 0, s, 
       (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, rays_o, rays_d, num_rays, max_t, w.counts, w.status + 1);
-  A3D_LAUNCH_CHECK();
   A3D_TRY((device_exclusive_scan<int32_t, int64_t>(w.counts, offsets_out, num_rays, w.scan_tmp,
                                                    offsets_out + num_rays, s)));
   return A3D_OK;
@@ -545,9 +547,8 @@ extern "C" int a3d_ray_all_collect(const a3d_bvh_view* bvh, const float* rays_o,
   A3D_REQUIRE(rays_o && rays_d && offsets && ray_idx && t && face_ids && sign, A3D_ERR_ARGUMENT,
               "ray_all: null pointer");
   const AllOut out{ray_idx, t, face_ids, sign, hit_points, uvw};
-  ray_all_collect_kernel<<<(unsigned)ceil_div(num_rays, 128), 128, 0, s>>>(
+  A3D_PDL(ray_all_collect_kernel, dim3((unsigned)ceil_div(num_rays, 128)), dim3(128), 0, s, 
       (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, rays_o, rays_d, num_rays, max_t, offsets, out);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
 
@@ -562,10 +563,9 @@ extern "C" int a3d_ray_parity_votes(const a3d_bvh_view* bvh, const float* points
   A3D_CUDA_TRY(cudaMemsetAsync(w.status, 0, 4 * sizeof(uint32_t), s));
   if (num_points == 0) return A3D_OK;
   A3D_REQUIRE(points && dirs && votes, A3D_ERR_ARGUMENT, "ray_parity: null pointer");
-  ray_parity_kernel<<<(unsigned)ceil_div(num_points, 64), 64, 0, s>>>(
+  A3D_PDL(ray_parity_kernel, dim3((unsigned)ceil_div(num_points, 64)), dim3(64), 0, s, 
       (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, points, num_points, dirs, num_dirs, max_t, coalesce_t,
       votes, w.status + 1);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
 

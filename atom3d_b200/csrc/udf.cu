@@ -380,6 +380,7 @@ __global__ void __launch_bounds__(kUdfThreads)
                int64_t n, int chunk, const uint32_t* __restrict__ perm, const float* __restrict__ bound,
                QueryOut out, SignArgs sg, unsigned long long* stats, uint32_t* __restrict__ rerun,
                uint32_t* __restrict__ nrerun) {
+  pdl_wait();
   __shared__ uint2 s_stack[kSharedDepth * kUdfThreads];
   __shared__ uint32_t s_next[kUdfThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -518,6 +519,7 @@ __global__ void __maxnreg__(kTaskMaxRegs)
                     const float* __restrict__ bound, QueryOut out, SignArgs sg, unsigned long long* stats,
                     uint32_t* __restrict__ rerun, uint32_t* __restrict__ nrerun, uint32_t* __restrict__ pool_counter,
                     uint2* __restrict__ spill, int64_t spill_owners, uint32_t seeding, MeshSel sel, int pool) {
+  pdl_wait();
   __shared__ TaskSmem smem[kTaskWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   TaskSmem& S = smem[warp];
@@ -813,6 +815,7 @@ __global__ void __launch_bounds__(64)
     udf_rerun_kernel(TreeT<kBatch> T, const float* __restrict__ pts, const uint32_t* __restrict__ rerun,
                      const uint32_t* __restrict__ nrerun, QueryOut out, SignArgs sg, unsigned long long* stats,
                      uint32_t* __restrict__ overflow, uint32_t* __restrict__ total_reruns, MeshSel sel) {
+  pdl_wait();
   const uint32_t m = *nrerun;
   if (blockIdx.x == 0 && threadIdx.x == 0 && m > 0) atomicAdd(total_reruns, m);
   Counters ctr{0, 0};
@@ -839,6 +842,7 @@ __global__ void __launch_bounds__(64)
 __global__ void query_morton_kernel(const float* __restrict__ pts, int64_t n, float lox, float loy, float loz,
                                     float ix, float iy, float iz, uint32_t* __restrict__ keys,
                                     uint32_t* __restrict__ vals) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float q[3] = {(pts[3 * i] - lox) * ix, (pts[3 * i + 1] - loy) * iy, (pts[3 * i + 2] - loz) * iz};
@@ -930,13 +934,12 @@ int launch_udf(const TreeT<kBatch>& T, const float* pts, int64_t n, const uint32
     const int64_t pools = ceil_div(n, pool);
     const int64_t want_blocks = ceil_div(pools, kTaskWarps);
     const int64_t grid = want_blocks < (int64_t)sms * bps ? want_blocks : (int64_t)sms * bps;
-    udf_task_kernel<kSign, kStats, kBatch><<<(unsigned)grid, kTaskWarps * 32, 0, s>>>(
-        T, pts, n, perm, bound, out, sg, stats, w.rerun, w.nrerun, w.nrerun + 2, w.spill, w.spill_owners, seeding,
-        sel, pool);
+    A3D_PDL((udf_task_kernel<kSign, kStats, kBatch>), dim3((unsigned)grid), dim3(kTaskWarps * 32), 0, s, T, pts, n,
+            perm, bound, out, sg, stats, w.rerun, w.nrerun, w.nrerun + 2, w.spill, w.spill_owners, seeding, sel, pool);
   } else {
     if constexpr (!kBatch) {
-      udf_kernel<kSign, kStats><<<(unsigned)ceil_div(n, kUdfThreads), kUdfThreads, 0, s>>>(
-          T, pts, n, 1, perm, bound, out, sg, stats, w.rerun, w.nrerun);
+      A3D_PDL((udf_kernel<kSign, kStats>), dim3((unsigned)ceil_div(n, kUdfThreads)), dim3(kUdfThreads), 0, s, T, pts, n,
+              1, perm, bound, out, sg, stats, w.rerun, w.nrerun);
     } else {
       A3D_REQUIRE(false, A3D_ERR_ARGUMENT, "udf: batches are always sorted");
     }
@@ -946,9 +949,8 @@ int launch_udf(const TreeT<kBatch>& T, const float* pts, int64_t n, const uint32
   // threads for a few percent of the queries, each thread strides
   const int64_t rr_min = (int64_t)num_sms() * 256;
   const int64_t rr_threads = n / 16 > rr_min ? n / 16 : rr_min;
-  udf_rerun_kernel<kSign, kStats, kBatch><<<(unsigned)ceil_div(rr_threads, 64), 64, 0, s>>>(
+  A3D_PDL((udf_rerun_kernel<kSign, kStats, kBatch>), dim3((unsigned)ceil_div(rr_threads, 64)), dim3(64), 0, s, 
       T, pts, w.rerun, w.nrerun, out, sg, stats, w.nrerun + 1, w.nrerun + 4, sel);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
 
@@ -959,6 +961,7 @@ __global__ void udf_backward_kernel(const float* __restrict__ pts, int64_t n, co
                                     const int32_t* __restrict__ fid, const float* __restrict__ uvw,
                                     const float* __restrict__ gd, const int32_t* __restrict__ faces,
                                     float* __restrict__ gp, float* __restrict__ gv) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float dx = pts[3 * i] - cp[3 * i], dy = pts[3 * i + 1] - cp[3 * i + 1], dz = pts[3 * i + 2] - cp[3 * i + 2];
@@ -1050,9 +1053,8 @@ extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num
     const float lo[3] = {0.5f * (bvh->lo[0] + bvh->hi[0]) - emax, 0.5f * (bvh->lo[1] + bvh->hi[1]) - emax,
                          0.5f * (bvh->lo[2] + bvh->hi[2]) - emax};
     const float inv = 1023.0f / (2.0f * emax);
-    query_morton_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(points, n, lo[0], lo[1], lo[2], inv, inv, inv,
+    A3D_PDL(query_morton_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, s, points, n, lo[0], lo[1], lo[2], inv, inv, inv,
                                                                    w.keys, w.vals);
-    A3D_LAUNCH_CHECK();
     bool alt = false;
     A3D_TRY(radix_sort_pairs<uint32_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, n, 0, 32, w.rs_scratch, &alt, s));
     perm = alt ? w.vals_alt : w.vals;
@@ -1096,9 +1098,8 @@ extern "C" int a3d_udf_backward(const float* points, int64_t num_points, const f
   A3D_REQUIRE(points && closest_points && grad_dist, A3D_ERR_ARGUMENT, "udf_backward: null input");
   A3D_REQUIRE(!grad_vertices || (face_ids && uvw && faces), A3D_ERR_ARGUMENT,
               "udf_backward: vertex adjoint needs face ids, uvw and faces");
-  udf_backward_kernel<<<(unsigned)ceil_div(num_points, 256), 256, 0, s>>>(
+  A3D_PDL(udf_backward_kernel, dim3((unsigned)ceil_div(num_points, 256)), dim3(256), 0, s, 
       points, num_points, closest_points, face_ids, uvw, grad_dist, faces, grad_points, grad_vertices);
-  A3D_LAUNCH_CHECK();
   return A3D_OK;
 }
 
@@ -1128,6 +1129,7 @@ __global__ void batch_query_morton_kernel(const float* __restrict__ pts, int64_t
                                           const int64_t* __restrict__ qoff, int nmesh,
                                           const float* __restrict__ bounds, int bits, uint32_t* __restrict__ keys,
                                           uint32_t* __restrict__ vals) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int m = segment_of64(qoff, nmesh, qbase + i);
@@ -1198,9 +1200,8 @@ int batch_udf(const a3d_bvh_batch* bvh, const float* points, const int64_t* qoff
   for (int64_t base = 0; base < n; base += kBatchChunk) {
     const int64_t cn = n - base < kBatchChunk ? n - base : kBatchChunk;
     const float* pts = points + 3 * base;
-    batch_query_morton_kernel<<<(unsigned)ceil_div(cn, 256), 256, 0, s>>>(pts, cn, base, qoff, bvh->num_meshes,
+    A3D_PDL(batch_query_morton_kernel, dim3((unsigned)ceil_div(cn, 256)), dim3(256), 0, s, pts, cn, base, qoff, bvh->num_meshes,
                                                                           bvh->bounds, bits, w.keys, w.vals);
-    A3D_LAUNCH_CHECK();
     bool alt = false;
     A3D_TRY(radix_sort_pairs<uint32_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, cn, 0, 3 * bits + mbits,
                                        w.rs_scratch, &alt, s));
@@ -1224,6 +1225,7 @@ int batch_udf(const a3d_bvh_batch* bvh, const float* points, const int64_t* qoff
 // every stride-th query, with the offsets of the sample per mesh
 __global__ void sample_queries_kernel(const float* __restrict__ pts, int64_t stride, const int64_t* __restrict__ qoff,
                                       int nmesh, float* __restrict__ spts, int64_t ns, int64_t* __restrict__ sqoff) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < ns) {
     const int64_t j = i * stride;
@@ -1316,9 +1318,8 @@ extern "C" int a3d_batch_autotune(const a3d_bvh_batch* bvh, const float* points,
   carve_tune(t, ws, ns, bvh->num_meshes);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "batch_autotune: workspace too small");
   const int64_t th = ns > (int64_t)bvh->num_meshes + 1 ? ns : (int64_t)bvh->num_meshes + 1;
-  sample_queries_kernel<<<(unsigned)ceil_div(th, 256), 256, 0, s>>>(points, stride, query_offsets, bvh->num_meshes,
+  A3D_PDL(sample_queries_kernel, dim3((unsigned)ceil_div(th, 256)), dim3(256), 0, s, points, stride, query_offsets, bvh->num_meshes,
                                                                     t.pts, ns, t.qoff);
-  A3D_LAUNCH_CHECK();
   int occ = 0;
   A3D_TRY((task_blocks_per_sm<false, false, true>(&occ)));
   const int pools[4] = {32, 64, 128, 256};
