@@ -397,11 +397,10 @@ int launch_write(const a3d_bvh_view* bvh, const float* bmin, const float* bmax, 
                  int32_t* out_box, int32_t* out_face, cudaStream_t s) {
   const WideNode* nodes = (const WideNode*)bvh->nodes;
   const TriRec* tris = (const TriRec*)bvh->tris;
-  A3D_PDL(pairs_write_kernel<kSlots>, dim3((unsigned)ceil_div(n, kSatThreads)), dim3(kSatThreads), 0, s, nodes, tris, bmin, bmax, n,
-                                                                                        w.offs, out_box, out_face,
-                                                                                        w.misc);
-  A3D_PDL(pairs_write_spill_kernel<kSlots>, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, bmin, bmax, w.offs, w.spill, w.misc,
-                                                              out_box, out_face);
+  A3D_PDL(pairs_write_kernel<kSlots>, dim3((unsigned)ceil_div(n, kSatThreads)), dim3(kSatThreads), 0, s, nodes, tris,
+          bmin, bmax, n, w.offs, out_box, out_face, w.misc);
+  A3D_PDL(pairs_write_spill_kernel<kSlots>, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, bmin, bmax, w.offs,
+          w.spill, w.misc, out_box, out_face);
   return A3D_OK;
 }
 
@@ -449,9 +448,10 @@ extern "C" int a3d_aabb_pairs_count(const a3d_bvh_view* bvh, const float* box_mi
   uint8_t* h = mode == 1 ? hit : nullptr;
   const WideNode* nodes = (const WideNode*)bvh->nodes;
   const TriRec* tris = (const TriRec*)bvh->tris;
-  A3D_PDL(pairs_count_kernel, dim3((unsigned)ceil_div(n, kSatThreads)), dim3(kSatThreads), 0, s, nodes, tris, box_min, box_max, n,
-                                                                                 w.counts, h, w.spill, w.misc);
-  A3D_PDL(pairs_count_spill_kernel, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, box_min, box_max, w.counts, h, w.spill, w.misc);
+  A3D_PDL(pairs_count_kernel, dim3((unsigned)ceil_div(n, kSatThreads)), dim3(kSatThreads), 0, s, nodes, tris, box_min,
+          box_max, n, w.counts, h, w.spill, w.misc);
+  A3D_PDL(pairs_count_spill_kernel, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, box_min, box_max, w.counts, h,
+          w.spill, w.misc);
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.counts, w.offs, n, w.scan_tmp, w.offs + n, s)));
   unsigned long long misc[4];
   int64_t total = 0;
@@ -485,9 +485,8 @@ extern "C" int a3d_aabb_pairs_clip(const a3d_bvh_view* bvh, const float* box_min
   A3D_CUDA_TRY(cudaMemsetAsync(hit, 0, n, s));
   if (num_candidates == 0) return A3D_OK;
   A3D_TRY(launch_write<true>(bvh, box_min, box_max, n, w, (int32_t*)c.cand_box, (int32_t*)c.cand_slot, s));
-  A3D_PDL(clip_flags_kernel, dim3((unsigned)ceil_div(num_candidates, 256)), dim3(256), 0, s, 
-      (const TriRec*)bvh->tris, box_min, box_max, c.cand_box, c.cand_slot, num_candidates, c.flags, hit, n,
-      bvh->num_tris, w.misc + 2);
+  A3D_PDL(clip_flags_kernel, dim3((unsigned)ceil_div(num_candidates, 256)), dim3(256), 0, s, (const TriRec*)bvh->tris,
+          box_min, box_max, c.cand_box, c.cand_slot, num_candidates, c.flags, hit, n, bvh->num_tris, w.misc + 2);
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(c.flags, c.coffs, num_candidates, c.scan_tmp,
                                                      c.coffs + num_candidates, s)));
   int64_t total = 0;

@@ -692,11 +692,11 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
   const int mbits = mesh_bits_of(nmesh);
   const int bits = (64 - mbits) / 3 < 21 ? (64 - mbits) / 3 : 21;
   const int64_t init_threads = 12ll * nmesh > kMaxLevels + 1 ? 12ll * nmesh : kMaxLevels + 1;
-  A3D_PDL(init_kernel, dim3((unsigned)ceil_div(init_threads, kThreads)), dim3(kThreads), 0, s, face_off, nmesh, n, w.bounds, w.err,
-                                                                              w.counters, w.work_a);
+  A3D_PDL(init_kernel, dim3((unsigned)ceil_div(init_threads, kThreads)), dim3(kThreads), 0, s, face_off, nmesh, n,
+          w.bounds, w.err, w.counters, w.work_a);
   const unsigned g = (unsigned)ceil_div(n, kThreads);
-  A3D_PDL(tri_prep_kernel, dim3(g), dim3(kThreads), 0, s, V, vert_off, F, face_off, nmesh, n, w.tri_lo, w.tri_hi, w.centroid,
-                                         w.mesh_of, w.bounds, w.err);
+  A3D_PDL(tri_prep_kernel, dim3(g), dim3(kThreads), 0, s, V, vert_off, F, face_off, nmesh, n, w.tri_lo, w.tri_hi,
+          w.centroid, w.mesh_of, w.bounds, w.err);
   A3D_PDL(morton_kernel, dim3(g), dim3(kThreads), 0, s, w.centroid, w.mesh_of, n, w.bounds, bits, w.keys, w.vals);
   bool alt = false;
   A3D_TRY(radix_sort_pairs<uint64_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, n, 0, 3 * bits + mbits, w.rs_scratch,
@@ -704,19 +704,21 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
   const uint64_t* keys = alt ? w.keys_alt : w.keys;
   const uint32_t* order = alt ? w.vals_alt : w.vals;
 
-  A3D_PDL(radix_tree_kernel, dim3(g), dim3(kThreads), 0, s, keys, face_off, nmesh, n, w.left, w.right, w.parent, w.first, w.last);
+  A3D_PDL(radix_tree_kernel, dim3(g), dim3(kThreads), 0, s, keys, face_off, nmesh, n, w.left, w.right, w.parent,
+          w.first, w.last);
   // SAH refinement of every subtree of <= kSahMax triangles below the top
   A3D_CUDA_TRY(cudaMemsetAsync(w.ncl, 0, sizeof(uint32_t), s));
-  A3D_PDL(sah_find_kernel, dim3(g), dim3(kThreads), 0, s, face_off, nmesh, n, w.parent, w.first, w.last, w.clusters, w.ncl);
+  A3D_PDL(sah_find_kernel, dim3(g), dim3(kThreads), 0, s, face_off, nmesh, n, w.parent, w.first, w.last, w.clusters,
+          w.ncl);
   int sah_grid = 0;
   A3D_TRY(sah_grid_size(&sah_grid));
   const int64_t max_clusters = n / 3 + 1;
-  A3D_PDL(sah_cluster_kernel, dim3((unsigned)(max_clusters < sah_grid ? max_clusters : sah_grid)), dim3(kSahThreads), sizeof(SahSmem), s, w.clusters, w.ncl, SahTree{w.left, w.right, w.parent, w.first, w.last, n},
-                            const_cast<uint32_t*>(order), w.sah_tmp, w.sah_small,
-                            SahPrims{w.centroid, w.tri_lo, w.tri_hi});
+  A3D_PDL(sah_cluster_kernel, dim3((unsigned)(max_clusters < sah_grid ? max_clusters : sah_grid)), dim3(kSahThreads),
+          sizeof(SahSmem), s, w.clusters, w.ncl, SahTree{w.left, w.right, w.parent, w.first, w.last, n},
+          const_cast<uint32_t*>(order), w.sah_tmp, w.sah_small, SahPrims{w.centroid, w.tri_lo, w.tri_hi});
   A3D_CUDA_TRY(cudaMemsetAsync(w.visit, 0, sizeof(uint32_t) * n, s));
-  A3D_PDL(refit_kernel, dim3(g), dim3(kThreads), 0, s, order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.first, w.last,
-                                      leaf_max, w.box_lo, w.box_hi, w.dp_cost, w.dp_dec, w.visit);
+  A3D_PDL(refit_kernel, dim3(g), dim3(kThreads), 0, s, order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.first,
+          w.last, leaf_max, w.box_lo, w.box_hi, w.dp_cost, w.dp_dec, w.visit);
   A3D_PDL(write_tris_kernel, dim3(g), dim3(kThreads), 0, s, V, vert_off, F, face_off, w.mesh_of, order, n, tris_out);
 
   // collapse: a fixed number of level launches (empty levels return at once)
@@ -725,9 +727,8 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
   const int64_t lb = ceil_div(n, kThreads) < level_blocks ? ceil_div(n, kThreads) : level_blocks;
   int32_t *cur = w.work_a, *nxt = w.work_b;
   for (int level = 0; level < kMaxLevels; ++level) {
-    A3D_PDL(collapse_level_kernel, dim3((unsigned)lb), dim3(kThreads), 0, s, level, w.counters, cur, nxt, n, leaf_max, w.left,
-                                                            w.right, w.first, w.last, w.box_lo, w.box_hi,
-                                                            w.dp_dec, w.tmp_nodes, w.lvl);
+    A3D_PDL(collapse_level_kernel, dim3((unsigned)lb), dim3(kThreads), 0, s, level, w.counters, cur, nxt, n, leaf_max,
+            w.left, w.right, w.first, w.last, w.box_lo, w.box_hi, w.dp_dec, w.tmp_nodes, w.lvl);
     int32_t* t = cur;
     cur = nxt;
     nxt = t;
@@ -741,9 +742,8 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
   const uint32_t* sslot = lalt ? w.slot_alt : w.slot;
   A3D_PDL(layout_index_kernel, dim3(g), dim3(kThreads), 0, s, slvl, sslot, n, w.newidx);
   A3D_PDL(layout_copy_kernel, dim3(g), dim3(kThreads), 0, s, slvl, sslot, n, w.newidx, w.tmp_nodes, nodes_out);
-  A3D_PDL(finish_kernel, dim3((unsigned)ceil_div(nmesh, kThreads)), dim3(kThreads), 0, s, face_off, nmesh, w.counters, w.newidx,
-                                                                         w.bounds, roots_out, bounds_out,
-                                                                         num_nodes_out);
+  A3D_PDL(finish_kernel, dim3((unsigned)ceil_div(nmesh, kThreads)), dim3(kThreads), 0, s, face_off, nmesh, w.counters,
+          w.newidx, w.bounds, roots_out, bounds_out, num_nodes_out);
   if (status_out) A3D_CUDA_TRY(cudaMemcpyAsync(status_out, w.err, 2 * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
   return A3D_OK;
 }

@@ -1212,8 +1212,8 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   A3D_PDL(case_fix_kernel, dim3(gsz(n)), dim3(256), 0, s, in, ns_dev, w.list, w.cases, w.table, w.table_mask, w.case_s);
   A3D_PDL(cross_count_kernel, dim3(gsz(n)), dim3(256), 0, s, in, ns_dev, w.list, w.cases, w.mask12, w.ccnt);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ccnt, w.coff, n, w.scan_tmp, w.coff + n, s)));
-  A3D_PDL(cross_write_kernel, dim3(gsz(n, kCrossThreads)), dim3(kCrossThreads), 0, s, in, ns_dev, w.list, w.mask12, w.coff, w.keys,
-                                                                     w.vals);
+  A3D_PDL(cross_write_kernel, dim3(gsz(n, kCrossThreads)), dim3(kCrossThreads), 0, s, in, ns_dev, w.list, w.mask12,
+          w.coff, w.keys, w.vals);
   // the one round trip before the edge sort: surface cubes, crossings and
   // the out-of-range flag
   uint32_t h3[3];
@@ -1231,13 +1231,15 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   A3D_PDL(edge_count_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, nc, (uint64_t)m, w.rid, w.ecnt);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ecnt, w.estart, m, w.scan_tmp, w.estart + m, s)));
   A3D_TRY(fill_async<uint32_t>(w.ecnt, m, 0u, s));
-  A3D_PDL(edge_scatter_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.rid, w.estart, w.ecnt, w.keys2, w.vals2, w.rflag);
+  A3D_PDL(edge_scatter_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.rid, w.estart, w.ecnt, w.keys2,
+          w.vals2, w.rflag);
   A3D_PDL(edge_rank_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys2, w.vals2, nc, w.rflag, w.estart, w.keys, w.vals);
   A3D_PDL(run_flag_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, nc, w.rflag);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.rflag, w.rid, nc, w.scan_tmp, w.misc, s)));
   // idx_map is read only at crossing (cube, edge) pairs, all of which
   // run_info_kernel writes: no clear
-  A3D_PDL(run_info_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.rflag, w.rid, m, w.idx_map, w.e0, w.e1, w.rfirst);
+  A3D_PDL(run_info_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.rflag, w.rid, m, w.idx_map, w.e0, w.e1,
+          w.rfirst);
   A3D_PDL(quad_flag_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.misc, nc, w.rfirst, w.qflag);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.qflag, w.qoff, nc, w.scan_tmp, w.qoff + nc, s)));
   // dual vertices numbered per vertex-count class (two packed scans)
@@ -1245,7 +1247,8 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   A3D_PDL(vd_class_kernel, dim3(gsz(ns)), dim3(256), 0, s, ns, w.case_s, w.cls_a, w.cls_b);
   A3D_TRY((device_exclusive_scan<uint64_t, uint64_t>(w.cls_a, w.cls_ra, ns, w.scan_tmp64, w.cls_ra + ns, s)));
   A3D_TRY((device_exclusive_scan<uint64_t, uint64_t>(w.cls_b, w.cls_rb, ns, w.scan_tmp64, w.cls_rb + ns, s)));
-  A3D_PDL(vd_assign_kernel, dim3(gsz(ns)), dim3(256), 0, s, ns, w.case_s, w.cls_ra, w.cls_rb, w.vd_cube, w.vd_slot, w.vd_ne);
+  A3D_PDL(vd_assign_kernel, dim3(gsz(ns)), dim3(256), 0, s, ns, w.case_s, w.cls_ra, w.cls_rb, w.vd_cube, w.vd_slot,
+          w.vd_ne);
   // per-vertex edge offsets over the 4 Ns bound (entries past the last
   // vertex are zero)
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.vd_ne, w.goff, 4 * ns, w.scan_tmp, w.goff + 4 * ns, s)));
@@ -1253,8 +1256,8 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   // low word first)
   const uint32_t* ra = reinterpret_cast<const uint32_t*>(w.cls_ra + ns);
   const uint32_t* rb = reinterpret_cast<const uint32_t*>(w.cls_rb + ns);
-  A3D_PDL(gather_words_kernel, dim3(1), dim3(32), 0, s, WordList{{w.misc, w.qoff + nc, w.goff + 4 * ns, ra, ra + 1, rb, rb + 1}, 7},
-                                       w.misc + 8);
+  A3D_PDL(gather_words_kernel, dim3(1), dim3(32), 0, s,
+          WordList{{w.misc, w.qoff + nc, w.goff + 4 * ns, ra, ra + 1, rb, rb + 1}, 7}, w.misc + 8);
   uint32_t h7[7];
   A3D_CUDA_TRY(cudaMemcpyAsync(h7, w.misc + 8, sizeof(h7), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1284,11 +1287,13 @@ extern "C" int a3d_dmc_emit(const a3d_dmc_inputs* p, void* workspace, size_t wor
   DmcIn in = make_in(p);
   EdgeData ed{w.e0, w.e1, w.idx_map};
   VdOut out{vertices, l_dev, p_alpha, n_alpha};
-  A3D_PDL(vd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, out);
+  A3D_PDL(vd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed,
+          out);
   (void)nc;
   if (nq > 0) {
-    A3D_PDL(quad_kernel, dim3(gsz(ne, kQuadThreads)), dim3(kQuadThreads), 0, s, ne, nc, w.qflag, w.qoff, w.rfirst, w.vals, VdNumbering{w.case_s, w.cls_ra, w.cls_rb, ns}, w.e0, p->sdf, p->isovalue,
-                                        nv, vertices, faces, w.quads);
+    A3D_PDL(quad_kernel, dim3(gsz(ne, kQuadThreads)), dim3(kQuadThreads), 0, s, ne, nc, w.qflag, w.qoff, w.rfirst,
+            w.vals, VdNumbering{w.case_s, w.cls_ra, w.cls_rb, ns}, w.e0, p->sdf, p->isovalue, nv, vertices, faces,
+            w.quads);
   }
   return A3D_OK;
 }
@@ -1313,7 +1318,8 @@ extern "C" int a3d_dmc_backward(const a3d_dmc_inputs* p, void* workspace, size_t
     A3D_PDL(quad_bwd_kernel, dim3(gsz(nq)), dim3(256), 0, s, nq, nv, w.quads, gr);
   }
   EdgeData ed{w.e0, w.e1, w.idx_map};
-  A3D_PDL(vd_bwd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, gr);
+  A3D_PDL(vd_bwd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, nv, w.list, w.case_s, w.vd_cube, w.vd_slot, w.goff,
+          ed, gr);
   return A3D_OK;
 }
 
@@ -1332,7 +1338,8 @@ extern "C" int a3d_dmc_features(const a3d_dmc_inputs* p, void* workspace, size_t
   DmcIn in = make_in(p);
   EdgeData ed{w.e0, w.e1, w.idx_map};
   const int C = channels;
-  A3D_PDL(vd_feat_kernel, dim3(gsz(nv * C)), dim3(256), 0, s, in, nv, C, features, w.list, w.case_s, w.vd_cube, w.vd_slot, ed, out);
+  A3D_PDL(vd_feat_kernel, dim3(gsz(nv * C)), dim3(256), 0, s, in, nv, C, features, w.list, w.case_s, w.vd_cube,
+          w.vd_slot, ed, out);
   if (with_centres && nq > 0) {
     A3D_PDL(quad_feat_kernel, dim3(gsz(nq * C)), dim3(256), 0, s, nq, nv, C, w.quads, out);
   }
@@ -1363,8 +1370,8 @@ extern "C" int a3d_dmc_features_backward(const a3d_dmc_inputs* p, void* workspac
     A3D_PDL(quad_feat_bwd_kernel, dim3(gsz(nq * C)), dim3(256), 0, s, nq, nv, C, w.quads, g_out, scratch);
   }
   FeatGrad gr{g_out, centres ? scratch : nullptr, g_features, g_sdf, g_alpha, g_beta};
-  A3D_PDL(vd_feat_bwd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, nv, C, features, w.list, w.case_s, w.vd_cube, w.vd_slot, ed,
-                                                   gr);
+  A3D_PDL(vd_feat_bwd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, nv, C, features, w.list, w.case_s, w.vd_cube,
+          w.vd_slot, ed, gr);
   return A3D_OK;
 }
 
@@ -2191,11 +2198,11 @@ extern "C" int a3d_dmc_emit_qef(const a3d_dmc_inputs* p, void* workspace, size_t
   // corner world positions (the training path computes them per edge)
   A3D_PDL(init_pos_kernel, dim3(gsz(m)), dim3(256), 0, s, m, p->deform, w.x, nullptr);
   A3D_PDL(corner_pos_kernel, dim3(gsz(8 * n)), dim3(256), 0, s, in, world_scale_host(p->resolution), w.x);
-  A3D_PDL(vd_qef_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, w.x, corner_gradients, qef_reg_scale, nv, w.list, w.case_s,
-                                             w.vd_cube, w.vd_slot, w.goff, ed, out);
+  A3D_PDL(vd_qef_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, w.x, corner_gradients, qef_reg_scale, nv, w.list,
+          w.case_s, w.vd_cube, w.vd_slot, w.goff, ed, out);
   if (nq > 0) {
-    A3D_PDL(quad_eval_kernel, dim3(gsz(ne, kQuadThreads)), dim3(kQuadThreads), 0, s, ne, w.qflag, w.qoff, w.rfirst, w.vals, VdNumbering{w.case_s, w.cls_ra, w.cls_rb, ns}, w.e0, p->sdf,
-                                             p->isovalue, vertices, faces);
+    A3D_PDL(quad_eval_kernel, dim3(gsz(ne, kQuadThreads)), dim3(kQuadThreads), 0, s, ne, w.qflag, w.qoff, w.rfirst,
+            w.vals, VdNumbering{w.case_s, w.cls_ra, w.cls_rb, ns}, w.e0, p->sdf, p->isovalue, vertices, faces);
   }
   return A3D_OK;
 }
@@ -2219,7 +2226,7 @@ extern "C" int a3d_dmc_backward_qef(const a3d_dmc_inputs* p, void* workspace, si
   A3D_PDL(init_pos_kernel, dim3(gsz(m)), dim3(256), 0, s, m, p->deform, w.x, nullptr);
   A3D_PDL(corner_pos_kernel, dim3(gsz(8 * n)), dim3(256), 0, s, in, world_scale_host(p->resolution), w.x);
   QefGrad gq{g_vertices, g_l_dev, g_p_alpha, g_n_alpha, g_sdf, g_deform, g_alpha, g_corner_gradients};
-  A3D_PDL(vd_qef_bwd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, w.x, corner_gradients, qef_reg_scale, nv, w.list, w.case_s,
-                                                 w.vd_cube, w.vd_slot, w.goff, gq);
+  A3D_PDL(vd_qef_bwd_kernel, dim3(gsz(nv, 128)), dim3(128), 0, s, in, w.x, corner_gradients, qef_reg_scale, nv, w.list,
+          w.case_s, w.vd_cube, w.vd_slot, w.goff, gq);
   return A3D_OK;
 }

@@ -416,9 +416,11 @@ extern "C" int a3d_dual_graph_count(const int32_t* const* lists, const int64_t* 
   for (int l = 0; l < num_lists; ++l) {
     A3D_REQUIRE(counts[l] >= 0 && (counts[l] == 0 || lists[l]), A3D_ERR_ARGUMENT, "dual_graph_count: bad list");
     if (counts[l] == 0) continue;
-    A3D_PDL(set_cells_kernel, dim3((unsigned)ceil_div(counts[l], 256)), dim3(256), 0, s, lists[l], counts[l], g, w.cells);
+    A3D_PDL(set_cells_kernel, dim3((unsigned)ceil_div(counts[l], 256)), dim3(256), 0, s, lists[l], counts[l], g,
+            w.cells);
   }
-  A3D_PDL(corners_kernel, dim3((unsigned)ceil_div(nwords, 256)), dim3(256), 0, s, g, w.cells, w.verts, w.ccnt, w.vcnt, nwords);
+  A3D_PDL(corners_kernel, dim3((unsigned)ceil_div(nwords, 256)), dim3(256), 0, s, g, w.cells, w.verts, w.ccnt, w.vcnt,
+          nwords);
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.ccnt, w.coffs, nwords, w.scan_tmp, w.coffs + nwords, s)));
   A3D_TRY((device_exclusive_scan<uint32_t, int64_t>(w.vcnt, w.voffs, nwords, w.scan_tmp, w.voffs + nwords, s)));
   A3D_CUDA_TRY(cudaMemcpyAsync(counts_out, w.coffs + nwords, 8, cudaMemcpyDeviceToHost, s));
@@ -447,10 +449,12 @@ extern "C" int a3d_dual_graph_emit(const a3d_dual_geom* geom, void* workspace, s
   const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
   const unsigned gw = (unsigned)ceil_div(nwords, 256);
   const float3 o = make_float3(origin[0], origin[1], origin[2]), c = make_float3(cell[0], cell[1], cell[2]);
-  A3D_PDL(extract_kernel<false>, dim3(gw), dim3(256), 0, s, g, w.cells, w.coffs, nwords, cells_ijk, nullptr, nullptr, o, c);
-  A3D_PDL(extract_kernel<true>, dim3(gw), dim3(256), 0, s, g, w.verts, w.voffs, nwords, nullptr, vertices_ijk, vertices_world, o, c);
-  A3D_PDL(links_kernel, dim3((unsigned)ceil_div(num_cells, 256)), dim3(256), 0, s, g, geom->resolution, cells_ijk, num_cells, w.cells,
-                                                                   w.coffs, w.verts, w.voffs, cube_idx, adj_idx);
+  A3D_PDL(extract_kernel<false>, dim3(gw), dim3(256), 0, s, g, w.cells, w.coffs, nwords, cells_ijk, nullptr, nullptr, o,
+          c);
+  A3D_PDL(extract_kernel<true>, dim3(gw), dim3(256), 0, s, g, w.verts, w.voffs, nwords, nullptr, vertices_ijk,
+          vertices_world, o, c);
+  A3D_PDL(links_kernel, dim3((unsigned)ceil_div(num_cells, 256)), dim3(256), 0, s, g, geom->resolution, cells_ijk,
+          num_cells, w.cells, w.coffs, w.verts, w.voffs, cube_idx, adj_idx);
   return A3D_OK;
 }
 
@@ -488,6 +492,7 @@ extern "C" int a3d_dam_wet(const int32_t* dam_ijk, int64_t n, const int32_t* col
   A3D_CUDA_TRY(cudaMemsetAsync(vol, 0, nwords * 4, s));
   A3D_PDL(set_cells_kernel, dim3((unsigned)ceil_div(m, 256)), dim3(256), 0, s, collision_ijk, m, g, vol);
   static const WetMasks wm = make_wet_masks();
-  A3D_PDL(dam_wet_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, s, g, vol, dam_ijk, n, wm, wet_faces, wet_edges, wet_corners);
+  A3D_PDL(dam_wet_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, s, g, vol, dam_ijk, n, wm, wet_faces,
+          wet_edges, wet_corners);
   return A3D_OK;
 }

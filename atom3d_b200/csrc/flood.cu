@@ -743,7 +743,8 @@ extern "C" int a3d_flood_test(const a3d_flood_geom* geom, void* workspace, size_
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "flood_test: workspace too small");
   if (n == 0) return A3D_OK;
   const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
-  A3D_PDL(test_bits_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, s, g, w.lab + (int64_t)label * nwords, ijk, n, out);
+  A3D_PDL(test_bits_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, s, g, w.lab + (int64_t)label * nwords, ijk,
+          n, out);
   return A3D_OK;
 }
 
@@ -773,10 +774,11 @@ extern "C" int a3d_ring_signs(const int64_t* dam_ijk, int64_t n_dam, const int64
   A3D_PDL(set_bits_kernel, dim3((unsigned)ceil_div(n_dam, 256)), dim3(256), 0, s, dam_ijk, n_dam, g, v_dam);
   if (n_water > 0) {
     A3D_PDL(set_bits_kernel, dim3((unsigned)ceil_div(n_water, 256)), dim3(256), 0, s, water_ijk, n_water, g,
-                                                                     w.lab + (int64_t)kWater * nwords);
+            w.lab + (int64_t)kWater * nwords);
   }
   if (n_dry > 0) {
-    A3D_PDL(set_bits_kernel, dim3((unsigned)ceil_div(n_dry, 256)), dim3(256), 0, s, dry_ijk, n_dry, g, w.lab + (int64_t)kDry * nwords);
+    A3D_PDL(set_bits_kernel, dim3((unsigned)ceil_div(n_dry, 256)), dim3(256), 0, s, dry_ijk, n_dry, g,
+            w.lab + (int64_t)kDry * nwords);
   }
   const unsigned gw = (unsigned)ceil_div(nwords, 256);
   uint32_t* ring_out = w.lab + (int64_t)kExtTide * nwords;
@@ -811,8 +813,7 @@ extern "C" int a3d_ring_signs_emit(const a3d_flood_geom* geom, void* workspace, 
   FloodWs w;
   carve_flood(w, ws, g);
   const int64_t nwords = (int64_t)g.nx * g.ny * g.nw;
-  A3D_PDL(ring_sign_kernel, dim3((unsigned)ceil_div(count, 256)), dim3(256), 0, s, 
-      g, w.lab + (int64_t)kDam * nwords, w.lab + (int64_t)kWater * nwords, w.lab + (int64_t)kDry * nwords, out_ijk,
-      count, out_signs);
+  A3D_PDL(ring_sign_kernel, dim3((unsigned)ceil_div(count, 256)), dim3(256), 0, s, g, w.lab + (int64_t)kDam * nwords,
+          w.lab + (int64_t)kWater * nwords, w.lab + (int64_t)kDry * nwords, out_ijk, count, out_signs);
   return A3D_OK;
 }

@@ -176,10 +176,10 @@ extern "C" int a3d_mesh_normals(const float* vertices, int64_t num_vertices, con
   const int64_t nh = 3 * num_faces;
   A3D_CUDA_TRY(cudaMemsetAsync(w.vacc, 0, sizeof(float) * 3 * num_vertices, s));
   A3D_CUDA_TRY(cudaMemsetAsync(w.total, 0, sizeof(uint32_t) * 2, s));
-  A3D_PDL(face_kernel, dim3((unsigned)ceil_div(num_faces, 256)), dim3(256), 0, s, vertices, faces, num_faces, num_vertices,
-                                                                 face_normals_sign, w.fn_unit, face_angles, w.vacc,
-                                                                 w.keys, w.vals, w.total + 1);
-  A3D_PDL(normalize_rows_kernel, dim3((unsigned)ceil_div(num_vertices, 256)), dim3(256), 0, s, w.vacc, vertex_pn, num_vertices);
+  A3D_PDL(face_kernel, dim3((unsigned)ceil_div(num_faces, 256)), dim3(256), 0, s, vertices, faces, num_faces,
+          num_vertices, face_normals_sign, w.fn_unit, face_angles, w.vacc, w.keys, w.vals, w.total + 1);
+  A3D_PDL(normalize_rows_kernel, dim3((unsigned)ceil_div(num_vertices, 256)), dim3(256), 0, s, w.vacc, vertex_pn,
+          num_vertices);
   // key bits: lo*V+hi < V^2
   int bits = 1;
   while (bits < 64 && ((unsigned __int128)1 << bits) < (unsigned __int128)num_vertices * num_vertices) ++bits;
@@ -198,6 +198,6 @@ extern "C" int a3d_mesh_normals(const float* vertices, int64_t num_vertices, con
   if (num_edges_out) *num_edges_out = ne;
   A3D_REQUIRE((int64_t)ne <= edge_capacity, A3D_ERR_WORKSPACE, "mesh_normals: edge capacity too small");
   A3D_PDL(edge_kernel, dim3((unsigned)ceil_div(nh, 256)), dim3(256), 0, s, k, he, nh, w.flag, w.eid, w.fn_unit, edge_pn,
-                                                          he_edge_idx);
+          he_edge_idx);
   return A3D_OK;
 }

@@ -224,7 +224,8 @@ extern "C" int a3d_morton_encode(const int64_t* ijk, int64_t n, int64_t* morton,
 extern "C" int a3d_morton_decode(const int64_t* morton, int64_t n, int level, int64_t* ijk, a3d_stream_t stream) {
   A3D_REQUIRE(n >= 0 && level >= 0, A3D_ERR_ARGUMENT, "morton_decode: bad argument");
   if (n == 0) return A3D_OK;
-  A3D_PDL(morton_decode_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, (cudaStream_t)stream, morton, n, level, ijk);
+  A3D_PDL(morton_decode_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, (cudaStream_t)stream, morton, n, level,
+          ijk);
   return A3D_OK;
 }
 
@@ -246,10 +247,10 @@ extern "C" int a3d_aabb_hit(const a3d_bvh_view* bvh, const float* box_min, const
   uint32_t* nspill = ws.take<uint32_t>(4);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "aabb_hit: workspace too small");
   A3D_CUDA_TRY(cudaMemsetAsync(nspill, 0, 4 * sizeof(uint32_t), s));
-  A3D_PDL(aabb_hit_kernel, dim3((unsigned)ceil_div(n, kSatThreads)), dim3(kSatThreads), 0, s, 
-      (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, box_min, box_max, n, hit, spill, nspill);
-  A3D_PDL(aabb_hit_spill_kernel, dim3(num_sms() * 4), dim3(64), 0, s, (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, box_min,
-                                                   box_max, hit, spill, nspill, (int*)(nspill + 1));
+  A3D_PDL(aabb_hit_kernel, dim3((unsigned)ceil_div(n, kSatThreads)), dim3(kSatThreads), 0, s,
+          (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, box_min, box_max, n, hit, spill, nspill);
+  A3D_PDL(aabb_hit_spill_kernel, dim3(num_sms() * 4), dim3(64), 0, s, (const WideNode*)bvh->nodes,
+          (const TriRec*)bvh->tris, box_min, box_max, hit, spill, nspill, (int*)(nspill + 1));
   int ov = 0;
   A3D_CUDA_TRY(cudaMemcpyAsync(&ov, nspill + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
   A3D_CUDA_TRY(cudaStreamSynchronize(s));
@@ -332,10 +333,10 @@ extern "C" int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo
     }
     A3D_CUDA_TRY(cudaMemsetAsync(w.misc, 0, 8 * sizeof(uint32_t), s));
     const unsigned gk = (unsigned)ceil_div(ncand, kSatThreads);
-    A3D_PDL(octree_level_kernel, dim3(gk), dim3(kSatThreads), 0, s, nodes, tris, ncand, first_level, res, parents, parent_hint, g,
-                                                   w.flags, w.ctri, w.spill, w.misc + 1);
-    A3D_PDL(octree_spill_kernel, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, first_level, res, parents, parent_hint, g, w.flags,
-                                                   w.ctri, w.spill, w.misc + 1, (int*)(w.misc + 2));
+    A3D_PDL(octree_level_kernel, dim3(gk), dim3(kSatThreads), 0, s, nodes, tris, ncand, first_level, res, parents,
+            parent_hint, g, w.flags, w.ctri, w.spill, w.misc + 1);
+    A3D_PDL(octree_spill_kernel, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, first_level, res, parents,
+            parent_hint, g, w.flags, w.ctri, w.spill, w.misc + 1, (int*)(w.misc + 2));
     A3D_PDL(flags_to_u8_kernel, dim3((unsigned)ceil_div(ncand, 256)), dim3(256), 0, s, w.flags, ncand, w.hit);
     A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.flags, w.flags, ncand, w.scan_tmp, w.misc, s)));
     uint32_t hm[3];
@@ -353,10 +354,9 @@ extern "C" int a3d_octree_traverse(const a3d_bvh_view* bvh, const float* grid_lo
       *count_out = -1;
       A3D_REQUIRE(false, A3D_ERR_WORKSPACE, "octree: level capacity exceeded");
     }
-    A3D_PDL(octree_compact_kernel, dim3((unsigned)ceil_div(ncand, 256)), dim3(256), 0, s, ncand, first_level, res, parents, w.hit,
-                                                                         w.flags, w.ctri, last ? nullptr : next,
-                                                                         last ? nullptr : next_hint,
-                                                                         last ? out_ijk : nullptr);
+    A3D_PDL(octree_compact_kernel, dim3((unsigned)ceil_div(ncand, 256)), dim3(256), 0, s, ncand, first_level, res,
+            parents, w.hit, w.flags, w.ctri, last ? nullptr : next, last ? nullptr : next_hint,
+            last ? out_ijk : nullptr);
     if (last || total == 0) {
       if (!last) *count_out = 0;
       break;

@@ -511,10 +511,10 @@ extern "C" int a3d_ray_nearest(const a3d_bvh_view* bvh, const float* rays_o, con
   const WideNode* nodes = (const WideNode*)bvh->nodes;
   const TriRec* tris = (const TriRec*)bvh->tris;
   const RayOut out{hit, t, face_ids, hit_points, normals, uvw};
-  A3D_PDL(ray_nearest_kernel, dim3((unsigned)ceil_div(num_rays, kRayThreads)), dim3(kRayThreads), 0, s, 
-      nodes, tris, face_normals, rays_o, rays_d, num_rays, max_t, out, w.rerun, w.status);
-  A3D_PDL(ray_nearest_rerun_kernel, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, face_normals, rays_o, rays_d, max_t, out, w.rerun,
-                                                      w.status, w.status + 1);
+  A3D_PDL(ray_nearest_kernel, dim3((unsigned)ceil_div(num_rays, kRayThreads)), dim3(kRayThreads), 0, s, nodes, tris,
+          face_normals, rays_o, rays_d, num_rays, max_t, out, w.rerun, w.status);
+  A3D_PDL(ray_nearest_rerun_kernel, dim3(num_sms() * 4), dim3(64), 0, s, nodes, tris, face_normals, rays_o, rays_d,
+          max_t, out, w.rerun, w.status, w.status + 1);
   return A3D_OK;
 }
 
@@ -529,8 +529,8 @@ extern "C" int a3d_ray_all_count(const a3d_bvh_view* bvh, const float* rays_o, c
   A3D_CUDA_TRY(cudaMemsetAsync(w.status, 0, 4 * sizeof(uint32_t), s));
   if (num_rays == 0) return cudaMemsetAsync(offsets_out, 0, sizeof(int64_t), s) == cudaSuccess ? A3D_OK : A3D_ERR_CUDA;
   A3D_REQUIRE(rays_o && rays_d, A3D_ERR_ARGUMENT, "ray_all: null pointer");
-  A3D_PDL(ray_all_count_kernel, dim3((unsigned)ceil_div(num_rays, 128)), dim3(128), 0, s, 
-      (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, rays_o, rays_d, num_rays, max_t, w.counts, w.status + 1);
+  A3D_PDL(ray_all_count_kernel, dim3((unsigned)ceil_div(num_rays, 128)), dim3(128), 0, s, (const WideNode*)bvh->nodes,
+          (const TriRec*)bvh->tris, rays_o, rays_d, num_rays, max_t, w.counts, w.status + 1);
   A3D_TRY((device_exclusive_scan<int32_t, int64_t>(w.counts, offsets_out, num_rays, w.scan_tmp,
                                                    offsets_out + num_rays, s)));
   return A3D_OK;
@@ -547,8 +547,8 @@ extern "C" int a3d_ray_all_collect(const a3d_bvh_view* bvh, const float* rays_o,
   A3D_REQUIRE(rays_o && rays_d && offsets && ray_idx && t && face_ids && sign, A3D_ERR_ARGUMENT,
               "ray_all: null pointer");
   const AllOut out{ray_idx, t, face_ids, sign, hit_points, uvw};
-  A3D_PDL(ray_all_collect_kernel, dim3((unsigned)ceil_div(num_rays, 128)), dim3(128), 0, s, 
-      (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, rays_o, rays_d, num_rays, max_t, offsets, out);
+  A3D_PDL(ray_all_collect_kernel, dim3((unsigned)ceil_div(num_rays, 128)), dim3(128), 0, s, (const WideNode*)bvh->nodes,
+          (const TriRec*)bvh->tris, rays_o, rays_d, num_rays, max_t, offsets, out);
   return A3D_OK;
 }
 
@@ -563,9 +563,8 @@ extern "C" int a3d_ray_parity_votes(const a3d_bvh_view* bvh, const float* points
   A3D_CUDA_TRY(cudaMemsetAsync(w.status, 0, 4 * sizeof(uint32_t), s));
   if (num_points == 0) return A3D_OK;
   A3D_REQUIRE(points && dirs && votes, A3D_ERR_ARGUMENT, "ray_parity: null pointer");
-  A3D_PDL(ray_parity_kernel, dim3((unsigned)ceil_div(num_points, 64)), dim3(64), 0, s, 
-      (const WideNode*)bvh->nodes, (const TriRec*)bvh->tris, points, num_points, dirs, num_dirs, max_t, coalesce_t,
-      votes, w.status + 1);
+  A3D_PDL(ray_parity_kernel, dim3((unsigned)ceil_div(num_points, 64)), dim3(64), 0, s, (const WideNode*)bvh->nodes,
+          (const TriRec*)bvh->tris, points, num_points, dirs, num_dirs, max_t, coalesce_t, votes, w.status + 1);
   return A3D_OK;
 }
 

@@ -949,8 +949,8 @@ int launch_udf(const TreeT<kBatch>& T, const float* pts, int64_t n, const uint32
   // threads for a few percent of the queries, each thread strides
   const int64_t rr_min = (int64_t)num_sms() * 256;
   const int64_t rr_threads = n / 16 > rr_min ? n / 16 : rr_min;
-  A3D_PDL((udf_rerun_kernel<kSign, kStats, kBatch>), dim3((unsigned)ceil_div(rr_threads, 64)), dim3(64), 0, s, 
-      T, pts, w.rerun, w.nrerun, out, sg, stats, w.nrerun + 1, w.nrerun + 4, sel);
+  A3D_PDL((udf_rerun_kernel<kSign, kStats, kBatch>), dim3((unsigned)ceil_div(rr_threads, 64)), dim3(64), 0, s, T, pts,
+          w.rerun, w.nrerun, out, sg, stats, w.nrerun + 1, w.nrerun + 4, sel);
   return A3D_OK;
 }
 
@@ -1053,8 +1053,8 @@ extern "C" int a3d_udf(const a3d_bvh_view* bvh, const float* points, int64_t num
     const float lo[3] = {0.5f * (bvh->lo[0] + bvh->hi[0]) - emax, 0.5f * (bvh->lo[1] + bvh->hi[1]) - emax,
                          0.5f * (bvh->lo[2] + bvh->hi[2]) - emax};
     const float inv = 1023.0f / (2.0f * emax);
-    A3D_PDL(query_morton_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, s, points, n, lo[0], lo[1], lo[2], inv, inv, inv,
-                                                                   w.keys, w.vals);
+    A3D_PDL(query_morton_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, s, points, n, lo[0], lo[1], lo[2], inv,
+            inv, inv, w.keys, w.vals);
     bool alt = false;
     A3D_TRY(radix_sort_pairs<uint32_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, n, 0, 32, w.rs_scratch, &alt, s));
     perm = alt ? w.vals_alt : w.vals;
@@ -1098,8 +1098,8 @@ extern "C" int a3d_udf_backward(const float* points, int64_t num_points, const f
   A3D_REQUIRE(points && closest_points && grad_dist, A3D_ERR_ARGUMENT, "udf_backward: null input");
   A3D_REQUIRE(!grad_vertices || (face_ids && uvw && faces), A3D_ERR_ARGUMENT,
               "udf_backward: vertex adjoint needs face ids, uvw and faces");
-  A3D_PDL(udf_backward_kernel, dim3((unsigned)ceil_div(num_points, 256)), dim3(256), 0, s, 
-      points, num_points, closest_points, face_ids, uvw, grad_dist, faces, grad_points, grad_vertices);
+  A3D_PDL(udf_backward_kernel, dim3((unsigned)ceil_div(num_points, 256)), dim3(256), 0, s, points, num_points,
+          closest_points, face_ids, uvw, grad_dist, faces, grad_points, grad_vertices);
   return A3D_OK;
 }
 
@@ -1200,8 +1200,8 @@ int batch_udf(const a3d_bvh_batch* bvh, const float* points, const int64_t* qoff
   for (int64_t base = 0; base < n; base += kBatchChunk) {
     const int64_t cn = n - base < kBatchChunk ? n - base : kBatchChunk;
     const float* pts = points + 3 * base;
-    A3D_PDL(batch_query_morton_kernel, dim3((unsigned)ceil_div(cn, 256)), dim3(256), 0, s, pts, cn, base, qoff, bvh->num_meshes,
-                                                                          bvh->bounds, bits, w.keys, w.vals);
+    A3D_PDL(batch_query_morton_kernel, dim3((unsigned)ceil_div(cn, 256)), dim3(256), 0, s, pts, cn, base, qoff,
+            bvh->num_meshes, bvh->bounds, bits, w.keys, w.vals);
     bool alt = false;
     A3D_TRY(radix_sort_pairs<uint32_t>(w.keys, w.vals, w.keys_alt, w.vals_alt, cn, 0, 3 * bits + mbits,
                                        w.rs_scratch, &alt, s));
@@ -1318,8 +1318,8 @@ extern "C" int a3d_batch_autotune(const a3d_bvh_batch* bvh, const float* points,
   carve_tune(t, ws, ns, bvh->num_meshes);
   A3D_REQUIRE(workspace && ws.ok(), A3D_ERR_WORKSPACE, "batch_autotune: workspace too small");
   const int64_t th = ns > (int64_t)bvh->num_meshes + 1 ? ns : (int64_t)bvh->num_meshes + 1;
-  A3D_PDL(sample_queries_kernel, dim3((unsigned)ceil_div(th, 256)), dim3(256), 0, s, points, stride, query_offsets, bvh->num_meshes,
-                                                                    t.pts, ns, t.qoff);
+  A3D_PDL(sample_queries_kernel, dim3((unsigned)ceil_div(th, 256)), dim3(256), 0, s, points, stride, query_offsets,
+          bvh->num_meshes, t.pts, ns, t.qoff);
   int occ = 0;
   A3D_TRY((task_blocks_per_sm<false, false, true>(&occ)));
   const int pools[4] = {32, 64, 128, 256};
