@@ -103,15 +103,29 @@ __global__ void scan_tile_sums_kernel(T* __restrict__ sums, int64_t nb, T* __res
 // owning kScanItems consecutive elements (one padding slot per 32 keeps the
 // per-thread reads off a single bank).  out may alias in: a block reads its
 // whole tile before writing it.
+//
+// kFused: tile_offsets holds the raw tile sums of scan_tile_reduce_kernel and
+// each block adds up those before its own (at most kScanFuseTiles of them,
+// read from L2), so the single-block scan of the tile sums is skipped; the
+// last block writes the total.
 __host__ __device__ constexpr int scan_pad(int i) { return i + (i >> 5); }
+constexpr int64_t kScanFuseTiles = 2048;
 
-template <typename TIn, typename T>
+template <typename TIn, typename T, bool kFused>
 __global__ void scan_tile_down_kernel(const TIn* __restrict__ in, T* __restrict__ out, int64_t n,
-                                      const T* __restrict__ tile_offsets) {
+                                      const T* __restrict__ tile_offsets, T* __restrict__ total) {
   pdl_wait();
   __shared__ T s_warp[kBlockScanSlots];
   __shared__ T s_tile[scan_pad(kScanTile)];
   const int64_t base = (int64_t)blockIdx.x * kScanTile;
+  T offset;
+  if constexpr (kFused) {
+    T part = 0;
+    for (int64_t b = threadIdx.x; b < (int64_t)blockIdx.x; b += kScanThreads) part += tile_offsets[b];
+    block_exclusive_scan<T>(part, s_warp, &offset);
+  } else {
+    offset = tile_offsets[blockIdx.x];
+  }
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     const int li = i * kScanThreads + threadIdx.x;
@@ -127,7 +141,9 @@ __global__ void scan_tile_down_kernel(const TIn* __restrict__ in, T* __restrict_
     vals[i] = s_tile[scan_pad(threadIdx.x * kScanItems + i)];
     acc += vals[i];
   }
-  T run = block_exclusive_scan<T>(acc, s_warp, (T*)nullptr) + tile_offsets[blockIdx.x];
+  T tile_total;
+  T run = block_exclusive_scan<T>(acc, s_warp, &tile_total) + offset;
+  if (kFused && total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *total = offset + tile_total;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     s_tile[scan_pad(threadIdx.x * kScanItems + i)] = run;
@@ -145,8 +161,11 @@ __global__ void scan_tile_down_kernel(const TIn* __restrict__ in, T* __restrict_
 inline size_t scan_workspace_elems(int64_t n) { return (size_t)ceil_div(n > 0 ? n : 1, kScanTile) + 1; }
 
 // Exclusive scan of in[0..n) into out (may alias in).  tmp must hold
-// scan_workspace_elems(n) elements of T; tmp[num_tiles] receives the total on
-// the device (total_dev, if non-null, also receives it).
+// scan_workspace_elems(n) elements of T; the total goes to total_dev on the
+// device, or to tmp[num_tiles] when total_dev is null.  Up to
+// kScanFuseTiles tiles (4M elements) the scan is two launches (tile sums,
+// then the tiles with their offsets summed in each block), above it three
+// (the tile sums scanned by one block in between).
 template <typename TIn, typename T>
 int device_exclusive_scan(const TIn* in, T* out, int64_t n, T* tmp, T* total_dev, cudaStream_t s) {
   if (n <= 0) {
@@ -156,10 +175,17 @@ int device_exclusive_scan(const TIn* in, T* out, int64_t n, T* tmp, T* total_dev
   const int64_t nb = ceil_div(n, kScanTile);
   // The down pass reads thread-contiguous items, the reduce pass strided
   // items: both cover the same tile so tile sums agree.
-  // the three passes back to back with programmatic dependent launch
+  // the passes back to back with programmatic dependent launch
+  T* total = total_dev ? total_dev : tmp + nb;
   A3D_PDL(scan_tile_reduce_kernel<TIn, T>, dim3((unsigned)nb), dim3(kScanThreads), 0, s, in, n, tmp);
-  A3D_PDL(scan_tile_sums_kernel<T>, dim3(1), dim3(1024), 0, s, tmp, nb, total_dev ? total_dev : tmp + nb);
-  A3D_PDL(scan_tile_down_kernel<TIn, T>, dim3((unsigned)nb), dim3(kScanThreads), 0, s, in, out, n, tmp);
+  if (nb <= kScanFuseTiles) {
+    A3D_PDL((scan_tile_down_kernel<TIn, T, true>), dim3((unsigned)nb), dim3(kScanThreads), 0, s, in, out, n,
+            (const T*)tmp, total);
+  } else {
+    A3D_PDL(scan_tile_sums_kernel<T>, dim3(1), dim3(1024), 0, s, tmp, nb, total);
+    A3D_PDL((scan_tile_down_kernel<TIn, T, false>), dim3((unsigned)nb), dim3(kScanThreads), 0, s, in, out, n,
+            (const T*)tmp, (T*)nullptr);
+  }
   return A3D_OK;
 }
 

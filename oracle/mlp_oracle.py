@@ -3,7 +3,11 @@
 Forward and backward of x -> Fourier features (sin, cos of 2*pi*B x_hat)
 -> 3 ReLU layers -> linear head with the weighted squared loss used in
 training (weight under_weight where the prediction is below the target).
-Used to check the GPU training kernels' gradients.
+Used to check the GPU training kernels' gradients.  With ``act_round``
+(a rounding function, BF16 in the tests) the oracle rounds the tensors the
+training kernels store in BF16 between their GEMMs: the features, the three
+activations and the three masked activation gradients; everything else
+stays FP64.
 """
 
 import numpy as np
@@ -18,15 +22,16 @@ def features(x, norm, freq):
     return f
 
 
-def forward_backward(x, target, P, norm, freq, under_weight=4.0):
+def forward_backward(x, target, P, norm, freq, under_weight=4.0, act_round=None):
     """P: dict W1 [64,128], W2, W3 [128,128], b1, b2, b3, w4 [128], b4 [1]."""
-    f = features(x, norm, freq)
+    r = act_round if act_round is not None else (lambda a: a)
+    f = r(features(x, norm, freq))
     z1 = f @ P["W1"] + P["b1"]
-    h1 = np.maximum(z1, 0)
+    h1 = r(np.maximum(z1, 0))
     z2 = h1 @ P["W2"] + P["b2"]
-    h2 = np.maximum(z2, 0)
+    h2 = r(np.maximum(z2, 0))
     z3 = h2 @ P["W3"] + P["b3"]
-    h3 = np.maximum(z3, 0)
+    h3 = r(np.maximum(z3, 0))
     y = h3 @ P["w4"] + P["b4"][0]
     n = x.shape[0]
     e = y - target
@@ -34,13 +39,13 @@ def forward_backward(x, target, P, norm, freq, under_weight=4.0):
     loss = float((w * e * e).sum() / n)
     dy = w * 2 * e / n
     G = {"w4": h3.T @ dy, "b4": np.array([dy.sum()])}
-    dz3 = np.outer(dy, P["w4"]) * (z3 > 0)
+    dz3 = r(np.outer(dy, P["w4"]) * (h3 > 0))
     G["W3"] = h2.T @ dz3
     G["b3"] = dz3.sum(0)
-    dz2 = (dz3 @ P["W3"].T) * (z2 > 0)
+    dz2 = r((dz3 @ P["W3"].T) * (h2 > 0))
     G["W2"] = h1.T @ dz2
     G["b2"] = dz2.sum(0)
-    dz1 = (dz2 @ P["W2"].T) * (z1 > 0)
+    dz1 = r((dz2 @ P["W2"].T) * (h1 > 0))
     G["W1"] = f.T @ dz1
     G["b1"] = dz1.sum(0)
     return y, loss, G

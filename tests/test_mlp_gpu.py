@@ -29,17 +29,26 @@ def test_training_gradients_match_fp64_oracle():
     torch.cuda.synchronize()
     P = {k: bf16_round(v.detach().cpu().numpy()) if k in ("W1", "W2", "W3") else v.detach().cpu().double().numpy()
          for k, v in lb.views.items()}
-    yr, lr_, G = O.forward_backward(x.cpu().numpy(), t.cpu().numpy(), P, lb.norm, lb.freq.cpu().numpy())
-    # BF16 activations on the GPU: compare with relative tolerances
-    assert np.abs(y.cpu().numpy() - yr).max() <= 0.03 * max(1.0, np.abs(yr).max())
-    assert abs(float(loss) - lr_) <= 0.05 * lr_ + 1e-6
+    xs, ts, fq = x.cpu().numpy(), t.cpu().numpy(), lb.freq.cpu().numpy()
+    # the oracle with the kernels' BF16 roundings (features, activations,
+    # activation gradients): only FP32 summation order and the odd rounding
+    # flip differ, so the bounds are tight
+    yr, lr_, G = O.forward_backward(xs, ts, P, lb.norm, fq, act_round=bf16_round)
+    err = {"y": np.abs(y.cpu().numpy() - yr).max() / max(1.0, np.abs(yr).max()),
+           "loss": abs(float(loss) - lr_) / (lr_ + 1e-6)}
+    assert err["y"] <= 5e-3 and err["loss"] <= 1e-2, err
+    # and the plain FP64 model, with the BF16 error budget
+    y64, l64, G64 = O.forward_backward(xs, ts, P, lb.norm, fq)
+    assert np.abs(y.cpu().numpy() - y64).max() <= 0.03 * max(1.0, np.abs(y64).max())
     off = 0
     for name in ("W1", "W2", "W3", "b1", "b2", "b3", "w4", "b4"):
         gg = lb.grads[off:off + G[name].size].view(G[name].shape).cpu().double().numpy()
         off += G[name].size
-        ref = G[name]
-        scale = np.abs(ref).max() + 1e-12
-        assert np.abs(gg - ref).max() <= 0.06 * scale, (name, np.abs(gg - ref).max(), scale)
+        scale = np.abs(G[name]).max() + 1e-12
+        err[name] = np.abs(gg - G[name]).max() / scale
+        assert err[name] <= 0.015, (name, err)
+        assert np.abs(gg - G64[name]).max() <= 0.06 * (np.abs(G64[name]).max() + 1e-12), name
+    print("relative errors against the BF16-rounding oracle:", {k: float(f"{v:.2e}") for k, v in err.items()})
 
 
 def test_inference_kernel_matches_training_forward():

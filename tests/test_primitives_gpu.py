@@ -1,7 +1,9 @@
 """The device-wide exclusive scan and radix sort at sizes where every part
 of the tile-sum pass is used: element counts whose tile count reaches the
-last warp of the 1024-thread tile-sum block, in several bucket sizes, and
-a sort whose digit histogram (256 x tiles entries) does the same."""
+last warp of the 1024-thread tile-sum block, in several bucket sizes, both
+sides of the 2,048-tile switch between the two-launch scan (offsets summed
+in each block) and the three-launch scan, and a sort whose digit histogram
+(256 x tiles entries) does the same."""
 
 import ctypes
 
@@ -27,7 +29,8 @@ def _scan(x: torch.Tensor) -> torch.Tensor:
 
 
 @pytest.mark.parametrize("n", [0, 1, 2047, 2049, 992 * TILE + 1, 1024 * TILE, 2 * 992 * TILE + 5,
-                               3 * 992 * TILE + 77, 6_195_477, 17 * 1000 * TILE + 3])
+                               3 * 992 * TILE + 77, 6_195_477, 2048 * TILE, 2048 * TILE + 1,
+                               17 * 1000 * TILE + 3])
 def test_exclusive_scan_matches_cumsum(n):
     g = torch.Generator(device="cuda")
     g.manual_seed(n)
