@@ -36,7 +36,7 @@ def test_training_gradients_match_fp64_oracle():
     yr, lr_, G = O.forward_backward(xs, ts, P, lb.norm, fq, act_round=bf16_round)
     err = {"y": np.abs(y.cpu().numpy() - yr).max() / max(1.0, np.abs(yr).max()),
            "loss": abs(float(loss) - lr_) / (lr_ + 1e-6)}
-    assert err["y"] <= 5e-3 and err["loss"] <= 1e-2, err
+    assert err["y"] <= 1e-2 and err["loss"] <= 1e-3, err
     # and the plain FP64 model, with the BF16 error budget
     y64, l64, G64 = O.forward_backward(xs, ts, P, lb.norm, fq)
     assert np.abs(y.cpu().numpy() - y64).max() <= 0.03 * max(1.0, np.abs(y64).max())
@@ -46,7 +46,7 @@ def test_training_gradients_match_fp64_oracle():
         off += G[name].size
         scale = np.abs(G[name]).max() + 1e-12
         err[name] = np.abs(gg - G[name]).max() / scale
-        assert err[name] <= 0.015, (name, err)
+        assert err[name] <= 3e-3, (name, err)
         assert np.abs(gg - G64[name]).max() <= 0.06 * (np.abs(G64[name]).max() + 1e-12), name
     print("relative errors against the BF16-rounding oracle:", {k: float(f"{v:.2e}") for k, v in err.items()})
 
