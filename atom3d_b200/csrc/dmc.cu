@@ -515,8 +515,10 @@ __device__ __forceinline__ float ldf(const float* p, int64_t i) { return __ldg(p
 // An edge's corner ids are the cube's own corner ids at the edge's two local
 // corners (the unique-edge key was made from them), read from the cube's
 // 64-B row of cube_idx, which stays in L1 for the vertex's edges, instead
-// of through the crossing's unique-edge index.
-__global__ void vd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
+// of through the crossing's unique-edge index.  Eight 128-thread blocks per
+// SM (<= 64 registers, no spills): the gathers are latency-bound, so the
+// resident warps (32 instead of 28 at 68 registers) set the throughput.
+__global__ void __launch_bounds__(128, 8) vd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
                           const uint8_t* __restrict__ case_s, const uint32_t* __restrict__ vd_cube,
                           const uint8_t* __restrict__ vd_slot, const uint32_t* __restrict__ goff, EdgeData ed,
                           VdOut out) {
@@ -734,7 +736,7 @@ __device__ __forceinline__ float bwd_dist(const BwdSlot& q, const float* vd) {
   return sqrtf(d2);
 }
 
-__global__ void __launch_bounds__(128) vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
+__global__ void __launch_bounds__(128, 8) vd_bwd_kernel(DmcIn in, int64_t nv, const uint32_t* __restrict__ list,
                                                      const uint8_t* __restrict__ case_s,
                                                      const uint32_t* __restrict__ vd_cube,
                                                      const uint8_t* __restrict__ vd_slot,
@@ -1590,8 +1592,9 @@ __device__ __forceinline__ void crossing_normal(const float* __restrict__ grad, 
 // one thread per dual vertex: crossings, normals, the QEF the reference
 // assembles (constraint j of k in row (j - (k-1)) mod 10; sqrt(lambda) at
 // (7,0) (8,1) (9,2) and rows 7-9 of b pulled to the cell centre), solved in
-// FP64; centroid when the solution is NaN or a cell outside the cell
-__global__ void vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float* __restrict__ grad, float lam,
+// FP64; centroid when the solution is NaN or a cell outside the cell.  Eight
+// 128-thread blocks per SM (<= 64 registers, no spills).
+__global__ void __launch_bounds__(128, 8) vd_qef_kernel(DmcIn in, const float* __restrict__ x, const float* __restrict__ grad, float lam,
                               int64_t nv, const uint32_t* __restrict__ list, const uint8_t* __restrict__ case_s,
                               const uint32_t* __restrict__ vd_cube, const uint8_t* __restrict__ vd_slot,
                               const uint32_t* __restrict__ goff, EdgeData ed, VdOut out) {
