@@ -24,7 +24,12 @@ namespace a3d {
 namespace {
 
 constexpr int kRayThreads = 128;
-constexpr int kRayShared = 32;   // shared-memory stack entries per ray
+// shared-memory stack entries per ray: 20 KB per 128-thread block, and the
+// nearest-hit kernel bounded to 48 registers, so that 10 blocks (40 warps)
+// are resident per SM; a ray that needs more entries is re-run with a deep
+// local stack
+constexpr int kRayShared = 20;
+constexpr int kRayBlocksPerSm = 10;
 constexpr int kRayDeep = 256;    // local-memory stack of the re-run kernel
 constexpr int kAllDepth = 192;   // node stack of the all-hit traversals
 constexpr int kParityCap = 256;  // hits per (point, direction) kept by the parity kernel
@@ -274,7 +279,7 @@ __device__ void write_nearest(const TriRec* __restrict__ tris, const float* __re
   }
 }
 
-__global__ void __launch_bounds__(kRayThreads)
+__global__ void __launch_bounds__(kRayThreads, kRayBlocksPerSm)
     ray_nearest_kernel(const WideNode* __restrict__ nodes, const TriRec* __restrict__ tris,
                        const float* __restrict__ face_normals, const float* __restrict__ ro,
                        const float* __restrict__ rd, int64_t n, float max_t, RayOut out, uint32_t* __restrict__ rerun,
