@@ -658,7 +658,8 @@ __global__ void write_tris_kernel(const float* __restrict__ V, const int64_t* __
 }
 
 // resident blocks of the SAH kernel on the current device (its shared
-// memory needs the opt-in above 48 KB), set up once per device
+// memory needs the opt-in above 48 KB), set up once per device and block size
+template <int kThreads>
 int sah_grid_size(int* grid) {
   static int cached[kMaxDevices] = {0};
   int dev = 0;
@@ -667,15 +668,27 @@ int sah_grid_size(int* grid) {
     *grid = cached[dev];
     return A3D_OK;
   }
-  A3D_CUDA_TRY(cudaFuncSetAttribute(sah_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(SahSmem)));
+  A3D_CUDA_TRY(cudaFuncSetAttribute(sah_cluster_kernel<kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(SahSmem<kThreads>)));
   int sms = 0, per_sm = 0;
   A3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sah_cluster_kernel, kSahThreads,
-                                                             sizeof(SahSmem)));
+  A3D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sah_cluster_kernel<kThreads>, kThreads,
+                                                             sizeof(SahSmem<kThreads>)));
   const int g = (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
   if (dev >= 0 && dev < kMaxDevices) cached[dev] = g;
   *grid = g;
+  return A3D_OK;
+}
+
+template <int kThreads>
+int launch_sah(int64_t n, BuildWs& w, const uint32_t* order, cudaStream_t s) {
+  int sah_grid = 0;
+  A3D_TRY(sah_grid_size<kThreads>(&sah_grid));
+  const int64_t max_clusters = n / 3 + 1;
+  A3D_PDL(sah_cluster_kernel<kThreads>, dim3((unsigned)(max_clusters < sah_grid ? max_clusters : sah_grid)),
+          dim3(kThreads), sizeof(SahSmem<kThreads>), s, w.clusters, w.ncl,
+          SahTree{w.left, w.right, w.parent, w.first, w.last, n}, const_cast<uint32_t*>(order), w.sah_tmp,
+          w.sah_small, SahPrims{w.centroid, w.tri_lo, w.tri_hi});
   return A3D_OK;
 }
 
@@ -710,12 +723,9 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
   A3D_CUDA_TRY(cudaMemsetAsync(w.ncl, 0, sizeof(uint32_t), s));
   A3D_PDL(sah_find_kernel, dim3(g), dim3(kThreads), 0, s, face_off, nmesh, n, w.parent, w.first, w.last, w.clusters,
           w.ncl);
-  int sah_grid = 0;
-  A3D_TRY(sah_grid_size(&sah_grid));
-  const int64_t max_clusters = n / 3 + 1;
-  A3D_PDL(sah_cluster_kernel, dim3((unsigned)(max_clusters < sah_grid ? max_clusters : sah_grid)), dim3(kSahThreads),
-          sizeof(SahSmem), s, w.clusters, w.ncl, SahTree{w.left, w.right, w.parent, w.first, w.last, n},
-          const_cast<uint32_t*>(order), w.sah_tmp, w.sah_small, SahPrims{w.centroid, w.tri_lo, w.tri_hi});
+  A3D_TRY(n <= (int64_t)kSahMax * num_sms()
+              ? launch_sah<kSahThreadsWide>(n, w, order, s)
+              : launch_sah<kSahThreadsNarrow>(n, w, order, s));
   A3D_CUDA_TRY(cudaMemsetAsync(w.visit, 0, sizeof(uint32_t) * n, s));
   A3D_PDL(refit_kernel, dim3(g), dim3(kThreads), 0, s, order, w.tri_lo, w.tri_hi, n, w.left, w.right, w.parent, w.first,
           w.last, leaf_max, w.box_lo, w.box_hi, w.dp_cost, w.dp_dec, w.visit);

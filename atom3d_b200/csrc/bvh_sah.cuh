@@ -35,12 +35,17 @@ namespace {
 constexpr int kSahMax = 16384;
 constexpr int kSahBins = 16;
 constexpr int kSahWarpMax = 128;
-constexpr int kSahThreads = 256;
-constexpr int kSahWarps = kSahThreads / 32;
+// block size of the cluster kernel: 1024 threads when the clusters are
+// about as many as the SMs (one mesh up to kSahMax x SMs triangles: each
+// block's 32 warps share out its small nodes), 256 when there are many
+// (batches: more blocks per SM, cheaper block-wide steps)
+constexpr int kSahThreadsWide = 1024;
+constexpr int kSahThreadsNarrow = 256;
 constexpr int kSahMaxDepth = 48;
 // nodes this small split at their median position: 2 = SAH all the way down
-// (median splits at 8 and below built the 1.31M-triangle tree in 7.1 ms
-// instead of 10.5 ms but cost 21 more triangle tests per query, +1.2% query time)
+// (median splits at 8 and below cut a third of the 256-thread build time of
+// the 1.31M-triangle tree but cost 21 more triangle tests per query, +1.2%
+// query time)
 constexpr int kSahTiny = 2;
 constexpr int kSahCand = 3 * (kSahBins - 1);            // 45 split candidates
 constexpr int kBinWords = 3 * kSahBins * 7;              // count, lo xyz, hi xyz
@@ -53,12 +58,14 @@ struct SahNode {
   int b, e, parent, sd;  // sd = side | depth << 1
 };
 
+template <int kThreads>
 struct SahSmem {
-  uint32_t bins[kSahWarps + 1][kBinWords];  // per warp, then the block's
-  SahNode wstack[kSahWarps][kSahWarpStack];
+  static constexpr int kWarps = kThreads / 32;
+  uint32_t bins[kWarps + 1][kBinWords];  // per warp, then the block's
+  SahNode wstack[kWarps][kSahWarpStack];
   SahNode bstack[kSahBlockStack];
-  float red[kSahWarps][6];
-  uint32_t wsum[kSahWarps];
+  float red[kWarps][6];
+  uint32_t wsum[kWarps];
   float cb[6];
   int nsmall, nb, m, axis, kk, root_nat;
 };
@@ -210,13 +217,15 @@ __device__ __forceinline__ void sah_emit(const SahTree& T, int f, int b, int m, 
 // (tmp: a scratch slice of the same positions); small nodes waiting for the
 // warps are listed in `small` at the cluster's positions (a cluster of n
 // triangles has fewer than n of them).
-__global__ void __launch_bounds__(kSahThreads)
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads)
     sah_cluster_kernel(const int32_t* __restrict__ clusters, const uint32_t* __restrict__ ncl, SahTree T,
                        uint32_t* __restrict__ order, uint32_t* __restrict__ tmp_all, SahNode* __restrict__ small_all,
                        SahPrims P) {
   pdl_wait();
   extern __shared__ __align__(16) unsigned char sah_raw[];
-  SahSmem& S = *reinterpret_cast<SahSmem*>(sah_raw);
+  constexpr int kWarps = kThreads / 32;
+  SahSmem<kThreads>& S = *reinterpret_cast<SahSmem<kThreads>*>(sah_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const unsigned FULL = 0xffffffffu;
   const uint32_t count = *ncl;
@@ -247,7 +256,7 @@ __global__ void __launch_bounds__(kSahThreads)
       const bool is_root = plabel < 0;
       // centroid bounds
       float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-      for (int i = b + tid; i < e; i += kSahThreads) {
+      for (int i = b + tid; i < e; i += kThreads) {
         const float4 c = __ldg(P.cen + ord[i]);
         mn[0] = fminf(mn[0], c.x); mn[1] = fminf(mn[1], c.y); mn[2] = fminf(mn[2], c.z);
         mx[0] = fmaxf(mx[0], c.x); mx[1] = fmaxf(mx[1], c.y); mx[2] = fmaxf(mx[2], c.z);
@@ -261,11 +270,11 @@ __global__ void __launch_bounds__(kSahThreads)
         }
       if (lane == 0)
         for (int a = 0; a < 3; ++a) { S.red[warp][a] = mn[a]; S.red[warp][3 + a] = mx[a]; }
-      sah_clear_bins(S.bins[kSahWarps], tid, kSahThreads);
+      sah_clear_bins(S.bins[kWarps], tid, kThreads);
       __syncthreads();
       if (tid < 6) {
         float v = S.red[0][tid];
-        for (int w = 1; w < kSahWarps; ++w) v = tid < 3 ? fminf(v, S.red[w][tid]) : fmaxf(v, S.red[w][tid]);
+        for (int w = 1; w < kWarps; ++w) v = tid < 3 ? fminf(v, S.red[w][tid]) : fmaxf(v, S.red[w][tid]);
         S.cb[tid] = v;
       }
       __syncthreads();
@@ -276,11 +285,11 @@ __global__ void __launch_bounds__(kSahThreads)
       for (int a = 0; a < 3; ++a) scale[a] = cb[3 + a] > cb[a] ? (float)kSahBins / (cb[3 + a] - cb[a]) : 0.f;
       const bool median = depth >= kSahMaxDepth;
       if (!median)
-        for (int i = b + tid; i < e; i += kSahThreads) sah_bin_prim(S.bins[kSahWarps], P, ord[i], cb, scale);
+        for (int i = b + tid; i < e; i += kThreads) sah_bin_prim(S.bins[kWarps], P, ord[i], cb, scale);
       __syncthreads();
       if (warp == 0) {
         int axis = 0, kk = 0, nl = 0;
-        if (!median) nl = sah_pick(S.bins[kSahWarps], cb, lane, axis, kk);
+        if (!median) nl = sah_pick(S.bins[kWarps], cb, lane, axis, kk);
         if (lane == 0) {
           S.m = nl > 0 ? b + nl : b + (e - b) / 2;
           S.axis = nl > 0 ? axis : -1;
@@ -292,7 +301,7 @@ __global__ void __launch_bounds__(kSahThreads)
       if (axis >= 0) {
         // stable partition: block-wide ranks of the left flags, chunk by chunk
         int lbase = b, rbase = m;
-        for (int i0 = b; i0 < e; i0 += kSahThreads) {
+        for (int i0 = b; i0 < e; i0 += kThreads) {
           const int i = i0 + tid;
           uint32_t p = 0;
           bool lft = false;
@@ -305,7 +314,7 @@ __global__ void __launch_bounds__(kSahThreads)
           if (lane == 0) S.wsum[warp] = (uint32_t)__popc(bl) | ((uint32_t)__popc(br) << 16);
           __syncthreads();
           int lb = 0, rb = 0, lt = 0, rt = 0;
-          for (int w = 0; w < kSahWarps; ++w) {
+          for (int w = 0; w < kWarps; ++w) {
             const uint32_t v = S.wsum[w];
             if (w < warp) { lb += (int)(v & 0xffffu); rb += (int)(v >> 16); }
             lt += (int)(v & 0xffffu);
@@ -320,7 +329,7 @@ __global__ void __launch_bounds__(kSahThreads)
           rbase += rt;
         }
         __syncthreads();
-        for (int i = b + tid; i < e; i += kSahThreads) ord[i] = tmp[i];
+        for (int i = b + tid; i < e; i += kThreads) ord[i] = tmp[i];
       }
       __syncthreads();
       if (tid == 0) {
@@ -339,7 +348,7 @@ __global__ void __launch_bounds__(kSahThreads)
     uint32_t* wb = S.bins[warp];
     SahNode* ws = S.wstack[warp];
     const int nsmall = S.nsmall;
-    for (int si = warp; si < nsmall; si += kSahWarps) {
+    for (int si = warp; si < nsmall; si += kWarps) {
       if (lane == 0) ws[0] = small[si];
       int sp = 1;
       __syncwarp();
