@@ -719,10 +719,15 @@ int build_wide_bvh(const float* V, const int64_t* vert_off, const int32_t* F, co
 
   A3D_PDL(radix_tree_kernel, dim3(g), dim3(kThreads), 0, s, keys, face_off, nmesh, n, w.left, w.right, w.parent,
           w.first, w.last);
-  // SAH refinement of every subtree of <= kSahMax triangles below the top
+  // SAH refinement of every subtree of <= sah_max triangles below the top:
+  // kSahMax from 64 x kSahMax triangles up, below it n / 64 rounded down to
+  // a power of two (at least 2,048), so that a small mesh still has about
+  // 64 clusters for the SMs
+  int sah_max = kSahMax;
+  while (sah_max > 2048 && (int64_t)sah_max * 64 > n) sah_max >>= 1;
   A3D_CUDA_TRY(cudaMemsetAsync(w.ncl, 0, sizeof(uint32_t), s));
-  A3D_PDL(sah_find_kernel, dim3(g), dim3(kThreads), 0, s, face_off, nmesh, n, w.parent, w.first, w.last, w.clusters,
-          w.ncl);
+  A3D_PDL(sah_find_kernel, dim3(g), dim3(kThreads), 0, s, face_off, nmesh, n, w.parent, w.first, w.last, sah_max,
+          w.clusters, w.ncl);
   A3D_TRY(n <= (int64_t)kSahMax * num_sms()
               ? launch_sah<kSahThreadsWide>(n, w, order, s)
               : launch_sah<kSahThreadsNarrow>(n, w, order, s));

@@ -435,11 +435,11 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// clusters: internal nodes of 3..kSahMax triangles whose parent has more (or
-// that are a mesh root)
+// clusters: internal nodes of 3..sah_max triangles whose parent has more (or
+// that are a mesh root); sah_max <= kSahMax
 __global__ void sah_find_kernel(const int64_t* __restrict__ face_off, int nmesh, int64_t n,
                                 const int32_t* __restrict__ parent, const int32_t* __restrict__ first,
-                                const int32_t* __restrict__ last, int32_t* __restrict__ clusters,
+                                const int32_t* __restrict__ last, int sah_max, int32_t* __restrict__ clusters,
                                 uint32_t* __restrict__ ncl) {
   pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -452,9 +452,9 @@ __global__ void sah_find_kernel(const int64_t* __restrict__ face_off, int nmesh,
   }
   if (i >= face_off[lo + 1] - 1) return;  // the last position of a range has no internal node
   const int cnt = last[i] - first[i] + 1;
-  if (cnt < 3 || cnt > kSahMax) return;
+  if (cnt < 3 || cnt > sah_max) return;
   const int p = parent[i];
-  if (p >= 0 && last[p] - first[p] + 1 <= kSahMax) return;
+  if (p >= 0 && last[p] - first[p] + 1 <= sah_max) return;
   clusters[atomicAdd(ncl, 1u)] = (int32_t)i;
 }
 
