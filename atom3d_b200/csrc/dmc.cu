@@ -345,9 +345,13 @@ __global__ void edge_scatter_kernel(const uint64_t* __restrict__ keys, const uin
   lo_g[p] = i0;
 }
 
+// Also writes the run-start flags of the sorted entries (entry j starts a
+// run of equal keys when j == 0 or key[j] != key[j - 1]): an entry starts
+// its run when no entry of its group has the same key and a smaller val.
 __global__ void edge_rank_kernel(const uint64_t* __restrict__ keys_g, const uint32_t* __restrict__ vals_g, int64_t nc,
                                  const uint32_t* __restrict__ lo_g, const uint32_t* __restrict__ start,
-                                 uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                                 uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                 uint32_t* __restrict__ run_flag) {
   pdl_wait();
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nc) return;
@@ -355,19 +359,16 @@ __global__ void edge_rank_kernel(const uint64_t* __restrict__ keys_g, const uint
   const uint32_t b = start[i0], e = start[i0 + 1];
   const uint64_t k = keys_g[p];
   const uint32_t v = vals_g[p];
-  uint32_t rank = 0;
+  uint32_t rank = 0, dup_before = 0;
   for (uint32_t q = b; q < e; ++q) {
     const uint64_t kq = keys_g[q];
-    rank += (kq < k || (kq == k && vals_g[q] < v)) ? 1u : 0u;
+    const bool same_before = kq == k && vals_g[q] < v;
+    rank += (kq < k || same_before) ? 1u : 0u;
+    dup_before += same_before ? 1u : 0u;
   }
   keys[b + rank] = k;
   vals[b + rank] = v;
-}
-
-__global__ void run_flag_kernel(const uint64_t* __restrict__ k, int64_t n, uint32_t* __restrict__ flag) {
-  pdl_wait();
-  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < n) flag[j] = (j == 0 || k[j] != k[j - 1]) ? 1u : 0u;
+  run_flag[b + rank] = dup_before == 0 ? 1u : 0u;
 }
 
 __global__ void run_info_kernel(const uint64_t* __restrict__ k, const uint32_t* __restrict__ v, int64_t n,
@@ -1235,12 +1236,15 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   A3D_TRY(fill_async<uint32_t>(w.ecnt, m, 0u, s));
   A3D_PDL(edge_scatter_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.rid, w.estart, w.ecnt, w.keys2,
           w.vals2, w.rflag);
-  A3D_PDL(edge_rank_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys2, w.vals2, nc, w.rflag, w.estart, w.keys, w.vals);
-  A3D_PDL(run_flag_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, nc, w.rflag);
-  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.rflag, w.rid, nc, w.scan_tmp, w.misc, s)));
+  // the run-start flags go to qflag, free until quad_flag_kernel rewrites it
+  // after run_info_kernel has read them (rflag still holds the lower
+  // endpoints edge_rank_kernel reads)
+  A3D_PDL(edge_rank_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys2, w.vals2, nc, w.rflag, w.estart, w.keys, w.vals,
+          w.qflag);
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.qflag, w.rid, nc, w.scan_tmp, w.misc, s)));
   // idx_map is read only at crossing (cube, edge) pairs, all of which
   // run_info_kernel writes: no clear
-  A3D_PDL(run_info_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.rflag, w.rid, m, w.idx_map, w.e0, w.e1,
+  A3D_PDL(run_info_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.qflag, w.rid, m, w.idx_map, w.e0, w.e1,
           w.rfirst);
   A3D_PDL(quad_flag_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.misc, nc, w.rfirst, w.qflag);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.qflag, w.qoff, nc, w.scan_tmp, w.qoff + nc, s)));
