@@ -371,10 +371,16 @@ __global__ void edge_rank_kernel(const uint64_t* __restrict__ keys_g, const uint
   run_flag[b + rank] = dup_before == 0 ? 1u : 0u;
 }
 
+// Per run of equal keys (a unique grid edge): its endpoints, its first
+// entry and its quad flag (the edge lies in 4 cubes, i.e. its run has 4
+// entries).  The quad flags cover all n >= ne entries (ne, the run count,
+// stays on the device): entries at ne and beyond get zero, so that the scan
+// can run over n.
 __global__ void run_info_kernel(const uint64_t* __restrict__ k, const uint32_t* __restrict__ v, int64_t n,
                                 const uint32_t* __restrict__ flag, const uint32_t* __restrict__ rid, int64_t m,
                                 int32_t* __restrict__ idx_map, int64_t* __restrict__ e0, int64_t* __restrict__ e1,
-                                uint32_t* __restrict__ rfirst) {
+                                uint32_t* __restrict__ rfirst, const uint32_t* __restrict__ ne_dev,
+                                uint32_t* __restrict__ qflag) {
   pdl_wait();
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
@@ -382,27 +388,16 @@ __global__ void run_info_kernel(const uint64_t* __restrict__ k, const uint32_t* 
   // is the number of starts up to and including j, minus one
   const uint32_t r = rid[j] + flag[j] - 1u;
   idx_map[v[j]] = (int32_t)r;
+  if (j >= (int64_t)*ne_dev) qflag[j] = 0u;
   if (flag[j]) {
-    e0[r] = (int64_t)(k[j] >> 32);
-    e1[r] = (int64_t)(k[j] & 0xffffffffull);
+    const uint64_t kj = k[j];
+    e0[r] = (int64_t)(kj >> 32);
+    e1[r] = (int64_t)(kj & 0xffffffffull);
     rfirst[r] = (uint32_t)j;
+    int64_t len = 1;
+    while (len < 5 && j + len < n && k[j + len] == kj) ++len;
+    qflag[r] = len == 4 ? 1u : 0u;
   }
-}
-
-// runs over nc >= ne entries (ne, the unique-edge count, stays on the device);
-// flags beyond ne are zero so the scan can run over nc
-__global__ void quad_flag_kernel(const uint32_t* __restrict__ ne_dev, int64_t nc, const uint32_t* __restrict__ rfirst,
-                                 uint32_t* __restrict__ qflag) {
-  pdl_wait();
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nc) return;
-  const int64_t ne = *ne_dev;
-  if (r >= ne) {
-    qflag[r] = 0;
-    return;
-  }
-  const int64_t end = r + 1 < ne ? rfirst[r + 1] : nc;
-  qflag[r] = (end - rfirst[r]) == 4 ? 1u : 0u;
 }
 
 // per-surface-cube dual-vertex bookkeeping (vertex count class 1..4)
@@ -1228,25 +1223,21 @@ extern "C" int a3d_dmc_prepare(const a3d_dmc_inputs* p, void* workspace, size_t 
   counts[0] = ns;
   counts[1] = nc;  // crossing (cube, edge) entries == groups
   if (ns == 0) return A3D_OK;
-  // counting sort of the crossings by (key, val); rid / rflag hold the
-  // lower endpoints until the run pass needs them
+  // counting sort of the crossings by (key, val); rid, then qflag, hold the
+  // lower endpoints until the rank pass has read them
   A3D_TRY(fill_async<uint32_t>(w.ecnt, m, 0u, s));
   A3D_PDL(edge_count_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, nc, (uint64_t)m, w.rid, w.ecnt);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.ecnt, w.estart, m, w.scan_tmp, w.estart + m, s)));
   A3D_TRY(fill_async<uint32_t>(w.ecnt, m, 0u, s));
   A3D_PDL(edge_scatter_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.rid, w.estart, w.ecnt, w.keys2,
-          w.vals2, w.rflag);
-  // the run-start flags go to qflag, free until quad_flag_kernel rewrites it
-  // after run_info_kernel has read them (rflag still holds the lower
-  // endpoints edge_rank_kernel reads)
-  A3D_PDL(edge_rank_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys2, w.vals2, nc, w.rflag, w.estart, w.keys, w.vals,
-          w.qflag);
-  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.qflag, w.rid, nc, w.scan_tmp, w.misc, s)));
+          w.vals2, w.qflag);
+  A3D_PDL(edge_rank_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys2, w.vals2, nc, w.qflag, w.estart, w.keys, w.vals,
+          w.rflag);
+  A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.rflag, w.rid, nc, w.scan_tmp, w.misc, s)));
   // idx_map is read only at crossing (cube, edge) pairs, all of which
-  // run_info_kernel writes: no clear
-  A3D_PDL(run_info_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.qflag, w.rid, m, w.idx_map, w.e0, w.e1,
-          w.rfirst);
-  A3D_PDL(quad_flag_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.misc, nc, w.rfirst, w.qflag);
+  // run_info_kernel writes: no clear.  The run count is in misc[0].
+  A3D_PDL(run_info_kernel, dim3(gsz(nc)), dim3(256), 0, s, w.keys, w.vals, nc, w.rflag, w.rid, m, w.idx_map, w.e0, w.e1,
+          w.rfirst, (const uint32_t*)w.misc, w.qflag);
   A3D_TRY((device_exclusive_scan<uint32_t, uint32_t>(w.qflag, w.qoff, nc, w.scan_tmp, w.qoff + nc, s)));
   // dual vertices numbered per vertex-count class (two packed scans)
   A3D_TRY(fill_async<uint32_t>(w.vd_ne, 4 * ns + 1, 0u, s));
